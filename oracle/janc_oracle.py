@@ -1,0 +1,784 @@
+"""CPU oracle: a NumPy float64 restatement of JANC's per-step reacting-flow
+path (``src/janc_v2`` of luofx23/JANC).
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` may import this module; the product
+(``janc_b200``) never calls it.
+
+Every function follows the reference array-for-array and keeps its operation
+order (Python left-to-right evaluation of the same expressions), so on the
+reference's golden vectors it agrees to the last bit except where libm
+``exp``/``log``/``pow`` or LAPACK's pivoted solve order differ.  Arrays use the
+reference layout: ``U`` is ``(nv, nx)`` in 1D and ``(nv, nx, ny)`` in 2D with
+``nv = 3 + 8`` resp. ``4 + 8``; ``aux`` is ``(2, ...)`` = ``[gamma, T]``.
+
+Cited reference files (paths inside the JANC repository):
+  preprocess/load.py, preprocess/nondim.py, model/thermo_model.py,
+  model/reaction_model.py, solver_{1D,2D}/aux_func.py,
+  solver_{1D,2D}/flux.py, solver_{1D,2D}/flux_splitting/LF.py,
+  solver_{1D,2D}/reconstruction/WENO5_JS.py, boundary/boundary.py,
+  boundary/boundary_padding.py, boundary/boundary_conditions_{1D,2D}/*.py,
+  simulation/time_step/TVD_RK3.py, simulation/set_simulator.py,
+  examples/janc_basic_example2.ipynb (rotating-detonation injector).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+import yaml
+
+RG = 8.314463  # preprocess/nondim.py:3
+MAX_ITER = 5   # model/thermo_model.py:17
+TOL = 5e-9     # model/thermo_model.py:18
+ATOMIC_WEIGHT = {"H": 1.008, "He": 4.002602, "C": 12.011, "N": 14.007, "O": 15.999, "Ar": 39.95}
+EA_TO_J_PER_KMOL = {"cal/mol": 4184.0, "kcal/mol": 4184000.0, "J/mol": 1000.0,
+                    "kJ/mol": 1.0e6, "J/kmol": 1.0}
+
+
+# --------------------------------------------------------------------------
+# reference scales  (preprocess/nondim.py:14-25)
+# --------------------------------------------------------------------------
+@dataclass
+class Nondim:
+    P0: float = 1.0
+    T0: float = 1.0
+    R0: float = 1.0
+    x0: float = 1.0
+
+    @property
+    def rho0(self):
+        return self.P0 / (self.R0 * self.T0)
+
+    @property
+    def M0(self):
+        return RG / self.R0
+
+    @property
+    def e0(self):
+        return self.P0 / self.rho0
+
+    @property
+    def u0(self):
+        return np.sqrt(self.P0 / self.rho0)
+
+    @property
+    def t0(self):
+        return self.x0 / self.u0
+
+
+# --------------------------------------------------------------------------
+# mechanism tables
+# --------------------------------------------------------------------------
+@dataclass
+class Mech:
+    species: list
+    nondim: Nondim
+    species_M: np.ndarray
+    Tcr: np.ndarray
+    cp_cof_low: np.ndarray
+    cp_cof_high: np.ndarray
+    dcp_cof_low: np.ndarray
+    dcp_cof_high: np.ndarray
+    h_cof_low: np.ndarray
+    h_cof_high: np.ndarray
+    h_cof_low_chem: np.ndarray
+    h_cof_high_chem: np.ndarray
+    s_cof_low: np.ndarray
+    s_cof_high: np.ndarray
+    logcof_low: np.ndarray
+    logcof_high: np.ndarray
+    A: np.ndarray
+    B: np.ndarray
+    EaR: np.ndarray
+    vf: np.ndarray
+    vb: np.ndarray
+    third_body: np.ndarray
+    is_third_body: np.ndarray
+    vsum: np.ndarray
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def ns(self):
+        return len(self.species)
+
+    @property
+    def nr(self):
+        return self.vf.shape[1]
+
+    def tables(self):
+        keys = ["species_M", "Tcr", "cp_cof_low", "cp_cof_high", "dcp_cof_low", "dcp_cof_high",
+                "h_cof_low", "h_cof_high", "h_cof_low_chem", "h_cof_high_chem", "s_cof_low",
+                "s_cof_high", "logcof_low", "logcof_high", "A", "B", "EaR", "vf", "vb",
+                "third_body", "is_third_body", "vsum"]
+        return {k: getattr(self, k) for k in keys}
+
+
+def _parse_side(side):
+    out, has_m = {}, False
+    for tok in side.split(" + "):
+        tok = tok.strip()
+        if tok == "M":
+            has_m = True
+            continue
+        parts = tok.split()
+        if len(parts) == 2:
+            nu, sp = float(parts[0]), parts[1]
+        else:
+            nu, sp = 1.0, tok
+        out[sp] = out.get(sp, 0.0) + nu
+    return out, has_m
+
+
+def load_mechanism(path, nondim=None):
+    """Cantera-style YAML -> the reference's constant tables.
+
+    Restates ``preprocess/load.py:8-135`` (``read_reaction_mechanism`` and
+    ``get_cantera_coeffs``) together with the Cantera 3.x conventions it relies
+    on (A to SI-kmol by (1e-3)**(order-1) for cm/mol input, Ea to J/kmol by
+    4184 per cal/mol, NASA7 coefficient packing, IUPAC atomic weights).
+    """
+    nd = nondim if isinstance(nondim, Nondim) else (Nondim(**nondim) if nondim else Nondim())
+    with open(path) as f:
+        doc = yaml.safe_load(f)
+    units = doc.get("units", {})
+    cgs = (units.get("length", "m"), units.get("quantity", "kmol")) == ("cm", "mol")
+    ea_f = EA_TO_J_PER_KMOL[units.get("activation-energy", "J/kmol")]
+    phase = doc["phases"][0]
+    species = list(phase["species"])
+    elements = list(phase["elements"])
+    sp_by = {s["name"]: s for s in doc["species"]}
+    ns = len(species)
+    # --- species thermo (load.py:91-135)
+    Tcr, low, high, MW = [], [], [], []
+    for name in species:
+        s = sp_by[name]
+        w = 0.0
+        for el in elements:
+            if el in s["composition"]:
+                w += s["composition"][el] * ATOMIC_WEIGHT[el]
+        MW.append(w)
+        th = s["thermo"]
+        Tcr.append(th["temperature-ranges"][1])
+        low.append(th["data"][0])
+        high.append(th["data"][1])
+    scale = np.array([[1, nd.T0, nd.T0 ** 2, nd.T0 ** 3, nd.T0 ** 4, 1 / nd.T0, 1]])
+    coeffs_low = np.array(low, dtype=np.float64) * scale
+    coeffs_high = np.array(high, dtype=np.float64) * scale
+    species_M = np.array(MW) / (1000 * nd.M0)
+    Tcr = np.array(Tcr, dtype=np.float64) / nd.T0
+    cp_cof_low = np.flip(coeffs_low[:, 0:5], axis=1) / species_M[:, None]
+    cp_cof_high = np.flip(coeffs_high[:, 0:5], axis=1) / species_M[:, None]
+    dcp_cof_low = cp_cof_low[:, 0:-1] * np.array([[4, 3, 2, 1]])
+    dcp_cof_high = cp_cof_high[:, 0:-1] * np.array([[4, 3, 2, 1]])
+    hw = np.array([[1 / 5, 1 / 4, 1 / 3, 1 / 2, 1, 1]])
+    h_cof_low = np.flip(np.roll(coeffs_low[:, 0:6], 1, axis=1), axis=1) * hw / species_M[:, None]
+    h_cof_high = np.flip(np.roll(coeffs_high[:, 0:6], 1, axis=1), axis=1) * hw / species_M[:, None]
+    h_cof_low_chem = np.flip(np.roll(coeffs_low[:, 0:6], 1, axis=1), axis=1) * hw
+    h_cof_high_chem = np.flip(np.roll(coeffs_high[:, 0:6], 1, axis=1), axis=1) * hw
+    sw = np.array([[1 / 4, 1 / 3, 1 / 2, 1, 1]])
+    s_cof_low = np.flip(np.concatenate([coeffs_low[:, -1:], coeffs_low[:, 1:5]], axis=1), axis=1) * sw
+    s_cof_high = np.flip(np.concatenate([coeffs_high[:, -1:], coeffs_high[:, 1:5]], axis=1), axis=1) * sw
+    logcof_low = coeffs_low[:, 0]
+    logcof_high = coeffs_high[:, 0]
+    # --- reactions (load.py:8-88)
+    rxns = doc.get("reactions", [])
+    nreac = len(rxns)
+    vf = np.zeros((nreac, ns))
+    vb = np.zeros((nreac, ns))
+    A, B, Ea = [], [], []
+    tb = np.zeros((nreac, ns))
+    is_tb = np.zeros(nreac)
+    idx = {n: i for i, n in enumerate(species)}
+    for i, r in enumerate(rxns):
+        eq = r["equation"]
+        for arrow in ("<=>", "=>", "="):
+            if arrow in eq:
+                lhs, rhs = eq.split(arrow)
+                break
+        reac, m_l = _parse_side(lhs)
+        prod, _ = _parse_side(rhs)
+        three = r.get("type", "elementary") == "three-body" or m_l
+        for sp, nu in reac.items():
+            vf[i, idx[sp]] = nu
+        for sp, nu in prod.items():
+            vb[i, idx[sp]] = nu
+        order = sum(reac.values())
+        if three:
+            order += 1
+            eff = r.get("efficiencies", {})
+            for j, sp in enumerate(species):
+                tb[i, j] = eff.get(sp, 1.0)
+        is_tb[i] = 1.0 * bool(np.any(tb[i, :] > 0))
+        rc = r["rate-constant"]
+        a_si = float(rc["A"]) * (1.0e-3) ** (order - 1) if cgs else float(rc["A"])
+        A.append(a_si * ((1e-3) ** (order - 1)))
+        B.append(float(rc["b"]))
+        Ea.append(float(rc["Ea"]) * ea_f / 1000)
+    nonzero = np.any(vf + vb != 0, axis=0)
+    vf = vf[:, nonzero]
+    vb = vb[:, nonzero]
+    vf_sum = np.sum(vf, axis=1)
+    vb_sum = np.sum(vb, axis=1)
+    A = np.array(A)
+    B = np.array(B)
+    Ea = np.array(Ea)
+    A = (nd.t0 / nd.rho0) * (nd.T0 ** B) * ((nd.rho0 / nd.M0) ** vf_sum) * nd.M0 * A
+    EaR = Ea / (nd.e0 * nd.M0)
+    tb = tb * (nd.rho0 / nd.M0)
+    return Mech(species, nd, species_M, Tcr, cp_cof_low, cp_cof_high, dcp_cof_low, dcp_cof_high,
+                h_cof_low, h_cof_high, h_cof_low_chem, h_cof_high_chem, s_cof_low, s_cof_high,
+                logcof_low, logcof_high, A, B, EaR, vf, vb, tb, is_tb, vb_sum - vf_sum,
+                extra={"MW": np.array(MW)})
+
+
+def _ex(v, nd):
+    """Broadcast a per-species column over ``nd`` spatial axes."""
+    return v.reshape(v.shape + (1,) * nd)
+
+
+# --------------------------------------------------------------------------
+# thermo  (model/thermo_model.py)
+# --------------------------------------------------------------------------
+def fill_Y(Y):
+    """thermo_model.py:80-82"""
+    return np.concatenate([Y, 1.0 - np.sum(Y, axis=0, keepdims=True)], axis=0)
+
+
+def get_R(m, Y):
+    """thermo_model.py:87-92"""
+    Yf = fill_Y(Y)
+    return np.sum(1 / _ex(m.species_M, Y.ndim - 1) * Yf, axis=0, keepdims=True)
+
+
+def _polyval(p, x):
+    y = np.zeros_like(x)
+    for c in p:
+        y = y * x + c
+    return y
+
+
+def get_thermo_properties(m, T):
+    """thermo_model.py:100-112 (T without the leading axis)."""
+    cp, dcp, h = [], [], []
+    for k in range(m.ns):
+        mask = T < m.Tcr[k]
+        cp.append(np.where(mask, _polyval(m.cp_cof_low[k], T), _polyval(m.cp_cof_high[k], T)))
+        dcp.append(np.where(mask, _polyval(m.dcp_cof_low[k], T), _polyval(m.dcp_cof_high[k], T)))
+        h.append(np.where(mask, _polyval(m.h_cof_low[k], T), _polyval(m.h_cof_high[k], T)))
+    return np.stack(cp), np.stack(dcp), np.stack(h)
+
+
+def get_thermo(m, T, Y):
+    """thermo_model.py:115-126 -> (cp, gamma, h, R, dcp)"""
+    R = get_R(m, Y)
+    Yf = fill_Y(Y)
+    cp_i, dcp_i, h_i = get_thermo_properties(m, T[0])
+    cp = np.sum(cp_i * Yf, axis=0, keepdims=True)
+    h = np.sum(h_i * Yf, axis=0, keepdims=True)
+    dcp = np.sum(dcp_i * Yf, axis=0, keepdims=True)
+    gamma = cp / (cp - R)
+    return cp, gamma, h, R, dcp
+
+
+def _e_eqn(m, T, e, Y):
+    """thermo_model.py:128-133"""
+    cp, gamma, h, R, dcp = get_thermo(m, T, Y)
+    res = (h - R * T) - e
+    return res, cp - R, dcp, gamma
+
+
+def get_T(m, e, Y, T0, return_iters=False):
+    """Halley solve with the reference's global stop test
+    (thermo_model.py:135-153): iterate while max|res| > tol and i < 5."""
+    res, d1, d2, gamma = _e_eqn(m, T0, e, Y)
+    T = T0
+    i = 0
+    while (np.max(np.abs(res)) > TOL) and (i < MAX_ITER):
+        dT = -2 * res * d1 / (2 * (d1 * d1) - res * d2)
+        T = T + dT
+        res, d1, d2, gamma = _e_eqn(m, T, e, Y)
+        i += 1
+    out = np.concatenate([gamma, T], axis=0)
+    return (out, i) if return_iters else out
+
+
+# --------------------------------------------------------------------------
+# conserved <-> primitive  (solver_{1D,2D}/aux_func.py)
+# --------------------------------------------------------------------------
+def nY_of(U):
+    return 3 if U.ndim == 2 else 4
+
+
+def update_aux(m, U, aux, return_iters=False):
+    """aux_func.py:21-28 (1D) / 21-29 (2D)"""
+    rho = U[0:1]
+    u = U[1:2] / rho
+    if U.ndim == 2:
+        e = U[2:3] / rho - 0.5 * (u ** 2)
+        Y = U[3:] / rho
+    else:
+        v = U[2:3] / rho
+        e = U[3:4] / rho - 0.5 * (u ** 2 + v ** 2)
+        Y = U[4:] / rho
+    r = get_T(m, e, Y, aux[1:2], return_iters)
+    if return_iters:
+        out, it = r
+        return out, it
+    return r
+
+
+def U_to_prim(m, U, aux):
+    """aux_func.py:39-50 (1D) / 39-51 (2D); returns (rho, u, [v,] Y, p, a)"""
+    gamma, T = aux[0:1], aux[1:2]
+    rho = U[0:1]
+    u = U[1:2] / rho
+    if U.ndim == 2:
+        Y = U[3:] / rho
+        R = get_R(m, Y)
+        p = rho * R * T
+        a = np.sqrt(gamma * p / rho)
+        return rho, u, Y, p, a
+    v = U[2:3] / rho
+    Y = U[4:] / rho
+    R = get_R(m, Y)
+    p = rho * R * T
+    a = np.sqrt(gamma * p / rho)
+    return rho, u, v, Y, p, a
+
+
+# --------------------------------------------------------------------------
+# chemistry  (model/reaction_model.py)
+# --------------------------------------------------------------------------
+def get_gibbs(m, T):
+    """reaction_model.py:78-89 for the nr reactive species; T without the
+    leading axis."""
+    out = []
+    for k in range(m.nr):
+        mask = T < m.Tcr[k]
+        h = np.where(mask, _polyval(m.h_cof_low_chem[k], T), _polyval(m.h_cof_high_chem[k], T))
+        s = np.where(mask, _polyval(m.s_cof_low[k], T) + m.logcof_low[k] * np.log((m.nondim.T0) * T),
+                     _polyval(m.s_cof_high[k], T) + m.logcof_high[k] * np.log((m.nondim.T0) * T))
+        out.append(s - h / T)
+    return np.stack(out)
+
+
+def construct_matrix_equation(m, T, X, dt):
+    """reaction_model.py:91-159: rates, analytic Jacobian and the 8x8 solve.
+    T is (1, ...), X is (ns, ...); returns drhoY (nr, ...)."""
+    nr, nreac = m.nr, len(m.A)
+    nd = T.ndim - 1
+    g = get_gibbs(m, T[0])                       # (nr, ...)
+    Xc = np.clip(X, 1e-50, None)
+    log_X = np.log(Xc[0:nr])
+    kf_l, kb_l, M_l = [], [], []
+    for i in range(nreac):
+        vf_i = _ex(m.vf[i], nd)
+        vb_i = _ex(m.vb[i], nd)
+        aij = _ex(m.third_body[i], nd)
+        kf_i = m.A[i] * np.power(T, m.B[i]) * np.exp(-m.EaR[i] / T)
+        aij_X_sum = np.sum(aij * X, axis=0, keepdims=True)
+        aij_X_sum = m.is_third_body[i] * aij_X_sum + (1 - m.is_third_body[i])
+        kf = kf_i * np.exp(np.sum(vf_i * log_X, axis=0, keepdims=True))
+        kb = kf_i / (np.exp(np.sum((vb_i - vf_i) * g, axis=0, keepdims=True))
+                     * ((101325 / m.nondim.P0 / T) ** m.vsum[i])) \
+            * np.exp(np.sum(vb_i * log_X, axis=0, keepdims=True))
+        kf_l.append(kf)
+        kb_l.append(kb)
+        M_l.append(aij_X_sum)
+    w = []
+    J = np.empty((nr, nr) + T.shape[1:])
+    for k in range(nr):
+        Mk = m.species_M[k]
+        terms = [(m.vb[i, k] - m.vf[i, k]) * M_l[i] * (kf_l[i] - kb_l[i]) for i in range(nreac)]
+        w.append(Mk * np.sum(np.stack(terms), axis=0)[0])
+        for n in range(nr):
+            Mn = m.species_M[n]
+            Xn = Xc[n][None]
+            tn = []
+            for i in range(nreac):
+                dv = m.vb[i, k] - m.vf[i, k]
+                ain = m.third_body[i, n]
+                tn.append(dv * (kf_l[i] - kb_l[i]) * (ain / Mn)
+                          + 1 / (Mn * Xn) * dv * M_l[i] * (m.vf[i, n] * kf_l[i] - m.vb[i, n] * kb_l[i]))
+            J[k, n] = Mk * np.sum(np.stack(tn), axis=0)[0]
+    S = np.moveaxis(np.stack(w), 0, -1)[..., None]               # (..., nr, 1)
+    DSDU = np.moveaxis(np.moveaxis(J, 0, -1), 0, -1)             # (..., nr, nr)
+    Amat = np.eye(nr) / dt - DSDU
+    x = np.linalg.solve(Amat, S)
+    return np.moveaxis(x[..., 0], -1, 0)
+
+
+def reaction_source_terms(m, U, aux, dt):
+    """reaction_model.py:183-193 (detailed_reaction)"""
+    nY = nY_of(U)
+    nd = U.ndim - 1
+    rho = U[0:1]
+    Y = fill_Y(U[nY:] / rho)
+    rhoY = rho * Y
+    T = aux[1:2]
+    X = rhoY / _ex(m.species_M, nd)
+    drhoY = construct_matrix_equation(m, T, X, dt)
+    dY = drhoY / rho
+    dY = np.clip(dY, -Y[0:-1], 1 - Y[0:-1])
+    return np.concatenate([np.zeros_like(U[:nY]), rho * dY], axis=0)
+
+
+# --------------------------------------------------------------------------
+# boundaries  (boundary/*.py and the RDC notebook injector)
+# --------------------------------------------------------------------------
+def _pressure_outlet_state(m, state, gamma, T, normal_vel, Pb):
+    """boundary_conditions_{1D,2D}/pressure_outlet.py:5-22"""
+    nY = nY_of(state) if state.ndim > 2 else 3
+    two_d = state.ndim == 3
+    rho = state[0:1]
+    u = state[1:2] / rho
+    v = state[2:3] / rho if two_d else None
+    Y = state[nY:] / rho
+    R = get_R(m, Y)
+    p = rho * (R * T)
+    a = np.sqrt(gamma * p / rho)
+    mask = normal_vel / a < 1
+    rho_c = np.where(mask, Pb / (p / rho), rho)
+    p_c = np.where(mask, Pb * np.ones_like(p), p)
+    T_c = np.where(mask, p_c / (rho_c * R), T)
+    _, gamma_c, h_c, _, _ = get_thermo(m, T_c, Y)
+    if two_d:
+        Ub = np.concatenate([rho_c, rho_c * u, rho_c * v,
+                             rho_c * h_c - p_c + 0.5 * rho_c * (u ** 2 + v ** 2), rho_c * Y], axis=0)
+    else:
+        Ub = np.concatenate([rho_c, rho_c * u, rho_c * h_c - p_c + 0.5 * rho_c * (u ** 2), rho_c * Y], axis=0)
+    return Ub, np.concatenate([gamma_c, T_c], axis=0)
+
+
+def inj_model(m, p, Y_inj):
+    """Injector pressure-feedback model of examples/janc_basic_example2.ipynb
+    (``inj_model``, after Fievisohn et al. 2017): 20 bisection steps on the
+    throat Mach number, nondimensional with manifold P0, T0."""
+    A1, A3 = 1, 5
+    A2 = A3 - A1
+    R = get_R(m, Y_inj)
+    gamma = 1.29
+    C0 = np.sqrt(gamma * R * 1.0)
+    P3 = p
+    M1 = np.zeros_like(p)
+    M2 = np.ones_like(p)
+    for _ in range(20):
+        M = 0.5 * (M1 + M2)
+        P1 = 1.0 * (1 + (gamma - 1) / 2 * M ** 2) ** (-gamma / (gamma - 1))
+        V1 = M * (1 + (gamma - 1) / 2 * M ** 2) ** (-0.5) * C0
+        MFC = A1 * 1.0 / np.sqrt(1.0) * np.sqrt(gamma / R) * M * (1 + (gamma - 1) / 2 * M ** 2) ** (-(gamma + 1) / 2 / (gamma - 1))
+        A = 0.5
+        B = gamma / (gamma - 1) * P3 * A3 / MFC
+        C = -gamma / (gamma - 1) * R * 1.0
+        V3 = (-B + np.sqrt(B ** 2 - 4 * A * C)) / (2 * A)
+        P2 = (MFC * (V3 - V1) - P1 * A1 + P3 * A3) / A2
+        M2 = np.where(P2 >= P1, M, M2)
+        M1 = np.where(P2 < P1, M, M1)
+    rho_c = MFC / V3 / A3
+    v_c = V3
+    T_c = p / (R * rho_c)
+    _, gamma_c, h_c, _, _ = get_thermo(m, T_c, Y_inj)
+    return v_c, T_c, h_c, gamma_c
+
+
+def _injector_state(m, state, aux, Yinj):
+    """``bottom_boundary`` of examples/janc_basic_example2.ipynb on the first
+    interior row; Yinj broadcasts as (8, nx, 1)."""
+    rho, u, v, Y, p, a = U_to_prim(m, state, aux)
+    T = aux[1:2]
+    gamma = aux[0:1]
+    _, _, h, R, _ = get_thermo(m, T, Y)
+    u_inj = np.zeros_like(u)
+    v_inj, T_inj, h_inj, g_inj = inj_model(m, p, Yinj)
+    R_inj = get_R(m, Yinj)
+    rho_inj = p / (R_inj * T_inj)
+    blk = p >= 1.0
+    rho_c = np.where(blk, rho, rho_inj)
+    u_c = np.where(blk, u, u_inj)
+    v_c = np.where(blk, -v, v_inj)
+    T_c = np.where(blk, T, T_inj)
+    p_c = p
+    h_c = np.where(blk, h, h_inj)
+    Y_c = np.where(np.tile(blk, (Yinj.shape[0], 1, 1)), Y, Yinj)
+    g_c = np.where(blk, gamma, g_inj)
+    Ub = np.concatenate([rho_c, rho_c * u_c, rho_c * v_c,
+                         rho_c * h_c - p_c + 0.5 * rho_c * (u_c ** 2 + v_c ** 2), rho_c * Y_c], axis=0)
+    return Ub, np.concatenate([g_c, T_c], axis=0)
+
+
+def _bc_side(m, kind, side, Ub, auxb, theta):
+    """One side's 3 ghost layers from the 3 boundary-adjacent layers
+    (boundary_conditions_{1D,2D}/*.py).  ``side`` in L/R/B/T; layers are
+    along axis 1 (L/R) or axis 2 (B/T), ordered as in the padded array."""
+    ax = 1 if side in "LR" else 2
+    lo = side in "LB"
+    two_d = Ub.ndim == 3
+
+    def take(a, j):
+        return np.take(a, [j], axis=ax)
+
+    def cat(parts):
+        return np.concatenate(parts, axis=ax)
+
+    if kind == "zero_gradient" or kind == "no_slip_wall":
+        order = [2, 1, 0] if lo else [-1, -2, -3]
+        U = cat([take(Ub, j) for j in order])
+        A = cat([take(auxb, j) for j in order])
+        if kind == "no_slip_wall":
+            U = U.copy()
+            if two_d:
+                U[1:3] *= -1
+            else:
+                U[1:2] *= -1
+        return U, A
+    if kind == "slip_wall":
+        j = 0 if lo else -1
+        U = cat([take(Ub, j)] * 3).copy()
+        A = cat([take(auxb, j)] * 3)
+        mom = 1 if (side in "LR") else 2
+        U[mom:mom + 1] *= -1
+        return U, A
+    if kind == "pressure_outlet":
+        j = 0 if lo else -1
+        st, ga, Tt = take(Ub, j), take(auxb[0:1], j), take(auxb[1:2], j)
+        mom = 1 if side in "LR" else 2
+        nv = st[mom:mom + 1] / st[0:1]
+        if lo:
+            nv = -nv
+        Us, As = _pressure_outlet_state(m, st, ga, Tt, nv, theta["Pb"])
+        return cat([Us] * 3), cat([As] * 3)
+    if kind == "rdc_injector":
+        assert side == "B" and two_d
+        st, au = Ub[:, :, 0:1], auxb[:, :, 0:1]
+        Yinj = np.asarray(theta["Yinj"])
+        if Yinj.ndim == 1:
+            Yinj = np.tile(Yinj[:, None, None], (1, Ub.shape[1], 1))
+        Us, As = _injector_state(m, st, au, Yinj)
+        return np.tile(Us, (1, 1, 3)), np.tile(As, (1, 1, 3))
+    raise KeyError(kind)
+
+
+def boundary_conditions(m, U, aux, bc, theta=None):
+    """Periodic pad (boundary_padding.py:4-25, node-periodic quirk), then
+    overwrite L, R (, B, T) in that order (boundary.py:120-132)."""
+    f = np.concatenate([U, aux], axis=0)
+    f = np.concatenate([f[:, -4:-3], f[:, -3:-2], f[:, -2:-1], f, f[:, 1:2], f[:, 2:3], f[:, 3:4]], axis=1)
+    two_d = U.ndim == 3
+    if two_d:
+        f = np.concatenate([f[:, :, -4:-3], f[:, :, -3:-2], f[:, :, -2:-1], f,
+                            f[:, :, 1:2], f[:, :, 2:3], f[:, :, 3:4]], axis=2)
+    Up, Ap = f[:-2].copy(), f[-2:].copy()
+    sides = (("L", "left_boundary"), ("R", "right_boundary"))
+    if two_d:
+        sides += (("B", "bottom_boundary"), ("T", "top_boundary"))
+    for s, key in sides:
+        kind = bc[key]
+        if kind == "periodic":
+            continue
+        if two_d:
+            sl = {"L": (slice(None), slice(3, 6), slice(3, -3)), "R": (slice(None), slice(-6, -3), slice(3, -3)),
+                  "B": (slice(None), slice(3, -3), slice(3, 6)), "T": (slice(None), slice(3, -3), slice(-6, -3))}[s]
+            dst = {"L": (slice(None), slice(0, 3), slice(3, -3)), "R": (slice(None), slice(-3, None), slice(3, -3)),
+                   "B": (slice(None), slice(3, -3), slice(0, 3)), "T": (slice(None), slice(3, -3), slice(-3, None))}[s]
+        else:
+            sl = {"L": (slice(None), slice(3, 6)), "R": (slice(None), slice(-6, -3))}[s]
+            dst = {"L": (slice(None), slice(0, 3)), "R": (slice(None), slice(-3, None))}[s]
+        Ug, Ag = _bc_side(m, kind, s, Up[sl], Ap[sl], theta)
+        Up[dst] = Ug
+        Ap[dst] = Ag
+    return Up, Ap
+
+
+# --------------------------------------------------------------------------
+# LF splitting + WENO5-JS  (flux_splitting/LF.py, reconstruction/WENO5_JS.py)
+# --------------------------------------------------------------------------
+_EPS, _C1, _C2, _C3 = 1e-6, 1 / 10, 3 / 5, 3 / 10
+
+
+def _sq(x):
+    """jnp.power(x, 2) with an integer exponent is x*x (lax.integer_pow)."""
+    return x * x
+
+
+def _weno_L(fjm2, fjm1, fj, fjp1, fjp2):
+    IS1 = 1 / 4 * _sq(fjm2 - 4 * fjm1 + 3 * fj) + 13 / 12 * _sq(fjm2 - 2 * fjm1 + fj)
+    IS2 = 1 / 4 * _sq(fjm1 - fjp1) + 13 / 12 * _sq(fjm1 - 2 * fj + fjp1)
+    IS3 = 1 / 4 * _sq(3 * fj - 4 * fjp1 + fjp2) + 13 / 12 * _sq(fj - 2 * fjp1 + fjp2)
+    a1 = _C1 / _sq(_EPS + IS1)
+    a2 = _C2 / _sq(_EPS + IS2)
+    a3 = _C3 / _sq(_EPS + IS3)
+    w1 = a1 / (a1 + a2 + a3)
+    w2 = a2 / (a1 + a2 + a3)
+    w3 = a3 / (a1 + a2 + a3)
+    q1 = 1 / 3 * fjm2 - 7 / 6 * fjm1 + 11 / 6 * fj
+    q2 = -1 / 6 * fjm1 + 5 / 6 * fj + 1 / 3 * fjp1
+    q3 = 1 / 3 * fj + 5 / 6 * fjp1 - 1 / 6 * fjp2
+    return w1 * q1 + w2 * q2 + w3 * q3
+
+
+def _weno_R(fjm2, fjm1, fj, fjp1, fjp2):
+    IS1 = 1 / 4 * _sq(fjp2 - 4 * fjp1 + 3 * fj) + 13 / 12 * _sq(fjp2 - 2 * fjp1 + fj)
+    IS2 = 1 / 4 * _sq(fjp1 - fjm1) + 13 / 12 * _sq(fjp1 - 2 * fj + fjm1)
+    IS3 = 1 / 4 * _sq(3 * fj - 4 * fjm1 + fjm2) + 13 / 12 * _sq(fj - 2 * fjm1 + fjm2)
+    a1 = _C1 / _sq(_EPS + IS1)
+    a2 = _C2 / _sq(_EPS + IS2)
+    a3 = _C3 / _sq(_EPS + IS3)
+    w1 = a1 / (a1 + a2 + a3)
+    w2 = a2 / (a1 + a2 + a3)
+    w3 = a3 / (a1 + a2 + a3)
+    q1 = 1 / 3 * fjp2 - 7 / 6 * fjp1 + 11 / 6 * fj
+    q2 = -1 / 6 * fjp1 + 5 / 6 * fj + 1 / 3 * fjm1
+    q3 = 1 / 3 * fj + 5 / 6 * fjm1 - 1 / 6 * fjm2
+    return w1 * q1 + w2 * q2 + w3 * q3
+
+
+def _interface_L(q, axis, other_interior):
+    """WENO5_JS.interface_L_{x,y}: face values from cells j-2..j+2."""
+    def s(a, b):
+        idx = [slice(None)] * q.ndim
+        idx[axis] = slice(a, b)
+        if other_interior is not None:
+            idx[other_interior] = slice(3, -3)
+        return q[tuple(idx)]
+    return _weno_L(s(0, -5), s(1, -4), s(2, -3), s(3, -2), s(4, -1))
+
+
+def _interface_R(q, axis, other_interior):
+    def s(a, b):
+        idx = [slice(None)] * q.ndim
+        idx[axis] = slice(a, b)
+        if other_interior is not None:
+            idx[other_interior] = slice(3, -3)
+        return q[tuple(idx)]
+    return _weno_R(s(1, -4), s(2, -3), s(3, -2), s(4, -1), s(5, None))
+
+
+def split_flux_1d(m, U, aux):
+    """solver_1D/flux_splitting/LF.py:4-13"""
+    rho, u, Y, p, a = U_to_prim(m, U, aux)
+    rhoE = U[2:3]
+    zx = 1.0
+    F = zx * np.concatenate([rho * u, rho * u ** 2 + p, u * (rhoE + p), rho * u * Y], axis=0)
+    um = zx * np.nanmax(abs(u) + a)
+    return 0.5 * (F + um * U), 0.5 * (F - um * U)
+
+
+def split_flux_2d(m, ixy, U, aux):
+    """solver_2D/flux_splitting/LF.py:4-16"""
+    rho, u, v, Y, p, a = U_to_prim(m, U, aux)
+    rhoE = U[3:4]
+    zx = (ixy == 1) * 1.0
+    zy = (ixy == 2) * 1.0
+    F = zx * np.concatenate([rho * u, rho * u ** 2 + p, rho * u * v, u * (rhoE + p), rho * u * Y], axis=0) \
+        + zy * np.concatenate([rho * v, rho * u * v, rho * v ** 2 + p, v * (rhoE + p), rho * v * Y], axis=0)
+    um = np.nanmax(abs(u) + a)
+    vm = np.nanmax(abs(v) + a)
+    th = zx * um + zy * vm
+    return 0.5 * (F + th * U), 0.5 * (F - th * U)
+
+
+def total_flux(m, Up, Ap, dx, dy=None):
+    """flux_splitting (solver_1D/flux.py:51-58, solver_2D/flux.py:56-68) on
+    the ghost-padded arrays; returns -(dF/dx [+ dG/dy])."""
+    if Up.ndim == 2:
+        Fplus, Fminus = split_flux_1d(m, Up, Ap)
+        F = _interface_L(Fplus, 1, None) + _interface_R(Fminus, 1, None)
+        dF = F[:, 1:] - F[:, :-1]
+        return -(dF / dx)
+    Fplus, Fminus = split_flux_2d(m, 1, Up, Ap)
+    Gplus, Gminus = split_flux_2d(m, 2, Up, Ap)
+    F = _interface_L(Fplus, 1, 2) + _interface_R(Fminus, 1, 2)
+    G = _interface_L(Gplus, 2, 1) + _interface_R(Gminus, 2, 1)
+    dF = F[:, 1:, :] - F[:, :-1, :]
+    dG = G[:, :, 1:] - G[:, :, :-1]
+    return -(dF / dx + dG / dy)
+
+
+# --------------------------------------------------------------------------
+# solver wiring  (simulation/set_simulator.py, time_step/TVD_RK3.py)
+# --------------------------------------------------------------------------
+class Solver:
+    """Configured oracle for one grid: ``flux_func``, ``update_func``,
+    ``advance_one_step`` and ``advance_func`` with the reference's
+    signatures (set_simulator.py:20-125, 410-447)."""
+
+    def __init__(self, mech, dim, dx, dy=None, bc=None, cfl=None):
+        self.m = mech
+        self.dim = dim
+        self.dx, self.dy = dx, dy
+        self.bc = bc
+        self.cfl = cfl
+        self.last_iters = []
+
+    def flux_func(self, U, aux, dx, dy, dt, theta=None):
+        Up, Ap = boundary_conditions(self.m, U, aux, self.bc, theta)
+        return dt * (total_flux(self.m, Up, Ap, dx, dy))
+
+    def update_func(self, U, aux):
+        out, it = update_aux(self.m, U, aux, return_iters=True)
+        self.last_iters.append(it)
+        return out
+
+    def rk3(self, U, aux, dx, dy, dt, theta, rhs_func=None, update_func=None):
+        """TVD_RK3.py:5-12"""
+        rhs_func = rhs_func or self.flux_func
+        update_func = update_func or self.update_func
+        U1 = U + rhs_func(U, aux, dx, dy, dt, theta)
+        aux1 = update_func(U1, aux)
+        U2 = 3 / 4 * U + 1 / 4 * (U1 + rhs_func(U1, aux1, dx, dy, dt, theta))
+        aux2 = update_func(U2, aux1)
+        U3 = 1 / 3 * U + 2 / 3 * (U2 + rhs_func(U2, aux2, dx, dy, dt, theta))
+        aux3 = update_func(U3, aux2)
+        return U3, aux3
+
+    def advance_one_step(self, U, aux, dx, dy, dt, theta=None):
+        """set_simulator.py:117-122 (Lie splitting: RK3 flux, chemistry, T)"""
+        U, aux = self.rk3(U, aux, dx, dy, dt, theta)
+        dU = reaction_source_terms(self.m, U, aux, dt)
+        U = U + dU
+        aux = self.update_func(U, aux)
+        return U, aux
+
+    def cfl_dt(self, U, aux):
+        """CFL_1D / CFL_2D, set_simulator.py:420-443"""
+        if U.ndim == 2:
+            _, u, _, _, a = U_to_prim(self.m, U, aux)
+            sx = np.abs(u) + a
+            return self.cfl * np.min(self.dx / sx)
+        _, u, v, _, _, a = U_to_prim(self.m, U, aux)
+        sx = np.abs(u) + a
+        sy = np.abs(v) + a
+        return self.cfl * np.min(1 / (sx / self.dx + sy / self.dy))
+
+    def advance_func(self, U, aux, t, theta=None):
+        dt = self.cfl_dt(U, aux)
+        U, aux = self.advance_one_step(U, aux, self.dx, self.dy, dt, theta)
+        return U, aux, t + dt, dt
+
+
+# --------------------------------------------------------------------------
+# initial-state builder (the examples' pattern)
+# --------------------------------------------------------------------------
+def state_from_PTY(m, P, T, Y, vel=None):
+    """rho = P/(R T), rhoE = rho h - P (+ kinetic), aux = [gamma, T]
+    (examples/janc_basic_example1.ipynb, ``initial_conditions``)."""
+    _, gamma, h, R, _ = get_thermo(m, T, Y)
+    rho = P / (R * T)
+    E = rho * h - P
+    nd = T.ndim - 1
+    if vel is None:
+        vel = [np.zeros_like(T) for _ in range(nd)]
+    for v in vel:
+        E = E + 0.5 * rho * v ** 2
+    U = np.concatenate([rho] + [rho * v for v in vel] + [E, rho * Y], axis=0)
+    return U, np.concatenate([gamma, T], axis=0)
+
+
+def stoich_Y(m, phi=1.0):
+    """H2:O2:N2 = 2 phi : 1 : 3.76 by mole -> the 8 carried mass fractions."""
+    W = {s: m.extra["MW"][i] for i, s in enumerate(m.species)}
+    n = {"H2": 2.0 * phi, "O2": 1.0, "N2": 3.76}
+    tot = sum(n[s] * W[s] for s in n)
+    Y = np.zeros(m.ns - 1)
+    Y[m.species.index("H2")] = n["H2"] * W["H2"] / tot
+    Y[m.species.index("O2")] = n["O2"] * W["O2"] / tot
+    return Y
