@@ -1,0 +1,470 @@
+#!/usr/bin/env python
+"""Benchmark: reacting cell-updates/s of JANC's per-step path on B200.
+
+Workload (one "step" = one full time step of the whole grid): the 2D H2-air
+detonation channel, 1024 x 256 cells over 0.2 m x 0.05 m, stoichiometric
+H2:O2:N2 = 2:1:3.76 at 1 atm / 300 K, at rest; an ignition slab over x-columns
+0..20 (2 % of 1024, rounded) at 30 atm and 3000 K with eight seeded Gaussian
+temperature blobs of +-5 % (radius 2-6 cells, numpy default_rng(1)); slip
+walls on all four sides; WENO5-JS + global Lax-Friedrichs splitting, SSP-RK3,
+point-implicit chemistry of the 9-species / 19-reaction mechanism; CFL time
+steps.  CFL is 0.1: at the stated CFL 0.5 the reference's own algorithm goes
+non-finite within ~17 steps (first-order point-implicit chemistry burns a
+slab-edge cell in one step; tests/golden/config0_cfl05.npz records it), and
+the work per step does not depend on the CFL number.
+
+Arms:
+  default            our CUDA path (fp64 unless --precision), device-timed
+                     with inputs resident (value) and end to end through the
+                     public API from pinned host buffers (e2e)
+  --impl reference   the reference algorithm's CPU implementation: the
+                     NumPy oracle restating src/janc_v2 (JAX is not available
+                     on the box), run as independent replicas on all host
+                     cores
+Multi-GPU: the path does not shard in this build (replicas only): each rank
+advances its own copy of the workload; value = total cells x steps / max time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY = 1024, 256
+LX, LY = 0.2, 0.05
+SLAB = 21
+CFL = 0.1
+METRIC = "reacting cell-updates/s"
+UNIT = "cell-updates/s"
+BYTES_CHEM_PER_CELL = 224      # read U,aux (112 B) + write U,aux (112 B), float64
+BYTES_STEP_PER_CELL = 864 + 224  # fused-step minimum + separate chemistry pass (2D)
+
+
+RDC_NX, RDC_NY = 1600, 1000
+RDC_ND = {"P0": 10 * 101325, "T0": 300, "R0": 369, "x0": 0.08}
+
+
+def rdc_fields(nx=RDC_NX, ny=RDC_NY):
+    """Rotating-detonation annulus (unrolled), nondimensional with the
+    injection-manifold scales of the reference's example 2: ambient air at
+    1 atm / 300 K; a fresh stoichiometric layer whose height falls linearly
+    from 360 cells at x = 0 to 0 at x = nx/2; a 40 x 100-cell kernel at the
+    bottom-left at 3000 K / 30 atm inside the layer.  Returns (P, T, Y, Yinj)."""
+    import numpy as np
+    P0, T0 = RDC_ND["P0"], RDC_ND["T0"]
+    yH2 = (1.0 / 8 * 0.232) / (1 + 1.0 / 8 * 0.232)
+    yO2 = 0.232 / (1 + 1.0 / 8 * 0.232)
+    Yenv = np.array([0, 0.232, 0, 0, 0, 0, 0, 0.0])
+    Yfill = np.array([yH2, yO2, 0, 0, 0, 0, 0, 0.0])
+    Yinj = np.concatenate([[yH2, yO2], 1e-20 * np.ones(6)])
+    x = np.arange(nx)[:, None]
+    y = np.arange(ny)[None, :]
+    height = np.maximum(0.0, 360.0 * (1.0 - x / (nx / 2)))
+    fresh = (y < height)
+    Y = np.where(fresh[None], Yfill[:, None, None], Yenv[:, None, None])
+    P = np.full((1, nx, ny), 101325.0 / P0)
+    T = np.full((1, nx, ny), 300.0 / T0)
+    P[0, :40, :100] = 30 * 101325.0 / P0
+    T[0, :40, :100] = 3000.0 / T0
+    return np.ascontiguousarray(P), np.ascontiguousarray(T), np.ascontiguousarray(Y), Yinj
+
+
+def c1_fields(nx=NX, ny=NY, slab=SLAB, seed=1):
+    """(P, T, Y) of the channel workload as float64 numpy arrays."""
+    import numpy as np
+    from janc_b200 import mechanism as jm
+    mech = jm.load()
+    rng = np.random.default_rng(seed)
+    P = np.full((1, nx, ny), 101325.0)
+    T = np.full((1, nx, ny), 300.0)
+    Y = np.ascontiguousarray(np.tile(jm.stoichiometric_Y(mech, 1.0)[:, None, None], (1, nx, ny)))
+    xs = np.arange(slab)[:, None]
+    ys = np.arange(ny)[None, :]
+    bump = np.zeros((slab, ny))
+    for _ in range(8):
+        a = rng.uniform(-0.05, 0.05)
+        sig = rng.uniform(2.0, 6.0)
+        cx = rng.uniform(0, slab)
+        cy = rng.uniform(0, ny)
+        bump += a * np.exp(-((xs - cx) ** 2 + (ys - cy) ** 2) / (2 * sig ** 2))
+    P[0, :slab] = 30 * 101325.0
+    T[0, :slab] = 3000.0 * (1 + bump)
+    return P, T, Y
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 1
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    lr = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(lr)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return dist, dist.get_rank(), ws
+
+
+def fp64_peak_tflops(L, torch):
+    """Measured FP64 FMA throughput of this device (TFLOP/s)."""
+    import ctypes
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    blocks = props.multi_processor_count * 8
+    iters = 2000
+    scratch = torch.empty(blocks, dtype=torch.float64, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ptr = ctypes.c_void_p(scratch.data_ptr())
+    for _ in range(2):
+        L.jb_probe_fp64_fma(blocks, iters, ptr, st)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        L.jb_probe_fp64_fma(blocks, iters, ptr, st)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    flops = blocks * 256.0 * iters * 16 * 8 * 2
+    return flops / (ms * 1e-3) / 1e12
+
+
+def chem_flops_per_cell():
+    """Algorithmic FP64 operations of one chemistry cell-update (+, -, x,
+    FMA = 1 each; exp/log/pow/div/sqrt counted separately), from the
+    mechanism's sparsity, as the kernel evaluates it."""
+    import numpy as np
+    from janc_b200 import mechanism as jm
+    t = jm.load().tables
+    vf, vb, tb = t["vf"], t["vb"], t["third_body"]
+    nreac, nr = vf.shape
+    ns = tb.shape[1]
+    arith, special = 0, 0
+    arith += 8 + ns * 2 + nr * 12 + 1   # fill_Y, X and clip, gibbs polynomials (h, s)
+    special += nr + 1 + nr * 1          # log X, log T, h/T
+    for i in range(nreac):
+        arith += 2 + 2 * ns + 2 + 3 * 2 * nr + 4   # kf_i, third body, exponent sums, kb
+        special += 5                               # pow, 3 exp, exp(-Ea/T), plus divisions below
+        for k in range(nr):
+            if vb[i, k] - vf[i, k] == 0:
+                continue
+            arith += 3
+            for n in range(nr):
+                if tb[i, n] != 0 or vf[i, n] != 0 or vb[i, n] != 0:
+                    arith += 8
+    arith += nr * nr + nr               # scale by M_k, A = I/dt - J
+    arith += 2 * nr ** 3 // 3 + nr ** 2  # LU + substitution
+    special += nr + nr                  # divisions by pivots, dY = x / rho
+    arith += 4 * nr                     # clip and S
+    arith += 5 * (3 * ns * 16)          # Halley iterates: 5 x thermo (cp, dcp, h over 9 species)
+    return arith, special
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from janc_b200.solver import Solver
+    from janc_b200 import _native
+
+    dist, rank, ws = _dist()
+    dev = torch.cuda.current_device()
+    theta = None
+    if args.workload == "channel":
+        nx, ny = NX, NY
+        dx, dy = LX / NX, LY / NY
+        bc = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
+        s = Solver(2, nx, ny, dx, dy, bc, precision=args.precision)
+        P, T, Y = c1_fields()
+        workload = ("2D H2-air detonation channel 1024x256 (0.2 m x 0.05 m), 9sp/19r mechanism, "
+                    "30 atm / 3000 K slab with 8 seeded +-5% blobs, slip walls, "
+                    "WENO5-JS + LF + SSP-RK3 + point-implicit chemistry")
+    else:
+        nx, ny = RDC_NX, RDC_NY
+        dx = dy = 1e-4 / RDC_ND["x0"]
+        bc = {"left_boundary": "periodic", "right_boundary": "periodic",
+              "bottom_boundary": "rdc_injector", "top_boundary": "pressure_outlet"}
+        s = Solver(2, nx, ny, dx, dy, bc, nondim_config=RDC_ND, precision=args.precision)
+        P, T, Y, Yinj = rdc_fields()
+        theta = {"Yinj": Yinj, "Pb": 101325.0 / RDC_ND["P0"]}
+        s.set_theta(theta)
+        workload = ("2D unrolled rotating-detonation annulus 1600x1000 (dx = 0.1 mm, nondimensional "
+                    "P0 = 10 atm, T0 = 300 K, R0 = 369, x0 = 0.08 m), periodic x, choked-injector "
+                    "bottom, pressure outlet top (Pb = 1 atm), linear reactant layer, 40x100 kernel")
+    U0, aux0 = s.state_from_PTY(torch.tensor(P, device="cuda"), torch.tensor(T, device="cuda"),
+                                torch.tensor(Y, device="cuda"))
+    ncell = nx * ny
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    # advance the state past the initial transient so the timed steps see a
+    # burning slab; then time single steps (each one kernel sequence)
+    U, aux, _ = s.advance(U0, aux0, max(args.warmup, 3), cfl=CFL, theta=theta)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    t_wall0 = time.time()
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record()
+        U, aux, _ = s.advance(U, aux, 1, cfl=CFL, theta=theta)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    t_wall = time.time() - t_wall0
+    clk = clocks.stop()
+    ms_steps = [a.elapsed_time(b) for a, b in ev]
+    ms_total = sum(ms_steps)
+    status = s.status()
+    if dist:
+        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_per_step = ms_total / args.steps
+    value = ws * ncell * args.steps / (ms_total * 1e-3)
+
+    # per-kernel split over further steps (events around each launch)
+    s.set_kernel_timing(True)
+    kt_steps = min(args.steps, 5)
+    acc = {"flux": [0.0, 0], "select": [0.0, 0], "chem": [0.0, 0], "other": [0.0, 0]}
+    for _ in range(kt_steps):
+        flush.zero_()
+        U, aux, _ = s.advance(U, aux, 1, cfl=CFL, theta=theta)
+        for kk, (ms, n) in s.kernel_times().items():
+            acc[kk][0] += ms
+            acc[kk][1] += n
+        s.set_kernel_timing(True)
+    s.set_kernel_timing(False)
+    kernel_ms = {k: v[0] / kt_steps for k, v in acc.items()}
+    chem_ms = acc["chem"][0] / max(acc["chem"][1], 1)
+    L = _native.lib()
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak, hbm_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        try:
+            hbm_peak = float(json.load(open(peaks_path))["hbm_gbs"])
+            hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except Exception:
+            pass
+    fp64_peak = fp64_peak_tflops(L, torch)
+    arith, special = chem_flops_per_cell()
+    chem_gbs = BYTES_CHEM_PER_CELL * ncell / (chem_ms * 1e-3) / 1e9
+    chem_tflops = arith * ncell / (chem_ms * 1e-3) / 1e12
+    step_gbs = BYTES_STEP_PER_CELL * ncell / (ms_per_step * 1e-3) / 1e9
+
+    # end to end through the public API: pinned host state in, state out
+    hU = U.cpu().pin_memory()
+    haux = aux.cpu().pin_memory()
+    oU = torch.empty_like(hU).pin_memory()
+    oaux = torch.empty_like(haux).pin_memory()
+    e2e_steps = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        dU = hU.to("cuda", non_blocking=True)
+        daux = haux.to("cuda", non_blocking=True)
+        rU, raux, _ = s.advance(dU, daux, 1, cfl=CFL, theta=theta)
+        oU.copy_(rU, non_blocking=True)
+        oaux.copy_(raux, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = ws * ncell * e2e_steps / (e2e_ms * 1e-3)
+    hbytes = (hU.numel() + haux.numel()) * 8
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "channel":
+        cpu = cpu_baseline(args.cpu_steps)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "precision": args.precision,
+        "config": {"workload": workload, "cells": ncell, "cfl": CFL, "precision": args.precision,
+                   "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+        "status_bits": status,
+        "kernel_ms_per_step": kernel_ms,
+        "gpu_launches": 11 * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "k_chem (point-implicit chemistry + final Halley)",
+                     "achieved": chem_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": chem_gbs / hbm_peak, "traffic": None,
+                     "peak_source": hbm_src,
+                     "algorithmic_bytes_per_cell": BYTES_CHEM_PER_CELL,
+                     "launch_ms": chem_ms,
+                     "step_achieved_gbs": step_gbs,
+                     "step_algorithmic_bytes_per_cell": BYTES_STEP_PER_CELL},
+        "compute_roofline": {"bound": "fp64", "kernel": "k_chem", "achieved": chem_tflops,
+                             "peak": fp64_peak, "unit": "TFLOP/s", "frac": chem_tflops / fp64_peak,
+                             "peak_source": "measured live (jb_probe_fp64_fma)",
+                             "flops_per_cell": arith, "special_ops_per_cell": special},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": hbytes, "d2h_bytes_per_step": hbytes,
+                "steps": e2e_steps},
+        "clocks": clk,
+        "wall_s_timed_region": t_wall,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- CPU side
+def _oracle_replica(args):
+    """One replica: the NumPy oracle advancing a 32 x 256 strip of the channel
+    (slab columns included, same boundaries and CFL) for `steps` steps."""
+    nx, steps = args
+    import warnings
+    import numpy as np
+    warnings.simplefilter("ignore")
+    sys.path.insert(0, ROOT)
+    from oracle import janc_oracle as jo
+    from janc_b200.mechanism import DEFAULT_MECHANISM
+    m = jo.load_mechanism(DEFAULT_MECHANISM)
+    P, T, Y = c1_fields(nx=nx, ny=NY)
+    U, aux = jo.state_from_PTY(m, P, T, Y)
+    bc = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
+    s = jo.Solver(m, "2D", LX / NX, LY / NY, bc, CFL)
+    U, aux, t, _ = s.advance_func(U, aux, 0.0)  # warm-up step
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        U, aux, t, _ = s.advance_func(U, aux, t)
+    return time.perf_counter() - t0, nx * NY * steps
+
+
+def cpu_baseline(steps):
+    """The oracle on all host cores as independent replicas (spawned
+    processes, one BLAS thread each); returns the cpu_baseline record."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    nrep = max(1, min(cores, 64))
+    nx = 32
+    env_keep = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
+    for k in env_keep:
+        os.environ[k] = "1"
+    t0 = time.perf_counter()
+    with cf.ProcessPoolExecutor(nrep, mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_oracle_replica, [(nx, steps)] * nrep))
+    wall = time.perf_counter() - t0
+    for k, v in env_keep.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v
+    slowest = max(r[0] for r in res)
+    cells = sum(r[1] for r in res)
+    return {"value": cells / slowest, "unit": UNIT, "cores": nrep, "kind": "port",
+            "sample": f"{nrep} replicas x {nx}x{NY} cells x {steps} steps of the same channel physics "
+                      f"(NumPy oracle restating src/janc_v2; one process per core)",
+            "wall_s": wall}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 20))
+    cpu = cpu_baseline(steps)
+    line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT,
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "2D H2-air detonation channel (strips of 32x256 cells of the 1024x256 "
+                                   "workload), CPU reference path", "cfl": CFL},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "JAX is not installed here; the reference's CPU path is the NumPy oracle, a "
+                    "bitwise-pinned restatement of src/janc_v2 (tests/test_oracle_golden.py)"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_strict", "mixed"])
+    ap.add_argument("--workload", default="channel", choices=["channel", "rdc"])
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,115 @@
+/*
+ * janc_b200 C ABI: the per-step reacting-flow path of JANC (luofx23/JANC,
+ * src/janc_v2) on NVIDIA B200 (sm_100a).
+ *
+ * All arrays are device pointers to C-contiguous float64 in the reference's
+ * layout:
+ *   U    [nv][nx][ny]  nv = 12 in 2D: rho, rho*u, rho*v, rho*E, rho*Y_1..8
+ *                      nv = 11 in 1D (ny = 1): rho, rho*u, rho*E, rho*Y_1..8
+ *   aux  [2][nx][ny]   gamma, T
+ * Species order is the mechanism's; the last species (N2) is implicit,
+ * Y_N2 = 1 - sum(Y).  Every call is asynchronous on the given CUDA stream
+ * (a cudaStream_t passed as void*; NULL = legacy default stream), allocates
+ * nothing, and returns 0 or a jb_status bit set.  The handle owns only its
+ * tables and a workspace sized at jb_create; it never frees caller memory.
+ * Calls on one handle are stream-ordered and not thread-safe.
+ */
+#ifndef JANC_B200_H
+#define JANC_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#include "../janc_b200/csrc/jb_types.h"
+
+typedef struct jb_handle jb_handle;
+
+/* Library version string. */
+const char* jb_version(void);
+
+/* Configure one solver: mechanism tables (preprocess/load.py:8-135 packing,
+ * already non-dimensionalised), grid, the four side boundary kinds
+ * (jb_bc_kind; 1D uses bc[0..1]) and the arithmetic variant (jb_precision).
+ * Replaces the module-global set_thermo / set_reaction / set_flux_solver /
+ * set_boundary calls made by Simulator.__init__
+ * (src/janc_v2/simulation/set_simulator.py:384-390). */
+int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, double dy,
+              const int bc[4], int precision, jb_handle** out);
+int jb_destroy(jb_handle* h);
+
+/* theta of the reference's boundary callables: pressure_outlet back pressure
+ * 'Pb' (boundary_conditions_2D/pressure_outlet.py:25) and the injector's
+ * 'Yinj' [8][nx] device array (examples/janc_basic_example2.ipynb) with the
+ * blocked-injector pressure (1.0 in the notebook's nondimensional units). */
+int jb_set_theta(jb_handle* h, double Pb, const double* Yinj, double inj_block_p);
+
+/* flux_func(U, aux, dx, dy, dt, theta) -> dt * total_flux(BC(U, aux))
+ * (src/janc_v2/simulation/set_simulator.py:26-29 1D, :44-47 2D). */
+int jb_flux_func(jb_handle* h, const double* U, const double* aux, double dt, double* rhs,
+                 void* stream);
+
+/* update_aux(U, aux) -> aux (src/janc_v2/solver_2D/aux_func.py:21-29,
+ * solver_1D/aux_func.py:21-28; Halley solve thermo_model.py:135-153 with the
+ * reference's global stopping rule). */
+int jb_update_aux(jb_handle* h, const double* U, const double* aux_in, double* aux_out,
+                  void* stream);
+
+/* reaction_source_terms(U, aux, dt) -> dU
+ * (src/janc_v2/model/reaction_model.py:202-203 -> detailed_reaction :183-193). */
+int jb_reaction_source_terms(jb_handle* h, const double* U, const double* aux, double dt,
+                             double* S, void* stream);
+
+/* nsteps of advance_one_step (set_simulator.py:117-122: SSP-RK3 flux stages
+ * TVD_RK3.py:5-12, chemistry, temperature solve).  cfl > 0: each step's dt is
+ * cfl * min(...) as Simulator.advance_func (set_simulator.py:420-447);
+ * otherwise dt_fixed.  dt_hist (device, nsteps doubles, may be NULL) receives
+ * each step's dt.  U/aux are not modified; U_out/aux_out receive the result. */
+int jb_advance(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
+               double dt_fixed, double cfl, int nsteps, double* dt_hist, void* stream);
+
+/* CFL_1D / CFL_2D (set_simulator.py:420-443): *dt_out (device) =
+ * cfl * min(dx/(|u|+a)) resp. cfl * min(1/((|u|+a)/dx + (|v|+a)/dy)). */
+int jb_cfl_dt(jb_handle* h, const double* U, const double* aux, double cfl, double* dt_out,
+              void* stream);
+
+/* get_thermo(T, Y) -> cp, gamma, h, R, dcp for n points
+ * (src/janc_v2/model/thermo_model.py:115-126); Y is [8][n]. */
+int jb_get_thermo(jb_handle* h, long long n, const double* T, const double* Y, double* cp,
+                  double* gamma, double* hh, double* R, double* dcp, void* stream);
+
+/* Synchronise `stream` and return the device status bits accumulated since
+ * the last call (non-finite state, singular chemistry matrix), then clear. */
+int jb_status(jb_handle* h, unsigned* status, void* stream);
+
+/* Bytes of device workspace the handle holds. */
+long long jb_workspace_bytes(const jb_handle* h);
+
+/* Change the grid spacing of a configured handle (the reference passes dx, dy
+ * on every call: set_simulator.py:26,44). */
+int jb_set_spacing(jb_handle* h, double dx, double dy);
+
+/* sizeof(jb_mech_params) and sizeof(jb_grid) as compiled, for binding checks. */
+int jb_sizeof_mech_params(void);
+int jb_sizeof_grid(void);
+
+/* Measurement helpers (no reference counterpart).  jb_set_kernel_timing
+ * enables CUDA events around each launch of jb_advance (at most JB_TIMED_MAX
+ * launches between reads) and clears the totals; jb_kernel_times waits for
+ * the recorded events and returns accumulated milliseconds and launch counts
+ * per jb_kernel_cat (arrays of JB_KCAT_COUNT). */
+int jb_set_kernel_timing(jb_handle* h, int enable);
+int jb_kernel_times(jb_handle* h, double* ms, long long* launches);
+
+/* Measurement helper (no reference counterpart): launches `blocks` x 256
+ * threads, each doing iters*128 float64 FMAs (2 FLOP each), for measuring
+ * the device's FP64 peak.  `scratch` is a device buffer of `blocks` doubles. */
+int jb_probe_fp64_fma(int blocks, int iters, double* scratch, void* stream);
+
+/* Human-readable description of the last error on this handle. */
+const char* jb_last_error(const jb_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JANC_B200_H */

@@ -1,0 +1,80 @@
+"""ctypes binding of the C ABI in ``include/janc_b200.h``.
+
+The shared library is built in-tree (``janc_b200/libjanc_b200.so``) by
+``janc_b200._build``.  There is no CPU fallback: every compute entry point
+needs the library and a CUDA device, and a missing library raises.
+"""
+import ctypes
+import os
+
+from . import mechanism as _mech
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libjanc_b200.so")
+
+BC_KIND = {"periodic": 0, "slip_wall": 1, "zero_gradient": 2, "no_slip_wall": 3,
+           "pressure_outlet": 4, "rdc_injector": 5}
+PRECISION = {"fp64_strict": 0, "fp64": 1, "mixed": 2}
+STATUS = {1: "bad argument", 2: "CUDA error", 4: "non-finite state", 8: "singular chemistry matrix",
+          16: "device wait timed out", 32: "unsupported configuration"}
+
+EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_func", "jb_update_aux",
+           "jb_reaction_source_terms", "jb_advance", "jb_cfl_dt", "jb_get_thermo", "jb_status",
+           "jb_workspace_bytes", "jb_set_spacing", "jb_sizeof_mech_params", "jb_sizeof_grid",
+           "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times"]
+
+_lib = None
+
+
+class JancError(RuntimeError):
+    pass
+
+
+def status_text(code):
+    return ", ".join(v for k, v in STATUS.items() if code & k) or "ok"
+
+
+def lib(path=None):
+    """Load (once) and return the shared library with argument types set."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise JancError(f"janc_b200 native library not found at {p}; build it with "
+                        "`python -m janc_b200._build` (nvcc, sm_100a)")
+    L = ctypes.CDLL(p)
+    vp, dp, i, d, ll = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+    L.jb_version.restype = ctypes.c_char_p
+    L.jb_create.argtypes = [ctypes.POINTER(_mech.MechParams), i, i, i, d, d, ctypes.POINTER(ctypes.c_int),
+                            i, ctypes.POINTER(vp)]
+    L.jb_destroy.argtypes = [vp]
+    L.jb_set_theta.argtypes = [vp, d, dp, d]
+    L.jb_flux_func.argtypes = [vp, dp, dp, d, dp, vp]
+    L.jb_update_aux.argtypes = [vp, dp, dp, dp, vp]
+    L.jb_reaction_source_terms.argtypes = [vp, dp, dp, d, dp, vp]
+    L.jb_advance.argtypes = [vp, dp, dp, dp, dp, d, d, i, dp, vp]
+    L.jb_cfl_dt.argtypes = [vp, dp, dp, d, dp, vp]
+    L.jb_get_thermo.argtypes = [vp, ll, dp, dp, dp, dp, dp, dp, dp, vp]
+    L.jb_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), vp]
+    L.jb_workspace_bytes.argtypes = [vp]
+    L.jb_workspace_bytes.restype = ll
+    L.jb_set_spacing.argtypes = [vp, d, d]
+    L.jb_probe_fp64_fma.argtypes = [i, i, dp, vp]
+    L.jb_set_kernel_timing.argtypes = [vp, i]
+    L.jb_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
+    L.jb_last_error.argtypes = [vp]
+    L.jb_last_error.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        getattr(L, name)
+    if L.jb_sizeof_mech_params() != ctypes.sizeof(_mech.MechParams):
+        raise JancError("jb_mech_params layout mismatch between Python and the library")
+    _lib = L
+    return L
+
+
+def check(rc, handle=None, what=""):
+    if rc != 0:
+        msg = ""
+        if handle is not None:
+            msg = lib().jb_last_error(handle).decode()
+        raise JancError(f"{what} failed: {status_text(rc)} (code {rc}) {msg}".strip())

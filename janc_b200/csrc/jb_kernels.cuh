@@ -1,0 +1,1096 @@
+// JANC per-step hot path as sm_100a kernels.
+//
+// This header is compiled twice: jb_strict.cu (namespace jb::strict, built
+// with -fmad=false so every expression rounds exactly as the reference's
+// float64 array code does) and jb_fast.cu (namespace jb::fast, FMA
+// contraction allowed).  Each function cites the reference file it restates
+// (paths inside the JANC repository, src/janc_v2/...).
+//
+// Data layout (the reference's, C-contiguous float64):
+//   U   [nv][nx][ny]   nv = 4 + 8 in 2D (rho, rho u, rho v, rho E, rho Y_1..8)
+//                      nv = 3 + 8 in 1D (ny == 1)
+//   aux [2][nx][ny]    gamma, T
+//   cand[6][nx][ny]    Halley iterates T_0..T_5 of the last temperature solve
+//   strips[4][nv+2][L] ghost states of pressure-outlet / injector sides
+//                      (L = max(nx, ny)); fields U..., gamma, T
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "jb_types.h"
+
+#ifndef JB_NS
+#error "define JB_NS before including jb_kernels.cuh"
+#endif
+
+namespace jb {
+namespace JB_NS {
+
+constexpr int NS = 9;
+constexpr int NR = 8;
+constexpr int NREAC = 19;
+constexpr double HALLEY_TOL = 5e-9;  // model/thermo_model.py:18
+constexpr int HALLEY_MAX = 5;        // model/thermo_model.py:17
+
+typedef jb_mech_params MP;
+
+typedef jb_grid Grid;
+typedef jb_slots Slots;
+
+__device__ __forceinline__ unsigned long long dbits(double x) {
+  return (unsigned long long)__double_as_longlong(x);
+}
+__device__ __forceinline__ double bitsd(unsigned long long b) {
+  return __longlong_as_double((long long)b);
+}
+
+// ---------------------------------------------------------------------------
+// block reductions
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ unsigned warp_or(unsigned v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// All threads of the block must call; returns the result in thread 0.
+__device__ __forceinline__ void block_reduce_store(double ax, double ay, double dtm,
+                                                   unsigned bits, Slots* s, int aidx,
+                                                   bool do_alpha, bool do_dt, int midx) {
+  __shared__ double rax[32], ray[32], rdt[32];
+  __shared__ unsigned rbits[32];
+  ax = warp_max(ax);
+  ay = warp_max(ay);
+  dtm = warp_min(dtm);
+  bits = warp_or(bits);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { rax[w] = ax; ray[w] = ay; rdt[w] = dtm; rbits[w] = bits; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int nw = (blockDim.x + 31) >> 5;
+    for (int i = 1; i < nw; ++i) {
+      ax = fmax(ax, rax[i]); ay = fmax(ay, ray[i]); dtm = fmin(dtm, rdt[i]); bits |= rbits[i];
+    }
+    if (do_alpha) {
+      if (ax > 0.0) atomicMax(&s->ax[aidx], dbits(ax));
+      if (ay > 0.0) atomicMax(&s->ay[aidx], dbits(ay));
+    }
+    if (do_dt) atomicMin(&s->dtmin_next, dbits(dtm));
+    if (midx >= 0 && (bits & 0xffffu)) atomicOr(&s->mask[midx], bits & 0xffffu);
+    if (bits >> 16) atomicOr(&s->status, bits >> 16);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// NASA7 thermo (model/thermo_model.py:80-133)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double poly4(const double* c, double T) {
+  double y = c[0];
+  y = y * T + c[1];
+  y = y * T + c[2];
+  y = y * T + c[3];
+  return y;
+}
+__device__ __forceinline__ double poly5(const double* c, double T) {
+  double y = c[0];
+  y = y * T + c[1];
+  y = y * T + c[2];
+  y = y * T + c[3];
+  y = y * T + c[4];
+  return y;
+}
+__device__ __forceinline__ double poly6(const double* c, double T) {
+  double y = c[0];
+  y = y * T + c[1];
+  y = y * T + c[2];
+  y = y * T + c[3];
+  y = y * T + c[4];
+  y = y * T + c[5];
+  return y;
+}
+
+// fill_Y (thermo_model.py:80-82): the last species closes the mass balance.
+__device__ __forceinline__ void fill_Y(const double* Y8, double* Yf) {
+  double s = Y8[0];
+#pragma unroll
+  for (int k = 1; k < NR; ++k) s = s + Y8[k];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Yf[k] = Y8[k];
+  Yf[NR] = 1.0 - s;
+}
+
+// get_R (thermo_model.py:87-92): R = sum_k (1/M_k) Y_k
+__device__ __forceinline__ double get_R(const MP& m, const double* Yf) {
+  double r = m.invM[0] * Yf[0];
+#pragma unroll
+  for (int k = 1; k < NS; ++k) r = r + m.invM[k] * Yf[k];
+  return r;
+}
+
+struct Th {
+  double cp, h, dcp;
+};
+
+// get_thermo_nasa7 mixture sums (thermo_model.py:100-126)
+__device__ __forceinline__ Th thermo_mix(const MP& m, double T, const double* Yf) {
+  Th t;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    const bool lo = T < m.Tcr[k];
+    double cpk = lo ? poly5(m.cp_lo[k], T) : poly5(m.cp_hi[k], T);
+    double dck = lo ? poly4(m.dcp_lo[k], T) : poly4(m.dcp_hi[k], T);
+    double hk = lo ? poly6(m.h_lo[k], T) : poly6(m.h_hi[k], T);
+    if (k == 0) {
+      t.cp = cpk * Yf[0]; t.h = hk * Yf[0]; t.dcp = dck * Yf[0];
+    } else {
+      t.cp = t.cp + cpk * Yf[k]; t.h = t.h + hk * Yf[k]; t.dcp = t.dcp + dck * Yf[k];
+    }
+  }
+  return t;
+}
+
+__device__ __forceinline__ double cp_mix(const MP& m, double T, const double* Yf) {
+  double cp = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    const bool lo = T < m.Tcr[k];
+    double cpk = lo ? poly5(m.cp_lo[k], T) : poly5(m.cp_hi[k], T);
+    cp = (k == 0) ? cpk * Yf[0] : cp + cpk * Yf[k];
+  }
+  return cp;
+}
+
+// Halley iterates of the temperature solve (thermo_model.py:135-153).  The
+// reference stops all cells together when max|res| <= tol, so every cell
+// runs the five iterations, keeps T_0..T_5, and reports per iteration whether
+// its residual exceeded tol (bits 0..4) or was NaN (bits 8..12).  The
+// iteration count is fixed later from the OR of all cells' masks.
+__device__ __forceinline__ unsigned halley_iterates(const MP& m, double e, const double* Yf,
+                                                    double R, double T0, double* cand) {
+  unsigned bits = 0;
+  double T = T0;
+  cand[0] = T;
+#pragma unroll
+  for (int i = 0; i < HALLEY_MAX; ++i) {
+    Th t = thermo_mix(m, T, Yf);
+    double res = (t.h - R * T) - e;
+    double d1 = t.cp - R;
+    double d2 = t.dcp;
+    if (fabs(res) > HALLEY_TOL) bits |= 1u << i;
+    if (res != res) bits |= 1u << (8 + i);
+    double dT = ((-2.0 * res) * d1) / ((2.0 * (d1 * d1)) - res * d2);
+    T = T + dT;
+    cand[i + 1] = T;
+  }
+  return bits;
+}
+
+// Number of Halley iterations the reference's global while-loop performs.
+__device__ __forceinline__ int halley_count(unsigned word) {
+  for (int i = 0; i < HALLEY_MAX; ++i) {
+    bool any_gt = (word >> i) & 1u;
+    bool any_nan = (word >> (8 + i)) & 1u;
+    if (!any_gt || any_nan) return i;
+  }
+  return HALLEY_MAX;
+}
+
+// ---------------------------------------------------------------------------
+// primitive recovery (solver_{1D,2D}/aux_func.py U_to_prim)
+// ---------------------------------------------------------------------------
+template <int DIM>
+struct Prim {
+  double rho, u, v, p, a, R;
+};
+
+template <int DIM>
+__device__ __forceinline__ Prim<DIM> u_to_prim(const MP& m, const double* q, double gamma, double T) {
+  Prim<DIM> r;
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  r.rho = q[0];
+  r.u = q[1] / r.rho;
+  r.v = DIM == 2 ? q[2] / r.rho : 0.0;
+  double Y8[NR], Yf[NS];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / r.rho;
+  fill_Y(Y8, Yf);
+  r.R = get_R(m, Yf);
+  r.p = r.rho * r.R * T;
+  r.a = sqrt(gamma * r.p / r.rho);
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// boundary ghost states that are not plain copies
+// ---------------------------------------------------------------------------
+// pressure_outlet (boundary_conditions_{1D,2D}/pressure_outlet.py:5-22);
+// q is the boundary-adjacent cell, out receives U (nv), gamma, T.
+template <int DIM>
+__device__ void pressure_outlet_state(const MP& m, const double* q, double gamma, double T,
+                                      double normal_vel, double Pb, double* out) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  constexpr int nv = nY + NR;
+  double rho = q[0];
+  double u = q[1] / rho;
+  double v = DIM == 2 ? q[2] / rho : 0.0;
+  double Y8[NR], Yf[NS];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / rho;
+  fill_Y(Y8, Yf);
+  double R = get_R(m, Yf);
+  double p = rho * (R * T);
+  double a = sqrt(gamma * p / rho);
+  bool sub = normal_vel / a < 1.0;
+  double rho_c = sub ? Pb / (p / rho) : rho;
+  double p_c = sub ? Pb * 1.0 : p;
+  double T_c = sub ? p_c / (rho_c * R) : T;
+  Th t = thermo_mix(m, T_c, Yf);
+  double g_c = t.cp / (t.cp - R);
+  out[0] = rho_c;
+  out[1] = rho_c * u;
+  if (DIM == 2) {
+    out[2] = rho_c * v;
+    out[3] = rho_c * t.h - p_c + 0.5 * rho_c * (u * u + v * v);
+  } else {
+    out[2] = rho_c * t.h - p_c + 0.5 * rho_c * (u * u);
+  }
+#pragma unroll
+  for (int k = 0; k < NR; ++k) out[nY + k] = rho_c * Y8[k];
+  out[nv] = g_c;
+  out[nv + 1] = T_c;
+}
+
+// Rotating-detonation injector of examples/janc_basic_example2.ipynb
+// (bottom_boundary + inj_model, after Fievisohn et al. 2017): bisection on
+// the throat Mach number of a choked injector fed at nondimensional total
+// pressure 1 and temperature 1; blocked (slip-like) when p_in >= 1.
+__device__ void injector_state(const MP& m, const double* q, double gamma, double T,
+                               const double* Yinj8, double block_p, double* out) {
+  constexpr int nY = 4;
+  constexpr int nv = nY + NR;
+  double rho = q[0];
+  double u = q[1] / rho;
+  double v = q[2] / rho;
+  double Y8[NR], Yf[NS];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / rho;
+  fill_Y(Y8, Yf);
+  double R = get_R(m, Yf);
+  double p = rho * R * T;
+  // inj_model
+  double Yi[NS];
+  fill_Y(Yinj8, Yi);
+  double Ri = get_R(m, Yi);
+  const double gam = 1.29;
+  const double A1 = 1.0, A3 = 5.0, A2 = 4.0;
+  const double C0 = sqrt(gam * Ri * 1.0);
+  const double gh = (gam - 1.0) / 2.0;
+  const double e1 = -gam / (gam - 1.0);
+  const double e2 = -(gam + 1.0) / 2.0 / (gam - 1.0);
+  const double gg = gam / (gam - 1.0);
+  const double P3 = p;
+  double M1 = 0.0, M2 = 1.0, MFC = 0.0, V3 = 0.0;
+  for (int it = 0; it < 20; ++it) {
+    double M = 0.5 * (M1 + M2);
+    double base = 1.0 + gh * (M * M);
+    double P1 = 1.0 * pow(base, e1);
+    double V1 = M * pow(base, -0.5) * C0;
+    MFC = 1.0 * sqrt(gam / Ri) * M * pow(base, e2);
+    double B = gg * P3 * A3 / MFC;
+    double C = -gam / (gam - 1.0) * Ri * 1.0;
+    V3 = (-B + sqrt(B * B - 2.0 * C)) / 1.0;
+    double P2 = (MFC * (V3 - V1) - P1 * A1 + P3 * A3) / A2;
+    M2 = (P2 >= P1) ? M : M2;
+    M1 = (P2 < P1) ? M : M1;
+  }
+  double rho_i = MFC / V3 / A3;
+  double T_i = P3 / (Ri * rho_i);
+  Th ti = thermo_mix(m, T_i, Yi);
+  double g_i = ti.cp / (ti.cp - Ri);
+  double rho_inj = p / (Ri * T_i);
+  // bottom_boundary selection
+  bool blk = p >= block_p;
+  double rho_c = blk ? rho : rho_inj;
+  double u_c = blk ? u : 0.0;
+  double v_c = blk ? -v : V3;
+  double T_c = blk ? T : T_i;
+  double h_c;
+  if (blk) {
+    Th t = thermo_mix(m, T, Yf);
+    h_c = t.h;
+  } else {
+    h_c = ti.h;
+  }
+  double g_c = blk ? gamma : g_i;
+  out[0] = rho_c;
+  out[1] = rho_c * u_c;
+  out[2] = rho_c * v_c;
+  out[3] = rho_c * h_c - p + 0.5 * rho_c * (u_c * u_c + v_c * v_c);
+#pragma unroll
+  for (int k = 0; k < NR; ++k) out[nY + k] = rho_c * (blk ? Y8[k] : Yinj8[k]);
+  out[nv] = g_c;
+  out[nv + 1] = T_c;
+}
+
+// ---------------------------------------------------------------------------
+// WENO5-JS (solver_{1D,2D}/reconstruction/WENO5_JS.py), reference order
+// ---------------------------------------------------------------------------
+constexpr double W_EPS = 1e-6;
+constexpr double W_C1 = 1.0 / 10.0, W_C2 = 3.0 / 5.0, W_C3 = 3.0 / 10.0;
+constexpr double W_Q = 1.0 / 4.0, W_D = 13.0 / 12.0;
+constexpr double W_13 = 1.0 / 3.0, W_76 = 7.0 / 6.0, W_116 = 11.0 / 6.0;
+constexpr double W_m16 = -1.0 / 6.0, W_56 = 5.0 / 6.0, W_16 = 1.0 / 6.0;
+
+// left-biased value at j+1/2 from cells j-2..j+2 (interface_L_*)
+__device__ __forceinline__ double weno_L(double fjm2, double fjm1, double fj, double fjp1, double fjp2) {
+  double t1 = fjm2 - 4.0 * fjm1 + 3.0 * fj, s1 = fjm2 - 2.0 * fjm1 + fj;
+  double t2 = fjm1 - fjp1, s2 = fjm1 - 2.0 * fj + fjp1;
+  double t3 = 3.0 * fj - 4.0 * fjp1 + fjp2, s3 = fj - 2.0 * fjp1 + fjp2;
+  double IS1 = W_Q * (t1 * t1) + W_D * (s1 * s1);
+  double IS2 = W_Q * (t2 * t2) + W_D * (s2 * s2);
+  double IS3 = W_Q * (t3 * t3) + W_D * (s3 * s3);
+  double e1 = W_EPS + IS1, e2 = W_EPS + IS2, e3 = W_EPS + IS3;
+  double a1 = W_C1 / (e1 * e1), a2 = W_C2 / (e2 * e2), a3 = W_C3 / (e3 * e3);
+  double w1 = a1 / (a1 + a2 + a3), w2 = a2 / (a1 + a2 + a3), w3 = a3 / (a1 + a2 + a3);
+  double q1 = W_13 * fjm2 - W_76 * fjm1 + W_116 * fj;
+  double q2 = W_m16 * fjm1 + W_56 * fj + W_13 * fjp1;
+  double q3 = W_13 * fj + W_56 * fjp1 - W_16 * fjp2;
+  return w1 * q1 + w2 * q2 + w3 * q3;
+}
+
+// right-biased value at j-1/2 from cells j-2..j+2 (interface_R_*)
+__device__ __forceinline__ double weno_R(double fjm2, double fjm1, double fj, double fjp1, double fjp2) {
+  double t1 = fjp2 - 4.0 * fjp1 + 3.0 * fj, s1 = fjp2 - 2.0 * fjp1 + fj;
+  double t2 = fjp1 - fjm1, s2 = fjp1 - 2.0 * fj + fjm1;
+  double t3 = 3.0 * fj - 4.0 * fjm1 + fjm2, s3 = fj - 2.0 * fjm1 + fjm2;
+  double IS1 = W_Q * (t1 * t1) + W_D * (s1 * s1);
+  double IS2 = W_Q * (t2 * t2) + W_D * (s2 * s2);
+  double IS3 = W_Q * (t3 * t3) + W_D * (s3 * s3);
+  double e1 = W_EPS + IS1, e2 = W_EPS + IS2, e3 = W_EPS + IS3;
+  double a1 = W_C1 / (e1 * e1), a2 = W_C2 / (e2 * e2), a3 = W_C3 / (e3 * e3);
+  double w1 = a1 / (a1 + a2 + a3), w2 = a2 / (a1 + a2 + a3), w3 = a3 / (a1 + a2 + a3);
+  double q1 = W_13 * fjp2 - W_76 * fjp1 + W_116 * fj;
+  double q2 = W_m16 * fjp1 + W_56 * fj + W_13 * fjm1;
+  double q3 = W_13 * fj + W_56 * fjm1 - W_16 * fjm2;
+  return w1 * q1 + w2 * q2 + w3 * q3;
+}
+
+// ---------------------------------------------------------------------------
+// ghost-cell source mapping (boundary/boundary.py:120-132,
+// boundary/boundary_padding.py:4-45, boundary_conditions_{1D,2D}/*.py)
+// ---------------------------------------------------------------------------
+// kind: 0 interior copy of (xs, ys) with sign flips, 1 strip value, 2 unused
+struct Src {
+  int kind, xs, ys, side, pos, flip;
+};
+
+// One axis: coordinate c on an axis of length n, lo/hi side kinds.
+__device__ __forceinline__ bool map_axis(int c, int n, int kind, bool lo, int& cs, int& flip,
+                                         bool& strip, int normal_field, int dim) {
+  strip = false;
+  flip = 0;
+  switch (kind) {
+    case JB_BC_PERIODIC:  // node-periodic quirk: ghosts are n-4..n-2 and 1..3
+      cs = lo ? n - 1 + c : c - n + 1;
+      return true;
+    case JB_BC_SLIP_WALL:
+      cs = lo ? 0 : n - 1;
+      flip = 1 << normal_field;
+      return true;
+    case JB_BC_ZERO_GRADIENT:
+      cs = lo ? -1 - c : 2 * n - 1 - c;
+      return true;
+    case JB_BC_NO_SLIP_WALL:
+      cs = lo ? -1 - c : 2 * n - 1 - c;
+      flip = dim == 2 ? 6 : 2;
+      return true;
+    default:
+      strip = true;
+      return true;
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ Src map_cell(const Grid& g, int x, int y) {
+  Src s;
+  s.kind = 2; s.xs = 0; s.ys = 0; s.side = 0; s.pos = 0; s.flip = 0;
+  bool xin = x >= 0 && x < g.nx;
+  bool yin = DIM == 1 ? true : (y >= 0 && y < g.ny);
+  if (xin && yin) {
+    s.kind = 0; s.xs = x; s.ys = y;
+    return s;
+  }
+  if (!xin && yin) {
+    if (x < -3 || x >= g.nx + 3) return s;
+    bool lo = x < 0;
+    int side = lo ? 0 : 1;
+    int cs, flip;
+    bool strip;
+    map_axis(x, g.nx, g.bc[side], lo, cs, flip, strip, 1, DIM);
+    if (strip) { s.kind = 1; s.side = side; s.pos = y; return s; }
+    s.kind = 0; s.xs = cs; s.ys = y; s.flip = flip;
+    return s;
+  }
+  if (DIM == 2 && xin && !yin) {
+    if (y < -3 || y >= g.ny + 3) return s;
+    bool lo = y < 0;
+    int side = lo ? 2 : 3;
+    int cs, flip;
+    bool strip;
+    map_axis(y, g.ny, g.bc[side], lo, cs, flip, strip, 2, DIM);
+    if (strip) { s.kind = 1; s.side = side; s.pos = x; return s; }
+    s.kind = 0; s.xs = x; s.ys = cs; s.flip = flip;
+    return s;
+  }
+  return s;  // corner: never read by a stencil
+}
+
+__device__ __forceinline__ size_t strip_idx(const Grid& g, int side, int q, int pos) {
+  return ((size_t)side * (g.nv + 2) + q) * g.lstrip + pos;
+}
+
+// LF split flux F(f) of one cell in direction dir (0: x, 1: y) as the
+// reference assembles it (flux_splitting/LF.py); Y = U_f / rho for species.
+template <int DIM>
+__device__ __forceinline__ double lf_flux(int f, int dir, double q, double rho, double u, double v,
+                                          double p, double E) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  double vn = dir == 0 ? u : v;
+  if (f == 0) return rho * vn;
+  if (DIM == 1) {
+    if (f == 1) return rho * (u * u) + p;
+    if (f == 2) return u * (E + p);
+  } else {
+    if (f == 1) return dir == 0 ? rho * (u * u) + p : rho * u * v;
+    if (f == 2) return dir == 0 ? rho * u * v : rho * (v * v) + p;
+    if (f == 3) return vn * (E + p);
+  }
+  (void)nY;
+  return rho * vn * (q / rho);
+}
+
+// ---------------------------------------------------------------------------
+// stage kernels
+// ---------------------------------------------------------------------------
+// STAGE 0: flux_func only, out = dt * total_flux(BC(U, aux))
+//           (simulation/set_simulator.py:26-29, 44-47)
+// STAGE 1..3: SSP-RK3 stage (simulation/time_step/TVD_RK3.py:5-12)
+//           out = a U^n + b (U_k + dt L(U_k)), followed by the Halley
+//           iterates of update_aux (solver_{1D,2D}/aux_func.py:21-29)
+constexpr int TX2 = 15, TY2 = 16, PX2 = TX2 + 6, PY2 = TY2 + 6;
+constexpr int NT2 = 256;
+constexpr int SM2_Q = PX2 * PY2;                  // per field
+constexpr int SM2_HX = PX2 * TY2, SM2_HY = TX2 * PY2;
+constexpr int SM2_FX = (TX2 + 1) * TY2, SM2_FY = TX2 * (TY2 + 1);
+
+__host__ __device__ constexpr size_t smem2d_bytes(int nq) {
+  return sizeof(double) * ((size_t)nq * SM2_Q + 4 * SM2_Q + 2 * SM2_HX + 2 * SM2_HY + SM2_FX + SM2_FY);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(NT2) k_flux2d(MP m, Grid g, const double* __restrict__ Uk,
+                                                 const double* __restrict__ auxk,
+                                                 const double* __restrict__ Un,
+                                                 double* __restrict__ out, double* __restrict__ cand,
+                                                 const double* __restrict__ strips, Slots* slots,
+                                                 int aidx, int midx, double dt_arg) {
+  extern __shared__ double sm[];
+  constexpr int nv = 12, nq = nv + 1;
+  double* sQ = sm;                       // [nq][PX2][PY2]
+  double* sP = sQ + (size_t)nq * SM2_Q;   // [4][PX2][PY2]: rho, u, v, p
+  double* sHxp = sP + 4 * SM2_Q;          // [PX2][TY2]
+  double* sHxm = sHxp + SM2_HX;
+  double* sHyp = sHxm + SM2_HX;           // [TX2][PY2]
+  double* sHym = sHyp + SM2_HY;
+  double* sFx = sHym + SM2_HY;            // [TX2+1][TY2]
+  double* sFy = sFx + SM2_FX;             // [TX2][TY2+1]
+
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * TX2, y0 = blockIdx.y * TY2;
+  const long long nc = g.ncell;
+  const double dt = STAGE == 0 ? dt_arg : slots->dt;
+  const double ax = bitsd(slots->ax[aidx]);
+  const double ay = bitsd(slots->ay[aidx]);
+
+  // ---- load the padded tile with ghost cells
+  for (int i = tid; i < SM2_Q; i += NT2) {
+    int px = i / PY2, py = i % PY2;
+    int x = x0 + px - 3, y = y0 + py - 3;
+    Src s = map_cell<2>(g, x, y);
+    if (s.kind == 0) {
+      size_t c = (size_t)s.xs * g.ny + s.ys;
+      for (int q = 0; q < nv; ++q) {
+        double v = Uk[q * nc + c];
+        sQ[q * SM2_Q + i] = ((s.flip >> q) & 1) ? -v : v;
+      }
+      sQ[nv * SM2_Q + i] = auxk[nc + c];
+    } else if (s.kind == 1) {
+      for (int q = 0; q < nv; ++q) sQ[q * SM2_Q + i] = strips[strip_idx(g, s.side, q, s.pos)];
+      sQ[nv * SM2_Q + i] = strips[strip_idx(g, s.side, nv + 1, s.pos)];
+    } else {
+      for (int q = 0; q < nq; ++q) sQ[q * SM2_Q + i] = 1.0;
+    }
+  }
+  __syncthreads();
+  // ---- primitives (aux_func.U_to_prim) on every padded cell
+  for (int i = tid; i < SM2_Q; i += NT2) {
+    double q[16];
+    for (int f = 0; f < nv; ++f) q[f] = sQ[f * SM2_Q + i];
+    double T = sQ[nv * SM2_Q + i];
+    Prim<2> pr = u_to_prim<2>(m, q, 1.0, T);
+    sP[i] = pr.rho;
+    sP[SM2_Q + i] = pr.u;
+    sP[2 * SM2_Q + i] = pr.v;
+    sP[3 * SM2_Q + i] = pr.p;
+  }
+  __syncthreads();
+
+  const bool owner = tid < TX2 * TY2;
+  const int ix = owner ? tid / TY2 : 0, iy = owner ? tid % TY2 : 0;
+  const int gx = x0 + ix, gy = y0 + iy;
+  const bool live = owner && gx < g.nx && gy < g.ny;
+  const size_t cell = (size_t)gx * g.ny + gy;
+
+  for (int f = 0; f < nv; ++f) {
+    // ---- split fluxes H+/- = 0.5 (F +/- alpha U)
+    for (int i = tid; i < SM2_HX + SM2_HY; i += NT2) {
+      int px, py, dir;
+      if (i < SM2_HX) { px = i / TY2; py = i % TY2 + 3; dir = 0; }
+      else { int j = i - SM2_HX; px = j / PY2 + 3; py = j % PY2; dir = 1; }
+      int c = px * PY2 + py;
+      double rho = sP[c], u = sP[SM2_Q + c], v = sP[2 * SM2_Q + c], p = sP[3 * SM2_Q + c];
+      double E = sQ[3 * SM2_Q + c];
+      double qf = sQ[f * SM2_Q + c];
+      double F = lf_flux<2>(f, dir, qf, rho, u, v, p, E);
+      double al = dir == 0 ? ax : ay;
+      double hp = 0.5 * (F + al * qf), hm = 0.5 * (F - al * qf);
+      if (dir == 0) { sHxp[px * TY2 + (py - 3)] = hp; sHxm[px * TY2 + (py - 3)] = hm; }
+      else { sHyp[(px - 3) * PY2 + py] = hp; sHym[(px - 3) * PY2 + py] = hm; }
+    }
+    __syncthreads();
+    // ---- face values: F = L(H+) + R(H-)
+    {
+      int mxf = tid / TY2, jy = tid % TY2;  // x-faces: 16 x 16 = 256
+      const double* hp = sHxp + jy;
+      const double* hm = sHxm + jy;
+      double L = weno_L(hp[(mxf) * TY2], hp[(mxf + 1) * TY2], hp[(mxf + 2) * TY2], hp[(mxf + 3) * TY2],
+                        hp[(mxf + 4) * TY2]);
+      double R = weno_R(hm[(mxf + 1) * TY2], hm[(mxf + 2) * TY2], hm[(mxf + 3) * TY2], hm[(mxf + 4) * TY2],
+                        hm[(mxf + 5) * TY2]);
+      sFx[mxf * TY2 + jy] = L + R;
+      if (tid < SM2_FY) {
+        int jx = tid / (TY2 + 1), myf = tid % (TY2 + 1);
+        const double* gp = sHyp + jx * PY2 + myf;
+        const double* gm = sHym + jx * PY2 + myf;
+        double Lg = weno_L(gp[0], gp[1], gp[2], gp[3], gp[4]);
+        double Rg = weno_R(gm[1], gm[2], gm[3], gm[4], gm[5]);
+        sFy[jx * (TY2 + 1) + myf] = Lg + Rg;
+      }
+    }
+    __syncthreads();
+    // ---- divergence and the RK combination
+    if (live) {
+      double dF = sFx[(ix + 1) * TY2 + iy] - sFx[ix * TY2 + iy];
+      double dG = sFy[ix * (TY2 + 1) + iy + 1] - sFy[ix * (TY2 + 1) + iy];
+      double rhs = dt * (-(dF / g.dx + dG / g.dy));
+      double uk = sQ[f * SM2_Q + (ix + 3) * PY2 + (iy + 3)];
+      double r;
+      if (STAGE == 0) r = rhs;
+      else if (STAGE == 1) r = uk + rhs;
+      else if (STAGE == 2) r = 3.0 / 4.0 * Un[f * nc + cell] + 1.0 / 4.0 * (uk + rhs);
+      else r = 1.0 / 3.0 * Un[f * nc + cell] + 2.0 / 3.0 * (uk + rhs);
+      out[f * nc + cell] = r;
+    }
+    __syncthreads();
+  }
+
+  if (STAGE == 0) return;
+  // ---- Halley iterates of update_aux on the new state
+  unsigned bits = 0;
+  if (live) {
+    double q[12];
+    for (int f = 0; f < 12; ++f) q[f] = out[f * nc + cell];
+    double rho = q[0];
+    double u = q[1] / rho, v = q[2] / rho;
+    double e = q[3] / rho - 0.5 * (u * u + v * v);
+    double Y8[NR], Yf[NS];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) Y8[k] = q[4 + k] / rho;
+    fill_Y(Y8, Yf);
+    double R = get_R(m, Yf);
+    double T0 = sQ[nv * SM2_Q + (ix + 3) * PY2 + (iy + 3)];
+    double cnd[JB_NCAND];
+    bits = halley_iterates(m, e, Yf, R, T0, cnd);
+#pragma unroll
+    for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
+  }
+  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
+}
+
+// 1D: tiles of 255 cells so the 256 faces map one-to-one onto threads.
+constexpr int TX1 = 255, PX1 = TX1 + 6, NT1 = 256;
+
+__host__ __device__ constexpr size_t smem1d_bytes(int nq) {
+  return sizeof(double) * ((size_t)nq * PX1 + 3 * PX1 + 2 * PX1 + (TX1 + 1));
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __restrict__ Uk,
+                                                 const double* __restrict__ auxk,
+                                                 const double* __restrict__ Un,
+                                                 double* __restrict__ out, double* __restrict__ cand,
+                                                 const double* __restrict__ strips, Slots* slots,
+                                                 int aidx, int midx, double dt_arg) {
+  extern __shared__ double sm[];
+  constexpr int nv = 11, nq = nv + 1;
+  double* sQ = sm;                      // [nq][PX1]
+  double* sP = sQ + (size_t)nq * PX1;    // [3][PX1]: rho, u, p
+  double* sHp = sP + 3 * PX1;
+  double* sHm = sHp + PX1;
+  double* sF = sHm + PX1;                // [TX1+1]
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * TX1;
+  const long long nc = g.ncell;
+  const double dt = STAGE == 0 ? dt_arg : slots->dt;
+  const double ax = bitsd(slots->ax[aidx]);
+
+  for (int i = tid; i < PX1; i += NT1) {
+    int x = x0 + i - 3;
+    Src s = map_cell<1>(g, x, 0);
+    if (s.kind == 0) {
+      for (int q = 0; q < nv; ++q) {
+        double v = Uk[q * nc + s.xs];
+        sQ[q * PX1 + i] = ((s.flip >> q) & 1) ? -v : v;
+      }
+      sQ[nv * PX1 + i] = auxk[nc + s.xs];
+    } else if (s.kind == 1) {
+      for (int q = 0; q < nv; ++q) sQ[q * PX1 + i] = strips[strip_idx(g, s.side, q, 0)];
+      sQ[nv * PX1 + i] = strips[strip_idx(g, s.side, nv + 1, 0)];
+    } else {
+      for (int q = 0; q < nq; ++q) sQ[q * PX1 + i] = 1.0;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < PX1; i += NT1) {
+    double q[16];
+    for (int f = 0; f < nv; ++f) q[f] = sQ[f * PX1 + i];
+    Prim<1> pr = u_to_prim<1>(m, q, 1.0, sQ[nv * PX1 + i]);
+    sP[i] = pr.rho;
+    sP[PX1 + i] = pr.u;
+    sP[2 * PX1 + i] = pr.p;
+  }
+  __syncthreads();
+  const bool live = tid < TX1 && x0 + tid < g.nx;
+  const size_t cell = (size_t)(x0 + tid);
+  for (int f = 0; f < nv; ++f) {
+    for (int i = tid; i < PX1; i += NT1) {
+      double rho = sP[i], u = sP[PX1 + i], p = sP[2 * PX1 + i];
+      double qf = sQ[f * PX1 + i];
+      double F = lf_flux<1>(f, 0, qf, rho, u, 0.0, p, sQ[2 * PX1 + i]);
+      sHp[i] = 0.5 * (F + ax * qf);
+      sHm[i] = 0.5 * (F - ax * qf);
+    }
+    __syncthreads();
+    {
+      int mf = tid;  // 256 faces
+      double L = weno_L(sHp[mf], sHp[mf + 1], sHp[mf + 2], sHp[mf + 3], sHp[mf + 4]);
+      double R = weno_R(sHm[mf + 1], sHm[mf + 2], sHm[mf + 3], sHm[mf + 4], sHm[mf + 5]);
+      sF[mf] = L + R;
+    }
+    __syncthreads();
+    if (live) {
+      double dF = sF[tid + 1] - sF[tid];
+      double rhs = dt * (-(dF / g.dx));
+      double uk = sQ[f * PX1 + tid + 3];
+      double r;
+      if (STAGE == 0) r = rhs;
+      else if (STAGE == 1) r = uk + rhs;
+      else if (STAGE == 2) r = 3.0 / 4.0 * Un[f * nc + cell] + 1.0 / 4.0 * (uk + rhs);
+      else r = 1.0 / 3.0 * Un[f * nc + cell] + 2.0 / 3.0 * (uk + rhs);
+      out[f * nc + cell] = r;
+    }
+    __syncthreads();
+  }
+  if (STAGE == 0) return;
+  unsigned bits = 0;
+  if (live) {
+    double q[11];
+    for (int f = 0; f < 11; ++f) q[f] = out[f * nc + cell];
+    double rho = q[0];
+    double u = q[1] / rho;
+    double e = q[2] / rho - 0.5 * (u * u);
+    double Y8[NR], Yf[NS];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) Y8[k] = q[3 + k] / rho;
+    fill_Y(Y8, Yf);
+    double R = get_R(m, Yf);
+    double cnd[JB_NCAND];
+    bits = halley_iterates(m, e, Yf, R, sQ[nv * PX1 + tid + 3], cnd);
+#pragma unroll
+    for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
+  }
+  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
+}
+
+// ---------------------------------------------------------------------------
+// Halley iterates for a standalone update_aux (aux_func.update_aux)
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void k_halley(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux,
+                         double* __restrict__ cand, Slots* slots, int midx) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  const long long nc = g.ncell;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned bits = 0;
+  if (c < nc) {
+    double rho = U[c];
+    double u = U[nc + c] / rho;
+    double v = DIM == 2 ? U[2 * nc + c] / rho : 0.0;
+    double e = DIM == 2 ? U[3 * nc + c] / rho - 0.5 * (u * u + v * v) : U[2 * nc + c] / rho - 0.5 * (u * u);
+    double Y8[NR], Yf[NS];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) Y8[k] = U[(nY + k) * nc + c] / rho;
+    fill_Y(Y8, Yf);
+    double R = get_R(m, Yf);
+    double cnd[JB_NCAND];
+    bits = halley_iterates(m, e, Yf, R, aux[nc + c], cnd);
+#pragma unroll
+    for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + c] = cnd[i];
+  }
+  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
+}
+
+// ---------------------------------------------------------------------------
+// select / reduce pass: finishes a temperature solve (SELECT) or takes aux
+// as given, then the LF wave-speed maxima over the padded grid (ALPHA:
+// flux_splitting/LF.py "nanmax(|u|+a)"), the CFL minimum (CFL:
+// set_simulator.py:420-443) and the non-copy ghost strips (STRIPS).
+// ---------------------------------------------------------------------------
+template <int DIM, bool SELECT, bool ALPHA, bool CFL>
+__global__ void k_select(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux_in,
+                         const double* __restrict__ cand, double* __restrict__ aux_out,
+                         double* __restrict__ strips, Slots* slots, int midx, int aidx) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  constexpr int nv = nY + NR;
+  const long long nc = g.ncell;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
+  unsigned st = 0;
+  if (c < nc) {
+    double q[nv];
+#pragma unroll
+    for (int f = 0; f < nv; ++f) q[f] = U[f * nc + c];
+    double gamma, T;
+    if (SELECT) {
+      int n = halley_count(slots->mask[midx]);
+      T = cand[n * nc + c];
+      double Y8[NR], Yf[NS];
+#pragma unroll
+      for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / q[0];
+      fill_Y(Y8, Yf);
+      double R = get_R(m, Yf);
+      double cp = cp_mix(m, T, Yf);
+      gamma = cp / (cp - R);
+      aux_out[c] = gamma;
+      aux_out[nc + c] = T;
+    } else {
+      gamma = aux_in[c];
+      T = aux_in[nc + c];
+    }
+    if (ALPHA || CFL) {
+      Prim<DIM> pr = u_to_prim<DIM>(m, q, gamma, T);
+      double sx = fabs(pr.u) + pr.a;
+      double sy = fabs(pr.v) + pr.a;
+      amx = sx;
+      amy = sy;
+      if (!(sx == sx) || !(T == T)) st |= JB_ERR_NONFINITE;
+      if (CFL) {
+        double d = DIM == 1 ? g.dx / sx : 1.0 / (sx / g.dx + sy / g.dy);
+        dtm = d;
+        if (!(d == d) || !(d > 0.0)) st |= JB_ERR_NONFINITE;
+        // jnp.min (set_simulator.py:423,441) returns NaN if any candidate is
+        // NaN; the reduction below skips NaN, so record it separately
+        if (!(d == d)) atomicOr(&slots->dtnan, 1u);
+      }
+      if (ALPHA) {
+        // ghost states that are not copies of interior cells
+        int x = DIM == 1 ? (int)c : (int)(c / g.ny);
+        int y = DIM == 1 ? 0 : (int)(c % g.ny);
+        for (int side = 0; side < 2 * DIM; ++side) {
+          int kind = g.bc[side];
+          if (kind != JB_BC_PRESSURE_OUTLET && kind != JB_BC_RDC_INJECTOR) continue;
+          bool on = side == 0 ? x == 0 : side == 1 ? x == g.nx - 1 : side == 2 ? y == 0 : y == g.ny - 1;
+          if (!on) continue;
+          double gs[nv + 2];
+          if (kind == JB_BC_PRESSURE_OUTLET) {
+            double un = side < 2 ? q[1] / q[0] : q[2] / q[0];
+            if (side == 0 || side == 2) un = -un;
+            pressure_outlet_state<DIM>(m, q, gamma, T, un, g.Pb, gs);
+          } else {
+            if (DIM == 2) {
+              double Yi[NR];
+              for (int k = 0; k < NR; ++k) Yi[k] = g.Yinj[k * g.nx + x];
+              injector_state(m, q, gamma, T, Yi, g.inj_block_p, gs);
+            }
+          }
+          int pos = side < 2 ? y : x;
+          for (int f = 0; f < nv + 2; ++f) strips[strip_idx(g, side, f, pos)] = gs[f];
+          Prim<DIM> pg = u_to_prim<DIM>(m, gs, gs[nv], gs[nv + 1]);
+          double gx = fabs(pg.u) + pg.a, gy = fabs(pg.v) + pg.a;
+          amx = fmax(amx, gx);
+          amy = fmax(amy, gy);
+        }
+      }
+    }
+  }
+  if (ALPHA || CFL) block_reduce_store(amx, amy, dtm, st << 16, slots, aidx, ALPHA, CFL, -1);
+}
+
+// ---------------------------------------------------------------------------
+// point-implicit chemistry (model/reaction_model.py:91-193)
+// ---------------------------------------------------------------------------
+// Rates, analytic Jacobian d(omega)/d(rho Y) and the solve of
+// (I/dt - J) x = omega for one cell.  Returns S_k = rho * clip(x_k/rho).
+__device__ void chem_cell(const MP& m, double rho, const double* Y8, double T, double dt,
+                          double* S, unsigned& st) {
+  double Yf[NS], X[NS], Xc[NS], logX[NR], gk[NR];
+  fill_Y(Y8, Yf);
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    X[k] = rho * Yf[k] / m.M[k];
+    Xc[k] = X[k] < 1e-50 ? 1e-50 : X[k];
+  }
+#pragma unroll
+  for (int k = 0; k < NR; ++k) logX[k] = log(Xc[k]);
+  // get_gibbs (reaction_model.py:78-89): g = s/R - h/(R T)
+  const double lT = log(m.T0 * T);
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    const bool lo = T < m.Tcr[k];
+    double h = lo ? poly6(m.hc_lo[k], T) : poly6(m.hc_hi[k], T);
+    double s = lo ? poly5(m.s_lo[k], T) + m.lg_lo[k] * lT : poly5(m.s_hi[k], T) + m.lg_hi[k] * lT;
+    gk[k] = s - h / T;
+  }
+  double w[NR], J[NR][NR], rMX[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    w[k] = 0.0;
+    rMX[k] = 1.0 / (m.M[k] * Xc[k]);
+#pragma unroll
+    for (int n = 0; n < NR; ++n) J[k][n] = 0.0;
+  }
+  const double rT = m.pref / T;
+#pragma unroll 1
+  for (int i = 0; i < NREAC; ++i) {
+    // reactionConstant_i (reaction_model.py:91-122)
+    double kfi = m.A[i] * pow(T, m.B[i]) * exp(-m.EaR[i] / T);
+    double Ms = m.tb[i][0] * X[0];
+#pragma unroll
+    for (int j = 1; j < NS; ++j) Ms = Ms + m.tb[i][j] * X[j];
+    double Mi = m.is_tb[i] * Ms + (1.0 - m.is_tb[i]);
+    double sf = m.vf[i][0] * logX[0], sb = m.vb[i][0] * logX[0], sg = m.dv[i][0] * gk[0];
+#pragma unroll
+    for (int k = 1; k < NR; ++k) {
+      sf = sf + m.vf[i][k] * logX[k];
+      sb = sb + m.vb[i][k] * logX[k];
+      sg = sg + m.dv[i][k] * gk[k];
+    }
+    double kf = kfi * exp(sf);
+    double vs = m.vsum[i];
+    double pw = vs == 0.0 ? 1.0 : (vs == 1.0 ? rT : (vs == -1.0 ? 1.0 / rT : pow(rT, vs)));
+    double kb = kfi / (exp(sg) * pw) * exp(sb);
+    double dq = kf - kb;
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      const double dv = m.dv[i][k];
+      if (dv == 0.0) continue;
+      w[k] = w[k] + dv * Mi * dq;
+#pragma unroll
+      for (int n = 0; n < NR; ++n) {
+        const double a = m.tb[i][n];
+        const double vfn = m.vf[i][n], vbn = m.vb[i][n];
+        const bool t2 = vfn != 0.0 || vbn != 0.0;
+        if (a == 0.0 && !t2) continue;
+        double term;
+        double t1v = dv * dq * (a / m.M[n]);
+        if (t2) {
+          double t2v = rMX[n] * dv * Mi * (vfn * kf - vbn * kb);
+          term = a == 0.0 ? t2v : t1v + t2v;
+        } else {
+          term = t1v;
+        }
+        J[k][n] = J[k][n] + term;
+      }
+    }
+  }
+  // A = I/dt - M_k J ; b = M_k w   (construct_matrix_equation, :132-159)
+  double A[NR][NR], b[NR];
+  const double idt = 1.0 / dt;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    b[k] = m.M[k] * w[k];
+#pragma unroll
+    for (int n = 0; n < NR; ++n) {
+      double jk = m.M[k] * J[k][n];
+      A[k][n] = (k == n ? idt : 0.0) - jk;
+    }
+  }
+  // LU with partial pivoting (first maximal |pivot|, as LAPACK idamax)
+#pragma unroll
+  for (int c = 0; c < NR; ++c) {
+    int p = c;
+    double best = fabs(A[c][c]);
+#pragma unroll
+    for (int r = c + 1; r < NR; ++r) {
+      double v = fabs(A[r][c]);
+      if (v > best) { best = v; p = r; }
+    }
+#pragma unroll
+    for (int r = c + 1; r < NR; ++r) {
+      if (p == r) {
+#pragma unroll
+        for (int j = 0; j < NR; ++j) { double t = A[c][j]; A[c][j] = A[r][j]; A[r][j] = t; }
+        double t = b[c]; b[c] = b[r]; b[r] = t;
+      }
+    }
+    if (A[c][c] == 0.0) st |= JB_ERR_SINGULAR;
+#pragma unroll
+    for (int r = c + 1; r < NR; ++r) {
+      double l = A[r][c] / A[c][c];
+#pragma unroll
+      for (int j = c + 1; j < NR; ++j) A[r][j] = A[r][j] - l * A[c][j];
+      b[r] = b[r] - l * b[c];
+    }
+  }
+  double x[NR];
+#pragma unroll
+  for (int r = NR - 1; r >= 0; --r) {
+    double s = b[r];
+#pragma unroll
+    for (int j = r + 1; j < NR; ++j) s = s - A[r][j] * x[j];
+    x[r] = s / A[r][r];
+  }
+  // detailed_reaction (:183-193): dY = clip(drhoY/rho, -Y, 1-Y); S = rho dY
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    double dY = x[k] / rho;
+    double lo = -Y8[k], hi = 1.0 - Y8[k];
+    dY = dY < lo ? lo : dY;
+    dY = dY > hi ? hi : dY;
+    S[k] = rho * dY;
+  }
+}
+
+// WRITE_S: reaction_source_terms output S (zeros for the flow fields).
+// Otherwise U_out = U + S followed by the Halley iterates of the final
+// update_aux (set_simulator.py:117-122).
+template <int DIM, bool WRITE_S>
+__global__ void k_chem(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux,
+                       double* __restrict__ out, double* __restrict__ cand, Slots* slots, int midx,
+                       double dt_arg) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  constexpr int nv = nY + NR;
+  const long long nc = g.ncell;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = WRITE_S ? dt_arg : slots->dt;
+  unsigned bits = 0, st = 0;
+  if (c < nc) {
+    double q[nv];
+#pragma unroll
+    for (int f = 0; f < nv; ++f) q[f] = U[f * nc + c];
+    double rho = q[0];
+    double Y8[NR], S[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / rho;
+    double T = aux[nc + c];
+    chem_cell(m, rho, Y8, T, dt, S, st);
+    if (WRITE_S) {
+#pragma unroll
+      for (int f = 0; f < nY; ++f) out[f * nc + c] = 0.0;
+#pragma unroll
+      for (int k = 0; k < NR; ++k) out[(nY + k) * nc + c] = S[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < NR; ++k) q[nY + k] = q[nY + k] + S[k];
+#pragma unroll
+      for (int f = 0; f < nv; ++f) out[f * nc + c] = q[f];
+      double u = q[1] / rho;
+      double v = DIM == 2 ? q[2] / rho : 0.0;
+      double e = DIM == 2 ? q[3] / rho - 0.5 * (u * u + v * v) : q[2] / rho - 0.5 * (u * u);
+      double Yn[NR], Yf[NS];
+#pragma unroll
+      for (int k = 0; k < NR; ++k) Yn[k] = q[nY + k] / rho;
+      fill_Y(Yn, Yf);
+      double R = get_R(m, Yf);
+      double cnd[JB_NCAND];
+      bits = halley_iterates(m, e, Yf, R, T, cnd);
+#pragma unroll
+      for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + c] = cnd[i];
+    }
+  }
+  block_reduce_store(0.0, 0.0, 0.0, bits | (st << 16), slots, 0, false, false, WRITE_S ? -1 : midx);
+}
+
+// ---------------------------------------------------------------------------
+// thermo evaluation for state building (thermo_model.get_thermo)
+// ---------------------------------------------------------------------------
+__global__ void k_thermo(MP m, long long n, const double* __restrict__ T, const double* __restrict__ Y,
+                         double* __restrict__ cp, double* __restrict__ gamma, double* __restrict__ h,
+                         double* __restrict__ R, double* __restrict__ dcp) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double Y8[NR], Yf[NS];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y8[k] = Y[k * n + c];
+  fill_Y(Y8, Yf);
+  double r = get_R(m, Yf);
+  Th t = thermo_mix(m, T[c], Yf);
+  cp[c] = t.cp;
+  gamma[c] = t.cp / (t.cp - r);
+  h[c] = t.h;
+  R[c] = r;
+  dcp[c] = t.dcp;
+}
+
+// ---------------------------------------------------------------------------
+// per-step slot bookkeeping (one thread)
+// ---------------------------------------------------------------------------
+__global__ void k_slots_reset(Slots* s) {
+  for (int i = 0; i < 4; ++i) { s->ax[i] = 0ull; s->ay[i] = 0ull; s->mask[i] = 0u; }
+  s->dtmin_next = 0x7ff0000000000000ull;
+  s->dtnan = 0u;
+  s->dt = 0.0;  // status is cleared only when the host reads it (jb_status)
+}
+
+// Start of a time step: alpha of stage 1 and the CFL minimum come from the
+// previous select pass; dt = CFL * min (set_simulator.py:420-447) or given.
+__global__ void k_step_begin(Slots* s, double cfl, double dt_fixed, double* dt_hist, int step) {
+  s->ax[0] = s->ax[3];
+  s->ay[0] = s->ay[3];
+  double dt = cfl > 0.0 ? cfl * (s->dtnan ? __longlong_as_double(0x7ff8000000000000LL)
+                                         : bitsd(s->dtmin_next))
+                        : dt_fixed;
+  s->dtnan = 0u;
+  s->dt = dt;
+  if (dt_hist) dt_hist[step] = dt;
+  for (int i = 1; i < 4; ++i) { s->ax[i] = 0ull; s->ay[i] = 0ull; }
+  for (int i = 0; i < 4; ++i) s->mask[i] = 0u;
+  s->dtmin_next = 0x7ff0000000000000ull;
+}
+
+__global__ void k_dt_from_slots(const Slots* s, double cfl, double* dt_out) {
+  *dt_out = cfl * (s->dtnan ? __longlong_as_double(0x7ff8000000000000LL) : bitsd(s->dtmin_next));
+}
+
+}  // namespace JB_NS
+}  // namespace jb

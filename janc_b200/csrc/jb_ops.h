@@ -1,0 +1,39 @@
+// Host-side launch table: one instance per compiled arithmetic variant
+// (jb::strict_ops from jb_strict.cu, jb::fast_ops from jb_fast.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "jb_types.h"
+
+namespace jb {
+
+struct Ops {
+  const char* name;
+  // STAGE 0 writes dt * flux; STAGE 1..3 writes the RK stage and Halley iterates
+  cudaError_t (*flux)(int dim, int stage, const jb_mech_params& m, const jb_grid& g,
+                      const double* Uk, const double* auxk, const double* Un, double* out,
+                      double* cand, const double* strips, jb_slots* slots, int aidx, int midx,
+                      double dt, cudaStream_t st);
+  cudaError_t (*select)(int dim, bool select, bool alpha, bool cfl, const jb_mech_params& m,
+                        const jb_grid& g, const double* U, const double* aux_in,
+                        const double* cand, double* aux_out, double* strips, jb_slots* slots,
+                        int midx, int aidx, cudaStream_t st);
+  cudaError_t (*halley)(int dim, const jb_mech_params& m, const jb_grid& g, const double* U,
+                        const double* aux, double* cand, jb_slots* slots, int midx,
+                        cudaStream_t st);
+  cudaError_t (*chem)(int dim, bool write_s, const jb_mech_params& m, const jb_grid& g,
+                      const double* U, const double* aux, double* out, double* cand,
+                      jb_slots* slots, int midx, double dt, cudaStream_t st);
+  cudaError_t (*thermo)(const jb_mech_params& m, long long n, const double* T, const double* Y,
+                        double* cp, double* gamma, double* h, double* R, double* dcp,
+                        cudaStream_t st);
+  cudaError_t (*slots_reset)(jb_slots* s, cudaStream_t st);
+  cudaError_t (*step_begin)(jb_slots* s, double cfl, double dt_fixed, double* dt_hist, int step,
+                            cudaStream_t st);
+  cudaError_t (*dt_from_slots)(const jb_slots* s, double cfl, double* dt_out, cudaStream_t st);
+};
+
+extern const Ops strict_ops;
+extern const Ops fast_ops;
+
+}  // namespace jb

@@ -1,0 +1,7 @@
+// FP64 path with the reference's rounding: compiled with -fmad=false so that
+// no multiply-add pair is contracted and each expression rounds as NumPy/XLA
+// float64 does.  Transcendentals (exp, log, pow) are CUDA's.
+#define JB_NS strict
+#define JB_NS_NAME "fp64_strict"
+#define JB_OPS_NAME strict_ops
+#include "jb_variant.inc"

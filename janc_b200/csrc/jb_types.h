@@ -1,0 +1,90 @@
+// Plain-old-data types shared by the host launcher and the device kernels.
+// No torch or CUDA-runtime types appear here so the C ABI header can mirror
+// the layouts one-for-one.
+#pragma once
+#include <stdint.h>
+
+#define JB_NS_MAX 9      // species including the implicit last (inert) one
+#define JB_NR_MAX 8      // reactive species (the linear system size)
+#define JB_NREAC_MAX 19  // reactions
+#define JB_NCAND 6       // Halley iterates kept per cell: T_0 .. T_5
+
+// Mechanism tables in the reference's packing (preprocess/load.py:91-135 and
+// :8-88), already non-dimensionalised.  Polynomials are highest power first
+// (numpy/jax polyval order).
+typedef struct jb_mech_params {
+  int ns, nr, nreac, pad_;
+  double M[JB_NS_MAX];      // species_M
+  double invM[JB_NS_MAX];   // 1/species_M (thermo_model.py:91 "1/Mex")
+  double Tcr[JB_NS_MAX];
+  double cp_lo[JB_NS_MAX][5], cp_hi[JB_NS_MAX][5];
+  double dcp_lo[JB_NS_MAX][4], dcp_hi[JB_NS_MAX][4];
+  double h_lo[JB_NS_MAX][6], h_hi[JB_NS_MAX][6];
+  double hc_lo[JB_NS_MAX][6], hc_hi[JB_NS_MAX][6];  // h/R (chemistry)
+  double s_lo[JB_NS_MAX][5], s_hi[JB_NS_MAX][5];
+  double lg_lo[JB_NS_MAX], lg_hi[JB_NS_MAX];
+  double A[JB_NREAC_MAX], B[JB_NREAC_MAX], EaR[JB_NREAC_MAX];
+  double vsum[JB_NREAC_MAX], is_tb[JB_NREAC_MAX];
+  double vf[JB_NREAC_MAX][JB_NR_MAX], vb[JB_NREAC_MAX][JB_NR_MAX];
+  double dv[JB_NREAC_MAX][JB_NR_MAX];  // vb - vf
+  double tb[JB_NREAC_MAX][JB_NS_MAX];  // third-body efficiencies (scaled)
+  double T0;        // nondim reference temperature (gibbs uses log(T0*T))
+  double pref;      // 101325 / P0 (reaction_model.py:113)
+} jb_mech_params;
+
+enum jb_bc_kind {
+  JB_BC_PERIODIC = 0,
+  JB_BC_SLIP_WALL = 1,
+  JB_BC_ZERO_GRADIENT = 2,
+  JB_BC_NO_SLIP_WALL = 3,
+  JB_BC_PRESSURE_OUTLET = 4,
+  JB_BC_RDC_INJECTOR = 5
+};
+
+// kernel categories reported by jb_kernel_times
+enum jb_kernel_cat {
+  JB_KCAT_FLUX = 0,    // LF + WENO5 + RK stage + Halley iterates
+  JB_KCAT_SELECT = 1,  // Halley selection, wave-speed / CFL reductions, ghost strips
+  JB_KCAT_CHEM = 2,    // point-implicit chemistry + final Halley iterates
+  JB_KCAT_OTHER = 3,   // per-step bookkeeping
+  JB_KCAT_COUNT = 4
+};
+#define JB_TIMED_MAX 64  // timed launches buffered between jb_kernel_times calls
+
+enum jb_precision { JB_PREC_STRICT = 0, JB_PREC_FP64 = 1, JB_PREC_MIXED = 2 };
+
+// status bits (device status word and C-ABI return codes)
+enum jb_status {
+  JB_OK = 0,
+  JB_ERR_ARG = 1,
+  JB_ERR_CUDA = 2,
+  JB_ERR_NONFINITE = 4,
+  JB_ERR_SINGULAR = 8,
+  JB_ERR_TIMEOUT = 16,
+  JB_ERR_UNSUPPORTED = 32
+};
+
+// Grid, boundary and theta parameters of one configured solver.
+typedef struct jb_grid {
+  int nx, ny;            // ny == 1 in 1D
+  int nv, nY;            // number of conserved fields, index of first species
+  long long ncell;
+  double dx, dy;
+  int bc[4];             // left, right, bottom, top (jb_bc_kind)
+  double Pb;             // pressure_outlet back pressure (theta['Pb'])
+  const double* Yinj;    // injector mass fractions [nr][nx] (theta['Yinj'])
+  double inj_block_p;    // injector blocked when p_in >= this (1.0 nondim)
+  int lstrip;            // ghost strip length max(nx, ny)
+  int pad_;
+} jb_grid;
+
+// Per-step reduction results.  Doubles reduced with atomics are stored as
+// their bit patterns: for non-negative values integer order is float order.
+typedef struct jb_slots {
+  unsigned long long ax[4], ay[4];  // [0..2]: LF alpha of RK stage 1..3; [3]: next step
+  unsigned long long dtmin_next;    // CFL minimum for the next step
+  unsigned int mask[4];             // Halley masks of the 4 temperature solves
+  unsigned int status;              // jb_status bits seen on the device
+  unsigned int dtnan;               // a CFL candidate was NaN (jnp.min propagates it)
+  double dt;                        // time step of the current step
+} jb_slots;

@@ -1,0 +1,248 @@
+"""One configured solver = one native handle (grid, boundaries, mechanism,
+arithmetic variant) with the reference's call signatures.
+
+Tensors are torch CUDA float64, C-contiguous, in the reference layout
+(``U`` (nv, nx[, ny]), ``aux`` (2, nx[, ny])).  PyTorch only provides the
+device buffers and the current stream; every computation is a kernel of
+``libjanc_b200.so``.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native
+from . import mechanism as _mech
+
+BOUNDARY_KEYS = ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Solver:
+    """Native solver for a fixed grid.
+
+    ``boundary_config`` maps ``left_boundary``/``right_boundary``
+    (``bottom_boundary``/``top_boundary`` in 2D) to one of ``periodic``,
+    ``slip_wall``, ``zero_gradient``, ``no_slip_wall``, ``pressure_outlet`` or
+    ``rdc_injector`` (the rotating-detonation injector of the reference's
+    example 2, bottom side only).
+    """
+
+    def __init__(self, dim, nx, ny=None, dx=1.0, dy=None, boundary_config=None,
+                 mechanism=_mech.DEFAULT_MECHANISM, nondim_config=None, precision="fp64",
+                 device=None):
+        if dim in ("1D", 1):
+            dim = 1
+        elif dim in ("2D", 2):
+            dim = 2
+        else:
+            raise KeyError(f"unsupported dimension {dim!r}")
+        if precision not in _native.PRECISION:
+            raise KeyError(f"precision must be one of {sorted(_native.PRECISION)}")
+        self.dim, self.nx = dim, int(nx)
+        self.ny = int(ny) if dim == 2 else 1
+        self.dx = float(dx)
+        self.dy = float(dy) if dim == 2 else 1.0
+        self.nv = 12 if dim == 2 else 11
+        self.precision = precision
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.mech = mechanism if isinstance(mechanism, _mech.Mechanism) else _mech.load(mechanism, nondim_config)
+        self._params = _mech.pack(self.mech)
+        bc = boundary_config or {}
+        kinds = []
+        for key in BOUNDARY_KEYS[: 2 * dim]:
+            name = bc.get(key, "periodic")
+            if callable(name):
+                raise NotImplementedError(
+                    f"{key}: Python callables cannot run inside the kernels; use a named "
+                    f"boundary ({', '.join(_native.BC_KIND)})")
+            if name not in _native.BC_KIND:
+                raise KeyError(f"{key}: unknown boundary condition {name!r}")
+            kinds.append(_native.BC_KIND[name])
+        kinds += [0] * (4 - len(kinds))
+        self.boundary_kinds = kinds
+        self._theta_key = None
+        self._theta_keep = None
+        L = _native.lib()
+        h = ctypes.c_void_p()
+        arr = (ctypes.c_int * 4)(*kinds)
+        with torch.cuda.device(self.device):
+            rc = L.jb_create(ctypes.byref(self._params), dim, self.nx, self.ny, self.dx, self.dy, arr,
+                             _native.PRECISION[precision], ctypes.byref(h))
+        _native.check(rc, None, "jb_create")
+        self._h = h
+        self._lib = L
+
+    # ------------------------------------------------------------------ utils
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.jb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny) if self.dim == 2 else (self.nx,)
+
+    def _check_state(self, U, aux=None):
+        for name, t, nv in (("U", U, self.nv), ("aux", aux, 2)):
+            if t is None:
+                continue
+            if not isinstance(t, torch.Tensor) or t.device.type != "cuda":
+                raise TypeError(f"{name} must be a CUDA tensor")
+            if t.dtype != torch.float64:
+                raise TypeError(f"{name} must be float64")
+            if tuple(t.shape) != (nv,) + self.shape:
+                raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {(nv,) + self.shape}")
+            if not t.is_contiguous():
+                raise ValueError(f"{name} must be contiguous")
+
+    def _spacing(self, dx, dy):
+        dx = self.dx if dx is None else float(dx)
+        dy = self.dy if (dy is None or self.dim == 1) else float(dy)
+        if dx != self.dx or dy != self.dy:
+            _native.check(self._lib.jb_set_spacing(self._h, dx, dy), self._h, "jb_set_spacing")
+            self.dx, self.dy = dx, dy
+
+    def set_theta(self, theta):
+        """theta['Pb'] for pressure outlets; theta['Yinj'] (8, nx[, 1]) or (8,)
+        for the injector."""
+        if theta is None:
+            theta = {}
+        Pb = float(theta.get("Pb", 0.0))
+        Yinj = theta.get("Yinj", None)
+        key = (Pb, None if Yinj is None else id(Yinj))
+        if key == self._theta_key:
+            return
+        yptr = None
+        if Yinj is not None:
+            y = torch.as_tensor(np.asarray(Yinj.cpu() if isinstance(Yinj, torch.Tensor) else Yinj),
+                                dtype=torch.float64)
+            if y.ndim == 1:
+                y = y[:, None].expand(y.shape[0], self.nx)
+            y = y.reshape(y.shape[0], self.nx).contiguous().to(self.device)
+            self._theta_keep = y
+            yptr = _ptr(y)
+        if any(k == _native.BC_KIND["pressure_outlet"] for k in self.boundary_kinds[: 2 * self.dim]) \
+                and "Pb" not in theta:
+            raise KeyError("Pb")
+        if any(k == _native.BC_KIND["rdc_injector"] for k in self.boundary_kinds[: 2 * self.dim]) \
+                and Yinj is None:
+            raise KeyError("Yinj")
+        _native.check(self._lib.jb_set_theta(self._h, Pb, yptr, 1.0), self._h, "jb_set_theta")
+        self._theta_key = key
+
+    def status(self):
+        st = ctypes.c_uint()
+        _native.check(self._lib.jb_status(self._h, ctypes.byref(st), _stream()), self._h, "jb_status")
+        return st.value
+
+    def set_kernel_timing(self, enable=True):
+        _native.check(self._lib.jb_set_kernel_timing(self._h, int(enable)), self._h, "jb_set_kernel_timing")
+
+    def kernel_times(self):
+        """{category: (milliseconds, launches)} accumulated since
+        set_kernel_timing (categories: flux, select, chem, other)."""
+        ms = (ctypes.c_double * 4)()
+        n = (ctypes.c_longlong * 4)()
+        _native.check(self._lib.jb_kernel_times(self._h, ms, n), self._h, "jb_kernel_times")
+        return {k: (ms[i], n[i]) for i, k in enumerate(("flux", "select", "chem", "other"))}
+
+    def workspace_bytes(self):
+        return int(self._lib.jb_workspace_bytes(self._h))
+
+    # ------------------------------------------------ reference entry points
+    def flux_func(self, U, aux, dx=None, dy=None, dt=1.0, theta=None):
+        """dt * total_flux(BC(U, aux)) (set_simulator.py:26-29 / 44-47)."""
+        self._check_state(U, aux)
+        self._spacing(dx, dy)
+        self.set_theta(theta)
+        out = torch.empty_like(U)
+        _native.check(self._lib.jb_flux_func(self._h, _ptr(U), _ptr(aux), float(dt), _ptr(out), _stream()),
+                      self._h, "jb_flux_func")
+        return out
+
+    def update_aux(self, U, aux):
+        """aux_func.update_aux: (gamma, T) from the Halley solve."""
+        self._check_state(U, aux)
+        out = torch.empty_like(aux)
+        _native.check(self._lib.jb_update_aux(self._h, _ptr(U), _ptr(aux), _ptr(out), _stream()),
+                      self._h, "jb_update_aux")
+        return out
+
+    def reaction_source_terms(self, U, aux, dt, theta=None):
+        """reaction_model.reaction_source_terms: point-implicit chemistry dU."""
+        self._check_state(U, aux)
+        out = torch.empty_like(U)
+        _native.check(self._lib.jb_reaction_source_terms(self._h, _ptr(U), _ptr(aux), float(dt), _ptr(out),
+                                                         _stream()), self._h, "jb_reaction_source_terms")
+        return out
+
+    def advance(self, U, aux, nsteps=1, dt=None, cfl=None, theta=None, dt_hist=None):
+        """``nsteps`` fused steps; CFL time steps when ``cfl`` is given,
+        otherwise the fixed ``dt``.  Returns (U, aux, dt_hist) with dt_hist a
+        device tensor of the step sizes."""
+        self._check_state(U, aux)
+        self.set_theta(theta)
+        if cfl is None and dt is None:
+            raise ValueError("need dt or cfl")
+        U_out = torch.empty_like(U)
+        aux_out = torch.empty_like(aux)
+        if dt_hist is None:
+            dt_hist = torch.empty(nsteps, dtype=torch.float64, device=U.device)
+        rc = self._lib.jb_advance(self._h, _ptr(U), _ptr(aux), _ptr(U_out), _ptr(aux_out),
+                                  float(dt or 0.0), float(cfl or 0.0), int(nsteps), _ptr(dt_hist), _stream())
+        _native.check(rc, self._h, "jb_advance")
+        return U_out, aux_out, dt_hist
+
+    def advance_one_step(self, U, aux, dx=None, dy=None, dt=None, theta=None):
+        """set_advance_func's advance_one_step(U, aux, dx, dy, dt, theta)."""
+        self._spacing(dx, dy)
+        U, aux, _ = self.advance(U, aux, 1, dt=dt, theta=theta)
+        return U, aux
+
+    def cfl_dt(self, U, aux, cfl):
+        self._check_state(U, aux)
+        out = torch.empty((), dtype=torch.float64, device=U.device)
+        _native.check(self._lib.jb_cfl_dt(self._h, _ptr(U), _ptr(aux), float(cfl), _ptr(out), _stream()),
+                      self._h, "jb_cfl_dt")
+        return out
+
+    def get_thermo(self, T, Y):
+        """thermo_model.get_thermo(T, Y) -> (cp, gamma, h, R, dcp), each with
+        T's shape; T is (1, ...) and Y (8, ...)."""
+        T = T.contiguous()
+        Y = Y.contiguous()
+        n = T.numel()
+        outs = [torch.empty_like(T) for _ in range(5)]
+        _native.check(self._lib.jb_get_thermo(self._h, n, _ptr(T), _ptr(Y), *[_ptr(o) for o in outs], _stream()),
+                      self._h, "jb_get_thermo")
+        return tuple(outs)
+
+    def state_from_PTY(self, P, T, Y, vel=None):
+        """Conserved state from pressure, temperature and mass fractions as the
+        reference's examples build it: rho = P/(R T), rho E = rho h - P
+        (+ kinetic), aux = [gamma, T]."""
+        _, gamma, h, R, _ = self.get_thermo(T, Y)
+        rho = P / (R * T)
+        E = rho * h - P
+        nd = T.ndim - 1
+        if vel is None:
+            vel = [torch.zeros_like(T) for _ in range(nd)]
+        for v in vel:
+            E = E + 0.5 * rho * v ** 2
+        U = torch.cat([rho] + [rho * v for v in vel] + [E, rho * Y], dim=0).contiguous()
+        aux = torch.cat([gamma, T], dim=0).contiguous()
+        return U, aux

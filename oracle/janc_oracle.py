@@ -238,15 +238,26 @@ def _ex(v, nd):
 # --------------------------------------------------------------------------
 # thermo  (model/thermo_model.py)
 # --------------------------------------------------------------------------
+def _seqsum(a):
+    """Sum over the leading axis in index order, keeping it (size 1).  This is
+    the order NumPy uses for a C-contiguous array; making it explicit keeps
+    the oracle independent of the caller's memory layout (NumPy sums a
+    Fortran-ordered array pairwise)."""
+    s = a[0:1]
+    for i in range(1, a.shape[0]):
+        s = s + a[i:i + 1]
+    return s
+
+
 def fill_Y(Y):
     """thermo_model.py:80-82"""
-    return np.concatenate([Y, 1.0 - np.sum(Y, axis=0, keepdims=True)], axis=0)
+    return np.concatenate([Y, 1.0 - _seqsum(Y)], axis=0)
 
 
 def get_R(m, Y):
     """thermo_model.py:87-92"""
     Yf = fill_Y(Y)
-    return np.sum(1 / _ex(m.species_M, Y.ndim - 1) * Yf, axis=0, keepdims=True)
+    return _seqsum(1 / _ex(m.species_M, Y.ndim - 1) * Yf)
 
 
 def _polyval(p, x):
@@ -272,9 +283,9 @@ def get_thermo(m, T, Y):
     R = get_R(m, Y)
     Yf = fill_Y(Y)
     cp_i, dcp_i, h_i = get_thermo_properties(m, T[0])
-    cp = np.sum(cp_i * Yf, axis=0, keepdims=True)
-    h = np.sum(h_i * Yf, axis=0, keepdims=True)
-    dcp = np.sum(dcp_i * Yf, axis=0, keepdims=True)
+    cp = _seqsum(cp_i * Yf)
+    h = _seqsum(h_i * Yf)
+    dcp = _seqsum(dcp_i * Yf)
     gamma = cp / (cp - R)
     return cp, gamma, h, R, dcp
 
@@ -375,12 +386,12 @@ def construct_matrix_equation(m, T, X, dt):
         vb_i = _ex(m.vb[i], nd)
         aij = _ex(m.third_body[i], nd)
         kf_i = m.A[i] * np.power(T, m.B[i]) * np.exp(-m.EaR[i] / T)
-        aij_X_sum = np.sum(aij * X, axis=0, keepdims=True)
+        aij_X_sum = _seqsum(aij * X)
         aij_X_sum = m.is_third_body[i] * aij_X_sum + (1 - m.is_third_body[i])
-        kf = kf_i * np.exp(np.sum(vf_i * log_X, axis=0, keepdims=True))
-        kb = kf_i / (np.exp(np.sum((vb_i - vf_i) * g, axis=0, keepdims=True))
+        kf = kf_i * np.exp(_seqsum(vf_i * log_X))
+        kb = kf_i / (np.exp(_seqsum((vb_i - vf_i) * g))
                      * ((101325 / m.nondim.P0 / T) ** m.vsum[i])) \
-            * np.exp(np.sum(vb_i * log_X, axis=0, keepdims=True))
+            * np.exp(_seqsum(vb_i * log_X))
         kf_l.append(kf)
         kb_l.append(kb)
         M_l.append(aij_X_sum)
@@ -389,7 +400,7 @@ def construct_matrix_equation(m, T, X, dt):
     for k in range(nr):
         Mk = m.species_M[k]
         terms = [(m.vb[i, k] - m.vf[i, k]) * M_l[i] * (kf_l[i] - kb_l[i]) for i in range(nreac)]
-        w.append(Mk * np.sum(np.stack(terms), axis=0)[0])
+        w.append(Mk * _seqsum(np.stack(terms))[0, 0])
         for n in range(nr):
             Mn = m.species_M[n]
             Xn = Xc[n][None]
@@ -399,7 +410,7 @@ def construct_matrix_equation(m, T, X, dt):
                 ain = m.third_body[i, n]
                 tn.append(dv * (kf_l[i] - kb_l[i]) * (ain / Mn)
                           + 1 / (Mn * Xn) * dv * M_l[i] * (m.vf[i, n] * kf_l[i] - m.vb[i, n] * kb_l[i]))
-            J[k, n] = Mk * np.sum(np.stack(tn), axis=0)[0]
+            J[k, n] = Mk * _seqsum(np.stack(tn))[0, 0]
     S = np.moveaxis(np.stack(w), 0, -1)[..., None]               # (..., nr, 1)
     DSDU = np.moveaxis(np.moveaxis(J, 0, -1), 0, -1)             # (..., nr, nr)
     Amat = np.eye(nr) / dt - DSDU

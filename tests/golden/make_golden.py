@@ -55,11 +55,19 @@ def _sim_config(dim, mech, grid, bc, nondim=None, cfl=0.5, dt=None):
     return cfg
 
 
+def C(x):
+    """C-contiguous float64 array.  NumPy sums a C-contiguous (n, ...) array over axis 0
+    row by row (sequentially); a Fortran-ordered one is summed pairwise.  All
+    inputs are made C-contiguous so the species sums run in index order."""
+    import jax.numpy as jnp
+    return jnp.array(np.ascontiguousarray(np.asarray(x, dtype=np.float64)))
+
+
 def _state(thermo_model, P, T, Y, vel=None):
     """Conserved state from (P, T, Y) with the reference's own get_thermo, as
     the examples build it: rho = P/(R T), rhoE = rho h - P (+ kinetic)."""
-    import jax.numpy as jnp
-    _, gamma, h, R, _ = thermo_model.get_thermo(jnp.array(T), jnp.array(Y))
+    P, T, Y = (np.ascontiguousarray(a) for a in (P, T, Y))
+    _, gamma, h, R, _ = thermo_model.get_thermo(C(T), C(Y))
     rho = P / (R * T)
     E = rho * h - P
     nd = T.ndim - 1
@@ -69,7 +77,7 @@ def _state(thermo_model, P, T, Y, vel=None):
         E = E + 0.5 * rho * v ** 2
     U = np.concatenate([rho] + [rho * v for v in vel] + [E, rho * Y], axis=0)
     aux = np.concatenate([gamma, T], axis=0)
-    return np.asarray(U), np.asarray(aux)
+    return np.ascontiguousarray(U), np.ascontiguousarray(aux)
 
 
 def _stoich_Y(phi=1.0):
@@ -150,8 +158,8 @@ def main():
     nT = 64
     T = np.concatenate([[250.0, 300.0, 999.999999, 1000.0, 1000.000001, 2500.0, 3400.0],
                         rng.uniform(260.0, 3500.0, nT - 7)])[None, :]
-    Y = rng.dirichlet(np.ones(9), nT).T[:8] * rng.uniform(0.2, 1.0, nT)
-    cp, gamma, h, R, dcp = thermo_model.get_thermo(jnp.array(T), jnp.array(Y))
+    Y = np.ascontiguousarray(rng.dirichlet(np.ones(9), nT).T[:8] * rng.uniform(0.2, 1.0, nT))
+    cp, gamma, h, R, dcp = thermo_model.get_thermo(C(T), C(Y))
     np.savez(os.path.join(HERE, "thermo_si.npz"), T=T, Y=Y, cp=cp, gamma=gamma, h=h, R=R, dcp=dcp)
 
     # temperature solve: three guesses per state (far, near, exact)
@@ -166,7 +174,7 @@ def main():
                         ("near", Ts * (1 + 1e-7 * rng.standard_normal(Ts.shape))),
                         ("exact", Ts.copy())):
         aux_in = np.concatenate([aux_s[0:1], guess])
-        out = aux1.update_aux(jnp.array(U_s), jnp.array(aux_in))
+        out = aux1.update_aux(C(U_s), C(aux_in))
         cases[f"aux_in_{name}"] = aux_in
         cases[f"aux_out_{name}"] = np.asarray(out)
     np.savez(os.path.join(HERE, "update_aux_si.npz"), U=U_s, **cases)
@@ -187,7 +195,7 @@ def main():
     Uc, auxc = _state(thermo_model, Pc, Tc, Yc)
     chem = {"U": Uc, "aux": auxc}
     for dt in (1e-9, 1e-8, 1e-7):
-        S = reaction_model.reaction_source_terms(jnp.array(Uc), jnp.array(auxc), dt, None)
+        S = reaction_model.reaction_source_terms(C(Uc), C(auxc), dt, None)
         chem[f"S_{dt:.0e}"] = np.asarray(S)
     np.savez(os.path.join(HERE, "chem_si.npz"), **chem)
     print("1D thermo/chem done", time.time() - t_start, flush=True)
@@ -202,8 +210,8 @@ def main():
     rec = {"U0": U0, "aux0": aux0, "dx": 0.1 / nx}
     # flux_func on the initial state, and on a state with motion
     flux_func, update_func, _ = set_simulator.set_rhs("1D", cfg["reaction_config"])
-    rec["rhs0"] = np.asarray(flux_func(jnp.array(U0), jnp.array(aux0), 0.1 / nx, None, 1e-7, None))
-    U, aux, t = jnp.array(U0), jnp.array(aux0), 0.0
+    rec["rhs0"] = np.asarray(flux_func(C(U0), C(aux0), 0.1 / nx, None, 1e-7, None))
+    U, aux, t = C(U0), C(aux0), 0.0
     dts = []
     for step in range(1, 11):
         U, aux, t, dt = sim.advance_func(U, aux, t, None)
@@ -214,6 +222,35 @@ def main():
     rec["dts"] = np.array(dts)
     np.savez(os.path.join(HERE, "step1d_si.npz"), **rec)
     print("1D steps done", time.time() - t_start, flush=True)
+
+    # config 0 at full size (2000 cells, slab = first 2 %, CFL 0.5): the
+    # reference's own step goes non-finite after a few steps because the
+    # first-order point-implicit chemistry burns a slab-edge cell in one step
+    # and the Halley solve then diverges beyond the NASA7 range.
+    nxc = 2000
+    cfgc = _sim_config("1D", mech, {"dx": 0.1 / nxc},
+                       {"left_boundary": "slip_wall", "right_boundary": "zero_gradient"})
+    simc = set_simulator.Simulator(cfgc)
+    P = np.full((1, nxc), 101325.0)
+    T = np.full((1, nxc), 300.0)
+    Y = np.tile(_stoich_Y(1.0)[:, None], (1, nxc))
+    P[:, :40] = 30 * 101325.0
+    T[:, :40] = 3000.0
+    U0, aux0 = _state(thermo_model, P, T, Y)
+    rec = {"U0": U0, "aux0": aux0, "dx": 0.1 / nxc}
+    U, aux, t = C(U0), C(aux0), 0.0
+    first_bad = -1
+    for step in range(1, 21):
+        U, aux, t, dt = simc.advance_func(U, aux, t, None)
+        if step in (1, 10):
+            rec[f"U_{step}"] = np.asarray(U)
+            rec[f"aux_{step}"] = np.asarray(aux)
+        if not np.all(np.isfinite(np.asarray(U))):
+            first_bad = step
+            break
+    rec["first_nonfinite_step"] = np.array(first_bad)
+    np.savez_compressed(os.path.join(HERE, "config0_cfl05.npz"), **rec)
+    print("config-0 CFL 0.5: first non-finite step", first_bad, time.time() - t_start, flush=True)
 
     # 1D boundary variants of flux_func on a moving, non-uniform state
     bvar = {}
@@ -228,7 +265,7 @@ def main():
                    ("pressure_outlet", "pressure_outlet"), ("no_slip_wall", "zero_gradient")):
         ref_boundary.set_boundary({"left_boundary": lb, "right_boundary": rb}, "1D")
         theta = {"Pb": 101325.0 * 1.3}
-        r = flux_func(jnp.array(Ub), jnp.array(auxb), 0.1 / nxb, None, 2e-8, theta)
+        r = flux_func(C(Ub), C(auxb), 0.1 / nxb, None, 2e-8, theta)
         bvar[f"rhs_{lb}_{rb}"] = np.asarray(r)
     np.savez(os.path.join(HERE, "bc1d_si.npz"), **bvar)
 
@@ -247,8 +284,8 @@ def main():
     U0, aux0 = _state(thermo_model, P, T, Y)
     rec = {"U0": U0, "aux0": aux0, "dx": Lx / nx2, "dy": Ly / ny2}
     flux2, _, _ = set_simulator.set_rhs("2D", cfg2["reaction_config"])
-    rec["rhs0"] = np.asarray(flux2(jnp.array(U0), jnp.array(aux0), Lx / nx2, Ly / ny2, 1e-8, None))
-    U, aux, t = jnp.array(U0), jnp.array(aux0), 0.0
+    rec["rhs0"] = np.asarray(flux2(C(U0), C(aux0), Lx / nx2, Ly / ny2, 1e-8, None))
+    U, aux, t = C(U0), C(aux0), 0.0
     dts = []
     for step in range(1, 4):
         U, aux, t, dt = sim2.advance_func(U, aux, t, None)
@@ -260,9 +297,9 @@ def main():
     # own rhs/update callables
     adv = set_simulator.set_advance_func("2D", cfg2["flux_config"], cfg2["reaction_config"],
                                          cfg2["time_config"], False, flux2, aux2.update_aux, None)
-    Ua, auxa = adv(jnp.array(U0), jnp.array(aux0), Lx / nx2, Ly / ny2, 2e-8, None)
+    Ua, auxa = adv(C(U0), C(aux0), Lx / nx2, Ly / ny2, 2e-8, None)
     rec["U_adv_dt2e-8"], rec["aux_adv_dt2e-8"] = np.asarray(Ua), np.asarray(auxa)
-    Ur, auxr = time_step_dict["TVD_RK3"](jnp.array(U0), jnp.array(aux0), Lx / nx2, Ly / ny2, 2e-8,
+    Ur, auxr = time_step_dict["TVD_RK3"](C(U0), C(aux0), Lx / nx2, Ly / ny2, 2e-8,
                                          None, flux2, aux2.update_aux)
     rec["U_rk3_dt2e-8"], rec["aux_rk3_dt2e-8"] = np.asarray(Ur), np.asarray(auxr)
     np.savez(os.path.join(HERE, "step2d_si.npz"), **rec)
@@ -286,7 +323,7 @@ def main():
         ref_boundary.set_boundary({"left_boundary": lb, "right_boundary": rb,
                                    "bottom_boundary": bb, "top_boundary": tb}, "2D")
         theta = {"Pb": 101325.0 * 1.3}
-        r = flux2(jnp.array(Ub), jnp.array(auxb), 1e-4, 2e-4, 2e-8, theta)
+        r = flux2(C(Ub), C(auxb), 1e-4, 2e-4, 2e-8, theta)
         bvar[f"rhs_{lb}_{rb}_{bb}_{tb}"] = np.asarray(r)
     np.savez(os.path.join(HERE, "bc2d_si.npz"), **bvar)
     print("2D BC done", time.time() - t_start, flush=True)
@@ -322,8 +359,8 @@ def main():
     U0, aux0 = _state(thermo_model, P, T, Y)
     rec = {"U0": U0, "aux0": aux0, "dx": dx3, "dy": dx3, "Yinj": Yinj, "Pb": 101325.0 / P0}
     flux3, _, _ = set_simulator.set_rhs("2D", cfg3["reaction_config"])
-    rec["rhs0"] = np.asarray(flux3(jnp.array(U0), jnp.array(aux0), dx3, dx3, 1e-3, theta))
-    U, aux, t = jnp.array(U0), jnp.array(aux0), 0.0
+    rec["rhs0"] = np.asarray(flux3(C(U0), C(aux0), dx3, dx3, 1e-3, theta))
+    U, aux, t = C(U0), C(aux0), 0.0
     dts = []
     for step in range(1, 4):
         U, aux, t, dt = sim3.advance_func(U, aux, t, theta)

@@ -155,3 +155,24 @@ def test_steps_2d_rdc(golden_dir, mech_rdc):
     for step in range(1, 4):
         U, aux, t, dt = s.advance_func(U, aux, t, theta)
         _check_state(U, aux, g[f"U_{step}"], g[f"aux_{step}"], 1e-12)
+
+
+def test_config0_cfl05_blows_up_like_reference(golden_dir, mech_si):
+    """Config 0 exactly as stated (2000 cells, 30 atm / 3000 K slab of fresh
+    mixture, CFL 0.5): the reference's own step goes non-finite at the same
+    step in the oracle, and the states before agree bitwise."""
+    g = _load(golden_dir, "config0_cfl05")
+    bc = {"left_boundary": "slip_wall", "right_boundary": "zero_gradient"}
+    s = jo.Solver(mech_si, "1D", float(g["dx"]), None, bc, 0.5)
+    U, aux, t = g["U0"], g["aux0"], 0.0
+    first_bad = -1
+    with np.errstate(all="ignore"):
+        for step in range(1, 21):
+            U, aux, t, dt = s.advance_func(U, aux, t)
+            if f"U_{step}" in g.files:
+                np.testing.assert_array_equal(U, g[f"U_{step}"])
+                np.testing.assert_array_equal(aux, g[f"aux_{step}"])
+            if not np.all(np.isfinite(U)):
+                first_bad = step
+                break
+    assert first_bad == int(g["first_nonfinite_step"]) > 0
