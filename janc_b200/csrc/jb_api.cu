@@ -7,7 +7,10 @@
 #include <cstring>
 #include <new>
 
+#include <cmath>
+
 #include "../../include/janc_b200.h"
+#include "jb_chem_gen.cuh"
 #include "jb_ops.h"
 
 struct jb_handle {
@@ -71,6 +74,26 @@ int check_cuda(jb_handle* h, cudaError_t e, const char* what) {
 
 bool bc_ok(int k) { return k >= JB_BC_PERIODIC && k <= JB_BC_RDC_INJECTOR; }
 
+// Derived tables and the structure check against the generated chemistry.
+void derive(jb_mech_params& m) {
+  int ok = m.ns == JB_GEN_NS && m.nr == JB_GEN_NR && m.nreac == JB_GEN_NREAC;
+  for (int i = 0; i < m.nreac; ++i) {
+    m.lnA[i] = std::log(m.A[i]);
+    if (!(m.A[i] > 0.0)) ok = 0;
+    for (int n = 0; n < m.nr; ++n) m.tbinvM[i][n] = m.tb[i][n] / m.M[n];
+    if (ok) {
+      if ((int)m.is_tb[i] != JB_GEN_ISTB[i] || (int)m.vsum[i] != JB_GEN_VSUM[i]) ok = 0;
+      for (int k = 0; k < m.nr; ++k)
+        if (m.vf[i][k] != (double)JB_GEN_VF[i][k] || m.vb[i][k] != (double)JB_GEN_VB[i][k]) ok = 0;
+      for (int j = 0; j < m.ns; ++j)
+        if ((m.tb[i][j] != 0.0) != (JB_GEN_TBNZ[i][j] != 0)) ok = 0;
+    }
+  }
+  m.lnpref = std::log(m.pref);
+  m.lnT0 = std::log(m.T0);
+  m.gen_ok = ok;
+}
+
 }  // namespace
 
 extern "C" {
@@ -94,6 +117,7 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   if (!h) return JB_ERR_ARG;
   std::memset(h, 0, sizeof(*h));
   h->mech = *mech;
+  derive(h->mech);
   h->dim = dim;
   h->precision = precision;
   h->ops = precision == JB_PREC_STRICT ? &jb::strict_ops : &jb::fast_ops;

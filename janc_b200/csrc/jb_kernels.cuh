@@ -217,6 +217,21 @@ template <int DIM>
 __device__ __forceinline__ Prim<DIM> u_to_prim(const MP& m, const double* q, double gamma, double T) {
   Prim<DIM> r;
   constexpr int nY = DIM == 1 ? 3 : 4;
+#if JB_FAST
+  // one reciprocal; p = T sum_k (rho Y_k)/M_k with rho Y_N2 = rho - sum rho Y_k
+  r.rho = q[0];
+  const double ri = 1.0 / r.rho;
+  r.u = q[1] * ri;
+  r.v = DIM == 2 ? q[2] * ri : 0.0;
+  double sr = q[nY], pr = m.invM[0] * q[nY];
+#pragma unroll
+  for (int k = 1; k < NR; ++k) { sr += q[nY + k]; pr += m.invM[k] * q[nY + k]; }
+  pr += m.invM[NR] * (r.rho - sr);
+  r.R = pr * ri;
+  r.p = pr * T;
+  r.a = sqrt(gamma * r.p * ri);
+  return r;
+#endif
   r.rho = q[0];
   r.u = q[1] / r.rho;
   r.v = DIM == 2 ? q[2] / r.rho : 0.0;
@@ -351,6 +366,44 @@ constexpr double W_Q = 1.0 / 4.0, W_D = 13.0 / 12.0;
 constexpr double W_13 = 1.0 / 3.0, W_76 = 7.0 / 6.0, W_116 = 11.0 / 6.0;
 constexpr double W_m16 = -1.0 / 6.0, W_56 = 5.0 / 6.0, W_16 = 1.0 / 6.0;
 
+#if JB_FAST
+// Same weights with one division: alpha_k = C_k / d_k^2 is scaled by
+// d_1^2 d_2^2 d_3^2, so w_k = C_k prod_{j!=k} d_j^2 / sum.  (The float64
+// range covers the squared products of the smoothness indicators met here.)
+__device__ __forceinline__ double weno_combine(double IS1, double IS2, double IS3, double q1, double q2,
+                                               double q3) {
+  const double e1 = W_EPS + IS1, e2 = W_EPS + IS2, e3 = W_EPS + IS3;
+  const double s1 = e1 * e1, s2 = e2 * e2, s3 = e3 * e3;
+  const double a1 = W_C1 * (s2 * s3), a2 = W_C2 * (s1 * s3), a3 = W_C3 * (s1 * s2);
+  return (a1 * q1 + a2 * q2 + a3 * q3) / (a1 + a2 + a3);
+}
+
+__device__ __forceinline__ double weno_L(double fjm2, double fjm1, double fj, double fjp1, double fjp2) {
+  double t1 = fjm2 - 4.0 * fjm1 + 3.0 * fj, s1 = fjm2 - 2.0 * fjm1 + fj;
+  double t2 = fjm1 - fjp1, s2 = fjm1 - 2.0 * fj + fjp1;
+  double t3 = 3.0 * fj - 4.0 * fjp1 + fjp2, s3 = fj - 2.0 * fjp1 + fjp2;
+  double IS1 = W_Q * (t1 * t1) + W_D * (s1 * s1);
+  double IS2 = W_Q * (t2 * t2) + W_D * (s2 * s2);
+  double IS3 = W_Q * (t3 * t3) + W_D * (s3 * s3);
+  double q1 = W_13 * fjm2 - W_76 * fjm1 + W_116 * fj;
+  double q2 = W_m16 * fjm1 + W_56 * fj + W_13 * fjp1;
+  double q3 = W_13 * fj + W_56 * fjp1 - W_16 * fjp2;
+  return weno_combine(IS1, IS2, IS3, q1, q2, q3);
+}
+
+__device__ __forceinline__ double weno_R(double fjm2, double fjm1, double fj, double fjp1, double fjp2) {
+  double t1 = fjp2 - 4.0 * fjp1 + 3.0 * fj, s1 = fjp2 - 2.0 * fjp1 + fj;
+  double t2 = fjp1 - fjm1, s2 = fjp1 - 2.0 * fj + fjm1;
+  double t3 = 3.0 * fj - 4.0 * fjm1 + fjm2, s3 = fj - 2.0 * fjm1 + fjm2;
+  double IS1 = W_Q * (t1 * t1) + W_D * (s1 * s1);
+  double IS2 = W_Q * (t2 * t2) + W_D * (s2 * s2);
+  double IS3 = W_Q * (t3 * t3) + W_D * (s3 * s3);
+  double q1 = W_13 * fjp2 - W_76 * fjp1 + W_116 * fj;
+  double q2 = W_m16 * fjp1 + W_56 * fj + W_13 * fjm1;
+  double q3 = W_13 * fj + W_56 * fjm1 - W_16 * fjm2;
+  return weno_combine(IS1, IS2, IS3, q1, q2, q3);
+}
+#else
 // left-biased value at j+1/2 from cells j-2..j+2 (interface_L_*)
 __device__ __forceinline__ double weno_L(double fjm2, double fjm1, double fj, double fjp1, double fjp2) {
   double t1 = fjm2 - 4.0 * fjm1 + 3.0 * fj, s1 = fjm2 - 2.0 * fjm1 + fj;
@@ -384,6 +437,7 @@ __device__ __forceinline__ double weno_R(double fjm2, double fjm1, double fj, do
   double q3 = W_13 * fj + W_56 * fjm1 - W_16 * fjm2;
   return w1 * q1 + w2 * q2 + w3 * q3;
 }
+#endif
 
 // ---------------------------------------------------------------------------
 // ghost-cell source mapping (boundary/boundary.py:120-132,
@@ -476,7 +530,11 @@ __device__ __forceinline__ double lf_flux(int f, int dir, double q, double rho, 
     if (f == 3) return vn * (E + p);
   }
   (void)nY;
+#if JB_FAST
+  return vn * q;
+#else
   return rho * vn * (q / rho);
+#endif
 }
 
 // ---------------------------------------------------------------------------
@@ -856,9 +914,95 @@ __global__ void k_select(MP m, Grid g, const double* __restrict__ U, const doubl
   if (ALPHA || CFL) block_reduce_store(amx, amy, dtm, st << 16, slots, aidx, ALPHA, CFL, -1);
 }
 
+}  // namespace JB_NS
+}  // namespace jb
+
+#include "jb_chem_gen.cuh"
+
+namespace jb {
+namespace JB_NS {
+
 // ---------------------------------------------------------------------------
 // point-implicit chemistry (model/reaction_model.py:91-193)
 // ---------------------------------------------------------------------------
+// (I/dt - M_k J) x = M_k w by LU with partial pivoting (first maximal
+// |pivot| as LAPACK idamax), then detailed_reaction's clip and S = rho dY
+// (construct_matrix_equation, reaction_model.py:132-159 and :183-193).
+__device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], const double* w, double rho,
+                                           const double* Y8, double dt, double* S, unsigned& st) {
+  double b[NR];
+  const double idt = 1.0 / dt;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    b[k] = m.M[k] * w[k];
+#pragma unroll
+    for (int n = 0; n < NR; ++n) {
+      double jk = m.M[k] * J[k][n];
+      J[k][n] = (k == n ? idt : 0.0) - jk;  // J now holds A
+    }
+  }
+  // Every loop has a constant trip count so the matrix stays in registers;
+  // the row exchange is branch-free (selects).
+#pragma unroll
+  for (int c = 0; c < NR; ++c) {
+    int p = c;
+    double best = fabs(J[c][c]);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (r > c) {
+        double v = fabs(J[r][c]);
+        if (v > best) { best = v; p = r; }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (r > c) {
+        const bool sw = p == r;
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+          const double x0 = J[c][j], x1 = J[r][j];
+          J[c][j] = sw ? x1 : x0;
+          J[r][j] = sw ? x0 : x1;
+        }
+        const double y0 = b[c], y1 = b[r];
+        b[c] = sw ? y1 : y0;
+        b[r] = sw ? y0 : y1;
+      }
+    }
+    if (J[c][c] == 0.0) st |= JB_ERR_SINGULAR;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (r > c) {
+        const double l = J[r][c] / J[c][c];
+#pragma unroll
+        for (int j = 0; j < NR; ++j)
+          if (j > c) J[r][j] = J[r][j] - l * J[c][j];
+        b[r] = b[r] - l * b[c];
+      }
+    }
+  }
+  double x[NR];
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    const int r = NR - 1 - i;
+    double s = b[r];
+#pragma unroll
+    for (int j = 0; j < NR; ++j)
+      if (j > r) s = s - J[r][j] * x[j];
+    x[r] = s / J[r][r];
+  }
+  // detailed_reaction (:183-193): dY = clip(drhoY/rho, -Y, 1-Y); S = rho dY
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    double dY = x[k] / rho;
+    double lo = -Y8[k], hi = 1.0 - Y8[k];
+    dY = dY < lo ? lo : dY;
+    dY = dY > hi ? hi : dY;
+    S[k] = rho * dY;
+  }
+}
+
+
 // Rates, analytic Jacobian d(omega)/d(rho Y) and the solve of
 // (I/dt - J) x = omega for one cell.  Returns S_k = rho * clip(x_k/rho).
 __device__ void chem_cell(const MP& m, double rho, const double* Y8, double T, double dt,
@@ -933,71 +1077,51 @@ __device__ void chem_cell(const MP& m, double rho, const double* Y8, double T, d
       }
     }
   }
-  // A = I/dt - M_k J ; b = M_k w   (construct_matrix_equation, :132-159)
-  double A[NR][NR], b[NR];
-  const double idt = 1.0 / dt;
-#pragma unroll
-  for (int k = 0; k < NR; ++k) {
-    b[k] = m.M[k] * w[k];
-#pragma unroll
-    for (int n = 0; n < NR; ++n) {
-      double jk = m.M[k] * J[k][n];
-      A[k][n] = (k == n ? idt : 0.0) - jk;
-    }
-  }
-  // LU with partial pivoting (first maximal |pivot|, as LAPACK idamax)
-#pragma unroll
-  for (int c = 0; c < NR; ++c) {
-    int p = c;
-    double best = fabs(A[c][c]);
-#pragma unroll
-    for (int r = c + 1; r < NR; ++r) {
-      double v = fabs(A[r][c]);
-      if (v > best) { best = v; p = r; }
-    }
-#pragma unroll
-    for (int r = c + 1; r < NR; ++r) {
-      if (p == r) {
-#pragma unroll
-        for (int j = 0; j < NR; ++j) { double t = A[c][j]; A[c][j] = A[r][j]; A[r][j] = t; }
-        double t = b[c]; b[c] = b[r]; b[r] = t;
-      }
-    }
-    if (A[c][c] == 0.0) st |= JB_ERR_SINGULAR;
-#pragma unroll
-    for (int r = c + 1; r < NR; ++r) {
-      double l = A[r][c] / A[c][c];
-#pragma unroll
-      for (int j = c + 1; j < NR; ++j) A[r][j] = A[r][j] - l * A[c][j];
-      b[r] = b[r] - l * b[c];
-    }
-  }
-  double x[NR];
-#pragma unroll
-  for (int r = NR - 1; r >= 0; --r) {
-    double s = b[r];
-#pragma unroll
-    for (int j = r + 1; j < NR; ++j) s = s - A[r][j] * x[j];
-    x[r] = s / A[r][r];
-  }
-  // detailed_reaction (:183-193): dY = clip(drhoY/rho, -Y, 1-Y); S = rho dY
-#pragma unroll
-  for (int k = 0; k < NR; ++k) {
-    double dY = x[k] / rho;
-    double lo = -Y8[k], hi = 1.0 - Y8[k];
-    dY = dY < lo ? lo : dY;
-    dY = dY > hi ? hi : dY;
-    S[k] = rho * dY;
-  }
+  chem_solve(m, J, w, rho, Y8, dt, S, st);
 }
+
+#if JB_FAST
+constexpr int CHEM_SH = 3 * NREAC;  // per-cell shared doubles of the specialised path
+
+// Specialised chemistry (structure compiled in by gen_chem.py), log-space
+// rates, FMA-contracted.  sh points at this thread's column of a
+// [CHEM_SH][stride] shared array.
+__device__ __forceinline__ void chem_cell_gen(const MP& m, double rho, const double* Y8, double T,
+                                              double dt, double* S, unsigned& st, double* sh,
+                                              int stride) {
+  double Yf[NS], X[NS], lnX[NR], g[NR], rMX[NR], w[NR];
+  fill_Y(Y8, Yf);
+#pragma unroll
+  for (int k = 0; k < NS; ++k) X[k] = rho * Yf[k] * m.invM[k];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    const double xc = X[k] < 1e-50 ? 1e-50 : X[k];
+    lnX[k] = log(xc);
+    rMX[k] = m.invM[k] / xc;
+  }
+  const double lT = log(T), invT = 1.0 / T, lT0T = lT + m.lnT0;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    const bool lo = T < m.Tcr[k];
+    const double h = lo ? poly6(m.hc_lo[k], T) : poly6(m.hc_hi[k], T);
+    const double s = lo ? poly5(m.s_lo[k], T) + m.lg_lo[k] * lT0T : poly5(m.s_hi[k], T) + m.lg_hi[k] * lT0T;
+    g[k] = s - h * invT;
+  }
+  chem_rates_gen(m, lT, invT, X, lnX, g, sh, stride, w);
+  double J[NR][NR];
+  chem_jac_gen(m, rMX, sh, stride, J);
+  chem_solve(m, J, w, rho, Y8, dt, S, st);
+}
+#endif
 
 // WRITE_S: reaction_source_terms output S (zeros for the flow fields).
 // Otherwise U_out = U + S followed by the Halley iterates of the final
 // update_aux (set_simulator.py:117-122).
-template <int DIM, bool WRITE_S>
-__global__ void k_chem(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux,
-                       double* __restrict__ out, double* __restrict__ cand, Slots* slots, int midx,
-                       double dt_arg) {
+template <int DIM, bool WRITE_S, bool GEN>
+__global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __restrict__ U,
+                                              const double* __restrict__ aux,
+                                              double* __restrict__ out, double* __restrict__ cand,
+                                              Slots* slots, int midx, double dt_arg) {
   constexpr int nY = DIM == 1 ? 3 : 4;
   constexpr int nv = nY + NR;
   const long long nc = g.ncell;
@@ -1013,7 +1137,13 @@ __global__ void k_chem(MP m, Grid g, const double* __restrict__ U, const double*
 #pragma unroll
     for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / rho;
     double T = aux[nc + c];
+#if JB_FAST
+    extern __shared__ double shc[];
+    if (GEN) chem_cell_gen(m, rho, Y8, T, dt, S, st, shc + threadIdx.x, blockDim.x);
+    else chem_cell(m, rho, Y8, T, dt, S, st);
+#else
     chem_cell(m, rho, Y8, T, dt, S, st);
+#endif
     if (WRITE_S) {
 #pragma unroll
       for (int f = 0; f < nY; ++f) out[f * nc + c] = 0.0;

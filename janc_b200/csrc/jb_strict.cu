@@ -2,6 +2,7 @@
 // no multiply-add pair is contracted and each expression rounds as NumPy/XLA
 // float64 does.  Transcendentals (exp, log, pow) are CUDA's.
 #define JB_NS strict
+#define JB_FAST 0
 #define JB_NS_NAME "fp64_strict"
 #define JB_OPS_NAME strict_ops
 #include "jb_variant.inc"

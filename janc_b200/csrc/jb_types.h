@@ -1,7 +1,8 @@
 // Plain-old-data types shared by the host launcher and the device kernels.
 // No torch or CUDA-runtime types appear here so the C ABI header can mirror
 // the layouts one-for-one.
-#pragma once
+#ifndef JB_TYPES_H
+#define JB_TYPES_H
 #include <stdint.h>
 
 #define JB_NS_MAX 9      // species including the implicit last (inert) one
@@ -30,6 +31,12 @@ typedef struct jb_mech_params {
   double tb[JB_NREAC_MAX][JB_NS_MAX];  // third-body efficiencies (scaled)
   double T0;        // nondim reference temperature (gibbs uses log(T0*T))
   double pref;      // 101325 / P0 (reaction_model.py:113)
+  // derived by jb_create (callers leave these zero)
+  double lnA[JB_NREAC_MAX];
+  double tbinvM[JB_NREAC_MAX][JB_NR_MAX];  // tb[i][n] / M[n]
+  double lnpref, lnT0;
+  int gen_ok;       // structure matches the generated specialised chemistry
+  int pad2_;
 } jb_mech_params;
 
 enum jb_bc_kind {
@@ -88,3 +95,5 @@ typedef struct jb_slots {
   unsigned int dtnan;               // a CFL candidate was NaN (jnp.min propagates it)
   double dt;                        // time step of the current step
 } jb_slots;
+
+#endif  // JB_TYPES_H

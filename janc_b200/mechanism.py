@@ -236,6 +236,10 @@ class MechParams(ctypes.Structure):
         ("vf", (ctypes.c_double * NR_MAX) * NREAC_MAX), ("vb", (ctypes.c_double * NR_MAX) * NREAC_MAX),
         ("dv", (ctypes.c_double * NR_MAX) * NREAC_MAX), ("tb", (ctypes.c_double * NS_MAX) * NREAC_MAX),
         ("T0", ctypes.c_double), ("pref", ctypes.c_double),
+        # derived by jb_create
+        ("lnA", ctypes.c_double * NREAC_MAX), ("tbinvM", (ctypes.c_double * NR_MAX) * NREAC_MAX),
+        ("lnpref", ctypes.c_double), ("lnT0", ctypes.c_double),
+        ("gen_ok", ctypes.c_int), ("pad2_", ctypes.c_int),
     ]
 
 
