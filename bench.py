@@ -319,16 +319,22 @@ def run_ours(args):
     if dist:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    legs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(e2e_steps)]
     e0.record()
-    for _ in range(e2e_steps):
+    for k in range(e2e_steps):
+        legs[k][0].record()
         dU = hU.to("cuda", non_blocking=True)
         daux = haux.to("cuda", non_blocking=True)
+        legs[k][1].record()
         rU, raux, _ = s.advance(dU, daux, 1, cfl=CFL, theta=theta)
+        legs[k][2].record()
         oU.copy_(rU, non_blocking=True)
         oaux.copy_(raux, non_blocking=True)
+        legs[k][3].record()
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
+    leg_ms = [sum(lg[i].elapsed_time(lg[i + 1]) for lg in legs) / e2e_steps for i in range(3)]
     if dist:
         t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -368,7 +374,7 @@ def run_ours(args):
                              "peak_source": "measured live (jb_probe_fp64_fma)",
                              "flops_per_cell": arith, "special_ops_per_cell": special},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": hbytes, "d2h_bytes_per_step": hbytes,
-                "steps": e2e_steps},
+                "steps": e2e_steps, "h2d_ms": leg_ms[0], "step_ms": leg_ms[1], "d2h_ms": leg_ms[2]},
         "clocks": clk,
         "wall_s_timed_region": t_wall,
     }
