@@ -93,6 +93,24 @@ int jb_set_spacing(jb_handle* h, double dx, double dy);
 int jb_sizeof_mech_params(void);
 int jb_sizeof_grid(void);
 
+/* update_aux without any device allocation (no counterpart in the reference,
+ * whose JAX functions always allocate their results through XLA).  For
+ * callers that cannot allocate device memory themselves - a plugin inside a
+ * host code that reserves all device memory at start-up, or a call made from
+ * within another runtime's operator whose memory that runtime owns - and so
+ * cannot call jb_create().  Same arguments and result as jb_update_aux() on a
+ * solver of that grid and precision, with U, aux_in and aux_out supplied by
+ * the caller.  Its scratch lives in one static device array inside the
+ * library, sized for at most JB_NOALLOC_MAX_CELLS cells (about 3.1 MB, held
+ * on every GPU that loads the library until exit); larger grids return
+ * JB_ERR_ARG.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller. */
+#define JB_NOALLOC_MAX_CELLS 65536
+int jb_update_aux_noalloc(const jb_mech_params* mech, int dim, int nx, int ny, int precision,
+                          const double* U, const double* aux_in, double* aux_out, void* stream);
+
 /* Measurement helpers (no reference counterpart).  jb_set_kernel_timing
  * enables CUDA events around each launch of jb_advance (at most JB_TIMED_MAX
  * launches between reads) and clears the totals; jb_kernel_times waits for

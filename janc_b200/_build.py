@@ -17,7 +17,7 @@ OBJ = os.path.join(HERE, "_objs")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 UNITS = [("jb_strict.cu", ["-fmad=false"]), ("jb_fast.cu", ["-fmad=true"]), ("jb_api.cu", []),
-         ("jb_probe.cu", [])]
+         ("jb_probe.cu", []), ("jb_noalloc.cu", [])]
 
 
 def _nvcc():

@@ -20,7 +20,8 @@ STATUS = {1: "bad argument", 2: "CUDA error", 4: "non-finite state", 8: "singula
 EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_func", "jb_update_aux",
            "jb_reaction_source_terms", "jb_advance", "jb_cfl_dt", "jb_get_thermo", "jb_status",
            "jb_workspace_bytes", "jb_set_spacing", "jb_sizeof_mech_params", "jb_sizeof_grid",
-           "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times"]
+           "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times",
+           "jb_update_aux_noalloc"]
 
 _lib = None
 
@@ -61,6 +62,7 @@ def lib(path=None):
     L.jb_set_spacing.argtypes = [vp, d, d]
     L.jb_probe_fp64_fma.argtypes = [i, i, dp, vp]
     L.jb_set_kernel_timing.argtypes = [vp, i]
+    L.jb_update_aux_noalloc.argtypes = [ctypes.POINTER(_mech.MechParams), i, i, i, i, dp, dp, dp, vp]
     L.jb_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
     L.jb_last_error.argtypes = [vp]
     L.jb_last_error.restype = ctypes.c_char_p

@@ -74,8 +74,10 @@ int check_cuda(jb_handle* h, cudaError_t e, const char* what) {
 
 bool bc_ok(int k) { return k >= JB_BC_PERIODIC && k <= JB_BC_RDC_INJECTOR; }
 
+}  // namespace
+
 // Derived tables and the structure check against the generated chemistry.
-void derive(jb_mech_params& m) {
+void jb::derive_mech(jb_mech_params& m) {
   int ok = m.ns == JB_GEN_NS && m.nr == JB_GEN_NR && m.nreac == JB_GEN_NREAC;
   for (int i = 0; i < m.nreac; ++i) {
     m.lnA[i] = std::log(m.A[i]);
@@ -94,7 +96,6 @@ void derive(jb_mech_params& m) {
   m.gen_ok = ok;
 }
 
-}  // namespace
 
 extern "C" {
 
@@ -117,7 +118,7 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   if (!h) return JB_ERR_ARG;
   std::memset(h, 0, sizeof(*h));
   h->mech = *mech;
-  derive(h->mech);
+  jb::derive_mech(h->mech);
   h->dim = dim;
   h->precision = precision;
   h->ops = precision == JB_PREC_STRICT ? &jb::strict_ops : &jb::fast_ops;

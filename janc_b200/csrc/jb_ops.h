@@ -36,4 +36,8 @@ struct Ops {
 extern const Ops strict_ops;
 extern const Ops fast_ops;
 
+// Fill the derived fields of a mechanism block (ln A, tb/M, ln pref, ln T0)
+// and flag whether its structure matches the generated chemistry.
+void derive_mech(jb_mech_params& m);
+
 }  // namespace jb
