@@ -14,9 +14,13 @@ slab-edge cell in one step; tests/golden/config0_cfl05.npz records it), and
 the work per step does not depend on the CFL number.
 
 Arms:
-  default            our CUDA path (fp64 unless --precision), device-timed
-                     with inputs resident (value) and end to end through the
-                     public API from pinned host buffers (e2e)
+  default            our CUDA path, mixed precision (float32 flux arithmetic;
+                     float64 state, temperature solve and chemistry) unless
+                     --precision; device-timed with inputs resident (value)
+                     and end to end through the public API from pinned host
+                     buffers (e2e).  The float64 path is timed beside it and
+                     the per-field relative L1 error of mixed against float64
+                     after --accuracy-steps steps is reported.
   --impl reference   the reference algorithm's CPU implementation: the
                      NumPy oracle restating src/janc_v2 (JAX is not available
                      on the box), run as independent replicas on all host
@@ -26,7 +30,6 @@ advances its own copy of the workload; value = total cells x steps / max time.
 """
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -45,6 +48,7 @@ METRIC = "reacting cell-updates/s"
 UNIT = "cell-updates/s"
 BYTES_CHEM_PER_CELL = 224      # read U,aux (112 B) + write U,aux (112 B), float64
 BYTES_STEP_PER_CELL = 864 + 224  # fused-step minimum + separate chemistry pass (2D)
+BYTES_FLUX_STAGE_PER_CELL = 288  # one RK stage of the fused minimum: (224 + 320 + 320) / 3
 
 
 RDC_NX, RDC_NY = 1600, 1000
@@ -216,20 +220,15 @@ def chem_flops_per_cell():
     return arith, special
 
 
-def run_ours(args):
-    import numpy as np
+def _setup_workload(args, precision):
     import torch
     from janc_b200.solver import Solver
-    from janc_b200 import _native
-
-    dist, rank, ws = _dist()
-    dev = torch.cuda.current_device()
     theta = None
     if args.workload == "channel":
         nx, ny = NX, NY
         dx, dy = LX / NX, LY / NY
         bc = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
-        s = Solver(2, nx, ny, dx, dy, bc, precision=args.precision)
+        s = Solver(2, nx, ny, dx, dy, bc, precision=precision)
         P, T, Y = c1_fields()
         workload = ("2D H2-air detonation channel 1024x256 (0.2 m x 0.05 m), 9sp/19r mechanism, "
                     "30 atm / 3000 K slab with 8 seeded +-5% blobs, slip walls, "
@@ -239,7 +238,7 @@ def run_ours(args):
         dx = dy = 1e-4 / RDC_ND["x0"]
         bc = {"left_boundary": "periodic", "right_boundary": "periodic",
               "bottom_boundary": "rdc_injector", "top_boundary": "pressure_outlet"}
-        s = Solver(2, nx, ny, dx, dy, bc, nondim_config=RDC_ND, precision=args.precision)
+        s = Solver(2, nx, ny, dx, dy, bc, nondim_config=RDC_ND, precision=precision)
         P, T, Y, Yinj = rdc_fields()
         theta = {"Yinj": Yinj, "Pb": 101325.0 / RDC_ND["P0"]}
         s.set_theta(theta)
@@ -248,19 +247,23 @@ def run_ours(args):
                     "bottom, pressure outlet top (Pb = 1 atm), linear reactant layer, 40x100 kernel")
     U0, aux0 = s.state_from_PTY(torch.tensor(P, device="cuda"), torch.tensor(T, device="cuda"),
                                 torch.tensor(Y, device="cuda"))
-    ncell = nx * ny
+    return s, U0, aux0, theta, nx * ny, workload
+
+
+def _time_path(args, s, U0, aux0, theta, ncell, dist, clocks=None):
+    """Device-timed steps (L2 flushed between steps), per-kernel split and the
+    end-to-end leg for one solver.  Returns a dict of measurements."""
+    import torch
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
-    # advance the state past the initial transient so the timed steps see a
-    # burning slab; then time single steps (each one kernel sequence)
     U, aux, _ = s.advance(U0, aux0, max(args.warmup, 3), cfl=CFL, theta=theta)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev)
-    clocks.start()
-    time.sleep(0.3)
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
     t_wall0 = time.time()
     for k in range(args.steps):
         flush.zero_()
@@ -269,18 +272,14 @@ def run_ours(args):
         ev[k][1].record()
     torch.cuda.synchronize()
     t_wall = time.time() - t_wall0
-    clk = clocks.stop()
-    ms_steps = [a.elapsed_time(b) for a, b in ev]
-    ms_total = sum(ms_steps)
+    clk = clocks.stop() if clocks else None
+    ms_total = sum(a.elapsed_time(b) for a, b in ev)
     status = s.status()
     if dist:
         t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_total = float(t.item())
-    ms_per_step = ms_total / args.steps
-    value = ws * ncell * args.steps / (ms_total * 1e-3)
-
-    # per-kernel split over further steps (events around each launch)
+    # per-kernel split (events around each launch)
     s.set_kernel_timing(True)
     kt_steps = min(args.steps, 5)
     acc = {"flux": [0.0, 0], "select": [0.0, 0], "chem": [0.0, 0], "other": [0.0, 0]}
@@ -292,23 +291,6 @@ def run_ours(args):
             acc[kk][1] += n
         s.set_kernel_timing(True)
     s.set_kernel_timing(False)
-    kernel_ms = {k: v[0] / kt_steps for k, v in acc.items()}
-    chem_ms = acc["chem"][0] / max(acc["chem"][1], 1)
-    L = _native.lib()
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    hbm_peak, hbm_src = 6650.0, "fallback"
-    if os.path.exists(peaks_path):
-        try:
-            hbm_peak = float(json.load(open(peaks_path))["hbm_gbs"])
-            hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
-        except Exception:
-            pass
-    fp64_peak = fp64_peak_tflops(L, torch)
-    arith, special = chem_flops_per_cell()
-    chem_gbs = BYTES_CHEM_PER_CELL * ncell / (chem_ms * 1e-3) / 1e9
-    chem_tflops = arith * ncell / (chem_ms * 1e-3) / 1e12
-    step_gbs = BYTES_STEP_PER_CELL * ncell / (ms_per_step * 1e-3) / 1e9
-
     # end to end through the public API: pinned host state in, state out
     hU = U.cpu().pin_memory()
     haux = aux.cpu().pin_memory()
@@ -339,8 +321,91 @@ def run_ours(args):
         t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_value = ws * ncell * e2e_steps / (e2e_ms * 1e-3)
-    hbytes = (hU.numel() + haux.numel()) * 8
+    ws = dist.get_world_size() if dist else 1
+    return {"value": ws * ncell * args.steps / (ms_total * 1e-3), "ms_per_step": ms_total / args.steps,
+            "status": status, "clocks": clk, "t_wall": t_wall,
+            "kernel_ms_per_step": {k: v[0] / kt_steps for k, v in acc.items()},
+            "kernel_ms_per_launch": {k: v[0] / max(v[1], 1) for k, v in acc.items()},
+            "e2e": {"value": ws * ncell * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": (hU.numel() + haux.numel()) * 8,
+                    "d2h_bytes_per_step": (hU.numel() + haux.numel()) * 8,
+                    "steps": e2e_steps, "h2d_ms": leg_ms[0], "step_ms": leg_ms[1], "d2h_ms": leg_ms[2]}}
+
+
+def _accuracy(args, s_test, s_ref, U0, aux0, theta, steps):
+    """Per-field relative L1 of the tested path against the float64 path after
+    `steps` steps from the same state, and the detonation-front offset."""
+    import torch
+    from janc_b200 import mechanism as jm
+    mech = s_ref.mech
+    Ua, auxa, _ = s_test.advance(U0, aux0, steps, cfl=CFL, theta=theta)
+    Ub, auxb, _ = s_ref.advance(U0, aux0, steps, cfl=CFL, theta=theta)
+    invM = torch.tensor(1.0 / mech.tables["species_M"], device="cuda")
+
+    def prim(U, aux):
+        rho = U[0]
+        Y8 = U[4:] / rho
+        Yf = torch.cat([Y8, (1.0 - Y8.sum(0))[None]], 0)
+        R = (invM[:, None, None] * Yf).sum(0)
+        return rho, rho * R * aux[1], aux[1], Y8
+
+    ra, pa, Ta, Ya = prim(Ua, auxa)
+    rb, pb, Tb, Yb = prim(Ub, auxb)
+
+    def l1(a, b):
+        return float((a - b).abs().sum() / b.abs().sum().clamp_min(1e-300))
+
+    errs = {"rho": l1(ra, rb), "p": l1(pa, pb), "T": l1(Ta, Tb)}
+    for k, name in enumerate(mech.species[:8]):
+        if float(Yb[k].abs().sum()) > 1e-30:
+            errs["Y_" + name] = l1(Ya[k], Yb[k])
+    pamb = float(pb.min())
+
+    def front(p):
+        mask = p > 2 * pamb
+        idx = torch.arange(p.shape[0], device="cuda")[:, None].expand_as(p)
+        return torch.where(mask, idx, torch.full_like(idx, -1)).max(0).values
+
+    dfront = int((front(pa) - front(pb)).abs().max())
+    return {"steps": steps, "l1_rel": errs, "front_max_offset_cells": dfront}
+
+
+def run_ours(args):
+    import torch
+    from janc_b200 import _native
+
+    dist, rank, ws = _dist()
+    dev = torch.cuda.current_device()
+    s, U0, aux0, theta, ncell, workload = _setup_workload(args, args.precision)
+    head = _time_path(args, s, U0, aux0, theta, ncell, dist, ClockSampler(dev))
+    other = None
+    acc = None
+    if args.precision != "fp64" and not args.no_compare:
+        sr, _, _, _, _, _ = _setup_workload(args, "fp64")
+        other = _time_path(args, sr, U0, aux0, theta, ncell, dist)
+        Uw, auxw, _ = sr.advance(U0, aux0, max(args.warmup, 3), cfl=CFL, theta=theta)
+        acc = _accuracy(args, s, sr, Uw, auxw, theta, args.accuracy_steps)
+    kms = head["kernel_ms_per_launch"]
+    chem_ms = kms["chem"]
+    flux_ms = kms["flux"]
+    L = _native.lib()
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    hbm_peak, hbm_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        try:
+            hbm_peak = float(json.load(open(peaks_path))["hbm_gbs"])
+            hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except Exception:
+            pass
+    fp64_peak = fp64_peak_tflops(L, torch)
+    arith, special = chem_flops_per_cell()
+    # dominant kernel of the headline path
+    dom = "chem" if head["kernel_ms_per_step"]["chem"] >= head["kernel_ms_per_step"]["flux"] else "flux"
+    bytes_cell = BYTES_CHEM_PER_CELL if dom == "chem" else BYTES_FLUX_STAGE_PER_CELL
+    launch_ms = chem_ms if dom == "chem" else flux_ms
+    achieved = bytes_cell * ncell / (launch_ms * 1e-3) / 1e9
+    chem_tflops = arith * ncell / (chem_ms * 1e-3) / 1e12
+    step_gbs = BYTES_STEP_PER_CELL * ncell / (head["ms_per_step"] * 1e-3) / 1e9
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "channel":
@@ -351,33 +416,39 @@ def run_ours(args):
     if rank != 0:
         return
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "precision": args.precision,
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision != "mixed" else "f32 flux / f64 state, T-solve, chemistry",
+        "data": "synthetic", "precision": args.precision,
         "config": {"workload": workload, "cells": ncell, "cfl": CFL, "precision": args.precision,
                    "l2": "flushed between timed steps (256 MB write)",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
-        "status_bits": status,
-        "kernel_ms_per_step": kernel_ms,
+        "status_bits": head["status"],
+        "kernel_ms_per_step": head["kernel_ms_per_step"],
         "gpu_launches": 11 * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "k_chem (point-implicit chemistry + final Halley)",
-                     "achieved": chem_gbs, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": chem_gbs / hbm_peak, "traffic": None,
-                     "peak_source": hbm_src,
-                     "algorithmic_bytes_per_cell": BYTES_CHEM_PER_CELL,
-                     "launch_ms": chem_ms,
+        "roofline": {"bound": "hbm", "kernel": {"chem": "k_chem (point-implicit chemistry + final Halley)",
+                                                 "flux": "k_flux2d (LF + WENO5 + RK stage + Halley)"}[dom],
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "traffic": None, "peak_source": hbm_src,
+                     "algorithmic_bytes_per_cell": bytes_cell, "launch_ms": launch_ms,
                      "step_achieved_gbs": step_gbs,
                      "step_algorithmic_bytes_per_cell": BYTES_STEP_PER_CELL},
         "compute_roofline": {"bound": "fp64", "kernel": "k_chem", "achieved": chem_tflops,
                              "peak": fp64_peak, "unit": "TFLOP/s", "frac": chem_tflops / fp64_peak,
                              "peak_source": "measured live (jb_probe_fp64_fma)",
-                             "flops_per_cell": arith, "special_ops_per_cell": special},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": hbytes, "d2h_bytes_per_step": hbytes,
-                "steps": e2e_steps, "h2d_ms": leg_ms[0], "step_ms": leg_ms[1], "d2h_ms": leg_ms[2]},
-        "clocks": clk,
-        "wall_s_timed_region": t_wall,
+                             "flops_per_cell": arith, "special_ops_per_cell": special, "launch_ms": chem_ms},
+        "e2e": head["e2e"],
+        "clocks": head["clocks"],
+        "wall_s_timed_region": head["t_wall"],
     }
+    if other is not None:
+        line["fp64"] = {"value": other["value"], "ms_per_step": other["ms_per_step"],
+                        "kernel_ms_per_step": other["kernel_ms_per_step"], "e2e": other["e2e"]["value"],
+                        "status_bits": other["status"]}
+        line["speedup_vs_fp64"] = head["value"] / other["value"]
+    if acc is not None:
+        line["accuracy_vs_fp64"] = acc
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -459,7 +530,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_strict", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "fp64_strict", "mixed"])
+    ap.add_argument("--no-compare", action="store_true", help="skip the float64 comparison run")
+    ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--workload", default="channel", choices=["channel", "rdc"])
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -91,6 +91,9 @@ void jb::derive_mech(jb_mech_params& m) {
         if ((m.tb[i][j] != 0.0) != (JB_GEN_TBNZ[i][j] != 0)) ok = 0;
     }
   }
+  m.tcr_uniform = 1;
+  for (int k = 1; k < m.ns; ++k)
+    if (m.Tcr[k] != m.Tcr[0]) m.tcr_uniform = 0;
   m.lnpref = std::log(m.pref);
   m.lnT0 = std::log(m.T0);
   m.gen_ok = ok;
@@ -113,7 +116,8 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   for (int s = 0; s < 2 * dim; ++s)
     if (!bc_ok(bc[s])) return JB_ERR_ARG;
   if (dim == 1 && (bc[0] == JB_BC_RDC_INJECTOR || bc[1] == JB_BC_RDC_INJECTOR)) return JB_ERR_UNSUPPORTED;
-  if (precision != JB_PREC_STRICT && precision != JB_PREC_FP64) return JB_ERR_UNSUPPORTED;
+  if (precision != JB_PREC_STRICT && precision != JB_PREC_FP64 && precision != JB_PREC_MIXED)
+    return JB_ERR_UNSUPPORTED;
   jb_handle* h = new (std::nothrow) jb_handle();
   if (!h) return JB_ERR_ARG;
   std::memset(h, 0, sizeof(*h));
@@ -121,7 +125,9 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   jb::derive_mech(h->mech);
   h->dim = dim;
   h->precision = precision;
-  h->ops = precision == JB_PREC_STRICT ? &jb::strict_ops : &jb::fast_ops;
+  h->ops = precision == JB_PREC_STRICT ? &jb::strict_ops
+          : precision == JB_PREC_MIXED  ? &jb::mixed_ops
+                                        : &jb::fast_ops;
   jb_grid& g = h->grid;
   g.nx = nx;
   g.ny = ny;
@@ -130,6 +136,8 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   g.ncell = (long long)nx * ny;
   g.dx = dx;
   g.dy = dim == 2 ? dy : 1.0;
+  g.idx = 1.0 / g.dx;
+  g.idy = 1.0 / g.dy;
   for (int s = 0; s < 4; ++s) g.bc[s] = s < 2 * dim ? bc[s] : JB_BC_PERIODIC;
   g.Pb = 0.0;
   g.Yinj = nullptr;
@@ -345,7 +353,11 @@ int jb_kernel_times(jb_handle* h, double* ms, long long* launches) {
 int jb_set_spacing(jb_handle* h, double dx, double dy) {
   if (!h || !(dx > 0.0) || (h->dim == 2 && !(dy > 0.0))) return set_err(h, JB_ERR_ARG, "bad spacing");
   h->grid.dx = dx;
-  if (h->dim == 2) h->grid.dy = dy;
+  h->grid.idx = 1.0 / dx;
+  if (h->dim == 2) {
+    h->grid.dy = dy;
+    h->grid.idy = 1.0 / dy;
+  }
   return JB_OK;
 }
 

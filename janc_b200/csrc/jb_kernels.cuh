@@ -195,6 +195,82 @@ __device__ __forceinline__ unsigned halley_iterates(const MP& m, double e, const
   return bits;
 }
 
+#if JB_FAST
+// Fast-variant Halley iterates.  When every species switches NASA7 ranges at
+// the same temperature (m.tcr_uniform), the mixture's cp, dcp/dT and h are
+// polynomials in T whose coefficients are the Y-weighted sums of the
+// species' coefficients; they are formed once per cell for the range the
+// iterate is in, so each iteration costs ~15 FMAs instead of ~140.  The
+// rounding differs from the reference's per-species sums at the ulp level.
+struct MixPoly {
+  double cp[5], dcp[4], h[6];
+};
+
+template <bool LO>
+__device__ __forceinline__ void mix_poly_range(const MP& m, const double* Yf, MixPoly& P) {
+  const auto& cp = LO ? m.cp_lo : m.cp_hi;
+  const auto& dcp = LO ? m.dcp_lo : m.dcp_hi;
+  const auto& h = LO ? m.h_lo : m.h_hi;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    double a = 0.0, b = 0.0, c = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      if (j < 5) a += Yf[k] * cp[k][j];
+      if (j < 4) b += Yf[k] * dcp[k][j];
+      c += Yf[k] * h[k][j];
+    }
+    if (j < 5) P.cp[j] = a;
+    if (j < 4) P.dcp[j] = b;
+    P.h[j] = c;
+  }
+}
+
+// branch (warp-uniform away from the switch isotherm) so the coefficients are
+// read straight from the parameter bank
+__device__ __forceinline__ void mix_poly(const MP& m, const double* Yf, bool lo, MixPoly& P) {
+  if (lo) mix_poly_range<true>(m, Yf, P);
+  else mix_poly_range<false>(m, Yf, P);
+}
+
+__device__ __forceinline__ unsigned halley_iterates_fast(const MP& m, double e, const double* Yf, double R,
+                                                         double T0, double* cand) {
+  unsigned bits = 0;
+  double T = T0;
+  cand[0] = T;
+  const double Tcr = m.Tcr[0];
+  bool lo = T < Tcr;
+  MixPoly P;
+  mix_poly(m, Yf, lo, P);
+#pragma unroll 1
+  for (int i = 0; i < HALLEY_MAX; ++i) {
+    const bool lo_i = T < Tcr;
+    if (lo_i != lo) {  // the iterate crossed the range boundary (rare)
+      lo = lo_i;
+      mix_poly(m, Yf, lo, P);
+    }
+    const double cp = poly5(P.cp, T), d2 = poly4(P.dcp, T), h = poly6(P.h, T);
+    const double res = (h - R * T) - e;
+    const double d1 = cp - R;
+    if (fabs(res) > HALLEY_TOL) bits |= 1u << i;
+    if (res != res) bits |= 1u << (8 + i);
+    const double dT = ((-2.0 * res) * d1) / ((2.0 * (d1 * d1)) - res * d2);
+    T = T + dT;
+    cand[i + 1] = T;
+  }
+  return bits;
+}
+#endif
+
+// Halley iterates in the variant's arithmetic (see halley_iterates).
+__device__ __forceinline__ unsigned halley_any(const MP& m, double e, const double* Yf, double R, double T0,
+                                               double* cand) {
+#if JB_FAST
+  if (m.tcr_uniform) return halley_iterates_fast(m, e, Yf, R, T0, cand);
+#endif
+  return halley_iterates(m, e, Yf, R, T0, cand);
+}
+
 // Number of Halley iterations the reference's global while-loop performs.
 __device__ __forceinline__ int halley_count(unsigned word) {
   for (int i = 0; i < HALLEY_MAX; ++i) {
@@ -537,6 +613,101 @@ __device__ __forceinline__ double lf_flux(int f, int dir, double q, double rho, 
 #endif
 }
 
+#if JB_FAST
+// ---------------------------------------------------------------------------
+// float32 flux arithmetic of the mixed-precision variant
+// ---------------------------------------------------------------------------
+// The reference's epsilon is absolute (1e-6) while SI flux magnitudes reach
+// ~1e11, so (eps + IS)^2 overflows float32.  The weights are formed as ratios
+// to the smallest (eps + IS_k), alpha_k ~ C_k (min/(eps + IS_k))^2, which is
+// the same normalised weight in real arithmetic and cannot overflow.
+__device__ __forceinline__ float weno_combine32(float IS1, float IS2, float IS3, float q1, float q2,
+                                                float q3, float eps) {
+  const float e1 = eps + IS1, e2 = eps + IS2, e3 = eps + IS3;
+  const float mn = fminf(e1, fminf(e2, e3));
+  const float r1 = __fdividef(mn, e1), r2 = __fdividef(mn, e2), r3 = __fdividef(mn, e3);
+  const float a1 = 0.1f * (r1 * r1), a2 = 0.6f * (r2 * r2), a3 = 0.3f * (r3 * r3);
+  return __fdividef(a1 * q1 + a2 * q2 + a3 * q3, a1 + a2 + a3);
+}
+
+// Left/right-biased float32 values.  The ratio form of the weights never
+// squares (eps + IS), so only IS itself must stay in range: |f| below ~1e18
+// (SI fluxes stay below ~1e12).  Tiny fields give IS << eps and the linear
+// weights, as the reference's absolute eps does.
+__device__ __forceinline__ float weno_L(float fjm2, float fjm1, float fj, float fjp1, float fjp2) {
+  const float t1 = fjm2 - 4.f * fjm1 + 3.f * fj, s1 = fjm2 - 2.f * fjm1 + fj;
+  const float t2 = fjm1 - fjp1, s2 = fjm1 - 2.f * fj + fjp1;
+  const float t3 = 3.f * fj - 4.f * fjp1 + fjp2, s3 = fj - 2.f * fjp1 + fjp2;
+  const float IS1 = 0.25f * (t1 * t1) + (13.f / 12.f) * (s1 * s1);
+  const float IS2 = 0.25f * (t2 * t2) + (13.f / 12.f) * (s2 * s2);
+  const float IS3 = 0.25f * (t3 * t3) + (13.f / 12.f) * (s3 * s3);
+  const float q1 = (1.f / 3.f) * fjm2 - (7.f / 6.f) * fjm1 + (11.f / 6.f) * fj;
+  const float q2 = (-1.f / 6.f) * fjm1 + (5.f / 6.f) * fj + (1.f / 3.f) * fjp1;
+  const float q3 = (1.f / 3.f) * fj + (5.f / 6.f) * fjp1 - (1.f / 6.f) * fjp2;
+  return weno_combine32(IS1, IS2, IS3, q1, q2, q3, 1e-6f);
+}
+
+__device__ __forceinline__ float weno_R(float fjm2, float fjm1, float fj, float fjp1, float fjp2) {
+  const float t1 = fjp2 - 4.f * fjp1 + 3.f * fj, s1 = fjp2 - 2.f * fjp1 + fj;
+  const float t2 = fjp1 - fjm1, s2 = fjp1 - 2.f * fj + fjm1;
+  const float t3 = 3.f * fj - 4.f * fjm1 + fjm2, s3 = fj - 2.f * fjm1 + fjm2;
+  const float IS1 = 0.25f * (t1 * t1) + (13.f / 12.f) * (s1 * s1);
+  const float IS2 = 0.25f * (t2 * t2) + (13.f / 12.f) * (s2 * s2);
+  const float IS3 = 0.25f * (t3 * t3) + (13.f / 12.f) * (s3 * s3);
+  const float q1 = (1.f / 3.f) * fjp2 - (7.f / 6.f) * fjp1 + (11.f / 6.f) * fj;
+  const float q2 = (-1.f / 6.f) * fjp1 + (5.f / 6.f) * fj + (1.f / 3.f) * fjm1;
+  const float q3 = (1.f / 3.f) * fj + (5.f / 6.f) * fjm1 - (1.f / 6.f) * fjm2;
+  return weno_combine32(IS1, IS2, IS3, q1, q2, q3, 1e-6f);
+}
+
+template <int DIM>
+__device__ __forceinline__ float lf_flux(int f, int dir, float q, float rho, float u, float v, float p,
+                                         float E) {
+  const float vn = dir == 0 ? u : v;
+  if (f == 0) return rho * vn;
+  if (DIM == 1) {
+    if (f == 1) return rho * (u * u) + p;
+    if (f == 2) return u * (E + p);
+  } else {
+    if (f == 1) return dir == 0 ? rho * (u * u) + p : rho * u * v;
+    if (f == 2) return dir == 0 ? rho * u * v : rho * (v * v) + p;
+    if (f == 3) return vn * (E + p);
+  }
+  return vn * q;
+}
+#endif
+
+// rho, u, v, p of one cell for the flux (U_to_prim; the flux needs no gamma)
+template <int DIM>
+__device__ __forceinline__ void flux_prims(const MP& m, const double* q, double T, double& rho,
+                                           double& u, double& v, double& p) {
+  Prim<DIM> pr = u_to_prim<DIM>(m, q, 1.0, T);
+  rho = pr.rho;
+  u = pr.u;
+  v = pr.v;
+  p = pr.p;
+}
+
+#if JB_FAST
+template <int DIM>
+__device__ __forceinline__ void flux_prims(const MP& m, const float* q, float T, float& rho, float& u,
+                                           float& v, float& p) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  rho = q[0];
+  const float ri = __fdividef(1.f, rho);
+  u = q[1] * ri;
+  v = DIM == 2 ? q[2] * ri : 0.f;
+  float sr = q[nY], pr = (float)m.invM[0] * q[nY];
+#pragma unroll
+  for (int k = 1; k < NR; ++k) {
+    sr += q[nY + k];
+    pr += (float)m.invM[k] * q[nY + k];
+  }
+  pr += (float)m.invM[NR] * (rho - sr);
+  p = pr * T;
+}
+#endif
+
 // ---------------------------------------------------------------------------
 // stage kernels
 // ---------------------------------------------------------------------------
@@ -551,34 +722,39 @@ constexpr int SM2_Q = PX2 * PY2;                  // per field
 constexpr int SM2_HX = PX2 * TY2, SM2_HY = TX2 * PY2;
 constexpr int SM2_FX = (TX2 + 1) * TY2, SM2_FY = TX2 * (TY2 + 1);
 
+template <class R>
 __host__ __device__ constexpr size_t smem2d_bytes(int nq) {
-  return sizeof(double) * ((size_t)nq * SM2_Q + 4 * SM2_Q + 2 * SM2_HX + 2 * SM2_HY + SM2_FX + SM2_FY);
+  return sizeof(R) * ((size_t)nq * SM2_Q + 4 * SM2_Q + 2 * SM2_HX + 2 * SM2_HY + SM2_FX + SM2_FY);
 }
 
-template <int STAGE>
-__global__ void __launch_bounds__(NT2) k_flux2d(MP m, Grid g, const double* __restrict__ Uk,
+// R is the arithmetic type of the flux (LF split, WENO, primitives): double
+// for the float64 variants, float for the mixed variant.  The RK combination
+// and the Halley iterates are float64 in every variant.
+template <int STAGE, class R>
+__global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk,
                                                  const double* __restrict__ Un,
                                                  double* __restrict__ out, double* __restrict__ cand,
                                                  const double* __restrict__ strips, Slots* slots,
                                                  int aidx, int midx, double dt_arg) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int nv = 12, nq = nv + 1;
-  double* sQ = sm;                       // [nq][PX2][PY2]
-  double* sP = sQ + (size_t)nq * SM2_Q;   // [4][PX2][PY2]: rho, u, v, p
-  double* sHxp = sP + 4 * SM2_Q;          // [PX2][TY2]
-  double* sHxm = sHxp + SM2_HX;
-  double* sHyp = sHxm + SM2_HX;           // [TX2][PY2]
-  double* sHym = sHyp + SM2_HY;
-  double* sFx = sHym + SM2_HY;            // [TX2+1][TY2]
-  double* sFy = sFx + SM2_FX;             // [TX2][TY2+1]
+  constexpr bool EXACT = sizeof(R) == sizeof(double);
+  R* sQ = reinterpret_cast<R*>(smraw);   // [nq][PX2][PY2]
+  R* sP = sQ + (size_t)nq * SM2_Q;       // [4][PX2][PY2]: rho, u, v, p
+  R* sHxp = sP + 4 * SM2_Q;              // [PX2][TY2]
+  R* sHxm = sHxp + SM2_HX;
+  R* sHyp = sHxm + SM2_HX;               // [TX2][PY2]
+  R* sHym = sHyp + SM2_HY;
+  R* sFx = sHym + SM2_HY;                // [TX2+1][TY2]
+  R* sFy = sFx + SM2_FX;                 // [TX2][TY2+1]
 
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * TX2, y0 = blockIdx.y * TY2;
   const long long nc = g.ncell;
   const double dt = STAGE == 0 ? dt_arg : slots->dt;
-  const double ax = bitsd(slots->ax[aidx]);
-  const double ay = bitsd(slots->ay[aidx]);
+  const R ax = (R)bitsd(slots->ax[aidx]);
+  const R ay = (R)bitsd(slots->ay[aidx]);
 
   // ---- load the padded tile with ghost cells
   for (int i = tid; i < SM2_Q; i += NT2) {
@@ -589,27 +765,28 @@ __global__ void __launch_bounds__(NT2) k_flux2d(MP m, Grid g, const double* __re
       size_t c = (size_t)s.xs * g.ny + s.ys;
       for (int q = 0; q < nv; ++q) {
         double v = Uk[q * nc + c];
-        sQ[q * SM2_Q + i] = ((s.flip >> q) & 1) ? -v : v;
+        sQ[q * SM2_Q + i] = (R)(((s.flip >> q) & 1) ? -v : v);
       }
-      sQ[nv * SM2_Q + i] = auxk[nc + c];
+      sQ[nv * SM2_Q + i] = (R)auxk[nc + c];
     } else if (s.kind == 1) {
-      for (int q = 0; q < nv; ++q) sQ[q * SM2_Q + i] = strips[strip_idx(g, s.side, q, s.pos)];
-      sQ[nv * SM2_Q + i] = strips[strip_idx(g, s.side, nv + 1, s.pos)];
+      for (int q = 0; q < nv; ++q) sQ[q * SM2_Q + i] = (R)strips[strip_idx(g, s.side, q, s.pos)];
+      sQ[nv * SM2_Q + i] = (R)strips[strip_idx(g, s.side, nv + 1, s.pos)];
     } else {
-      for (int q = 0; q < nq; ++q) sQ[q * SM2_Q + i] = 1.0;
+      for (int q = 0; q < nq; ++q) sQ[q * SM2_Q + i] = (R)1.0;
     }
   }
   __syncthreads();
   // ---- primitives (aux_func.U_to_prim) on every padded cell
   for (int i = tid; i < SM2_Q; i += NT2) {
-    double q[16];
+    R q[nv];
+#pragma unroll
     for (int f = 0; f < nv; ++f) q[f] = sQ[f * SM2_Q + i];
-    double T = sQ[nv * SM2_Q + i];
-    Prim<2> pr = u_to_prim<2>(m, q, 1.0, T);
-    sP[i] = pr.rho;
-    sP[SM2_Q + i] = pr.u;
-    sP[2 * SM2_Q + i] = pr.v;
-    sP[3 * SM2_Q + i] = pr.p;
+    R rho, u, v, p;
+    flux_prims<2>(m, q, sQ[nv * SM2_Q + i], rho, u, v, p);
+    sP[i] = rho;
+    sP[SM2_Q + i] = u;
+    sP[2 * SM2_Q + i] = v;
+    sP[3 * SM2_Q + i] = p;
   }
   __syncthreads();
 
@@ -619,49 +796,89 @@ __global__ void __launch_bounds__(NT2) k_flux2d(MP m, Grid g, const double* __re
   const bool live = owner && gx < g.nx && gy < g.ny;
   const size_t cell = (size_t)gx * g.ny + gy;
 
+#if JB_FAST
+  // H-phase work items of this thread (<= 3 of the 666), fixed for all fields
+  constexpr int NH2 = (SM2_HX + SM2_HY + NT2 - 1) / NT2;
+  int h_src[NH2], h_dst[NH2];
+#pragma unroll
+  for (int r = 0; r < NH2; ++r) {
+    const int i = tid + r * NT2;
+    int px = 0, py = 0, dst = -1;
+    if (i < SM2_HX) { px = i / TY2; py = i % TY2 + 3; dst = i; }
+    else if (i < SM2_HX + SM2_HY) { int j = i - SM2_HX; px = j / PY2 + 3; py = j % PY2; dst = i; }
+    h_src[r] = px * PY2 + py;
+    h_dst[r] = dst;
+  }
+#endif
   for (int f = 0; f < nv; ++f) {
     // ---- split fluxes H+/- = 0.5 (F +/- alpha U)
+#if JB_FAST
+    // F = vel q + pressure terms (x: p in rho u, u p in rho E; y: p in rho v,
+    // v p in rho E), the reference's LF flux regrouped
+#pragma unroll
+    for (int r = 0; r < NH2; ++r) {
+      const int dst = h_dst[r];
+      if (dst < 0) continue;
+      const int c = h_src[r];
+      const bool xdir = dst < SM2_HX;
+      const R vel = xdir ? sP[SM2_Q + c] : sP[2 * SM2_Q + c];
+      const R qf = sQ[f * SM2_Q + c];
+      R F = vel * qf;
+      if (f == (xdir ? 1 : 2)) F += sP[3 * SM2_Q + c];
+      if (f == 3) F += vel * sP[3 * SM2_Q + c];
+      const R al = xdir ? ax : ay;
+      const R hp = (R)0.5 * (F + al * qf), hm = (R)0.5 * (F - al * qf);
+      if (xdir) { sHxp[dst] = hp; sHxm[dst] = hm; }
+      else { sHyp[dst - SM2_HX] = hp; sHym[dst - SM2_HX] = hm; }
+    }
+#else
     for (int i = tid; i < SM2_HX + SM2_HY; i += NT2) {
       int px, py, dir;
       if (i < SM2_HX) { px = i / TY2; py = i % TY2 + 3; dir = 0; }
       else { int j = i - SM2_HX; px = j / PY2 + 3; py = j % PY2; dir = 1; }
       int c = px * PY2 + py;
-      double rho = sP[c], u = sP[SM2_Q + c], v = sP[2 * SM2_Q + c], p = sP[3 * SM2_Q + c];
-      double E = sQ[3 * SM2_Q + c];
-      double qf = sQ[f * SM2_Q + c];
-      double F = lf_flux<2>(f, dir, qf, rho, u, v, p, E);
-      double al = dir == 0 ? ax : ay;
-      double hp = 0.5 * (F + al * qf), hm = 0.5 * (F - al * qf);
+      R rho = sP[c], u = sP[SM2_Q + c], v = sP[2 * SM2_Q + c], p = sP[3 * SM2_Q + c];
+      R E = sQ[3 * SM2_Q + c];
+      R qf = sQ[f * SM2_Q + c];
+      R F = lf_flux<2>(f, dir, qf, rho, u, v, p, E);
+      R al = dir == 0 ? ax : ay;
+      R hp = (R)0.5 * (F + al * qf), hm = (R)0.5 * (F - al * qf);
       if (dir == 0) { sHxp[px * TY2 + (py - 3)] = hp; sHxm[px * TY2 + (py - 3)] = hm; }
       else { sHyp[(px - 3) * PY2 + py] = hp; sHym[(px - 3) * PY2 + py] = hm; }
     }
+#endif
     __syncthreads();
     // ---- face values: F = L(H+) + R(H-)
     {
       int mxf = tid / TY2, jy = tid % TY2;  // x-faces: 16 x 16 = 256
-      const double* hp = sHxp + jy;
-      const double* hm = sHxm + jy;
-      double L = weno_L(hp[(mxf) * TY2], hp[(mxf + 1) * TY2], hp[(mxf + 2) * TY2], hp[(mxf + 3) * TY2],
+      const R* hp = sHxp + jy;
+      const R* hm = sHxm + jy;
+      R L = weno_L(hp[(mxf) * TY2], hp[(mxf + 1) * TY2], hp[(mxf + 2) * TY2], hp[(mxf + 3) * TY2],
                         hp[(mxf + 4) * TY2]);
-      double R = weno_R(hm[(mxf + 1) * TY2], hm[(mxf + 2) * TY2], hm[(mxf + 3) * TY2], hm[(mxf + 4) * TY2],
-                        hm[(mxf + 5) * TY2]);
-      sFx[mxf * TY2 + jy] = L + R;
+      R Rr = weno_R(hm[(mxf + 1) * TY2], hm[(mxf + 2) * TY2], hm[(mxf + 3) * TY2], hm[(mxf + 4) * TY2],
+                    hm[(mxf + 5) * TY2]);
+      sFx[mxf * TY2 + jy] = L + Rr;
       if (tid < SM2_FY) {
         int jx = tid / (TY2 + 1), myf = tid % (TY2 + 1);
-        const double* gp = sHyp + jx * PY2 + myf;
-        const double* gm = sHym + jx * PY2 + myf;
-        double Lg = weno_L(gp[0], gp[1], gp[2], gp[3], gp[4]);
-        double Rg = weno_R(gm[1], gm[2], gm[3], gm[4], gm[5]);
+        const R* gp = sHyp + jx * PY2 + myf;
+        const R* gm = sHym + jx * PY2 + myf;
+        R Lg = weno_L(gp[0], gp[1], gp[2], gp[3], gp[4]);
+        R Rg = weno_R(gm[1], gm[2], gm[3], gm[4], gm[5]);
         sFy[jx * (TY2 + 1) + myf] = Lg + Rg;
       }
     }
     __syncthreads();
     // ---- divergence and the RK combination
     if (live) {
-      double dF = sFx[(ix + 1) * TY2 + iy] - sFx[ix * TY2 + iy];
-      double dG = sFy[ix * (TY2 + 1) + iy + 1] - sFy[ix * (TY2 + 1) + iy];
+      double dF = (double)(sFx[(ix + 1) * TY2 + iy] - sFx[ix * TY2 + iy]);
+      double dG = (double)(sFy[ix * (TY2 + 1) + iy + 1] - sFy[ix * (TY2 + 1) + iy]);
+#if JB_FAST
+      double rhs = dt * (-(dF * g.idx + dG * g.idy));
+#else
       double rhs = dt * (-(dF / g.dx + dG / g.dy));
-      double uk = sQ[f * SM2_Q + (ix + 3) * PY2 + (iy + 3)];
+#endif
+      // the state itself is float64 in every variant
+      double uk = EXACT ? (double)sQ[f * SM2_Q + (ix + 3) * PY2 + (iy + 3)] : Uk[f * nc + cell];
       double r;
       if (STAGE == 0) r = rhs;
       else if (STAGE == 1) r = uk + rhs;
@@ -685,10 +902,10 @@ __global__ void __launch_bounds__(NT2) k_flux2d(MP m, Grid g, const double* __re
 #pragma unroll
     for (int k = 0; k < NR; ++k) Y8[k] = q[4 + k] / rho;
     fill_Y(Y8, Yf);
-    double R = get_R(m, Yf);
-    double T0 = sQ[nv * SM2_Q + (ix + 3) * PY2 + (iy + 3)];
+    double Rmix = get_R(m, Yf);
+    double T0 = EXACT ? (double)sQ[nv * SM2_Q + (ix + 3) * PY2 + (iy + 3)] : auxk[nc + cell];
     double cnd[JB_NCAND];
-    bits = halley_iterates(m, e, Yf, R, T0, cnd);
+    bits = halley_any(m, e, Yf, Rmix, T0, cnd);
 #pragma unroll
     for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
   }
@@ -698,29 +915,31 @@ __global__ void __launch_bounds__(NT2) k_flux2d(MP m, Grid g, const double* __re
 // 1D: tiles of 255 cells so the 256 faces map one-to-one onto threads.
 constexpr int TX1 = 255, PX1 = TX1 + 6, NT1 = 256;
 
+template <class R>
 __host__ __device__ constexpr size_t smem1d_bytes(int nq) {
-  return sizeof(double) * ((size_t)nq * PX1 + 3 * PX1 + 2 * PX1 + (TX1 + 1));
+  return sizeof(R) * ((size_t)nq * PX1 + 3 * PX1 + 2 * PX1 + (TX1 + 1));
 }
 
-template <int STAGE>
+template <int STAGE, class R>
 __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk,
                                                  const double* __restrict__ Un,
                                                  double* __restrict__ out, double* __restrict__ cand,
                                                  const double* __restrict__ strips, Slots* slots,
                                                  int aidx, int midx, double dt_arg) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int nv = 11, nq = nv + 1;
-  double* sQ = sm;                      // [nq][PX1]
-  double* sP = sQ + (size_t)nq * PX1;    // [3][PX1]: rho, u, p
-  double* sHp = sP + 3 * PX1;
-  double* sHm = sHp + PX1;
-  double* sF = sHm + PX1;                // [TX1+1]
+  constexpr bool EXACT = sizeof(R) == sizeof(double);
+  R* sQ = reinterpret_cast<R*>(smraw);  // [nq][PX1]
+  R* sP = sQ + (size_t)nq * PX1;        // [3][PX1]: rho, u, p
+  R* sHp = sP + 3 * PX1;
+  R* sHm = sHp + PX1;
+  R* sF = sHm + PX1;                    // [TX1+1]
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * TX1;
   const long long nc = g.ncell;
   const double dt = STAGE == 0 ? dt_arg : slots->dt;
-  const double ax = bitsd(slots->ax[aidx]);
+  const R ax = (R)bitsd(slots->ax[aidx]);
 
   for (int i = tid; i < PX1; i += NT1) {
     int x = x0 + i - 3;
@@ -728,48 +947,62 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
     if (s.kind == 0) {
       for (int q = 0; q < nv; ++q) {
         double v = Uk[q * nc + s.xs];
-        sQ[q * PX1 + i] = ((s.flip >> q) & 1) ? -v : v;
+        sQ[q * PX1 + i] = (R)(((s.flip >> q) & 1) ? -v : v);
       }
-      sQ[nv * PX1 + i] = auxk[nc + s.xs];
+      sQ[nv * PX1 + i] = (R)auxk[nc + s.xs];
     } else if (s.kind == 1) {
-      for (int q = 0; q < nv; ++q) sQ[q * PX1 + i] = strips[strip_idx(g, s.side, q, 0)];
-      sQ[nv * PX1 + i] = strips[strip_idx(g, s.side, nv + 1, 0)];
+      for (int q = 0; q < nv; ++q) sQ[q * PX1 + i] = (R)strips[strip_idx(g, s.side, q, 0)];
+      sQ[nv * PX1 + i] = (R)strips[strip_idx(g, s.side, nv + 1, 0)];
     } else {
-      for (int q = 0; q < nq; ++q) sQ[q * PX1 + i] = 1.0;
+      for (int q = 0; q < nq; ++q) sQ[q * PX1 + i] = (R)1.0;
     }
   }
   __syncthreads();
   for (int i = tid; i < PX1; i += NT1) {
-    double q[16];
+    R q[nv];
+#pragma unroll
     for (int f = 0; f < nv; ++f) q[f] = sQ[f * PX1 + i];
-    Prim<1> pr = u_to_prim<1>(m, q, 1.0, sQ[nv * PX1 + i]);
-    sP[i] = pr.rho;
-    sP[PX1 + i] = pr.u;
-    sP[2 * PX1 + i] = pr.p;
+    R rho, u, v, p;
+    flux_prims<1>(m, q, sQ[nv * PX1 + i], rho, u, v, p);
+    sP[i] = rho;
+    sP[PX1 + i] = u;
+    sP[2 * PX1 + i] = p;
   }
   __syncthreads();
   const bool live = tid < TX1 && x0 + tid < g.nx;
   const size_t cell = (size_t)(x0 + tid);
   for (int f = 0; f < nv; ++f) {
     for (int i = tid; i < PX1; i += NT1) {
-      double rho = sP[i], u = sP[PX1 + i], p = sP[2 * PX1 + i];
-      double qf = sQ[f * PX1 + i];
-      double F = lf_flux<1>(f, 0, qf, rho, u, 0.0, p, sQ[2 * PX1 + i]);
-      sHp[i] = 0.5 * (F + ax * qf);
-      sHm[i] = 0.5 * (F - ax * qf);
+#if JB_FAST
+      // F = u q + p (rho u) + u p (rho E): the reference's LF flux regrouped
+      const R u = sP[PX1 + i], qf = sQ[f * PX1 + i];
+      R F = u * qf;
+      if (f == 1) F += sP[2 * PX1 + i];
+      if (f == 2) F += u * sP[2 * PX1 + i];
+#else
+      R rho = sP[i], u = sP[PX1 + i], p = sP[2 * PX1 + i];
+      R qf = sQ[f * PX1 + i];
+      R F = lf_flux<1>(f, 0, qf, rho, u, (R)0, p, sQ[2 * PX1 + i]);
+#endif
+      sHp[i] = (R)0.5 * (F + ax * qf);
+      sHm[i] = (R)0.5 * (F - ax * qf);
     }
     __syncthreads();
     {
       int mf = tid;  // 256 faces
-      double L = weno_L(sHp[mf], sHp[mf + 1], sHp[mf + 2], sHp[mf + 3], sHp[mf + 4]);
-      double R = weno_R(sHm[mf + 1], sHm[mf + 2], sHm[mf + 3], sHm[mf + 4], sHm[mf + 5]);
-      sF[mf] = L + R;
+      R L = weno_L(sHp[mf], sHp[mf + 1], sHp[mf + 2], sHp[mf + 3], sHp[mf + 4]);
+      R Rr = weno_R(sHm[mf + 1], sHm[mf + 2], sHm[mf + 3], sHm[mf + 4], sHm[mf + 5]);
+      sF[mf] = L + Rr;
     }
     __syncthreads();
     if (live) {
-      double dF = sF[tid + 1] - sF[tid];
+      double dF = (double)(sF[tid + 1] - sF[tid]);
+#if JB_FAST
+      double rhs = dt * (-(dF * g.idx));
+#else
       double rhs = dt * (-(dF / g.dx));
-      double uk = sQ[f * PX1 + tid + 3];
+#endif
+      double uk = EXACT ? (double)sQ[f * PX1 + tid + 3] : Uk[f * nc + cell];
       double r;
       if (STAGE == 0) r = rhs;
       else if (STAGE == 1) r = uk + rhs;
@@ -791,9 +1024,9 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
 #pragma unroll
     for (int k = 0; k < NR; ++k) Y8[k] = q[3 + k] / rho;
     fill_Y(Y8, Yf);
-    double R = get_R(m, Yf);
+    double Rmix = get_R(m, Yf);
     double cnd[JB_NCAND];
-    bits = halley_iterates(m, e, Yf, R, sQ[nv * PX1 + tid + 3], cnd);
+    bits = halley_any(m, e, Yf, Rmix, EXACT ? (double)sQ[nv * PX1 + tid + 3] : auxk[nc + cell], cnd);
 #pragma unroll
     for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
   }
@@ -821,7 +1054,7 @@ __global__ void k_halley(MP m, Grid g, const double* __restrict__ U, const doubl
     fill_Y(Y8, Yf);
     double R = get_R(m, Yf);
     double cnd[JB_NCAND];
-    bits = halley_iterates(m, e, Yf, R, aux[nc + c], cnd);
+    bits = halley_any(m, e, Yf, R, aux[nc + c], cnd);
 #pragma unroll
     for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + c] = cnd[i];
   }
@@ -1163,7 +1396,7 @@ __global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __r
       fill_Y(Yn, Yf);
       double R = get_R(m, Yf);
       double cnd[JB_NCAND];
-      bits = halley_iterates(m, e, Yf, R, T, cnd);
+      bits = halley_any(m, e, Yf, R, T, cnd);
 #pragma unroll
       for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + c] = cnd[i];
     }

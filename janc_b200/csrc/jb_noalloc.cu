@@ -76,6 +76,8 @@ extern "C" int jb_update_aux_noalloc(const jb_mech_params* mech, int dim, int nx
   g.ncell = ncell;
   g.dx = 1.0;
   g.dy = 1.0;
+  g.idx = 1.0;
+  g.idy = 1.0;
   g.inj_block_p = 1.0;
   g.lstrip = nx > ny ? nx : ny;
   jb_slots* slots = reinterpret_cast<jb_slots*>(base);

@@ -35,6 +35,7 @@ struct Ops {
 
 extern const Ops strict_ops;
 extern const Ops fast_ops;
+extern const Ops mixed_ops;
 
 // Fill the derived fields of a mechanism block (ln A, tb/M, ln pref, ln T0)
 // and flag whether its structure matches the generated chemistry.

@@ -36,7 +36,7 @@ typedef struct jb_mech_params {
   double tbinvM[JB_NREAC_MAX][JB_NR_MAX];  // tb[i][n] / M[n]
   double lnpref, lnT0;
   int gen_ok;       // structure matches the generated specialised chemistry
-  int pad2_;
+  int tcr_uniform;  // every species switches NASA7 ranges at the same temperature
 } jb_mech_params;
 
 enum jb_bc_kind {
@@ -77,6 +77,7 @@ typedef struct jb_grid {
   int nv, nY;            // number of conserved fields, index of first species
   long long ncell;
   double dx, dy;
+  double idx, idy;       // 1/dx, 1/dy
   int bc[4];             // left, right, bottom, top (jb_bc_kind)
   double Pb;             // pressure_outlet back pressure (theta['Pb'])
   const double* Yinj;    // injector mass fractions [nr][nx] (theta['Yinj'])

@@ -239,7 +239,7 @@ class MechParams(ctypes.Structure):
         # derived by jb_create
         ("lnA", ctypes.c_double * NREAC_MAX), ("tbinvM", (ctypes.c_double * NR_MAX) * NREAC_MAX),
         ("lnpref", ctypes.c_double), ("lnT0", ctypes.c_double),
-        ("gen_ok", ctypes.c_int), ("pad2_", ctypes.c_int),
+        ("gen_ok", ctypes.c_int), ("tcr_uniform", ctypes.c_int),
     ]
 
 

@@ -312,3 +312,79 @@ def test_periodic_mass_conservation(prec, omech):
     assert abs(m1 - m0) / m0 < 1e-12
     np.testing.assert_array_equal(U[:, 0, :], U[:, -1, :])
     np.testing.assert_array_equal(U[:, :, 0], U[:, :, -1])
+
+
+# --------------------------------------------------------------------------
+# mixed precision: float32 flux arithmetic, float64 state / T-solve / chemistry
+# bar (north star): density relative L1 <= 1e-4, front position within 1 cell
+# --------------------------------------------------------------------------
+def _front(U, aux, omech, two_d):
+    nY = 4 if two_d else 3
+    Y = U[nY:] / U[0]
+    p = U[0] * jo.get_R(omech, Y)[0] * aux[1]
+    if two_d:
+        return np.array([np.max(np.where(p[:, j] > 2 * 101325.0)[0], initial=-1) for j in range(p.shape[1])])
+    return np.max(np.where(p > 2 * 101325.0)[0], initial=-1)
+
+
+def _per_field(U, Uref, aux, auxref, omech, two_d):
+    nY = 4 if two_d else 3
+    out = {"rho": rel_l1(U[0], Uref[0]), "T": rel_l1(aux[1], auxref[1])}
+    p = U[0] * jo.get_R(omech, U[nY:] / U[0])[0] * aux[1]
+    pr = Uref[0] * jo.get_R(omech, Uref[nY:] / Uref[0])[0] * auxref[1]
+    out["p"] = rel_l1(p, pr)
+    for k in range(8):
+        if np.sum(np.abs(Uref[nY + k])) > 1e-30:
+            out[f"Y{k}"] = rel_l1(U[nY + k] / U[0], Uref[nY + k] / Uref[0])
+    return out
+
+
+def test_mixed_1d_config0_vs_oracle(omech):
+    nx = 2000
+    U0, aux0 = _c0_state(omech, nx, 40)
+    o = jo.Solver(omech, "1D", 0.1 / nx, None, BC1, 0.1)
+    U, aux, t = U0, aux0, 0.0
+    for _ in range(100):
+        U, aux, t, _dt = o.advance_func(U, aux, t)
+    s = Solver(1, nx, dx=0.1 / nx, boundary_config=BC1, precision="mixed")
+    Ug, auxg, _ = _run_cfl(s, U0, aux0, 100, cfl=0.1)
+    errs = _per_field(Ug, U, auxg, aux, omech, False)
+    assert errs["rho"] <= 1e-4, errs
+    assert errs["p"] <= 1e-4 and errs["T"] <= 1e-4, errs
+    assert abs(int(_front(Ug, auxg, omech, False)) - int(_front(U, aux, omech, False))) <= 1
+    assert s.status() == 0
+
+
+def test_mixed_2d_vs_oracle(omech):
+    nx, ny = 37, 23
+    rng = np.random.default_rng(7)
+    P = np.full((1, nx, ny), 101325.0)
+    T = np.full((1, nx, ny), 300.0)
+    Y = np.tile(jo.stoich_Y(omech, 1.0)[:, None, None], (1, nx, ny))
+    P[:, :4] = 30 * 101325.0
+    T[:, :4] = 3000.0 * (1 + 0.05 * rng.uniform(-1, 1, (1, 4, ny)))
+    U0, aux0 = jo.state_from_PTY(omech, P, T, Y)
+    dx = dy = 1.953125e-4
+    o = jo.Solver(omech, "2D", dx, dy, BC2, 0.1)
+    U, aux, t = U0, aux0, 0.0
+    for _ in range(10):
+        U, aux, t, _dt = o.advance_func(U, aux, t)
+    s = Solver(2, nx, ny, dx, dy, BC2, precision="mixed")
+    Ug, auxg, _ = _run_cfl(s, U0, aux0, 10, cfl=0.1)
+    errs = _per_field(Ug, U, auxg, aux, omech, True)
+    assert errs["rho"] <= 1e-4 and errs["p"] <= 1e-4, errs
+    assert np.max(np.abs(_front(Ug, auxg, omech, True) - _front(U, aux, omech, True))) <= 1
+
+
+def test_mixed_rdc_flux_close_to_fp64(golden_dir):
+    """The float32 flux against the reference's float64 flux_func on the RDC
+    state (nondimensional, injector + outlet): relative L1 per field."""
+    g = G(golden_dir, "step2d_rdc")
+    nx, ny = g["U0"].shape[1:]
+    dx, dy = float(g["dx"]), float(g["dy"])
+    s = Solver(2, nx, ny, dx, dy, BC_RDC, nondim_config=RDC_ND, precision="mixed")
+    theta = {"Yinj": g["Yinj"], "Pb": float(g["Pb"])}
+    r = host(s.flux_func(cuda(g["U0"]), cuda(g["aux0"]), dx, dy, 1e-3, theta))
+    assert field_err(r, g["rhs0"]) < 1e-5
+    U, aux, _ = _run_cfl(s, g["U0"], g["aux0"], 3, theta)
+    assert rel_l1(U[0], g["U_3"][0]) < 1e-6
