@@ -8,10 +8,13 @@ H2:O2:N2 = 2:1:3.76 at 1 atm / 300 K, at rest; an ignition slab over x-columns
 temperature blobs of +-5 % (radius 2-6 cells, numpy default_rng(1)); slip
 walls on all four sides; WENO5-JS + global Lax-Friedrichs splitting, SSP-RK3,
 point-implicit chemistry of the 9-species / 19-reaction mechanism; CFL time
-steps.  CFL is 0.1: at the stated CFL 0.5 the reference's own algorithm goes
-non-finite within ~17 steps (first-order point-implicit chemistry burns a
-slab-edge cell in one step; tests/golden/config0_cfl05.npz records it), and
-the work per step does not depend on the CFL number.
+steps.  CFL is 0.05 for the channel and 0.1 for the rotating-detonation
+workload: at larger CFL numbers the reference's own algorithm goes
+non-finite (first-order point-implicit chemistry burns a slab-edge cell in
+one step; tests/golden/config0_cfl05.npz records it for config 0 at CFL 0.5,
+and the channel at CFL 0.1 fails between steps 20 and 50 in the float64 path
+too), while at 0.05 it runs the full 2000 steps.  The work per step does not
+depend on the CFL number.
 
 Arms:
   default            our CUDA path, mixed precision (float32 flux arithmetic;
@@ -43,7 +46,8 @@ sys.path.insert(0, ROOT)
 NX, NY = 1024, 256
 LX, LY = 0.2, 0.05
 SLAB = 21
-CFL = 0.1
+CFL_BY_WORKLOAD = {"channel": 0.05, "rdc": 0.1}
+CFL = CFL_BY_WORKLOAD["channel"]
 METRIC = "reacting cell-updates/s"
 UNIT = "cell-updates/s"
 BYTES_CHEM_PER_CELL = 224      # read U,aux (112 B) + write U,aux (112 B), float64
@@ -167,6 +171,23 @@ def _dist():
     return dist, dist.get_rank(), ws
 
 
+def max_over_ranks(dist, x, device="cuda"):
+    """Largest value of x over all ranks (a device-timed duration); x itself
+    when not distributed.  Every rank must call it."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world_size, cells_per_rank, steps, ms_max):
+    """Whole-job throughput: all ranks' cell-updates over the slowest rank's
+    device time (each rank advances its own replica)."""
+    return world_size * cells_per_rank * steps / (ms_max * 1e-3)
+
+
 def fp64_peak_tflops(L, torch):
     """Measured FP64 FMA throughput of this device (TFLOP/s)."""
     import ctypes
@@ -221,6 +242,8 @@ def chem_flops_per_cell():
 
 
 def _setup_workload(args, precision):
+    global CFL
+    CFL = CFL_BY_WORKLOAD[args.workload]
     import torch
     from janc_b200.solver import Solver
     theta = None
@@ -273,12 +296,8 @@ def _time_path(args, s, U0, aux0, theta, ncell, dist, clocks=None):
     torch.cuda.synchronize()
     t_wall = time.time() - t_wall0
     clk = clocks.stop() if clocks else None
-    ms_total = sum(a.elapsed_time(b) for a, b in ev)
+    ms_total = max_over_ranks(dist, sum(a.elapsed_time(b) for a, b in ev))
     status = s.status()
-    if dist:
-        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
     # per-kernel split (events around each launch)
     s.set_kernel_timing(True)
     kt_steps = min(args.steps, 5)
@@ -315,18 +334,14 @@ def _time_path(args, s, U0, aux0, theta, ncell, dist, clocks=None):
         legs[k][3].record()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    e2e_ms = max_over_ranks(dist, e0.elapsed_time(e1))
     leg_ms = [sum(lg[i].elapsed_time(lg[i + 1]) for lg in legs) / e2e_steps for i in range(3)]
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
     ws = dist.get_world_size() if dist else 1
-    return {"value": ws * ncell * args.steps / (ms_total * 1e-3), "ms_per_step": ms_total / args.steps,
+    return {"value": job_value(ws, ncell, args.steps, ms_total), "ms_per_step": ms_total / args.steps,
             "status": status, "clocks": clk, "t_wall": t_wall,
             "kernel_ms_per_step": {k: v[0] / kt_steps for k, v in acc.items()},
             "kernel_ms_per_launch": {k: v[0] / max(v[1], 1) for k, v in acc.items()},
-            "e2e": {"value": ws * ncell * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
+            "e2e": {"value": job_value(ws, ncell, e2e_steps, e2e_ms), "unit": UNIT,
                     "h2d_bytes_per_step": (hU.numel() + haux.numel()) * 8,
                     "d2h_bytes_per_step": (hU.numel() + haux.numel()) * 8,
                     "steps": e2e_steps, "h2d_ms": leg_ms[0], "step_ms": leg_ms[1], "d2h_ms": leg_ms[2]}}

@@ -68,6 +68,19 @@ int jb_reaction_source_terms(jb_handle* h, const double* U, const double* aux, d
 int jb_advance(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
                double dt_fixed, double cfl, int nsteps, double* dt_hist, void* stream);
 
+/* One SSP-RK3 step of the flux alone, followed by update_aux after each
+ * stage: time_step_dict['TVD_RK3'](U, aux, dx, dy, dt, theta, flux_func,
+ * update_aux) (src/janc_v2/simulation/time_step/TVD_RK3.py:5-12), i.e. the
+ * advance_flux of set_simulator.py:83-84 without the chemistry split. */
+int jb_rk3(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
+           double dt, void* stream);
+
+/* U_to_prim(U, aux) -> rho, u, [v,] Y, p, a (src/janc_v2/solver_2D/aux_func.py:39-51,
+ * solver_1D/aux_func.py:39-50); each output is [ncell] except Y [8][ncell];
+ * v is ignored in 1D. */
+int jb_u_to_prim(jb_handle* h, const double* U, const double* aux, double* rho, double* u, double* v,
+                 double* Y, double* p, double* a, void* stream);
+
 /* CFL_1D / CFL_2D (set_simulator.py:420-443): *dt_out (device) =
  * cfl * min(dx/(|u|+a)) resp. cfl * min(1/((|u|+a)/dx + (|v|+a)/dy)). */
 int jb_cfl_dt(jb_handle* h, const double* U, const double* aux, double cfl, double* dt_out,

@@ -21,7 +21,7 @@ EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_fun
            "jb_reaction_source_terms", "jb_advance", "jb_cfl_dt", "jb_get_thermo", "jb_status",
            "jb_workspace_bytes", "jb_set_spacing", "jb_sizeof_mech_params", "jb_sizeof_grid",
            "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times",
-           "jb_update_aux_noalloc"]
+           "jb_update_aux_noalloc", "jb_rk3", "jb_u_to_prim"]
 
 _lib = None
 
@@ -55,6 +55,8 @@ def lib(path=None):
     L.jb_reaction_source_terms.argtypes = [vp, dp, dp, d, dp, vp]
     L.jb_advance.argtypes = [vp, dp, dp, dp, dp, d, d, i, dp, vp]
     L.jb_cfl_dt.argtypes = [vp, dp, dp, d, dp, vp]
+    L.jb_rk3.argtypes = [vp, dp, dp, dp, dp, d, vp]
+    L.jb_u_to_prim.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, dp, vp]
     L.jb_get_thermo.argtypes = [vp, ll, dp, dp, dp, dp, dp, dp, dp, vp]
     L.jb_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), vp]
     L.jb_workspace_bytes.argtypes = [vp]

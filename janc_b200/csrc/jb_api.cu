@@ -237,8 +237,9 @@ int jb_reaction_source_terms(jb_handle* h, const double* U, const double* aux, d
   return JB_OK;
 }
 
-int jb_advance(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
-               double dt_fixed, double cfl, int nsteps, double* dt_hist, void* stream) {
+static int advance_impl(jb_handle* h, const double* U, const double* aux, double* U_out,
+                        double* aux_out, double dt_fixed, double cfl, int nsteps, double* dt_hist,
+                        void* stream, bool chemistry) {
   if (!h || !U || !aux || !U_out || !aux_out) return set_err(h, JB_ERR_ARG, "null pointer");
   if (nsteps < 1) return set_err(h, JB_ERR_ARG, "nsteps must be >= 1");
   if (!(cfl > 0.0) && !(dt_fixed > 0.0)) return set_err(h, JB_ERR_ARG, "need cfl > 0 or dt > 0");
@@ -275,6 +276,15 @@ int jb_advance(jb_handle* h, const double* U, const double* aux, double* U_out, 
     JB_TIMED(JB_KCAT_FLUX, o.flux(d, 3, m, g, h->W[1], h->auxw[1], Un, h->W[0], h->cand, h->strips, h->slots, 2, 2,
                   0.0, st),
            "stage3");
+    if (!chemistry) {
+      // advance_flux only (TVD_RK3.py:5-12): U3, aux3 are the result
+      const size_t bytes = sizeof(double) * g.nv * (size_t)g.ncell;
+      JB_TRY(cudaMemcpyAsync(U_out, h->W[0], bytes, cudaMemcpyDeviceToDevice, st), "copy U3");
+      JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, U_out, nullptr, h->cand, aux_out,
+                                        h->strips, h->slots, 2, 3, st),
+               "select3");
+      continue;
+    }
     JB_TIMED(JB_KCAT_SELECT, o.select(d, true, false, false, m, g, h->W[0], nullptr, h->cand, h->auxw[0], h->strips,
                     h->slots, 2, 0, st),
            "select3");
@@ -284,6 +294,24 @@ int jb_advance(jb_handle* h, const double* U, const double* aux, double* U_out, 
                     h->slots, 3, 3, st),
            "select4");
   }
+  return JB_OK;
+}
+
+int jb_advance(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
+               double dt_fixed, double cfl, int nsteps, double* dt_hist, void* stream) {
+  return advance_impl(h, U, aux, U_out, aux_out, dt_fixed, cfl, nsteps, dt_hist, stream, true);
+}
+
+int jb_rk3(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
+           double dt, void* stream) {
+  return advance_impl(h, U, aux, U_out, aux_out, dt, 0.0, 1, nullptr, stream, false);
+}
+
+int jb_u_to_prim(jb_handle* h, const double* U, const double* aux, double* rho, double* u, double* v,
+                 double* Y, double* p, double* a, void* stream) {
+  if (!h || !U || !aux || !rho || !u || !Y || !p || !a || (h->dim == 2 && !v))
+    return set_err(h, JB_ERR_ARG, "null pointer");
+  JB_TRY(h->ops->prim(h->dim, h->mech, h->grid, U, aux, rho, u, v, Y, p, a, (cudaStream_t)stream), "prim");
   return JB_OK;
 }
 

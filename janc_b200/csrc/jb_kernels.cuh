@@ -1405,6 +1405,31 @@ __global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __r
 }
 
 // ---------------------------------------------------------------------------
+// U_to_prim (solver_{1D,2D}/aux_func.py:39-51): rho, u, [v,] Y, p, a
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void k_prim(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux,
+                       double* __restrict__ rho_o, double* __restrict__ u_o, double* __restrict__ v_o,
+                       double* __restrict__ Y_o, double* __restrict__ p_o, double* __restrict__ a_o) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  constexpr int nv = nY + NR;
+  const long long nc = g.ncell;
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double q[nv];
+#pragma unroll
+  for (int f = 0; f < nv; ++f) q[f] = U[f * nc + c];
+  Prim<DIM> pr = u_to_prim<DIM>(m, q, aux[c], aux[nc + c]);
+  rho_o[c] = pr.rho;
+  u_o[c] = pr.u;
+  if (DIM == 2) v_o[c] = pr.v;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y_o[k * nc + c] = q[nY + k] / pr.rho;
+  p_o[c] = pr.p;
+  a_o[c] = pr.a;
+}
+
+// ---------------------------------------------------------------------------
 // thermo evaluation for state building (thermo_model.get_thermo)
 // ---------------------------------------------------------------------------
 __global__ void k_thermo(MP m, long long n, const double* __restrict__ T, const double* __restrict__ Y,

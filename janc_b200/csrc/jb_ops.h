@@ -27,6 +27,9 @@ struct Ops {
   cudaError_t (*thermo)(const jb_mech_params& m, long long n, const double* T, const double* Y,
                         double* cp, double* gamma, double* h, double* R, double* dcp,
                         cudaStream_t st);
+  cudaError_t (*prim)(int dim, const jb_mech_params& m, const jb_grid& g, const double* U,
+                      const double* aux, double* rho, double* u, double* v, double* Y, double* p,
+                      double* a, cudaStream_t st);
   cudaError_t (*slots_reset)(jb_slots* s, cudaStream_t st);
   cudaError_t (*step_begin)(jb_slots* s, double cfl, double dt_fixed, double* dt_hist, int step,
                             cudaStream_t st);

@@ -1,0 +1,63 @@
+"""Module state shared by the mirror modules (the reference keeps the same
+configuration in module globals), and the cache of native solvers."""
+import numpy as np
+
+from .. import mechanism as _mech
+
+config = {
+    "mechanism": _mech.DEFAULT_MECHANISM,
+    "nondim": None,
+    "dim": "2D",
+    "boundary": None,
+    "precision": "fp64",
+    "flux": {"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS",
+             "split_method": "LF", "viscosity": "off"},
+    "detailed_chemistry": True,
+}
+_solvers = {}
+_mech_cache = {}
+
+
+def mechanism():
+    key = (config["mechanism"], repr(config["nondim"]))
+    if key not in _mech_cache:
+        _mech_cache[key] = _mech.load(config["mechanism"], config["nondim"])
+    return _mech_cache[key]
+
+
+def solver_for(shape, dx=1.0, dy=1.0):
+    """Cached native solver for a grid shape (1D: (nx,), 2D: (nx, ny))."""
+    from ..solver import Solver
+    dim = 1 if len(shape) == 1 else 2
+    bc = config["boundary"] or {}
+    key = (dim, tuple(shape), repr(sorted(bc.items())) if bc else "", config["precision"],
+           config["mechanism"], repr(config["nondim"]))
+    s = _solvers.get(key)
+    if s is None:
+        s = Solver(dim, shape[0], shape[1] if dim == 2 else None, dx, dy if dim == 2 else None,
+                   bc, mechanism(), precision=config["precision"])
+        _solvers[key] = s
+    s._spacing(dx, dy if dim == 2 else None)
+    return s
+
+
+def reset_solvers():
+    for s in _solvers.values():
+        s.close()
+    _solvers.clear()
+
+
+def to_device(x):
+    """(tensor, kind): CUDA float64 contiguous tensor and how to return results."""
+    import torch
+    if isinstance(x, torch.Tensor):
+        return x.to(device="cuda", dtype=torch.float64).contiguous(), "torch"
+    if hasattr(x, "__dlpack__") and not isinstance(x, np.ndarray):
+        return torch.from_dlpack(x).to(device="cuda", dtype=torch.float64).contiguous(), "torch"
+    return torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64), device="cuda"), "numpy"
+
+
+def back(t, kind):
+    if kind == "numpy":
+        return t.detach().cpu().numpy()
+    return t

@@ -213,6 +213,30 @@ class Solver:
         U, aux, _ = self.advance(U, aux, 1, dt=dt, theta=theta)
         return U, aux
 
+    def rk3(self, U, aux, dx=None, dy=None, dt=None, theta=None):
+        """time_step_dict['TVD_RK3'] with this solver's flux_func/update_aux:
+        the SSP-RK3 flux step without chemistry (TVD_RK3.py:5-12)."""
+        self._check_state(U, aux)
+        self._spacing(dx, dy)
+        self.set_theta(theta)
+        U_out = torch.empty_like(U)
+        aux_out = torch.empty_like(aux)
+        _native.check(self._lib.jb_rk3(self._h, _ptr(U), _ptr(aux), _ptr(U_out), _ptr(aux_out), float(dt),
+                                       _stream()), self._h, "jb_rk3")
+        return U_out, aux_out
+
+    def u_to_prim(self, U, aux):
+        """aux_func.U_to_prim: (rho, u, [v,] Y, p, a) with the reference's shapes."""
+        self._check_state(U, aux)
+        sh = (1,) + self.shape
+        rho, u, v, p, a = (torch.empty(sh, dtype=torch.float64, device=U.device) for _ in range(5))
+        Y = torch.empty((8,) + self.shape, dtype=torch.float64, device=U.device)
+        _native.check(self._lib.jb_u_to_prim(self._h, _ptr(U), _ptr(aux), _ptr(rho), _ptr(u), _ptr(v), _ptr(Y),
+                                             _ptr(p), _ptr(a), _stream()), self._h, "jb_u_to_prim")
+        if self.dim == 1:
+            return rho, u, Y, p, a
+        return rho, u, v, Y, p, a
+
     def cfl_dt(self, U, aux, cfl):
         self._check_state(U, aux)
         out = torch.empty((), dtype=torch.float64, device=U.device)
