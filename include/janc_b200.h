@@ -140,6 +140,55 @@ int jb_probe_fp64_fma(int blocks, int iters, double* scratch, void* stream);
 /* Human-readable description of the last error on this handle. */
 const char* jb_last_error(const jb_handle* h);
 
+/* ------------------------------------------------------------------------
+ * Batched ensemble of 1D instances (no single reference counterpart: the
+ * reference advances one case per Simulator; each instance here follows
+ * Simulator.advance_func, src/janc_v2/simulation/set_simulator.py:412-447,
+ * with its own CFL time step and LF alpha).  All instances use the same
+ * mechanism; they differ in length, spacing, side boundaries (bc[2i],
+ * bc[2i+1]: left, right; not the injector) and initial state.  The ensemble
+ * owns the state: U [11][nx_i] and aux [2][nx_i] of instance i live at the
+ * device pointers jb_ens_instance returns and are advanced in place.
+ * Precision: JB_PREC_FP64 or JB_PREC_MIXED.  cfl[i] > 0 selects the CFL time
+ * step, else dt[i] (dt may be NULL when every cfl[i] > 0).  Unlike the calls
+ * above, jb_ens_create, jb_ens_configure and jb_ens_autotune allocate device
+ * memory, and the first jb_ens_advance of a launch shape builds its graph.
+ * ------------------------------------------------------------------------ */
+typedef struct jb_ensemble jb_ensemble;
+
+int jb_ens_create(const jb_mech_params* mech, int n, const int* nx, const double* dx, const int* bc,
+                  const double* cfl, const double* dt, int precision, jb_ensemble** out);
+int jb_ens_destroy(jb_ensemble* e);
+/* Device pointers to instance i's state and its cell count. */
+int jb_ens_instance(jb_ensemble* e, int i, double** U, double** aux, int* nx);
+long long jb_ens_total_cells(const jb_ensemble* e);
+/* Launch shape: block = 64, 128 or 256 threads, blocks_per_sm resident CTAs
+ * per SM; CTAs are assigned to instances in proportion to their flux tiles. */
+int jb_ens_configure(jb_ensemble* e, int block, int blocks_per_sm);
+/* Times every launch shape the device fits on `trial_steps` steps (the
+ * state is restored afterwards) and keeps the fastest. */
+int jb_ens_autotune(jb_ensemble* e, int trial_steps, void* stream, int* best_block, int* best_bpsm,
+                    double* best_ms);
+int jb_ens_launch_shape(const jb_ensemble* e, int* block, int* blocks_per_sm, int* nblocks, int* max_tiles,
+                        int* graph_mode);
+/* Advance every instance nsteps steps with one persistent cooperative
+ * launch, replayed from a CUDA graph (rebuilt when nsteps, dt_hist or the
+ * launch shape change).  dt_hist: NULL or device [n][nsteps] time steps. */
+int jb_ens_advance(jb_ensemble* e, int nsteps, double* dt_hist, void* stream);
+/* The same launch without the graph. */
+int jb_ens_advance_direct(jb_ensemble* e, int nsteps, double* dt_hist, void* stream);
+/* Synchronises `stream`, returns the status bits seen per instance (array of
+ * n, or NULL) and combined (JB_ERR_TIMEOUT when a barrier wait gave up; the
+ * kernel then stopped early and later launches return at once until this
+ * call has reported it), and clears them. */
+int jb_ens_status(jb_ensemble* e, unsigned* per_instance, unsigned* combined, void* stream);
+const char* jb_ens_last_error(const jb_ensemble* e);
+/* Test hook for the timeout path: one launch in which instance 0's CTA
+ * group waits for a CTA that is never launched, so its first barrier gives
+ * up after wait_limit_ms (at most 1000) and every CTA returns; *combined
+ * then holds JB_ERR_TIMEOUT.  Leaves the ensemble's state undefined. */
+int jb_ens_selftest_timeout(jb_ensemble* e, double wait_limit_ms, unsigned* combined, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

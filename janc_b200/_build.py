@@ -1,7 +1,9 @@
 """Build the sm_100a shared library ``janc_b200/libjanc_b200.so`` in-tree.
 
-Three translation units: ``jb_strict.cu`` (-fmad=false, the reference's
-rounding), ``jb_fast.cu`` (FMA contraction) and ``jb_api.cu`` (the C ABI).
+Translation units: ``jb_strict.cu`` (-fmad=false, the reference's rounding),
+``jb_fast.cu`` (FMA contraction, FP64 and mixed variants), ``jb_ensemble.cu``
+(the persistent batched kernel and its C ABI), ``jb_api.cu`` (the C ABI of
+the single-case solver), ``jb_noalloc.cu`` and ``jb_probe.cu``.
 Compiled with nvcc for ``-gencode arch=compute_100a,code=sm_100a``.
 """
 import concurrent.futures as cf
@@ -16,8 +18,8 @@ LIB = os.path.join(HERE, "libjanc_b200.so")
 OBJ = os.path.join(HERE, "_objs")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-UNITS = [("jb_strict.cu", ["-fmad=false"]), ("jb_fast.cu", ["-fmad=true"]), ("jb_api.cu", []),
-         ("jb_probe.cu", []), ("jb_noalloc.cu", [])]
+UNITS = [("jb_ensemble.cu", ["-fmad=true"]), ("jb_strict.cu", ["-fmad=false"]), ("jb_fast.cu", ["-fmad=true"]),
+         ("jb_api.cu", []), ("jb_probe.cu", []), ("jb_noalloc.cu", [])]
 
 
 def _nvcc():

@@ -21,7 +21,10 @@ EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_fun
            "jb_reaction_source_terms", "jb_advance", "jb_cfl_dt", "jb_get_thermo", "jb_status",
            "jb_workspace_bytes", "jb_set_spacing", "jb_sizeof_mech_params", "jb_sizeof_grid",
            "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times",
-           "jb_update_aux_noalloc", "jb_rk3", "jb_u_to_prim"]
+           "jb_update_aux_noalloc", "jb_rk3", "jb_u_to_prim",
+           "jb_ens_create", "jb_ens_destroy", "jb_ens_instance", "jb_ens_total_cells", "jb_ens_configure",
+           "jb_ens_autotune", "jb_ens_launch_shape", "jb_ens_advance", "jb_ens_advance_direct",
+           "jb_ens_status", "jb_ens_last_error", "jb_ens_selftest_timeout"]
 
 _lib = None
 
@@ -68,6 +71,21 @@ def lib(path=None):
     L.jb_kernel_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
     L.jb_last_error.argtypes = [vp]
     L.jb_last_error.restype = ctypes.c_char_p
+    ip, dpp = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    L.jb_ens_create.argtypes = [ctypes.POINTER(_mech.MechParams), i, ip, dpp, ip, dpp, dpp, i, ctypes.POINTER(vp)]
+    L.jb_ens_destroy.argtypes = [vp]
+    L.jb_ens_instance.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(vp), ip]
+    L.jb_ens_total_cells.argtypes = [vp]
+    L.jb_ens_total_cells.restype = ll
+    L.jb_ens_configure.argtypes = [vp, i, i]
+    L.jb_ens_autotune.argtypes = [vp, i, vp, ip, ip, dpp]
+    L.jb_ens_launch_shape.argtypes = [vp, ip, ip, ip, ip, ip]
+    L.jb_ens_advance.argtypes = [vp, i, dp, vp]
+    L.jb_ens_advance_direct.argtypes = [vp, i, dp, vp]
+    L.jb_ens_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint), vp]
+    L.jb_ens_selftest_timeout.argtypes = [vp, d, ctypes.POINTER(ctypes.c_uint), vp]
+    L.jb_ens_last_error.argtypes = [vp]
+    L.jb_ens_last_error.restype = ctypes.c_char_p
     for name in EXPORTS:
         getattr(L, name)
     if L.jb_sizeof_mech_params() != ctypes.sizeof(_mech.MechParams):
@@ -76,9 +94,10 @@ def lib(path=None):
     return L
 
 
-def check(rc, handle=None, what=""):
+def check(rc, handle=None, what="", ensemble=False):
     if rc != 0:
         msg = ""
         if handle is not None:
-            msg = lib().jb_last_error(handle).decode()
+            err = lib().jb_ens_last_error if ensemble else lib().jb_last_error
+            msg = err(handle).decode()
         raise JancError(f"{what} failed: {status_text(rc)} (code {rc}) {msg}".strip())

@@ -912,22 +912,25 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
   block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
 }
 
-// 1D: tiles of 255 cells so the 256 faces map one-to-one onto threads.
-constexpr int TX1 = 255, PX1 = TX1 + 6, NT1 = 256;
+// 1D: a block of NT threads handles a tile of NT-1 cells, so its NT faces
+// map one-to-one onto threads.
+constexpr int NT1 = 256;
 
-template <class R>
+template <class R, int NT = NT1>
 __host__ __device__ constexpr size_t smem1d_bytes(int nq) {
-  return sizeof(R) * ((size_t)nq * PX1 + 3 * PX1 + 2 * PX1 + (TX1 + 1));
+  return sizeof(R) * ((size_t)nq * (NT + 5) + 3 * (NT + 5) + 2 * (NT + 5) + NT);
 }
 
-template <int STAGE, class R>
-__global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __restrict__ Uk,
-                                                 const double* __restrict__ auxk,
-                                                 const double* __restrict__ Un,
-                                                 double* __restrict__ out, double* __restrict__ cand,
-                                                 const double* __restrict__ strips, Slots* slots,
-                                                 int aidx, int midx, double dt_arg) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+// One tile [x0, x0 + NT - 1) of a 1D stage (see k_flux2d for STAGE and R).
+// Every thread of the block must call it; returns this thread's Halley mask.
+// Pointers are plain (not restrict) because the persistent ensemble kernel
+// calls it on buffers written by other blocks of the same launch.
+template <int STAGE, class R, int NT>
+__device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, const double* Uk,
+                                                const double* auxk, const double* Un, double* out,
+                                                double* cand, const double* strips, double alpha,
+                                                double dt, int x0, unsigned char* smraw) {
+  constexpr int TX1 = NT - 1, PX1 = NT + 5;
   constexpr int nv = 11, nq = nv + 1;
   constexpr bool EXACT = sizeof(R) == sizeof(double);
   R* sQ = reinterpret_cast<R*>(smraw);  // [nq][PX1]
@@ -936,12 +939,10 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
   R* sHm = sHp + PX1;
   R* sF = sHm + PX1;                    // [TX1+1]
   const int tid = threadIdx.x;
-  const int x0 = blockIdx.x * TX1;
   const long long nc = g.ncell;
-  const double dt = STAGE == 0 ? dt_arg : slots->dt;
-  const R ax = (R)bitsd(slots->ax[aidx]);
+  const R ax = (R)alpha;
 
-  for (int i = tid; i < PX1; i += NT1) {
+  for (int i = tid; i < PX1; i += NT) {
     int x = x0 + i - 3;
     Src s = map_cell<1>(g, x, 0);
     if (s.kind == 0) {
@@ -958,7 +959,7 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
     }
   }
   __syncthreads();
-  for (int i = tid; i < PX1; i += NT1) {
+  for (int i = tid; i < PX1; i += NT) {
     R q[nv];
 #pragma unroll
     for (int f = 0; f < nv; ++f) q[f] = sQ[f * PX1 + i];
@@ -972,7 +973,7 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
   const bool live = tid < TX1 && x0 + tid < g.nx;
   const size_t cell = (size_t)(x0 + tid);
   for (int f = 0; f < nv; ++f) {
-    for (int i = tid; i < PX1; i += NT1) {
+    for (int i = tid; i < PX1; i += NT) {
 #if JB_FAST
       // F = u q + p (rho u) + u p (rho E): the reference's LF flux regrouped
       const R u = sP[PX1 + i], qf = sQ[f * PX1 + i];
@@ -989,7 +990,7 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
     }
     __syncthreads();
     {
-      int mf = tid;  // 256 faces
+      int mf = tid;  // NT faces
       R L = weno_L(sHp[mf], sHp[mf + 1], sHp[mf + 2], sHp[mf + 3], sHp[mf + 4]);
       R Rr = weno_R(sHm[mf + 1], sHm[mf + 2], sHm[mf + 3], sHm[mf + 4], sHm[mf + 5]);
       sF[mf] = L + Rr;
@@ -1012,8 +1013,8 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
     }
     __syncthreads();
   }
-  if (STAGE == 0) return;
   unsigned bits = 0;
+  if (STAGE == 0) return bits;
   if (live) {
     double q[11];
     for (int f = 0; f < 11; ++f) q[f] = out[f * nc + cell];
@@ -1030,6 +1031,22 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
 #pragma unroll
     for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
   }
+  __syncthreads();  // the tile's shared memory is reused by the next tile
+  return bits;
+}
+
+template <int STAGE, class R>
+__global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __restrict__ Uk,
+                                                 const double* __restrict__ auxk,
+                                                 const double* __restrict__ Un,
+                                                 double* __restrict__ out, double* __restrict__ cand,
+                                                 const double* __restrict__ strips, Slots* slots,
+                                                 int aidx, int midx, double dt_arg) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const double dt = STAGE == 0 ? dt_arg : slots->dt;
+  unsigned bits = flux1d_tile<STAGE, R, NT1>(m, g, Uk, auxk, Un, out, cand, strips, bitsd(slots->ax[aidx]), dt,
+                                             blockIdx.x * (NT1 - 1), smraw);
+  if (STAGE == 0) return;
   block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
 }
 
@@ -1067,23 +1084,24 @@ __global__ void k_halley(MP m, Grid g, const double* __restrict__ U, const doubl
 // flux_splitting/LF.py "nanmax(|u|+a)"), the CFL minimum (CFL:
 // set_simulator.py:420-443) and the non-copy ghost strips (STRIPS).
 // ---------------------------------------------------------------------------
+// One cell of the select pass; folds its wave speeds / CFL candidate into
+// amx, amy, dtm and status bits into st.  mask: the Halley mask of the solve
+// being finished (SELECT); slots: where a NaN CFL candidate is flagged.
 template <int DIM, bool SELECT, bool ALPHA, bool CFL>
-__global__ void k_select(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux_in,
-                         const double* __restrict__ cand, double* __restrict__ aux_out,
-                         double* __restrict__ strips, Slots* slots, int midx, int aidx) {
+__device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const double* U, const double* aux_in,
+                                            const double* cand, double* aux_out, double* strips,
+                                            Slots* slots, unsigned mask, long long c, double& amx,
+                                            double& amy, double& dtm, unsigned& st) {
   constexpr int nY = DIM == 1 ? 3 : 4;
   constexpr int nv = nY + NR;
   const long long nc = g.ncell;
-  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
-  unsigned st = 0;
-  if (c < nc) {
+  {
     double q[nv];
 #pragma unroll
     for (int f = 0; f < nv; ++f) q[f] = U[f * nc + c];
     double gamma, T;
     if (SELECT) {
-      int n = halley_count(slots->mask[midx]);
+      int n = halley_count(mask);
       T = cand[n * nc + c];
       double Y8[NR], Yf[NS];
 #pragma unroll
@@ -1102,12 +1120,12 @@ __global__ void k_select(MP m, Grid g, const double* __restrict__ U, const doubl
       Prim<DIM> pr = u_to_prim<DIM>(m, q, gamma, T);
       double sx = fabs(pr.u) + pr.a;
       double sy = fabs(pr.v) + pr.a;
-      amx = sx;
-      amy = sy;
+      amx = fmax(amx, sx);
+      amy = fmax(amy, sy);
       if (!(sx == sx) || !(T == T)) st |= JB_ERR_NONFINITE;
       if (CFL) {
         double d = DIM == 1 ? g.dx / sx : 1.0 / (sx / g.dx + sy / g.dy);
-        dtm = d;
+        dtm = fmin(dtm, d);
         if (!(d == d) || !(d > 0.0)) st |= JB_ERR_NONFINITE;
         // jnp.min (set_simulator.py:423,441) returns NaN if any candidate is
         // NaN; the reduction below skips NaN, so record it separately
@@ -1144,6 +1162,18 @@ __global__ void k_select(MP m, Grid g, const double* __restrict__ U, const doubl
       }
     }
   }
+}
+
+template <int DIM, bool SELECT, bool ALPHA, bool CFL>
+__global__ void k_select(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux_in,
+                         const double* __restrict__ cand, double* __restrict__ aux_out,
+                         double* __restrict__ strips, Slots* slots, int midx, int aidx) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
+  unsigned st = 0;
+  if (c < g.ncell)
+    select_cell<DIM, SELECT, ALPHA, CFL>(m, g, U, aux_in, cand, aux_out, strips, slots,
+                                         SELECT ? slots->mask[midx] : 0u, c, amx, amy, dtm, st);
   if (ALPHA || CFL) block_reduce_store(amx, amy, dtm, st << 16, slots, aidx, ALPHA, CFL, -1);
 }
 
@@ -1347,21 +1377,19 @@ __device__ __forceinline__ void chem_cell_gen(const MP& m, double rho, const dou
 }
 #endif
 
-// WRITE_S: reaction_source_terms output S (zeros for the flow fields).
-// Otherwise U_out = U + S followed by the Halley iterates of the final
-// update_aux (set_simulator.py:117-122).
+// Chemistry of one cell at temperature T.  WRITE_S: reaction_source_terms
+// output S (zeros for the flow fields).  Otherwise U_out = U + S followed by
+// the Halley iterates of the final update_aux (set_simulator.py:117-122),
+// started from T.  sh: this thread's column of the [CHEM_SH][blockDim]
+// shared array.
 template <int DIM, bool WRITE_S, bool GEN>
-__global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __restrict__ U,
-                                              const double* __restrict__ aux,
-                                              double* __restrict__ out, double* __restrict__ cand,
-                                              Slots* slots, int midx, double dt_arg) {
+__device__ __forceinline__ void chem_cell_step(const MP& m, const Grid& g, const double* U, double T,
+                                               double* out, double* cand, long long c, double dt,
+                                               double* sh, unsigned& bits, unsigned& st) {
   constexpr int nY = DIM == 1 ? 3 : 4;
   constexpr int nv = nY + NR;
   const long long nc = g.ncell;
-  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const double dt = WRITE_S ? dt_arg : slots->dt;
-  unsigned bits = 0, st = 0;
-  if (c < nc) {
+  {
     double q[nv];
 #pragma unroll
     for (int f = 0; f < nv; ++f) q[f] = U[f * nc + c];
@@ -1369,12 +1397,11 @@ __global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __r
     double Y8[NR], S[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / rho;
-    double T = aux[nc + c];
 #if JB_FAST
-    extern __shared__ double shc[];
-    if (GEN) chem_cell_gen(m, rho, Y8, T, dt, S, st, shc + threadIdx.x, blockDim.x);
+    if (GEN) chem_cell_gen(m, rho, Y8, T, dt, S, st, sh, blockDim.x);
     else chem_cell(m, rho, Y8, T, dt, S, st);
 #else
+    (void)sh;
     chem_cell(m, rho, Y8, T, dt, S, st);
 #endif
     if (WRITE_S) {
@@ -1396,11 +1423,24 @@ __global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __r
       fill_Y(Yn, Yf);
       double R = get_R(m, Yf);
       double cnd[JB_NCAND];
-      bits = halley_any(m, e, Yf, R, T, cnd);
+      bits |= halley_any(m, e, Yf, R, T, cnd);
 #pragma unroll
       for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + c] = cnd[i];
     }
   }
+}
+
+template <int DIM, bool WRITE_S, bool GEN>
+__global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __restrict__ U,
+                                              const double* __restrict__ aux,
+                                              double* __restrict__ out, double* __restrict__ cand,
+                                              Slots* slots, int midx, double dt_arg) {
+  extern __shared__ double shc[];
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = WRITE_S ? dt_arg : slots->dt;
+  unsigned bits = 0, st = 0;
+  if (c < g.ncell)
+    chem_cell_step<DIM, WRITE_S, GEN>(m, g, U, aux[g.ncell + c], out, cand, c, dt, shc + threadIdx.x, bits, st);
   block_reduce_store(0.0, 0.0, 0.0, bits | (st << 16), slots, 0, false, false, WRITE_S ? -1 : midx);
 }
 
