@@ -28,6 +28,16 @@ Arms:
                      NumPy oracle restating src/janc_v2 (JAX is not available
                      on the box), run as independent replicas on all host
                      cores
+Batched ensemble (--workload ensemble, run with --steps 2000): 64 1D H2-air
+detonation tubes of log-uniform length 1000-16000 cells (dx = 50 um), equivalence
+ratio U(0.6, 1.4) and ignition temperature U(2500, 3500) K (numpy
+default_rng(4)), ignition slab over the first 2 % of each tube at 30 atm,
+reflective left / outflow right, CFL 0.1 per tube; one "step" advances every
+tube one time step, all K steps run as ONE persistent kernel replayed from a
+CUDA graph with the autotuned launch shape.  Compared with the 64 tubes run
+one after another through the single-case float64 path, and the mixed result
+is checked against those float64 runs per tube.
+
 Multi-GPU: the path does not shard in this build (replicas only): each rank
 advances its own copy of the workload; value = total cells x steps / max time.
 """
@@ -54,6 +64,13 @@ BYTES_CHEM_PER_CELL = 224      # read U,aux (112 B) + write U,aux (112 B), float
 BYTES_STEP_PER_CELL = 864 + 224  # fused-step minimum + separate chemistry pass (2D)
 BYTES_FLUX_STAGE_PER_CELL = 288  # one RK stage of the fused minimum: (224 + 320 + 320) / 3
 
+
+ENS_N, ENS_SEED, ENS_CFL = 64, 4, 0.1
+# 1D step, float64, each pass reading its inputs once and writing its outputs
+# once (fields: 11 conserved, aux T, 6 Halley iterates): stage 1 (12 in, 17
+# out), select 1 (12 in, 2 out), stages 2 and 3 (23 in, 17 out), select 2
+# (14), chemistry (12 in, 17 out), select 4 (14) -> 180 doubles
+BYTES_ENS_STEP_PER_CELL = 1440
 
 RDC_NX, RDC_NY = 1600, 1000
 RDC_ND = {"P0": 10 * 101325, "T0": 300, "R0": 369, "x0": 0.08}
@@ -469,6 +486,248 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------ ensemble arm
+BC1 = {"left_boundary": "slip_wall", "right_boundary": "zero_gradient"}
+
+
+def _ens_setup(precision):
+    from janc_b200.ensemble import Ensemble, detonation_tubes
+    tubes = detonation_tubes(ENS_N, seed=ENS_SEED)
+    ens = Ensemble([t["nx"] for t in tubes], [t["dx"] for t in tubes], cfl=ENS_CFL, precision=precision)
+    init = []
+    for i, t in enumerate(tubes):
+        U, aux = ens.state_from_PTY(t["P"], t["T"], t["Y"])
+        ens.set_state(i, U, aux)
+        init.append((U, aux))
+    return ens, tubes, init
+
+
+def _ens_reset(ens, init):
+    for i, (U, aux) in enumerate(init):
+        ens.set_state(i, U, aux)
+
+
+def _prim_1d(mech, U, aux):
+    """rho, p, T of a 1D state (U: rho, rho u, rho E, rho Y_1..8)."""
+    import torch
+    invM = torch.tensor(1.0 / mech.tables["species_M"], device=U.device)
+    rho = U[0]
+    Y8 = U[3:] / rho
+    Yf = torch.cat([Y8, (1.0 - Y8.sum(0))[None]], 0)
+    R = (invM[:, None] * Yf).sum(0)
+    return rho, rho * R * aux[1], aux[1]
+
+
+def run_ensemble(args):
+    import torch
+    from janc_b200 import _native
+    from janc_b200.solver import Solver
+    if args.precision not in ("fp64", "mixed"):
+        raise SystemExit("the ensemble runs in 'fp64' or 'mixed' precision")
+    dist, rank, ws = _dist()
+    dev = torch.cuda.current_device()
+    ens, tubes, init = _ens_setup(args.precision)
+    cells = ens.total_cells
+    K = args.steps
+    if args.ens_shape:
+        block, bpsm = (int(v) for v in args.ens_shape.split("x"))
+        ens.configure(block, bpsm)
+        tune = {"skipped": f"launch shape fixed by --ens-shape {args.ens_shape}"}
+    else:
+        tune = ens.autotune(trial_steps=20)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    _ens_reset(ens, init)
+    ens.advance(args.warmup)
+    _ens_reset(ens, init)
+    ens.advance(K)  # captures the K-step graph replayed below
+    _ens_reset(ens, init)
+    flush.zero_()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_wall0 = time.time()
+    e0.record()
+    ens.advance(K)
+    e1.record()
+    torch.cuda.synchronize()
+    t_wall = time.time() - t_wall0
+    clk = clocks.stop()
+    ms = max_over_ranks(dist, e0.elapsed_time(e1))
+    status, per_status = ens.status()
+    shape = ens.launch_shape()
+    final = [ens.get_state(i) for i in range(ENS_N)]
+    n_finite = sum(int(torch.all(torch.isfinite(U)).item()) for U, _ in final)
+    value = job_value(ws, cells, K, ms)
+    # end to end through the public API: pinned host states in, K steps, states out
+    hU = [U.cpu().pin_memory() for U, _ in init]
+    ha = [a.cpu().pin_memory() for _, a in init]
+    oU = [torch.empty_like(x).pin_memory() for x in hU]
+    oa = [torch.empty_like(x).pin_memory() for x in ha]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    legs = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    legs[0].record()
+    for i in range(ENS_N):
+        Ud, ad = ens.state(i)
+        Ud.copy_(hU[i], non_blocking=True)
+        ad.copy_(ha[i], non_blocking=True)
+    legs[1].record()
+    ens.advance(K)
+    legs[2].record()
+    for i in range(ENS_N):
+        Ud, ad = ens.state(i)
+        oU[i].copy_(Ud, non_blocking=True)
+        oa[i].copy_(ad, non_blocking=True)
+    legs[3].record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(dist, legs[0].elapsed_time(legs[3]))
+    io_bytes = sum(x.numel() for x in hU + ha) * 8
+    # the 64 tubes one after another through the single-case float64 path
+    seq_steps = args.seq_steps or K
+    seq_ms, seq_final = 0.0, []
+    for i, t in enumerate(tubes):
+        s = Solver(1, t["nx"], dx=t["dx"], boundary_config=BC1, precision="fp64")
+        s.advance(init[i][0], init[i][1], 3, cfl=ENS_CFL)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        U, aux, _ = s.advance(init[i][0], init[i][1], seq_steps, cfl=ENS_CFL)
+        b.record()
+        torch.cuda.synchronize()
+        seq_ms += a.elapsed_time(b)
+        seq_final.append((U, aux))
+        del s
+    seq_ms = max_over_ranks(dist, seq_ms)
+    seq_value = job_value(ws, cells, seq_steps, seq_ms)
+    acc = None
+    if seq_steps == K:
+        worst = {"rho": 0.0, "p": 0.0, "T": 0.0}
+        dfront = 0
+        for (Ua, aa), (Ub, ab) in zip(final, seq_final):
+            pa = _prim_1d(ens.mech, Ua, aa)
+            pb = _prim_1d(ens.mech, Ub, ab)
+            for name, x, y in zip(("rho", "p", "T"), pa, pb):
+                worst[name] = max(worst[name], float((x - y).abs().sum() / y.abs().sum()))
+            pamb = float(pb[1][-1])
+            fa = int(torch.nonzero(pa[1] > 2 * pamb).max()) if bool((pa[1] > 2 * pamb).any()) else -1
+            fb = int(torch.nonzero(pb[1] > 2 * pamb).max()) if bool((pb[1] > 2 * pamb).any()) else -1
+            dfront = max(dfront, abs(fa - fb))
+        acc = {"steps": K, "l1_rel_max_over_tubes": worst, "front_max_offset_cells": dfront,
+               "reference": "the same tubes through the single-case float64 path"}
+    hbm_peak, hbm_src = 6650.0, "fallback"
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        try:
+            hbm_peak = float(json.load(open(peaks_path))["hbm_gbs"])
+            hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except Exception:
+            pass
+    fp64_peak = fp64_peak_tflops(_native.lib(), torch)
+    arith, special = chem_flops_per_cell()
+    achieved = BYTES_ENS_STEP_PER_CELL * cells * K / (ms * 1e-3) / 1e9
+    chem_tflops = arith * cells * K / (ms * 1e-3) / 1e12
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_ensemble(args.cpu_steps)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    sizes = [t["nx"] for t in tubes]
+    line = {
+        "metric": "total " + METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32 flux / f64 state, T-solve, chemistry",
+        "data": "synthetic", "precision": args.precision,
+        "config": {"workload": f"batched ensemble: {ENS_N} 1D H2-air detonation tubes, lengths "
+                               f"log-uniform 1000-16000 cells (dx 50 um), phi U(0.6,1.4), T_ign "
+                               f"U(2500,3500) K, default_rng({ENS_SEED}); 30 atm slab over the first 2 %; "
+                               f"reflective left / outflow right; CFL {ENS_CFL} per tube",
+                   "cells": cells, "tubes": ENS_N, "cells_min": min(sizes), "cells_max": max(sizes),
+                   "launch": "one persistent cooperative kernel for all steps, replayed from a CUDA graph",
+                   "launch_shape": shape, "autotune": tune,
+                   "l2": "flushed once before the timed launch (256 MB write); inside the persistent "
+                         "launch each tube's working set stays wherever the cache keeps it",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+        "status_bits": status, "tubes_finite": n_finite,
+        "gpu_launches": 1,
+        "roofline": {"bound": "hbm", "kernel": "k_ensemble (all phases of all steps)", "achieved": achieved,
+                     "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                     "peak_source": hbm_src, "algorithmic_bytes_per_cell_step": BYTES_ENS_STEP_PER_CELL,
+                     "launch_ms": ms},
+        "compute_roofline": {"bound": "fp64", "kernel": "k_ensemble (chemistry share of the flops only)",
+                             "achieved": chem_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+                             "frac": chem_tflops / fp64_peak, "peak_source": "measured live (jb_probe_fp64_fma)"},
+        "e2e": {"value": job_value(ws, cells, K, e2e_ms), "unit": UNIT,
+                "h2d_bytes_per_step": io_bytes / K, "d2h_bytes_per_step": io_bytes / K,
+                "h2d_bytes_per_call": io_bytes, "d2h_bytes_per_call": io_bytes, "steps_per_call": K,
+                "h2d_ms": legs[0].elapsed_time(legs[1]), "run_ms": legs[1].elapsed_time(legs[2]),
+                "d2h_ms": legs[2].elapsed_time(legs[3])},
+        "sequential_fp64": {"value": seq_value, "steps": seq_steps, "ms_total": seq_ms,
+                            "path": "64 tubes one after another, single-case float64 solver (11 launches/step)"},
+        "speedup_vs_sequential_fp64": value / seq_value,
+        "clocks": clk, "wall_s_timed_region": t_wall,
+    }
+    if acc is not None:
+        line["accuracy_vs_fp64"] = acc
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def _oracle_tube(args):
+    """One replica: the NumPy oracle advancing ensemble tube i for `steps` steps."""
+    i, steps = args
+    import warnings
+    warnings.simplefilter("ignore")
+    sys.path.insert(0, ROOT)
+    from oracle import janc_oracle as jo
+    from janc_b200.ensemble import detonation_tubes
+    from janc_b200.mechanism import DEFAULT_MECHANISM
+    m = jo.load_mechanism(DEFAULT_MECHANISM)
+    t = detonation_tubes(ENS_N, seed=ENS_SEED)[i]
+    U, aux = jo.state_from_PTY(m, t["P"], t["T"], t["Y"])
+    s = jo.Solver(m, "1D", t["dx"], None, BC1, ENS_CFL)
+    U, aux, tt, _ = s.advance_func(U, aux, 0.0)  # warm-up step
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        U, aux, tt, _ = s.advance_func(U, aux, tt)
+    return time.perf_counter() - t0, t["nx"] * steps
+
+
+def cpu_baseline_ensemble(steps):
+    """The oracle on all host cores, one ensemble tube per process."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    nrep = max(1, min(cores, ENS_N))
+    env_keep = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
+    for k in env_keep:
+        os.environ[k] = "1"
+    t0 = time.perf_counter()
+    with cf.ProcessPoolExecutor(nrep, mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_oracle_tube, [(i, steps) for i in range(nrep)]))
+    wall = time.perf_counter() - t0
+    for k, v in env_keep.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v
+    slowest = max(r[0] for r in res)
+    cells = sum(r[1] for r in res)
+    return {"value": cells / slowest, "unit": UNIT, "cores": nrep, "kind": "port",
+            "sample": f"tubes 0..{nrep - 1} of the {ENS_N}-tube ensemble, {steps} steps each, one process "
+                      f"per core (NumPy oracle restating src/janc_v2)",
+            "wall_s": wall}
+
+
 # ----------------------------------------------------------------- CPU side
 def _oracle_replica(args):
     """One replica: the NumPy oracle advancing a 32 x 256 strip of the channel
@@ -524,6 +783,18 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.workload == "ensemble":
+        steps = max(1, min(args.steps, 10))
+        cpu = cpu_baseline_ensemble(steps)
+        line = {"impl": "reference", "metric": "total " + METRIC, "value": cpu["value"], "unit": UNIT,
+                "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": 1,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": f"batched ensemble of {ENS_N} 1D tubes, CPU reference path", "cfl": ENS_CFL},
+                "cpu_baseline": cpu,
+                "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     steps = max(1, min(args.steps, 20))
     cpu = cpu_baseline(steps)
     line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT,
@@ -548,7 +819,11 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "fp64_strict", "mixed"])
     ap.add_argument("--no-compare", action="store_true", help="skip the float64 comparison run")
     ap.add_argument("--accuracy-steps", type=int, default=100)
-    ap.add_argument("--workload", default="channel", choices=["channel", "rdc"])
+    ap.add_argument("--workload", default="channel", choices=["channel", "rdc", "ensemble"])
+    ap.add_argument("--ens-shape", default="",
+                    help="ensemble: fixed launch shape BLOCKxCTAS_PER_SM instead of the autotuner")
+    ap.add_argument("--seq-steps", type=int, default=0,
+                    help="ensemble: steps of the sequential float64 comparison (default: --steps)")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -556,6 +831,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble":
+        run_ensemble(args)
     else:
         run_ours(args)
 

@@ -100,7 +100,8 @@ def test_simulator_1d_matches_reference(golden_dir):
 
 
 @pytest.mark.gpu
-def test_2d_functions_match_reference(golden_dir):
+@pytest.mark.parametrize("precision", ["fp64_strict", "fp64"])
+def test_2d_functions_match_reference(golden_dir, precision):
     from janc_b200.janc.model import thermo_model
     from janc_b200.janc.simulation import set_simulator
     from janc_b200.janc.simulation.time_step import time_step_dict
@@ -109,27 +110,31 @@ def test_2d_functions_match_reference(golden_dir):
     dx, dy = float(g["dx"]), float(g["dy"])
     bc = {"left_boundary": "slip_wall", "right_boundary": "zero_gradient",
           "bottom_boundary": "slip_wall", "top_boundary": "slip_wall"}
-    cfg = sim_config("2D", {"dx": dx, "dy": dy}, bc)
+    cfg = sim_config("2D", {"dx": dx, "dy": dy}, bc, precision=precision)
     sim = set_simulator.Simulator(cfg)
     flux_func, update_func, _ = set_simulator.set_rhs("2D", cfg["reaction_config"])
     rhs = flux_func(g["U0"], g["aux0"], dx, dy, 1e-8, None)
-    assert rel_field(rhs, g["rhs0"]) < 1e-12
+    if precision == "fp64_strict":
+        np.testing.assert_array_equal(rhs, g["rhs0"])
+    # (the FMA variant's rhs differs from the reference's by round-off, which
+    # is all there is in the fields that vanish at rest; its steps are checked)
+    tol = 1e-12 if precision == "fp64_strict" else 1e-10
     adv = set_simulator.set_advance_func("2D", cfg["flux_config"], cfg["reaction_config"], cfg["time_config"],
                                          False, flux_func, update_func, None)
     Ua, auxa = adv(g["U0"], g["aux0"], dx, dy, 2e-8, None)
-    assert rel_field(Ua, g["U_adv_dt2e-8"]) < 1e-10
+    assert rel_field(Ua, g["U_adv_dt2e-8"]) < tol
     # fused RK3 with the solver's own rhs/update, and the composed form with
     # a user wrapper around the same functions
     Ur, auxr = time_step_dict["TVD_RK3"](g["U0"], g["aux0"], dx, dy, 2e-8, None, flux_func, update_func)
-    assert rel_field(Ur, g["U_rk3_dt2e-8"]) < 1e-10
-    assert rel_field(auxr, g["aux_rk3_dt2e-8"]) < 1e-10
+    assert rel_field(Ur, g["U_rk3_dt2e-8"]) < tol
+    assert rel_field(auxr, g["aux_rk3_dt2e-8"]) < tol
     Uc, auxc = time_step_dict["TVD_RK3"](g["U0"], g["aux0"], dx, dy, 2e-8, None,
                                          lambda *a: flux_func(*a), lambda U, a: aux_func.update_aux(U, a))
-    assert rel_field(Uc, g["U_rk3_dt2e-8"]) < 1e-10
+    assert rel_field(Uc, g["U_rk3_dt2e-8"]) < tol
     U, aux, t = g["U0"], g["aux0"], 0.0
     for step in range(1, 4):
         U, aux, t, dt = sim.advance_func(U, aux, t, None)
-        assert rel_field(U, g[f"U_{step}"]) < 1e-10
+        assert rel_field(U, g[f"U_{step}"]) < tol
     prims = aux_func.U_to_prim(g["U0"], g["aux0"])
     assert len(prims) == 6 and prims[3].shape == (8,) + g["U0"].shape[1:]
     th = G(golden_dir, "thermo_si")
