@@ -141,6 +141,46 @@ int jb_probe_fp64_fma(int blocks, int iters, double* scratch, void* stream);
 const char* jb_last_error(const jb_handle* h);
 
 /* ------------------------------------------------------------------------
+ * Reverse mode (the adjoint), 2D grids with periodic, slip, no-slip or
+ * zero-gradient sides.  The reference gets these derivatives from jax.grad
+ * through advance_one_step and the CFL time step (set_simulator.py:117-122,
+ * 420-447) with get_T's custom VJP (src/janc_v2/model/thermo_model.py:
+ * 155-190); these calls compute the same vector-Jacobian products with
+ * hand-written kernels.
+ * ------------------------------------------------------------------------ */
+/* Pressure probe: mean p over the wx x wy cells from (x0, y0). */
+int jb_set_probe(jb_handle* h, int x0, int y0, int wx, int wy);
+/* Scale every pre-exponential factor A_i of the handle's mechanism by
+ * exp(offset[i]) relative to the tables given to jb_create (NULL restores
+ * them); offset is a host array of nreac doubles. */
+int jb_set_log_A_offset(jb_handle* h, const double* offset);
+/* Doubles of one step's record (U, aux and the three RK stages' states). */
+long long jb_record_doubles(const jb_handle* h);
+/* jb_advance (chemistry on) plus: probe_p (device, nsteps doubles, may be
+ * NULL) receives the probe pressure after each step; rec (device,
+ * (nsteps + 1) * jb_record_doubles doubles, may be NULL) receives every
+ * step's record and the final state, and rec_slots (device, nsteps *
+ * sizeof(jb_slots) bytes) each step's time step and LF alphas. */
+int jb_advance_ex(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
+                  double dt_fixed, double cfl, int nsteps, double* dt_hist, double* probe_p, double* rec,
+                  double* rec_slots, void* stream);
+/* One step of the adjoint.  rec points at step n's record (step n+1's
+ * record follows it), rec_slots at step n's slots; cfl as given to the
+ * forward (<= 0: fixed time step).  On entry Ubar / Abar hold the adjoint
+ * of the state after the step (U_{n+1}: nv x ncell, aux_{n+1}: 2 x ncell);
+ * on return that of the state before it.  dt_bar, pp_bar (device scalars,
+ * may be NULL) are the adjoints of the step's time step and probe
+ * pressure; lnA_bar (device, nreac doubles) accumulates the adjoint of
+ * ln A. */
+int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, double cfl, double* Ubar,
+                    double* Abar, const double* dt_bar, const double* pp_bar, double* lnA_bar, void* stream);
+/* Adjoint of the initial-state builder (rho = P/(R T), rho E = rho h - P,
+ * aux = [gamma, T]; examples/janc_basic_example1.ipynb) with respect to T:
+ * Tbar (ncell) from Ubar, Abar of the built state. */
+int jb_state_from_PTY_vjp(jb_handle* h, const double* P, const double* T, const double* Y, const double* Ubar,
+                          const double* Abar, double* Tbar, void* stream);
+
+/* ------------------------------------------------------------------------
  * Batched ensemble of 1D instances (no single reference counterpart: the
  * reference advances one case per Simulator; each instance here follows
  * Simulator.advance_func, src/janc_v2/simulation/set_simulator.py:412-447,

@@ -2,8 +2,9 @@
 
 Translation units: ``jb_strict.cu`` (-fmad=false, the reference's rounding),
 ``jb_fast.cu`` (FMA contraction, FP64 and mixed variants), ``jb_ensemble.cu``
-(the persistent batched kernel and its C ABI), ``jb_api.cu`` (the C ABI of
-the single-case solver), ``jb_noalloc.cu`` and ``jb_probe.cu``.
+(the persistent batched kernel and its C ABI), ``jb_adjoint.cu`` (the
+reverse-mode kernels), ``jb_api.cu`` (the C ABI of the single-case solver),
+``jb_noalloc.cu`` and ``jb_probe.cu``.
 Compiled with nvcc for ``-gencode arch=compute_100a,code=sm_100a``.
 """
 import concurrent.futures as cf
@@ -19,7 +20,7 @@ OBJ = os.path.join(HERE, "_objs")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 UNITS = [("jb_ensemble.cu", ["-fmad=true"]), ("jb_strict.cu", ["-fmad=false"]), ("jb_fast.cu", ["-fmad=true"]),
-         ("jb_api.cu", []), ("jb_probe.cu", []), ("jb_noalloc.cu", [])]
+         ("jb_adjoint.cu", ["-fmad=true"]), ("jb_api.cu", []), ("jb_probe.cu", []), ("jb_noalloc.cu", [])]
 
 
 def _nvcc():

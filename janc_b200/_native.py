@@ -24,7 +24,9 @@ EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_fun
            "jb_update_aux_noalloc", "jb_rk3", "jb_u_to_prim",
            "jb_ens_create", "jb_ens_destroy", "jb_ens_instance", "jb_ens_total_cells", "jb_ens_configure",
            "jb_ens_autotune", "jb_ens_launch_shape", "jb_ens_advance", "jb_ens_advance_direct",
-           "jb_ens_status", "jb_ens_last_error", "jb_ens_selftest_timeout"]
+           "jb_ens_status", "jb_ens_last_error", "jb_ens_selftest_timeout",
+           "jb_set_probe", "jb_set_log_A_offset", "jb_record_doubles", "jb_advance_ex", "jb_adjoint_step",
+           "jb_state_from_PTY_vjp"]
 
 _lib = None
 
@@ -83,6 +85,13 @@ def lib(path=None):
     L.jb_ens_advance.argtypes = [vp, i, dp, vp]
     L.jb_ens_advance_direct.argtypes = [vp, i, dp, vp]
     L.jb_ens_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint), vp]
+    L.jb_set_probe.argtypes = [vp, i, i, i, i]
+    L.jb_set_log_A_offset.argtypes = [vp, dpp]
+    L.jb_record_doubles.argtypes = [vp]
+    L.jb_record_doubles.restype = ll
+    L.jb_advance_ex.argtypes = [vp, dp, dp, dp, dp, d, d, i, dp, dp, dp, dp, vp]
+    L.jb_adjoint_step.argtypes = [vp, dp, dp, d, dp, dp, dp, dp, dp, vp]
+    L.jb_state_from_PTY_vjp.argtypes = [vp, dp, dp, dp, dp, dp, dp, vp]
     L.jb_ens_selftest_timeout.argtypes = [vp, d, ctypes.POINTER(ctypes.c_uint), vp]
     L.jb_ens_last_error.argtypes = [vp]
     L.jb_ens_last_error.restype = ctypes.c_char_p

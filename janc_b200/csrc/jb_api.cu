@@ -3,13 +3,16 @@
 #include <cuda_runtime.h>
 
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include <cmath>
 
 #include "../../include/janc_b200.h"
+#include "jb_adjoint.h"
 #include "jb_chem_gen.cuh"
 #include "jb_ops.h"
 
@@ -34,6 +37,16 @@ struct jb_handle {
   int ev_cat[JB_TIMED_MAX];
   double acc_ms[JB_KCAT_COUNT];
   long long acc_n[JB_KCAT_COUNT];
+  // adjoint support
+  double base_A[JB_NREAC_MAX];  // pre-exponential factors as created (jb_set_log_A_offset)
+  int probe[4];                 // x0, y0, wx, wy of the pressure probe (wx*wy = 0: none)
+  double* adj_ws;               // Ubar stage buffers, abar, ghost adjoints, reductions
+  unsigned char* adj_mult;      // padded-grid multiplicity of each cell (alpha ties)
+  double* adj_B1;
+  double* adj_B2;
+  double* adj_A2;
+  double* adj_ghost;
+  double* adj_red;
   char err[512];
 };
 
@@ -123,6 +136,7 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   std::memset(h, 0, sizeof(*h));
   h->mech = *mech;
   jb::derive_mech(h->mech);
+  for (int i = 0; i < JB_NREAC_MAX; ++i) h->base_A[i] = h->mech.A[i];
   h->dim = dim;
   h->precision = precision;
   h->ops = precision == JB_PREC_STRICT ? &jb::strict_ops
@@ -177,6 +191,8 @@ int jb_destroy(jb_handle* h) {
   if (h->cand) cudaFree(h->cand);
   if (h->strips) cudaFree(h->strips);
   if (h->slots) cudaFree(h->slots);
+  if (h->adj_ws) cudaFree(h->adj_ws);
+  if (h->adj_mult) cudaFree(h->adj_mult);
   delete h;
   return JB_OK;
 }
@@ -237,62 +253,98 @@ int jb_reaction_source_terms(jb_handle* h, const double* U, const double* aux, d
   return JB_OK;
 }
 
+// Record of one step for the adjoint, in doubles from the step's base:
+// U, aux, U1, aux1, U2, aux2, U3, aux3 (each nv resp. 2 fields); the next
+// step's record (or the final state) follows.
+static long long rec_stride(const jb_handle* h) { return 4LL * (h->grid.nv + 2) * h->grid.ncell; }
+
 static int advance_impl(jb_handle* h, const double* U, const double* aux, double* U_out,
                         double* aux_out, double dt_fixed, double cfl, int nsteps, double* dt_hist,
-                        void* stream, bool chemistry) {
+                        void* stream, bool chemistry, double* probe_p = nullptr, double* rec = nullptr,
+                        double* rec_slots = nullptr) {
   if (!h || !U || !aux || !U_out || !aux_out) return set_err(h, JB_ERR_ARG, "null pointer");
   if (nsteps < 1) return set_err(h, JB_ERR_ARG, "nsteps must be >= 1");
   if (!(cfl > 0.0) && !(dt_fixed > 0.0)) return set_err(h, JB_ERR_ARG, "need cfl > 0 or dt > 0");
   if (U == U_out || aux == aux_out) return set_err(h, JB_ERR_ARG, "outputs must not alias inputs");
   if (int rc = check_theta(h)) return rc;
+  if (probe_p && (h->dim != 2 || h->probe[2] * h->probe[3] <= 0))
+    return set_err(h, JB_ERR_ARG, "probe pressures need a 2D handle with jb_set_probe");
+  if (rec && (!rec_slots || !chemistry)) return set_err(h, JB_ERR_ARG, "a record needs rec_slots");
   cudaStream_t st = (cudaStream_t)stream;
   const jb::Ops& o = *h->ops;
   const int d = h->dim;
   const bool use_cfl = cfl > 0.0;
   const jb_mech_params& m = h->mech;
   const jb_grid& g = h->grid;
+  const size_t nU = (size_t)g.nv * g.ncell, nA = 2 * (size_t)g.ncell;
+  const long long RS = rec ? rec_stride(h) : 0;
+  if (rec) {
+    JB_TRY(cudaMemcpyAsync(rec, U, sizeof(double) * nU, cudaMemcpyDeviceToDevice, st), "record U0");
+    JB_TRY(cudaMemcpyAsync(rec + nU, aux, sizeof(double) * nA, cudaMemcpyDeviceToDevice, st), "record aux0");
+  }
   JB_TIMED(JB_KCAT_OTHER, o.slots_reset(h->slots, st), "slots_reset");
   // alpha (and CFL minimum) of the initial state, ghost strips for stage 1
   JB_TIMED(JB_KCAT_SELECT, o.select(d, false, true, use_cfl, m, g, U, aux, nullptr, nullptr, h->strips, h->slots, -1, 3,
                   st),
          "prep");
   for (int s = 0; s < nsteps; ++s) {
-    const double* Un = s == 0 ? U : U_out;
-    const double* an = s == 0 ? aux : aux_out;
+    double* r = rec ? rec + s * RS : nullptr;
+    const double* Un = r ? r : (s == 0 ? U : U_out);
+    const double* an = r ? r + nU : (s == 0 ? aux : aux_out);
+    double* W1 = r ? r + (nU + nA) : h->W[0];
+    double* A1 = r ? W1 + nU : h->auxw[0];
+    double* W2 = r ? A1 + nA : h->W[1];
+    double* A2 = r ? W2 + nU : h->auxw[1];
+    double* W3 = r ? A2 + nA : h->W[0];
+    double* A3 = r ? W3 + nU : h->auxw[0];
+    double* Uo = r ? r + RS : U_out;
+    double* Ao = r ? r + RS + nU : aux_out;
     JB_TIMED(JB_KCAT_OTHER, o.step_begin(h->slots, use_cfl ? cfl : 0.0, dt_fixed, dt_hist, s, st), "step_begin");
     // stage 1: U1 = U + L(U)
-    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 1, m, g, Un, an, Un, h->W[0], h->cand, h->strips, h->slots, 0, 0, 0.0, st), "stage1");
-    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, h->W[0], nullptr, h->cand, h->auxw[0], h->strips,
+    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 1, m, g, Un, an, Un, W1, h->cand, h->strips, h->slots, 0, 0, 0.0, st), "stage1");
+    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W1, nullptr, h->cand, A1, h->strips,
                     h->slots, 0, 1, st),
            "select1");
     // stage 2: U2 = 3/4 U + 1/4 (U1 + L(U1))
-    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 2, m, g, h->W[0], h->auxw[0], Un, h->W[1], h->cand, h->strips, h->slots, 1, 1,
+    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 2, m, g, W1, A1, Un, W2, h->cand, h->strips, h->slots, 1, 1,
                   0.0, st),
            "stage2");
-    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, h->W[1], nullptr, h->cand, h->auxw[1], h->strips,
+    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W2, nullptr, h->cand, A2, h->strips,
                     h->slots, 1, 2, st),
            "select2");
     // stage 3: U3 = 1/3 U + 2/3 (U2 + L(U2))
-    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 3, m, g, h->W[1], h->auxw[1], Un, h->W[0], h->cand, h->strips, h->slots, 2, 2,
+    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 3, m, g, W2, A2, Un, W3, h->cand, h->strips, h->slots, 2, 2,
                   0.0, st),
            "stage3");
     if (!chemistry) {
       // advance_flux only (TVD_RK3.py:5-12): U3, aux3 are the result
       const size_t bytes = sizeof(double) * g.nv * (size_t)g.ncell;
-      JB_TRY(cudaMemcpyAsync(U_out, h->W[0], bytes, cudaMemcpyDeviceToDevice, st), "copy U3");
+      JB_TRY(cudaMemcpyAsync(U_out, W3, bytes, cudaMemcpyDeviceToDevice, st), "copy U3");
       JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, U_out, nullptr, h->cand, aux_out,
                                         h->strips, h->slots, 2, 3, st),
                "select3");
       continue;
     }
-    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, false, false, m, g, h->W[0], nullptr, h->cand, h->auxw[0], h->strips,
+    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, false, false, m, g, W3, nullptr, h->cand, A3, h->strips,
                     h->slots, 2, 0, st),
            "select3");
     // chemistry and the final temperature solve
-    JB_TIMED(JB_KCAT_CHEM, o.chem(d, false, m, g, h->W[0], h->auxw[0], U_out, h->cand, h->slots, 3, 0.0, st), "chem");
-    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, U_out, nullptr, h->cand, aux_out, h->strips,
+    JB_TIMED(JB_KCAT_CHEM, o.chem(d, false, m, g, W3, A3, Uo, h->cand, h->slots, 3, 0.0, st), "chem");
+    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, Uo, nullptr, h->cand, Ao, h->strips,
                     h->slots, 3, 3, st),
            "select4");
+    if (rec)
+      JB_TRY(cudaMemcpyAsync(rec_slots + s * (sizeof(jb_slots) / sizeof(double)), h->slots, sizeof(jb_slots),
+                             cudaMemcpyDeviceToDevice, st),
+             "record slots");
+    if (probe_p)
+      JB_TRY(jb::adj::probe_mean(m, g, Uo, Ao, h->probe[0], h->probe[1], h->probe[2], h->probe[3], probe_p + s, st),
+             "probe");
+  }
+  if (rec) {
+    JB_TRY(cudaMemcpyAsync(U_out, rec + nsteps * RS, sizeof(double) * nU, cudaMemcpyDeviceToDevice, st), "U_out");
+    JB_TRY(cudaMemcpyAsync(aux_out, rec + nsteps * RS + nU, sizeof(double) * nA, cudaMemcpyDeviceToDevice, st),
+           "aux_out");
   }
   return JB_OK;
 }
@@ -386,6 +438,153 @@ int jb_set_spacing(jb_handle* h, double dx, double dy) {
     h->grid.dy = dy;
     h->grid.idy = 1.0 / dy;
   }
+  return JB_OK;
+}
+
+int jb_set_probe(jb_handle* h, int x0, int y0, int wx, int wy) {
+  if (!h) return JB_ERR_ARG;
+  if (h->dim != 2 || x0 < 0 || y0 < 0 || wx < 0 || wy < 0 || x0 + wx > h->grid.nx || y0 + wy > h->grid.ny ||
+      wx * wy > 1024)
+    return set_err(h, JB_ERR_ARG, "probe outside the grid (or over 1024 cells)");
+  h->probe[0] = x0;
+  h->probe[1] = y0;
+  h->probe[2] = wx;
+  h->probe[3] = wy;
+  return JB_OK;
+}
+
+int jb_set_log_A_offset(jb_handle* h, const double* offset) {
+  if (!h) return JB_ERR_ARG;
+  for (int i = 0; i < h->mech.nreac; ++i) h->mech.A[i] = h->base_A[i] * (offset ? std::exp(offset[i]) : 1.0);
+  jb::derive_mech(h->mech);
+  return JB_OK;
+}
+
+long long jb_record_doubles(const jb_handle* h) { return h ? rec_stride(h) : 0; }
+
+int jb_advance_ex(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
+                  double dt_fixed, double cfl, int nsteps, double* dt_hist, double* probe_p, double* rec,
+                  double* rec_slots, void* stream) {
+  return advance_impl(h, U, aux, U_out, aux_out, dt_fixed, cfl, nsteps, dt_hist, stream, true, probe_p, rec,
+                      rec_slots);
+}
+
+// Multiplicity of every cell in the reference's padded array (periodic pad
+// of both axes, then the four sides; corners keep the periodic wrap): how
+// many padded entries copy it.  Only copy-type sides reach here.
+static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mult) {
+  const int nx = g.nx, ny = g.ny;
+  mult.assign((size_t)nx * ny, 0);
+  auto per = [](int c, int n) { return c < 0 ? n - 1 + c : (c >= n ? c - n + 1 : c); };
+  auto side = [](int c, int n, int kind, bool& ok) {
+    ok = true;
+    const bool lo = c < 0;
+    switch (kind) {
+      case JB_BC_PERIODIC: return lo ? n - 1 + c : c - n + 1;
+      case JB_BC_SLIP_WALL: return lo ? 0 : n - 1;
+      case JB_BC_ZERO_GRADIENT:
+      case JB_BC_NO_SLIP_WALL: return lo ? -1 - c : 2 * n - 1 - c;
+      default: ok = false; return 0;
+    }
+  };
+  for (int x = -3; x < nx + 3; ++x)
+    for (int y = -3; y < ny + 3; ++y) {
+      const bool xin = x >= 0 && x < nx, yin = y >= 0 && y < ny;
+      int sx = x, sy = y;
+      bool ok = true;
+      if (!xin && !yin) {
+        sx = per(x, nx);
+        sy = per(y, ny);
+      } else if (!xin) {
+        sx = side(x, nx, g.bc[x < 0 ? 0 : 1], ok);
+      } else if (!yin) {
+        sy = side(y, ny, g.bc[y < 0 ? 2 : 3], ok);
+      }
+      if (ok && sx >= 0 && sx < nx && sy >= 0 && sy < ny) mult[(size_t)sx * ny + sy] += 1;
+    }
+}
+
+static int adj_workspace(jb_handle* h) {
+  if (h->adj_ws) return JB_OK;
+  if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
+  for (int s = 0; s < 4; ++s)
+    if (h->grid.bc[s] == JB_BC_PRESSURE_OUTLET || h->grid.bc[s] == JB_BC_RDC_INJECTOR)
+      return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint supports periodic, slip, no-slip and zero-gradient sides");
+  const jb_grid& g = h->grid;
+  const size_t nc = (size_t)g.ncell, nU = (size_t)g.nv * nc;
+  const size_t L = (size_t)(g.nx > g.ny ? g.nx : g.ny);
+  const size_t n = 2 * nU + 2 * nc + 12 * 13 * L + 8;
+  JB_TRY(cudaMalloc(&h->adj_ws, sizeof(double) * n), "adjoint workspace");
+  JB_TRY(cudaMemset(h->adj_ws, 0, sizeof(double) * n), "adjoint workspace clear");
+  h->adj_B1 = h->adj_ws;
+  h->adj_B2 = h->adj_B1 + nU;
+  h->adj_A2 = h->adj_B2 + nU;
+  h->adj_ghost = h->adj_A2 + 2 * nc;
+  h->adj_red = h->adj_ghost + 12 * 13 * L;
+  std::vector<unsigned char> mult;
+  padded_multiplicity(g, mult);
+  JB_TRY(cudaMalloc(&h->adj_mult, nc), "multiplicity");
+  JB_TRY(cudaMemcpy(h->adj_mult, mult.data(), nc, cudaMemcpyHostToDevice), "multiplicity copy");
+  return JB_OK;
+}
+
+int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, double cfl, double* Ubar,
+                    double* Abar, const double* dt_bar, const double* pp_bar, double* lnA_bar, void* stream) {
+  if (!h || !rec || !rec_slots || !Ubar || !Abar || !lnA_bar) return set_err(h, JB_ERR_ARG, "null pointer");
+  if (pp_bar && h->probe[2] * h->probe[3] <= 0) return set_err(h, JB_ERR_ARG, "probe adjoint needs jb_set_probe");
+  if (int rc = adj_workspace(h)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const jb_mech_params& m = h->mech;
+  const jb_grid& g = h->grid;
+  const size_t nc = (size_t)g.ncell, nU = (size_t)g.nv * nc, nA = 2 * nc;
+  const double* Un = rec;
+  const double* An = Un + nU;
+  const double* W1 = An + nA;
+  const double* A1 = W1 + nU;
+  const double* W2 = A1 + nA;
+  const double* A2 = W2 + nU;
+  const double* W3 = A2 + nA;
+  const double* A3 = W3 + nU;
+  const double* U4 = rec + rec_stride(h);
+  const double* A4 = U4 + nU;
+  const double* slots = rec_slots;
+  const double* slot_dt = slots + offsetof(jb_slots, dt) / sizeof(double);
+  double* red = h->adj_red;
+  double *B1 = h->adj_B1, *B2 = h->adj_B2, *Ab2 = h->adj_A2, *gh = h->adj_ghost;
+  const double c_cfl = cfl > 0.0 ? cfl : 0.0;
+  JB_TRY(jb::adj::adj_begin(red, dt_bar, st), "adjoint begin");
+  // loss term of this step and the final temperature solve
+  JB_TRY(jb::adj::probe_seed(m, g, U4, A4, pp_bar, h->probe[0], h->probe[1], h->probe[2], h->probe[3], Ubar, Abar,
+                             st),
+         "probe seed");
+  JB_TRY(jb::adj::upd_vjp(m, g, U4, A4, Ubar, Abar, st), "update_aux 4");
+  // chemistry (and update_aux of U3): B1 = Ubar3
+  JB_TRY(jb::adj::chem_vjp(m, g, W3, A3, Ubar, B1, slot_dt, red + 2, lnA_bar, st), "chemistry");
+  JB_TRY(cudaMemsetAsync(Ubar, 0, sizeof(double) * nU, st), "Ubar_n clear");  // Ubar becomes Ubar_n
+  // stage 3: U3 = 1/3 U + 2/3 (U2 + dt L(U2, aux2))
+  JB_TRY(cudaMemsetAsync(B2, 0, sizeof(double) * nU, st), "Ubar2 clear");
+  JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
+  JB_TRY(jb::adj::flux_vjp(m, g, W2, A2, B1, 2.0 / 3.0, slots, 2, B2, Ab2, Ubar, 1.0 / 3.0, gh, red, st), "stage 3");
+  JB_TRY(jb::adj::speed_vjp(m, g, W2, A2, h->adj_mult, slots, 2, 0.0, red, B2, Ab2, st), "alpha 3");
+  JB_TRY(jb::adj::upd_vjp(m, g, W2, A2, B2, Ab2, st), "update_aux 2");
+  // stage 2: U2 = 3/4 U + 1/4 (U1 + dt L(U1, aux1)); B1 = Ubar1
+  JB_TRY(cudaMemsetAsync(B1, 0, sizeof(double) * nU, st), "Ubar1 clear");
+  JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
+  JB_TRY(jb::adj::flux_vjp(m, g, W1, A1, B2, 0.25, slots, 1, B1, Ab2, Ubar, 0.75, gh, red, st), "stage 2");
+  JB_TRY(jb::adj::speed_vjp(m, g, W1, A1, h->adj_mult, slots, 1, 0.0, red, B1, Ab2, st), "alpha 2");
+  JB_TRY(jb::adj::upd_vjp(m, g, W1, A1, B1, Ab2, st), "update_aux 1");
+  // stage 1: U1 = U + dt L(U, aux); then alpha 1 and the CFL time step
+  JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
+  JB_TRY(jb::adj::flux_vjp(m, g, Un, An, B1, 1.0, slots, 0, Ubar, Abar, nullptr, 0.0, gh, red, st), "stage 1");
+  JB_TRY(jb::adj::speed_vjp(m, g, Un, An, h->adj_mult, slots, 0, c_cfl, red, Ubar, Abar, st), "alpha 1 and dt");
+  return JB_OK;
+}
+
+int jb_state_from_PTY_vjp(jb_handle* h, const double* P, const double* T, const double* Y, const double* Ubar,
+                          const double* Abar, double* Tbar, void* stream) {
+  if (!h || !P || !T || !Y || !Ubar || !Abar || !Tbar) return set_err(h, JB_ERR_ARG, "null pointer");
+  if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
+  JB_TRY(jb::adj::init_vjp(h->mech, h->grid.ncell, P, T, Y, Ubar, Abar, Tbar, (cudaStream_t)stream), "init vjp");
   return JB_OK;
 }
 
