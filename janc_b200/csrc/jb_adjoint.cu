@@ -186,8 +186,9 @@ __global__ void k_upd_vjp(MP m, Grid g, const double* __restrict__ U, const doub
 // ---------------------------------------------------------------------------
 // chemistry VJP (reaction_model.py:91-193)
 // ---------------------------------------------------------------------------
-// x = A^-1 b for an 8x8 A (destroyed), partial pivoting with selects
-__device__ __forceinline__ void lu_solve8(double (&A)[NR][NR], double (&b)[NR], double (&x)[NR]) {
+// PA = LU of an 8x8 A in place (multipliers below the diagonal), partial
+// pivoting with selects; piv[c] is the row exchanged with row c at step c.
+__device__ __forceinline__ void lu8(double (&A)[NR][NR], int (&piv)[NR]) {
 #pragma unroll
   for (int c = 0; c < NR; ++c) {
     int p = c;
@@ -198,6 +199,7 @@ __device__ __forceinline__ void lu_solve8(double (&A)[NR][NR], double (&b)[NR], 
         const double v = fabs(A[r][c]);
         if (v > best) { best = v; p = r; }
       }
+    piv[c] = p;
 #pragma unroll
     for (int r = 0; r < NR; ++r)
       if (r > c) {
@@ -208,37 +210,94 @@ __device__ __forceinline__ void lu_solve8(double (&A)[NR][NR], double (&b)[NR], 
           A[c][j] = sw ? x1 : x0;
           A[r][j] = sw ? x0 : x1;
         }
-        const double y0 = b[c], y1 = b[r];
-        b[c] = sw ? y1 : y0;
-        b[r] = sw ? y0 : y1;
       }
+    const double ip = 1.0 / A[c][c];
 #pragma unroll
     for (int r = 0; r < NR; ++r)
       if (r > c) {
-        const double l = A[r][c] / A[c][c];
+        const double l = A[r][c] * ip;
+        A[r][c] = l;
 #pragma unroll
         for (int j = 0; j < NR; ++j)
           if (j > c) A[r][j] = A[r][j] - l * A[c][j];
-        b[r] = b[r] - l * b[c];
       }
-  }
-#pragma unroll
-  for (int i = 0; i < NR; ++i) {
-    const int r = NR - 1 - i;
-    double s = b[r];
-#pragma unroll
-    for (int j = 0; j < NR; ++j)
-      if (j > r) s = s - A[r][j] * x[j];
-    x[r] = s / A[r][r];
   }
 }
 
+// x = A^-1 b from lu8's factors
+__device__ __forceinline__ void lu8_solve(const double (&A)[NR][NR], const int (&piv)[NR], const double* b,
+                                          double* x) {
+  double y[NR];
+#pragma unroll
+  for (int i = 0; i < NR; ++i) y[i] = b[i];
+#pragma unroll
+  for (int c = 0; c < NR; ++c)
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      if (r > c) {
+        const bool sw = piv[c] == r;
+        const double y0 = y[c], y1 = y[r];
+        y[c] = sw ? y1 : y0;
+        y[r] = sw ? y0 : y1;
+      }
+#pragma unroll
+  for (int i = 0; i < NR; ++i)
+#pragma unroll
+    for (int j = 0; j < NR; ++j)
+      if (j < i) y[i] = y[i] - A[i][j] * y[j];
+#pragma unroll
+  for (int ii = 0; ii < NR; ++ii) {
+    const int i = NR - 1 - ii;
+    double t = y[i];
+#pragma unroll
+    for (int j = 0; j < NR; ++j)
+      if (j > i) t = t - A[i][j] * x[j];
+    x[i] = t / A[i][i];
+  }
+}
+
+// y = A^-T c from lu8's factors (A^T = U^T L^T P)
+__device__ __forceinline__ void lu8_solve_t(const double (&A)[NR][NR], const int (&piv)[NR], const double* c,
+                                            double* y) {
+  double z[NR];
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    double t = c[i];
+#pragma unroll
+    for (int j = 0; j < NR; ++j)
+      if (j < i) t = t - A[j][i] * z[j];
+    z[i] = t / A[i][i];
+  }
+#pragma unroll
+  for (int ii = 0; ii < NR; ++ii) {
+    const int i = NR - 1 - ii;
+#pragma unroll
+    for (int j = 0; j < NR; ++j)
+      if (j > i) z[i] = z[i] - A[j][i] * z[j];
+  }
+#pragma unroll
+  for (int cc = 0; cc < NR; ++cc) {
+    const int k = NR - 1 - cc;
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      if (r > k) {
+        const bool sw = piv[k] == r;
+        const double z0 = z[k], z1 = z[r];
+        z[k] = sw ? z1 : z0;
+        z[r] = sw ? z0 : z1;
+      }
+  }
+#pragma unroll
+  for (int i = 0; i < NR; ++i) y[i] = z[i];
+}
+
 constexpr int CHEM_ADJ_NT = 128;
-constexpr int CHEM_ADJ_SH = 4 * NREAC;  // kf0, kf, kb, M per reaction
+constexpr int CHEM_ADJ_SH = 3 * NREAC;  // kf, kb, M per reaction
 
 // Per cell: Ub3 = Ub4 + (dS/dU3)^T Ub4, then update_aux(U3)'s VJP with the
 // chemistry's temperature adjoint; dt and ln A adjoints are reduced into
-// dtb and lnAb.
+// dtb and lnAb.  Rates in log space: kf = exp(ln A + B ln T - Ea/T +
+// sum vf ln X), kb = exp(ln kf0 - sum dv g - vsum ln(pref/T) + sum vb ln X).
 __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
     k_chem_vjp(MP m, Grid g, const double* __restrict__ U3, const double* __restrict__ A3, const double* Ub4,
                double* Ub3, const double* __restrict__ slot_dt, double* dtb, double* lnAb) {
@@ -249,26 +308,27 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
   double* sh = shk + threadIdx.x;
   const double dt = *slot_dt;
   double dtb_loc = 0.0;
-  double lnAb_loc[NREAC];
-#pragma unroll
-  for (int i = 0; i < NREAC; ++i) lnAb_loc[i] = 0.0;
+  double* sA = shk + CHEM_ADJ_SH * NT + threadIdx.x;  // ln A adjoint per reaction, this thread's column
+#pragma unroll 1
+  for (int i = 0; i < NREAC; ++i) sA[i * NT] = 0.0;
   if (c < nc) {
     double q[12];
 #pragma unroll
     for (int f = 0; f < 12; ++f) q[f] = U3[f * nc + c];
     const double T = A3[nc + c];
     const double rho = q[0], ri = 1.0 / rho;
-    double Y8[NR], Yf[NS], X[NS], Xc[NR], lnXc[NR], gg[NR], dg[NR];
+    double Y8[NR], Yf[NS], X[NS], Xc[NR], lnXc[NR], iXc[NR], gg[NR], dg[NR];
     cell_Y(q, ri, Y8, Yf);
 #pragma unroll
-    for (int j = 0; j < NS; ++j) X[j] = rho * Yf[j] / m.M[j];
+    for (int j = 0; j < NS; ++j) X[j] = rho * Yf[j] * m.invM[j];
 #pragma unroll
     for (int n = 0; n < NR; ++n) {
       Xc[n] = X[n] < 1e-50 ? 1e-50 : X[n];
       lnXc[n] = log(Xc[n]);
+      iXc[n] = 1.0 / Xc[n];
     }
     const double lT = log(T), iT = 1.0 / T;
-    const double lT0T = log(m.T0 * T);
+    const double lT0T = lT + m.lnT0;
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
       const bool lo = T < m.Tcr[k];
@@ -279,7 +339,6 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
       gg[k] = s + lg * lT0T - h * iT;
       dg[k] = ds + lg * iT - dh * iT + h * iT * iT;
     }
-    // forward rates, omega and the Jacobian as the reference forms them
     double w[NR], J[NR][NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
@@ -289,7 +348,7 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
     }
 #pragma unroll 1
     for (int i = 0; i < NREAC; ++i) {
-      const double kf0 = m.A[i] * pow(T, m.B[i]) * exp(-m.EaR[i] * iT);
+      const double lkf0 = m.lnA[i] + m.B[i] * lT - m.EaR[i] * iT;
       double Ms = 1.0;
       if (m.is_tb[i] != 0.0) {
         Ms = 0.0;
@@ -303,36 +362,35 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
         sb += m.vb[i][n] * lnXc[n];
         sg += m.dv[i][n] * gg[n];
       }
-      const double kf = kf0 * exp(sf);
-      const double kb = kf0 / (exp(sg) * exp(m.vsum[i] * (m.lnpref - lT))) * exp(sb);
-      sh[(4 * i + 0) * NT] = kf0;
-      sh[(4 * i + 1) * NT] = kf;
-      sh[(4 * i + 2) * NT] = kb;
-      sh[(4 * i + 3) * NT] = Ms;
+      const double kf = exp(lkf0 + sf);
+      const double kb = exp(lkf0 - sg - m.vsum[i] * (m.lnpref - lT) + sb);
+      sh[(3 * i + 0) * NT] = kf;
+      sh[(3 * i + 1) * NT] = kb;
+      sh[(3 * i + 2) * NT] = Ms;
+      const double net = kf - kb;
+      double tn[NR];
+#pragma unroll
+      for (int n = 0; n < NR; ++n)
+        tn[n] = net * m.tbinvM[i][n] + Ms * (m.vf[i][n] * kf - m.vb[i][n] * kb) * m.invM[n] * iXc[n];
 #pragma unroll
       for (int k = 0; k < NR; ++k) {
         const double dvk = m.dv[i][k];
         if (dvk == 0.0) continue;
-        w[k] += m.M[k] * dvk * Ms * (kf - kb);
+        const double mk = m.M[k] * dvk;
+        w[k] += mk * Ms * net;
 #pragma unroll
-        for (int n = 0; n < NR; ++n)
-          J[k][n] += m.M[k] * dvk * ((kf - kb) * m.tb[i][n] / m.M[n] +
-                                    Ms * (m.vf[i][n] * kf - m.vb[i][n] * kb) / (m.M[n] * Xc[n]));
+        for (int n = 0; n < NR; ++n) J[k][n] += mk * tn[n];
       }
     }
-    double Am[NR][NR], At[NR][NR], x[NR], bw[NR];
     const double idt = 1.0 / dt;
 #pragma unroll
-    for (int k = 0; k < NR; ++k) {
-      bw[k] = w[k];
+    for (int k = 0; k < NR; ++k)
 #pragma unroll
-      for (int n = 0; n < NR; ++n) {
-        const double a = (k == n ? idt : 0.0) - J[k][n];
-        Am[k][n] = a;
-        At[n][k] = a;
-      }
-    }
-    lu_solve8(Am, bw, x);
+      for (int n = 0; n < NR; ++n) J[k][n] = (k == n ? idt : 0.0) - J[k][n];  // J now holds A
+    int piv[NR];
+    lu8(J, piv);
+    double x[NR];
+    lu8_solve(J, piv, w, x);
     // S = rho clip(x / rho, -Y, 1 - Y)
     double rb = 0.0, Y8b[NR], xb[NR];
 #pragma unroll
@@ -353,7 +411,7 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
       rb -= dYb * dY * ri;
     }
     double bb[NR];
-    lu_solve8(At, xb, bb);  // bbar = A^-T xbar
+    lu8_solve_t(J, piv, xb, bb);  // bbar = A^-T xbar
 #pragma unroll
     for (int k = 0; k < NR; ++k) dtb_loc += bb[k] * x[k] * idt * idt;
     double Xb[NS], Xcb[NR], gb[NR], Tb = 0.0;
@@ -363,25 +421,23 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
     for (int n = 0; n < NR; ++n) { Xcb[n] = 0.0; gb[n] = 0.0; }
     double xw[NR];
 #pragma unroll
-    for (int n = 0; n < NR; ++n) xw[n] = x[n] / m.M[n];
+    for (int n = 0; n < NR; ++n) xw[n] = x[n] * m.invM[n];
 #pragma unroll 1
     for (int i = 0; i < NREAC; ++i) {
       double beta = 0.0;
 #pragma unroll
       for (int k = 0; k < NR; ++k) beta += bb[k] * m.M[k] * m.dv[i][k];
       if (beta == 0.0) continue;
-      const double kf0 = sh[(4 * i + 0) * NT], kf = sh[(4 * i + 1) * NT];
-      const double kb = sh[(4 * i + 2) * NT], Ms = sh[(4 * i + 3) * NT];
+      const double kf = sh[(3 * i + 0) * NT], kb = sh[(3 * i + 1) * NT], Ms = sh[(3 * i + 2) * NT];
       double sF = 0.0, sB = 0.0, sMb = kf - kb;
 #pragma unroll
       for (int n = 0; n < NR; ++n) {
         const double vfn = m.vf[i][n], vbn = m.vb[i][n], tbn = m.tb[i][n];
-        const double iX = 1.0 / Xc[n];
-        sF += xw[n] * (tbn + Ms * vfn * iX);
-        sB += xw[n] * (tbn + Ms * vbn * iX);
+        sF += xw[n] * (tbn + Ms * vfn * iXc[n]);
+        sB += xw[n] * (tbn + Ms * vbn * iXc[n]);
         const double d = vfn * kf - vbn * kb;
-        sMb += xw[n] * d * iX;
-        Xcb[n] -= beta * Ms * xw[n] * d * iX * iX;
+        sMb += xw[n] * d * iXc[n];
+        Xcb[n] -= beta * Ms * xw[n] * d * iXc[n] * iXc[n];
       }
       const double kfb = beta * (Ms + sF);
       const double kbb = -beta * (Ms + sB);
@@ -390,16 +446,15 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
 #pragma unroll
         for (int j = 0; j < NS; ++j) Xb[j] += Mb * m.tb[i][j];
       }
+      const double fkf = kfb * kf, fkb = kbb * kb;
 #pragma unroll
       for (int n = 0; n < NR; ++n) {
-        const double iX = 1.0 / Xc[n];
-        Xcb[n] += (kfb * kf * m.vf[i][n] + kbb * kb * m.vb[i][n]) * iX;
-        gb[n] -= kbb * kb * m.dv[i][n];
+        Xcb[n] += (fkf * m.vf[i][n] + fkb * m.vb[i][n]) * iXc[n];
+        gb[n] -= fkb * m.dv[i][n];
       }
-      const double kf0b = (kfb * kf + kbb * kb) / kf0;
-      Tb += kbb * kb * m.vsum[i] * iT;
-      Tb += kf0b * kf0 * (m.B[i] * iT + m.EaR[i] * iT * iT);
-      lnAb_loc[i] += kf0b * kf0;
+      const double a0 = fkf + fkb;  // adjoint of ln kf0 (and of ln A_i)
+      Tb += fkb * m.vsum[i] * iT + a0 * (m.B[i] * iT + m.EaR[i] * iT * iT);
+      sA[i * NT] += a0;
     }
 #pragma unroll
     for (int n = 0; n < NR; ++n) {
@@ -409,7 +464,7 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
     double Yfb[NS];
 #pragma unroll
     for (int j = 0; j < NS; ++j) {
-      const double ryb = Xb[j] / m.M[j];
+      const double ryb = Xb[j] * m.invM[j];
       rb += ryb * Yf[j];
       Yfb[j] = rho * ryb;
     }
@@ -429,7 +484,7 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
   }
   block_add(dtb_loc, dtb);
 #pragma unroll 1
-  for (int i = 0; i < NREAC; ++i) block_add(lnAb_loc[i], lnAb + i);
+  for (int i = 0; i < NREAC; ++i) block_add(sA[i * NT], lnAb + i);
 }
 
 // ---------------------------------------------------------------------------
@@ -445,16 +500,19 @@ __device__ __forceinline__ double weno_d(double v0, double v1, double v2, double
   const double b2 = 0.25 * d2 * d2 + 13.0 / 12.0 * e2 * e2;
   const double b3 = 0.25 * d3 * d3 + 13.0 / 12.0 * e3 * e3;
   const double s1 = 1e-6 + b1, s2 = 1e-6 + b2, s3 = 1e-6 + b3;
-  const double a1 = 0.1 / (s1 * s1), a2 = 0.6 / (s2 * s2), a3 = 0.3 / (s3 * s3);
+  // one division for the three reciprocals (s_k lies in [1e-6, ~1e20])
+  const double s12 = s1 * s2, r = 1.0 / (s12 * s3);
+  const double i1 = s2 * s3 * r, i2 = s1 * s3 * r, i3 = s12 * r;
+  const double a1 = 0.1 * i1 * i1, a2 = 0.6 * i2 * i2, a3 = 0.3 * i3 * i3;
   const double iS = 1.0 / (a1 + a2 + a3);
   const double w1 = a1 * iS, w2 = a2 * iS, w3 = a3 * iS;
   const double q1 = 1.0 / 3.0 * v0 - 7.0 / 6.0 * v1 + 11.0 / 6.0 * v2;
   const double q2 = -1.0 / 6.0 * v1 + 5.0 / 6.0 * v2 + 1.0 / 3.0 * v3;
   const double q3 = 1.0 / 3.0 * v2 + 5.0 / 6.0 * v3 - 1.0 / 6.0 * v4;
   const double f = w1 * q1 + w2 * q2 + w3 * q3;
-  const double g1 = -2.0 * w1 * (q1 - f) / s1;
-  const double g2 = -2.0 * w2 * (q2 - f) / s2;
-  const double g3 = -2.0 * w3 * (q3 - f) / s3;
+  const double g1 = -2.0 * w1 * (q1 - f) * i1;
+  const double g2 = -2.0 * w2 * (q2 - f) * i2;
+  const double g3 = -2.0 * w3 * (q3 - f) * i3;
   dv[0] = w1 * (1.0 / 3.0) + g1 * (0.5 * d1 + 13.0 / 6.0 * e1);
   dv[1] = w1 * (-7.0 / 6.0) + w2 * (-1.0 / 6.0) + g1 * (-2.0 * d1 - 13.0 / 3.0 * e1) + g2 * (0.5 * d2 + 13.0 / 6.0 * e2);
   dv[2] = w1 * (11.0 / 6.0) + w2 * (5.0 / 6.0) + w3 * (1.0 / 3.0) + g1 * (1.5 * d1 + 13.0 / 6.0 * e1) +
@@ -471,22 +529,35 @@ __device__ __forceinline__ double weno_d(double v0, double v1, double v2, double
 // x TA cells across it (interior only).  threadIdx.x runs along y, so the
 // y direction is the coalesced one for both kernels.
 constexpr int TO = 16, TA = 16, NE = TO + 10, NF = TO + 5;
+constexpr int NEP = NE + 1, NFP = NF;  // odd strides (in doubles) of the across-major layout
+constexpr int EA = TA * NEP, FA = TA * NFP;  // doubles per extended-cell / face array
+
+template <int D>
+__device__ __forceinline__ int ie(int e, int c) { return D == 0 ? e * TA + c : c * NEP + e; }
+template <int D>
+__device__ __forceinline__ int iff(int f, int c) { return D == 0 ? f * TA + c : c * NFP + f; }
 
 template <int D>  // 0: x faces (F), 1: y faces (G)
-__global__ void __launch_bounds__(256) k_flux_vjp(MP m, Grid g, const double* __restrict__ Uk,
+__global__ void __launch_bounds__(256, 3) k_flux_vjp(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ Ak, const double* __restrict__ Uo_b,
                                                  double coef, const double* __restrict__ slots_rec, int stage,
                                                  double* Ub, double* Abk, double* Un_b, double un_coef,
                                                  double* ghost, double* red) {
+  // Shared arrays: per extended cell rho, u, v, p, the field, H+, H- and its
+  // source (cell index, flip bits); per face the 5 + 5 WENO partials times
+  // the face-flux adjoint and the face value.  The layout runs along the
+  // across index for x faces and along the direction for y faces, so a
+  // warp's accesses are unit-stride in both kernels.
   extern __shared__ __align__(16) double sm_flux[];
-  // rho, u, v, p; the field (ghost copies flipped); H+-; face partials and values
-  double(*sP)[NE][TA] = reinterpret_cast<double(*)[NE][TA]>(sm_flux);
-  double(*sQ)[TA] = reinterpret_cast<double(*)[TA]>(sm_flux + 4 * NE * TA);
-  double(*sHp)[TA] = sQ + NE;
-  double(*sHm)[TA] = sHp + NE;
-  double(*sPL)[NF][TA] = reinterpret_cast<double(*)[NF][TA]>(sm_flux + 7 * NE * TA);
-  double(*sPR)[NF][TA] = sPL + 5;
-  double(*sFv)[TA] = reinterpret_cast<double(*)[TA]>(sm_flux + 7 * NE * TA + 10 * NF * TA);
+  double* sP = sm_flux;          // [4][EA]
+  double* sQ = sP + 4 * EA;
+  double* sHp = sQ + EA;
+  double* sHm = sHp + EA;
+  double* sPL = sHm + EA;        // [5][FA]
+  double* sPR = sPL + 5 * FA;    // [5][FA]
+  double* sFv = sPR + 5 * FA;    // [FA]
+  long long* sSrc = reinterpret_cast<long long*>(sFv + FA);  // [EA], -1: outside the padded grid
+  int* sFlip = reinterpret_cast<int*>(sSrc + EA);            // [EA]
   const int nA = D == 0 ? g.nx : g.ny;
   const int nC = D == 0 ? g.ny : g.nx;
   const long long nc = g.ncell;
@@ -496,45 +567,49 @@ __global__ void __launch_bounds__(256) k_flux_vjp(MP m, Grid g, const double* __
   const int a0 = -3 + (int)blockIdx.x * TO;
   const int c0 = (int)blockIdx.y * TA;
   const double dA = D == 0 ? g.dx : g.dy;
-  // alpha and dt of the recorded step (jb_slots of that step)
   const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
   const double alpha = bitsd(D == 0 ? rs->ax[stage] : rs->ay[stage]);
   const double dt = rs->dt;
   const int dirf = D == 0 ? 1 : 2;  // normal momentum field
-  // primitives of the extended cells
+  // sources and primitives of the extended cells
   for (int i = tid; i < NE * TA; i += 256) {
     const int e = D == 0 ? i / TA : i % NE, cc = D == 0 ? i % TA : i / NE;
     const int a = a0 - 5 + e, cidx = c0 + cc;
     double q[12], T = 1.0;
-    bool ok = false;
+    long long src = -1;
+    int flip = 0;
     if (cidx < nC) {
       const int x = D == 0 ? a : cidx, y = D == 0 ? cidx : a;
       Src s = map_cell<2>(g, x, y);
       if (s.kind == 0) {
-        const long long src = (long long)s.xs * g.ny + s.ys;
-#pragma unroll
-        for (int f = 0; f < 12; ++f) {
-          const double v = Uk[f * nc + src];
-          q[f] = ((s.flip >> f) & 1) ? -v : v;
-        }
-        T = Ak[nc + src];
-        ok = true;
+        src = (long long)s.xs * g.ny + s.ys;
+        flip = s.flip;
       }
     }
-    if (!ok) {
+    if (src >= 0) {
+#pragma unroll
+      for (int f = 0; f < 12; ++f) {
+        const double v = Uk[f * nc + src];
+        q[f] = ((flip >> f) & 1) ? -v : v;
+      }
+      T = Ak[nc + src];
+    } else {
 #pragma unroll
       for (int f = 0; f < 12; ++f) q[f] = 1.0;
     }
     const double rho = q[0], ri = 1.0 / rho;
     double Y8[NR], Yf[NS];
     cell_Y(q, ri, Y8, Yf);
-    sP[0][e][cc] = rho;
-    sP[1][e][cc] = q[1] * ri;
-    sP[2][e][cc] = q[2] * ri;
-    sP[3][e][cc] = rho * get_R(m, Yf) * T;
+    const int k = ie<D>(e, cc);
+    sSrc[k] = src;
+    sFlip[k] = flip;
+    sP[k] = rho;
+    sP[EA + k] = q[1] * ri;
+    sP[2 * EA + k] = q[2] * ri;
+    sP[3 * EA + k] = rho * get_R(m, Yf) * T;
   }
   __syncthreads();
-  const int ao = a0 + tA;        // padded along coordinate of the owned cell
+  const int ao = a0 + tA;  // padded along coordinate of the owned cell
   const int co = c0 + tC;
   const bool owned = co < nC && ao < nA + 3;
   const bool interior = owned && ao >= 0 && ao < nA;
@@ -546,17 +621,14 @@ __global__ void __launch_bounds__(256) k_flux_vjp(MP m, Grid g, const double* __
     // H+- of the field on the extended cells
     for (int i = tid; i < NE * TA; i += 256) {
       const int e = D == 0 ? i / TA : i % NE, cc = D == 0 ? i % TA : i / NE;
-      const int a = a0 - 5 + e, cidx = c0 + cc;
+      const int k = ie<D>(e, cc);
+      const long long src = sSrc[k];
       double qf = 1.0;
-      if (cidx < nC) {
-        const int x = D == 0 ? a : cidx, y = D == 0 ? cidx : a;
-        Src s = map_cell<2>(g, x, y);
-        if (s.kind == 0) {
-          const double v = Uk[f * nc + (long long)s.xs * g.ny + s.ys];
-          qf = ((s.flip >> f) & 1) ? -v : v;
-        }
+      if (src >= 0) {
+        const double v = Uk[f * nc + src];
+        qf = ((sFlip[k] >> f) & 1) ? -v : v;
       }
-      const double rho = sP[0][e][cc], u = sP[1][e][cc], v = sP[2][e][cc], p = sP[3][e][cc];
+      const double rho = sP[k], u = sP[EA + k], v = sP[2 * EA + k], p = sP[3 * EA + k];
       const double un = D == 0 ? u : v;
       double F;
       if (f == 0) F = rho * un;
@@ -564,9 +636,9 @@ __global__ void __launch_bounds__(256) k_flux_vjp(MP m, Grid g, const double* __
       else if (f == 3 - dirf) F = rho * u * v;
       else if (f == 3) F = un * (qf + p);
       else F = rho * un * (qf / rho);
-      sQ[e][cc] = qf;
-      sHp[e][cc] = 0.5 * (F + alpha * qf);
-      sHm[e][cc] = 0.5 * (F - alpha * qf);
+      sQ[k] = qf;
+      sHp[k] = 0.5 * (F + alpha * qf);
+      sHm[k] = 0.5 * (F - alpha * qf);
     }
     __syncthreads();
     // faces: adjoint of the face flux and the WENO partials
@@ -588,14 +660,17 @@ __global__ void __launch_bounds__(256) k_flux_vjp(MP m, Grid g, const double* __
       // L_i = -(F_{i+1} - F_i) / d  ->  Fbar_f = (Lbar_f - Lbar_{f-1}) / d
       const double Fb_face = (Lp - Lm) / dA;
       double dl[5], dr[5];
-      const double vl = weno_d(sHp[fl][cc], sHp[fl + 1][cc], sHp[fl + 2][cc], sHp[fl + 3][cc], sHp[fl + 4][cc], dl);
+      const double vl = weno_d(sHp[ie<D>(fl, cc)], sHp[ie<D>(fl + 1, cc)], sHp[ie<D>(fl + 2, cc)],
+                               sHp[ie<D>(fl + 3, cc)], sHp[ie<D>(fl + 4, cc)], dl);
       // right-biased: the left form of the mirrored stencil (cells fa+2 .. fa-2)
-      const double vr = weno_d(sHm[fl + 5][cc], sHm[fl + 4][cc], sHm[fl + 3][cc], sHm[fl + 2][cc], sHm[fl + 1][cc], dr);
-      sFv[fl][cc] = vl + vr;
+      const double vr = weno_d(sHm[ie<D>(fl + 5, cc)], sHm[ie<D>(fl + 4, cc)], sHm[ie<D>(fl + 3, cc)],
+                               sHm[ie<D>(fl + 2, cc)], sHm[ie<D>(fl + 1, cc)], dr);
+      const int kf = iff<D>(fl, cc);
+      sFv[kf] = vl + vr;
 #pragma unroll
       for (int j = 0; j < 5; ++j) {
-        sPL[j][fl][cc] = Fb_face * dl[j];      // cell fa-3+j
-        sPR[j][fl][cc] = Fb_face * dr[4 - j];  // cell fa-2+j
+        sPL[j * FA + kf] = Fb_face * dl[j];      // cell fa-3+j
+        sPR[j * FA + kf] = Fb_face * dr[4 - j];  // cell fa-2+j
       }
     }
     __syncthreads();
@@ -603,15 +678,15 @@ __global__ void __launch_bounds__(256) k_flux_vjp(MP m, Grid g, const double* __
       const int o = tA;
       double hp = 0.0, hm = 0.0;
 #pragma unroll
-      for (int d = -1; d <= 3; ++d) hp += sPL[3 - d][o + d + 2][tC];
+      for (int d = -1; d <= 3; ++d) hp += sPL[(3 - d) * FA + iff<D>(o + d + 2, tC)];
 #pragma unroll
-      for (int d = -2; d <= 2; ++d) hm += sPR[2 - d][o + d + 2][tC];
-      const double qf = sQ[o + 5][tC];
+      for (int d = -2; d <= 2; ++d) hm += sPR[(2 - d) * FA + iff<D>(o + d + 2, tC)];
+      const double qf = sQ[ie<D>(o + 5, tC)];
       Fb[f] = 0.5 * (hp + hm);
       Ua[f] = 0.5 * alpha * (hp - hm);
       ab += 0.5 * qf * (hp - hm);
       if (interior) {
-        const double Lphys = -(sFv[o + 3][tC] - sFv[o + 2][tC]) / dA;
+        const double Lphys = -(sFv[iff<D>(o + 3, tC)] - sFv[iff<D>(o + 2, tC)]) / dA;
         dtb += Lphys * coef * Uo_b[f * nc + cell];
       }
     }
@@ -619,22 +694,19 @@ __global__ void __launch_bounds__(256) k_flux_vjp(MP m, Grid g, const double* __
   }
   if (owned) {
     // flux function VJP of this padded cell
-    const int e = tA + 5;
-    const double rho = sP[0][e][tC], u = sP[1][e][tC], v = sP[2][e][tC], p = sP[3][e][tC];
+    const int k = ie<D>(tA + 5, tC);
+    const double rho = sP[k], u = sP[EA + k], v = sP[2 * EA + k], p = sP[3 * EA + k];
     const double un = D == 0 ? u : v, ut = D == 0 ? v : u;
-    // the padded cell's own state (flipped for ghosts) for rhoE and Y
-    double q[12], T = 1.0;
-    {
-      const int x = D == 0 ? ao : co, y = D == 0 ? co : ao;
-      Src s = map_cell<2>(g, x, y);  // copy-type sides only (checked on the host)
-      const long long src = s.kind == 0 ? (long long)s.xs * g.ny + s.ys : 0;
+    // the padded cell's own state (flipped for ghosts) for rho E and Y
+    const long long src = sSrc[k] >= 0 ? sSrc[k] : 0;
+    const int flip = sFlip[k];
+    double q[12];
 #pragma unroll
-      for (int f = 0; f < 12; ++f) {
-        const double vv = Uk[f * nc + src];
-        q[f] = ((s.flip >> f) & 1) ? -vv : vv;
-      }
-      T = Ak[nc + src];
+    for (int f = 0; f < 12; ++f) {
+      const double vv = Uk[f * nc + src];
+      q[f] = ((flip >> f) & 1) ? -vv : vv;
     }
+    const double T = Ak[nc + src];
     const double ri = 1.0 / rho;
     double Y8[NR], Yf[NS];
     cell_Y(q, ri, Y8, Yf);
@@ -650,35 +722,36 @@ __global__ void __launch_bounds__(256) k_flux_vjp(MP m, Grid g, const double* __
     ub[3] += Fb[3] * un;
     double Yb[NR];
 #pragma unroll
-    for (int k = 0; k < NR; ++k) {
-      rb += Fb[4 + k] * un * Y8[k];
-      unb += Fb[4 + k] * rho * Y8[k];
-      Yb[k] = Fb[4 + k] * rho * un;
+    for (int kk = 0; kk < NR; ++kk) {
+      rb += Fb[4 + kk] * un * Y8[kk];
+      unb += Fb[4 + kk] * rho * Y8[kk];
+      Yb[kk] = Fb[4 + kk] * rho * un;
     }
     rb += pb * R * T;
     const double Rb = pb * rho * T;
     const double Tb = pb * rho * R;
 #pragma unroll
-    for (int k = 0; k < NR; ++k) Yb[k] += Rb * (m.invM[k] - m.invM[NR]);
+    for (int kk = 0; kk < NR; ++kk) Yb[kk] += Rb * (m.invM[kk] - m.invM[NR]);
     const double ubx = D == 0 ? unb : utb, uby = D == 0 ? utb : unb;
     ub[1] += ubx * ri;
     ub[2] += uby * ri;
     rb -= ubx * u * ri + uby * v * ri;
 #pragma unroll
-    for (int k = 0; k < NR; ++k) {
-      ub[4 + k] += Yb[k] * ri;
-      rb -= Yb[k] * Y8[k] * ri;
+    for (int kk = 0; kk < NR; ++kk) {
+      ub[4 + kk] += Yb[kk] * ri;
+      rb -= Yb[kk] * Y8[kk] * ri;
     }
     ub[0] += rb;
     if (interior) {
 #pragma unroll
       for (int f = 0; f < 12; ++f) {
         double val = ub[f];
-        if (D == 0 && Un_b) {
-          // first pass over the cell in this stage: the RK combination
-          Un_b[f * nc + cell] += un_coef * Uo_b[f * nc + cell];
+        if (D == 0) {
+          const double uo = Uo_b[f * nc + cell];
+          // the RK combination, once per cell and stage
+          if (Un_b) Un_b[f * nc + cell] += un_coef * uo;
+          val += coef * uo;
         }
-        if (D == 0) val += coef * Uo_b[f * nc + cell];
         Ub[f * nc + cell] += val;
       }
       Abk[nc + cell] += Tb;
@@ -765,6 +838,9 @@ __global__ void k_speed_count(MP m, Grid g, const double* __restrict__ U, const 
   block_add(cd, red + 5);
 }
 
+// UPD: then the update_aux VJP of the same state with the completed aux
+// adjoint (consumed and zeroed), as k_upd_vjp.
+template <bool UPD>
 __global__ void k_speed_scatter(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ A,
                                 const unsigned char* __restrict__ mult, const double* __restrict__ slots_rec,
                                 int stage, double cfl, const double* __restrict__ red, double* Ub, double* Ab) {
@@ -785,17 +861,23 @@ __global__ void k_speed_scatter(MP m, Grid g, const double* __restrict__ U, cons
     wx += -db * s.d * s.d / g.dx;
     wy += -db * s.d * s.d / g.dy;
   }
-  if (wx == 0.0 && wy == 0.0) return;
+  double gb = UPD ? Ab[c] : 0.0, Tb = UPD ? Ab[nc + c] : 0.0;
+  if (wx == 0.0 && wy == 0.0 && gb == 0.0 && Tb == 0.0) return;
   double ub[12];
 #pragma unroll
   for (int f = 0; f < 12; ++f) ub[f] = 0.0;
-  double gb = 0.0, Tb = 0.0;
   speed_vjp(m, q, gamma, T, 1, wx, ub, gb, Tb);
   speed_vjp(m, q, gamma, T, 2, wy, ub, gb, Tb);
+  if (UPD) {
+    upd_vjp(m, q, T, gb, Tb, ub);
+    Ab[c] = 0.0;
+    Ab[nc + c] = 0.0;
+  } else {
+    Ab[c] += gb;
+    Ab[nc + c] += Tb;
+  }
 #pragma unroll
   for (int f = 0; f < 12; ++f) Ub[f * nc + c] += ub[f];
-  Ab[c] += gb;
-  Ab[nc + c] += Tb;
 }
 
 // ---------------------------------------------------------------------------
@@ -916,14 +998,14 @@ cudaError_t upd_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, 
 cudaError_t chem_vjp(const jb_mech_params& m, const jb_grid& g, const double* U3, const double* A3,
                      const double* Ub4, double* Ub3, const double* slot_dt, double* dtb, double* lnAb,
                      cudaStream_t st) {
-  const size_t sm = sizeof(double) * CHEM_ADJ_SH * CHEM_ADJ_NT;
+  const size_t sm = sizeof(double) * (CHEM_ADJ_SH + NREAC) * CHEM_ADJ_NT;
   cudaError_t e = cudaFuncSetAttribute(k_chem_vjp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   k_chem_vjp<<<blocks_for(g.ncell, CHEM_ADJ_NT), CHEM_ADJ_NT, sm, st>>>(m, g, U3, A3, Ub4, Ub3, slot_dt, dtb, lnAb);
   return cudaGetLastError();
 }
 
-constexpr size_t FLUX_VJP_SMEM = sizeof(double) * (7 * NE * TA + 11 * NF * TA);
+constexpr size_t FLUX_VJP_SMEM = sizeof(double) * (7 * EA + 11 * FA) + (sizeof(long long) + sizeof(int)) * EA;
 
 cudaError_t flux_vjp(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
                      const double* Uo_b, double coef, const double* slots_rec, int stage, double* Ub, double* Abk,
@@ -948,11 +1030,14 @@ cudaError_t flux_vjp(const jb_mech_params& m, const jb_grid& g, const double* Uk
 
 cudaError_t speed_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A,
                       const unsigned char* mult, const double* slots_rec, int stage, double cfl, double* red,
-                      double* Ub, double* Ab, cudaStream_t st) {
+                      double* Ub, double* Ab, bool upd, cudaStream_t st) {
   k_speed_count<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U, A, mult, slots_rec, stage, cfl, red);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_speed_scatter<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U, A, mult, slots_rec, stage, cfl, red, Ub, Ab);
+  if (upd)
+    k_speed_scatter<true><<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U, A, mult, slots_rec, stage, cfl, red, Ub, Ab);
+  else
+    k_speed_scatter<false><<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U, A, mult, slots_rec, stage, cfl, red, Ub, Ab);
   return cudaGetLastError();
 }
 

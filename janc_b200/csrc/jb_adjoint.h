@@ -16,9 +16,10 @@ cudaError_t chem_vjp(const jb_mech_params& m, const jb_grid& g, const double* U3
 cudaError_t flux_vjp(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
                      const double* Uo_b, double coef, const double* slots_rec, int stage, double* Ub, double* Abk,
                      double* Un_b, double un_coef, double* ghost, double* red, cudaStream_t st);
+// upd: also the update_aux VJP of (U, A) with the completed aux adjoint
 cudaError_t speed_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A,
                       const unsigned char* mult, const double* slots_rec, int stage, double cfl, double* red,
-                      double* Ub, double* Ab, cudaStream_t st);
+                      double* Ub, double* Ab, bool upd, cudaStream_t st);
 cudaError_t probe_seed(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A,
                        const double* pp_bar, int px, int py, int wx, int wy, double* Ub, double* Ab, cudaStream_t st);
 cudaError_t probe_mean(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A, int px, int py,

@@ -565,18 +565,18 @@ int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, do
   JB_TRY(cudaMemsetAsync(B2, 0, sizeof(double) * nU, st), "Ubar2 clear");
   JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
   JB_TRY(jb::adj::flux_vjp(m, g, W2, A2, B1, 2.0 / 3.0, slots, 2, B2, Ab2, Ubar, 1.0 / 3.0, gh, red, st), "stage 3");
-  JB_TRY(jb::adj::speed_vjp(m, g, W2, A2, h->adj_mult, slots, 2, 0.0, red, B2, Ab2, st), "alpha 3");
-  JB_TRY(jb::adj::upd_vjp(m, g, W2, A2, B2, Ab2, st), "update_aux 2");
+  // alpha 3, then update_aux of U2 with its completed aux adjoint
+  JB_TRY(jb::adj::speed_vjp(m, g, W2, A2, h->adj_mult, slots, 2, 0.0, red, B2, Ab2, true, st), "alpha 3");
   // stage 2: U2 = 3/4 U + 1/4 (U1 + dt L(U1, aux1)); B1 = Ubar1
   JB_TRY(cudaMemsetAsync(B1, 0, sizeof(double) * nU, st), "Ubar1 clear");
   JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
   JB_TRY(jb::adj::flux_vjp(m, g, W1, A1, B2, 0.25, slots, 1, B1, Ab2, Ubar, 0.75, gh, red, st), "stage 2");
-  JB_TRY(jb::adj::speed_vjp(m, g, W1, A1, h->adj_mult, slots, 1, 0.0, red, B1, Ab2, st), "alpha 2");
-  JB_TRY(jb::adj::upd_vjp(m, g, W1, A1, B1, Ab2, st), "update_aux 1");
+  JB_TRY(jb::adj::speed_vjp(m, g, W1, A1, h->adj_mult, slots, 1, 0.0, red, B1, Ab2, true, st), "alpha 2");
   // stage 1: U1 = U + dt L(U, aux); then alpha 1 and the CFL time step
   JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
   JB_TRY(jb::adj::flux_vjp(m, g, Un, An, B1, 1.0, slots, 0, Ubar, Abar, nullptr, 0.0, gh, red, st), "stage 1");
-  JB_TRY(jb::adj::speed_vjp(m, g, Un, An, h->adj_mult, slots, 0, c_cfl, red, Ubar, Abar, st), "alpha 1 and dt");
+  JB_TRY(jb::adj::speed_vjp(m, g, Un, An, h->adj_mult, slots, 0, c_cfl, red, Ubar, Abar, false, st),
+         "alpha 1 and dt");
   return JB_OK;
 }
 
