@@ -325,11 +325,15 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
                "select3");
       continue;
     }
-    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, false, false, m, g, W3, nullptr, h->cand, A3, h->strips,
-                    h->slots, 2, 0, st),
-           "select3");
-    // chemistry and the final temperature solve
-    JB_TIMED(JB_KCAT_CHEM, o.chem(d, false, m, g, W3, A3, Uo, h->cand, h->slots, 3, 0.0, st), "chem");
+    // chemistry and the final temperature solve; without a record the
+    // stage-3 temperature is taken from the iterates inside the chemistry
+    // kernel (its gamma is not used by anything that follows)
+    if (rec)
+      JB_TIMED(JB_KCAT_SELECT, o.select(d, true, false, false, m, g, W3, nullptr, h->cand, A3, h->strips,
+                      h->slots, 2, 0, st),
+             "select3");
+    JB_TIMED(JB_KCAT_CHEM, o.chem(d, false, m, g, W3, rec ? A3 : nullptr, Uo, h->cand, h->slots, 3, 0.0, st),
+             "chem");
     JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, Uo, nullptr, h->cand, Ao, h->strips,
                     h->slots, 3, 3, st),
            "select4");

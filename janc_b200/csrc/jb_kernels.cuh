@@ -1165,7 +1165,7 @@ __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const do
 }
 
 template <int DIM, bool SELECT, bool ALPHA, bool CFL>
-__global__ void k_select(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux_in,
+__global__ void __launch_bounds__(256, 3) k_select(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux_in,
                          const double* __restrict__ cand, double* __restrict__ aux_out,
                          double* __restrict__ strips, Slots* slots, int midx, int aidx) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1439,8 +1439,12 @@ __global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __r
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const double dt = WRITE_S ? dt_arg : slots->dt;
   unsigned bits = 0, st = 0;
-  if (c < g.ncell)
-    chem_cell_step<DIM, WRITE_S, GEN>(m, g, U, aux[g.ncell + c], out, cand, c, dt, shc + threadIdx.x, bits, st);
+  if (c < g.ncell) {
+    // aux == null: the temperature is the selected iterate of the previous
+    // solve (mask midx - 1), i.e. that solve's select pass is fused here
+    const double T = aux ? aux[g.ncell + c] : cand[(long long)halley_count(slots->mask[midx - 1]) * g.ncell + c];
+    chem_cell_step<DIM, WRITE_S, GEN>(m, g, U, T, out, cand, c, dt, shc + threadIdx.x, bits, st);
+  }
   block_reduce_store(0.0, 0.0, 0.0, bits | (st << 16), slots, 0, false, false, WRITE_S ? -1 : midx);
 }
 

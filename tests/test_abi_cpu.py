@@ -34,7 +34,7 @@ def test_pack_layout():
 
 def _declared():
     src = open(HEADER).read()
-    decl = r"^(?:int|long long|const char\*)\s+(jb_[a-z0-9_]+)\s*\("
+    decl = r"^(?:int|long long|const char\*)\s+(jb_[A-Za-z0-9_]+)\s*\("
     return sorted(set(re.findall(decl, src, re.M)))
 
 
