@@ -73,6 +73,11 @@ UNIT = "cell-updates/s"
 BYTES_CHEM_PER_CELL = 224      # read U,aux (112 B) + write U,aux (112 B), float64
 BYTES_STEP_PER_CELL = 864 + 224  # fused-step minimum + separate chemistry pass (2D)
 BYTES_FLUX_STAGE_PER_CELL = 288  # one RK stage of the fused minimum: (224 + 320 + 320) / 3
+# DRAM bytes per cell measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+# on the 1024x256 channel, mixed precision: an RK stage 2/3 launch and a
+# chemistry launch; and per cell-step of the persistent ensemble kernel
+TRAFFIC_PER_CELL = {"flux": 305.0, "chem": 148.0}
+TRAFFIC_ENS_PER_CELL_STEP = 1125.0
 
 
 ENS_N, ENS_SEED, ENS_CFL = 64, 4, 0.1
@@ -362,7 +367,7 @@ def _time_path(args, s, U0, aux0, theta, ncell, dist, clocks=None):
     haux = aux.cpu().pin_memory()
     oU = torch.empty_like(hU).pin_memory()
     oaux = torch.empty_like(haux).pin_memory()
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = max(5, min(args.steps, 20))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -381,7 +386,11 @@ def _time_path(args, s, U0, aux0, theta, ncell, dist, clocks=None):
         legs[k][3].record()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(dist, e0.elapsed_time(e1))
+    # per-step end-to-end time; the median keeps one-off host stalls (other
+    # processes, driver calls) out of the rate, the mean is reported beside it
+    per_step = sorted(lg[0].elapsed_time(lg[3]) for lg in legs)
+    e2e_mean = e0.elapsed_time(e1) / e2e_steps
+    e2e_ms = max_over_ranks(dist, statistics.median(per_step) * e2e_steps)
     leg_ms = [sum(lg[i].elapsed_time(lg[i + 1]) for lg in legs) / e2e_steps for i in range(3)]
     ws = dist.get_world_size() if dist else 1
     return {"value": job_value(ws, ncell, args.steps, ms_total), "ms_per_step": ms_total / args.steps,
@@ -391,7 +400,8 @@ def _time_path(args, s, U0, aux0, theta, ncell, dist, clocks=None):
             "e2e": {"value": job_value(ws, ncell, e2e_steps, e2e_ms), "unit": UNIT,
                     "h2d_bytes_per_step": (hU.numel() + haux.numel()) * 8,
                     "d2h_bytes_per_step": (hU.numel() + haux.numel()) * 8,
-                    "steps": e2e_steps, "h2d_ms": leg_ms[0], "step_ms": leg_ms[1], "d2h_ms": leg_ms[2]}}
+                    "steps": e2e_steps, "h2d_ms": leg_ms[0], "step_ms": leg_ms[1], "d2h_ms": leg_ms[2],
+                    "statistic": "median step", "mean_step_ms": e2e_mean}}
 
 
 def _accuracy(args, s_test, s_ref, U0, aux0, theta, steps):
@@ -500,7 +510,10 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": {"chem": "k_chem (point-implicit chemistry + final Halley)",
                                                  "flux": "k_flux2d (LF + WENO5 + RK stage + Halley)"}[dom],
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "traffic": None, "peak_source": hbm_src,
+                     "traffic": (TRAFFIC_PER_CELL[dom] * ncell if args.workload == "channel" and
+                                 args.precision == "mixed" else None),
+                     "traffic_source": "ncu dram bytes of one launch on this workload (mixed precision)",
+                     "peak_source": hbm_src,
                      "algorithmic_bytes_per_cell": bytes_cell, "launch_ms": launch_ms,
                      "step_achieved_gbs": step_gbs,
                      "step_algorithmic_bytes_per_cell": BYTES_STEP_PER_CELL},
@@ -822,7 +835,9 @@ def run_ensemble(args):
         "status_bits": status, "tubes_finite": n_finite,
         "gpu_launches": 1,
         "roofline": {"bound": "hbm", "kernel": "k_ensemble (all phases of all steps)", "achieved": achieved,
-                     "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                     "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "traffic": TRAFFIC_ENS_PER_CELL_STEP * cells * K if args.precision == "mixed" else None,
+                     "traffic_source": "ncu dram bytes of a 20-step launch, scaled to this launch's cell-steps",
                      "peak_source": hbm_src, "algorithmic_bytes_per_cell_step": BYTES_ENS_STEP_PER_CELL,
                      "launch_ms": ms},
         "compute_roofline": {"bound": "fp64", "kernel": "k_ensemble (chemistry share of the flops only)",
