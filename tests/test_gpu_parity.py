@@ -388,3 +388,4 @@ def test_mixed_rdc_flux_close_to_fp64(golden_dir):
     assert field_err(r, g["rhs0"]) < 1e-5
     U, aux, _ = _run_cfl(s, g["U0"], g["aux0"], 3, theta)
     assert rel_l1(U[0], g["U_3"][0]) < 1e-6
+
