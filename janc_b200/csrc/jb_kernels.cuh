@@ -1087,7 +1087,9 @@ __global__ void k_halley(MP m, Grid g, const double* __restrict__ U, const doubl
 // One cell of the select pass; folds its wave speeds / CFL candidate into
 // amx, amy, dtm and status bits into st.  mask: the Halley mask of the solve
 // being finished (SELECT); slots: where a NaN CFL candidate is flagged.
-template <int DIM, bool SELECT, bool ALPHA, bool CFL>
+// STRIPS: a boundary cell of a pressure-outlet / injector side also builds
+// its ghost state here (k_select leaves that to k_strips).
+template <int DIM, bool SELECT, bool ALPHA, bool CFL, bool STRIPS = true>
 __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const double* U, const double* aux_in,
                                             const double* cand, double* aux_out, double* strips,
                                             Slots* slots, unsigned mask, long long c, double& amx,
@@ -1131,7 +1133,7 @@ __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const do
         // NaN; the reduction below skips NaN, so record it separately
         if (!(d == d)) atomicOr(&slots->dtnan, 1u);
       }
-      if (ALPHA) {
+      if (ALPHA && STRIPS) {
         // ghost states that are not copies of interior cells
         int x = DIM == 1 ? (int)c : (int)(c / g.ny);
         int y = DIM == 1 ? 0 : (int)(c % g.ny);
@@ -1172,9 +1174,56 @@ __global__ void __launch_bounds__(256, 3) k_select(MP m, Grid g, const double* _
   double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
   unsigned st = 0;
   if (c < g.ncell)
-    select_cell<DIM, SELECT, ALPHA, CFL>(m, g, U, aux_in, cand, aux_out, strips, slots,
-                                         SELECT ? slots->mask[midx] : 0u, c, amx, amy, dtm, st);
+    select_cell<DIM, SELECT, ALPHA, CFL, false>(m, g, U, aux_in, cand, aux_out, strips, slots,
+                                                SELECT ? slots->mask[midx] : 0u, c, amx, amy, dtm, st);
   if (ALPHA || CFL) block_reduce_store(amx, amy, dtm, st << 16, slots, aidx, ALPHA, CFL, -1);
+}
+
+// Ghost strips of the pressure-outlet and injector sides (the padded grid's
+// entries that are not copies of interior cells) and their wave speeds into
+// the alpha maxima: one thread per boundary position, after the select pass
+// that wrote the boundary cells' (gamma, T) into aux.  Positions: side 0 and
+// 1 (x = 0, nx-1) ny each, then sides 2 and 3 (y = 0, ny-1) nx each.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_strips(MP m, Grid g, const double* __restrict__ U,
+                                                const double* __restrict__ aux, double* __restrict__ strips,
+                                                Slots* slots, int aidx) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  constexpr int nv = nY + NR;
+  const long long nc = g.ncell;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ns = DIM == 1 ? 1 : g.ny;
+  double amx = 0.0, amy = 0.0;
+  int side = -1, pos = 0;
+  if (t < 2 * ns) { side = t / ns; pos = t % ns; }
+  else if (DIM == 2 && t < 2 * ns + 2 * g.nx) { side = 2 + (t - 2 * ns) / g.nx; pos = (t - 2 * ns) % g.nx; }
+  const int kind = side >= 0 ? g.bc[side] : JB_BC_PERIODIC;
+  if (kind == JB_BC_PRESSURE_OUTLET || kind == JB_BC_RDC_INJECTOR) {
+    const int x = side == 0 ? 0 : side == 1 ? g.nx - 1 : pos;
+    const int y = DIM == 1 ? 0 : (side == 2 ? 0 : side == 3 ? g.ny - 1 : pos);
+    const long long c = DIM == 1 ? (long long)x : (long long)x * g.ny + y;
+    double q[nv];
+#pragma unroll
+    for (int f = 0; f < nv; ++f) q[f] = U[f * nc + c];
+    const double gamma = aux[c], T = aux[nc + c];
+    double gs[nv + 2];
+    if (kind == JB_BC_PRESSURE_OUTLET) {
+      double un = side < 2 ? q[1] / q[0] : q[2] / q[0];
+      if (side == 0 || side == 2) un = -un;
+      pressure_outlet_state<DIM>(m, q, gamma, T, un, g.Pb, gs);
+    } else {
+      if (DIM == 2) {
+        double Yi[NR];
+        for (int k = 0; k < NR; ++k) Yi[k] = g.Yinj[k * g.nx + x];
+        injector_state(m, q, gamma, T, Yi, g.inj_block_p, gs);
+      }
+    }
+    for (int f = 0; f < nv + 2; ++f) strips[strip_idx(g, side, f, pos)] = gs[f];
+    Prim<DIM> pg = u_to_prim<DIM>(m, gs, gs[nv], gs[nv + 1]);
+    amx = fabs(pg.u) + pg.a;
+    amy = fabs(pg.v) + pg.a;
+  }
+  block_reduce_store(amx, amy, 0.0, 0u, slots, aidx, true, false, -1);
 }
 
 }  // namespace JB_NS
