@@ -1167,7 +1167,7 @@ __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const do
 }
 
 template <int DIM, bool SELECT, bool ALPHA, bool CFL>
-__global__ void __launch_bounds__(256, 3) k_select(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux_in,
+__global__ void __launch_bounds__(256, 4) k_select(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux_in,
                          const double* __restrict__ cand, double* __restrict__ aux_out,
                          double* __restrict__ strips, Slots* slots, int midx, int aidx) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
