@@ -21,8 +21,8 @@
 //   k_upd_vjp       Ubar += d(gamma,T)/dU^T abar           (update_aux)
 //   k_chem_vjp      chemistry: Ubar3 = Ubar4 + dS/dU3^T Ubar4, with the
 //                   temperature, dt and ln A adjoints, then update_aux of U3
-//   k_flux_vjp<D>   one direction of one RK stage's L (tile per block)
-//   k_ghost_fold    ghost-cell adjoints back to the cells they copy
+//   k_flux_vjp      both directions of one RK stage's L (tile per block)
+//   k_flux_merge    y-face adjoints and ghost-cell adjoints into the cells
 //   k_speed_count / k_speed_scatter   alpha and CFL ties and their adjoint
 //   k_probe_seed    the probe-pressure term of the loss
 //   k_init_vjp      initial state from (P, T, Y): T adjoint
@@ -537,12 +537,15 @@ __device__ __forceinline__ int ie(int e, int c) { return D == 0 ? e * TA + c : c
 template <int D>
 __device__ __forceinline__ int iff(int f, int c) { return D == 0 ? f * TA + c : c * NFP + f; }
 
+// One tile (bx, by) of one direction.  D = 0 (x faces) adds into Ub, Abk
+// (T adjoint at Abk[nc + c]) and applies the RK combination; D = 1 (y faces)
+// stores into its own Ub, Abk (T adjoint at Abk[c]), merged afterwards.
 template <int D>  // 0: x faces (F), 1: y faces (G)
-__global__ void __launch_bounds__(256, 3) k_flux_vjp(MP m, Grid g, const double* __restrict__ Uk,
-                                                 const double* __restrict__ Ak, const double* __restrict__ Uo_b,
-                                                 double coef, const double* __restrict__ slots_rec, int stage,
-                                                 double* Ub, double* Abk, double* Un_b, double un_coef,
-                                                 double* ghost, double* red) {
+__device__ __forceinline__ void flux_vjp_body(const MP& m, const Grid& g, const double* __restrict__ Uk,
+                                              const double* __restrict__ Ak, const double* __restrict__ Uo_b,
+                                              double coef, const double* __restrict__ slots_rec, int stage,
+                                              double* Ub, double* Abk, double* Un_b, double un_coef,
+                                              double* ghost, double* red, int bx, int by) {
   // Shared arrays: per extended cell rho, u, v, p, the field, H+, H- and its
   // source (cell index, flip bits); per face the 5 + 5 WENO partials times
   // the face-flux adjoint and the face value.  The layout runs along the
@@ -564,8 +567,8 @@ __global__ void __launch_bounds__(256, 3) k_flux_vjp(MP m, Grid g, const double*
   const int tA = D == 0 ? threadIdx.y : threadIdx.x;  // along index of the owned cell
   const int tC = D == 0 ? threadIdx.x : threadIdx.y;  // across index
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const int a0 = -3 + (int)blockIdx.x * TO;
-  const int c0 = (int)blockIdx.y * TA;
+  const int a0 = -3 + bx * TO;
+  const int c0 = by * TA;
   const double dA = D == 0 ? g.dx : g.dy;
   const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
   const double alpha = bitsd(D == 0 ? rs->ax[stage] : rs->ay[stage]);
@@ -752,9 +755,11 @@ __global__ void __launch_bounds__(256, 3) k_flux_vjp(MP m, Grid g, const double*
           if (Un_b) Un_b[f * nc + cell] += un_coef * uo;
           val += coef * uo;
         }
-        Ub[f * nc + cell] += val;
+        if (D == 0) Ub[f * nc + cell] += val;
+        else Ub[f * nc + cell] = val;
       }
-      Abk[nc + cell] += Tb;
+      if (D == 0) Abk[nc + cell] += Tb;
+      else Abk[cell] = Tb;
     } else {
       // ghost entry: side, layer, position
       const int side = D == 0 ? (ao < 0 ? 0 : 1) : (ao < 0 ? 2 : 3);
@@ -770,32 +775,56 @@ __global__ void __launch_bounds__(256, 3) k_flux_vjp(MP m, Grid g, const double*
   block_add(dtb, red + 2);
 }
 
-// Ghost-entry adjoints back to the interior cells they copy (the BC's map,
-// with the normal-momentum flips undone).
-__global__ void k_ghost_fold(Grid g, const double* __restrict__ ghost, double* Ub, double* Ab) {
-  const int L = g.nx > g.ny ? g.nx : g.ny;
+// Both directions of one RK stage in one launch: blocks [0, nbx) are x-face
+// tiles (a grid of gxx tiles along x), the rest y-face tiles (gyy along y).
+__global__ void __launch_bounds__(256, 3) k_flux_vjp(MP m, Grid g, const double* __restrict__ Uk,
+                                                 const double* __restrict__ Ak, const double* __restrict__ Uo_b,
+                                                 double coef, const double* __restrict__ slots_rec, int stage,
+                                                 double* Ub, double* Abk, double* Ub2, double* Ab2, double* Un_b,
+                                                 double un_coef, double* ghost, double* red, int nbx, int gxx,
+                                                 int gyy) {
+  const int b = blockIdx.x;
+  if (b < nbx)
+    flux_vjp_body<0>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, Ub, Abk, Un_b, un_coef, ghost, red, b % gxx,
+                     b / gxx);
+  else
+    flux_vjp_body<1>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, Ub2, Ab2, nullptr, 0.0, ghost, red,
+                     (b - nbx) % gyy, (b - nbx) / gyy);
+}
+
+// Per interior cell: add the y-face adjoints (Ub2, Ab2) and gather the
+// adjoints of the ghost entries that copy this cell (the boundary map of
+// every side, with the normal-momentum flips undone).
+__global__ void k_flux_merge(Grid g, const double* __restrict__ ghost, const double* __restrict__ Ub2,
+                             const double* __restrict__ Ab2, double* Ub, double* Ab) {
   const long long nc = g.ncell;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // (side, layer, pos)
-  if (t >= 12 * L) return;
-  const int sl = t / L, pos = t % L;
-  const int side = sl / 3, layer = sl % 3;
-  const int n = side < 2 ? g.ny : g.nx;
-  if (pos >= n) return;
-  int x, y;
-  if (side == 0) { x = -1 - layer; y = pos; }
-  else if (side == 1) { x = g.nx + layer; y = pos; }
-  else if (side == 2) { x = pos; y = -1 - layer; }
-  else { x = pos; y = g.ny + layer; }
-  Src s = map_cell<2>(g, x, y);
-  if (s.kind != 0) return;
-  const long long src = (long long)s.xs * g.ny + s.ys;
-  const double* gp = ghost + ((size_t)(side * 3 + layer) * 13) * L + pos;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const int x = (int)(c / g.ny), y = (int)(c % g.ny);
+  const int L = g.nx > g.ny ? g.nx : g.ny;
+  double ub[12];
 #pragma unroll
-  for (int f = 0; f < 12; ++f) {
-    const double v = gp[(size_t)f * L];
-    atomicAdd(&Ub[f * nc + src], ((s.flip >> f) & 1) ? -v : v);
+  for (int f = 0; f < 12; ++f) ub[f] = Ub2[f * nc + c];
+  double tb = Ab2[c];
+  for (int side = 0; side < 4; ++side) {
+    const int pos = side < 2 ? y : x;
+    for (int layer = 0; layer < 3; ++layer) {
+      const int gx = side == 0 ? -1 - layer : side == 1 ? g.nx + layer : x;
+      const int gy = side == 2 ? -1 - layer : side == 3 ? g.ny + layer : y;
+      Src s = map_cell<2>(g, gx, gy);
+      if (s.kind != 0 || s.xs != x || s.ys != y) continue;
+      const double* gp = ghost + ((size_t)(side * 3 + layer) * 13) * L + pos;
+#pragma unroll
+      for (int f = 0; f < 12; ++f) {
+        const double v = gp[(size_t)f * L];
+        ub[f] += ((s.flip >> f) & 1) ? -v : v;
+      }
+      tb += gp[(size_t)12 * L];
+    }
   }
-  atomicAdd(&Ab[nc + src], gp[(size_t)12 * L]);
+#pragma unroll
+  for (int f = 0; f < 12; ++f) Ub[f * nc + c] += ub[f];
+  Ab[nc + c] += tb;
 }
 
 // ---------------------------------------------------------------------------
@@ -1009,22 +1038,18 @@ constexpr size_t FLUX_VJP_SMEM = sizeof(double) * (7 * EA + 11 * FA) + (sizeof(l
 
 cudaError_t flux_vjp(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
                      const double* Uo_b, double coef, const double* slots_rec, int stage, double* Ub, double* Abk,
-                     double* Un_b, double un_coef, double* ghost, double* red, cudaStream_t st) {
-  cudaError_t e0 = cudaFuncSetAttribute(k_flux_vjp<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FLUX_VJP_SMEM);
-  if (e0 == cudaSuccess)
-    e0 = cudaFuncSetAttribute(k_flux_vjp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FLUX_VJP_SMEM);
-  if (e0 != cudaSuccess) return e0;
-  dim3 blk(16, 16);
-  dim3 gx((g.nx + 6 + TO - 1) / TO, (g.ny + TA - 1) / TA);
-  k_flux_vjp<0><<<gx, blk, FLUX_VJP_SMEM, st>>>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, Ub, Abk, Un_b, un_coef, ghost, red);
-  cudaError_t e = cudaGetLastError();
+                     double* Un_b, double un_coef, double* ghost, double* Ub2, double* Ab2, double* red,
+                     cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(k_flux_vjp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FLUX_VJP_SMEM);
   if (e != cudaSuccess) return e;
-  dim3 gy((g.ny + 6 + TO - 1) / TO, (g.nx + TA - 1) / TA);
-  k_flux_vjp<1><<<gy, blk, FLUX_VJP_SMEM, st>>>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, Ub, Abk, nullptr, 0.0, ghost, red);
+  const int gxx = (g.nx + 6 + TO - 1) / TO, gxy = (g.ny + TA - 1) / TA;
+  const int gyy = (g.ny + 6 + TO - 1) / TO, gyx = (g.nx + TA - 1) / TA;
+  const int nbx = gxx * gxy, nby = gyy * gyx;
+  k_flux_vjp<<<nbx + nby, dim3(16, 16), FLUX_VJP_SMEM, st>>>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, Ub, Abk, Ub2,
+                                                             Ab2, Un_b, un_coef, ghost, red, nbx, gxx, gyy);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const int L = g.nx > g.ny ? g.nx : g.ny;
-  k_ghost_fold<<<blocks_for(12LL * L, 128), 128, 0, st>>>(g, ghost, Ub, Abk);
+  k_flux_merge<<<blocks_for(g.ncell, 128), 128, 0, st>>>(g, ghost, Ub2, Ab2, Ub, Abk);
   return cudaGetLastError();
 }
 

@@ -13,9 +13,11 @@ cudaError_t upd_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, 
 cudaError_t chem_vjp(const jb_mech_params& m, const jb_grid& g, const double* U3, const double* A3,
                      const double* Ub4, double* Ub3, const double* slot_dt, double* dtb, double* lnAb,
                      cudaStream_t st);
+// Ub2 (nv x ncell), Ab2 (ncell): scratch for the y-face adjoints
 cudaError_t flux_vjp(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
                      const double* Uo_b, double coef, const double* slots_rec, int stage, double* Ub, double* Abk,
-                     double* Un_b, double un_coef, double* ghost, double* red, cudaStream_t st);
+                     double* Un_b, double un_coef, double* ghost, double* Ub2, double* Ab2, double* red,
+                     cudaStream_t st);
 // upd: also the update_aux VJP of (U, A) with the completed aux adjoint
 cudaError_t speed_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A,
                       const unsigned char* mult, const double* slots_rec, int stage, double cfl, double* red,

@@ -46,6 +46,8 @@ struct jb_handle {
   double* adj_B2;
   double* adj_A2;
   double* adj_ghost;
+  double* adj_Ub2;   // y-face adjoints of a stage before the merge
+  double* adj_Ab2;
   double* adj_red;
   char err[512];
 };
@@ -517,14 +519,16 @@ static int adj_workspace(jb_handle* h) {
   const jb_grid& g = h->grid;
   const size_t nc = (size_t)g.ncell, nU = (size_t)g.nv * nc;
   const size_t L = (size_t)(g.nx > g.ny ? g.nx : g.ny);
-  const size_t n = 2 * nU + 2 * nc + 12 * 13 * L + 8;
+  const size_t n = 3 * nU + 3 * nc + 12 * 13 * L + 8;
   JB_TRY(cudaMalloc(&h->adj_ws, sizeof(double) * n), "adjoint workspace");
   JB_TRY(cudaMemset(h->adj_ws, 0, sizeof(double) * n), "adjoint workspace clear");
   h->adj_B1 = h->adj_ws;
   h->adj_B2 = h->adj_B1 + nU;
   h->adj_A2 = h->adj_B2 + nU;
   h->adj_ghost = h->adj_A2 + 2 * nc;
-  h->adj_red = h->adj_ghost + 12 * 13 * L;
+  h->adj_Ub2 = h->adj_ghost + 12 * 13 * L;
+  h->adj_Ab2 = h->adj_Ub2 + nU;
+  h->adj_red = h->adj_Ab2 + nc;
   std::vector<unsigned char> mult;
   padded_multiplicity(g, mult);
   JB_TRY(cudaMalloc(&h->adj_mult, nc), "multiplicity");
@@ -568,17 +572,17 @@ int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, do
   // stage 3: U3 = 1/3 U + 2/3 (U2 + dt L(U2, aux2))
   JB_TRY(cudaMemsetAsync(B2, 0, sizeof(double) * nU, st), "Ubar2 clear");
   JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
-  JB_TRY(jb::adj::flux_vjp(m, g, W2, A2, B1, 2.0 / 3.0, slots, 2, B2, Ab2, Ubar, 1.0 / 3.0, gh, red, st), "stage 3");
+  JB_TRY(jb::adj::flux_vjp(m, g, W2, A2, B1, 2.0 / 3.0, slots, 2, B2, Ab2, Ubar, 1.0 / 3.0, gh, h->adj_Ub2, h->adj_Ab2, red, st), "stage 3");
   // alpha 3, then update_aux of U2 with its completed aux adjoint
   JB_TRY(jb::adj::speed_vjp(m, g, W2, A2, h->adj_mult, slots, 2, 0.0, red, B2, Ab2, true, st), "alpha 3");
   // stage 2: U2 = 3/4 U + 1/4 (U1 + dt L(U1, aux1)); B1 = Ubar1
   JB_TRY(cudaMemsetAsync(B1, 0, sizeof(double) * nU, st), "Ubar1 clear");
   JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
-  JB_TRY(jb::adj::flux_vjp(m, g, W1, A1, B2, 0.25, slots, 1, B1, Ab2, Ubar, 0.75, gh, red, st), "stage 2");
+  JB_TRY(jb::adj::flux_vjp(m, g, W1, A1, B2, 0.25, slots, 1, B1, Ab2, Ubar, 0.75, gh, h->adj_Ub2, h->adj_Ab2, red, st), "stage 2");
   JB_TRY(jb::adj::speed_vjp(m, g, W1, A1, h->adj_mult, slots, 1, 0.0, red, B1, Ab2, true, st), "alpha 2");
   // stage 1: U1 = U + dt L(U, aux); then alpha 1 and the CFL time step
   JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
-  JB_TRY(jb::adj::flux_vjp(m, g, Un, An, B1, 1.0, slots, 0, Ubar, Abar, nullptr, 0.0, gh, red, st), "stage 1");
+  JB_TRY(jb::adj::flux_vjp(m, g, Un, An, B1, 1.0, slots, 0, Ubar, Abar, nullptr, 0.0, gh, h->adj_Ub2, h->adj_Ab2, red, st), "stage 1");
   JB_TRY(jb::adj::speed_vjp(m, g, Un, An, h->adj_mult, slots, 0, c_cfl, red, Ubar, Abar, false, st),
          "alpha 1 and dt");
   return JB_OK;
