@@ -17,14 +17,16 @@
 // tied entries (entries within a relative 1e-13 count as tied), clip
 // passes the gradient to whichever bound is active.
 //
-// Kernels (one thread per cell unless noted):
-//   k_upd_vjp       Ubar += d(gamma,T)/dU^T abar           (update_aux)
+// Kernels (one thread per cell unless noted), in the order of one step:
+//   k_vjp_begin     the probe term of the loss and update_aux of U4; the
+//                   primitives and alpha / CFL tie counts of U, U1, U2
 //   k_chem_vjp      chemistry: Ubar3 = Ubar4 + dS/dU3^T Ubar4, with the
 //                   temperature, dt and ln A adjoints, then update_aux of U3
-//   k_flux_vjp      both directions of one RK stage's L (tile per block)
-//   k_flux_merge    y-face adjoints and ghost-cell adjoints into the cells
-//   k_speed_count / k_speed_scatter   alpha and CFL ties and their adjoint
-//   k_probe_seed    the probe-pressure term of the loss
+//   per RK stage (3, 2, 1):
+//   k_flux_sweep    one thread per (direction, line, segment, field): the
+//                   WENO5 / LF face adjoints along the line (registers only)
+//   k_stage_merge   flux-function VJPs, ghost copies, RK combination, alpha
+//                   (and CFL) ties, update_aux of the stage state
 //   k_init_vjp      initial state from (P, T, Y): T adjoint
 #define JB_NS adj
 #define JB_FAST 1
@@ -165,24 +167,6 @@ __device__ __forceinline__ void block_add(double v, double* dst) {
 
 // ---------------------------------------------------------------------------
 // update_aux VJP over a whole state: Ubar += ..., abar consumed (zeroed)
-// ---------------------------------------------------------------------------
-__global__ void k_upd_vjp(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux,
-                          double* __restrict__ Ub, double* __restrict__ Ab) {
-  const long long nc = g.ncell;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
-  const double gb = Ab[c], Tb = Ab[nc + c];
-  if (gb == 0.0 && Tb == 0.0) return;
-  double q[12], ub[12];
-#pragma unroll
-  for (int f = 0; f < 12; ++f) { q[f] = U[f * nc + c]; ub[f] = 0.0; }
-  upd_vjp(m, q, aux[nc + c], gb, Tb, ub);
-#pragma unroll
-  for (int f = 0; f < 12; ++f) Ub[f * nc + c] += ub[f];
-  Ab[c] = 0.0;
-  Ab[nc + c] = 0.0;
-}
-
 // ---------------------------------------------------------------------------
 // chemistry VJP (reaction_model.py:91-193)
 // ---------------------------------------------------------------------------
@@ -523,319 +507,13 @@ __device__ __forceinline__ double weno_d(double v0, double v1, double v2, double
 }
 
 // ---------------------------------------------------------------------------
-// flux VJP of one direction of one RK stage
-// ---------------------------------------------------------------------------
-// Block: TO cells along the direction (padded coordinates, ghosts included)
-// x TA cells across it (interior only).  threadIdx.x runs along y, so the
-// y direction is the coalesced one for both kernels.
-constexpr int TO = 16, TA = 16, NE = TO + 10, NF = TO + 5;
-constexpr int NEP = NE + 1, NFP = NF;  // odd strides (in doubles) of the across-major layout
-constexpr int EA = TA * NEP, FA = TA * NFP;  // doubles per extended-cell / face array
-
-template <int D>
-__device__ __forceinline__ int ie(int e, int c) { return D == 0 ? e * TA + c : c * NEP + e; }
-template <int D>
-__device__ __forceinline__ int iff(int f, int c) { return D == 0 ? f * TA + c : c * NFP + f; }
-
-// One tile (bx, by) of one direction.  D = 0 (x faces) adds into Ub, Abk
-// (T adjoint at Abk[nc + c]) and applies the RK combination; D = 1 (y faces)
-// stores into its own Ub, Abk (T adjoint at Abk[c]), merged afterwards.
-template <int D>  // 0: x faces (F), 1: y faces (G)
-__device__ __forceinline__ void flux_vjp_body(const MP& m, const Grid& g, const double* __restrict__ Uk,
-                                              const double* __restrict__ Ak, const double* __restrict__ Uo_b,
-                                              double coef, const double* __restrict__ slots_rec, int stage,
-                                              double* Ub, double* Abk, double* Un_b, double un_coef,
-                                              double* ghost, double* red, int bx, int by) {
-  // Shared arrays: per extended cell rho, u, v, p, the field, H+, H- and its
-  // source (cell index, flip bits); per face the 5 + 5 WENO partials times
-  // the face-flux adjoint and the face value.  The layout runs along the
-  // across index for x faces and along the direction for y faces, so a
-  // warp's accesses are unit-stride in both kernels.
-  extern __shared__ __align__(16) double sm_flux[];
-  double* sP = sm_flux;          // [4][EA]
-  double* sQ = sP + 4 * EA;
-  double* sHp = sQ + EA;
-  double* sHm = sHp + EA;
-  double* sPL = sHm + EA;        // [5][FA]
-  double* sPR = sPL + 5 * FA;    // [5][FA]
-  double* sFv = sPR + 5 * FA;    // [FA]
-  long long* sSrc = reinterpret_cast<long long*>(sFv + FA);  // [EA], -1: outside the padded grid
-  int* sFlip = reinterpret_cast<int*>(sSrc + EA);            // [EA]
-  const int nA = D == 0 ? g.nx : g.ny;
-  const int nC = D == 0 ? g.ny : g.nx;
-  const long long nc = g.ncell;
-  const int tA = D == 0 ? threadIdx.y : threadIdx.x;  // along index of the owned cell
-  const int tC = D == 0 ? threadIdx.x : threadIdx.y;  // across index
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const int a0 = -3 + bx * TO;
-  const int c0 = by * TA;
-  const double dA = D == 0 ? g.dx : g.dy;
-  const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
-  const double alpha = bitsd(D == 0 ? rs->ax[stage] : rs->ay[stage]);
-  const double dt = rs->dt;
-  const int dirf = D == 0 ? 1 : 2;  // normal momentum field
-  // sources and primitives of the extended cells
-  for (int i = tid; i < NE * TA; i += 256) {
-    const int e = D == 0 ? i / TA : i % NE, cc = D == 0 ? i % TA : i / NE;
-    const int a = a0 - 5 + e, cidx = c0 + cc;
-    double q[12], T = 1.0;
-    long long src = -1;
-    int flip = 0;
-    if (cidx < nC) {
-      const int x = D == 0 ? a : cidx, y = D == 0 ? cidx : a;
-      Src s = map_cell<2>(g, x, y);
-      if (s.kind == 0) {
-        src = (long long)s.xs * g.ny + s.ys;
-        flip = s.flip;
-      }
-    }
-    if (src >= 0) {
-#pragma unroll
-      for (int f = 0; f < 12; ++f) {
-        const double v = Uk[f * nc + src];
-        q[f] = ((flip >> f) & 1) ? -v : v;
-      }
-      T = Ak[nc + src];
-    } else {
-#pragma unroll
-      for (int f = 0; f < 12; ++f) q[f] = 1.0;
-    }
-    const double rho = q[0], ri = 1.0 / rho;
-    double Y8[NR], Yf[NS];
-    cell_Y(q, ri, Y8, Yf);
-    const int k = ie<D>(e, cc);
-    sSrc[k] = src;
-    sFlip[k] = flip;
-    sP[k] = rho;
-    sP[EA + k] = q[1] * ri;
-    sP[2 * EA + k] = q[2] * ri;
-    sP[3 * EA + k] = rho * get_R(m, Yf) * T;
-  }
-  __syncthreads();
-  const int ao = a0 + tA;  // padded along coordinate of the owned cell
-  const int co = c0 + tC;
-  const bool owned = co < nC && ao < nA + 3;
-  const bool interior = owned && ao >= 0 && ao < nA;
-  const long long cell = D == 0 ? (long long)ao * g.ny + co : (long long)co * g.ny + ao;
-  double Fb[12], Ua[12];
-  double ab = 0.0, dtb = 0.0;
-#pragma unroll 1
-  for (int f = 0; f < 12; ++f) {
-    // H+- of the field on the extended cells
-    for (int i = tid; i < NE * TA; i += 256) {
-      const int e = D == 0 ? i / TA : i % NE, cc = D == 0 ? i % TA : i / NE;
-      const int k = ie<D>(e, cc);
-      const long long src = sSrc[k];
-      double qf = 1.0;
-      if (src >= 0) {
-        const double v = Uk[f * nc + src];
-        qf = ((sFlip[k] >> f) & 1) ? -v : v;
-      }
-      const double rho = sP[k], u = sP[EA + k], v = sP[2 * EA + k], p = sP[3 * EA + k];
-      const double un = D == 0 ? u : v;
-      double F;
-      if (f == 0) F = rho * un;
-      else if (f == dirf) F = rho * un * un + p;
-      else if (f == 3 - dirf) F = rho * u * v;
-      else if (f == 3) F = un * (qf + p);
-      else F = rho * un * (qf / rho);
-      sQ[k] = qf;
-      sHp[k] = 0.5 * (F + alpha * qf);
-      sHm[k] = 0.5 * (F - alpha * qf);
-    }
-    __syncthreads();
-    // faces: adjoint of the face flux and the WENO partials
-    for (int i = tid; i < NF * TA; i += 256) {
-      const int fl = D == 0 ? i / TA : i % NF, cc = D == 0 ? i % TA : i / NF;
-      const int fa = a0 - 2 + fl;  // face between cells fa-1 and fa
-      const int cidx = c0 + cc;
-      double Lm = 0.0, Lp = 0.0;
-      if (cidx < nC) {
-        if (fa - 1 >= 0 && fa - 1 < nA) {
-          const long long cl = D == 0 ? (long long)(fa - 1) * g.ny + cidx : (long long)cidx * g.ny + (fa - 1);
-          Lm = coef * dt * Uo_b[f * nc + cl];
-        }
-        if (fa >= 0 && fa < nA) {
-          const long long cr = D == 0 ? (long long)fa * g.ny + cidx : (long long)cidx * g.ny + fa;
-          Lp = coef * dt * Uo_b[f * nc + cr];
-        }
-      }
-      // L_i = -(F_{i+1} - F_i) / d  ->  Fbar_f = (Lbar_f - Lbar_{f-1}) / d
-      const double Fb_face = (Lp - Lm) / dA;
-      double dl[5], dr[5];
-      const double vl = weno_d(sHp[ie<D>(fl, cc)], sHp[ie<D>(fl + 1, cc)], sHp[ie<D>(fl + 2, cc)],
-                               sHp[ie<D>(fl + 3, cc)], sHp[ie<D>(fl + 4, cc)], dl);
-      // right-biased: the left form of the mirrored stencil (cells fa+2 .. fa-2)
-      const double vr = weno_d(sHm[ie<D>(fl + 5, cc)], sHm[ie<D>(fl + 4, cc)], sHm[ie<D>(fl + 3, cc)],
-                               sHm[ie<D>(fl + 2, cc)], sHm[ie<D>(fl + 1, cc)], dr);
-      const int kf = iff<D>(fl, cc);
-      sFv[kf] = vl + vr;
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        sPL[j * FA + kf] = Fb_face * dl[j];      // cell fa-3+j
-        sPR[j * FA + kf] = Fb_face * dr[4 - j];  // cell fa-2+j
-      }
-    }
-    __syncthreads();
-    if (owned) {
-      const int o = tA;
-      double hp = 0.0, hm = 0.0;
-#pragma unroll
-      for (int d = -1; d <= 3; ++d) hp += sPL[(3 - d) * FA + iff<D>(o + d + 2, tC)];
-#pragma unroll
-      for (int d = -2; d <= 2; ++d) hm += sPR[(2 - d) * FA + iff<D>(o + d + 2, tC)];
-      const double qf = sQ[ie<D>(o + 5, tC)];
-      Fb[f] = 0.5 * (hp + hm);
-      Ua[f] = 0.5 * alpha * (hp - hm);
-      ab += 0.5 * qf * (hp - hm);
-      if (interior) {
-        const double Lphys = -(sFv[iff<D>(o + 3, tC)] - sFv[iff<D>(o + 2, tC)]) / dA;
-        dtb += Lphys * coef * Uo_b[f * nc + cell];
-      }
-    }
-    __syncthreads();
-  }
-  if (owned) {
-    // flux function VJP of this padded cell
-    const int k = ie<D>(tA + 5, tC);
-    const double rho = sP[k], u = sP[EA + k], v = sP[2 * EA + k], p = sP[3 * EA + k];
-    const double un = D == 0 ? u : v, ut = D == 0 ? v : u;
-    // the padded cell's own state (flipped for ghosts) for rho E and Y
-    const long long src = sSrc[k] >= 0 ? sSrc[k] : 0;
-    const int flip = sFlip[k];
-    double q[12];
-#pragma unroll
-    for (int f = 0; f < 12; ++f) {
-      const double vv = Uk[f * nc + src];
-      q[f] = ((flip >> f) & 1) ? -vv : vv;
-    }
-    const double T = Ak[nc + src];
-    const double ri = 1.0 / rho;
-    double Y8[NR], Yf[NS];
-    cell_Y(q, ri, Y8, Yf);
-    const double R = get_R(m, Yf);
-    const int mn = dirf, mt = 3 - dirf;
-    double rb = Fb[0] * un + Fb[mn] * un * un + Fb[mt] * u * v;
-    double unb = Fb[0] * rho + Fb[mn] * 2.0 * rho * un + Fb[mt] * rho * ut + Fb[3] * (q[3] + p);
-    double utb = Fb[mt] * rho * un;
-    const double pb = Fb[mn] + Fb[3] * un;
-    double ub[12];
-#pragma unroll
-    for (int f = 0; f < 12; ++f) ub[f] = Ua[f];
-    ub[3] += Fb[3] * un;
-    double Yb[NR];
-#pragma unroll
-    for (int kk = 0; kk < NR; ++kk) {
-      rb += Fb[4 + kk] * un * Y8[kk];
-      unb += Fb[4 + kk] * rho * Y8[kk];
-      Yb[kk] = Fb[4 + kk] * rho * un;
-    }
-    rb += pb * R * T;
-    const double Rb = pb * rho * T;
-    const double Tb = pb * rho * R;
-#pragma unroll
-    for (int kk = 0; kk < NR; ++kk) Yb[kk] += Rb * (m.invM[kk] - m.invM[NR]);
-    const double ubx = D == 0 ? unb : utb, uby = D == 0 ? utb : unb;
-    ub[1] += ubx * ri;
-    ub[2] += uby * ri;
-    rb -= ubx * u * ri + uby * v * ri;
-#pragma unroll
-    for (int kk = 0; kk < NR; ++kk) {
-      ub[4 + kk] += Yb[kk] * ri;
-      rb -= Yb[kk] * Y8[kk] * ri;
-    }
-    ub[0] += rb;
-    if (interior) {
-#pragma unroll
-      for (int f = 0; f < 12; ++f) {
-        double val = ub[f];
-        if (D == 0) {
-          const double uo = Uo_b[f * nc + cell];
-          // the RK combination, once per cell and stage
-          if (Un_b) Un_b[f * nc + cell] += un_coef * uo;
-          val += coef * uo;
-        }
-        if (D == 0) Ub[f * nc + cell] += val;
-        else Ub[f * nc + cell] = val;
-      }
-      if (D == 0) Abk[nc + cell] += Tb;
-      else Abk[cell] = Tb;
-    } else {
-      // ghost entry: side, layer, position
-      const int side = D == 0 ? (ao < 0 ? 0 : 1) : (ao < 0 ? 2 : 3);
-      const int layer = ao < 0 ? -1 - ao : ao - nA;
-      const int L = g.nx > g.ny ? g.nx : g.ny;
-      double* gp = ghost + ((size_t)(side * 3 + layer) * 13) * L + co;
-#pragma unroll
-      for (int f = 0; f < 12; ++f) gp[(size_t)f * L] = ub[f];
-      gp[(size_t)12 * L] = Tb;
-    }
-  }
-  block_add(ab, red + (D == 0 ? 0 : 1));
-  block_add(dtb, red + 2);
-}
-
-// Both directions of one RK stage in one launch: blocks [0, nbx) are x-face
-// tiles (a grid of gxx tiles along x), the rest y-face tiles (gyy along y).
-__global__ void __launch_bounds__(256, 3) k_flux_vjp(MP m, Grid g, const double* __restrict__ Uk,
-                                                 const double* __restrict__ Ak, const double* __restrict__ Uo_b,
-                                                 double coef, const double* __restrict__ slots_rec, int stage,
-                                                 double* Ub, double* Abk, double* Ub2, double* Ab2, double* Un_b,
-                                                 double un_coef, double* ghost, double* red, int nbx, int gxx,
-                                                 int gyy) {
-  const int b = blockIdx.x;
-  if (b < nbx)
-    flux_vjp_body<0>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, Ub, Abk, Un_b, un_coef, ghost, red, b % gxx,
-                     b / gxx);
-  else
-    flux_vjp_body<1>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, Ub2, Ab2, nullptr, 0.0, ghost, red,
-                     (b - nbx) % gyy, (b - nbx) / gyy);
-}
-
-// Per interior cell: add the y-face adjoints (Ub2, Ab2) and gather the
-// adjoints of the ghost entries that copy this cell (the boundary map of
-// every side, with the normal-momentum flips undone).
-__global__ void k_flux_merge(Grid g, const double* __restrict__ ghost, const double* __restrict__ Ub2,
-                             const double* __restrict__ Ab2, double* Ub, double* Ab) {
-  const long long nc = g.ncell;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
-  const int x = (int)(c / g.ny), y = (int)(c % g.ny);
-  const int L = g.nx > g.ny ? g.nx : g.ny;
-  double ub[12];
-#pragma unroll
-  for (int f = 0; f < 12; ++f) ub[f] = Ub2[f * nc + c];
-  double tb = Ab2[c];
-  for (int side = 0; side < 4; ++side) {
-    const int pos = side < 2 ? y : x;
-    for (int layer = 0; layer < 3; ++layer) {
-      const int gx = side == 0 ? -1 - layer : side == 1 ? g.nx + layer : x;
-      const int gy = side == 2 ? -1 - layer : side == 3 ? g.ny + layer : y;
-      Src s = map_cell<2>(g, gx, gy);
-      if (s.kind != 0 || s.xs != x || s.ys != y) continue;
-      const double* gp = ghost + ((size_t)(side * 3 + layer) * 13) * L + pos;
-#pragma unroll
-      for (int f = 0; f < 12; ++f) {
-        const double v = gp[(size_t)f * L];
-        ub[f] += ((s.flip >> f) & 1) ? -v : v;
-      }
-      tb += gp[(size_t)12 * L];
-    }
-  }
-#pragma unroll
-  for (int f = 0; f < 12; ++f) Ub[f * nc + c] += ub[f];
-  Ab[nc + c] += tb;
-}
-
-// ---------------------------------------------------------------------------
 // alpha (max over the padded grid) and CFL (min over cells) ties
 // ---------------------------------------------------------------------------
 struct Speeds {
   double sx, sy, d;
 };
 
-__device__ __forceinline__ Speeds speeds(const MP& m, const Grid& g, const double* q, double gamma, double T) {
-  Prim<2> pr = u_to_prim<2>(m, q, gamma, T);
+__device__ __forceinline__ Speeds speeds_of(const Grid& g, const Prim<2>& pr) {
   Speeds s;
   s.sx = fabs(pr.u) + pr.a;
   s.sy = fabs(pr.v) + pr.a;
@@ -845,101 +523,378 @@ __device__ __forceinline__ Speeds speeds(const MP& m, const Grid& g, const doubl
 
 __device__ __forceinline__ bool tied(double v, double ref) { return fabs(v - ref) <= TIE_REL * fabs(ref); }
 
-// red layout (doubles): [0] abar_x, [1] abar_y, [2] dtbar, [3] nx ties, [4] ny ties, [5] n CFL ties
-__global__ void k_speed_count(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ A,
-                              const unsigned char* __restrict__ mult, const double* __restrict__ slots_rec,
-                              int stage, double cfl, double* red) {
-  const long long nc = g.ncell;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double cx = 0.0, cy = 0.0, cd = 0.0;
-  if (c < nc) {
-    const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
-    double q[12];
-#pragma unroll
-    for (int f = 0; f < 12; ++f) q[f] = U[f * nc + c];
-    Speeds s = speeds(m, g, q, A[c], A[nc + c]);
-    if (tied(s.sx, bitsd(rs->ax[stage]))) cx = mult[c];
-    if (tied(s.sy, bitsd(rs->ay[stage]))) cy = mult[c];
-    if (cfl > 0.0 && tied(s.d, rs->dt / cfl)) cd = 1.0;
-  }
-  block_add(cx, red + 3);
-  block_add(cy, red + 4);
-  block_add(cd, red + 5);
-}
-
-// UPD: then the update_aux VJP of the same state with the completed aux
-// adjoint (consumed and zeroed), as k_upd_vjp.
-template <bool UPD>
-__global__ void k_speed_scatter(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ A,
-                                const unsigned char* __restrict__ mult, const double* __restrict__ slots_rec,
-                                int stage, double cfl, const double* __restrict__ red, double* Ub, double* Ab) {
-  const long long nc = g.ncell;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nc) return;
-  const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
-  double q[12];
-#pragma unroll
-  for (int f = 0; f < 12; ++f) q[f] = U[f * nc + c];
-  const double gamma = A[c], T = A[nc + c];
-  Speeds s = speeds(m, g, q, gamma, T);
-  double wx = 0.0, wy = 0.0;
-  if (red[3] > 0.0 && tied(s.sx, bitsd(rs->ax[stage]))) wx = red[0] * mult[c] / red[3];
-  if (red[4] > 0.0 && tied(s.sy, bitsd(rs->ay[stage]))) wy = red[1] * mult[c] / red[4];
-  if (cfl > 0.0 && red[5] > 0.0 && tied(s.d, rs->dt / cfl)) {
-    const double db = cfl * red[2] / red[5];
-    wx += -db * s.d * s.d / g.dx;
-    wy += -db * s.d * s.d / g.dy;
-  }
-  double gb = UPD ? Ab[c] : 0.0, Tb = UPD ? Ab[nc + c] : 0.0;
-  if (wx == 0.0 && wy == 0.0 && gb == 0.0 && Tb == 0.0) return;
-  double ub[12];
-#pragma unroll
-  for (int f = 0; f < 12; ++f) ub[f] = 0.0;
-  speed_vjp(m, q, gamma, T, 1, wx, ub, gb, Tb);
-  speed_vjp(m, q, gamma, T, 2, wy, ub, gb, Tb);
-  if (UPD) {
-    upd_vjp(m, q, T, gb, Tb, ub);
-    Ab[c] = 0.0;
-    Ab[nc + c] = 0.0;
-  } else {
-    Ab[c] += gb;
-    Ab[nc + c] += Tb;
-  }
-#pragma unroll
-  for (int f = 0; f < 12; ++f) Ub[f * nc + c] += ub[f];
-}
-
 // ---------------------------------------------------------------------------
-// loss seed: L += dt_n * mean probe p(U_{n+1}); red[2] (dtbar) += dt_bar_ext
+// the probe term of the loss: L += dt_n * mean probe p(U_{n+1}), p = rho R T
 // ---------------------------------------------------------------------------
-__global__ void k_probe_seed(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ A,
-                             const double* __restrict__ pp_bar, int px, int py, int wx, int wy, double* Ub,
-                             double* Ab) {
-  const int t = threadIdx.x;
-  if (t >= wx * wy || !pp_bar) return;
-  const long long nc = g.ncell;
-  const long long c = (long long)(px + t / wy) * g.ny + (py + t % wy);
-  const double w = *pp_bar / (double)(wx * wy);
-  if (w == 0.0) return;
-  double q[12];
-#pragma unroll
-  for (int f = 0; f < 12; ++f) q[f] = U[f * nc + c];
-  const double T = A[nc + c];
+__device__ __forceinline__ void probe_vjp(const MP& m, const double* q, double T, double w, double* ub, double& Tb) {
   const double rho = q[0], ri = 1.0 / rho;
   double Y8[NR], Yf[NS];
   cell_Y(q, ri, Y8, Yf);
   const double R = get_R(m, Yf);
-  // p = rho R T, R = sum Yf / M
   double rb = w * R * T;
   const double Rb = w * rho * T;
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
     const double yb = Rb * (m.invM[k] - m.invM[NR]);
-    Ub[(4 + k) * nc + c] += yb * ri;
+    ub[4 + k] += yb * ri;
     rb -= yb * Y8[k] * ri;
   }
-  Ub[c] += rb;
-  Ab[nc + c] += w * rho * R;
+  ub[0] += rb;
+  Tb += w * rho * R;
+}
+
+// Start of one adjoint step, one thread per cell: the probe term and the
+// update_aux VJP of U4 (the aux adjoint is consumed and cleared), the
+// primitives (rho, u, v, p) of the three stage states U, U1, U2, and the
+// alpha and CFL tie counts of the three stages.
+__global__ void __launch_bounds__(128) k_vjp_begin(MP m, Grid g, const double* __restrict__ U4,
+                                                   const double* __restrict__ A4, const double* __restrict__ pp_bar,
+                                                   int px, int py, int wx, int wy, double* Ub, double* Ab,
+                                                   const double* __restrict__ rec, double* prims,
+                                                   const unsigned char* __restrict__ mult,
+                                                   const double* __restrict__ slots_rec, double cfl, double* red) {
+  const long long nc = g.ncell, nU = 12 * nc;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double cnt[7];
+#pragma unroll
+  for (int i = 0; i < 7; ++i) cnt[i] = 0.0;
+  if (c < nc) {
+    const int x = (int)(c / g.ny), y = (int)(c % g.ny);
+    double q[12], ub[12];
+    double gb = Ab[c], Tb = Ab[nc + c];
+#pragma unroll
+    for (int f = 0; f < 12; ++f) ub[f] = 0.0;
+    const bool in_probe = pp_bar && x >= px && x < px + wx && y >= py && y < py + wy;
+    if (in_probe || gb != 0.0 || Tb != 0.0) {
+#pragma unroll
+      for (int f = 0; f < 12; ++f) q[f] = U4[f * nc + c];
+      const double T = A4[nc + c];
+      if (in_probe) probe_vjp(m, q, T, *pp_bar / (double)(wx * wy), ub, Tb);
+      upd_vjp(m, q, T, gb, Tb, ub);
+#pragma unroll
+      for (int f = 0; f < 12; ++f) Ub[f * nc + c] += ub[f];
+      Ab[c] = 0.0;
+      Ab[nc + c] = 0.0;
+    }
+    const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
+#pragma unroll 1
+    for (int s = 0; s < 3; ++s) {
+      const double* S = rec + (long long)s * (nU + 2 * nc);
+      const double* A = S + nU;
+#pragma unroll
+      for (int f = 0; f < 12; ++f) q[f] = S[f * nc + c];
+      const Prim<2> pr = u_to_prim<2>(m, q, A[c], A[nc + c]);
+      double* P = prims + (long long)s * 4 * nc;
+      P[c] = pr.rho;
+      P[nc + c] = pr.u;
+      P[2 * nc + c] = pr.v;
+      P[3 * nc + c] = pr.p;
+      const Speeds sp = speeds_of(g, pr);
+      if (tied(sp.sx, bitsd(rs->ax[s]))) cnt[2 * s] = mult[c];
+      if (tied(sp.sy, bitsd(rs->ay[s]))) cnt[2 * s + 1] = mult[c];
+      if (s == 0 && cfl > 0.0 && tied(sp.d, rs->dt / cfl)) cnt[6] = 1.0;
+    }
+  }
+#pragma unroll 1
+  for (int s = 0; s < 3; ++s) {
+    block_add(cnt[2 * s], red + red_cnt(s, 0));
+    block_add(cnt[2 * s + 1], red + red_cnt(s, 1));
+  }
+  block_add(cnt[6], red + red_cnt(0, 2));
+}
+
+// ---------------------------------------------------------------------------
+// flux VJP of one RK stage: line sweeps, then a per-cell merge
+// ---------------------------------------------------------------------------
+// The sweep thread of (direction D, line, segment, field f) owns SW_R
+// consecutive padded cells of the line (ghosts included) and walks the
+// faces that touch them, keeping a six-cell window of H+, H- and the field
+// in registers: per face the two WENO5 reconstructions and their partials,
+// scaled by the face-flux adjoint, accumulate into the window's cells, and a
+// cell whose five + five contributions are complete is written out as the
+// adjoint of its physical flux (Fb) and its LF term (Ua = alpha/2 (h+ - h-)).
+// Only faces 0..n carry a flux into the interior, so faces outside are
+// skipped.  No shared memory and no barriers: one thread's faces are
+// independent of the other threads'.
+constexpr int SW_R = 24;
+constexpr int SW_NT = 128;
+
+// H+ and H- of field f at padded cell a of a line, from the stage state and
+// its primitives (those of the source cell; ghosts flip the momentum).
+template <int D>
+__device__ __forceinline__ void sweep_load(const Grid& g, const double* __restrict__ Uk,
+                                           const double* __restrict__ Pk, int f, int line, int a, double alpha,
+                                           double& hp, double& hm, double& qv) {
+  const Src s = map_cell<2>(g, D == 0 ? a : line, D == 0 ? line : a);
+  const long long nc = g.ncell, src = (long long)s.xs * g.ny + s.ys;
+  double qf = Uk[f * nc + src];
+  if ((s.flip >> f) & 1) qf = -qf;
+  const double rho = Pk[src], p = Pk[3 * nc + src];
+  double u = Pk[nc + src], v = Pk[2 * nc + src];
+  if (s.flip & 2) u = -u;
+  if (s.flip & 4) v = -v;
+  const double un = D == 0 ? u : v;
+  constexpr int mn = D == 0 ? 1 : 2;
+  double F;
+  if (f == 0) F = rho * un;
+  else if (f == mn) F = rho * un * un + p;
+  else if (f == 3 - mn) F = rho * u * v;
+  else if (f == 3) F = un * (qf + p);
+  else F = un * qf;
+  hp = 0.5 * (F + alpha * qf);
+  hm = 0.5 * (F - alpha * qf);
+  qv = qf;
+}
+
+template <int D>
+__device__ __forceinline__ void sweep_body(const Grid& g, const double* __restrict__ Uk,
+                                           const double* __restrict__ Pk, const double* __restrict__ Uo_b,
+                                           double coef, double alpha, double dt, int f, int line, int seg,
+                                           double* __restrict__ Fb, double* __restrict__ Ua, double& ab,
+                                           double& dtb) {
+  const int nA = D == 0 ? g.nx : g.ny;
+  const long long nc = g.ncell;
+  const double dA = D == 0 ? g.dx : g.dy;
+  const int a0 = -3 + seg * SW_R, a1 = min(a0 + SW_R, nA + 3);  // owned padded cells [a0, a1)
+  const int flo = max(a0 - 2, 0), fhi = min(a1 + 2, nA);        // faces touching them
+  const size_t npad = D == 0 ? (size_t)(g.nx + 6) * g.ny : (size_t)g.nx * (g.ny + 6);
+  const double* ob = Uo_b + f * nc;
+  double* fbo = Fb + f * npad;
+  double* uao = Ua + f * npad;
+  // adjoint of L at cell a of the line, without dt (zero outside the interior)
+  auto lbar = [&](int a) -> double {
+    if (a < 0 || a >= nA) return 0.0;
+    return coef * ob[D == 0 ? (long long)a * g.ny + line : (long long)line * g.ny + a];
+  };
+  auto emit = [&](int a, double ap, double am, double qv) {
+    ab += 0.5 * qv * (ap - am);
+    const size_t k = D == 0 ? (size_t)(a + 3) * g.ny + line : (size_t)line * (g.ny + 6) + (a + 3);
+    fbo[k] = 0.5 * (ap + am);
+    uao[k] = 0.5 * alpha * (ap - am);
+  };
+  // window slot k holds padded cell fa - 3 + k while face fa is processed
+  double Hp[6], Hm[6], Q[6], Ap[6], Am[6];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    sweep_load<D>(g, Uk, Pk, f, line, flo - 3 + k, alpha, Hp[k], Hm[k], Q[k]);
+    Ap[k] = 0.0;
+    Am[k] = 0.0;
+  }
+  Ap[5] = 0.0;
+  Am[5] = 0.0;
+  double lbm = lbar(flo - 1), Fprev = 0.0;
+#pragma unroll 1
+  for (int fa = flo; fa <= fhi; ++fa) {
+    sweep_load<D>(g, Uk, Pk, f, line, fa + 2, alpha, Hp[5], Hm[5], Q[5]);
+    const double lbp = lbar(fa);
+    // L_i = -(F_{i+1} - F_i) / d  ->  Fbar_fa = dt (Lbar_fa - Lbar_{fa-1}) / d
+    const double Fbf = dt * (lbp - lbm) / dA;
+    double dl[5], dr[5];
+    const double vl = weno_d(Hp[0], Hp[1], Hp[2], Hp[3], Hp[4], dl);
+    // right-biased: the left form of the mirrored stencil (cells fa+2 .. fa-2)
+    const double vr = weno_d(Hm[5], Hm[4], Hm[3], Hm[2], Hm[1], dr);
+    const double Fv = vl + vr;
+    // dt adjoint: L of the owned interior cell fa-1, both of its faces known
+    const int ci = fa - 1;
+    if (fa > flo && ci >= a0 && ci < a1 && ci >= 0 && ci < nA) dtb -= (Fv - Fprev) / dA * lbm;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      Ap[j] += Fbf * dl[j];          // cell fa-3+j
+      Am[j + 1] += Fbf * dr[4 - j];  // cell fa-2+j
+    }
+    // cell fa-3 has all of its contributions (faces fa-5 .. fa)
+    if (fa - 3 >= a0 && fa - 3 < a1) emit(fa - 3, Ap[0], Am[0], Q[0]);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      Hp[k] = Hp[k + 1];
+      Hm[k] = Hm[k + 1];
+      Q[k] = Q[k + 1];
+      Ap[k] = Ap[k + 1];
+      Am[k] = Am[k + 1];
+    }
+    Ap[5] = 0.0;
+    Am[5] = 0.0;
+    lbm = lbp;
+    Fprev = Fv;
+  }
+  // owned cells past the last face (it was clipped at the boundary): slot k
+  // now holds cell fhi - 2 + k
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const int a = fhi - 2 + k;
+    if (a >= a0 && a < a1) emit(a, Ap[k], Am[k], Q[k]);
+  }
+}
+
+// Both directions of one RK stage: blocks [0, nbx) sweep x lines (SW_NT
+// consecutive y per block), the rest y lines (SW_NT consecutive x); the
+// field runs fastest over blocks, then the line block, then the segment.
+__global__ void __launch_bounds__(SW_NT, 4) k_flux_sweep(Grid g, const double* __restrict__ Uk,
+                                                      const double* __restrict__ Pk,
+                                                      const double* __restrict__ Uo_b, double coef,
+                                                      const double* __restrict__ slots_rec, int stage, double* FbX,
+                                                      double* UaX, double* FbY, double* UaY, double* red, int nbx,
+                                                      int nlx, int nly) {
+  const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
+  int b = blockIdx.x;
+  const int D = b < nbx ? 0 : 1;
+  if (D) b -= nbx;
+  const int f = b % 12;
+  b /= 12;
+  const int nl = D == 0 ? nlx : nly;
+  const int line = (b % nl) * SW_NT + threadIdx.x, seg = b / nl;
+  double ab = 0.0, dtb = 0.0;
+  if (D == 0) {
+    if (line < g.ny)
+      sweep_body<0>(g, Uk, Pk, Uo_b, coef, bitsd(rs->ax[stage]), rs->dt, f, line, seg, FbX, UaX, ab, dtb);
+  } else {
+    if (line < g.nx)
+      sweep_body<1>(g, Uk, Pk, Uo_b, coef, bitsd(rs->ay[stage]), rs->dt, f, line, seg, FbY, UaY, ab, dtb);
+  }
+  block_add(ab, red + red_ab(stage, D));
+  block_add(dtb, red + RED_DTB);
+}
+
+// ub, Tb += the VJP of the direction-D physical flux F(q, T) (rho un, rho un
+// u + p e_n, un (rho E + p), rho un Y) with adjoint Fb.
+template <int D>
+__device__ __forceinline__ void flux_fn_vjp(const MP& m, const double* q, double T, const double* Fb, double* ub,
+                                            double& Tb) {
+  const double rho = q[0], ri = 1.0 / rho;
+  const double u = q[1] * ri, v = q[2] * ri;
+  double Y8[NR], Yf[NS];
+  cell_Y(q, ri, Y8, Yf);
+  const double R = get_R(m, Yf);
+  const double p = rho * R * T;
+  const double un = D == 0 ? u : v, ut = D == 0 ? v : u;
+  constexpr int mn = D == 0 ? 1 : 2, mt = 3 - mn;
+  double rb = Fb[0] * un + Fb[mn] * un * un + Fb[mt] * u * v;
+  double unb = Fb[0] * rho + Fb[mn] * 2.0 * rho * un + Fb[mt] * rho * ut + Fb[3] * (q[3] + p);
+  const double utb = Fb[mt] * rho * un;
+  const double pb = Fb[mn] + Fb[3] * un;
+  ub[3] += Fb[3] * un;
+  double Yb[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    rb += Fb[4 + k] * un * Y8[k];
+    unb += Fb[4 + k] * rho * Y8[k];
+    Yb[k] = Fb[4 + k] * rho * un;
+  }
+  rb += pb * R * T;
+  const double Rb = pb * rho * T;
+  Tb += pb * rho * R;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Yb[k] += Rb * (m.invM[k] - m.invM[NR]);
+  const double ubx = D == 0 ? unb : utb, uby = D == 0 ? utb : unb;
+  ub[1] += ubx * ri;
+  ub[2] += uby * ri;
+  rb -= ubx * u * ri + uby * v * ri;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    ub[4 + k] += Yb[k] * ri;
+    rb -= Yb[k] * Y8[k] * ri;
+  }
+  ub[0] += rb;
+}
+
+// The ghost entries of the two direction-D sides that copy interior cell
+// (x, y): their flux-function VJP at the ghost state (flipped momentum), with
+// the flips undone on the way back.
+template <int D>
+__device__ __forceinline__ void merge_ghosts(const MP& m, const Grid& g, const double* q, double T, int x, int y,
+                                             const double* __restrict__ Fb, const double* __restrict__ Ua,
+                                             double* ub, double& Tb) {
+  const int nA = D == 0 ? g.nx : g.ny;
+  const size_t npad = D == 0 ? (size_t)(g.nx + 6) * g.ny : (size_t)g.nx * (g.ny + 6);
+#pragma unroll 1
+  for (int i = 0; i < 6; ++i) {
+    const int a = i < 3 ? -1 - i : nA + i - 3;
+    const Src s = map_cell<2>(g, D == 0 ? a : x, D == 0 ? y : a);
+    if (s.kind != 0 || s.xs != x || s.ys != y) continue;
+    const size_t k = D == 0 ? (size_t)(a + 3) * g.ny + y : (size_t)x * (g.ny + 6) + (a + 3);
+    double qg[12], ug[12], fb[12];
+#pragma unroll
+    for (int f = 0; f < 12; ++f) {
+      qg[f] = ((s.flip >> f) & 1) ? -q[f] : q[f];
+      ug[f] = Ua[f * npad + k];
+      fb[f] = Fb[f * npad + k];
+    }
+    flux_fn_vjp<D>(m, qg, T, fb, ug, Tb);
+#pragma unroll
+    for (int f = 0; f < 12; ++f) ub[f] += ((s.flip >> f) & 1) ? -ug[f] : ug[f];
+  }
+}
+
+// One RK stage U' = a Un + b (Uk + dt L(Uk, auxk)), per interior cell of Uk:
+// the sweeps' LF terms of the cell and of the ghost entries that copy it,
+// the flux-function VJPs of both directions, the RK combination (Ubar_k +=
+// b Ubar', Ubar_n += a Ubar'), the alpha ties of the stage (and for stage 0
+// the CFL ties of dt), then either the update_aux VJP of Uk with its
+// completed aux adjoint (Ab null) or the aux adjoint itself added to Ab.
+// ub_add / un_add: add to Ub / Un_b instead of storing.
+__global__ void __launch_bounds__(128) k_stage_merge(
+    MP m, Grid g, const double* __restrict__ Uk, const double* __restrict__ Ak, const double* __restrict__ Uo_b,
+    double coef, const double* __restrict__ slots_rec, int stage, double cfl, const unsigned char* __restrict__ mult,
+    const double* __restrict__ red, const double* __restrict__ dt_bar_ext, const double* __restrict__ FbX,
+    const double* __restrict__ UaX, const double* __restrict__ FbY, const double* __restrict__ UaY, double* Ub,
+    int ub_add, double* Ab, double* Un_b, double un_coef, int un_add) {
+  const long long nc = g.ncell;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const int x = (int)(c / g.ny), y = (int)(c % g.ny);
+  double q[12], ub[12], fb[12];
+#pragma unroll
+  for (int f = 0; f < 12; ++f) q[f] = Uk[f * nc + c];
+  const double gamma = Ak[c], T = Ak[nc + c];
+  double Tb = 0.0, gb = 0.0;
+  {
+    const size_t npx = (size_t)(g.nx + 6) * g.ny, npy = (size_t)g.nx * (g.ny + 6);
+    const size_t ix = (size_t)(x + 3) * g.ny + y, iy = (size_t)x * (g.ny + 6) + y + 3;
+#pragma unroll
+    for (int f = 0; f < 12; ++f) {
+      ub[f] = UaX[f * npx + ix] + UaY[f * npy + iy];
+      fb[f] = FbX[f * npx + ix];
+    }
+    flux_fn_vjp<0>(m, q, T, fb, ub, Tb);
+#pragma unroll
+    for (int f = 0; f < 12; ++f) fb[f] = FbY[f * npy + iy];
+    flux_fn_vjp<1>(m, q, T, fb, ub, Tb);
+  }
+  // only cells within four of a side are copied into ghosts
+  if (x < 4 || x >= g.nx - 4) merge_ghosts<0>(m, g, q, T, x, y, FbX, UaX, ub, Tb);
+  if (y < 4 || y >= g.ny - 4) merge_ghosts<1>(m, g, q, T, x, y, FbY, UaY, ub, Tb);
+#pragma unroll
+  for (int f = 0; f < 12; ++f) {
+    const double uo = Uo_b[f * nc + c];
+    ub[f] += coef * uo;
+    if (Un_b) Un_b[f * nc + c] = (un_add ? Un_b[f * nc + c] : 0.0) + un_coef * uo;
+  }
+  // alpha ties (evenly over the tied padded entries) and the CFL ties of dt
+  const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
+  const Prim<2> pr = u_to_prim<2>(m, q, gamma, T);
+  const Speeds sp = speeds_of(g, pr);
+  double wx = 0.0, wy = 0.0;
+  const double cx = red[red_cnt(stage, 0)], cy = red[red_cnt(stage, 1)];
+  if (cx > 0.0 && tied(sp.sx, bitsd(rs->ax[stage]))) wx = red[red_ab(stage, 0)] * mult[c] / cx;
+  if (cy > 0.0 && tied(sp.sy, bitsd(rs->ay[stage]))) wy = red[red_ab(stage, 1)] * mult[c] / cy;
+  if (stage == 0 && cfl > 0.0) {
+    const double cd = red[red_cnt(0, 2)];
+    if (cd > 0.0 && tied(sp.d, rs->dt / cfl)) {
+      const double db = cfl * (red[RED_DTB] + (dt_bar_ext ? *dt_bar_ext : 0.0)) / cd;
+      wx += -db * sp.d * sp.d / g.dx;
+      wy += -db * sp.d * sp.d / g.dy;
+    }
+  }
+  speed_vjp(m, q, gamma, T, 1, wx, ub, gb, Tb);
+  speed_vjp(m, q, gamma, T, 2, wy, ub, gb, Tb);
+  if (Ab) {
+    Ab[c] += gb;
+    Ab[nc + c] += Tb;
+  } else {
+    upd_vjp(m, q, T, gb, Tb, ub);
+  }
+#pragma unroll
+  for (int f = 0; f < 12; ++f) Ub[f * nc + c] = (ub_add ? Ub[f * nc + c] : 0.0) + ub[f];
 }
 
 // mean pressure over the probe rectangle (one block)
@@ -967,18 +922,6 @@ __global__ void k_probe_mean(MP m, Grid g, const double* __restrict__ U, const d
     for (int i = 0; i < (int)(blockDim.x + 31) / 32; ++i) t += red[i];
     *out = t / (double)(wx * wy);
   }
-}
-
-__global__ void k_adj_begin(double* red, const double* __restrict__ dt_bar_ext) {
-  for (int i = 0; i < 8; ++i) red[i] = 0.0;
-  if (dt_bar_ext) red[2] = *dt_bar_ext;
-}
-
-__global__ void k_adj_clear_alpha(double* red) {
-  red[0] = 0.0;
-  red[1] = 0.0;
-  red[3] = 0.0;
-  red[4] = 0.0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1018,9 +961,13 @@ namespace adj {
 
 static inline unsigned blocks_for(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
-cudaError_t upd_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A, double* Ub,
-                    double* Ab, cudaStream_t st) {
-  k_upd_vjp<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U, A, Ub, Ab);
+cudaError_t vjp_begin(const jb_mech_params& m, const jb_grid& g, const double* U4, const double* A4,
+                      const double* pp_bar, const int* probe, double* Ub, double* Ab, const double* rec,
+                      double* prims, const unsigned char* mult, const double* slots_rec, double cfl, double* red,
+                      cudaStream_t st) {
+  k_vjp_begin<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U4, A4, probe[2] * probe[3] > 0 ? pp_bar : nullptr,
+                                                        probe[0], probe[1], probe[2], probe[3], Ub, Ab, rec, prims,
+                                                        mult, slots_rec, cfl, red);
   return cudaGetLastError();
 }
 
@@ -1034,58 +981,33 @@ cudaError_t chem_vjp(const jb_mech_params& m, const jb_grid& g, const double* U3
   return cudaGetLastError();
 }
 
-constexpr size_t FLUX_VJP_SMEM = sizeof(double) * (7 * EA + 11 * FA) + (sizeof(long long) + sizeof(int)) * EA;
-
-cudaError_t flux_vjp(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
-                     const double* Uo_b, double coef, const double* slots_rec, int stage, double* Ub, double* Abk,
-                     double* Un_b, double un_coef, double* ghost, double* Ub2, double* Ab2, double* red,
-                     cudaStream_t st) {
-  cudaError_t e = cudaFuncSetAttribute(k_flux_vjp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FLUX_VJP_SMEM);
-  if (e != cudaSuccess) return e;
-  const int gxx = (g.nx + 6 + TO - 1) / TO, gxy = (g.ny + TA - 1) / TA;
-  const int gyy = (g.ny + 6 + TO - 1) / TO, gyx = (g.nx + TA - 1) / TA;
-  const int nbx = gxx * gxy, nby = gyy * gyx;
-  k_flux_vjp<<<nbx + nby, dim3(16, 16), FLUX_VJP_SMEM, st>>>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, Ub, Abk, Ub2,
-                                                             Ab2, Un_b, un_coef, ghost, red, nbx, gxx, gyy);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_flux_merge<<<blocks_for(g.ncell, 128), 128, 0, st>>>(g, ghost, Ub2, Ab2, Ub, Abk);
-  return cudaGetLastError();
+size_t flux_scratch_doubles(const jb_grid& g) {
+  return 2 * 12 * ((size_t)(g.nx + 6) * g.ny + (size_t)g.nx * (g.ny + 6));
 }
 
-cudaError_t speed_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A,
-                      const unsigned char* mult, const double* slots_rec, int stage, double cfl, double* red,
-                      double* Ub, double* Ab, bool upd, cudaStream_t st) {
-  k_speed_count<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U, A, mult, slots_rec, stage, cfl, red);
+cudaError_t flux_stage(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
+                       const double* Pk, const double* Uo_b, double coef, const double* slots_rec, int stage,
+                       double cfl, const unsigned char* mult, double* red, const double* dt_bar_ext, double* scratch,
+                       double* Ub, bool ub_add, double* Ab, double* Un_b, double un_coef, bool un_add,
+                       cudaStream_t st) {
+  const size_t npx = 12 * (size_t)(g.nx + 6) * g.ny, npy = 12 * (size_t)g.nx * (g.ny + 6);
+  double *FbX = scratch, *UaX = FbX + npx, *FbY = UaX + npx, *UaY = FbY + npy;
+  const int nlx = (g.ny + SW_NT - 1) / SW_NT, nsx = (g.nx + 6 + SW_R - 1) / SW_R;
+  const int nly = (g.nx + SW_NT - 1) / SW_NT, nsy = (g.ny + 6 + SW_R - 1) / SW_R;
+  const int nbx = nlx * nsx * 12, nby = nly * nsy * 12;
+  k_flux_sweep<<<nbx + nby, SW_NT, 0, st>>>(g, Uk, Pk, Uo_b, coef, slots_rec, stage, FbX, UaX, FbY, UaY, red, nbx,
+                                            nlx, nly);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if (upd)
-    k_speed_scatter<true><<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U, A, mult, slots_rec, stage, cfl, red, Ub, Ab);
-  else
-    k_speed_scatter<false><<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U, A, mult, slots_rec, stage, cfl, red, Ub, Ab);
-  return cudaGetLastError();
-}
-
-cudaError_t probe_seed(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A,
-                       const double* pp_bar, int px, int py, int wx, int wy, double* Ub, double* Ab, cudaStream_t st) {
-  if (!pp_bar || wx * wy <= 0) return cudaSuccess;
-  k_probe_seed<<<1, 32 * ((wx * wy + 31) / 32), 0, st>>>(m, g, U, A, pp_bar, px, py, wx, wy, Ub, Ab);
+  k_stage_merge<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, cfl, mult, red,
+                                                          dt_bar_ext, FbX, UaX, FbY, UaY, Ub, ub_add ? 1 : 0, Ab,
+                                                          Un_b, un_coef, un_add ? 1 : 0);
   return cudaGetLastError();
 }
 
 cudaError_t probe_mean(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A, int px, int py,
                        int wx, int wy, double* out, cudaStream_t st) {
   k_probe_mean<<<1, 128, 0, st>>>(m, g, U, A, px, py, wx, wy, out);
-  return cudaGetLastError();
-}
-
-cudaError_t adj_begin(double* red, const double* dt_bar_ext, cudaStream_t st) {
-  k_adj_begin<<<1, 1, 0, st>>>(red, dt_bar_ext);
-  return cudaGetLastError();
-}
-
-cudaError_t clear_alpha(double* red, cudaStream_t st) {
-  k_adj_clear_alpha<<<1, 1, 0, st>>>(red);
   return cudaGetLastError();
 }
 

@@ -7,27 +7,36 @@
 namespace jb {
 namespace adj {
 
-// red: 8 device doubles [abar_x, abar_y, dtbar, ties_x, ties_y, ties_cfl, -, -]
-cudaError_t upd_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A, double* Ub,
-                    double* Ab, cudaStream_t st);
+// Reduction slots of one adjoint step (device doubles, cleared before it):
+// [0] the dt adjoint; per RK stage s = 0, 1, 2 from 1 + 5 s: the alpha_x and
+// alpha_y adjoints, the alpha_x and alpha_y tie counts (padded-grid
+// multiplicity) and, for stage 0, the CFL tie count.
+constexpr int RED_DTB = 0, RED_N = 16;
+__host__ __device__ constexpr int red_ab(int s, int d) { return 1 + 5 * s + d; }
+__host__ __device__ constexpr int red_cnt(int s, int d) { return 3 + 5 * s + d; }
+
+// probe = {px, py, wx, wy}; pp_bar may be null.  prims: 3 x 4 x ncell.
+cudaError_t vjp_begin(const jb_mech_params& m, const jb_grid& g, const double* U4, const double* A4,
+                      const double* pp_bar, const int* probe, double* Ub, double* Ab, const double* rec,
+                      double* prims, const unsigned char* mult, const double* slots_rec, double cfl, double* red,
+                      cudaStream_t st);
 cudaError_t chem_vjp(const jb_mech_params& m, const jb_grid& g, const double* U3, const double* A3,
                      const double* Ub4, double* Ub3, const double* slot_dt, double* dtb, double* lnAb,
                      cudaStream_t st);
-// Ub2 (nv x ncell), Ab2 (ncell): scratch for the y-face adjoints
-cudaError_t flux_vjp(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
-                     const double* Uo_b, double coef, const double* slots_rec, int stage, double* Ub, double* Abk,
-                     double* Un_b, double un_coef, double* ghost, double* Ub2, double* Ab2, double* red,
-                     cudaStream_t st);
-// upd: also the update_aux VJP of (U, A) with the completed aux adjoint
-cudaError_t speed_vjp(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A,
-                      const unsigned char* mult, const double* slots_rec, int stage, double cfl, double* red,
-                      double* Ub, double* Ab, bool upd, cudaStream_t st);
-cudaError_t probe_seed(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A,
-                       const double* pp_bar, int px, int py, int wx, int wy, double* Ub, double* Ab, cudaStream_t st);
+// Doubles of the scratch that flux_stage needs (the per-face-direction
+// flux and LF-term adjoints of the padded cells).
+size_t flux_scratch_doubles(const jb_grid& g);
+// One RK stage U' = a Un + b (Uk + dt L(Uk)) with b = coef, a = un_coef:
+// Ub (store, or add with ub_add) = Ubar_k; Un_b (store / add) += a Ubar'.
+// Ab null: the update_aux VJP of Uk is applied; else its aux adjoint is
+// added to Ab.  cfl > 0 only for stage 0 (the CFL time step).
+cudaError_t flux_stage(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
+                       const double* Pk, const double* Uo_b, double coef, const double* slots_rec, int stage,
+                       double cfl, const unsigned char* mult, double* red, const double* dt_bar_ext, double* scratch,
+                       double* Ub, bool ub_add, double* Ab, double* Un_b, double un_coef, bool un_add,
+                       cudaStream_t st);
 cudaError_t probe_mean(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A, int px, int py,
                        int wx, int wy, double* out, cudaStream_t st);
-cudaError_t adj_begin(double* red, const double* dt_bar_ext, cudaStream_t st);
-cudaError_t clear_alpha(double* red, cudaStream_t st);
 cudaError_t init_vjp(const jb_mech_params& m, long long n, const double* P, const double* T, const double* Y,
                      const double* Ub, const double* Ab, double* Tb, cudaStream_t st);
 

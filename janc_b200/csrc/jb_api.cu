@@ -40,14 +40,12 @@ struct jb_handle {
   // adjoint support
   double base_A[JB_NREAC_MAX];  // pre-exponential factors as created (jb_set_log_A_offset)
   int probe[4];                 // x0, y0, wx, wy of the pressure probe (wx*wy = 0: none)
-  double* adj_ws;               // Ubar stage buffers, abar, ghost adjoints, reductions
+  double* adj_ws;               // stage adjoints, primitives, face scratch, reductions
   unsigned char* adj_mult;      // padded-grid multiplicity of each cell (alpha ties)
   double* adj_B1;
   double* adj_B2;
-  double* adj_A2;
-  double* adj_ghost;
-  double* adj_Ub2;   // y-face adjoints of a stage before the merge
-  double* adj_Ab2;
+  double* adj_prims;  // rho, u, v, p of the three stage states of a step
+  double* adj_scratch;
   double* adj_red;
   char err[512];
 };
@@ -518,17 +516,15 @@ static int adj_workspace(jb_handle* h) {
       return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint supports periodic, slip, no-slip and zero-gradient sides");
   const jb_grid& g = h->grid;
   const size_t nc = (size_t)g.ncell, nU = (size_t)g.nv * nc;
-  const size_t L = (size_t)(g.nx > g.ny ? g.nx : g.ny);
-  const size_t n = 3 * nU + 3 * nc + 12 * 13 * L + 8;
+  const size_t nsc = jb::adj::flux_scratch_doubles(g);
+  const size_t n = 2 * nU + 12 * nc + nsc + jb::adj::RED_N;
   JB_TRY(cudaMalloc(&h->adj_ws, sizeof(double) * n), "adjoint workspace");
   JB_TRY(cudaMemset(h->adj_ws, 0, sizeof(double) * n), "adjoint workspace clear");
   h->adj_B1 = h->adj_ws;
   h->adj_B2 = h->adj_B1 + nU;
-  h->adj_A2 = h->adj_B2 + nU;
-  h->adj_ghost = h->adj_A2 + 2 * nc;
-  h->adj_Ub2 = h->adj_ghost + 12 * 13 * L;
-  h->adj_Ab2 = h->adj_Ub2 + nU;
-  h->adj_red = h->adj_Ab2 + nc;
+  h->adj_prims = h->adj_B2 + nU;
+  h->adj_scratch = h->adj_prims + 12 * nc;
+  h->adj_red = h->adj_scratch + nsc;
   std::vector<unsigned char> mult;
   padded_multiplicity(g, mult);
   JB_TRY(cudaMalloc(&h->adj_mult, nc), "multiplicity");
@@ -558,33 +554,28 @@ int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, do
   const double* slots = rec_slots;
   const double* slot_dt = slots + offsetof(jb_slots, dt) / sizeof(double);
   double* red = h->adj_red;
-  double *B1 = h->adj_B1, *B2 = h->adj_B2, *Ab2 = h->adj_A2, *gh = h->adj_ghost;
+  double *B1 = h->adj_B1, *B2 = h->adj_B2, *P = h->adj_prims, *sc = h->adj_scratch;
+  const unsigned char* mult = h->adj_mult;
   const double c_cfl = cfl > 0.0 ? cfl : 0.0;
-  JB_TRY(jb::adj::adj_begin(red, dt_bar, st), "adjoint begin");
-  // loss term of this step and the final temperature solve
-  JB_TRY(jb::adj::probe_seed(m, g, U4, A4, pp_bar, h->probe[0], h->probe[1], h->probe[2], h->probe[3], Ubar, Abar,
-                             st),
-         "probe seed");
-  JB_TRY(jb::adj::upd_vjp(m, g, U4, A4, Ubar, Abar, st), "update_aux 4");
+  JB_TRY(cudaMemsetAsync(red, 0, sizeof(double) * jb::adj::RED_N, st), "reduction clear");
+  // loss term of this step, the final temperature solve; primitives and tie
+  // counts of the three stage states
+  JB_TRY(jb::adj::vjp_begin(m, g, U4, A4, pp_bar, h->probe, Ubar, Abar, rec, P, mult, slots, c_cfl, red, st),
+         "adjoint begin");
   // chemistry (and update_aux of U3): B1 = Ubar3
-  JB_TRY(jb::adj::chem_vjp(m, g, W3, A3, Ubar, B1, slot_dt, red + 2, lnA_bar, st), "chemistry");
-  JB_TRY(cudaMemsetAsync(Ubar, 0, sizeof(double) * nU, st), "Ubar_n clear");  // Ubar becomes Ubar_n
-  // stage 3: U3 = 1/3 U + 2/3 (U2 + dt L(U2, aux2))
-  JB_TRY(cudaMemsetAsync(B2, 0, sizeof(double) * nU, st), "Ubar2 clear");
-  JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
-  JB_TRY(jb::adj::flux_vjp(m, g, W2, A2, B1, 2.0 / 3.0, slots, 2, B2, Ab2, Ubar, 1.0 / 3.0, gh, h->adj_Ub2, h->adj_Ab2, red, st), "stage 3");
-  // alpha 3, then update_aux of U2 with its completed aux adjoint
-  JB_TRY(jb::adj::speed_vjp(m, g, W2, A2, h->adj_mult, slots, 2, 0.0, red, B2, Ab2, true, st), "alpha 3");
-  // stage 2: U2 = 3/4 U + 1/4 (U1 + dt L(U1, aux1)); B1 = Ubar1
-  JB_TRY(cudaMemsetAsync(B1, 0, sizeof(double) * nU, st), "Ubar1 clear");
-  JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
-  JB_TRY(jb::adj::flux_vjp(m, g, W1, A1, B2, 0.25, slots, 1, B1, Ab2, Ubar, 0.75, gh, h->adj_Ub2, h->adj_Ab2, red, st), "stage 2");
-  JB_TRY(jb::adj::speed_vjp(m, g, W1, A1, h->adj_mult, slots, 1, 0.0, red, B1, Ab2, true, st), "alpha 2");
-  // stage 1: U1 = U + dt L(U, aux); then alpha 1 and the CFL time step
-  JB_TRY(jb::adj::clear_alpha(red, st), "alpha clear");
-  JB_TRY(jb::adj::flux_vjp(m, g, Un, An, B1, 1.0, slots, 0, Ubar, Abar, nullptr, 0.0, gh, h->adj_Ub2, h->adj_Ab2, red, st), "stage 1");
-  JB_TRY(jb::adj::speed_vjp(m, g, Un, An, h->adj_mult, slots, 0, c_cfl, red, Ubar, Abar, false, st),
-         "alpha 1 and dt");
+  JB_TRY(jb::adj::chem_vjp(m, g, W3, A3, Ubar, B1, slot_dt, red + jb::adj::RED_DTB, lnA_bar, st), "chemistry");
+  // stage 3: U3 = 1/3 U + 2/3 (U2 + dt L(U2, aux2)); B2 = Ubar2, Ubar = 1/3 B1
+  JB_TRY(jb::adj::flux_stage(m, g, W2, A2, P + 8 * nc, B1, 2.0 / 3.0, slots, 2, 0.0, mult, red, dt_bar, sc, B2, false,
+                             nullptr, Ubar, 1.0 / 3.0, false, st),
+         "stage 3");
+  // stage 2: U2 = 3/4 U + 1/4 (U1 + dt L(U1, aux1)); B1 = Ubar1, Ubar += 3/4 B2
+  JB_TRY(jb::adj::flux_stage(m, g, W1, A1, P + 4 * nc, B2, 0.25, slots, 1, 0.0, mult, red, dt_bar, sc, B1, false,
+                             nullptr, Ubar, 0.75, true, st),
+         "stage 2");
+  // stage 1: U1 = U + dt L(U, aux), with alpha 1 and the CFL time step
+  JB_TRY(jb::adj::flux_stage(m, g, Un, An, P, B1, 1.0, slots, 0, c_cfl, mult, red, dt_bar, sc, Ubar, true, Abar,
+                             nullptr, 0.0, false, st),
+         "stage 1");
   return JB_OK;
 }
 
