@@ -654,7 +654,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
                                            double& dtb) {
   const int nA = D == 0 ? g.nx : g.ny;
   const long long nc = g.ncell;
-  const double dA = D == 0 ? g.dx : g.dy;
+  const double idA = 1.0 / (D == 0 ? g.dx : g.dy), dt_dA = dt * idA;
   const int a0 = -3 + seg * SW_R, a1 = min(a0 + SW_R, nA + 3);  // owned padded cells [a0, a1)
   const int flo = max(a0 - 2, 0), fhi = min(a1 + 2, nA);        // faces touching them
   const size_t npad = D == 0 ? (size_t)(g.nx + 6) * g.ny : (size_t)g.nx * (g.ny + 6);
@@ -688,7 +688,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
     sweep_load<D>(g, Uk, Pk, f, line, fa + 2, alpha, Hp[5], Hm[5], Q[5]);
     const double lbp = lbar(fa);
     // L_i = -(F_{i+1} - F_i) / d  ->  Fbar_fa = dt (Lbar_fa - Lbar_{fa-1}) / d
-    const double Fbf = dt * (lbp - lbm) / dA;
+    const double Fbf = dt_dA * (lbp - lbm);
     double dl[5], dr[5];
     const double vl = weno_d(Hp[0], Hp[1], Hp[2], Hp[3], Hp[4], dl);
     // right-biased: the left form of the mirrored stencil (cells fa+2 .. fa-2)
@@ -696,7 +696,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
     const double Fv = vl + vr;
     // dt adjoint: L of the owned interior cell fa-1, both of its faces known
     const int ci = fa - 1;
-    if (fa > flo && ci >= a0 && ci < a1 && ci >= 0 && ci < nA) dtb -= (Fv - Fprev) / dA * lbm;
+    if (fa > flo && ci >= a0 && ci < a1 && ci >= 0 && ci < nA) dtb -= (Fv - Fprev) * idA * lbm;
 #pragma unroll
     for (int j = 0; j < 5; ++j) {
       Ap[j] += Fbf * dl[j];          // cell fa-3+j
@@ -832,7 +832,7 @@ __device__ __forceinline__ void merge_ghosts(const MP& m, const Grid& g, const d
 // the CFL ties of dt), then either the update_aux VJP of Uk with its
 // completed aux adjoint (Ab null) or the aux adjoint itself added to Ab.
 // ub_add / un_add: add to Ub / Un_b instead of storing.
-__global__ void __launch_bounds__(128) k_stage_merge(
+__global__ void __launch_bounds__(128, 4) k_stage_merge(
     MP m, Grid g, const double* __restrict__ Uk, const double* __restrict__ Ak, const double* __restrict__ Uo_b,
     double coef, const double* __restrict__ slots_rec, int stage, double cfl, const unsigned char* __restrict__ mult,
     const double* __restrict__ red, const double* __restrict__ dt_bar_ext, const double* __restrict__ FbX,
