@@ -40,6 +40,7 @@ struct jb_handle {
   // adjoint support
   double base_A[JB_NREAC_MAX];  // pre-exponential factors as created (jb_set_log_A_offset)
   int probe[4];                 // x0, y0, wx, wy of the pressure probe (wx*wy = 0: none)
+  void* fwork;                  // mixed 2D flux scratch (float32 primitives, x flux differences)
   double* adj_ws;               // stage adjoints, primitives, face scratch, reductions
   unsigned char* adj_mult;      // padded-grid multiplicity of each cell (alpha ties)
   double* adj_B1;
@@ -171,11 +172,14 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   if (e == cudaSuccess) e = cudaMalloc(&h->slots, sizeof(jb_slots));
   if (e == cudaSuccess) e = cudaMemset(h->strips, 0, bytes_strip);
   if (e == cudaSuccess) e = cudaMemset(h->slots, 0, sizeof(jb_slots));
+  // mixed 2D: float32 primitives and x flux differences of a stage
+  const size_t bytes_fwork = precision == JB_PREC_MIXED && dim == 2 ? sizeof(float) * 15 * nc : 0;
+  if (e == cudaSuccess && bytes_fwork) e = cudaMalloc(&h->fwork, bytes_fwork);
   if (e != cudaSuccess) {
     jb_destroy(h);
     return JB_ERR_CUDA;
   }
-  h->ws_bytes = (long long)(2 * bytes_W + 2 * bytes_aux + bytes_cand + bytes_strip + sizeof(jb_slots));
+  h->ws_bytes = (long long)(2 * bytes_W + 2 * bytes_aux + bytes_cand + bytes_strip + sizeof(jb_slots) + bytes_fwork);
   *out = h;
   return JB_OK;
 }
@@ -191,6 +195,7 @@ int jb_destroy(jb_handle* h) {
   if (h->cand) cudaFree(h->cand);
   if (h->strips) cudaFree(h->strips);
   if (h->slots) cudaFree(h->slots);
+  if (h->fwork) cudaFree(h->fwork);
   if (h->adj_ws) cudaFree(h->adj_ws);
   if (h->adj_mult) cudaFree(h->adj_mult);
   delete h;
@@ -222,10 +227,10 @@ int jb_flux_func(jb_handle* h, const double* U, const double* aux, double dt, do
   const jb::Ops& o = *h->ops;
   JB_TRY(o.slots_reset(h->slots, st), "slots_reset");
   JB_TRY(o.select(h->dim, false, true, false, h->mech, h->grid, U, aux, nullptr, nullptr, h->strips,
-                  h->slots, -1, 3, st),
+                  h->slots, -1, 3, nullptr, st),
          "alpha");
   JB_TRY(o.flux(h->dim, 0, h->mech, h->grid, U, aux, nullptr, rhs, nullptr, h->strips, h->slots, 3,
-                -1, dt, st),
+                -1, dt, nullptr, st),
          "flux");
   return JB_OK;
 }
@@ -238,7 +243,7 @@ int jb_update_aux(jb_handle* h, const double* U, const double* aux_in, double* a
   JB_TRY(o.slots_reset(h->slots, st), "slots_reset");
   JB_TRY(o.halley(h->dim, h->mech, h->grid, U, aux_in, h->cand, h->slots, 0, st), "halley");
   JB_TRY(o.select(h->dim, true, false, false, h->mech, h->grid, U, nullptr, h->cand, aux_out,
-                  h->strips, h->slots, 0, 0, st),
+                  h->strips, h->slots, 0, 0, nullptr, st),
          "select");
   return JB_OK;
 }
@@ -285,7 +290,7 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
   JB_TIMED(JB_KCAT_OTHER, o.slots_reset(h->slots, st), "slots_reset");
   // alpha (and CFL minimum) of the initial state, ghost strips for stage 1
   JB_TIMED(JB_KCAT_SELECT, o.select(d, false, true, use_cfl, m, g, U, aux, nullptr, nullptr, h->strips, h->slots, -1, 3,
-                  st),
+                  h->fwork, st),
          "prep");
   for (int s = 0; s < nsteps; ++s) {
     double* r = rec ? rec + s * RS : nullptr;
@@ -301,27 +306,27 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     double* Ao = r ? r + RS + nU : aux_out;
     JB_TIMED(JB_KCAT_OTHER, o.step_begin(h->slots, use_cfl ? cfl : 0.0, dt_fixed, dt_hist, s, st), "step_begin");
     // stage 1: U1 = U + L(U)
-    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 1, m, g, Un, an, Un, W1, h->cand, h->strips, h->slots, 0, 0, 0.0, st), "stage1");
+    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 1, m, g, Un, an, Un, W1, h->cand, h->strips, h->slots, 0, 0, 0.0, h->fwork, st), "stage1");
     JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W1, nullptr, h->cand, A1, h->strips,
-                    h->slots, 0, 1, st),
+                    h->slots, 0, 1, h->fwork, st),
            "select1");
     // stage 2: U2 = 3/4 U + 1/4 (U1 + L(U1))
     JB_TIMED(JB_KCAT_FLUX, o.flux(d, 2, m, g, W1, A1, Un, W2, h->cand, h->strips, h->slots, 1, 1,
-                  0.0, st),
+                  0.0, h->fwork, st),
            "stage2");
     JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W2, nullptr, h->cand, A2, h->strips,
-                    h->slots, 1, 2, st),
+                    h->slots, 1, 2, h->fwork, st),
            "select2");
     // stage 3: U3 = 1/3 U + 2/3 (U2 + L(U2))
     JB_TIMED(JB_KCAT_FLUX, o.flux(d, 3, m, g, W2, A2, Un, W3, h->cand, h->strips, h->slots, 2, 2,
-                  0.0, st),
+                  0.0, h->fwork, st),
            "stage3");
     if (!chemistry) {
       // advance_flux only (TVD_RK3.py:5-12): U3, aux3 are the result
       const size_t bytes = sizeof(double) * g.nv * (size_t)g.ncell;
       JB_TRY(cudaMemcpyAsync(U_out, W3, bytes, cudaMemcpyDeviceToDevice, st), "copy U3");
       JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, U_out, nullptr, h->cand, aux_out,
-                                        h->strips, h->slots, 2, 3, st),
+                                        h->strips, h->slots, 2, 3, h->fwork, st),
                "select3");
       continue;
     }
@@ -330,12 +335,12 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     // kernel (its gamma is not used by anything that follows)
     if (rec)
       JB_TIMED(JB_KCAT_SELECT, o.select(d, true, false, false, m, g, W3, nullptr, h->cand, A3, h->strips,
-                      h->slots, 2, 0, st),
+                      h->slots, 2, 0, nullptr, st),
              "select3");
     JB_TIMED(JB_KCAT_CHEM, o.chem(d, false, m, g, W3, rec ? A3 : nullptr, Uo, h->cand, h->slots, 3, 0.0, st),
              "chem");
     JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, Uo, nullptr, h->cand, Ao, h->strips,
-                    h->slots, 3, 3, st),
+                    h->slots, 3, 3, h->fwork, st),
            "select4");
     if (rec)
       JB_TRY(cudaMemcpyAsync(rec_slots + s * (sizeof(jb_slots) / sizeof(double)), h->slots, sizeof(jb_slots),
@@ -378,7 +383,7 @@ int jb_cfl_dt(jb_handle* h, const double* U, const double* aux, double cfl, doub
   const jb::Ops& o = *h->ops;
   JB_TRY(o.slots_reset(h->slots, st), "slots_reset");
   JB_TRY(o.select(h->dim, false, false, true, h->mech, h->grid, U, aux, nullptr, nullptr, h->strips,
-                  h->slots, -1, 3, st),
+                  h->slots, -1, 3, nullptr, st),
          "cfl");
   JB_TRY(o.dt_from_slots(h->slots, cfl, dt_out, st), "dt");
   return JB_OK;

@@ -912,6 +912,224 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
   block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
 }
 
+#if JB_FAST
+// ---------------------------------------------------------------------------
+// mixed-precision 2D RK stage as an x-line sweep plus y runs (STAGE 1..3)
+// ---------------------------------------------------------------------------
+// The same arithmetic as k_flux2d<S, float> (float32 LF / WENO on float32
+// primitives, float64 RK combination and Halley iterates), organised
+// without block barriers:
+//   k_sweep_x    one thread per (y line, x segment of SX_R cells, field):
+//                a register window of H+ / H- walks the segment's faces and
+//                writes the x flux difference F_{i+1} - F_i of each cell
+//   k_flux_y_rk  one warp per run of 32 cells along y: H+ / H- of all fields
+//                on the run and its 3 + 3 halo cells, the 33 y faces and the
+//                differences, then the RK combination with the x part and
+//                the Halley iterates of the new state
+// The primitives (u, v, p as float32) of the stage state come from the
+// select pass that produced its temperature (prims[3][ncell]).
+constexpr int SX_R = 16, SX_NT = 128;
+constexpr int YR_W = 8, YR_NT = 32 * YR_W;     // warps (runs) per block
+constexpr int YR_C = 38, YR_F = 33;            // window cells, faces per run
+constexpr size_t YR_SMEM = sizeof(float) * YR_W * (2 * 12 * YR_C + 12 * YR_F);
+
+// Split fluxes of field f at one cell: F = vel q (+ p in the normal
+// momentum, + vel p in rho E), H+- = (F +- alpha q) / 2.
+__device__ __forceinline__ void split_h(int f, int fn, float q, float vel, float p, float al, float& hp,
+                                        float& hm) {
+  float F = vel * q;
+  if (f == fn) F += p;
+  if (f == 3) F += vel * p;
+  hp = 0.5f * (F + al * q);
+  hm = 0.5f * (F - al * q);
+}
+
+// Field f, normal velocity and pressure of padded cell (x, y) for an x sweep
+// (dir 0) or all fields for a y run (dir 1): interior and copied ghosts from
+// the state and the primitives, outlet / injector ghosts from their strips.
+// DIR 2: field f and the y velocity (halo items of a y run).
+template <int DIR>
+__device__ __forceinline__ void win_load(const MP& m, const Grid& g, const double* __restrict__ Uk,
+                                         const float* __restrict__ prims, const double* __restrict__ strips, int x,
+                                         int y, int f, float* q, float& vel, float& p) {
+  constexpr int NQ = DIR == 1 ? 12 : 1;
+  const long long nc = g.ncell;
+  const Src s = map_cell<2>(g, x, y);
+  if (s.kind == 0) {
+    const long long src = (long long)s.xs * g.ny + s.ys;
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+      const int ff = DIR == 1 ? i : f;
+      const double v = Uk[ff * nc + src];
+      q[i] = (float)(((s.flip >> ff) & 1) ? -v : v);
+    }
+    vel = prims[(DIR == 0 ? 0 : nc) + src];
+    if (s.flip & (DIR == 0 ? 2 : 4)) vel = -vel;
+    p = prims[2 * nc + src];
+  } else if (s.kind == 1) {
+    float qa[12];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) qa[i] = (float)strips[strip_idx(g, s.side, i, s.pos)];
+    float rho, u, v;
+    flux_prims<2>(m, qa, (float)strips[strip_idx(g, s.side, 13, s.pos)], rho, u, v, p);
+    vel = DIR == 0 ? u : v;
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) q[i] = qa[DIR == 1 ? i : f];
+  } else {
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) q[i] = 1.f;
+    vel = 1.f;
+    p = 1.f;
+  }
+}
+
+__global__ void __launch_bounds__(SX_NT) k_sweep_x(MP m, Grid g, const double* __restrict__ Uk,
+                                                   const float* __restrict__ prims,
+                                                   const double* __restrict__ strips, const Slots* slots, int aidx,
+                                                   float* __restrict__ dfx, int nlb) {
+  const int f = blockIdx.x % 12;
+  const int rest = blockIdx.x / 12;
+  const int y = (rest % nlb) * SX_NT + threadIdx.x, seg = rest / nlb;
+  if (y >= g.ny) return;
+  const long long nc = g.ncell;
+  const double* uf = Uk + f * nc;
+  const float al = (float)bitsd(slots->ax[aidx]);
+  const int a0 = seg * SX_R, a1 = min(a0 + SX_R, g.nx);  // cells [a0, a1), faces a0 .. a1
+  float Hp[6], Hm[6];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    float q, vel, p;
+    win_load<0>(m, g, Uk, prims, strips, a0 - 3 + k, y, f, &q, vel, p);
+    split_h(f, 1, q, vel, p, al, Hp[k], Hm[k]);
+  }
+  // the next cell to enter the window, fetched one face ahead and left
+  // untouched until then so that its loads overlap the WENO arithmetic
+  double nq;
+  float nv, np;
+  auto fetch = [&](int a) {
+    if (a >= 0 && a < g.nx) {
+      const long long src = (long long)a * g.ny + y;
+      nq = uf[src];
+      nv = prims[src];
+      np = prims[2 * nc + src];
+    } else {
+      float q;
+      win_load<0>(m, g, Uk, prims, strips, a, y, f, &q, nv, np);
+      nq = q;
+    }
+  };
+  fetch(a0 + 2);
+  float* out = dfx + (long long)f * nc + y;
+  float Fprev = 0.f;
+#pragma unroll 1
+  for (int fa = a0; fa <= a1; ++fa) {
+    split_h(f, 1, (float)nq, nv, np, al, Hp[5], Hm[5]);  // cell fa+2
+    if (fa < a1) fetch(fa + 3);
+    // face fa (cells fa-1 | fa): H+ of cells fa-3 .. fa+1, H- of fa-2 .. fa+2
+    const float F = weno_L(Hp[0], Hp[1], Hp[2], Hp[3], Hp[4]) + weno_R(Hm[1], Hm[2], Hm[3], Hm[4], Hm[5]);
+    if (fa > a0) out[(long long)(fa - 1) * g.ny] = F - Fprev;
+    Fprev = F;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      Hp[k] = Hp[k + 1];
+      Hm[k] = Hm[k + 1];
+    }
+  }
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const double* __restrict__ Uk,
+                                                       const double* __restrict__ auxk,
+                                                       const double* __restrict__ Un, const float* __restrict__ prims,
+                                                       const double* __restrict__ strips,
+                                                       const float* __restrict__ dfx, double* __restrict__ out,
+                                                       double* __restrict__ cand, Slots* slots, int aidx, int midx,
+                                                       int nry) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  float* sHp = reinterpret_cast<float*>(smraw) + (size_t)w * (2 * 12 * YR_C + 12 * YR_F);  // [12][YR_C]
+  float* sHm = sHp + 12 * YR_C;
+  float* sF = sHm + 12 * YR_C;  // [12][YR_F]
+  const long long nc = g.ncell;
+  const int run = blockIdx.x * YR_W + w;
+  const int x = run / nry, y0 = (run % nry) * 32;
+  const bool xin = x < g.nx;
+  const float al = (float)bitsd(slots->ay[aidx]);
+  // ---- split fluxes on the window: cell y0 - 3 + j in slot j; the run's
+  // own cells one per lane, the 3 + 3 halo cells as 72 (cell, field) items
+  // spread over the warp
+  if (xin) {
+    {
+      const int j = l + 3;
+      float q[12], vel, p;
+      win_load<1>(m, g, Uk, prims, strips, x, y0 + l, 0, q, vel, p);
+#pragma unroll
+      for (int f = 0; f < 12; ++f) split_h(f, 2, q[f], vel, p, al, sHp[f * YR_C + j], sHm[f * YR_C + j]);
+    }
+#pragma unroll 1
+    for (int i = l; i < 72; i += 32) {
+      const int h = i / 12, f = i % 12;
+      const int j = h < 3 ? h : 32 + h;
+      float q, vel, p;
+      win_load<2>(m, g, Uk, prims, strips, x, y0 - 3 + j, f, &q, vel, p);
+      split_h(f, 2, q, vel, p, al, sHp[f * YR_C + j], sHm[f * YR_C + j]);
+    }
+  }
+  __syncwarp();
+  // ---- faces y0 + k (cells y0+k-1 | y0+k): lane k for all fields, then
+  // the run's last face by lanes 0..11, one field each
+  if (xin) {
+#pragma unroll 1
+    for (int f = 0; f < 12; ++f) {
+      const float* hp = sHp + f * YR_C + l;
+      const float* hm = sHm + f * YR_C + l;
+      sF[f * YR_F + l] = weno_L(hp[0], hp[1], hp[2], hp[3], hp[4]) + weno_R(hm[1], hm[2], hm[3], hm[4], hm[5]);
+    }
+    if (l < 12) {
+      const float* hp = sHp + l * YR_C + 32;
+      const float* hm = sHm + l * YR_C + 32;
+      sF[l * YR_F + 32] = weno_L(hp[0], hp[1], hp[2], hp[3], hp[4]) + weno_R(hm[1], hm[2], hm[3], hm[4], hm[5]);
+    }
+  }
+  __syncwarp();
+  // ---- RK combination (float64) and the Halley iterates of the new state
+  const int y = y0 + l;
+  const bool live = xin && y < g.ny;
+  unsigned bits = 0;
+  if (live) {
+    const long long cell = (long long)x * g.ny + y;
+    const double dt = slots->dt;
+    double q[12];
+#pragma unroll
+    for (int f = 0; f < 12; ++f) {
+      const double dF = (double)dfx[f * nc + cell];
+      const double dG = (double)(sF[f * YR_F + l + 1] - sF[f * YR_F + l]);
+      const double rhs = dt * (-(dF * g.idx + dG * g.idy));
+      const double uk = Uk[f * nc + cell];
+      double r;
+      if (STAGE == 1) r = uk + rhs;
+      else if (STAGE == 2) r = 3.0 / 4.0 * Un[f * nc + cell] + 1.0 / 4.0 * (uk + rhs);
+      else r = 1.0 / 3.0 * Un[f * nc + cell] + 2.0 / 3.0 * (uk + rhs);
+      out[f * nc + cell] = r;
+      q[f] = r;
+    }
+    const double rho = q[0];
+    const double u = q[1] / rho, v = q[2] / rho;
+    const double e = q[3] / rho - 0.5 * (u * u + v * v);
+    double Y8[NR], Yf[NS];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) Y8[k] = q[4 + k] / rho;
+    fill_Y(Y8, Yf);
+    const double Rmix = get_R(m, Yf);
+    double cnd[JB_NCAND];
+    bits = halley_any(m, e, Yf, Rmix, auxk[nc + cell], cnd);
+#pragma unroll
+    for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
+  }
+  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
+}
+#endif  // JB_FAST
+
 // 1D: a block of NT threads handles a tile of NT-1 cells, so its NT faces
 // map one-to-one onto threads.
 constexpr int NT1 = 256;
@@ -1093,7 +1311,8 @@ template <int DIM, bool SELECT, bool ALPHA, bool CFL, bool STRIPS = true>
 __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const double* U, const double* aux_in,
                                             const double* cand, double* aux_out, double* strips,
                                             Slots* slots, unsigned mask, long long c, double& amx,
-                                            double& amy, double& dtm, unsigned& st) {
+                                            double& amy, double& dtm, unsigned& st,
+                                            float* prims = nullptr) {
   constexpr int nY = DIM == 1 ? 3 : 4;
   constexpr int nv = nY + NR;
   const long long nc = g.ncell;
@@ -1120,6 +1339,11 @@ __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const do
     }
     if (ALPHA || CFL) {
       Prim<DIM> pr = u_to_prim<DIM>(m, q, gamma, T);
+      if (DIM == 2 && prims) {  // float32 primitives for the next mixed-precision flux stage
+        prims[c] = (float)pr.u;
+        prims[nc + c] = (float)pr.v;
+        prims[2 * nc + c] = (float)pr.p;
+      }
       double sx = fabs(pr.u) + pr.a;
       double sy = fabs(pr.v) + pr.a;
       amx = fmax(amx, sx);
@@ -1169,13 +1393,15 @@ __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const do
 template <int DIM, bool SELECT, bool ALPHA, bool CFL>
 __global__ void __launch_bounds__(256, 4) k_select(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ aux_in,
                          const double* __restrict__ cand, double* __restrict__ aux_out,
-                         double* __restrict__ strips, Slots* slots, int midx, int aidx) {
+                         double* __restrict__ strips, Slots* slots, int midx, int aidx,
+                         float* __restrict__ prims) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
   unsigned st = 0;
   if (c < g.ncell)
     select_cell<DIM, SELECT, ALPHA, CFL, false>(m, g, U, aux_in, cand, aux_out, strips, slots,
-                                                SELECT ? slots->mask[midx] : 0u, c, amx, amy, dtm, st);
+                                                SELECT ? slots->mask[midx] : 0u, c, amx, amy, dtm, st,
+                                                ALPHA ? prims : nullptr);
   if (ALPHA || CFL) block_reduce_store(amx, amy, dtm, st << 16, slots, aidx, ALPHA, CFL, -1);
 }
 

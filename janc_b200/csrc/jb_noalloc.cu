@@ -89,7 +89,7 @@ extern "C" int jb_update_aux_noalloc(const jb_mech_params* mech, int dim, int nx
   if (o.halley(dim, m, g, U, aux_in, cand, slots, 0, st) != cudaSuccess) return JB_ERR_CUDA;
   // cand planes are addressed with the grid's own cell count, so only the
   // first JB_NCAND * ncell doubles are touched
-  if (o.select(dim, true, false, false, m, g, U, nullptr, cand, aux_out, nullptr, slots, 0, 0, st) !=
+  if (o.select(dim, true, false, false, m, g, U, nullptr, cand, aux_out, nullptr, slots, 0, 0, nullptr, st) !=
       cudaSuccess)
     return JB_ERR_CUDA;
   return JB_OK;

@@ -9,15 +9,18 @@ namespace jb {
 
 struct Ops {
   const char* name;
-  // STAGE 0 writes dt * flux; STAGE 1..3 writes the RK stage and Halley iterates
+  // STAGE 0 writes dt * flux; STAGE 1..3 writes the RK stage and Halley iterates.
+  // work: the mixed variant's float32 scratch of a 2D handle (primitives
+  // [3][ncell], then x flux differences [12][ncell]) or null; select writes
+  // the primitives of its state there when it computes alpha.
   cudaError_t (*flux)(int dim, int stage, const jb_mech_params& m, const jb_grid& g,
                       const double* Uk, const double* auxk, const double* Un, double* out,
                       double* cand, const double* strips, jb_slots* slots, int aidx, int midx,
-                      double dt, cudaStream_t st);
+                      double dt, void* work, cudaStream_t st);
   cudaError_t (*select)(int dim, bool select, bool alpha, bool cfl, const jb_mech_params& m,
                         const jb_grid& g, const double* U, const double* aux_in,
                         const double* cand, double* aux_out, double* strips, jb_slots* slots,
-                        int midx, int aidx, cudaStream_t st);
+                        int midx, int aidx, void* work, cudaStream_t st);
   cudaError_t (*halley)(int dim, const jb_mech_params& m, const jb_grid& g, const double* U,
                         const double* aux, double* cand, jb_slots* slots, int midx,
                         cudaStream_t st);
