@@ -1055,6 +1055,7 @@ __global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const doub
   const int x = run / nry, y0 = (run % nry) * 32;
   const bool xin = x < g.nx;
   const float al = (float)bitsd(slots->ay[aidx]);
+  double ukr[12];
   // ---- split fluxes on the window: cell y0 - 3 + j in slot j; the run's
   // own cells one per lane, the 3 + 3 halo cells as 72 (cell, field) items
   // spread over the warp
@@ -1062,7 +1063,18 @@ __global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const doub
     {
       const int j = l + 3;
       float q[12], vel, p;
-      win_load<1>(m, g, Uk, prims, strips, x, y0 + l, 0, q, vel, p);
+      if (y0 + l < g.ny) {
+        const long long cell = (long long)x * g.ny + y0 + l;
+#pragma unroll
+        for (int f = 0; f < 12; ++f) {
+          ukr[f] = Uk[f * nc + cell];
+          q[f] = (float)ukr[f];
+        }
+        vel = prims[nc + cell];
+        p = prims[2 * nc + cell];
+      } else {
+        win_load<1>(m, g, Uk, prims, strips, x, y0 + l, 0, q, vel, p);
+      }
 #pragma unroll
       for (int f = 0; f < 12; ++f) split_h(f, 2, q[f], vel, p, al, sHp[f * YR_C + j], sHm[f * YR_C + j]);
     }
@@ -1105,7 +1117,7 @@ __global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const doub
       const double dF = (double)dfx[f * nc + cell];
       const double dG = (double)(sF[f * YR_F + l + 1] - sF[f * YR_F + l]);
       const double rhs = dt * (-(dF * g.idx + dG * g.idy));
-      const double uk = Uk[f * nc + cell];
+      const double uk = ukr[f];
       double r;
       if (STAGE == 1) r = uk + rhs;
       else if (STAGE == 2) r = 3.0 / 4.0 * Un[f * nc + cell] + 1.0 / 4.0 * (uk + rhs);
