@@ -73,10 +73,11 @@ UNIT = "cell-updates/s"
 BYTES_CHEM_PER_CELL = 224      # read U,aux (112 B) + write U,aux (112 B), float64
 BYTES_STEP_PER_CELL = 864 + 224  # fused-step minimum + separate chemistry pass (2D)
 BYTES_FLUX_STAGE_PER_CELL = 288  # one RK stage of the fused minimum: (224 + 320 + 320) / 3
-# DRAM bytes per cell measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-# on the 1024x256 channel, mixed precision: an RK stage 2/3 launch and a
-# chemistry launch; and per cell-step of the persistent ensemble kernel
-TRAFFIC_PER_CELL = {"flux": 305.0, "chem": 148.0}
+# DRAM bytes per cell measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum,
+# each launch cold) on the 1024x256 channel, mixed precision: one RK stage 2/3
+# (k_sweep_x 27.3 + 0.8 MB, k_flux_y_rk 67.2 + 34.8 MB) and one chemistry
+# launch; and per cell-step of the persistent ensemble kernel
+TRAFFIC_PER_CELL = {"flux": 496.5, "chem": 148.0}
 TRAFFIC_ENS_PER_CELL_STEP = 1125.0
 
 
@@ -505,14 +506,21 @@ def run_ours(args):
         "status_bits": head["status"],
         "kernel_ms_per_step": head["kernel_ms_per_step"],
         # per timed step (one jb_advance call of one step): slots reset, first
-        # select, step begin, 3 flux stages, 2 stage selects, chemistry, final select
-        "gpu_launches": 10 * args.steps,
-        "roofline": {"bound": "hbm", "kernel": {"chem": "k_chem (point-implicit chemistry + final Halley)",
-                                                 "flux": "k_flux2d (LF + WENO5 + RK stage + Halley)"}[dom],
+        # select, step begin, 3 flux stages (two kernels each in the mixed
+        # variant), 2 stage selects, chemistry, final select
+        # (+ 4 ghost-strip launches on the RDC workload's outlet / injector sides)
+        "gpu_launches": ((13 if args.precision == "mixed" else 10) + (4 if args.workload == "rdc" else 0))
+                        * args.steps,
+        "roofline": {"bound": "hbm", "kernel": {
+                         "chem": "k_chem (point-implicit chemistry + final Halley)",
+                         "flux": ("flux stage: k_sweep_x + k_flux_y_rk (LF + WENO5 + RK stage + Halley)"
+                                  if args.precision == "mixed" else
+                                  "k_flux2d (LF + WENO5 + RK stage + Halley)")}[dom],
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "traffic": (TRAFFIC_PER_CELL[dom] * ncell if args.workload == "channel" and
                                  args.precision == "mixed" else None),
-                     "traffic_source": "ncu dram bytes of one launch on this workload (mixed precision)",
+                     "traffic_source": "ncu dram bytes of one stage's launches on this workload, each "
+                                       "launch cold (mixed precision)",
                      "peak_source": hbm_src,
                      "algorithmic_bytes_per_cell": bytes_cell, "launch_ms": launch_ms,
                      "step_achieved_gbs": step_gbs,
@@ -655,9 +663,12 @@ def run_adjoint(args):
                                     "note": "full-field directions perturb the exactly uniform ambient gas, "
                                             "where WENO5-JS (eps = 1e-6 against split fluxes ~1e8) is linear "
                                             "only below ~1e-11 relative perturbations"},
-        # forward: 9 per step + 2 per checkpoint segment; backward: the recorded
-        # recomputation (9 per step + 2 per segment) and 22 adjoint kernels per step
-        "gpu_launches": 40 * N + 4 * ((N + ADJ_K - 1) // ADJ_K), "clocks": clk,
+        # forward: 9 per step (step begin, 3 flux stages, 2 selects, chemistry,
+        # final select, probe) + 2 per checkpoint segment; backward: the
+        # recorded recomputation (10 per step: + the stage-3 select) + 2 per
+        # segment and 8 adjoint kernels per step (begin, chemistry VJP, and a
+        # sweep and a merge per RK stage)
+        "gpu_launches": 27 * N + 4 * ((N + ADJ_K - 1) // ADJ_K), "clocks": clk,
     }
     print(json.dumps(line), flush=True)
 
