@@ -1493,6 +1493,9 @@ __device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], con
   }
   // Every loop has a constant trip count so the matrix stays in registers;
   // the row exchange is branch-free (selects).
+#if JB_FAST
+  double ipv[NR];
+#endif
 #pragma unroll
   for (int c = 0; c < NR; ++c) {
     int p = c;
@@ -1520,10 +1523,18 @@ __device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], con
       }
     }
     if (J[c][c] == 0.0) st |= JB_ERR_SINGULAR;
+#if JB_FAST
+    // one reciprocal per pivot (kept for the back substitution)
+    ipv[c] = 1.0 / J[c][c];
+#endif
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
       if (r > c) {
+#if JB_FAST
+        const double l = J[r][c] * ipv[c];
+#else
         const double l = J[r][c] / J[c][c];
+#endif
 #pragma unroll
         for (int j = 0; j < NR; ++j)
           if (j > c) J[r][j] = J[r][j] - l * J[c][j];
@@ -1539,12 +1550,23 @@ __device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], con
 #pragma unroll
     for (int j = 0; j < NR; ++j)
       if (j > r) s = s - J[r][j] * x[j];
+#if JB_FAST
+    x[r] = s * ipv[r];
+#else
     x[r] = s / J[r][r];
+#endif
   }
   // detailed_reaction (:183-193): dY = clip(drhoY/rho, -Y, 1-Y); S = rho dY
+#if JB_FAST
+  const double irho = 1.0 / rho;
+#endif
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
+#if JB_FAST
+    double dY = x[k] * irho;
+#else
     double dY = x[k] / rho;
+#endif
     double lo = -Y8[k], hi = 1.0 - Y8[k];
     dY = dY < lo ? lo : dY;
     dY = dY > hi ? hi : dY;
@@ -1678,8 +1700,16 @@ __device__ __forceinline__ void chem_cell_step(const MP& m, const Grid& g, const
   const long long nc = g.ncell;
   {
     double q[nv];
+#if JB_FAST
+    // only rho and the species enter the chemistry; the other fields are
+    // read after it so that they hold no registers across the solve
+    q[0] = U[c];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) q[nY + k] = U[(nY + k) * nc + c];
+#else
 #pragma unroll
     for (int f = 0; f < nv; ++f) q[f] = U[f * nc + c];
+#endif
     double rho = q[0];
     double Y8[NR], S[NR];
 #pragma unroll
@@ -1687,6 +1717,8 @@ __device__ __forceinline__ void chem_cell_step(const MP& m, const Grid& g, const
 #if JB_FAST
     if (GEN) chem_cell_gen(m, rho, Y8, T, dt, S, st, sh, blockDim.x);
     else chem_cell(m, rho, Y8, T, dt, S, st);
+#pragma unroll
+    for (int f = 1; f < nY; ++f) q[f] = U[f * nc + c];
 #else
     (void)sh;
     chem_cell(m, rho, Y8, T, dt, S, st);
