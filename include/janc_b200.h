@@ -102,6 +102,15 @@ long long jb_workspace_bytes(const jb_handle* h);
  * on every call: set_simulator.py:26,44). */
 int jb_set_spacing(jb_handle* h, double dx, double dy);
 
+/* Select the advective flux (replaces set_flux_solver, solver_1D/flux.py:18-35,
+ * solver_2D/flux.py:19-40): JB_FLUX_LF = flux splitting with LF and WENO5-JS
+ * (the default), JB_FLUX_HLLC / JB_FLUX_AUSMPW = godunov_flux
+ * (solver_2D/flux.py:43-54) with WENO5-JS on the primitives and the HLLC
+ * (riemann_solver/HLLC.py) or AUSMPW+ (riemann_solver/AUSMPW_plus.py)
+ * Riemann solver.  The Godunov path computes in float64 in every variant;
+ * jb_adjoint_step supports JB_FLUX_LF only. */
+int jb_set_flux_scheme(jb_handle* h, int scheme);
+
 /* sizeof(jb_mech_params) and sizeof(jb_grid) as compiled, for binding checks. */
 int jb_sizeof_mech_params(void);
 int jb_sizeof_grid(void);

@@ -439,6 +439,14 @@ int jb_kernel_times(jb_handle* h, double* ms, long long* launches) {
   return JB_OK;
 }
 
+int jb_set_flux_scheme(jb_handle* h, int scheme) {
+  if (!h) return JB_ERR_ARG;
+  if (scheme != JB_FLUX_LF && scheme != JB_FLUX_HLLC && scheme != JB_FLUX_AUSMPW)
+    return set_err(h, JB_ERR_ARG, "unknown flux scheme");
+  h->grid.scheme = scheme;
+  return JB_OK;
+}
+
 int jb_set_spacing(jb_handle* h, double dx, double dy) {
   if (!h || !(dx > 0.0) || (h->dim == 2 && !(dy > 0.0))) return set_err(h, JB_ERR_ARG, "bad spacing");
   h->grid.dx = dx;
@@ -516,6 +524,8 @@ static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mu
 static int adj_workspace(jb_handle* h) {
   if (h->adj_ws) return JB_OK;
   if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
+  if (h->grid.scheme != JB_FLUX_LF)
+    return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint differentiates the LF flux-splitting path");
   for (int s = 0; s < 4; ++s)
     if (h->grid.bc[s] == JB_BC_PRESSURE_OUTLET || h->grid.bc[s] == JB_BC_RDC_INJECTOR)
       return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint supports periodic, slip, no-slip and zero-gradient sides");

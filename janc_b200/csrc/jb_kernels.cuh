@@ -1843,5 +1843,7 @@ __global__ void k_dt_from_slots(const Slots* s, double cfl, double* dt_out) {
   *dt_out = cfl * (s->dtnan ? __longlong_as_double(0x7ff8000000000000LL) : bitsd(s->dtmin_next));
 }
 
+#include "jb_godunov.cuh"
+
 }  // namespace JB_NS
 }  // namespace jb

@@ -60,6 +60,11 @@ enum jb_kernel_cat {
 
 enum jb_precision { JB_PREC_STRICT = 0, JB_PREC_FP64 = 1, JB_PREC_MIXED = 2 };
 
+// Advective flux (solver_{1D,2D}/flux.py set_flux_solver): flux splitting
+// (LF, WENO5-JS on the split fluxes) or Godunov (WENO5-JS on the primitives
+// and a Riemann solver).
+enum jb_flux_scheme { JB_FLUX_LF = 0, JB_FLUX_HLLC = 1, JB_FLUX_AUSMPW = 2 };
+
 // status bits (device status word and C-ABI return codes)
 enum jb_status {
   JB_OK = 0,
@@ -83,7 +88,7 @@ typedef struct jb_grid {
   const double* Yinj;    // injector mass fractions [nr][nx] (theta['Yinj'])
   double inj_block_p;    // injector blocked when p_in >= this (1.0 nondim)
   int lstrip;            // ghost strip length max(nx, ny)
-  int pad_;
+  int scheme;            // advective flux (jb_flux_scheme): LF splitting or Godunov + Riemann solver
 } jb_grid;
 
 // Per-step reduction results.  Doubles reduced with atomics are stored as

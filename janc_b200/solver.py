@@ -21,6 +21,37 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def flux_scheme(flux_config):
+    """Validate a reference ``flux_solver_config`` (set_flux_solver,
+    solver_2D/flux.py:19-40) and name the native flux: ``LF``, ``HLLC`` or
+    ``AUSMPW_plus``.  Raises as the reference does: KeyError for an unknown
+    solver type or dictionary entry; what the reference has but this build
+    does not (MUSCL, SW splitting, viscous fluxes) raises NotImplementedError."""
+    if flux_config is None:
+        return "LF"
+    solver_type = flux_config["solver_type"]
+    if solver_type not in ("godunov", "flux_splitting"):
+        raise KeyError("JANC only support 'godunov' and 'flux_splitting'")
+    recon = flux_config["interface_reconstruction"]
+    if recon == "MUSCL":
+        raise NotImplementedError("MUSCL reconstruction is not built; use WENO5_JS")
+    if recon != "WENO5_JS":
+        raise KeyError(recon)
+    if flux_config.get("viscosity", "off") == "on":
+        raise NotImplementedError("viscous fluxes are not built")
+    if solver_type == "godunov":
+        rs = flux_config["riemann_solver"]
+        if rs not in ("HLLC", "AUSMPW_plus"):
+            raise KeyError(rs)
+        return rs
+    split = flux_config["split_method"]
+    if split == "SW":
+        raise NotImplementedError("Steger-Warming splitting is not built; use LF")
+    if split != "LF":
+        raise KeyError(split)
+    return "LF"
+
+
 def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -33,11 +64,17 @@ class Solver:
     ``slip_wall``, ``zero_gradient``, ``no_slip_wall``, ``pressure_outlet`` or
     ``rdc_injector`` (the rotating-detonation injector of the reference's
     example 2, bottom side only).
+
+    ``flux_config`` is the reference's ``flux_solver_config``
+    (solver_{1D,2D}/flux.py set_flux_solver): ``solver_type``
+    ``flux_splitting`` (``split_method`` ``LF``) or ``godunov``
+    (``riemann_solver`` ``HLLC`` or ``AUSMPW_plus``), with
+    ``interface_reconstruction`` ``WENO5_JS``.  Default: LF flux splitting.
     """
 
     def __init__(self, dim, nx, ny=None, dx=1.0, dy=None, boundary_config=None,
                  mechanism=_mech.DEFAULT_MECHANISM, nondim_config=None, precision="fp64",
-                 device=None):
+                 device=None, flux_config=None):
         if dim in ("1D", 1):
             dim = 1
         elif dim in ("2D", 2):
@@ -79,6 +116,8 @@ class Solver:
         _native.check(rc, None, "jb_create")
         self._h = h
         self._lib = L
+        self.flux_scheme = flux_scheme(flux_config)
+        _native.check(L.jb_set_flux_scheme(h, _native.FLUX_SCHEME[self.flux_scheme]), h, "jb_set_flux_scheme")
 
     # ------------------------------------------------------------------ utils
     def close(self):

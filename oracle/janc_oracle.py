@@ -705,6 +705,147 @@ def total_flux(m, Up, Ap, dx, dy=None):
 
 
 # --------------------------------------------------------------------------
+# Godunov path: WENO5-JS on primitives + HLLC / AUSMPW+
+# (solver_{1D,2D}/flux.py godunov_flux, riemann_solver/HLLC.py,
+#  riemann_solver/AUSMPW_plus.py)
+# --------------------------------------------------------------------------
+def _face_thermo(m, rho, p, Y):
+    """T = p / (R rho) of a reconstructed face state, then its gamma and h
+    (HLLC.py:8-12 in 2D, :7-11 in 1D; AUSMPW_plus.py:86-92 / 62-66)."""
+    R = get_R(m, Y)
+    T = p / (R * rho)
+    _, gamma, h, _, _ = get_thermo(m, T, Y)
+    return gamma, h
+
+
+def _hllc(m, qL, qR, dim, n):
+    """HLLC flux through faces with normal velocity component n (1: x,
+    2: y) of primitive face states q = [rho, u, (v), p, Y]
+    (solver_2D/riemann_solver/HLLC.py:15-43 x, :45-73 y; solver_1D HLLC.py:13-42)."""
+    ip = 1 + dim
+    rho_L, rho_R = qL[0:1], qR[0:1]
+    p_L, p_R = qL[ip:ip + 1], qR[ip:ip + 1]
+    Y_L, Y_R = qL[ip + 1:], qR[ip + 1:]
+    gamma_L, h_L = _face_thermo(m, rho_L, p_L, Y_L)
+    gamma_R, h_R = _face_thermo(m, rho_R, p_R, Y_R)
+    a_L = np.sqrt(gamma_L * p_L / rho_L)
+    a_R = np.sqrt(gamma_R * p_R / rho_R)
+    vel_L = [qL[1 + k:2 + k] for k in range(dim)]
+    vel_R = [qR[1 + k:2 + k] for k in range(dim)]
+    un_L, un_R = vel_L[n - 1], vel_R[n - 1]
+    if dim == 2:
+        E_L = rho_L * h_L - p_L + 0.5 * rho_L * (vel_L[0] ** 2 + vel_L[1] ** 2)
+        E_R = rho_R * h_R - p_R + 0.5 * rho_R * (vel_R[0] ** 2 + vel_R[1] ** 2)
+    else:
+        E_L = rho_L * h_L - p_L + 0.5 * rho_L * (vel_L[0] ** 2)
+        E_R = rho_R * h_R - p_R + 0.5 * rho_R * (vel_R[0] ** 2)
+    s_L = np.minimum(un_L - a_L, un_R - a_R)
+    s_R = np.maximum(un_L + a_L, un_R + a_R)
+    s_M = (p_R - p_L + rho_L * un_L * (s_L - un_L) - rho_R * un_R * (s_R - un_R)) / \
+        (rho_L * (s_L - un_L) - rho_R * (s_R - un_R))
+
+    def side(rho, vel, un, p, E, Y, s):
+        U = np.concatenate([rho] + [rho * v for v in vel] + [E, rho * Y], axis=0)
+        star_vel = [s_M if k == n - 1 else vel[k] for k in range(dim)]
+        U_M = rho * (s - un) / (s - s_M) * np.concatenate(
+            [np.ones_like(s_M)] + star_vel + [E / rho + (s_M - un) * (s_M + p / (rho * (s - un))), Y], axis=0)
+        mom = []
+        for k in range(dim):
+            if k == n - 1:
+                mom.append(rho * un ** 2 + p)
+            elif n == 1:
+                mom.append(rho * un * vel[k])      # rho u v through x faces
+            else:
+                mom.append(rho * vel[k] * un)      # rho u v through y faces
+        F = np.concatenate([rho * un] + mom + [un * (E + p), rho * un * Y], axis=0)
+        return F, F + s * (U_M - U)
+
+    F_L, F_L_M = side(rho_L, vel_L, un_L, p_L, E_L, Y_L, s_L)
+    F_R, F_R_M = side(rho_R, vel_R, un_R, p_R, E_R, Y_R, s_R)
+    cond1 = s_L >= 0
+    cond2 = np.logical_and(s_L <= 0, s_M >= 0)
+    cond3 = np.logical_and(s_M <= 0, s_R >= 0)
+    F1 = np.where(cond1, F_L, F_R)
+    F2 = np.where(cond2, F_L_M, F1)
+    return np.where(cond3, F_R_M, F2)
+
+
+def _split_M_and_P(M):
+    """AUSMPW_plus.py:5-11"""
+    ind = np.abs(M) <= 1
+    Mplus = np.where(ind, 1 / 4 * (M + 1) ** 2, 1 / 2 * (M + np.abs(M)))
+    Mminus = np.where(ind, -1 / 4 * (M - 1) ** 2, 1 / 2 * (M - np.abs(M)))
+    Pplus = np.where(ind, 1 / 4 * (M + 1) ** 2 * (2 - M), 1 / 2 * (1 + np.sign(M)))
+    Pminus = np.where(ind, 1 / 4 * (M - 1) ** 2 * (2 + M), 1 / 2 * (1 - np.sign(M)))
+    return Mplus, Mminus, Pplus, Pminus
+
+
+def _ausmpw(m, qL, qR, dim, n):
+    """AUSMPW+ flux (solver_2D/riemann_solver/AUSMPW_plus.py:13-24, 77-131;
+    solver_1D AUSMPW_plus.py).  At y faces the reference takes gamma_R from
+    the x-face states (2D AUSMPW_plus.py:54), whose shape does not broadcast
+    with the y-face arrays, so the reference's 2D AUSMPW+ cannot run; the
+    y faces here use their own gamma_R."""
+    ip = 1 + dim
+    rho_L, rho_R = qL[0:1], qR[0:1]
+    p_L, p_R = qL[ip:ip + 1], qR[ip:ip + 1]
+    Y_L, Y_R = qL[ip + 1:], qR[ip + 1:]
+    gamma_L, h_L = _face_thermo(m, rho_L, p_L, Y_L)
+    gamma_R, h_R = _face_thermo(m, rho_R, p_R, Y_R)
+    un_L, un_R = qL[n:n + 1], qR[n:n + 1]
+    c_L = np.sqrt(gamma_L * p_L / rho_L)
+    c_R = np.sqrt(gamma_R * p_R / rho_R)
+    c = 0.5 * (c_L + c_R)
+    M_L, M_R = un_L / c, un_R / c
+
+    def phi(rho, q, h, Y):
+        vel = [q[1 + k:2 + k] for k in range(dim)]
+        kin = vel[0] ** 2 + vel[1] ** 2 if dim == 2 else vel[0] ** 2
+        return np.concatenate([rho] + [rho * v for v in vel] + [rho * h + 0.5 * rho * kin, rho * Y], axis=0)
+
+    phi_L, phi_R = phi(rho_L, qL, h_L, Y_L), phi(rho_R, qR, h_R, Y_R)
+    M_L_plus, _, P_L_plus, _ = _split_M_and_P(M_L)
+    _, M_R_minus, _, P_R_minus = _split_M_and_P(M_R)
+    p_s = P_L_plus * p_L + P_R_minus * p_R
+    mask = np.minimum(p_L / p_R, p_R / p_L)
+    w = 1 - mask * (mask * mask)  # jnp x**3 is lax.integer_pow: x * (x * x)
+    fL = np.where(np.abs(M_L) < 1.0, p_L / p_s - 1, np.zeros_like(p_L))
+    fR = np.where(np.abs(M_R) < 1.0, p_R / p_s - 1, np.zeros_like(p_R))
+    ind = M_L_plus + M_R_minus >= 0
+    M_L_av = np.where(ind, M_L_plus + M_R_minus * ((1 - w) * (1 + fR) - fL), M_L_plus * w * (1 + fL))
+    M_R_av = np.where(ind, M_R_minus * w * (1 + fR), M_R_minus + M_L_plus * ((1 - w) * (1 + fL) - fR))
+    P_L = np.zeros_like(phi_L)
+    P_L[n:n + 1] = p_L
+    P_R = np.zeros_like(phi_R)
+    P_R[n:n + 1] = p_R
+    return M_L_av * c * phi_L + M_R_av * c * phi_R + (P_L_plus * P_L + P_R_minus * P_R)
+
+
+RIEMANN = {"HLLC": _hllc, "AUSMPW_plus": _ausmpw}
+
+
+def godunov_flux(m, Up, Ap, dx, dy=None, riemann="HLLC"):
+    """godunov_flux (solver_1D/flux.py:41-49, solver_2D/flux.py:43-54) on the
+    ghost-padded arrays: primitives q = [rho, u, (v), p, Y], WENO5-JS
+    left / right face states per component, the Riemann flux, and
+    -(dF/dx [+ dG/dy])."""
+    rs = RIEMANN[riemann]
+    if Up.ndim == 2:
+        rho, u, Y, p, a = U_to_prim(m, Up, Ap)
+        q = np.concatenate([rho, u, p, Y], axis=0)
+        F = rs(m, _interface_L(q, 1, None), _interface_R(q, 1, None), 1, 1)
+        dF = F[:, 1:] - F[:, :-1]
+        return -(dF / dx)
+    rho, u, v, Y, p, a = U_to_prim(m, Up, Ap)
+    q = np.concatenate([rho, u, v, p, Y], axis=0)
+    F = rs(m, _interface_L(q, 1, 2), _interface_R(q, 1, 2), 2, 1)
+    G = rs(m, _interface_L(q, 2, 1), _interface_R(q, 2, 1), 2, 2)
+    dF = F[:, 1:, :] - F[:, :-1, :]
+    dG = G[:, :, 1:] - G[:, :, :-1]
+    return -(dF / dx + dG / dy)
+
+
+# --------------------------------------------------------------------------
 # solver wiring  (simulation/set_simulator.py, time_step/TVD_RK3.py)
 # --------------------------------------------------------------------------
 class Solver:
@@ -712,16 +853,23 @@ class Solver:
     ``advance_one_step`` and ``advance_func`` with the reference's
     signatures (set_simulator.py:20-125, 410-447)."""
 
-    def __init__(self, mech, dim, dx, dy=None, bc=None, cfl=None):
+    def __init__(self, mech, dim, dx, dy=None, bc=None, cfl=None, flux_config=None):
         self.m = mech
         self.dim = dim
         self.dx, self.dy = dx, dy
         self.bc = bc
         self.cfl = cfl
         self.last_iters = []
+        # solver_{1D,2D}/flux.py set_flux_solver: flux splitting (LF) or
+        # godunov with a Riemann solver, WENO5-JS reconstruction
+        fc = flux_config or {"solver_type": "flux_splitting"}
+        self.solver_type = fc["solver_type"]
+        self.riemann = fc.get("riemann_solver", "HLLC")
 
     def flux_func(self, U, aux, dx, dy, dt, theta=None):
         Up, Ap = boundary_conditions(self.m, U, aux, self.bc, theta)
+        if self.solver_type == "godunov":
+            return dt * godunov_flux(self.m, Up, Ap, dx, dy, self.riemann)
         return dt * (total_flux(self.m, Up, Ap, dx, dy))
 
     def update_func(self, U, aux):
