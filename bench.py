@@ -284,11 +284,17 @@ def _setup_workload(args, precision):
         nx, ny = NX, NY
         dx, dy = LX / NX, LY / NY
         bc = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
-        s = Solver(2, nx, ny, dx, dy, bc, precision=precision)
+        fc = None
+        if args.flux != "LF":
+            fc = {"solver_type": "godunov", "interface_reconstruction": "WENO5_JS",
+                  "riemann_solver": args.flux, "viscosity": "off"}
+        s = Solver(2, nx, ny, dx, dy, bc, precision=precision, flux_config=fc)
         P, T, Y = c1_fields()
+        scheme = ("WENO5-JS + LF" if args.flux == "LF" else
+                  f"Godunov (WENO5-JS on primitives + {args.flux}, float64)")
         workload = ("2D H2-air detonation channel 1024x256 (0.2 m x 0.05 m), 9sp/19r mechanism, "
                     "30 atm / 3000 K slab with 8 seeded +-5% blobs, slip walls, "
-                    "WENO5-JS + LF + SSP-RK3 + point-implicit chemistry")
+                    f"{scheme} + SSP-RK3 + point-implicit chemistry")
     else:
         nx, ny = RDC_NX, RDC_NY
         dx = dy = 1e-4 / RDC_ND["x0"]
@@ -509,15 +515,18 @@ def run_ours(args):
         # select, step begin, 3 flux stages (two kernels each in the mixed
         # variant), 2 stage selects, chemistry, final select
         # (+ 4 ghost-strip launches on the RDC workload's outlet / injector sides)
-        "gpu_launches": ((13 if args.precision == "mixed" else 10) + (4 if args.workload == "rdc" else 0))
-                        * args.steps,
+        "gpu_launches": ((13 if args.precision == "mixed" and args.flux == "LF" else 10)
+                         + (4 if args.workload == "rdc" else 0)) * args.steps,
         "roofline": {"bound": "hbm", "kernel": {
                          "chem": "k_chem (point-implicit chemistry + final Halley)",
-                         "flux": ("flux stage: k_sweep_x + k_flux_y_rk (LF + WENO5 + RK stage + Halley)"
+                         "flux": ("k_god2d (WENO5 on primitives + Riemann solver + RK stage + Halley)"
+                                  if args.flux != "LF" else
+                                  "flux stage: k_sweep_x + k_flux_y_rk (LF + WENO5 + RK stage + Halley)"
                                   if args.precision == "mixed" else
                                   "k_flux2d (LF + WENO5 + RK stage + Halley)")}[dom],
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "traffic": (TRAFFIC_PER_CELL[dom] * ncell if args.workload == "channel" and
+                                 args.flux == "LF" and
                                  args.precision == "mixed" else None),
                      "traffic_source": "ncu dram bytes of one stage's launches on this workload, each "
                                        "launch cold (mixed precision)",
@@ -1009,6 +1018,9 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the float64 comparison run")
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--workload", default="channel", choices=["channel", "rdc", "ensemble", "adjoint"])
+    ap.add_argument("--flux", default="LF", choices=["LF", "HLLC", "AUSMPW_plus"],
+                    help="advective flux of the channel workload (LF flux splitting or a Godunov "
+                         "Riemann solver)")
     ap.add_argument("--fd-directions", type=int, default=16,
                     help="adjoint: finite-difference directions per kind")
     ap.add_argument("--ens-shape", default="",
