@@ -111,6 +111,15 @@ int jb_set_spacing(jb_handle* h, double dx, double dy);
  * jb_adjoint_step supports JB_FLUX_LF only. */
 int jb_set_flux_scheme(jb_handle* h, int scheme);
 
+/* Viscous fluxes (flux_solver_config 'viscosity': 'on'; replaces
+ * transport_model.set_transport, model/transport_model.py:26-104, and
+ * viscous_flux, solver_2D/flux.py:70-115 / solver_1D/flux.py:67-99): the
+ * laminar transport model of *tr is used by every later flux evaluation of
+ * the handle (added to the advective flux as NS_flux does, solver_2D/flux.py:117).
+ * tr = NULL switches back to Euler fluxes.  Allocates its scratch on the first
+ * call.  jb_adjoint_step supports the inviscid path only. */
+int jb_set_transport(jb_handle* h, const jb_transport* tr);
+
 /* sizeof(jb_mech_params) and sizeof(jb_grid) as compiled, for binding checks. */
 int jb_sizeof_mech_params(void);
 int jb_sizeof_grid(void);

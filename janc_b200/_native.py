@@ -20,7 +20,7 @@ STATUS = {1: "bad argument", 2: "CUDA error", 4: "non-finite state", 8: "singula
 
 EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_func", "jb_update_aux",
            "jb_reaction_source_terms", "jb_advance", "jb_cfl_dt", "jb_get_thermo", "jb_status",
-           "jb_workspace_bytes", "jb_set_spacing", "jb_set_flux_scheme", "jb_sizeof_mech_params",
+           "jb_workspace_bytes", "jb_set_spacing", "jb_set_flux_scheme", "jb_set_transport", "jb_sizeof_mech_params",
            "jb_sizeof_grid",
            "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times",
            "jb_update_aux_noalloc", "jb_rk3", "jb_u_to_prim",
@@ -39,6 +39,13 @@ class JancError(RuntimeError):
 
 def status_text(code):
     return ", ".join(v for k, v in STATUS.items() if code & k) or "ok"
+
+
+class Transport(ctypes.Structure):
+    """jb_transport (laminar transport model of the viscous fluxes)."""
+    _fields_ = [("viscosity_model", ctypes.c_int), ("conductivity_model", ctypes.c_int),
+                ("diffusivity_model", ctypes.c_int), ("pad_", ctypes.c_int)] + \
+        [(n, ctypes.c_double) for n in ("mu_ref", "T_ref", "S", "nu0", "Pr", "Le", "k0", "D0", "Pr_t", "Le_t")]
 
 
 def lib(path=None):
@@ -70,6 +77,7 @@ def lib(path=None):
     L.jb_workspace_bytes.restype = ll
     L.jb_set_spacing.argtypes = [vp, d, d]
     L.jb_set_flux_scheme.argtypes = [vp, i]
+    L.jb_set_transport.argtypes = [vp, ctypes.POINTER(Transport)]
     L.jb_probe_fp64_fma.argtypes = [i, i, dp, vp]
     L.jb_set_kernel_timing.argtypes = [vp, i]
     L.jb_update_aux_noalloc.argtypes = [ctypes.POINTER(_mech.MechParams), i, i, i, i, dp, dp, dp, vp]

@@ -41,6 +41,9 @@ struct jb_handle {
   double base_A[JB_NREAC_MAX];  // pre-exponential factors as created (jb_set_log_A_offset)
   int probe[4];                 // x0, y0, wx, wy of the pressure probe (wx*wy = 0: none)
   void* fwork;                  // mixed 2D flux scratch (float32 primitives, x flux differences)
+  jb_transport tr;              // laminar transport model (viscous fluxes when grid.visc is set)
+  double* vbuf;                 // viscous node planes and node fluxes
+  double* vcell;                // viscous rhs of the current stage state (nv x ncell)
   double* adj_ws;               // stage adjoints, primitives, face scratch, reductions
   unsigned char* adj_mult;      // padded-grid multiplicity of each cell (alpha ties)
   double* adj_B1;
@@ -196,6 +199,7 @@ int jb_destroy(jb_handle* h) {
   if (h->strips) cudaFree(h->strips);
   if (h->slots) cudaFree(h->slots);
   if (h->fwork) cudaFree(h->fwork);
+  if (h->vbuf) cudaFree(h->vbuf);
   if (h->adj_ws) cudaFree(h->adj_ws);
   if (h->adj_mult) cudaFree(h->adj_mult);
   delete h;
@@ -229,6 +233,8 @@ int jb_flux_func(jb_handle* h, const double* U, const double* aux, double dt, do
   JB_TRY(o.select(h->dim, false, true, false, h->mech, h->grid, U, aux, nullptr, nullptr, h->strips,
                   h->slots, -1, 3, nullptr, st),
          "alpha");
+  if (h->grid.visc)
+    JB_TRY(o.visc(h->dim, h->mech, h->grid, h->tr, U, aux, h->strips, h->vbuf, h->vcell, st), "viscous");
   JB_TRY(o.flux(h->dim, 0, h->mech, h->grid, U, aux, nullptr, rhs, nullptr, h->strips, h->slots, 3,
                 -1, dt, nullptr, st),
          "flux");
@@ -306,11 +312,15 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     double* Ao = r ? r + RS + nU : aux_out;
     JB_TIMED(JB_KCAT_OTHER, o.step_begin(h->slots, use_cfl ? cfl : 0.0, dt_fixed, dt_hist, s, st), "step_begin");
     // stage 1: U1 = U + L(U)
+    if (g.visc)
+      JB_TIMED(JB_KCAT_FLUX, o.visc(d, m, g, h->tr, Un, an, h->strips, h->vbuf, h->vcell, st), "viscous");
     JB_TIMED(JB_KCAT_FLUX, o.flux(d, 1, m, g, Un, an, Un, W1, h->cand, h->strips, h->slots, 0, 0, 0.0, h->fwork, st), "stage1");
     JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W1, nullptr, h->cand, A1, h->strips,
                     h->slots, 0, 1, h->fwork, st),
            "select1");
     // stage 2: U2 = 3/4 U + 1/4 (U1 + L(U1))
+    if (g.visc)
+      JB_TIMED(JB_KCAT_FLUX, o.visc(d, m, g, h->tr, W1, A1, h->strips, h->vbuf, h->vcell, st), "viscous");
     JB_TIMED(JB_KCAT_FLUX, o.flux(d, 2, m, g, W1, A1, Un, W2, h->cand, h->strips, h->slots, 1, 1,
                   0.0, h->fwork, st),
            "stage2");
@@ -318,6 +328,8 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
                     h->slots, 1, 2, h->fwork, st),
            "select2");
     // stage 3: U3 = 1/3 U + 2/3 (U2 + L(U2))
+    if (g.visc)
+      JB_TIMED(JB_KCAT_FLUX, o.visc(d, m, g, h->tr, W2, A2, h->strips, h->vbuf, h->vcell, st), "viscous");
     JB_TIMED(JB_KCAT_FLUX, o.flux(d, 3, m, g, W2, A2, Un, W3, h->cand, h->strips, h->slots, 2, 2,
                   0.0, h->fwork, st),
            "stage3");
@@ -439,6 +451,32 @@ int jb_kernel_times(jb_handle* h, double* ms, long long* launches) {
   return JB_OK;
 }
 
+int jb_set_transport(jb_handle* h, const jb_transport* tr) {
+  if (!h) return JB_ERR_ARG;
+  if (!tr) {  // Euler fluxes again
+    if (h->vbuf) cudaFree(h->vbuf);
+    h->vbuf = h->vcell = nullptr;
+    h->grid.visc = nullptr;
+    return JB_OK;
+  }
+  const jb_transport& t = *tr;
+  auto bad01 = [](int v) { return v != 0 && v != 1; };
+  if (bad01(t.viscosity_model) || bad01(t.conductivity_model) || bad01(t.diffusivity_model))
+    return set_err(h, JB_ERR_ARG, "unknown transport model");
+  if (!(t.Pr > 0.0) || !(t.Le > 0.0) || !(t.Pr_t > 0.0) || !(t.Le_t > 0.0) ||
+      (t.viscosity_model == 0 && !(t.T_ref > 0.0)))
+    return set_err(h, JB_ERR_ARG, "transport parameters must be positive");
+  if (!h->vbuf) {
+    const long long n = jb::visc_scratch_doubles(h->dim, h->grid) + (long long)h->grid.nv * h->grid.ncell;
+    JB_TRY(cudaMalloc(&h->vbuf, sizeof(double) * n), "viscous scratch");
+    h->vcell = h->vbuf + jb::visc_scratch_doubles(h->dim, h->grid);
+    h->ws_bytes += (long long)sizeof(double) * n;
+  }
+  h->tr = t;
+  h->grid.visc = h->vcell;
+  return JB_OK;
+}
+
 int jb_set_flux_scheme(jb_handle* h, int scheme) {
   if (!h) return JB_ERR_ARG;
   if (scheme != JB_FLUX_LF && scheme != JB_FLUX_HLLC && scheme != JB_FLUX_AUSMPW)
@@ -524,8 +562,8 @@ static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mu
 static int adj_workspace(jb_handle* h) {
   if (h->adj_ws) return JB_OK;
   if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
-  if (h->grid.scheme != JB_FLUX_LF)
-    return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint differentiates the LF flux-splitting path");
+  if (h->grid.scheme != JB_FLUX_LF || h->grid.visc)
+    return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint differentiates the inviscid LF flux-splitting path");
   for (int s = 0; s < 4; ++s)
     if (h->grid.bc[s] == JB_BC_PRESSURE_OUTLET || h->grid.bc[s] == JB_BC_RDC_INJECTOR)
       return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint supports periodic, slip, no-slip and zero-gradient sides");

@@ -8,6 +8,10 @@
 
 constexpr int RS_HLLC = 0, RS_AUSMPW = 1;
 
+// jnp.minimum / jnp.maximum: a NaN operand gives NaN (fmin / fmax drop it)
+__device__ __forceinline__ double nan_min(double a, double b) { return (a != a || b != b) ? a + b : fmin(a, b); }
+__device__ __forceinline__ double nan_max(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
+
 // gamma and h of a reconstructed face state from T = p / (R rho)
 // (HLLC.py:8-12 / AUSMPW_plus.py:86-92 in 2D).
 __device__ __forceinline__ void face_thermo(const MP& m, double rho, double p, const double* Y8, double& gamma,
@@ -38,8 +42,8 @@ __device__ __forceinline__ void hllc_flux(const MP& m, const double* wL, const d
   const double kR = DIM == 2 ? wR[1] * wR[1] + wR[2] * wR[2] : wR[1] * wR[1];
   const double EL = rL * hL - pL + 0.5 * rL * kL;
   const double ER = rR * hR - pR + 0.5 * rR * kR;
-  const double sL = fmin(unL - aL, unR - aR);
-  const double sR = fmax(unL + aL, unR + aR);
+  const double sL = nan_min(unL - aL, unR - aR);
+  const double sR = nan_max(unL + aL, unR + aR);
   const double sM = (pR - pL + rL * unL * (sL - unL) - rR * unR * (sR - unR)) / (rL * (sL - unL) - rR * (sR - unR));
   const bool c1 = sL >= 0.0, c2 = sL <= 0.0 && sM >= 0.0, c3 = sM <= 0.0 && sR >= 0.0;
   // the star-state factor and energy of each side
@@ -105,7 +109,7 @@ __device__ __forceinline__ void ausmpw_flux(const MP& m, const double* wL, const
     PRm = 1.0 / 2.0 * (1.0 - ausm_sign(MR));
   }
   const double ps = PLp * pL + PRm * pR;
-  const double mk = fmin(pL / pR, pR / pL);
+  const double mk = nan_min(pL / pR, pR / pL);
   const double w = 1.0 - mk * (mk * mk);
   const double fl = fabs(ML) < 1.0 ? pL / ps - 1.0 : 0.0;
   const double fr = fabs(MR) < 1.0 ? pR / ps - 1.0 : 0.0;
@@ -246,9 +250,9 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
       const double dF = sFx[f * SM2_FX + (ix + 1) * TY2 + iy] - sFx[f * SM2_FX + ix * TY2 + iy];
       const double dG = sFy[f * SM2_FY + ix * (TY2 + 1) + iy + 1] - sFy[f * SM2_FY + ix * (TY2 + 1) + iy];
 #if JB_FAST
-      const double rhs = dt * (-(dF * g.idx + dG * g.idy));
+      const double rhs = dt * visc_add(g, f, cell, -(dF * g.idx + dG * g.idy));
 #else
-      const double rhs = dt * (-(dF / g.dx + dG / g.dy));
+      const double rhs = dt * visc_add(g, f, cell, -(dF / g.dx + dG / g.dy));
 #endif
       const double uk = Uk[f * nc + cell];
       double r;
@@ -342,9 +346,9 @@ __global__ void __launch_bounds__(NT1) k_god1d(MP m, Grid g, const double* __res
     for (int f = 0; f < 11; ++f) {
       const double dF = sF[f * NT1 + tid + 1] - sF[f * NT1 + tid];
 #if JB_FAST
-      const double rhs = dt * (-(dF * g.idx));
+      const double rhs = dt * visc_add(g, f, cell, -(dF * g.idx));
 #else
-      const double rhs = dt * (-(dF / g.dx));
+      const double rhs = dt * visc_add(g, f, cell, -(dF / g.dx));
 #endif
       const double uk = Uk[f * nc + cell];
       double r;

@@ -119,6 +119,12 @@ __device__ __forceinline__ double poly6(const double* c, double T) {
   return y;
 }
 
+// advective + viscous rhs of field f at cell (NS_flux, solver_2D/flux.py:117-118);
+// g.visc holds the viscous part computed for the stage state, or is null
+__device__ __forceinline__ double visc_add(const Grid& g, int f, long long cell, double adv) {
+  return g.visc ? adv + g.visc[f * g.ncell + cell] : adv;
+}
+
 // fill_Y (thermo_model.py:80-82): the last species closes the mass balance.
 __device__ __forceinline__ void fill_Y(const double* Y8, double* Yf) {
   double s = Y8[0];
@@ -873,9 +879,9 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       double dF = (double)(sFx[(ix + 1) * TY2 + iy] - sFx[ix * TY2 + iy]);
       double dG = (double)(sFy[ix * (TY2 + 1) + iy + 1] - sFy[ix * (TY2 + 1) + iy]);
 #if JB_FAST
-      double rhs = dt * (-(dF * g.idx + dG * g.idy));
+      double rhs = dt * visc_add(g, f, cell, -(dF * g.idx + dG * g.idy));
 #else
-      double rhs = dt * (-(dF / g.dx + dG / g.dy));
+      double rhs = dt * visc_add(g, f, cell, -(dF / g.dx + dG / g.dy));
 #endif
       // the state itself is float64 in every variant
       double uk = EXACT ? (double)sQ[f * SM2_Q + (ix + 3) * PY2 + (iy + 3)] : Uk[f * nc + cell];
@@ -1116,7 +1122,7 @@ __global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const doub
     for (int f = 0; f < 12; ++f) {
       const double dF = (double)dfx[f * nc + cell];
       const double dG = (double)(sF[f * YR_F + l + 1] - sF[f * YR_F + l]);
-      const double rhs = dt * (-(dF * g.idx + dG * g.idy));
+      const double rhs = dt * visc_add(g, f, cell, -(dF * g.idx + dG * g.idy));
       const double uk = ukr[f];
       double r;
       if (STAGE == 1) r = uk + rhs;
@@ -1229,9 +1235,9 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
     if (live) {
       double dF = (double)(sF[tid + 1] - sF[tid]);
 #if JB_FAST
-      double rhs = dt * (-(dF * g.idx));
+      double rhs = dt * visc_add(g, f, cell, -(dF * g.idx));
 #else
-      double rhs = dt * (-(dF / g.dx));
+      double rhs = dt * visc_add(g, f, cell, -(dF / g.dx));
 #endif
       double uk = EXACT ? (double)sQ[f * PX1 + tid + 3] : Uk[f * nc + cell];
       double r;
@@ -1844,6 +1850,7 @@ __global__ void k_dt_from_slots(const Slots* s, double cfl, double* dt_out) {
 }
 
 #include "jb_godunov.cuh"
+#include "jb_viscous.cuh"
 
 }  // namespace JB_NS
 }  // namespace jb

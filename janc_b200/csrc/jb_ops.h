@@ -33,11 +33,23 @@ struct Ops {
   cudaError_t (*prim)(int dim, const jb_mech_params& m, const jb_grid& g, const double* U,
                       const double* aux, double* rho, double* u, double* v, double* Y, double* p,
                       double* a, cudaStream_t st);
+  // viscous rhs of (Uk, auxk) into V; vbuf: visc_scratch_doubles(dim, g)
+  cudaError_t (*visc)(int dim, const jb_mech_params& m, const jb_grid& g, const jb_transport& tr,
+                      const double* Uk, const double* auxk, const double* strips, double* vbuf, double* V,
+                      cudaStream_t st);
   cudaError_t (*slots_reset)(jb_slots* s, cudaStream_t st);
   cudaError_t (*step_begin)(jb_slots* s, double cfl, double dt_fixed, double* dt_hist, int step,
                             cudaStream_t st);
   cudaError_t (*dt_from_slots)(const jb_slots* s, double cfl, double* dt_out, cudaStream_t st);
 };
+
+// Doubles of the viscous scratch (node planes and node fluxes) of a grid.
+inline long long visc_scratch_doubles(int dim, const jb_grid& g) {
+  const long long PY = dim == 2 ? g.ny + 6 : 1, np = (long long)(g.nx + 6) * PY;
+  const long long sF = dim == 2 ? (long long)(g.nx + 6) * g.ny : g.nx + 6;
+  const long long sG = dim == 2 ? (long long)g.nx * PY : 0;
+  return (dim == 2 ? 13 : 12) * np + (dim == 2 ? 12 : 11) * (sF + sG);
+}
 
 extern const Ops strict_ops;
 extern const Ops fast_ops;

@@ -65,6 +65,16 @@ enum jb_precision { JB_PREC_STRICT = 0, JB_PREC_FP64 = 1, JB_PREC_MIXED = 2 };
 // and a Riemann solver).
 enum jb_flux_scheme { JB_FLUX_LF = 0, JB_FLUX_HLLC = 1, JB_FLUX_AUSMPW = 2 };
 
+// Laminar transport (model/transport_model.py set_transport): viscosity
+// 0 Sutherland mu_ref (T/T_ref)^1.5 (T_ref+S)/(T+S), 1 constant rho nu0;
+// conductivity 0 Prandtl number mu cp/Pr, 1 constant k0; diffusivity 0 Lewis
+// number rho D_k = k_k/(Le cp_k) (a Schmidt number gives Le = Sc/Pr), 1
+// constant D0.  Pr_t and Le_t enter only through the zero turbulent viscosity.
+typedef struct jb_transport {
+  int viscosity_model, conductivity_model, diffusivity_model, pad_;
+  double mu_ref, T_ref, S, nu0, Pr, Le, k0, D0, Pr_t, Le_t;
+} jb_transport;
+
 // status bits (device status word and C-ABI return codes)
 enum jb_status {
   JB_OK = 0,
@@ -89,6 +99,7 @@ typedef struct jb_grid {
   double inj_block_p;    // injector blocked when p_in >= this (1.0 nondim)
   int lstrip;            // ghost strip length max(nx, ny)
   int scheme;            // advective flux (jb_flux_scheme): LF splitting or Godunov + Riemann solver
+  const double* visc;    // viscous rhs of the stage state (ncell x nv) or null: Euler fluxes
 } jb_grid;
 
 // Per-step reduction results.  Doubles reduced with atomics are stored as

@@ -1,0 +1,253 @@
+// Laminar viscous flux (solver_{1D,2D}/flux.py viscous_flux_node /
+// viscous_flux; model/transport_model.py; finite_difference/CENTRAL6.py;
+// reconstruction/CENTRAL6.py).  Three passes over the ghost-padded grid:
+//   k_visc_nodes  rho, u, (v), T, Y (9, filled) of every padded node,
+//                 corners included (they hold the periodic wrap of the pad)
+//   k_visc_flux   the node fluxes F_hat (x) and G_hat (y) from sixth-order
+//                 derivatives (one-sided at the padded array's ends) and the
+//                 transport model
+//   k_visc_div    sixth-order interface values and their divergence per cell
+// The result V = dF_hat/dx (+ dG_hat/dy) is added to the advective rhs by the
+// stage kernels (NS_flux = advective + viscous, solver_2D/flux.py:117-118).
+// Included by jb_kernels.cuh inside namespace jb::JB_NS.
+#pragma once
+
+// The padded grid's entry (x, y): interior, side ghost (boundary conditions)
+// or corner (periodic wrap of both axes, boundary_padding.py pad_2D).
+template <int DIM>
+__device__ __forceinline__ Src map_padded(const Grid& g, int x, int y) {
+  if (DIM == 2 && (x < 0 || x >= g.nx) && (y < 0 || y >= g.ny)) {
+    Src s;
+    s.kind = 0;
+    s.xs = x < 0 ? g.nx - 1 + x : x - g.nx + 1;
+    s.ys = y < 0 ? g.ny - 1 + y : y - g.ny + 1;
+    s.side = 0;
+    s.pos = 0;
+    s.flip = 0;
+    return s;
+  }
+  return map_cell<DIM>(g, x, y);
+}
+
+// node planes: 2D rho, u, v, T, Y0..Y8 (13); 1D rho, u, T, Y0..Y8 (12)
+template <int DIM>
+__global__ void __launch_bounds__(256) k_visc_nodes(MP m, Grid g, const double* __restrict__ Uk,
+                                                    const double* __restrict__ auxk,
+                                                    const double* __restrict__ strips, double* __restrict__ nodes) {
+  constexpr int nY = DIM == 1 ? 3 : 4, nv = nY + NR;
+  const int PY = DIM == 2 ? g.ny + 6 : 1;
+  const long long np = (long long)(g.nx + 6) * PY;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int px = (int)(i / PY), py = (int)(i % PY);
+  const Src s = map_padded<DIM>(g, px - 3, DIM == 2 ? py - 3 : 0);
+  const long long nc = g.ncell;
+  double q[nv], T = 1.0;
+  if (s.kind == 0) {
+    const long long c = DIM == 2 ? (long long)s.xs * g.ny + s.ys : s.xs;
+#pragma unroll
+    for (int f = 0; f < nv; ++f) {
+      const double v = Uk[f * nc + c];
+      q[f] = ((s.flip >> f) & 1) ? -v : v;
+    }
+    T = auxk[nc + c];
+  } else {
+#pragma unroll
+    for (int f = 0; f < nv; ++f) q[f] = strips[strip_idx(g, s.side, f, s.pos)];
+    T = strips[strip_idx(g, s.side, nv + 1, s.pos)];
+  }
+  const double rho = q[0];
+  double Y8[NR], Yf[NS];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / rho;
+  fill_Y(Y8, Yf);
+  nodes[i] = rho;
+  nodes[np + i] = q[1] / rho;
+  if (DIM == 2) nodes[2 * np + i] = q[2] / rho;
+  nodes[(DIM + 1) * np + i] = T;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) nodes[(DIM + 2 + k) * np + i] = Yf[k];
+}
+
+// d/dx of a node plane along one line (finite_difference/CENTRAL6.py d_dx):
+// f points at position 0 of the line, stride st, n positions, at position p.
+__device__ __forceinline__ double d_line(const double* f, long long st, int n, int p, double d) {
+  auto F = [&](int j) { return f[(long long)j * st]; };
+  if (p >= 3 && p < n - 3)
+    return (-F(p - 3) + 9.0 * F(p - 2) - 45.0 * F(p - 1) + 45.0 * F(p + 1) - 9.0 * F(p + 2) + F(p + 3)) /
+           (60.0 * d);
+  if (p == 0) return (F(1) - F(0)) / d;
+  if (p == 1) return (F(2) - F(0)) / (2.0 * d);
+  if (p == 2) return (F(0) - 8.0 * F(1) + 8.0 * F(3) - F(4)) / (12.0 * d);
+  if (p == n - 3) return (F(n - 5) - 8.0 * F(n - 4) + 8.0 * F(n - 2) - F(n - 1)) / (12.0 * d);
+  if (p == n - 2) return (F(n - 1) - F(n - 3)) / (2.0 * d);
+  return (F(n - 1) - F(n - 2)) / d;
+}
+
+// transport at one node (transport_model.py:106-157, laminar: mu_t = 0)
+struct NodeTransport {
+  double mu, k, D[NS], h[NS];
+};
+
+__device__ __forceinline__ void node_transport(const MP& m, const jb_transport& tr, double rho, double T,
+                                               const double* Yf, NodeTransport& o) {
+  double cpk[NS], cp = 0.0;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    const bool lo = T < m.Tcr[k];
+    cpk[k] = lo ? poly5(m.cp_lo[k], T) : poly5(m.cp_hi[k], T);
+    o.h[k] = lo ? poly6(m.h_lo[k], T) : poly6(m.h_hi[k], T);
+    cp = k == 0 ? cpk[0] * Yf[0] : cp + cpk[k] * Yf[k];
+  }
+  const double mu_t = 0.0;
+  if (tr.viscosity_model == 0) o.mu = tr.mu_ref * pow(T / tr.T_ref, 1.5) * (tr.T_ref + tr.S) / (T + tr.S);
+  else o.mu = rho * tr.nu0;
+  if (tr.conductivity_model == 0) o.k = o.mu * cp / tr.Pr + mu_t * cp / tr.Pr_t;
+  else o.k = tr.k0 + mu_t * cp / tr.Pr_t;
+  const double pr_on = tr.conductivity_model == 0 ? 1.0 : 0.0, k_on = tr.conductivity_model == 0 ? 0.0 : 1.0;
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    if (tr.diffusivity_model == 0) {
+      const double k_i = pr_on * o.mu * cpk[k] / tr.Pr + k_on * tr.k0;
+      const double rhoD_i = k_i / (tr.Le * cpk[k]);
+      const double k_t = mu_t / tr.Pr_t;
+      const double rhoD_t = k_t / (tr.Le_t * cpk[k]);
+      o.D[k] = (rhoD_i + rhoD_t) / rho;
+    } else {
+      const double k_t = mu_t / tr.Pr_t;
+      const double rhoD_t = k_t / tr.Le_t * cpk[k];
+      o.D[k] = tr.D0 + rhoD_t / rho;
+    }
+  }
+}
+
+// Node fluxes: 2D threads [0, nF) take F_hat at padded (px, py), px in
+// [0, nx+6), py in [3, ny+3) -> fh[c][px][py-3]; the rest G_hat at px in
+// [3, nx+3), py in [0, ny+6) -> gh[c][px-3][py].  1D: F_hat at every padded px.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_visc_flux(MP m, Grid g, jb_transport tr, const double* __restrict__ nodes,
+                                                   double* __restrict__ fh, double* __restrict__ gh) {
+  const int PX = g.nx + 6, PY = DIM == 2 ? g.ny + 6 : 1;
+  const long long np = (long long)PX * PY;
+  const long long nF = DIM == 2 ? (long long)PX * g.ny : PX;
+  const long long nG = DIM == 2 ? (long long)g.nx * PY : 0;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nF + nG) return;
+  const bool xf = t < nF;
+  int px, py;
+  if (DIM == 1) {
+    px = (int)t;
+    py = 0;
+  } else if (xf) {
+    px = (int)(t / g.ny);
+    py = (int)(t % g.ny) + 3;
+  } else {
+    px = (int)((t - nF) / PY) + 3;
+    py = (int)((t - nF) % PY);
+  }
+  const long long i = (long long)px * PY + py;
+  const double* N = nodes;
+  const double rho = N[i], u = N[np + i];
+  const double v = DIM == 2 ? N[2 * np + i] : 0.0;
+  const double T = N[(DIM + 1) * np + i];
+  double Yf[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) Yf[k] = N[(DIM + 2 + k) * np + i];
+  NodeTransport tp;
+  node_transport(m, tr, rho, T, Yf, tp);
+  // derivatives along x (stride PY, PX positions) and y (stride 1, PY positions)
+  const double* lx = N + (long long)py;           // line at this y, position px
+  const double* ly = N + (long long)px * PY;      // line at this x, position py
+  auto ddx = [&](int plane) { return d_line(lx + plane * np, PY, PX, px, g.dx); };
+  auto ddy = [&](int plane) { return d_line(ly + plane * np, 1, PY, py, g.dy); };
+  double* out;
+  long long ostride, oidx;
+  if (DIM == 1) {
+    const double du_dx = ddx(1), dT_dx = ddx(2);
+    const double div_u = du_dx;
+    const double tau = 2.0 * tp.mu * du_dx - 2.0 / 3.0 * tp.mu * div_u;
+    const double qx = -tp.k * dT_dx;
+    double jx[NS], e = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      jx[k] = -rho * tp.D[k] * ddx(3 + k);
+      e = k == 0 ? jx[0] * tp.h[0] : e + jx[k] * tp.h[k];
+    }
+    out = fh;
+    ostride = PX;
+    oidx = px;
+    out[oidx] = 0.0;
+    out[ostride + oidx] = tau;
+    out[2 * ostride + oidx] = u * tau - qx - e;
+#pragma unroll
+    for (int k = 0; k < NR; ++k) out[(3 + k) * ostride + oidx] = -jx[k];
+    return;
+  }
+  const double du_dx = ddx(1), du_dy = ddy(1), dv_dx = ddx(2), dv_dy = ddy(2);
+  const double lam = -2.0 / 3.0 * tp.mu;
+  const double S12 = 0.5 * (du_dy + dv_dx);
+  const double div_u = du_dx + dv_dy;
+  double jn[NS], e = 0.0;
+  const double dTn = xf ? ddx(3) : ddy(3);
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    jn[k] = -rho * tp.D[k] * (xf ? ddx(4 + k) : ddy(4 + k));
+    e = k == 0 ? jn[0] * tp.h[0] : e + jn[k] * tp.h[k];
+  }
+  const double qn = -tp.k * dTn;
+  const double tau_xy = 2.0 * tp.mu * S12;
+  double f1, f2, f3;
+  if (xf) {
+    const double tau_xx = 2.0 * tp.mu * du_dx + lam * div_u;
+    f1 = tau_xx;
+    f2 = tau_xy;
+    f3 = u * tau_xx + v * tau_xy - qn - e;
+    out = fh;
+    ostride = (long long)PX * g.ny;
+    oidx = (long long)px * g.ny + (py - 3);
+  } else {
+    const double tau_yy = 2.0 * tp.mu * dv_dy + lam * div_u;
+    f1 = tau_xy;
+    f2 = tau_yy;
+    f3 = u * tau_xy + v * tau_yy - qn - e;
+    out = gh;
+    ostride = (long long)g.nx * PY;
+    oidx = (long long)(px - 3) * PY + py;
+  }
+  out[oidx] = 0.0;
+  out[ostride + oidx] = f1;
+  out[2 * ostride + oidx] = f2;
+  out[3 * ostride + oidx] = f3;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) out[(4 + k) * ostride + oidx] = -jn[k];
+}
+
+// interface value from six node fluxes (reconstruction/CENTRAL6.py)
+__device__ __forceinline__ double central6(const double* f, long long st) {
+  return (3.0 * f[0] - 25.0 * f[st] + 150.0 * f[2 * st] + 150.0 * f[3 * st] - 25.0 * f[4 * st] + 3.0 * f[5 * st]) /
+         256.0;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) k_visc_div(Grid g, const double* __restrict__ fh,
+                                                  const double* __restrict__ gh, double* __restrict__ V) {
+  constexpr int nv = DIM == 1 ? 11 : 12;
+  const long long nc = g.ncell;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const int x = DIM == 2 ? (int)(c / g.ny) : (int)c, y = DIM == 2 ? (int)(c % g.ny) : 0;
+  const int PX = g.nx + 6, PY = g.ny + 6;
+  const long long sF = DIM == 2 ? (long long)PX * g.ny : PX, sG = (long long)g.nx * PY;
+#pragma unroll
+  for (int f = 0; f < nv; ++f) {
+    // faces x and x+1 of this cell: node fluxes at padded x .. x+6
+    const double* a = fh + f * sF + (DIM == 2 ? (long long)x * g.ny + y : x);
+    const long long st = DIM == 2 ? g.ny : 1;
+    double r = (central6(a + st, st) - central6(a, st)) / g.dx;
+    if (DIM == 2) {
+      const double* b = gh + f * sG + (long long)x * PY + y;
+      r = r + (central6(b + 1, 1) - central6(b, 1)) / g.dy;
+    }
+    V[f * nc + c] = r;
+  }
+}

@@ -13,6 +13,7 @@ config = {
     "flux": {"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS",
              "split_method": "LF", "viscosity": "off"},
     "detailed_chemistry": True,
+    "transport": None,
 }
 _solvers = {}
 _mech_cache = {}
@@ -31,11 +32,12 @@ def solver_for(shape, dx=1.0, dy=1.0):
     dim = 1 if len(shape) == 1 else 2
     bc = config["boundary"] or {}
     key = (dim, tuple(shape), repr(sorted(bc.items())) if bc else "", config["precision"],
-           config["mechanism"], repr(config["nondim"]))
+           config["mechanism"], repr(config["nondim"]), repr(config["flux"]), repr(config["transport"]))
     s = _solvers.get(key)
     if s is None:
         s = Solver(dim, shape[0], shape[1] if dim == 2 else None, dx, dy if dim == 2 else None,
-                   bc, mechanism(), precision=config["precision"])
+                   bc, mechanism(), precision=config["precision"], flux_config=config["flux"],
+                   transport_config=config["transport"])
         _solvers[key] = s
     s._spacing(dx, dy if dim == 2 else None)
     return s

@@ -78,7 +78,8 @@ class Simulator:
         _state.config["precision"] = simulation_config.get("precision", "fp64")
         thermo_model.set_thermo(thermo_config, nondim_config, dim)
         reaction_model.set_reaction(reaction_config, nondim_config, dim)
-        (flux_1D if dim == "1D" else flux).set_flux_solver(flux_config, None, nondim_config)
+        (flux_1D if dim == "1D" else flux).set_flux_solver(
+            flux_config, simulation_config.get("transport_config", None), nondim_config)
         boundary.set_boundary(boundary_config, dim)
         if time_control["temporal_evolution_scheme"] != "TVD_RK3":
             raise KeyError("only 'TVD_RK3' time stepping is built")

@@ -3,15 +3,12 @@ from .. import _state
 
 
 def set_flux_solver(flux_solver_config, transport_config=None, nondim_config=None):
-    solver_type = flux_solver_config["solver_type"]
-    if solver_type == "godunov":
-        raise NotImplementedError("the Godunov (HLLC/AUSMPW+) path is not built; use 'flux_splitting'")
-    elif solver_type != "flux_splitting":
-        raise KeyError("JANC only support 'godunov' and 'flux_splitting'")
-    if flux_solver_config["interface_reconstruction"] != "WENO5_JS":
-        raise KeyError("only 'WENO5_JS' reconstruction is built")
-    if flux_solver_config["split_method"] != "LF":
-        raise KeyError("only the 'LF' flux splitting is built")
+    """Validate as set_flux_solver does and keep the configuration for the
+    native solvers: LF flux splitting or Godunov (HLLC / AUSMPW+), WENO5_JS,
+    optionally with the laminar viscous fluxes of transport_config."""
+    from ...solver import flux_scheme, transport_params
+    flux_scheme(flux_solver_config)
     if flux_solver_config.get("viscosity", "off") == "on":
-        raise NotImplementedError("viscous fluxes are not built")
+        transport_params(transport_config)
     _state.config["flux"] = dict(flux_solver_config)
+    _state.config["transport"] = dict(transport_config) if transport_config else None

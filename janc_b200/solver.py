@@ -26,7 +26,7 @@ def flux_scheme(flux_config):
     solver_2D/flux.py:19-40) and name the native flux: ``LF``, ``HLLC`` or
     ``AUSMPW_plus``.  Raises as the reference does: KeyError for an unknown
     solver type or dictionary entry; what the reference has but this build
-    does not (MUSCL, SW splitting, viscous fluxes) raises NotImplementedError."""
+    does not (MUSCL, SW splitting) raises NotImplementedError."""
     if flux_config is None:
         return "LF"
     solver_type = flux_config["solver_type"]
@@ -37,8 +37,6 @@ def flux_scheme(flux_config):
         raise NotImplementedError("MUSCL reconstruction is not built; use WENO5_JS")
     if recon != "WENO5_JS":
         raise KeyError(recon)
-    if flux_config.get("viscosity", "off") == "on":
-        raise NotImplementedError("viscous fluxes are not built")
     if solver_type == "godunov":
         rs = flux_config["riemann_solver"]
         if rs not in ("HLLC", "AUSMPW_plus"):
@@ -50,6 +48,48 @@ def flux_scheme(flux_config):
     if split != "LF":
         raise KeyError(split)
     return "LF"
+
+
+def transport_params(transport_config):
+    """jb_transport from a reference ``transport_config`` (set_transport,
+    model/transport_model.py:26-104), with its defaults and errors; only the
+    laminar model is built (LES raises NotImplementedError)."""
+    c = transport_config
+    t = _native.Transport()
+    t.mu_ref, t.T_ref, t.S, t.nu0 = 1.716e-5, 273.15, 110.4, 1e-4
+    t.Pr, t.Pr_t, t.Le, t.Le_t, t.k0, t.D0 = 0.72, 0.72, 1.0, 1.0, 0.0, 0.0
+    if c["viscosity_model"] == "constant":
+        t.viscosity_model, t.nu0 = 1, c["dynamic_viscosity"]
+    elif c["viscosity_model"] == "Sutherland":
+        t.mu_ref = c.get("reference_viscosity", t.mu_ref)
+        t.T_ref = c.get("reference_temperature", t.T_ref)
+        t.S = c.get("effective_temperature", t.S)
+    else:
+        raise KeyError("Only 'Sutherland' and 'constant' viscosity model are supported.")
+    if c["thermal_conductivity_model"] == "constant":
+        t.conductivity_model, t.k0 = 1, c["thermal_conductivity"]
+    elif c["thermal_conductivity_model"] == "Prandtl number":
+        assert "Pr" in c, "Key 'Pr' must be provided"
+        t.Pr = c["Pr"]
+    else:
+        raise KeyError("Only 'Prandtl number' and 'constant' thermal conductivity model are supported.")
+    if c["species_diffusivity_model"] == "constant":
+        t.diffusivity_model, t.D0 = 1, c["species_diffusivity"]
+    elif c["species_diffusivity_model"] == "Schmidt number":
+        assert "Sc" in c, "Key 'Sc' must be provided"
+        t.Le = c["Sc"] / t.Pr
+    elif c["species_diffusivity_model"] == "Lewis number":
+        assert "Le" in c, "Key 'Le' must be provided"
+        t.Le = c["Le"]
+    else:
+        raise KeyError("Only 'Schmidt number', 'Lewis number', and 'constant' species diffusivity model "
+                       "are supported.")
+    model = c.get("turbulence_model", "laminar")
+    if model == "LES":
+        raise NotImplementedError("LES sub-grid models are not built")
+    if model != "laminar":
+        raise KeyError("Only 'laminar' and 'LES' model are supported.")
+    return t
 
 
 def _stream():
@@ -70,11 +110,15 @@ class Solver:
     ``flux_splitting`` (``split_method`` ``LF``) or ``godunov``
     (``riemann_solver`` ``HLLC`` or ``AUSMPW_plus``), with
     ``interface_reconstruction`` ``WENO5_JS``.  Default: LF flux splitting.
+    ``viscosity`` ``on`` adds the laminar viscous fluxes of
+    ``transport_config`` (the reference's transport_config: Sutherland or
+    constant viscosity, Prandtl-number or constant conductivity, Lewis /
+    Schmidt-number or constant diffusivity).
     """
 
     def __init__(self, dim, nx, ny=None, dx=1.0, dy=None, boundary_config=None,
                  mechanism=_mech.DEFAULT_MECHANISM, nondim_config=None, precision="fp64",
-                 device=None, flux_config=None):
+                 device=None, flux_config=None, transport_config=None):
         if dim in ("1D", 1):
             dim = 1
         elif dim in ("2D", 2):
@@ -118,6 +162,13 @@ class Solver:
         self._lib = L
         self.flux_scheme = flux_scheme(flux_config)
         _native.check(L.jb_set_flux_scheme(h, _native.FLUX_SCHEME[self.flux_scheme]), h, "jb_set_flux_scheme")
+        self.viscous = bool(flux_config) and flux_config.get("viscosity", "off") == "on"
+        if self.viscous:
+            if transport_config is None:
+                raise KeyError("transport_config")  # set_flux_solver passes it to set_transport
+            self._transport = transport_params(transport_config)
+            with torch.cuda.device(self.device):
+                _native.check(L.jb_set_transport(h, ctypes.byref(self._transport)), h, "jb_set_transport")
 
     # ------------------------------------------------------------------ utils
     def close(self):

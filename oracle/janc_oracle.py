@@ -846,6 +846,156 @@ def godunov_flux(m, Up, Ap, dx, dy=None, riemann="HLLC"):
 
 
 # --------------------------------------------------------------------------
+# viscous flux, laminar (solver_{1D,2D}/flux.py viscous_flux_node /
+# viscous_flux, model/transport_model.py, finite_difference/CENTRAL6.py,
+# reconstruction/CENTRAL6.py)
+# --------------------------------------------------------------------------
+class Transport:
+    """set_transport (transport_model.py:26-104) for the laminar model."""
+
+    def __init__(self, cfg):
+        self.mu_ref, self.T_ref, self.S, self.nu0 = 1.716e-5, 273.15, 110.4, 1e-4
+        self.Pr, self.Pr_t, self.Sc, self.Sc_t, self.Le, self.Le_t = 0.72, 0.72, 0.72, 0.72, 1.0, 1.0
+        self.k0, self.D0 = 0.0, 0.0
+        self.nu_type, self.k_type, self.D_type = "Sutherland", "Prandtl number", "Lewis number"
+        if cfg["viscosity_model"] == "constant":
+            self.nu_type = "constant"
+            self.nu0 = cfg["dynamic_viscosity"]
+        elif cfg["viscosity_model"] == "Sutherland":
+            self.mu_ref = cfg.get("reference_viscosity", self.mu_ref)
+            self.T_ref = cfg.get("reference_temperature", self.T_ref)
+            self.S = cfg.get("effective_temperature", self.S)
+        else:
+            raise KeyError("Only 'Sutherland' and 'constant' viscosity model are supported.")
+        if cfg["thermal_conductivity_model"] == "constant":
+            self.k_type = "constant"
+            self.k0 = cfg["thermal_conductivity"]
+        elif cfg["thermal_conductivity_model"] == "Prandtl number":
+            self.Pr = cfg["Pr"]
+        else:
+            raise KeyError("Only 'Prandtl number' and 'constant' thermal conductivity model are supported.")
+        if cfg["species_diffusivity_model"] == "constant":
+            self.D_type = "constant"
+            self.D0 = cfg["species_diffusivity"]
+        elif cfg["species_diffusivity_model"] == "Schmidt number":
+            self.Sc = cfg["Sc"]
+            self.Le = self.Sc / self.Pr
+        elif cfg["species_diffusivity_model"] == "Lewis number":
+            self.Le = cfg["Le"]
+            self.Sc = self.Le * self.Pr
+        else:
+            raise KeyError("Only 'Schmidt number', 'Lewis number', and 'constant' species diffusivity "
+                           "model are supported.")
+        if cfg.get("turbulence_model", "laminar") != "laminar":
+            raise NotImplementedError("LES")
+
+    def mu(self, rho, T):
+        """mu_Sutherland / mu_constant (:106-112); laminar mu_t = 0"""
+        if self.nu_type == "Sutherland":
+            return self.mu_ref * (T / self.T_ref) ** 1.5 * (self.T_ref + self.S) / (T + self.S)
+        return rho * self.nu0
+
+    def kappa(self, mu, cp, mu_t=0.0):
+        """kappa_Pr / kappa_constant (:133-137)"""
+        if self.k_type == "Prandtl number":
+            return mu * cp / self.Pr + mu_t * cp / self.Pr_t
+        return self.k0 + mu_t * cp / self.Pr_t
+
+    def D(self, mu, rho, cp_i, mu_t=0.0):
+        """D_Le / D_constant (:146-157)"""
+        if self.D_type == "Lewis number" or self.D_type == "Schmidt number":
+            k_i = (self.k_type == "Prandtl number") * mu * cp_i / self.Pr + (self.k_type == "constant") * self.k0
+            rhoD_i = k_i / (self.Le * cp_i)
+            k_t = mu_t / self.Pr_t
+            rhoD_t = k_t / (self.Le_t * cp_i)
+            return (rhoD_i + rhoD_t) / rho
+        k_t = mu_t / self.Pr_t
+        rhoD_t = k_t / self.Le_t * cp_i
+        return self.D0 + rhoD_t / rho
+
+
+def _d_axis(f, d, axis):
+    """finite_difference/CENTRAL6.py d_dx / d_dy: sixth-order central inside,
+    (4th, 2nd, 1st)-order one-sided forms at the first and last three."""
+    def s(a, b):
+        idx = [slice(None)] * f.ndim
+        idx[axis] = slice(a, b)
+        return f[tuple(idx)]
+    n = f.shape[axis]
+    center = (-s(0, n - 6) + 9 * s(1, n - 5) - 45 * s(2, n - 4) + 45 * s(4, n - 2) - 9 * s(5, n - 1)
+              + s(6, n)) / (60 * d)
+    left3 = (s(0, 1) - 8 * s(1, 2) + 8 * s(3, 4) - s(4, 5)) / (12 * d)
+    left2 = (s(2, 3) - s(0, 1)) / (2 * d)
+    left1 = (s(1, 2) - s(0, 1)) / d
+    right1 = (s(n - 5, n - 4) - 8 * s(n - 4, n - 3) + 8 * s(n - 2, n - 1) - s(n - 1, n)) / (12 * d)
+    right2 = (s(n - 1, n) - s(n - 3, n - 2)) / (2 * d)
+    right3 = (s(n - 1, n) - s(n - 2, n - 1)) / d
+    return np.concatenate([left1, left2, left3, center, right1, right2, right3], axis=axis)
+
+
+def _central6_interface(fv, axis, other_interior):
+    """reconstruction/CENTRAL6.py interface_x / interface_y"""
+    def s(a, b):
+        idx = [slice(None)] * fv.ndim
+        idx[axis] = slice(a, b)
+        if other_interior is not None:
+            idx[other_interior] = slice(3, -3)
+        return fv[tuple(idx)]
+    return (3 * s(0, -5) - 25 * s(1, -4) + 150 * s(2, -3) + 150 * s(3, -2) - 25 * s(4, -1)
+            + 3 * s(5, None)) / 256
+
+
+def viscous_flux(m, tr, Up, Ap, dx, dy=None):
+    """viscous_flux (solver_2D/flux.py:70-115, solver_1D/flux.py:67-99) on the
+    ghost-padded arrays (corners keep the periodic wrap): returns
+    dF_v/dx [+ dG_v/dy] (added to the advective -(dF/dx + dG/dy))."""
+    T = Ap[1:2]
+    cp_k, _, h_k = get_thermo_properties(m, T[0])
+    if Up.ndim == 2:
+        rho, u, Y, p, a = U_to_prim(m, Up, Ap)
+        cp = get_thermo(m, T, Y)[0]
+        Yf = fill_Y(Y)
+        du_dx = _d_axis(u, dx, 1)
+        dT_dx = _d_axis(T, dx, 1)
+        dY_dx = _d_axis(Yf, dx, 1)
+        mu = tr.mu(rho, T)
+        k = tr.kappa(mu, cp)
+        D_k = tr.D(mu, rho, cp_k)
+        div_u = du_dx
+        tau_xx = 2 * mu * du_dx - 2 / 3 * mu * div_u
+        qx = -k * dT_dx
+        jx = -rho * D_k * dY_dx
+        ex = _seqsum(jx * h_k)
+        F_hat = np.concatenate([np.zeros_like(rho), tau_xx, u * tau_xx - qx - ex, -jx[0:-1]], axis=0)
+        Fi = _central6_interface(F_hat, 1, None)
+        return (Fi[:, 1:] - Fi[:, :-1]) / dx
+    rho, u, v, Y, p, a = U_to_prim(m, Up, Ap)
+    cp = get_thermo(m, T, Y)[0]
+    Yf = fill_Y(Y)
+    du_dx, du_dy = _d_axis(u, dx, 1), _d_axis(u, dy, 2)
+    dv_dx, dv_dy = _d_axis(v, dx, 1), _d_axis(v, dy, 2)
+    dT_dx, dT_dy = _d_axis(T, dx, 1), _d_axis(T, dy, 2)
+    dY_dx, dY_dy = _d_axis(Yf, dx, 1), _d_axis(Yf, dy, 2)
+    mu = tr.mu(rho, T)
+    k = tr.kappa(mu, cp)
+    D_k = tr.D(mu, rho, cp_k)
+    lam = -2 / 3 * mu
+    S12 = 0.5 * (du_dy + dv_dx)
+    div_u = du_dx + dv_dy
+    tau_xx = 2 * mu * du_dx + lam * div_u
+    tau_yy = 2 * mu * dv_dy + lam * div_u
+    tau_xy = 2 * mu * S12
+    qx, qy = -k * dT_dx, -k * dT_dy
+    jx, jy = -rho * D_k * dY_dx, -rho * D_k * dY_dy
+    ex, ey = _seqsum(jx * h_k), _seqsum(jy * h_k)
+    F_hat = np.concatenate([np.zeros_like(rho), tau_xx, tau_xy, u * tau_xx + v * tau_xy - qx - ex, -jx[0:-1]], axis=0)
+    G_hat = np.concatenate([np.zeros_like(rho), tau_xy, tau_yy, u * tau_xy + v * tau_yy - qy - ey, -jy[0:-1]], axis=0)
+    Fi = _central6_interface(F_hat, 1, 2)
+    Gi = _central6_interface(G_hat, 2, 1)
+    return (Fi[:, 1:, :] - Fi[:, :-1, :]) / dx + (Gi[:, :, 1:] - Gi[:, :, :-1]) / dy
+
+
+# --------------------------------------------------------------------------
 # solver wiring  (simulation/set_simulator.py, time_step/TVD_RK3.py)
 # --------------------------------------------------------------------------
 class Solver:
@@ -853,7 +1003,7 @@ class Solver:
     ``advance_one_step`` and ``advance_func`` with the reference's
     signatures (set_simulator.py:20-125, 410-447)."""
 
-    def __init__(self, mech, dim, dx, dy=None, bc=None, cfl=None, flux_config=None):
+    def __init__(self, mech, dim, dx, dy=None, bc=None, cfl=None, flux_config=None, transport_config=None):
         self.m = mech
         self.dim = dim
         self.dx, self.dy = dx, dy
@@ -865,12 +1015,17 @@ class Solver:
         fc = flux_config or {"solver_type": "flux_splitting"}
         self.solver_type = fc["solver_type"]
         self.riemann = fc.get("riemann_solver", "HLLC")
+        self.transport = Transport(transport_config) if fc.get("viscosity", "off") == "on" else None
 
     def flux_func(self, U, aux, dx, dy, dt, theta=None):
         Up, Ap = boundary_conditions(self.m, U, aux, self.bc, theta)
         if self.solver_type == "godunov":
-            return dt * godunov_flux(self.m, Up, Ap, dx, dy, self.riemann)
-        return dt * (total_flux(self.m, Up, Ap, dx, dy))
+            adv = godunov_flux(self.m, Up, Ap, dx, dy, self.riemann)
+        else:
+            adv = total_flux(self.m, Up, Ap, dx, dy)
+        if self.transport is not None:  # NS_flux = advective + viscous (solver_2D/flux.py:117-118)
+            return dt * (adv + viscous_flux(self.m, self.transport, Up, Ap, dx, dy))
+        return dt * adv
 
     def update_func(self, U, aux):
         out, it = update_aux(self.m, U, aux, return_iters=True)
