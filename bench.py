@@ -284,14 +284,20 @@ def _setup_workload(args, precision):
         nx, ny = NX, NY
         dx, dy = LX / NX, LY / NY
         bc = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
-        fc = None
+        visc = "on" if args.viscous else "off"
+        fc = {"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS", "split_method": "LF",
+              "viscosity": visc}
         if args.flux != "LF":
             fc = {"solver_type": "godunov", "interface_reconstruction": "WENO5_JS",
-                  "riemann_solver": args.flux, "viscosity": "off"}
-        s = Solver(2, nx, ny, dx, dy, bc, precision=precision, flux_config=fc)
+                  "riemann_solver": args.flux, "viscosity": visc}
+        tc = ({"viscosity_model": "Sutherland", "thermal_conductivity_model": "Prandtl number", "Pr": 0.72,
+               "species_diffusivity_model": "Lewis number", "Le": 1.0} if args.viscous else None)
+        s = Solver(2, nx, ny, dx, dy, bc, precision=precision, flux_config=fc, transport_config=tc)
         P, T, Y = c1_fields()
         scheme = ("WENO5-JS + LF" if args.flux == "LF" else
                   f"Godunov (WENO5-JS on primitives + {args.flux}, float64)")
+        if args.viscous:
+            scheme += " + laminar viscous fluxes (Sutherland, Pr 0.72, Le 1, CENTRAL6)"
         workload = ("2D H2-air detonation channel 1024x256 (0.2 m x 0.05 m), 9sp/19r mechanism, "
                     "30 atm / 3000 K slab with 8 seeded +-5% blobs, slip walls, "
                     f"{scheme} + SSP-RK3 + point-implicit chemistry")
@@ -516,7 +522,7 @@ def run_ours(args):
         # variant), 2 stage selects, chemistry, final select
         # (+ 4 ghost-strip launches on the RDC workload's outlet / injector sides)
         "gpu_launches": ((13 if args.precision == "mixed" and args.flux == "LF" else 10)
-                         + (4 if args.workload == "rdc" else 0)) * args.steps,
+                         + (4 if args.workload == "rdc" else 0) + (9 if args.viscous else 0)) * args.steps,
         "roofline": {"bound": "hbm", "kernel": {
                          "chem": "k_chem (point-implicit chemistry + final Halley)",
                          "flux": ("k_god2d (WENO5 on primitives + Riemann solver + RK stage + Halley)"
@@ -526,7 +532,7 @@ def run_ours(args):
                                   "k_flux2d (LF + WENO5 + RK stage + Halley)")}[dom],
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "traffic": (TRAFFIC_PER_CELL[dom] * ncell if args.workload == "channel" and
-                                 args.flux == "LF" and
+                                 args.flux == "LF" and not args.viscous and
                                  args.precision == "mixed" else None),
                      "traffic_source": "ncu dram bytes of one stage's launches on this workload, each "
                                        "launch cold (mixed precision)",
@@ -1018,6 +1024,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the float64 comparison run")
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--workload", default="channel", choices=["channel", "rdc", "ensemble", "adjoint"])
+    ap.add_argument("--viscous", action="store_true",
+                    help="channel workload with the laminar viscous fluxes")
     ap.add_argument("--flux", default="LF", choices=["LF", "HLLC", "AUSMPW_plus"],
                     help="advective flux of the channel workload (LF flux splitting or a Godunov "
                          "Riemann solver)")
