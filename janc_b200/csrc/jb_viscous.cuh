@@ -71,8 +71,21 @@ __global__ void __launch_bounds__(256) k_visc_nodes(MP m, Grid g, const double* 
 
 // d/dx of a node plane along one line (finite_difference/CENTRAL6.py d_dx):
 // f points at position 0 of the line, stride st, n positions, at position p.
+// The fast variants multiply by the stencils' reciprocal denominators.
 __device__ __forceinline__ double d_line(const double* f, long long st, int n, int p, double d) {
   auto F = [&](int j) { return f[(long long)j * st]; };
+#if JB_FAST
+  const double id = 1.0 / d;
+  if (p >= 3 && p < n - 3)
+    return (-F(p - 3) + 9.0 * F(p - 2) - 45.0 * F(p - 1) + 45.0 * F(p + 1) - 9.0 * F(p + 2) + F(p + 3)) *
+           (id * (1.0 / 60.0));
+  if (p == 0) return (F(1) - F(0)) * id;
+  if (p == 1) return (F(2) - F(0)) * (0.5 * id);
+  if (p == 2) return (F(0) - 8.0 * F(1) + 8.0 * F(3) - F(4)) * (id * (1.0 / 12.0));
+  if (p == n - 3) return (F(n - 5) - 8.0 * F(n - 4) + 8.0 * F(n - 2) - F(n - 1)) * (id * (1.0 / 12.0));
+  if (p == n - 2) return (F(n - 1) - F(n - 3)) * (0.5 * id);
+  return (F(n - 1) - F(n - 2)) * id;
+#else
   if (p >= 3 && p < n - 3)
     return (-F(p - 3) + 9.0 * F(p - 2) - 45.0 * F(p - 1) + 45.0 * F(p + 1) - 9.0 * F(p + 2) + F(p + 3)) /
            (60.0 * d);
@@ -82,6 +95,7 @@ __device__ __forceinline__ double d_line(const double* f, long long st, int n, i
   if (p == n - 3) return (F(n - 5) - 8.0 * F(n - 4) + 8.0 * F(n - 2) - F(n - 1)) / (12.0 * d);
   if (p == n - 2) return (F(n - 1) - F(n - 3)) / (2.0 * d);
   return (F(n - 1) - F(n - 2)) / d;
+#endif
 }
 
 // transport at one node (transport_model.py:106-157, laminar: mu_t = 0)
@@ -100,8 +114,26 @@ __device__ __forceinline__ void node_transport(const MP& m, const jb_transport& 
     cp = k == 0 ? cpk[0] * Yf[0] : cp + cpk[k] * Yf[k];
   }
   const double mu_t = 0.0;
+#if JB_FAST
+  if (tr.viscosity_model == 0) {
+    const double x = T / tr.T_ref;
+    o.mu = tr.mu_ref * (x * sqrt(x)) * (tr.T_ref + tr.S) / (T + tr.S);
+  } else {
+    o.mu = rho * tr.nu0;
+  }
+  if (tr.conductivity_model == 0 && tr.diffusivity_model == 0) {
+    // Prandtl and Lewis numbers: rho D_k = mu / (Pr Le) for every species
+    // (cp_k cancels), k = mu cp / Pr
+    o.k = o.mu * cp / tr.Pr;
+    const double D = o.mu / (tr.Pr * tr.Le * rho);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) o.D[k] = D;
+    return;
+  }
+#else
   if (tr.viscosity_model == 0) o.mu = tr.mu_ref * pow(T / tr.T_ref, 1.5) * (tr.T_ref + tr.S) / (T + tr.S);
   else o.mu = rho * tr.nu0;
+#endif
   if (tr.conductivity_model == 0) o.k = o.mu * cp / tr.Pr + mu_t * cp / tr.Pr_t;
   else o.k = tr.k0 + mu_t * cp / tr.Pr_t;
   const double pr_on = tr.conductivity_model == 0 ? 1.0 : 0.0, k_on = tr.conductivity_model == 0 ? 0.0 : 1.0;
@@ -243,11 +275,19 @@ __global__ void __launch_bounds__(128) k_visc_div(Grid g, const double* __restri
     // faces x and x+1 of this cell: node fluxes at padded x .. x+6
     const double* a = fh + f * sF + (DIM == 2 ? (long long)x * g.ny + y : x);
     const long long st = DIM == 2 ? g.ny : 1;
+#if JB_FAST
+    double r = (central6(a + st, st) - central6(a, st)) * g.idx;
+    if (DIM == 2) {
+      const double* b = gh + f * sG + (long long)x * PY + y;
+      r = r + (central6(b + 1, 1) - central6(b, 1)) * g.idy;
+    }
+#else
     double r = (central6(a + st, st) - central6(a, st)) / g.dx;
     if (DIM == 2) {
       const double* b = gh + f * sG + (long long)x * PY + y;
       r = r + (central6(b + 1, 1) - central6(b, 1)) / g.dy;
     }
+#endif
     V[f * nc + c] = r;
   }
 }
