@@ -120,7 +120,17 @@ __device__ __forceinline__ double poly6(const double* c, double T) {
 }
 
 // advective + viscous rhs of field f at cell (NS_flux, solver_2D/flux.py:117-118);
-// g.visc holds the viscous part computed for the stage state, or is null
+// g.visc holds the viscous part computed for the stage state, or is null.
+// The LF stage kernels take VISC as a template flag, so that their inviscid
+// instantiations read no viscous pointer: a pointer not known to be free of
+// aliasing with the kernel's output keeps the compiler from batching the
+// epilogue's loads ahead of its stores.
+template <bool VISC>
+__device__ __forceinline__ double visc_add(const Grid& g, int f, long long cell, double adv) {
+  return VISC ? adv + g.visc[f * g.ncell + cell] : adv;
+}
+
+// Runtime form (Godunov stage kernels).
 __device__ __forceinline__ double visc_add(const Grid& g, int f, long long cell, double adv) {
   return g.visc ? adv + g.visc[f * g.ncell + cell] : adv;
 }
@@ -736,7 +746,7 @@ __host__ __device__ constexpr size_t smem2d_bytes(int nq) {
 // R is the arithmetic type of the flux (LF split, WENO, primitives): double
 // for the float64 variants, float for the mixed variant.  The RK combination
 // and the Halley iterates are float64 in every variant.
-template <int STAGE, class R>
+template <int STAGE, class R, bool VISC>
 __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk,
                                                  const double* __restrict__ Un,
@@ -879,9 +889,9 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       double dF = (double)(sFx[(ix + 1) * TY2 + iy] - sFx[ix * TY2 + iy]);
       double dG = (double)(sFy[ix * (TY2 + 1) + iy + 1] - sFy[ix * (TY2 + 1) + iy]);
 #if JB_FAST
-      double rhs = dt * visc_add(g, f, cell, -(dF * g.idx + dG * g.idy));
+      double rhs = dt * visc_add<VISC>(g, f, cell, -(dF * g.idx + dG * g.idy));
 #else
-      double rhs = dt * visc_add(g, f, cell, -(dF / g.dx + dG / g.dy));
+      double rhs = dt * visc_add<VISC>(g, f, cell, -(dF / g.dx + dG / g.dy));
 #endif
       // the state itself is float64 in every variant
       double uk = EXACT ? (double)sQ[f * SM2_Q + (ix + 3) * PY2 + (iy + 3)] : Uk[f * nc + cell];
@@ -1043,7 +1053,7 @@ __global__ void __launch_bounds__(SX_NT) k_sweep_x(MP m, Grid g, const double* _
   }
 }
 
-template <int STAGE>
+template <int STAGE, bool VISC>
 __global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const double* __restrict__ Uk,
                                                        const double* __restrict__ auxk,
                                                        const double* __restrict__ Un, const float* __restrict__ prims,
@@ -1122,7 +1132,7 @@ __global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const doub
     for (int f = 0; f < 12; ++f) {
       const double dF = (double)dfx[f * nc + cell];
       const double dG = (double)(sF[f * YR_F + l + 1] - sF[f * YR_F + l]);
-      const double rhs = dt * visc_add(g, f, cell, -(dF * g.idx + dG * g.idy));
+      const double rhs = dt * visc_add<VISC>(g, f, cell, -(dF * g.idx + dG * g.idy));
       const double uk = ukr[f];
       double r;
       if (STAGE == 1) r = uk + rhs;
@@ -1161,7 +1171,7 @@ __host__ __device__ constexpr size_t smem1d_bytes(int nq) {
 // Every thread of the block must call it; returns this thread's Halley mask.
 // Pointers are plain (not restrict) because the persistent ensemble kernel
 // calls it on buffers written by other blocks of the same launch.
-template <int STAGE, class R, int NT>
+template <int STAGE, class R, int NT, bool VISC = false>
 __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, const double* Uk,
                                                 const double* auxk, const double* Un, double* out,
                                                 double* cand, const double* strips, double alpha,
@@ -1235,9 +1245,9 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
     if (live) {
       double dF = (double)(sF[tid + 1] - sF[tid]);
 #if JB_FAST
-      double rhs = dt * visc_add(g, f, cell, -(dF * g.idx));
+      double rhs = dt * visc_add<VISC>(g, f, cell, -(dF * g.idx));
 #else
-      double rhs = dt * visc_add(g, f, cell, -(dF / g.dx));
+      double rhs = dt * visc_add<VISC>(g, f, cell, -(dF / g.dx));
 #endif
       double uk = EXACT ? (double)sQ[f * PX1 + tid + 3] : Uk[f * nc + cell];
       double r;
@@ -1271,7 +1281,7 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
   return bits;
 }
 
-template <int STAGE, class R>
+template <int STAGE, class R, bool VISC>
 __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk,
                                                  const double* __restrict__ Un,
@@ -1280,7 +1290,7 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
                                                  int aidx, int midx, double dt_arg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const double dt = STAGE == 0 ? dt_arg : slots->dt;
-  unsigned bits = flux1d_tile<STAGE, R, NT1>(m, g, Uk, auxk, Un, out, cand, strips, bitsd(slots->ax[aidx]), dt,
+  unsigned bits = flux1d_tile<STAGE, R, NT1, VISC>(m, g, Uk, auxk, Un, out, cand, strips, bitsd(slots->ax[aidx]), dt,
                                              blockIdx.x * (NT1 - 1), smraw);
   if (STAGE == 0) return;
   block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
