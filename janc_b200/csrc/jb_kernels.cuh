@@ -1353,8 +1353,14 @@ __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const do
       int n = halley_count(mask);
       T = cand[n * nc + c];
       double Y8[NR], Yf[NS];
+#if JB_FAST
+      const double ri = 1.0 / q[0];
+#pragma unroll
+      for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] * ri;
+#else
 #pragma unroll
       for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / q[0];
+#endif
       fill_Y(Y8, Yf);
       double R = get_R(m, Yf);
       double cp = cp_mix(m, T, Yf);
@@ -1378,7 +1384,11 @@ __device__ __forceinline__ void select_cell(const MP& m, const Grid& g, const do
       amy = fmax(amy, sy);
       if (!(sx == sx) || !(T == T)) st |= JB_ERR_NONFINITE;
       if (CFL) {
+#if JB_FAST
+        double d = DIM == 1 ? g.dx / sx : 1.0 / (sx * g.idx + sy * g.idy);
+#else
         double d = DIM == 1 ? g.dx / sx : 1.0 / (sx / g.dx + sy / g.dy);
+#endif
         dtm = fmin(dtm, d);
         if (!(d == d) || !(d > 0.0)) st |= JB_ERR_NONFINITE;
         // jnp.min (set_simulator.py:423,441) returns NaN if any candidate is
