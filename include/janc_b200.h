@@ -107,7 +107,8 @@ int jb_set_spacing(jb_handle* h, double dx, double dy);
  * (the default), JB_FLUX_HLLC / JB_FLUX_AUSMPW = godunov_flux
  * (solver_2D/flux.py:43-54) with WENO5-JS on the primitives and the HLLC
  * (riemann_solver/HLLC.py) or AUSMPW+ (riemann_solver/AUSMPW_plus.py)
- * Riemann solver.  The Godunov path computes in float64 in every variant;
+ * Riemann solver.  The mixed variant reconstructs the primitives in float32;
+ * the Riemann solver, RK and temperature solve are float64 in every variant.
  * jb_adjoint_step supports JB_FLUX_LF only. */
 int jb_set_flux_scheme(jb_handle* h, int scheme);
 

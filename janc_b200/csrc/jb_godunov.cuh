@@ -1,9 +1,10 @@
 // Godunov path of the advective flux (solver_{1D,2D}/flux.py godunov_flux):
 // WENO5-JS face states of the primitives w = [rho, u, (v), p, Y], then an
 // HLLC (riemann_solver/HLLC.py) or AUSMPW+ (riemann_solver/AUSMPW_plus.py)
-// flux per face.  Included by jb_kernels.cuh inside namespace jb::JB_NS;
-// float64 in every variant, operation order as the reference's expressions
-// evaluate.
+// flux per face.  Included by jb_kernels.cuh inside namespace jb::JB_NS.
+// The reconstruction runs in RW (float32 in the mixed variant), the Riemann
+// solver, RK combination and Halley iterates in float64; operation order as
+// the reference's expressions evaluate.
 #pragma once
 
 constexpr int RS_HLLC = 0, RS_AUSMPW = 1;
@@ -163,21 +164,31 @@ __device__ __forceinline__ void cons_to_w(const MP& m, const double* q, double T
 // stage kernels (STAGE as k_flux2d / k_flux1d: 0 flux_func, 1..3 RK stage
 // followed by the Halley iterates of update_aux)
 // ---------------------------------------------------------------------------
-constexpr size_t GOD2_SMEM = sizeof(double) * 12 * (SM2_Q + SM2_FX + SM2_FY);
+// Shared memory: the padded tile's primitives in RW (float32 in the mixed
+// variant: the reconstruction runs in RW; the Riemann solver, RK and Halley
+// stay float64), then the face fluxes in float64 at a 16-byte aligned offset.
+template <class RW>
+__host__ __device__ constexpr size_t god2_wbytes() {
+  return (sizeof(RW) * 12 * SM2_Q + 15) / 16 * 16;
+}
+template <class RW>
+__host__ __device__ constexpr size_t god2_smem() {
+  return god2_wbytes<RW>() + sizeof(double) * 12 * (SM2_FX + SM2_FY);
+}
 
 // 2D: the tile of k_flux2d (15 x 16 cells, 3-cell halo); primitives of the
 // padded tile in shared memory, then one thread per x face and per y face
 // reconstructs all 12 components on both sides and solves the Riemann
 // problem.
-template <int STAGE, int RS>
+template <int STAGE, int RS, class RW>
 __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk, const double* __restrict__ Un,
                                                  double* __restrict__ out, double* __restrict__ cand,
                                                  const double* __restrict__ strips, Slots* slots, int midx,
                                                  double dt_arg) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  double* sW = reinterpret_cast<double*>(smraw);  // [12][PX2][PY2]
-  double* sFx = sW + 12 * SM2_Q;                   // [12][TX2+1][TY2]
+  RW* sW = reinterpret_cast<RW*>(smraw);                                // [12][PX2][PY2]
+  double* sFx = reinterpret_cast<double*>(smraw + god2_wbytes<RW>());  // [12][TX2+1][TY2]
   double* sFy = sFx + 12 * SM2_FX;                 // [12][TX2][TY2+1]
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * TX2, y0 = blockIdx.y * TY2;
@@ -206,7 +217,7 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
     double w[12];
     cons_to_w<2>(m, q, T, w);
 #pragma unroll
-    for (int f = 0; f < 12; ++f) sW[f * SM2_Q + i] = w[f];
+    for (int f = 0; f < 12; ++f) sW[f * SM2_Q + i] = (RW)w[f];
   }
   __syncthreads();
   {
@@ -215,7 +226,7 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
     double wL[12], wR[12], F[12];
 #pragma unroll
     for (int f = 0; f < 12; ++f) {
-      const double* b = sW + f * SM2_Q + mxf * PY2 + jy + 3;
+      const RW* b = sW + f * SM2_Q + mxf * PY2 + jy + 3;
       wL[f] = weno_L(b[0], b[PY2], b[2 * PY2], b[3 * PY2], b[4 * PY2]);
       wR[f] = weno_R(b[PY2], b[2 * PY2], b[3 * PY2], b[4 * PY2], b[5 * PY2]);
     }
@@ -228,7 +239,7 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
     double wL[12], wR[12], F[12];
 #pragma unroll
     for (int f = 0; f < 12; ++f) {
-      const double* b = sW + f * SM2_Q + (jx + 3) * PY2 + myf;
+      const RW* b = sW + f * SM2_Q + (jx + 3) * PY2 + myf;
       wL[f] = weno_L(b[0], b[1], b[2], b[3], b[4]);
       wR[f] = weno_R(b[1], b[2], b[3], b[4], b[5]);
     }
@@ -281,9 +292,16 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
 }
 
 // 1D: a block of NT1 threads covers NT1 - 1 cells and their NT1 faces.
-constexpr size_t GOD1_SMEM = sizeof(double) * 11 * ((NT1 + 5) + NT1);
+template <class RW>
+__host__ __device__ constexpr size_t god1_wbytes() {
+  return (sizeof(RW) * 11 * (NT1 + 5) + 15) / 16 * 16;
+}
+template <class RW>
+__host__ __device__ constexpr size_t god1_smem() {
+  return god1_wbytes<RW>() + sizeof(double) * 11 * NT1;
+}
 
-template <int STAGE, int RS>
+template <int STAGE, int RS, class RW>
 __global__ void __launch_bounds__(NT1) k_god1d(MP m, Grid g, const double* __restrict__ Uk,
                                               const double* __restrict__ auxk, const double* __restrict__ Un,
                                               double* __restrict__ out, double* __restrict__ cand,
@@ -291,8 +309,8 @@ __global__ void __launch_bounds__(NT1) k_god1d(MP m, Grid g, const double* __res
                                               double dt_arg) {
   constexpr int PW = NT1 + 5;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double* sW = reinterpret_cast<double*>(smraw);  // [11][PW]: padded cell x0 - 3 + j
-  double* sF = sW + 11 * PW;                       // [11][NT1]: face x0 + t
+  RW* sW = reinterpret_cast<RW*>(smraw);                               // [11][PW]: padded cell x0 - 3 + j
+  double* sF = reinterpret_cast<double*>(smraw + god1_wbytes<RW>());  // [11][NT1]: face x0 + t
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * (NT1 - 1);
   const long long nc = g.ncell;
@@ -319,7 +337,7 @@ __global__ void __launch_bounds__(NT1) k_god1d(MP m, Grid g, const double* __res
     double w[11];
     cons_to_w<1>(m, q, T, w);
 #pragma unroll
-    for (int f = 0; f < 11; ++f) sW[f * PW + j] = w[f];
+    for (int f = 0; f < 11; ++f) sW[f * PW + j] = (RW)w[f];
   }
   __syncthreads();
   {
@@ -327,7 +345,7 @@ __global__ void __launch_bounds__(NT1) k_god1d(MP m, Grid g, const double* __res
     double wL[11], wR[11], F[11];
 #pragma unroll
     for (int f = 0; f < 11; ++f) {
-      const double* b = sW + f * PW + tid;
+      const RW* b = sW + f * PW + tid;
       wL[f] = weno_L(b[0], b[1], b[2], b[3], b[4]);
       wR[f] = weno_R(b[1], b[2], b[3], b[4], b[5]);
     }

@@ -6,7 +6,8 @@ Riemann fluxes against identities that pin them without the reference
 (consistency F(q, q) = Euler flux, a uniform gas stays at rest).
 GPU (through the C ABI): flux_func and RK steps against the oracle.
 Tolerances: ``fp64_strict`` 1e-13 relative L1 per field for one flux
-evaluation and 1e-12 over steps; ``fp64`` 1e-12 and 1e-10.
+evaluation and 1e-12 over steps; ``fp64`` 1e-12 and 1e-10; ``mixed``
+(float32 reconstruction) 1e-4 per field and 1e-6 on the density.
 """
 import numpy as np
 import pytest
@@ -183,9 +184,10 @@ def test_steps_2d_vs_oracle(omech, prec, rs):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("rs", ["HLLC", "AUSMPW_plus"])
-def test_mixed_equals_fp64_on_godunov(omech, rs):
-    """The Godunov path is float64 in every variant: the mixed build's steps
-    equal the fp64 build's."""
+def test_mixed_godunov_close_to_fp64(omech, rs):
+    """The mixed build reconstructs the primitives in float32 (Riemann
+    solver, RK and temperature solve in float64): within the mixed bar of
+    the fp64 build after three steps."""
     from janc_b200.solver import Solver
     nx, ny = 40, 24
     U0, aux0 = _state2d(omech, nx, ny, 9)
@@ -194,5 +196,7 @@ def test_mixed_equals_fp64_on_godunov(omech, rs):
         s = Solver(2, nx, ny, 1e-4, 1e-4, BC2, precision=prec, flux_config=GOD[rs])
         U, a, _ = s.advance(cuda(U0), cuda(aux0), 3, cfl=0.5)
         out.append((host(U), host(a)))
-    np.testing.assert_array_equal(out[0][0], out[1][0])
-    np.testing.assert_array_equal(out[0][1], out[1][1])
+        assert s.status() == 0
+    assert field_err(out[1][0], out[0][0]) < 1e-4
+    assert field_err(out[1][0][:1], out[0][0][:1]) < 1e-6
+    assert field_err(out[1][1], out[0][1]) < 1e-6

@@ -26,6 +26,8 @@ PATHS = {
     "lf_mixed": ("mixed", None, None),
     "hllc": ("fp64", {"solver_type": "godunov", "interface_reconstruction": "WENO5_JS",
                       "riemann_solver": "HLLC", "viscosity": "off"}, None),
+    "hllc_mixed": ("mixed", {"solver_type": "godunov", "interface_reconstruction": "WENO5_JS",
+                             "riemann_solver": "HLLC", "viscosity": "off"}, None),
     "lf_viscous": ("fp64", {"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS",
                             "split_method": "LF", "viscosity": "on"},
                    {"viscosity_model": "Sutherland", "thermal_conductivity_model": "Prandtl number",
@@ -94,7 +96,7 @@ def test_2d_shapes_vs_oracle(omech, path, shape):
     assert field_err(Ug[:1], U[:1]) < (1e-6 if prec == "mixed" else 1e-10)
 
 
-@pytest.mark.parametrize("path", ["lf_fp64", "lf_mixed", "hllc"])
+@pytest.mark.parametrize("path", ["lf_fp64", "lf_mixed", "hllc", "hllc_mixed"])
 @pytest.mark.parametrize("nx", [4, 5, 254, 255, 256, 511])
 def test_1d_shapes_vs_oracle(omech, path, nx):
     prec, fc, tc = PATHS[path]

@@ -8,7 +8,7 @@ GPU (through the C ABI): flux_func with viscosity against the oracle for
 each transport model and boundary set (padded corners included), and RK
 steps.  Tolerances: ``fp64_strict`` 1e-12 relative L1 per field (the
 Sutherland law goes through pow), ``fp64`` 1e-11 per flux and 1e-10 over
-steps.
+steps, ``mixed`` 1e-4 per field and 1e-6 on the density.
 """
 import numpy as np
 import pytest
@@ -161,9 +161,11 @@ def test_viscous_godunov_steps_2d_vs_oracle(omech, prec):
         U, aux, t, _ = o.advance_func(U, aux, t)
     s = Solver(2, nx, ny, dx, dx, bc, precision=prec, flux_config=HLLC_VISC, transport_config=tc)
     Ug, ag, _ = s.advance(cuda(U0), cuda(aux0), 3, cfl=0.3)
-    tol = 1e-11 if prec == "fp64_strict" else 1e-10
-    assert field_err(host(Ug), U) < tol
+    tol = {"fp64_strict": 1e-11, "fp64": 1e-10, "mixed": 1e-4}[prec]
+    Ug = host(Ug)
+    assert field_err(Ug, U) < tol
     assert field_err(host(ag), aux) < tol
+    assert field_err(Ug[:1], U[:1]) < (1e-6 if prec == "mixed" else tol)
     assert s.status() == 0
 
 
