@@ -153,29 +153,39 @@ __device__ __forceinline__ void node_transport(const MP& m, const jb_transport& 
   }
 }
 
-// Node fluxes: 2D threads [0, nF) take F_hat at padded (px, py), px in
-// [0, nx+6), py in [3, ny+3) -> fh[c][px][py-3]; the rest G_hat at px in
-// [3, nx+3), py in [0, ny+6) -> gh[c][px-3][py].  1D: F_hat at every padded px.
+// Node fluxes, one thread per node.  2D threads [0, nF) take the nodes of
+// the F_hat region (padded px in [0, nx+6), py in [3, ny+3) ->
+// fh[c][px][py-3]); those with px in [3, nx+3) also lie in the G_hat region
+// and write G_hat (gh[c][px-3][py]) from the same transport and velocity
+// derivatives.  The rest are the G_hat-only nodes of the 3 + 3 ghost rows.
+// 1D: F_hat at every padded px.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_visc_flux(MP m, Grid g, jb_transport tr, const double* __restrict__ nodes,
                                                    double* __restrict__ fh, double* __restrict__ gh) {
   const int PX = g.nx + 6, PY = DIM == 2 ? g.ny + 6 : 1;
   const long long np = (long long)PX * PY;
   const long long nF = DIM == 2 ? (long long)PX * g.ny : PX;
-  const long long nG = DIM == 2 ? (long long)g.nx * PY : 0;
+  const long long nGo = DIM == 2 ? (long long)g.nx * 6 : 0;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nF + nG) return;
-  const bool xf = t < nF;
+  if (t >= nF + nGo) return;
   int px, py;
+  bool do_f, do_g;
   if (DIM == 1) {
     px = (int)t;
     py = 0;
-  } else if (xf) {
+    do_f = true;
+    do_g = false;
+  } else if (t < nF) {
     px = (int)(t / g.ny);
     py = (int)(t % g.ny) + 3;
+    do_f = true;
+    do_g = px >= 3 && px < g.nx + 3;
   } else {
-    px = (int)((t - nF) / PY) + 3;
-    py = (int)((t - nF) % PY);
+    const int j = (int)((t - nF) % 6);
+    px = (int)((t - nF) / 6) + 3;
+    py = j < 3 ? j : g.ny + j;
+    do_f = false;
+    do_g = true;
   }
   const long long i = (long long)px * PY + py;
   const double* N = nodes;
@@ -192,9 +202,9 @@ __global__ void __launch_bounds__(128) k_visc_flux(MP m, Grid g, jb_transport tr
   const double* ly = N + (long long)px * PY;      // line at this x, position py
   auto ddx = [&](int plane) { return d_line(lx + plane * np, PY, PX, px, g.dx); };
   auto ddy = [&](int plane) { return d_line(ly + plane * np, 1, PY, py, g.dy); };
-  double* out;
-  long long ostride, oidx;
   if (DIM == 1) {
+    double* out;
+    long long ostride, oidx;
     const double du_dx = ddx(1), dT_dx = ddx(2);
     const double div_u = du_dx;
     const double tau = 2.0 * tp.mu * du_dx - 2.0 / 3.0 * tp.mu * div_u;
@@ -219,39 +229,46 @@ __global__ void __launch_bounds__(128) k_visc_flux(MP m, Grid g, jb_transport tr
   const double lam = -2.0 / 3.0 * tp.mu;
   const double S12 = 0.5 * (du_dy + dv_dx);
   const double div_u = du_dx + dv_dy;
-  double jn[NS], e = 0.0;
-  const double dTn = xf ? ddx(3) : ddy(3);
-#pragma unroll
-  for (int k = 0; k < NS; ++k) {
-    jn[k] = -rho * tp.D[k] * (xf ? ddx(4 + k) : ddy(4 + k));
-    e = k == 0 ? jn[0] * tp.h[0] : e + jn[k] * tp.h[k];
-  }
-  const double qn = -tp.k * dTn;
   const double tau_xy = 2.0 * tp.mu * S12;
-  double f1, f2, f3;
-  if (xf) {
-    const double tau_xx = 2.0 * tp.mu * du_dx + lam * div_u;
-    f1 = tau_xx;
-    f2 = tau_xy;
-    f3 = u * tau_xx + v * tau_xy - qn - e;
-    out = fh;
-    ostride = (long long)PX * g.ny;
-    oidx = (long long)px * g.ny + (py - 3);
-  } else {
-    const double tau_yy = 2.0 * tp.mu * dv_dy + lam * div_u;
-    f1 = tau_xy;
-    f2 = tau_yy;
-    f3 = u * tau_xy + v * tau_yy - qn - e;
-    out = gh;
-    ostride = (long long)g.nx * PY;
-    oidx = (long long)(px - 3) * PY + py;
-  }
-  out[oidx] = 0.0;
-  out[ostride + oidx] = f1;
-  out[2 * ostride + oidx] = f2;
-  out[3 * ostride + oidx] = f3;
+  // one direction's heat and species fluxes and its node flux vector
+  auto emit = [&](bool xdir) {
+    double jn[NS], e = 0.0;
+    const double dTn = xdir ? ddx(3) : ddy(3);
 #pragma unroll
-  for (int k = 0; k < NR; ++k) out[(4 + k) * ostride + oidx] = -jn[k];
+    for (int k = 0; k < NS; ++k) {
+      jn[k] = -rho * tp.D[k] * (xdir ? ddx(4 + k) : ddy(4 + k));
+      e = k == 0 ? jn[0] * tp.h[0] : e + jn[k] * tp.h[k];
+    }
+    const double qn = -tp.k * dTn;
+    double f1, f2, f3;
+    double* o;
+    long long os, oi;
+    if (xdir) {
+      const double tau_xx = 2.0 * tp.mu * du_dx + lam * div_u;
+      f1 = tau_xx;
+      f2 = tau_xy;
+      f3 = u * tau_xx + v * tau_xy - qn - e;
+      o = fh;
+      os = (long long)PX * g.ny;
+      oi = (long long)px * g.ny + (py - 3);
+    } else {
+      const double tau_yy = 2.0 * tp.mu * dv_dy + lam * div_u;
+      f1 = tau_xy;
+      f2 = tau_yy;
+      f3 = u * tau_xy + v * tau_yy - qn - e;
+      o = gh;
+      os = (long long)g.nx * PY;
+      oi = (long long)(px - 3) * PY + py;
+    }
+    o[oi] = 0.0;
+    o[os + oi] = f1;
+    o[2 * os + oi] = f2;
+    o[3 * os + oi] = f3;
+#pragma unroll
+    for (int k = 0; k < NR; ++k) o[(4 + k) * os + oi] = -jn[k];
+  };
+  if (do_f) emit(true);
+  if (do_g) emit(false);
 }
 
 // interface value from six node fluxes (reconstruction/CENTRAL6.py)
