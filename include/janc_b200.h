@@ -112,6 +112,13 @@ int jb_set_spacing(jb_handle* h, double dx, double dy);
  * jb_adjoint_step supports JB_FLUX_LF only. */
 int jb_set_flux_scheme(jb_handle* h, int scheme);
 
+/* Select the face reconstruction of both flux paths (the
+ * 'interface_reconstruction' entry of set_flux_solver,
+ * solver_2D/reconstruction/__init__.py): JB_RECON_WENO5 (WENO5-JS, the
+ * default) or JB_RECON_MUSCL (reconstruction/MUSCL.py: minmod limiter,
+ * kappa = 1/3, beta = 1).  jb_adjoint_step supports WENO5-JS only. */
+int jb_set_reconstruction(jb_handle* h, int recon);
+
 /* Viscous fluxes (flux_solver_config 'viscosity': 'on'; replaces
  * transport_model.set_transport, model/transport_model.py:26-104, and
  * viscous_flux, solver_2D/flux.py:70-115 / solver_1D/flux.py:67-99): the

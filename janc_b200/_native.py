@@ -15,12 +15,13 @@ BC_KIND = {"periodic": 0, "slip_wall": 1, "zero_gradient": 2, "no_slip_wall": 3,
            "pressure_outlet": 4, "rdc_injector": 5}
 PRECISION = {"fp64_strict": 0, "fp64": 1, "mixed": 2}
 FLUX_SCHEME = {"LF": 0, "HLLC": 1, "AUSMPW_plus": 2}  # split method / Riemann solver
+RECONSTRUCTION = {"WENO5_JS": 0, "MUSCL": 1}
 STATUS = {1: "bad argument", 2: "CUDA error", 4: "non-finite state", 8: "singular chemistry matrix",
           16: "device wait timed out", 32: "unsupported configuration"}
 
 EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_func", "jb_update_aux",
            "jb_reaction_source_terms", "jb_advance", "jb_cfl_dt", "jb_get_thermo", "jb_status",
-           "jb_workspace_bytes", "jb_set_spacing", "jb_set_flux_scheme", "jb_set_transport", "jb_sizeof_mech_params",
+           "jb_workspace_bytes", "jb_set_spacing", "jb_set_flux_scheme", "jb_set_reconstruction", "jb_set_transport", "jb_sizeof_mech_params",
            "jb_sizeof_grid",
            "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times",
            "jb_update_aux_noalloc", "jb_rk3", "jb_u_to_prim",
@@ -77,6 +78,7 @@ def lib(path=None):
     L.jb_workspace_bytes.restype = ll
     L.jb_set_spacing.argtypes = [vp, d, d]
     L.jb_set_flux_scheme.argtypes = [vp, i]
+    L.jb_set_reconstruction.argtypes = [vp, i]
     L.jb_set_transport.argtypes = [vp, ctypes.POINTER(Transport)]
     L.jb_probe_fp64_fma.argtypes = [i, i, dp, vp]
     L.jb_set_kernel_timing.argtypes = [vp, i]

@@ -451,6 +451,13 @@ int jb_kernel_times(jb_handle* h, double* ms, long long* launches) {
   return JB_OK;
 }
 
+int jb_set_reconstruction(jb_handle* h, int recon) {
+  if (!h) return JB_ERR_ARG;
+  if (recon != JB_RECON_WENO5 && recon != JB_RECON_MUSCL) return set_err(h, JB_ERR_ARG, "unknown reconstruction");
+  h->grid.recon = recon;
+  return JB_OK;
+}
+
 int jb_set_transport(jb_handle* h, const jb_transport* tr) {
   if (!h) return JB_ERR_ARG;
   if (!tr) {  // Euler fluxes again
@@ -562,8 +569,8 @@ static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mu
 static int adj_workspace(jb_handle* h) {
   if (h->adj_ws) return JB_OK;
   if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
-  if (h->grid.scheme != JB_FLUX_LF || h->grid.visc)
-    return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint differentiates the inviscid LF flux-splitting path");
+  if (h->grid.scheme != JB_FLUX_LF || h->grid.visc || h->grid.recon != JB_RECON_WENO5)
+    return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint differentiates the inviscid LF / WENO5-JS path");
   for (int s = 0; s < 4; ++s)
     if (h->grid.bc[s] == JB_BC_PRESSURE_OUTLET || h->grid.bc[s] == JB_BC_RDC_INJECTOR)
       return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint supports periodic, slip, no-slip and zero-gradient sides");

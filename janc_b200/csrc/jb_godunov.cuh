@@ -9,9 +9,6 @@
 
 constexpr int RS_HLLC = 0, RS_AUSMPW = 1;
 
-// jnp.minimum / jnp.maximum: a NaN operand gives NaN (fmin / fmax drop it)
-__device__ __forceinline__ double nan_min(double a, double b) { return (a != a || b != b) ? a + b : fmin(a, b); }
-__device__ __forceinline__ double nan_max(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
 
 // gamma and h of a reconstructed face state from T = p / (R rho)
 // (HLLC.py:8-12 / AUSMPW_plus.py:86-92 in 2D).
@@ -227,8 +224,8 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
 #pragma unroll
     for (int f = 0; f < 12; ++f) {
       const RW* b = sW + f * SM2_Q + mxf * PY2 + jy + 3;
-      wL[f] = weno_L(b[0], b[PY2], b[2 * PY2], b[3 * PY2], b[4 * PY2]);
-      wR[f] = weno_R(b[PY2], b[2 * PY2], b[3 * PY2], b[4 * PY2], b[5 * PY2]);
+      wL[f] = recon_L(g, b[0], b[PY2], b[2 * PY2], b[3 * PY2], b[4 * PY2]);
+      wR[f] = recon_R(g, b[PY2], b[2 * PY2], b[3 * PY2], b[4 * PY2], b[5 * PY2]);
     }
     riemann_flux<2, 1, RS>(m, wL, wR, F);
 #pragma unroll
@@ -240,8 +237,8 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
 #pragma unroll
     for (int f = 0; f < 12; ++f) {
       const RW* b = sW + f * SM2_Q + (jx + 3) * PY2 + myf;
-      wL[f] = weno_L(b[0], b[1], b[2], b[3], b[4]);
-      wR[f] = weno_R(b[1], b[2], b[3], b[4], b[5]);
+      wL[f] = recon_L(g, b[0], b[1], b[2], b[3], b[4]);
+      wR[f] = recon_R(g, b[1], b[2], b[3], b[4], b[5]);
     }
     riemann_flux<2, 2, RS>(m, wL, wR, F);
 #pragma unroll
@@ -346,8 +343,8 @@ __global__ void __launch_bounds__(NT1) k_god1d(MP m, Grid g, const double* __res
 #pragma unroll
     for (int f = 0; f < 11; ++f) {
       const RW* b = sW + f * PW + tid;
-      wL[f] = weno_L(b[0], b[1], b[2], b[3], b[4]);
-      wR[f] = weno_R(b[1], b[2], b[3], b[4], b[5]);
+      wL[f] = recon_L(g, b[0], b[1], b[2], b[3], b[4]);
+      wR[f] = recon_R(g, b[1], b[2], b[3], b[4], b[5]);
     }
     riemann_flux<1, 1, RS>(m, wL, wR, F);
 #pragma unroll

@@ -693,6 +693,47 @@ __device__ __forceinline__ float lf_flux(int f, int dir, float q, float rho, flo
 }
 #endif
 
+// jnp.minimum / jnp.maximum: a NaN operand gives NaN (fmin / fmax drop it)
+__device__ __forceinline__ double nan_min(double a, double b) { return (a != a || b != b) ? a + b : fmin(a, b); }
+__device__ __forceinline__ double nan_max(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
+__device__ __forceinline__ float nan_min(float a, float b) { return (a != a || b != b) ? a + b : fminf(a, b); }
+__device__ __forceinline__ float nan_max(float a, float b) { return (a != a || b != b) ? a + b : fmaxf(a, b); }
+
+// jnp.sign: -1, 0 (signed zero kept), +1, NaN
+template <class R>
+__device__ __forceinline__ R sign_ref(R x) { return x > R(0) ? R(1) : (x < R(0) ? R(-1) : x); }
+
+// MUSCL (reconstruction/MUSCL.py): min_mod_limiter, kappa = 1/3, beta = 1.
+// Arguments as the WENO forms take them (cells j-2 .. j+2); MUSCL reads the
+// middle three.  Left: q_j + s_L; right: q_j - s_R.
+template <class R>
+__device__ __forceinline__ R minmod_ref(R x, R y) {
+  const R m1 = nan_min(x * sign_ref(y), y * sign_ref(x));
+  return sign_ref(x) * nan_max(R(0), m1);
+}
+template <class R>
+__device__ __forceinline__ R muscl_L(R, R fjm1, R fj, R fjp1, R) {
+  const R dm = fj - fjm1, dp = fjp1 - fj;
+  const R fw = minmod_ref(dp, R(1) * dm), bw = minmod_ref(dm, R(1) * dp);
+  return fj + R(0.25) * (R(1.0 - 1.0 / 3.0) * bw + R(1.0 + 1.0 / 3.0) * fw);
+}
+template <class R>
+__device__ __forceinline__ R muscl_R(R, R fjm1, R fj, R fjp1, R) {
+  const R dm = fj - fjm1, dp = fjp1 - fj;
+  const R fw = minmod_ref(dp, R(1) * dm), bw = minmod_ref(dm, R(1) * dp);
+  return fj - R(0.25) * (R(1.0 - 1.0 / 3.0) * fw + R(1.0 + 1.0 / 3.0) * bw);
+}
+
+// the grid's face reconstruction (a warp-uniform choice)
+template <class R>
+__device__ __forceinline__ R recon_L(const Grid& g, R a, R b, R c, R d, R e) {
+  return g.recon == JB_RECON_MUSCL ? muscl_L(a, b, c, d, e) : weno_L(a, b, c, d, e);
+}
+template <class R>
+__device__ __forceinline__ R recon_R(const Grid& g, R a, R b, R c, R d, R e) {
+  return g.recon == JB_RECON_MUSCL ? muscl_R(a, b, c, d, e) : weno_R(a, b, c, d, e);
+}
+
 // rho, u, v, p of one cell for the flux (U_to_prim; the flux needs no gamma)
 template <int DIM>
 __device__ __forceinline__ void flux_prims(const MP& m, const double* q, double T, double& rho,
@@ -869,17 +910,17 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       int mxf = tid / TY2, jy = tid % TY2;  // x-faces: 16 x 16 = 256
       const R* hp = sHxp + jy;
       const R* hm = sHxm + jy;
-      R L = weno_L(hp[(mxf) * TY2], hp[(mxf + 1) * TY2], hp[(mxf + 2) * TY2], hp[(mxf + 3) * TY2],
+      R L = recon_L(g, hp[(mxf) * TY2], hp[(mxf + 1) * TY2], hp[(mxf + 2) * TY2], hp[(mxf + 3) * TY2],
                         hp[(mxf + 4) * TY2]);
-      R Rr = weno_R(hm[(mxf + 1) * TY2], hm[(mxf + 2) * TY2], hm[(mxf + 3) * TY2], hm[(mxf + 4) * TY2],
+      R Rr = recon_R(g, hm[(mxf + 1) * TY2], hm[(mxf + 2) * TY2], hm[(mxf + 3) * TY2], hm[(mxf + 4) * TY2],
                     hm[(mxf + 5) * TY2]);
       sFx[mxf * TY2 + jy] = L + Rr;
       if (tid < SM2_FY) {
         int jx = tid / (TY2 + 1), myf = tid % (TY2 + 1);
         const R* gp = sHyp + jx * PY2 + myf;
         const R* gm = sHym + jx * PY2 + myf;
-        R Lg = weno_L(gp[0], gp[1], gp[2], gp[3], gp[4]);
-        R Rg = weno_R(gm[1], gm[2], gm[3], gm[4], gm[5]);
+        R Lg = recon_L(g, gp[0], gp[1], gp[2], gp[3], gp[4]);
+        R Rg = recon_R(g, gm[1], gm[2], gm[3], gm[4], gm[5]);
         sFy[jx * (TY2 + 1) + myf] = Lg + Rg;
       }
     }
@@ -1237,8 +1278,8 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
     __syncthreads();
     {
       int mf = tid;  // NT faces
-      R L = weno_L(sHp[mf], sHp[mf + 1], sHp[mf + 2], sHp[mf + 3], sHp[mf + 4]);
-      R Rr = weno_R(sHm[mf + 1], sHm[mf + 2], sHm[mf + 3], sHm[mf + 4], sHm[mf + 5]);
+      R L = recon_L(g, sHp[mf], sHp[mf + 1], sHp[mf + 2], sHp[mf + 3], sHp[mf + 4]);
+      R Rr = recon_R(g, sHm[mf + 1], sHm[mf + 2], sHm[mf + 3], sHm[mf + 4], sHm[mf + 5]);
       sF[mf] = L + Rr;
     }
     __syncthreads();

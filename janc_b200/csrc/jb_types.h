@@ -65,6 +65,10 @@ enum jb_precision { JB_PREC_STRICT = 0, JB_PREC_FP64 = 1, JB_PREC_MIXED = 2 };
 // and a Riemann solver).
 enum jb_flux_scheme { JB_FLUX_LF = 0, JB_FLUX_HLLC = 1, JB_FLUX_AUSMPW = 2 };
 
+// Face reconstruction (solver_{1D,2D}/reconstruction): WENO5-JS or MUSCL
+// (minmod limiter, kappa = 1/3, beta = 1).
+enum jb_reconstruction { JB_RECON_WENO5 = 0, JB_RECON_MUSCL = 1 };
+
 // Laminar transport (model/transport_model.py set_transport): viscosity
 // 0 Sutherland mu_ref (T/T_ref)^1.5 (T_ref+S)/(T+S), 1 constant rho nu0;
 // conductivity 0 Prandtl number mu cp/Pr, 1 constant k0; diffusivity 0 Lewis
@@ -99,6 +103,7 @@ typedef struct jb_grid {
   double inj_block_p;    // injector blocked when p_in >= this (1.0 nondim)
   int lstrip;            // ghost strip length max(nx, ny)
   int scheme;            // advective flux (jb_flux_scheme): LF splitting or Godunov + Riemann solver
+  int recon;             // face reconstruction (jb_reconstruction): WENO5-JS or MUSCL
   const double* visc;    // viscous rhs of the stage state (ncell x nv) or null: Euler fluxes
 } jb_grid;
 

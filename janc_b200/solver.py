@@ -26,16 +26,14 @@ def flux_scheme(flux_config):
     solver_2D/flux.py:19-40) and name the native flux: ``LF``, ``HLLC`` or
     ``AUSMPW_plus``.  Raises as the reference does: KeyError for an unknown
     solver type or dictionary entry; what the reference has but this build
-    does not (MUSCL, SW splitting) raises NotImplementedError."""
+    does not (SW splitting) raises NotImplementedError."""
     if flux_config is None:
         return "LF"
     solver_type = flux_config["solver_type"]
     if solver_type not in ("godunov", "flux_splitting"):
         raise KeyError("JANC only support 'godunov' and 'flux_splitting'")
     recon = flux_config["interface_reconstruction"]
-    if recon == "MUSCL":
-        raise NotImplementedError("MUSCL reconstruction is not built; use WENO5_JS")
-    if recon != "WENO5_JS":
+    if recon not in _native.RECONSTRUCTION:
         raise KeyError(recon)
     if solver_type == "godunov":
         rs = flux_config["riemann_solver"]
@@ -109,7 +107,8 @@ class Solver:
     (solver_{1D,2D}/flux.py set_flux_solver): ``solver_type``
     ``flux_splitting`` (``split_method`` ``LF``) or ``godunov``
     (``riemann_solver`` ``HLLC`` or ``AUSMPW_plus``), with
-    ``interface_reconstruction`` ``WENO5_JS``.  Default: LF flux splitting.
+    ``interface_reconstruction`` ``WENO5_JS`` or ``MUSCL``.  Default: LF flux
+    splitting with WENO5_JS.
     ``viscosity`` ``on`` adds the laminar viscous fluxes of
     ``transport_config`` (the reference's transport_config: Sutherland or
     constant viscosity, Prandtl-number or constant conductivity, Lewis /
@@ -162,6 +161,9 @@ class Solver:
         self._lib = L
         self.flux_scheme = flux_scheme(flux_config)
         _native.check(L.jb_set_flux_scheme(h, _native.FLUX_SCHEME[self.flux_scheme]), h, "jb_set_flux_scheme")
+        self.reconstruction = (flux_config or {}).get("interface_reconstruction", "WENO5_JS")
+        _native.check(L.jb_set_reconstruction(h, _native.RECONSTRUCTION[self.reconstruction]), h,
+                      "jb_set_reconstruction")
         self.viscous = bool(flux_config) and flux_config.get("viscosity", "off") == "on"
         if self.viscous:
             if transport_config is None:

@@ -663,6 +663,45 @@ def _interface_R(q, axis, other_interior):
     return _weno_R(s(1, -4), s(2, -3), s(3, -2), s(4, -1), s(5, None))
 
 
+def _minmod(x, y):
+    """min_mod_limiter (reconstruction/MUSCL.py:4-7)"""
+    mask1 = np.minimum(x * np.sign(y), y * np.sign(x))
+    mask = np.maximum(np.zeros_like(mask1), mask1)
+    return np.sign(x) * mask
+
+
+def _muscl(q, axis, other_interior, left, k=1 / 3, beta=1.0):
+    """MUSCL interface_L / interface_R (reconstruction/MUSCL.py, 1D and 2D):
+    face states of cells 1 .. n+4 of the padded axis, minmod-limited."""
+    def s(a, b):
+        idx = [slice(None)] * q.ndim
+        idx[axis] = slice(a, b)
+        if other_interior is not None:
+            idx[other_interior] = slice(3, -3)
+        return q[tuple(idx)]
+
+    def t(U, a, b):
+        idx = [slice(None)] * U.ndim
+        idx[axis] = slice(a, b)
+        return U[tuple(idx)]
+    U = s(1, -1)
+    d_minus = t(U, 1, -1) - t(U, None, -2)
+    d_plus = t(U, 2, None) - t(U, 1, -1)
+    phi_fw = _minmod(d_plus, beta * d_minus)
+    phi_bw = _minmod(d_minus, beta * d_plus)
+    if left:
+        s_L = 1 / 4 * ((1 - k) * phi_bw + (1 + k) * phi_fw)
+        return t(U, 1, -2) + t(s_L, None, -1)
+    s_R = 1 / 4 * ((1 - k) * phi_fw + (1 + k) * phi_bw)
+    return t(U, 2, -1) - t(s_R, 1, None)
+
+
+def _recon(q, axis, other_interior, left, recon):
+    if recon == "MUSCL":
+        return _muscl(q, axis, other_interior, left)
+    return (_interface_L if left else _interface_R)(q, axis, other_interior)
+
+
 def split_flux_1d(m, U, aux):
     """solver_1D/flux_splitting/LF.py:4-13"""
     rho, u, Y, p, a = U_to_prim(m, U, aux)
@@ -687,18 +726,18 @@ def split_flux_2d(m, ixy, U, aux):
     return 0.5 * (F + th * U), 0.5 * (F - th * U)
 
 
-def total_flux(m, Up, Ap, dx, dy=None):
+def total_flux(m, Up, Ap, dx, dy=None, recon="WENO5_JS"):
     """flux_splitting (solver_1D/flux.py:51-58, solver_2D/flux.py:56-68) on
     the ghost-padded arrays; returns -(dF/dx [+ dG/dy])."""
     if Up.ndim == 2:
         Fplus, Fminus = split_flux_1d(m, Up, Ap)
-        F = _interface_L(Fplus, 1, None) + _interface_R(Fminus, 1, None)
+        F = _recon(Fplus, 1, None, True, recon) + _recon(Fminus, 1, None, False, recon)
         dF = F[:, 1:] - F[:, :-1]
         return -(dF / dx)
     Fplus, Fminus = split_flux_2d(m, 1, Up, Ap)
     Gplus, Gminus = split_flux_2d(m, 2, Up, Ap)
-    F = _interface_L(Fplus, 1, 2) + _interface_R(Fminus, 1, 2)
-    G = _interface_L(Gplus, 2, 1) + _interface_R(Gminus, 2, 1)
+    F = _recon(Fplus, 1, 2, True, recon) + _recon(Fminus, 1, 2, False, recon)
+    G = _recon(Gplus, 2, 1, True, recon) + _recon(Gminus, 2, 1, False, recon)
     dF = F[:, 1:, :] - F[:, :-1, :]
     dG = G[:, :, 1:] - G[:, :, :-1]
     return -(dF / dx + dG / dy)
@@ -824,7 +863,7 @@ def _ausmpw(m, qL, qR, dim, n):
 RIEMANN = {"HLLC": _hllc, "AUSMPW_plus": _ausmpw}
 
 
-def godunov_flux(m, Up, Ap, dx, dy=None, riemann="HLLC"):
+def godunov_flux(m, Up, Ap, dx, dy=None, riemann="HLLC", recon="WENO5_JS"):
     """godunov_flux (solver_1D/flux.py:41-49, solver_2D/flux.py:43-54) on the
     ghost-padded arrays: primitives q = [rho, u, (v), p, Y], WENO5-JS
     left / right face states per component, the Riemann flux, and
@@ -833,13 +872,13 @@ def godunov_flux(m, Up, Ap, dx, dy=None, riemann="HLLC"):
     if Up.ndim == 2:
         rho, u, Y, p, a = U_to_prim(m, Up, Ap)
         q = np.concatenate([rho, u, p, Y], axis=0)
-        F = rs(m, _interface_L(q, 1, None), _interface_R(q, 1, None), 1, 1)
+        F = rs(m, _recon(q, 1, None, True, recon), _recon(q, 1, None, False, recon), 1, 1)
         dF = F[:, 1:] - F[:, :-1]
         return -(dF / dx)
     rho, u, v, Y, p, a = U_to_prim(m, Up, Ap)
     q = np.concatenate([rho, u, v, p, Y], axis=0)
-    F = rs(m, _interface_L(q, 1, 2), _interface_R(q, 1, 2), 2, 1)
-    G = rs(m, _interface_L(q, 2, 1), _interface_R(q, 2, 1), 2, 2)
+    F = rs(m, _recon(q, 1, 2, True, recon), _recon(q, 1, 2, False, recon), 2, 1)
+    G = rs(m, _recon(q, 2, 1, True, recon), _recon(q, 2, 1, False, recon), 2, 2)
     dF = F[:, 1:, :] - F[:, :-1, :]
     dG = G[:, :, 1:] - G[:, :, :-1]
     return -(dF / dx + dG / dy)
@@ -1015,14 +1054,15 @@ class Solver:
         fc = flux_config or {"solver_type": "flux_splitting"}
         self.solver_type = fc["solver_type"]
         self.riemann = fc.get("riemann_solver", "HLLC")
+        self.recon = fc.get("interface_reconstruction", "WENO5_JS")
         self.transport = Transport(transport_config) if fc.get("viscosity", "off") == "on" else None
 
     def flux_func(self, U, aux, dx, dy, dt, theta=None):
         Up, Ap = boundary_conditions(self.m, U, aux, self.bc, theta)
         if self.solver_type == "godunov":
-            adv = godunov_flux(self.m, Up, Ap, dx, dy, self.riemann)
+            adv = godunov_flux(self.m, Up, Ap, dx, dy, self.riemann, self.recon)
         else:
-            adv = total_flux(self.m, Up, Ap, dx, dy)
+            adv = total_flux(self.m, Up, Ap, dx, dy, self.recon)
         if self.transport is not None:  # NS_flux = advective + viscous (solver_2D/flux.py:117-118)
             return dt * (adv + viscous_flux(self.m, self.transport, Up, Ap, dx, dy))
         return dt * adv

@@ -49,8 +49,10 @@ def test_flux_config_validation():
         flux_scheme({"solver_type": "spectral"})
     with pytest.raises(KeyError):
         flux_scheme({"solver_type": "godunov", "interface_reconstruction": "WENO5_JS", "riemann_solver": "Roe"})
-    with pytest.raises(NotImplementedError):
-        flux_scheme({"solver_type": "godunov", "interface_reconstruction": "MUSCL", "riemann_solver": "HLLC"})
+    assert flux_scheme({"solver_type": "godunov", "interface_reconstruction": "MUSCL",
+                        "riemann_solver": "HLLC"}) == "HLLC"
+    with pytest.raises(KeyError):
+        flux_scheme({"solver_type": "godunov", "interface_reconstruction": "WENO7", "riemann_solver": "HLLC"})
     with pytest.raises(NotImplementedError):
         flux_scheme({"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS",
                      "split_method": "SW"})
