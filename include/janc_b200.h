@@ -128,6 +128,28 @@ int jb_set_reconstruction(jb_handle* h, int recon);
  * call.  jb_adjoint_step supports the inviscid path only. */
 int jb_set_transport(jb_handle* h, const jb_transport* tr);
 
+/* x-slab decomposition (replaces the reference's is_parallel mode:
+ * parallel/boundary_padding.py exchange_halo, parallel/boundary.py
+ * boundary_conditions_{1D,2D}, the jax.lax.pmin of CFL_1D / CFL_2D in
+ * simulation/set_simulator.py:413-436).  A handle holds one slab of
+ * nx columns; a left / right side created with JB_BC_HALO takes its 3 ghost
+ * columns from the neighbouring slab, a physical side keeps its boundary
+ * condition (the first and last slab of a non-periodic x axis).  Before each
+ * flux evaluation the handle packs its 3 edge columns of (U, aux) into
+ * send[2][nv+2][3][ny] (side 0: columns 0..2, side 1: columns nx-3..nx-1)
+ * and calls fn(user, flags, stream) on the launch stream; with JB_XCH_HALO
+ * the transport must deliver into halo[0] the left neighbour's send[1] and
+ * into halo[1] the right neighbour's send[0] (the ring wraps for every x
+ * side, as exchange_halo does; a physical side's halo supplies only its
+ * padded corners), with JB_XCH_DT replace red[0..1] by their MIN over the
+ * ranks (the CFL minimum).  Both stream-ordered on `stream`; fn returns 0 on
+ * success.  LF alpha and the temperature solve's stop stay per slab, as in
+ * the reference.  Buffers are caller-owned device memory and must outlive
+ * the handle's calls; fn = NULL detaches.  The adjoint is single-domain. */
+typedef int (*jb_exchange_fn)(void* user, int flags, void* stream);
+int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb_exchange_fn fn,
+                    void* user);
+
 /* sizeof(jb_mech_params) and sizeof(jb_grid) as compiled, for binding checks. */
 int jb_sizeof_mech_params(void);
 int jb_sizeof_grid(void);

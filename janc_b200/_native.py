@@ -13,6 +13,9 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libjanc_b20
 
 BC_KIND = {"periodic": 0, "slip_wall": 1, "zero_gradient": 2, "no_slip_wall": 3,
            "pressure_outlet": 4, "rdc_injector": 5}
+BC_HALO = 6  # x side bordering another slab (jb_set_exchange)
+XCH_DT, XCH_HALO = 1, 2  # jb_exchange_flags
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p)
 PRECISION = {"fp64_strict": 0, "fp64": 1, "mixed": 2}
 FLUX_SCHEME = {"LF": 0, "HLLC": 1, "AUSMPW_plus": 2}  # split method / Riemann solver
 RECONSTRUCTION = {"WENO5_JS": 0, "MUSCL": 1}
@@ -21,7 +24,8 @@ STATUS = {1: "bad argument", 2: "CUDA error", 4: "non-finite state", 8: "singula
 
 EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_func", "jb_update_aux",
            "jb_reaction_source_terms", "jb_advance", "jb_cfl_dt", "jb_get_thermo", "jb_status",
-           "jb_workspace_bytes", "jb_set_spacing", "jb_set_flux_scheme", "jb_set_reconstruction", "jb_set_transport", "jb_sizeof_mech_params",
+           "jb_workspace_bytes", "jb_set_spacing", "jb_set_flux_scheme", "jb_set_reconstruction", "jb_set_transport", "jb_set_exchange",
+           "jb_sizeof_mech_params",
            "jb_sizeof_grid",
            "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times",
            "jb_update_aux_noalloc", "jb_rk3", "jb_u_to_prim",
@@ -80,6 +84,7 @@ def lib(path=None):
     L.jb_set_flux_scheme.argtypes = [vp, i]
     L.jb_set_reconstruction.argtypes = [vp, i]
     L.jb_set_transport.argtypes = [vp, ctypes.POINTER(Transport)]
+    L.jb_set_exchange.argtypes = [vp, dp, dp, dp, EXCHANGE_FN, vp]
     L.jb_probe_fp64_fma.argtypes = [i, i, dp, vp]
     L.jb_set_kernel_timing.argtypes = [vp, i]
     L.jb_update_aux_noalloc.argtypes = [ctypes.POINTER(_mech.MechParams), i, i, i, i, dp, dp, dp, vp]

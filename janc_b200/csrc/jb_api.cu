@@ -51,6 +51,11 @@ struct jb_handle {
   double* adj_prims;  // rho, u, v, p of the three stage states of a step
   double* adj_scratch;
   double* adj_red;
+  // x-slab exchange (jb_set_exchange): caller-owned buffers and transport
+  jb_exchange_fn xch;
+  void* xch_user;
+  double* xsend;  // [2][nv+2][3][ny] edge columns packed for the neighbours
+  long long* xred;  // CFL pair reduced over the ranks
   char err[512];
 };
 
@@ -131,7 +136,7 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   if (dim == 1) ny = 1;
   if (!(dx > 0.0) || (dim == 2 && !(dy > 0.0))) return JB_ERR_ARG;
   for (int s = 0; s < 2 * dim; ++s)
-    if (!bc_ok(bc[s])) return JB_ERR_ARG;
+    if (!bc_ok(bc[s]) && !(s < 2 && bc[s] == JB_BC_HALO)) return JB_ERR_ARG;
   if (dim == 1 && (bc[0] == JB_BC_RDC_INJECTOR || bc[1] == JB_BC_RDC_INJECTOR)) return JB_ERR_UNSUPPORTED;
   if (precision != JB_PREC_STRICT && precision != JB_PREC_FP64 && precision != JB_PREC_MIXED)
     return JB_ERR_UNSUPPORTED;
@@ -219,7 +224,41 @@ static int check_theta(jb_handle* h) {
   for (int s = 0; s < 2 * h->dim; ++s) {
     if (g.bc[s] == JB_BC_RDC_INJECTOR && !g.Yinj)
       return set_err(h, JB_ERR_ARG, "injector boundary needs theta['Yinj'] (jb_set_theta)");
+    if (g.bc[s] == JB_BC_HALO && !h->xch)
+      return set_err(h, JB_ERR_ARG, "a halo side needs an exchange (jb_set_exchange)");
   }
+  return JB_OK;
+}
+
+// One slab exchange: pack, hand the stream to the transport, unpack.  No-op
+// for a handle without an exchange.
+static int exchange(jb_handle* h, const double* U, const double* aux, int flags, int aidx, cudaStream_t st) {
+  if (!h->xch) return JB_OK;
+  const jb::Ops& o = *h->ops;
+  JB_TRY(o.xch_pre(h->dim, h->grid, U, aux, h->xsend, h->slots, h->xred, flags, st), "exchange pack");
+  const int rc = h->xch(h->xch_user, flags, (void*)st);
+  if (rc != 0) return set_err(h, JB_ERR_ARG, "exchange transport failed (%d)", rc);
+  JB_TRY(o.xch_post(h->dim, h->mech, h->grid, h->slots, h->xred, aidx, flags, st), "exchange unpack");
+  return JB_OK;
+}
+
+int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb_exchange_fn fn, void* user) {
+  if (!h) return JB_ERR_ARG;
+  if (!fn) {
+    h->xch = nullptr;
+    h->xch_user = nullptr;
+    h->xsend = nullptr;
+    h->xred = nullptr;
+    h->grid.halo = nullptr;
+    return JB_OK;
+  }
+  if (!send || !halo || !red) return set_err(h, JB_ERR_ARG, "exchange needs send, halo and red buffers");
+  if (h->grid.nx < 3) return set_err(h, JB_ERR_ARG, "a slab needs at least 3 columns");
+  h->xch = fn;
+  h->xch_user = user;
+  h->xsend = send;
+  h->xred = red;
+  h->grid.halo = halo;
   return JB_OK;
 }
 
@@ -233,6 +272,7 @@ int jb_flux_func(jb_handle* h, const double* U, const double* aux, double dt, do
   JB_TRY(o.select(h->dim, false, true, false, h->mech, h->grid, U, aux, nullptr, nullptr, h->strips,
                   h->slots, -1, 3, nullptr, st),
          "alpha");
+  if (int rc = exchange(h, U, aux, JB_XCH_HALO, 3, st)) return rc;
   if (h->grid.visc)
     JB_TRY(o.visc(h->dim, h->mech, h->grid, h->tr, U, aux, h->strips, h->vbuf, h->vcell, st), "viscous");
   JB_TRY(o.flux(h->dim, 0, h->mech, h->grid, U, aux, nullptr, rhs, nullptr, h->strips, h->slots, 3,
@@ -281,6 +321,7 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
   if (probe_p && (h->dim != 2 || h->probe[2] * h->probe[3] <= 0))
     return set_err(h, JB_ERR_ARG, "probe pressures need a 2D handle with jb_set_probe");
   if (rec && (!rec_slots || !chemistry)) return set_err(h, JB_ERR_ARG, "a record needs rec_slots");
+  if (rec && h->xch) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint record is single-domain");
   cudaStream_t st = (cudaStream_t)stream;
   const jb::Ops& o = *h->ops;
   const int d = h->dim;
@@ -310,6 +351,8 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     double* A3 = r ? W3 + nU : h->auxw[0];
     double* Uo = r ? r + RS : U_out;
     double* Ao = r ? r + RS + nU : aux_out;
+    // slabs: the CFL minimum over the ranks and the halo of the step's state
+    if (int rc = exchange(h, Un, an, (use_cfl ? JB_XCH_DT : 0) | JB_XCH_HALO, 3, st)) return rc;
     JB_TIMED(JB_KCAT_OTHER, o.step_begin(h->slots, use_cfl ? cfl : 0.0, dt_fixed, dt_hist, s, st), "step_begin");
     // stage 1: U1 = U + L(U)
     if (g.visc)
@@ -318,6 +361,7 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W1, nullptr, h->cand, A1, h->strips,
                     h->slots, 0, 1, h->fwork, st),
            "select1");
+    if (int rc = exchange(h, W1, A1, JB_XCH_HALO, 1, st)) return rc;
     // stage 2: U2 = 3/4 U + 1/4 (U1 + L(U1))
     if (g.visc)
       JB_TIMED(JB_KCAT_FLUX, o.visc(d, m, g, h->tr, W1, A1, h->strips, h->vbuf, h->vcell, st), "viscous");
@@ -327,6 +371,7 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W2, nullptr, h->cand, A2, h->strips,
                     h->slots, 1, 2, h->fwork, st),
            "select2");
+    if (int rc = exchange(h, W2, A2, JB_XCH_HALO, 2, st)) return rc;
     // stage 3: U3 = 1/3 U + 2/3 (U2 + L(U2))
     if (g.visc)
       JB_TIMED(JB_KCAT_FLUX, o.visc(d, m, g, h->tr, W2, A2, h->strips, h->vbuf, h->vcell, st), "viscous");
@@ -397,6 +442,7 @@ int jb_cfl_dt(jb_handle* h, const double* U, const double* aux, double cfl, doub
   JB_TRY(o.select(h->dim, false, false, true, h->mech, h->grid, U, aux, nullptr, nullptr, h->strips,
                   h->slots, -1, 3, nullptr, st),
          "cfl");
+  if (int rc = exchange(h, U, aux, JB_XCH_DT, 3, st)) return rc;
   JB_TRY(o.dt_from_slots(h->slots, cfl, dt_out, st), "dt");
   return JB_OK;
 }
@@ -571,6 +617,8 @@ static int adj_workspace(jb_handle* h) {
   if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
   if (h->grid.scheme != JB_FLUX_LF || h->grid.visc || h->grid.recon != JB_RECON_WENO5)
     return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint differentiates the inviscid LF / WENO5-JS path");
+  if (h->xch || h->grid.bc[0] == JB_BC_HALO || h->grid.bc[1] == JB_BC_HALO)
+    return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is single-domain (no x slabs)");
   for (int s = 0; s < 4; ++s)
     if (h->grid.bc[s] == JB_BC_PRESSURE_OUTLET || h->grid.bc[s] == JB_BC_RDC_INJECTOR)
       return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint supports periodic, slip, no-slip and zero-gradient sides");

@@ -205,8 +205,8 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
       T = auxk[nc + c];
     } else if (s.kind == 1) {
 #pragma unroll
-      for (int f = 0; f < 12; ++f) q[f] = strips[strip_idx(g, s.side, f, s.pos)];
-      T = strips[strip_idx(g, s.side, 13, s.pos)];
+      for (int f = 0; f < 12; ++f) q[f] = ghost(g, strips, s, f);
+      T = ghost(g, strips, s, 13);
     } else {
 #pragma unroll
       for (int f = 0; f < 12; ++f) q[f] = 1.0;
@@ -325,8 +325,8 @@ __global__ void __launch_bounds__(NT1) k_god1d(MP m, Grid g, const double* __res
       T = auxk[nc + c];
     } else if (s.kind == 1) {
 #pragma unroll
-      for (int f = 0; f < 11; ++f) q[f] = strips[strip_idx(g, s.side, f, s.pos)];
-      T = strips[strip_idx(g, s.side, 12, s.pos)];
+      for (int f = 0; f < 11; ++f) q[f] = ghost(g, strips, s, f);
+      T = ghost(g, strips, s, 12);
     } else {
 #pragma unroll
       for (int f = 0; f < 11; ++f) q[f] = 1.0;

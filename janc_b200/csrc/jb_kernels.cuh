@@ -536,8 +536,11 @@ __device__ __forceinline__ double weno_R(double fjm2, double fjm1, double fj, do
 // boundary/boundary_padding.py:4-45, boundary_conditions_{1D,2D}/*.py)
 // ---------------------------------------------------------------------------
 // kind: 0 interior copy of (xs, ys) with sign flips, 1 strip value, 2 unused
+// kind 1 reads a ghost strip (layer < 0: one state per boundary position,
+// shared by the 3 ghost layers) or, on a JB_BC_HALO side, the neighbour's
+// column `layer` (0..2, outward order of the padded array) in g.halo.
 struct Src {
-  int kind, xs, ys, side, pos, flip;
+  int kind, xs, ys, side, pos, flip, layer;
 };
 
 // One axis: coordinate c on an axis of length n, lo/hi side kinds.
@@ -569,7 +572,7 @@ __device__ __forceinline__ bool map_axis(int c, int n, int kind, bool lo, int& c
 template <int DIM>
 __device__ __forceinline__ Src map_cell(const Grid& g, int x, int y) {
   Src s;
-  s.kind = 2; s.xs = 0; s.ys = 0; s.side = 0; s.pos = 0; s.flip = 0;
+  s.kind = 2; s.xs = 0; s.ys = 0; s.side = 0; s.pos = 0; s.flip = 0; s.layer = -1;
   bool xin = x >= 0 && x < g.nx;
   bool yin = DIM == 1 ? true : (y >= 0 && y < g.ny);
   if (xin && yin) {
@@ -583,7 +586,11 @@ __device__ __forceinline__ Src map_cell(const Grid& g, int x, int y) {
     int cs, flip;
     bool strip;
     map_axis(x, g.nx, g.bc[side], lo, cs, flip, strip, 1, DIM);
-    if (strip) { s.kind = 1; s.side = side; s.pos = y; return s; }
+    if (strip) {
+      s.kind = 1; s.side = side; s.pos = y;
+      if (g.bc[side] == JB_BC_HALO) s.layer = lo ? x + 3 : x - g.nx;
+      return s;
+    }
     s.kind = 0; s.xs = cs; s.ys = y; s.flip = flip;
     return s;
   }
@@ -603,6 +610,16 @@ __device__ __forceinline__ Src map_cell(const Grid& g, int x, int y) {
 
 __device__ __forceinline__ size_t strip_idx(const Grid& g, int side, int q, int pos) {
   return ((size_t)side * (g.nv + 2) + q) * g.lstrip + pos;
+}
+
+// halo[2][nv+2][3][ny]: x side, field (U..., gamma, T), ghost layer, row
+__device__ __forceinline__ size_t halo_idx(const Grid& g, int side, int layer, int q, int y) {
+  return (((size_t)side * (g.nv + 2) + q) * 3 + layer) * g.ny + y;
+}
+
+// Field q (U..., gamma at nv, T at nv + 1) of a kind-1 ghost.
+__device__ __forceinline__ double ghost(const Grid& g, const double* strips, const Src& s, int q) {
+  return s.layer < 0 ? strips[strip_idx(g, s.side, q, s.pos)] : g.halo[halo_idx(g, s.side, s.layer, q, s.pos)];
 }
 
 // LF split flux F(f) of one cell in direction dir (0: x, 1: y) as the
@@ -826,8 +843,8 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       }
       sQ[nv * SM2_Q + i] = (R)auxk[nc + c];
     } else if (s.kind == 1) {
-      for (int q = 0; q < nv; ++q) sQ[q * SM2_Q + i] = (R)strips[strip_idx(g, s.side, q, s.pos)];
-      sQ[nv * SM2_Q + i] = (R)strips[strip_idx(g, s.side, nv + 1, s.pos)];
+      for (int q = 0; q < nv; ++q) sQ[q * SM2_Q + i] = (R)ghost(g, strips, s, q);
+      sQ[nv * SM2_Q + i] = (R)ghost(g, strips, s, nv + 1);
     } else {
       for (int q = 0; q < nq; ++q) sQ[q * SM2_Q + i] = (R)1.0;
     }
@@ -1026,9 +1043,9 @@ __device__ __forceinline__ void win_load(const MP& m, const Grid& g, const doubl
   } else if (s.kind == 1) {
     float qa[12];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) qa[i] = (float)strips[strip_idx(g, s.side, i, s.pos)];
+    for (int i = 0; i < 12; ++i) qa[i] = (float)ghost(g, strips, s, i);
     float rho, u, v;
-    flux_prims<2>(m, qa, (float)strips[strip_idx(g, s.side, 13, s.pos)], rho, u, v, p);
+    flux_prims<2>(m, qa, (float)ghost(g, strips, s, 13), rho, u, v, p);
     vel = DIR == 0 ? u : v;
 #pragma unroll
     for (int i = 0; i < NQ; ++i) q[i] = qa[DIR == 1 ? i : f];
@@ -1239,8 +1256,8 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
       }
       sQ[nv * PX1 + i] = (R)auxk[nc + s.xs];
     } else if (s.kind == 1) {
-      for (int q = 0; q < nv; ++q) sQ[q * PX1 + i] = (R)strips[strip_idx(g, s.side, q, 0)];
-      sQ[nv * PX1 + i] = (R)strips[strip_idx(g, s.side, nv + 1, 0)];
+      for (int q = 0; q < nv; ++q) sQ[q * PX1 + i] = (R)ghost(g, strips, s, q);
+      sQ[nv * PX1 + i] = (R)ghost(g, strips, s, nv + 1);
     } else {
       for (int q = 0; q < nq; ++q) sQ[q * PX1 + i] = (R)1.0;
     }
@@ -1908,6 +1925,67 @@ __global__ void k_step_begin(Slots* s, double cfl, double dt_fixed, double* dt_h
 
 __global__ void k_dt_from_slots(const Slots* s, double cfl, double* dt_out) {
   *dt_out = cfl * (s->dtnan ? __longlong_as_double(0x7ff8000000000000LL) : bitsd(s->dtmin_next));
+}
+
+// ---------------------------------------------------------------------------
+// x-slab decomposition (parallel/boundary_padding.py exchange_halo,
+// parallel/boundary.py, the pmin of CFL_1D / CFL_2D in set_simulator.py)
+// ---------------------------------------------------------------------------
+// The 3 edge columns of each x side of (U, aux) as send[2][nv+2][3][ny]:
+// side 0 holds columns 0..2 (the left neighbour's right halo), side 1 columns
+// nx-3..nx-1 (the right neighbour's left halo), in halo_idx order.
+__global__ void __launch_bounds__(256) k_halo_pack(Grid g, const double* __restrict__ U,
+                                                   const double* __restrict__ aux, double* __restrict__ send) {
+  const long long n = 6LL * (g.nv + 2) * g.ny;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int y = (int)(i % g.ny);
+  long long r = i / g.ny;
+  const int l = (int)(r % 3);
+  r /= 3;
+  const int q = (int)(r % (g.nv + 2));
+  const int side = (int)(r / (g.nv + 2));
+  const long long c = (long long)(side == 0 ? l : g.nx - 3 + l) * g.ny + y;
+  send[i] = q < g.nv ? U[q * g.ncell + c] : aux[(q - g.nv) * g.ncell + c];
+}
+
+// Wave speeds of the received ghost columns into the LF alpha maxima of slot
+// aidx (flux_splitting/LF.py takes nanmax over the padded array).  A halo
+// side contributes every row; a physical x side of a 2D slab only the rows
+// its padded corners copy (y-periodic wrap: 1..3 and ny-4..ny-2), because the
+// boundary condition overwrites the ghost columns' rows 3:-3 only.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_halo_alpha(MP m, Grid g, Slots* slots, int aidx) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  constexpr int nv = nY + NR;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double amx = 0.0, amy = 0.0;
+  if (t < 6 * g.ny) {
+    const int side = t / (3 * g.ny), l = (t / g.ny) % 3, y = t % g.ny;
+    const bool corner_row = (y >= 1 && y <= 3) || (y >= g.ny - 4 && y <= g.ny - 2);
+    if (g.bc[side] == JB_BC_HALO || (DIM == 2 && corner_row)) {
+      double q[nv + 2];
+#pragma unroll
+      for (int f = 0; f < nv + 2; ++f) q[f] = g.halo[halo_idx(g, side, l, f, y)];
+      Prim<DIM> pr = u_to_prim<DIM>(m, q, q[nv], q[nv + 1]);
+      amx = fabs(pr.u) + pr.a;
+      amy = fabs(pr.v) + pr.a;
+    }
+  }
+  block_reduce_store(amx, amy, 0.0, 0u, slots, aidx, true, false, -1);
+}
+
+// The CFL minimum and NaN flag as an int64 pair whose MIN over the ranks is
+// the global pair: red[0] the bits of the (non-negative) minimum, red[1]
+// minus the NaN flag.
+__global__ void k_dt_pack(const Slots* s, long long* red) {
+  red[0] = (long long)s->dtmin_next;
+  red[1] = -(long long)s->dtnan;
+}
+
+__global__ void k_dt_unpack(Slots* s, const long long* red) {
+  s->dtmin_next = (unsigned long long)red[0];
+  s->dtnan = red[1] != 0 ? 1u : 0u;
 }
 
 #include "jb_godunov.cuh"

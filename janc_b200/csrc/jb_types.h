@@ -45,7 +45,17 @@ enum jb_bc_kind {
   JB_BC_ZERO_GRADIENT = 2,
   JB_BC_NO_SLIP_WALL = 3,
   JB_BC_PRESSURE_OUTLET = 4,
-  JB_BC_RDC_INJECTOR = 5
+  JB_BC_RDC_INJECTOR = 5,
+  // x side of an x slab that borders another slab (parallel/boundary.py):
+  // its 3 ghost columns are the neighbour's 3 edge columns, exchanged into
+  // the handle's halo buffer before each flux evaluation
+  JB_BC_HALO = 6
+};
+
+// What jb_exchange_fn is asked to do (bit flags).
+enum jb_exchange_flags {
+  JB_XCH_DT = 1,   // all-reduce MIN over the ranks of the int64 pair red[0..1]
+  JB_XCH_HALO = 2  // send send[side] to the neighbour across side, receive halo[side]
 };
 
 // kernel categories reported by jb_kernel_times
@@ -105,6 +115,7 @@ typedef struct jb_grid {
   int scheme;            // advective flux (jb_flux_scheme): LF splitting or Godunov + Riemann solver
   int recon;             // face reconstruction (jb_reconstruction): WENO5-JS or MUSCL
   const double* visc;    // viscous rhs of the stage state (ncell x nv) or null: Euler fluxes
+  const double* halo;    // x-slab mode: ghost columns [2][nv+2][3][ny] from the neighbours, else null
 } jb_grid;
 
 // Per-step reduction results.  Doubles reduced with atomics are stored as

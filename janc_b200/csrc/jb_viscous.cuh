@@ -13,7 +13,11 @@
 #pragma once
 
 // The padded grid's entry (x, y): interior, side ghost (boundary conditions)
-// or corner (periodic wrap of both axes, boundary_padding.py pad_2D).
+// or corner (periodic wrap of both axes, boundary_padding.py pad_2D).  In
+// x-slab mode the x pad is the exchanged neighbour columns on both sides,
+// physical sides included (parallel/boundary_padding.py exchange_halo; the
+// boundary conditions overwrite only the rows 3:-3), so a corner is the
+// y-periodic wrap of a halo column.
 template <int DIM>
 __device__ __forceinline__ Src map_padded(const Grid& g, int x, int y) {
   if (DIM == 2 && (x < 0 || x >= g.nx) && (y < 0 || y >= g.ny)) {
@@ -24,6 +28,13 @@ __device__ __forceinline__ Src map_padded(const Grid& g, int x, int y) {
     s.side = 0;
     s.pos = 0;
     s.flip = 0;
+    s.layer = -1;
+    if (g.halo) {
+      s.kind = 1;
+      s.side = x < 0 ? 0 : 1;
+      s.layer = x < 0 ? x + 3 : x - g.nx;
+      s.pos = s.ys;
+    }
     return s;
   }
   return map_cell<DIM>(g, x, y);
@@ -53,8 +64,8 @@ __global__ void __launch_bounds__(256) k_visc_nodes(MP m, Grid g, const double* 
     T = auxk[nc + c];
   } else {
 #pragma unroll
-    for (int f = 0; f < nv; ++f) q[f] = strips[strip_idx(g, s.side, f, s.pos)];
-    T = strips[strip_idx(g, s.side, nv + 1, s.pos)];
+    for (int f = 0; f < nv; ++f) q[f] = ghost(g, strips, s, f);
+    T = ghost(g, strips, s, nv + 1);
   }
   const double rho = q[0];
   double Y8[NR], Yf[NS];

@@ -14,6 +14,7 @@ config = {
              "split_method": "LF", "viscosity": "off"},
     "detailed_chemistry": True,
     "transport": None,
+    "slab": None,  # janc_b200.slab.Slab of this rank in the is_parallel mode
 }
 _solvers = {}
 _mech_cache = {}
@@ -31,13 +32,15 @@ def solver_for(shape, dx=1.0, dy=1.0):
     from ..solver import Solver
     dim = 1 if len(shape) == 1 else 2
     bc = config["boundary"] or {}
+    slab = config["slab"]
     key = (dim, tuple(shape), repr(sorted(bc.items())) if bc else "", config["precision"],
-           config["mechanism"], repr(config["nondim"]), repr(config["flux"]), repr(config["transport"]))
+           config["mechanism"], repr(config["nondim"]), repr(config["flux"]), repr(config["transport"]),
+           None if slab is None else (slab.rank, slab.size, id(slab.group)))
     s = _solvers.get(key)
     if s is None:
         s = Solver(dim, shape[0], shape[1] if dim == 2 else None, dx, dy if dim == 2 else None,
                    bc, mechanism(), precision=config["precision"], flux_config=config["flux"],
-                   transport_config=config["transport"])
+                   transport_config=config["transport"], slab=slab)
         _solvers[key] = s
     s._spacing(dx, dy if dim == 2 else None)
     return s

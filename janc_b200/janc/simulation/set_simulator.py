@@ -14,9 +14,17 @@ from .time_step import time_step_dict
 
 
 def set_rhs(dim, reaction_config, source_config=None, is_parallel=False, is_amr=False):
-    """(flux_func, update_func, source_func) as set_simulator.py:20-71."""
-    if is_parallel or is_amr:
-        raise NotImplementedError("multi-device slabs and AMR are not part of this build")
+    """(flux_func, update_func, source_func) as set_simulator.py:20-71.
+    ``is_parallel``: the arrays are this rank's x slab (one process per GPU
+    in an initialised torch.distributed group); ghost columns come from the
+    neighbouring slabs (parallel/boundary.py)."""
+    if is_amr:
+        raise NotImplementedError("AMR is not part of this build")
+    if is_parallel and _state.config["slab"] is None:
+        from ...slab import Slab
+        _state.config["slab"] = Slab()
+    elif not is_parallel:
+        _state.config["slab"] = None
     if source_config is not None:
         raise NotImplementedError("user source terms are outside the detailed-chemistry path")
 
@@ -58,7 +66,9 @@ class Simulator:
     """Simulator(simulation_config) with advance_func(U, aux, t, theta) ->
     (U, aux, t + dt, dt) and run(U_init, aux_init) (set_simulator.py:320-494).
     Snapshot output (H5Saver) is not part of this build; run() returns the
-    final state."""
+    final state.  ``computation_config['is_parallel']`` decomposes x into one
+    slab per rank of the initialised torch.distributed group (one process per
+    GPU); advance_func then takes and returns this rank's slab."""
 
     def __init__(self, simulation_config):
         dim = simulation_config["dimension"]
@@ -72,9 +82,9 @@ class Simulator:
         self.t_end = time_control["t_end"]
         self.theta = simulation_config.get("solver_parameters", None)
         comp = simulation_config.get("computation_config", {})
-        if comp.get("is_parallel", False):
-            raise NotImplementedError("multi-device slabs are not part of this build (replicas only)")
+        self.is_parallel = bool(comp.get("is_parallel", False))
         _state.reset_solvers()
+        _state.config["slab"] = None
         _state.config["precision"] = simulation_config.get("precision", "fp64")
         thermo_model.set_thermo(thermo_config, nondim_config, dim)
         reaction_model.set_reaction(reaction_config, nondim_config, dim)
@@ -86,7 +96,8 @@ class Simulator:
         self.dim = dim
         self.dx = grid_config["dx"]
         self.dy = grid_config.get("dy") if dim == "2D" else None
-        self.flux_func, self.update_func, _ = set_rhs(dim, reaction_config)
+        self.flux_func, self.update_func, _ = set_rhs(dim, reaction_config, None, self.is_parallel)
+        self.slab = _state.config["slab"]
         self._advance_body = set_advance_func(dim, flux_config, reaction_config, time_control, False,
                                               self.flux_func, self.update_func, None)
         self.dt = time_control.get("dt", None)
@@ -109,7 +120,14 @@ class Simulator:
         return _state.back(U1, kind), _state.back(aux1, kind), t + dt, dt
 
     def run(self, U_init, aux_init):
+        """Advance to t_end.  In the is_parallel mode the global initial
+        arrays are split into this rank's x slab first and the slab is
+        returned (the reference returns its device-sharded arrays)."""
         U, aux, t = U_init, aux_init, 0.0
+        if self.is_parallel:
+            from ...slab import split_and_distribute_grid
+            U = split_and_distribute_grid(U, self.slab)
+            aux = split_and_distribute_grid(aux, self.slab)
         while t < self.t_end:
             U, aux, t, dt = self.advance_func(U, aux, t, self.theta)
             t = float(t)

@@ -113,11 +113,17 @@ class Solver:
     ``transport_config`` (the reference's transport_config: Sutherland or
     constant viscosity, Prandtl-number or constant conductivity, Lewis /
     Schmidt-number or constant diffusivity).
+
+    ``slab`` (a ``janc_b200.slab.Slab``) makes this solver one x slab of a
+    grid decomposed over the ranks of a process group (the reference's
+    ``is_parallel`` mode): ``nx`` is the slab's column count, the
+    ``boundary_config`` is the global domain's, and every flux evaluation
+    exchanges 3 ghost columns with the neighbouring slabs.
     """
 
     def __init__(self, dim, nx, ny=None, dx=1.0, dy=None, boundary_config=None,
                  mechanism=_mech.DEFAULT_MECHANISM, nondim_config=None, precision="fp64",
-                 device=None, flux_config=None, transport_config=None):
+                 device=None, flux_config=None, transport_config=None, slab=None):
         if dim in ("1D", 1):
             dim = 1
         elif dim in ("2D", 2):
@@ -147,6 +153,9 @@ class Solver:
                 raise KeyError(f"{key}: unknown boundary condition {name!r}")
             kinds.append(_native.BC_KIND[name])
         kinds += [0] * (4 - len(kinds))
+        self.slab = slab
+        if slab is not None:
+            kinds = slab.boundary_kinds(kinds)
         self.boundary_kinds = kinds
         self._theta_key = None
         self._theta_keep = None
@@ -159,6 +168,11 @@ class Solver:
         _native.check(rc, None, "jb_create")
         self._h = h
         self._lib = L
+        self._exchange = None
+        if slab is not None:
+            from .slab import SlabExchange
+            self._exchange = SlabExchange(slab, self.nv, self.ny, self.device)
+            self._exchange.attach(L, h)
         self.flux_scheme = flux_scheme(flux_config)
         _native.check(L.jb_set_flux_scheme(h, _native.FLUX_SCHEME[self.flux_scheme]), h, "jb_set_flux_scheme")
         self.reconstruction = (flux_config or {}).get("interface_reconstruction", "WENO5_JS")
@@ -201,6 +215,13 @@ class Solver:
             if not t.is_contiguous():
                 raise ValueError(f"{name} must be contiguous")
 
+    def _check(self, rc, what):
+        """Raise for a failed call; a failed slab exchange raises its own error."""
+        if rc != 0 and self._exchange is not None and self._exchange.error is not None:
+            err, self._exchange.error = self._exchange.error, None
+            raise _native.JancError(f"{what}: slab exchange failed: {err!r}") from err
+        _native.check(rc, self._h, what)
+
     def _spacing(self, dx, dy):
         dx = self.dx if dx is None else float(dx)
         dy = self.dy if (dy is None or self.dim == 1) else float(dy)
@@ -224,6 +245,9 @@ class Solver:
                                 dtype=torch.float64)
             if y.ndim == 1:
                 y = y[:, None].expand(y.shape[0], self.nx)
+            y = y.reshape(y.shape[0], -1)
+            if self.slab is not None and y.shape[1] == self.nx * self.slab.size:
+                y = y[:, self.slab.rank * self.nx:(self.slab.rank + 1) * self.nx]  # PartitionDict along x
             y = y.reshape(y.shape[0], self.nx).contiguous().to(self.device)
             self._theta_keep = y
             yptr = _ptr(y)
@@ -262,8 +286,8 @@ class Solver:
         self._spacing(dx, dy)
         self.set_theta(theta)
         out = torch.empty_like(U)
-        _native.check(self._lib.jb_flux_func(self._h, _ptr(U), _ptr(aux), float(dt), _ptr(out), _stream()),
-                      self._h, "jb_flux_func")
+        self._check(self._lib.jb_flux_func(self._h, _ptr(U), _ptr(aux), float(dt), _ptr(out), _stream()),
+                    "jb_flux_func")
         return out
 
     def update_aux(self, U, aux):
@@ -296,7 +320,7 @@ class Solver:
             dt_hist = torch.empty(nsteps, dtype=torch.float64, device=U.device)
         rc = self._lib.jb_advance(self._h, _ptr(U), _ptr(aux), _ptr(U_out), _ptr(aux_out),
                                   float(dt or 0.0), float(cfl or 0.0), int(nsteps), _ptr(dt_hist), _stream())
-        _native.check(rc, self._h, "jb_advance")
+        self._check(rc, "jb_advance")
         return U_out, aux_out, dt_hist
 
     def advance_one_step(self, U, aux, dx=None, dy=None, dt=None, theta=None):
@@ -313,8 +337,8 @@ class Solver:
         self.set_theta(theta)
         U_out = torch.empty_like(U)
         aux_out = torch.empty_like(aux)
-        _native.check(self._lib.jb_rk3(self._h, _ptr(U), _ptr(aux), _ptr(U_out), _ptr(aux_out), float(dt),
-                                       _stream()), self._h, "jb_rk3")
+        self._check(self._lib.jb_rk3(self._h, _ptr(U), _ptr(aux), _ptr(U_out), _ptr(aux_out), float(dt),
+                                     _stream()), "jb_rk3")
         return U_out, aux_out
 
     def u_to_prim(self, U, aux):
@@ -332,8 +356,8 @@ class Solver:
     def cfl_dt(self, U, aux, cfl):
         self._check_state(U, aux)
         out = torch.empty((), dtype=torch.float64, device=U.device)
-        _native.check(self._lib.jb_cfl_dt(self._h, _ptr(U), _ptr(aux), float(cfl), _ptr(out), _stream()),
-                      self._h, "jb_cfl_dt")
+        self._check(self._lib.jb_cfl_dt(self._h, _ptr(U), _ptr(aux), float(cfl), _ptr(out), _stream()),
+                    "jb_cfl_dt")
         return out
 
     def get_thermo(self, T, Y):

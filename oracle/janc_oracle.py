@@ -581,6 +581,36 @@ def boundary_conditions(m, U, aux, bc, theta=None):
     sides = (("L", "left_boundary"), ("R", "right_boundary"))
     if two_d:
         sides += (("B", "bottom_boundary"), ("T", "top_boundary"))
+    return _apply_sides(m, Up, Ap, bc, theta, sides)
+
+
+def parallel_boundary_conditions(m, Us, auxs, r, bc, theta=None):
+    """Slab r of the reference's parallel mode (parallel/boundary.py:6-25 with
+    parallel/boundary_padding.py:6-27): the x pad is a ring exchange of 3
+    columns with the neighbouring slabs (exchange_halo, cell-periodic across
+    the domain's ends), the y pad the node-periodic one; then the left
+    condition on slab 0 only, the right on the last slab only, bottom and top
+    on every slab."""
+    P = len(Us)
+    f = [np.concatenate([U, a], axis=0) for U, a in zip(Us, auxs)]
+    fx = np.concatenate([f[(r - 1) % P][:, -3:], f[r], f[(r + 1) % P][:, :3]], axis=1)
+    two_d = Us[r].ndim == 3
+    if two_d:
+        fx = np.concatenate([fx[:, :, -4:-3], fx[:, :, -3:-2], fx[:, :, -2:-1], fx,
+                             fx[:, :, 1:2], fx[:, :, 2:3], fx[:, :, 3:4]], axis=2)
+    Up, Ap = fx[:-2].copy(), fx[-2:].copy()
+    sides = ()
+    if r == 0:
+        sides += (("L", "left_boundary"),)
+    if r == P - 1:
+        sides += (("R", "right_boundary"),)
+    if two_d:
+        sides += (("B", "bottom_boundary"), ("T", "top_boundary"))
+    return _apply_sides(m, Up, Ap, bc, theta, sides)
+
+
+def _apply_sides(m, Up, Ap, bc, theta, sides):
+    two_d = Up.ndim == 3
     for s, key in sides:
         kind = bc[key]
         if kind == "periodic":
@@ -1059,6 +1089,10 @@ class Solver:
 
     def flux_func(self, U, aux, dx, dy, dt, theta=None):
         Up, Ap = boundary_conditions(self.m, U, aux, self.bc, theta)
+        return self.padded_rhs(Up, Ap, dx, dy, dt)
+
+    def padded_rhs(self, Up, Ap, dx, dy, dt):
+        """dt * total_flux of ghost-padded arrays (set_simulator.py:26-47)."""
         if self.solver_type == "godunov":
             adv = godunov_flux(self.m, Up, Ap, dx, dy, self.riemann, self.recon)
         else:
@@ -1107,6 +1141,52 @@ class Solver:
         dt = self.cfl_dt(U, aux)
         U, aux = self.advance_one_step(U, aux, self.dx, self.dy, dt, theta)
         return U, aux, t + dt, dt
+
+
+class SlabSolver:
+    """The reference's parallel mode (``computation_config['is_parallel']``,
+    set_simulator.py:20-47, 410-455, parallel/*.py) for P x slabs advanced in
+    lockstep: lists of per-slab arrays in and out.  Each flux evaluation pads
+    slab r from its neighbours (parallel_boundary_conditions); the LF wave
+    speed and the temperature solve's stopping test are per slab (the pmapped
+    body reduces over its own slab); the CFL dt is the minimum over the slabs
+    (jax.lax.pmin).  ``thetas`` holds one theta per slab (PartitionDict)."""
+
+    def __init__(self, mech, dim, dx, dy=None, bc=None, cfl=None, flux_config=None, transport_config=None):
+        self.s = Solver(mech, dim, dx, dy, bc, cfl, flux_config, transport_config)
+        self.m, self.bc = mech, bc
+
+    def flux_func(self, Us, auxs, dx, dy, dt, thetas=None):
+        thetas = thetas or [None] * len(Us)
+        out = []
+        for r in range(len(Us)):
+            Up, Ap = parallel_boundary_conditions(self.m, Us, auxs, r, self.bc, thetas[r])
+            out.append(self.s.padded_rhs(Up, Ap, dx, dy, dt))
+        return out
+
+    def rk3(self, Us, auxs, dx, dy, dt, thetas=None):
+        """TVD_RK3.py:5-12 on every slab, one exchange per stage."""
+        upd = self.s.update_func
+        F = self.flux_func(Us, auxs, dx, dy, dt, thetas)
+        U1 = [U + f for U, f in zip(Us, F)]
+        A1 = [upd(U, a) for U, a in zip(U1, auxs)]
+        F = self.flux_func(U1, A1, dx, dy, dt, thetas)
+        U2 = [3 / 4 * U + 1 / 4 * (u1 + f) for U, u1, f in zip(Us, U1, F)]
+        A2 = [upd(U, a) for U, a in zip(U2, A1)]
+        F = self.flux_func(U2, A2, dx, dy, dt, thetas)
+        U3 = [1 / 3 * U + 2 / 3 * (u2 + f) for U, u2, f in zip(Us, U2, F)]
+        A3 = [upd(U, a) for U, a in zip(U3, A2)]
+        return U3, A3
+
+    def cfl_dt(self, Us, auxs):
+        return np.min(np.array([self.s.cfl_dt(U, a) for U, a in zip(Us, auxs)]))
+
+    def advance_func(self, Us, auxs, t, thetas=None):
+        dt = self.cfl_dt(Us, auxs)
+        Us, auxs = self.rk3(Us, auxs, self.s.dx, self.s.dy, dt, thetas)
+        Us = [U + reaction_source_terms(self.m, U, a, dt) for U, a in zip(Us, auxs)]
+        auxs = [self.s.update_func(U, a) for U, a in zip(Us, auxs)]
+        return Us, auxs, t + dt, dt
 
 
 # --------------------------------------------------------------------------
