@@ -62,13 +62,173 @@ def set_advance_func(dim, flux_config, reaction_config, time_control, is_amr, fl
     return advance_one_step
 
 
+def _h5_module():
+    """h5py when importable, else the built-in HDF5 subset (janc_b200.h5lite)."""
+    try:
+        import h5py
+        return h5py
+    except ImportError:
+        from ... import h5lite
+        return h5lite
+
+
+class H5Saver:
+    """Snapshot file in the reference's layout (set_simulator.py:126-318):
+    one group ``save_step{k}`` per snapshot with attributes ``time`` and
+    ``step`` and a dataset per saved array (``u``: the conserved state,
+    gzip-compressed).  ``parallel_save`` writes ``save_step{k}_device{d}``
+    groups, one per x slab, and ``collect`` concatenates them into
+    ``save_step{k}``.  Fixed from the reference: ``collect`` has its
+    defaultdict, ``get_prim`` uses the 2D aux functions, ``parallel_save``
+    gathers the slabs to rank 0, the only process that opens the file (no
+    I/O inside a mapped function), and a saved ``aux`` (the temperature and
+    gamma of the state) is used by ``load`` instead of the reference's
+    gamma = 1.4, T = 500 K initial guesses."""
+
+    def __init__(self, filepath, data_dim, slab=None, mode="a"):
+        from pathlib import Path
+        self.filepath = Path(filepath)
+        self.dim = data_dim
+        self.slab = slab
+        self._h5 = _h5_module()
+        self.file = self._h5.File(self.filepath, mode) if (self._writer or mode == "r") else None
+
+    @property
+    def _writer(self):
+        return self.slab is None or self.slab.rank == 0
+
+    def get_prim(self, U, aux):
+        """(density, x-velocity[, y-velocity], pressure, tempreature,
+        species) of a state, as the reference names them."""
+        if self.dim == "1D":
+            aux = aux_func_1D.update_aux(U, aux)
+            rho, u, Y, p, a = aux_func_1D.U_to_prim(U, aux)
+            return {"density": rho[0], "x-velocity": u[0], "pressure": p[0], "tempreature": aux[1], "species": Y}
+        aux = aux_func.update_aux(U, aux)
+        rho, u, v, Y, p, a = aux_func.U_to_prim(U, aux)
+        return {"density": rho[0], "x-velocity": u[0], "y-velocity": v[0], "pressure": p[0],
+                "tempreature": aux[1], "species": Y}
+
+    @staticmethod
+    def _host(a):
+        import numpy as np
+        if hasattr(a, "detach"):
+            a = a.detach().cpu().numpy()
+        return np.asarray(a)
+
+    def _write(self, key, t, step, arrays):
+        import numpy as np
+        if key in self.file:
+            del self.file[key]
+        grp = self.file.create_group(key)
+        grp.attrs["time"] = np.float64(float(t))
+        grp.attrs["step"] = np.int64(int(step))
+        for name, arr in arrays.items():
+            grp.create_dataset(name, data=self._host(arr), compression="gzip")
+        self.file.flush()
+
+    def save(self, save_step, t, step, **arrays):
+        """One snapshot group ``save_step{save_step}`` (replaced if present)."""
+        if self._writer:
+            self._write(f"save_step{save_step}", t, step, arrays)
+
+    def parallel_save(self, save_step, t, step, **arrays):
+        """Each rank's slab as ``save_step{k}_device{rank}``, written by rank 0
+        (every rank must call it)."""
+        if self.slab is None:
+            self._write(f"save_step{save_step}_device0", t, step, arrays)
+            return
+        from ...slab import gather_grid
+        import torch
+        full = {n: gather_grid(torch.as_tensor(a).to(dtype=torch.float64).contiguous(), self.slab)
+                for n, a in arrays.items()}
+        if not self._writer:
+            return
+        for d in range(self.slab.size):
+            part = {n: torch.chunk(a, self.slab.size, dim=1)[d] for n, a in full.items()}
+            self._write(f"save_step{save_step}_device{d}", t, step, part)
+
+    def list_snapshots(self):
+        return list(self.file.keys())
+
+    def collect(self, concat_axis=1):
+        """Concatenate the ``_device{d}`` groups of every snapshot into
+        ``save_step{k}`` (attributes from the last device)."""
+        import numpy as np
+        from collections import defaultdict
+        groups = defaultdict(list)
+        for g in list(self.file.keys()):
+            if g.startswith("save_step") and "_device" in g:
+                groups[g.split("_device")[0]].append(g)
+        for step, names in groups.items():
+            names.sort(key=lambda x: int(x.split("_device")[-1]))
+            data, attrs = {}, {}
+            for g in names:
+                grp = self.file[g]
+                attrs = dict(grp.attrs)
+                for k in grp.keys():
+                    data.setdefault(k, []).append(np.asarray(grp[k]))
+            if step in self.file:
+                del self.file[step]
+            new = self.file.create_group(step)
+            for k, v in attrs.items():
+                new.attrs[k] = v
+            for k, parts in data.items():
+                new.create_dataset(k, data=np.concatenate(parts, axis=concat_axis), compression="gzip")
+        self.file.flush()
+
+    def _state_of(self, grp):
+        import numpy as np
+        U = np.asarray(grp["u"])
+        if "aux" in grp:
+            aux = np.asarray(grp["aux"])
+        else:  # the reference's initial guesses for the temperature solve
+            aux = np.concatenate([np.full_like(U[0:1], 1.4), np.full_like(U[0:1], 500.0)], axis=0)
+        return U, aux
+
+    def load(self, key):
+        """(time, primitive dict) of snapshot ``key``."""
+        grp = self.file[key]
+        U, aux = self._state_of(grp)
+        return grp.attrs["time"], self.get_prim(U, aux)
+
+    def load_state(self, key=None):
+        """(U, aux, time, step) of snapshot ``key`` (default: the latest
+        ``save_step{k}``) for a restart."""
+        if key is None:
+            keys = [k for k in self.file.keys() if k.startswith("save_step") and "_device" not in k]
+            key = max(keys, key=lambda k: int(k[len("save_step"):]))
+        grp = self.file[key]
+        U, aux = self._state_of(grp)
+        return U, aux, float(grp.attrs["time"]), int(grp.attrs["step"])
+
+    def load_all(self):
+        """(times, primitive dict with a leading snapshot axis) over all
+        snapshots in step order."""
+        import numpy as np
+        keys = sorted(self.file.keys(), key=lambda s: int("".join(ch for ch in s if ch.isdigit())))
+        times, prims = [], []
+        for k in keys:
+            t, q = self.load(k)
+            times.append(t)
+            prims.append({n: self._host(v) for n, v in q.items()})
+        return np.stack(times), {n: np.stack([q[n] for q in prims]) for n in prims[0]}
+
+    def close(self):
+        if self.file is not None:
+            self.file.close()
+            self.file = None
+
+
 class Simulator:
     """Simulator(simulation_config) with advance_func(U, aux, t, theta) ->
     (U, aux, t + dt, dt) and run(U_init, aux_init) (set_simulator.py:320-494).
-    Snapshot output (H5Saver) is not part of this build; run() returns the
-    final state.  ``computation_config['is_parallel']`` decomposes x into one
-    slab per rank of the initialised torch.distributed group (one process per
-    GPU); advance_func then takes and returns this rank's slab."""
+    ``computation_config['output_settings']`` (``save_dt``, ``results_path``)
+    sets the snapshots run() writes with H5Saver (default: the initial and
+    final states in results.h5); the file is opened when run() starts.
+    ``computation_config['is_parallel']`` decomposes x into one slab per rank
+    of the initialised torch.distributed group (one process per GPU);
+    advance_func then takes and returns this rank's slab."""
 
     def __init__(self, simulation_config):
         dim = simulation_config["dimension"]
@@ -83,6 +243,9 @@ class Simulator:
         self.theta = simulation_config.get("solver_parameters", None)
         comp = simulation_config.get("computation_config", {})
         self.is_parallel = bool(comp.get("is_parallel", False))
+        out = comp.get("output_settings", {})
+        self.save_dt = out.get("save_dt", self.t_end)
+        self.results_path = out.get("results_path", "results.h5")
         _state.reset_solvers()
         _state.config["slab"] = None
         _state.config["precision"] = simulation_config.get("precision", "fp64")
@@ -119,16 +282,58 @@ class Simulator:
             dt = float(dt)
         return _state.back(U1, kind), _state.back(aux1, kind), t + dt, dt
 
-    def run(self, U_init, aux_init):
-        """Advance to t_end.  In the is_parallel mode the global initial
-        arrays are split into this rank's x slab first and the slab is
-        returned (the reference returns its device-sharded arrays)."""
-        U, aux, t = U_init, aux_init, 0.0
+    def run(self, U_init, aux_init, t0=0.0, step0=0, save=True):
+        """Advance to t_end, writing a snapshot (u and aux) at the start and
+        whenever t passes the next multiple of save_dt (set_simulator.py:
+        457-494).  ``t0``/``step0`` restart from a saved state (the reference
+        always starts at t = 0; see ``restart``).  In the is_parallel mode the
+        global initial arrays are split into this rank's x slab first, the
+        snapshots hold one group per slab, and the slab is returned (the
+        reference returns its device-sharded arrays)."""
+        U, aux, t, step = U_init, aux_init, float(t0), int(step0)
         if self.is_parallel:
             from ...slab import split_and_distribute_grid
             U = split_and_distribute_grid(U, self.slab)
             aux = split_and_distribute_grid(aux, self.slab)
-        while t < self.t_end:
-            U, aux, t, dt = self.advance_func(U, aux, t, self.theta)
-            t = float(t)
+        saver = H5Saver(self.results_path, self.dim, self.slab) if save else None
+        put = (lambda *a, **k: None) if saver is None else (saver.parallel_save if self.is_parallel else saver.save)
+        save_step = 0
+        if step == 0:
+            put(0, t, step, u=U, aux=aux)
+            save_step = 1
+        else:
+            save_step = 1 + int(t // self.save_dt)
+        next_save = save_step * self.save_dt if step else self.save_dt
+        try:
+            while t < self.t_end:
+                U, aux, t, dt = self.advance_func(U, aux, t, self.theta)
+                t = float(t)
+                step += 1
+                if t >= next_save or t >= self.t_end:
+                    put(save_step, t, step, u=U, aux=aux)
+                    next_save += self.save_dt
+                    save_step += 1
+        finally:
+            if saver is not None:
+                saver.close()
         return U, aux, t
+
+    def restart(self, key=None):
+        """(U, aux, t, step) of a snapshot in results_path (default: the
+        latest) for ``run(U, aux, t0=t, step0=step)``; a parallel file is
+        collected first."""
+        if self.slab is None or self.slab.rank == 0:
+            saver = H5Saver(self.results_path, self.dim)
+            try:
+                if any("_device" in k for k in saver.list_snapshots()):
+                    saver.collect()
+            finally:
+                saver.close()
+        if self.slab is not None:
+            import torch.distributed as dist
+            dist.barrier(group=self.slab.group)
+        saver = H5Saver(self.results_path, self.dim, mode="r")
+        try:
+            return saver.load_state(key)
+        finally:
+            saver.close()
