@@ -107,9 +107,12 @@ int jb_set_spacing(jb_handle* h, double dx, double dy);
  * (the default), JB_FLUX_HLLC / JB_FLUX_AUSMPW = godunov_flux
  * (solver_2D/flux.py:43-54) with WENO5-JS on the primitives and the HLLC
  * (riemann_solver/HLLC.py) or AUSMPW+ (riemann_solver/AUSMPW_plus.py)
- * Riemann solver.  The mixed variant reconstructs the primitives in float32;
- * the Riemann solver, RK and temperature solve are float64 in every variant.
- * jb_adjoint_step supports JB_FLUX_LF only. */
+ * Riemann solver, JB_FLUX_SW = flux splitting with Steger-Warming
+ * (flux_splitting/SW.py; the 1D form with the Jacobian and metric of 1, which
+ * the reference's 1D flux_splitting cannot call: its split_flux takes a third
+ * `metrics` argument it is not given).  The mixed variant reconstructs in
+ * float32; the Riemann solver, RK and temperature solve are float64 in every
+ * variant.  jb_adjoint_step supports JB_FLUX_LF only. */
 int jb_set_flux_scheme(jb_handle* h, int scheme);
 
 /* Select the face reconstruction of both flux paths (the

@@ -17,7 +17,7 @@ BC_HALO = 6  # x side bordering another slab (jb_set_exchange)
 XCH_DT, XCH_HALO = 1, 2  # jb_exchange_flags
 EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p)
 PRECISION = {"fp64_strict": 0, "fp64": 1, "mixed": 2}
-FLUX_SCHEME = {"LF": 0, "HLLC": 1, "AUSMPW_plus": 2}  # split method / Riemann solver
+FLUX_SCHEME = {"LF": 0, "HLLC": 1, "AUSMPW_plus": 2, "SW": 3}  # split method / Riemann solver
 RECONSTRUCTION = {"WENO5_JS": 0, "MUSCL": 1}
 STATUS = {1: "bad argument", 2: "CUDA error", 4: "non-finite state", 8: "singular chemistry matrix",
           16: "device wait timed out", 32: "unsupported configuration"}

@@ -532,7 +532,7 @@ int jb_set_transport(jb_handle* h, const jb_transport* tr) {
 
 int jb_set_flux_scheme(jb_handle* h, int scheme) {
   if (!h) return JB_ERR_ARG;
-  if (scheme != JB_FLUX_LF && scheme != JB_FLUX_HLLC && scheme != JB_FLUX_AUSMPW)
+  if (scheme != JB_FLUX_LF && scheme != JB_FLUX_HLLC && scheme != JB_FLUX_AUSMPW && scheme != JB_FLUX_SW)
     return set_err(h, JB_ERR_ARG, "unknown flux scheme");
   h->grid.scheme = scheme;
   return JB_OK;

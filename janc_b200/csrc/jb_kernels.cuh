@@ -646,6 +646,49 @@ __device__ __forceinline__ double lf_flux(int f, int dir, double q, double rho, 
 #endif
 }
 
+// Steger-Warming split fluxes of field f in direction dir (0: x, 1: y)
+// (flux_splitting/SW.py): H+- = sum over the eigenvalue groups theta - a,
+// theta, theta + a of lambda+- H_k, lambda+- = (lambda +- sqrt(lambda^2 +
+// eps^2)) / 2 with eps = 1e-6, H_1,4 = (rho, rho u -+ rho a n, E + p -+ rho a
+// theta, rho Y) / (2 gamma), H_2 = (gamma - 1) / gamma (rho, rho u,
+// rho |u|^2 / 2, rho Y); expressions in the reference's order.
+template <int DIM, class R>
+__device__ __forceinline__ void sw_split(int f, int dir, R qf, R rho, R u, R v, R p, R E, R a, R gamma,
+                                         R& hp, R& hm) {
+  constexpr int nE = DIM == 1 ? 2 : 3;
+  const R theta = dir == 0 ? u : v;
+  const R ra = rho * a;
+  R x1, x2, x4;
+  if (f == 0) {
+    x1 = x2 = x4 = rho;
+  } else if (f == 1 || (DIM == 2 && f == 2)) {
+    const R m = f == 1 ? rho * u : rho * v;
+    const bool normal = (f == 1) == (dir == 0);
+    x1 = normal ? m - ra : m;
+    x2 = m;
+    x4 = normal ? m + ra : m;
+  } else if (f == nE) {
+    x1 = (E + p) - ra * theta;
+    x2 = DIM == 1 ? (R)0.5 * rho * (u * u) : (R)0.5 * rho * (u * u + v * v);
+    x4 = (E + p) + ra * theta;
+  } else {
+#if JB_FAST
+    x1 = x2 = x4 = qf;
+#else
+    x1 = x2 = x4 = rho * (qf / rho);
+#endif
+  }
+  const R c1 = (R)1 / ((R)2 * gamma), c2 = (gamma - (R)1) / gamma;
+  const R h1 = c1 * x1, h2 = c2 * x2, h4 = c1 * x4;
+  const R l1 = theta - a, l2 = theta, l4 = theta + a;
+  const R e2 = (R)(1e-6 * 1e-6);
+  const R s1 = sqrt(l1 * l1 + e2), s2 = sqrt(l2 * l2 + e2), s4 = sqrt(l4 * l4 + e2);
+  const R lp1 = (R)0.5 * (l1 + s1), lp2 = (R)0.5 * (l2 + s2), lp4 = (R)0.5 * (l4 + s4);
+  const R lm1 = (R)0.5 * (l1 - s1), lm2 = (R)0.5 * (l2 - s2), lm4 = (R)0.5 * (l4 - s4);
+  hp = lp1 * h1 + lp2 * h2 + lp4 * h4;
+  hm = lm1 * h1 + lm2 * h2 + lm4 * h4;
+}
+
 #if JB_FAST
 // ---------------------------------------------------------------------------
 // float32 flux arithmetic of the mixed-precision variant
@@ -797,6 +840,11 @@ constexpr int SM2_HX = PX2 * TY2, SM2_HY = TX2 * PY2;
 constexpr int SM2_FX = (TX2 + 1) * TY2, SM2_FY = TX2 * (TY2 + 1);
 
 template <class R>
+__host__ __device__ constexpr size_t sw_smem2d_bytes() {
+  return sizeof(R) * 2 * SM2_Q;
+}
+
+template <class R>
 __host__ __device__ constexpr size_t smem2d_bytes(int nq) {
   return sizeof(R) * ((size_t)nq * SM2_Q + 4 * SM2_Q + 2 * SM2_HX + 2 * SM2_HY + SM2_FX + SM2_FY);
 }
@@ -804,7 +852,7 @@ __host__ __device__ constexpr size_t smem2d_bytes(int nq) {
 // R is the arithmetic type of the flux (LF split, WENO, primitives): double
 // for the float64 variants, float for the mixed variant.  The RK combination
 // and the Halley iterates are float64 in every variant.
-template <int STAGE, class R, bool VISC>
+template <int STAGE, class R, bool VISC, bool SW = false>
 __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk,
                                                  const double* __restrict__ Un,
@@ -822,6 +870,10 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
   R* sHym = sHyp + SM2_HY;
   R* sFx = sHym + SM2_HY;                // [TX2+1][TY2]
   R* sFy = sFx + SM2_FX;                 // [TX2][TY2+1]
+  // Steger-Warming only (launched with sw_smem2d more bytes): gamma, a
+  R* sG = sFy + SM2_FY;                  // [PX2][PY2]
+  R* sA = sG + SM2_Q;
+  constexpr bool sw = SW;
 
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * TX2, y0 = blockIdx.y * TY2;
@@ -842,11 +894,14 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
         sQ[q * SM2_Q + i] = (R)(((s.flip >> q) & 1) ? -v : v);
       }
       sQ[nv * SM2_Q + i] = (R)auxk[nc + c];
+      if (sw) sG[i] = (R)auxk[c];
     } else if (s.kind == 1) {
       for (int q = 0; q < nv; ++q) sQ[q * SM2_Q + i] = (R)ghost(g, strips, s, q);
       sQ[nv * SM2_Q + i] = (R)ghost(g, strips, s, nv + 1);
+      if (sw) sG[i] = (R)ghost(g, strips, s, nv);
     } else {
       for (int q = 0; q < nq; ++q) sQ[q * SM2_Q + i] = (R)1.0;
+      if (sw) sG[i] = (R)1.0;
     }
   }
   __syncthreads();
@@ -861,6 +916,7 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
     sP[SM2_Q + i] = u;
     sP[2 * SM2_Q + i] = v;
     sP[3 * SM2_Q + i] = p;
+    if (sw) sA[i] = sqrt(sG[i] * p / rho);
   }
   __syncthreads();
 
@@ -901,7 +957,10 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       if (f == (xdir ? 1 : 2)) F += sP[3 * SM2_Q + c];
       if (f == 3) F += vel * sP[3 * SM2_Q + c];
       const R al = xdir ? ax : ay;
-      const R hp = (R)0.5 * (F + al * qf), hm = (R)0.5 * (F - al * qf);
+      R hp = (R)0.5 * (F + al * qf), hm = (R)0.5 * (F - al * qf);
+      if (sw)
+        sw_split<2, R>(f, xdir ? 0 : 1, qf, sP[c], sP[SM2_Q + c], sP[2 * SM2_Q + c], sP[3 * SM2_Q + c],
+                       sQ[3 * SM2_Q + c], sA[c], sG[c], hp, hm);
       if (xdir) { sHxp[dst] = hp; sHxm[dst] = hm; }
       else { sHyp[dst - SM2_HX] = hp; sHym[dst - SM2_HX] = hm; }
     }
@@ -914,9 +973,15 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       R rho = sP[c], u = sP[SM2_Q + c], v = sP[2 * SM2_Q + c], p = sP[3 * SM2_Q + c];
       R E = sQ[3 * SM2_Q + c];
       R qf = sQ[f * SM2_Q + c];
-      R F = lf_flux<2>(f, dir, qf, rho, u, v, p, E);
-      R al = dir == 0 ? ax : ay;
-      R hp = (R)0.5 * (F + al * qf), hm = (R)0.5 * (F - al * qf);
+      R hp, hm;
+      if (sw) {
+        sw_split<2, R>(f, dir, qf, rho, u, v, p, E, sA[c], sG[c], hp, hm);
+      } else {
+        R F = lf_flux<2>(f, dir, qf, rho, u, v, p, E);
+        R al = dir == 0 ? ax : ay;
+        hp = (R)0.5 * (F + al * qf);
+        hm = (R)0.5 * (F - al * qf);
+      }
       if (dir == 0) { sHxp[px * TY2 + (py - 3)] = hp; sHxm[px * TY2 + (py - 3)] = hm; }
       else { sHyp[(px - 3) * PY2 + py] = hp; sHym[(px - 3) * PY2 + py] = hm; }
     }
@@ -1221,6 +1286,11 @@ __global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const doub
 constexpr int NT1 = 256;
 
 template <class R, int NT = NT1>
+__host__ __device__ constexpr size_t sw_smem1d_bytes() {
+  return sizeof(R) * 2 * (NT + 5);
+}
+
+template <class R, int NT = NT1>
 __host__ __device__ constexpr size_t smem1d_bytes(int nq) {
   return sizeof(R) * ((size_t)nq * (NT + 5) + 3 * (NT + 5) + 2 * (NT + 5) + NT);
 }
@@ -1229,7 +1299,7 @@ __host__ __device__ constexpr size_t smem1d_bytes(int nq) {
 // Every thread of the block must call it; returns this thread's Halley mask.
 // Pointers are plain (not restrict) because the persistent ensemble kernel
 // calls it on buffers written by other blocks of the same launch.
-template <int STAGE, class R, int NT, bool VISC = false>
+template <int STAGE, class R, int NT, bool VISC = false, bool SW = false>
 __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, const double* Uk,
                                                 const double* auxk, const double* Un, double* out,
                                                 double* cand, const double* strips, double alpha,
@@ -1242,6 +1312,9 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
   R* sHp = sP + 3 * PX1;
   R* sHm = sHp + PX1;
   R* sF = sHm + PX1;                    // [TX1+1]
+  R* sG = sF + NT;                      // Steger-Warming only: gamma, a [PX1] each
+  R* sA = sG + PX1;
+  constexpr bool sw = SW;
   const int tid = threadIdx.x;
   const long long nc = g.ncell;
   const R ax = (R)alpha;
@@ -1255,11 +1328,14 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
         sQ[q * PX1 + i] = (R)(((s.flip >> q) & 1) ? -v : v);
       }
       sQ[nv * PX1 + i] = (R)auxk[nc + s.xs];
+      if (sw) sG[i] = (R)auxk[s.xs];
     } else if (s.kind == 1) {
       for (int q = 0; q < nv; ++q) sQ[q * PX1 + i] = (R)ghost(g, strips, s, q);
       sQ[nv * PX1 + i] = (R)ghost(g, strips, s, nv + 1);
+      if (sw) sG[i] = (R)ghost(g, strips, s, nv);
     } else {
       for (int q = 0; q < nq; ++q) sQ[q * PX1 + i] = (R)1.0;
+      if (sw) sG[i] = (R)1.0;
     }
   }
   __syncthreads();
@@ -1272,6 +1348,7 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
     sP[i] = rho;
     sP[PX1 + i] = u;
     sP[2 * PX1 + i] = p;
+    if (sw) sA[i] = sqrt(sG[i] * p / rho);
   }
   __syncthreads();
   const bool live = tid < TX1 && x0 + tid < g.nx;
@@ -1289,8 +1366,13 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
       R qf = sQ[f * PX1 + i];
       R F = lf_flux<1>(f, 0, qf, rho, u, (R)0, p, sQ[2 * PX1 + i]);
 #endif
-      sHp[i] = (R)0.5 * (F + ax * qf);
-      sHm[i] = (R)0.5 * (F - ax * qf);
+      if (sw) {
+        sw_split<1, R>(f, 0, qf, sP[i], sP[PX1 + i], (R)0, sP[2 * PX1 + i], sQ[2 * PX1 + i], sA[i], sG[i],
+                       sHp[i], sHm[i]);
+      } else {
+        sHp[i] = (R)0.5 * (F + ax * qf);
+        sHm[i] = (R)0.5 * (F - ax * qf);
+      }
     }
     __syncthreads();
     {
@@ -1339,7 +1421,7 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
   return bits;
 }
 
-template <int STAGE, class R, bool VISC>
+template <int STAGE, class R, bool VISC, bool SW = false>
 __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk,
                                                  const double* __restrict__ Un,
@@ -1348,7 +1430,7 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
                                                  int aidx, int midx, double dt_arg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const double dt = STAGE == 0 ? dt_arg : slots->dt;
-  unsigned bits = flux1d_tile<STAGE, R, NT1, VISC>(m, g, Uk, auxk, Un, out, cand, strips, bitsd(slots->ax[aidx]), dt,
+  unsigned bits = flux1d_tile<STAGE, R, NT1, VISC, SW>(m, g, Uk, auxk, Un, out, cand, strips, bitsd(slots->ax[aidx]), dt,
                                              blockIdx.x * (NT1 - 1), smraw);
   if (STAGE == 0) return;
   block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);

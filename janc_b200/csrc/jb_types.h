@@ -71,9 +71,9 @@ enum jb_kernel_cat {
 enum jb_precision { JB_PREC_STRICT = 0, JB_PREC_FP64 = 1, JB_PREC_MIXED = 2 };
 
 // Advective flux (solver_{1D,2D}/flux.py set_flux_solver): flux splitting
-// (LF, WENO5-JS on the split fluxes) or Godunov (WENO5-JS on the primitives
-// and a Riemann solver).
-enum jb_flux_scheme { JB_FLUX_LF = 0, JB_FLUX_HLLC = 1, JB_FLUX_AUSMPW = 2 };
+// (LF or Steger-Warming, the face reconstruction on the split fluxes) or
+// Godunov (the reconstruction on the primitives and a Riemann solver).
+enum jb_flux_scheme { JB_FLUX_LF = 0, JB_FLUX_HLLC = 1, JB_FLUX_AUSMPW = 2, JB_FLUX_SW = 3 };
 
 // Face reconstruction (solver_{1D,2D}/reconstruction): WENO5-JS or MUSCL
 // (minmod limiter, kappa = 1/3, beta = 1).

@@ -23,10 +23,10 @@ def _ptr(t):
 
 def flux_scheme(flux_config):
     """Validate a reference ``flux_solver_config`` (set_flux_solver,
-    solver_2D/flux.py:19-40) and name the native flux: ``LF``, ``HLLC`` or
-    ``AUSMPW_plus``.  Raises as the reference does: KeyError for an unknown
-    solver type or dictionary entry; what the reference has but this build
-    does not (SW splitting) raises NotImplementedError."""
+    solver_2D/flux.py:19-40) and name the native flux: ``LF``, ``SW``
+    (flux splitting) or ``HLLC``, ``AUSMPW_plus`` (Godunov).  Raises as the
+    reference does: KeyError for an unknown solver type or dictionary
+    entry."""
     if flux_config is None:
         return "LF"
     solver_type = flux_config["solver_type"]
@@ -41,11 +41,9 @@ def flux_scheme(flux_config):
             raise KeyError(rs)
         return rs
     split = flux_config["split_method"]
-    if split == "SW":
-        raise NotImplementedError("Steger-Warming splitting is not built; use LF")
-    if split != "LF":
+    if split not in ("LF", "SW"):
         raise KeyError(split)
-    return "LF"
+    return split
 
 
 def transport_params(transport_config):
@@ -105,7 +103,7 @@ class Solver:
 
     ``flux_config`` is the reference's ``flux_solver_config``
     (solver_{1D,2D}/flux.py set_flux_solver): ``solver_type``
-    ``flux_splitting`` (``split_method`` ``LF``) or ``godunov``
+    ``flux_splitting`` (``split_method`` ``LF`` or ``SW``) or ``godunov``
     (``riemann_solver`` ``HLLC`` or ``AUSMPW_plus``), with
     ``interface_reconstruction`` ``WENO5_JS`` or ``MUSCL``.  Default: LF flux
     splitting with WENO5_JS.

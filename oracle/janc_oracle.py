@@ -756,16 +756,65 @@ def split_flux_2d(m, ixy, U, aux):
     return 0.5 * (F + th * U), 0.5 * (F - th * U)
 
 
-def total_flux(m, Up, Ap, dx, dy=None, recon="WENO5_JS"):
+def _sw_combine(theta, a, H1, H2, H4):
+    """Eigenvalue groups of flux_splitting/SW.py (smoothed |lambda|)."""
+    lambda1, lambda2, lambda4 = theta - a, theta, theta + a
+    eps = 1e-6
+    lap1 = 0.5 * (lambda1 + np.sqrt(np.power(lambda1, 2) + eps ** 2))
+    lam1 = 0.5 * (lambda1 - np.sqrt(np.power(lambda1, 2) + eps ** 2))
+    lap2 = 0.5 * (lambda2 + np.sqrt(np.power(lambda2, 2) + eps ** 2))
+    lam2 = 0.5 * (lambda2 - np.sqrt(np.power(lambda2, 2) + eps ** 2))
+    lap4 = 0.5 * (lambda4 + np.sqrt(np.power(lambda4, 2) + eps ** 2))
+    lam4 = 0.5 * (lambda4 - np.sqrt(np.power(lambda4, 2) + eps ** 2))
+    return lap1 * H1 + lap2 * H2 + lap4 * H4, lam1 * H1 + lam2 * H2 + lam4 * H4
+
+
+def split_sw_2d(m, ixy, U, aux):
+    """solver_2D/flux_splitting/SW.py:4-37 (Steger-Warming)"""
+    rho, u, v, Y, p, a = U_to_prim(m, U, aux)
+    rhoE = U[3:4]
+    gamma = aux[0:1]
+    zx = (ixy == 1) * 1.0
+    zy = (ixy == 2) * 1.0
+    theta = zx * u + zy * v
+    H1 = (1 / (2 * gamma)) * np.concatenate([rho, rho * u - rho * a * zx, rho * v - rho * a * zy,
+                                             rhoE + p - rho * a * theta, rho * Y], axis=0)
+    H2 = ((gamma - 1) / gamma) * np.concatenate([rho, rho * u, rho * v, 0.5 * rho * (u ** 2 + v ** 2), rho * Y],
+                                                axis=0)
+    H4 = (1 / (2 * gamma)) * np.concatenate([rho, rho * u + rho * a * zx, rho * v + rho * a * zy,
+                                             rhoE + p + rho * a * theta, rho * Y], axis=0)
+    return _sw_combine(theta, a, H1, H2, H4)
+
+
+def split_sw_1d(m, U, aux):
+    """solver_1D/flux_splitting/SW.py:4-36 with J = 1 and zx = 1 (the
+    reference's 1D flux_splitting calls split_flux(U, aux) without the
+    `metrics` argument this function declares, so the 1D SW path raises a
+    TypeError there; this is the arithmetic the function states)."""
+    rho, u, Y, p, a = U_to_prim(m, U, aux)
+    rhoE = U[2:3]
+    gamma = aux[0:1]
+    J, zx = 1.0, 1.0
+    theta = zx * u
+    H1 = J * (1 / (2 * gamma)) * np.concatenate([rho, rho * u - rho * a * zx, rhoE + p - rho * a * theta,
+                                                 rho * Y], axis=0)
+    H2 = J * ((gamma - 1) / gamma) * np.concatenate([rho, rho * u, 0.5 * rho * (u ** 2), rho * Y], axis=0)
+    H4 = J * (1 / (2 * gamma)) * np.concatenate([rho, rho * u + rho * a * zx, rhoE + p + rho * a * theta,
+                                                 rho * Y], axis=0)
+    return _sw_combine(theta, a, H1, H2, H4)
+
+
+def total_flux(m, Up, Ap, dx, dy=None, recon="WENO5_JS", split="LF"):
     """flux_splitting (solver_1D/flux.py:51-58, solver_2D/flux.py:56-68) on
     the ghost-padded arrays; returns -(dF/dx [+ dG/dy])."""
     if Up.ndim == 2:
-        Fplus, Fminus = split_flux_1d(m, Up, Ap)
+        Fplus, Fminus = (split_sw_1d if split == "SW" else split_flux_1d)(m, Up, Ap)
         F = _recon(Fplus, 1, None, True, recon) + _recon(Fminus, 1, None, False, recon)
         dF = F[:, 1:] - F[:, :-1]
         return -(dF / dx)
-    Fplus, Fminus = split_flux_2d(m, 1, Up, Ap)
-    Gplus, Gminus = split_flux_2d(m, 2, Up, Ap)
+    sf = split_sw_2d if split == "SW" else split_flux_2d
+    Fplus, Fminus = sf(m, 1, Up, Ap)
+    Gplus, Gminus = sf(m, 2, Up, Ap)
     F = _recon(Fplus, 1, 2, True, recon) + _recon(Fminus, 1, 2, False, recon)
     G = _recon(Gplus, 2, 1, True, recon) + _recon(Gminus, 2, 1, False, recon)
     dF = F[:, 1:, :] - F[:, :-1, :]
@@ -1085,6 +1134,7 @@ class Solver:
         self.solver_type = fc["solver_type"]
         self.riemann = fc.get("riemann_solver", "HLLC")
         self.recon = fc.get("interface_reconstruction", "WENO5_JS")
+        self.split = fc.get("split_method", "LF")
         self.transport = Transport(transport_config) if fc.get("viscosity", "off") == "on" else None
 
     def flux_func(self, U, aux, dx, dy, dt, theta=None):
@@ -1096,7 +1146,7 @@ class Solver:
         if self.solver_type == "godunov":
             adv = godunov_flux(self.m, Up, Ap, dx, dy, self.riemann, self.recon)
         else:
-            adv = total_flux(self.m, Up, Ap, dx, dy, self.recon)
+            adv = total_flux(self.m, Up, Ap, dx, dy, self.recon, self.split)
         if self.transport is not None:  # NS_flux = advective + viscous (solver_2D/flux.py:117-118)
             return dt * (adv + viscous_flux(self.m, self.transport, Up, Ap, dx, dy))
         return dt * adv

@@ -53,9 +53,11 @@ def test_flux_config_validation():
                         "riemann_solver": "HLLC"}) == "HLLC"
     with pytest.raises(KeyError):
         flux_scheme({"solver_type": "godunov", "interface_reconstruction": "WENO7", "riemann_solver": "HLLC"})
-    with pytest.raises(NotImplementedError):
+    assert flux_scheme({"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS",
+                        "split_method": "SW"}) == "SW"
+    with pytest.raises(KeyError):
         flux_scheme({"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS",
-                     "split_method": "SW"})
+                     "split_method": "VanLeer"})
 
 
 def _random_w(om, dim, n, rng):
