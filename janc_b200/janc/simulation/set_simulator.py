@@ -25,8 +25,8 @@ def set_rhs(dim, reaction_config, source_config=None, is_parallel=False, is_amr=
         _state.config["slab"] = Slab()
     elif not is_parallel:
         _state.config["slab"] = None
-    if source_config is not None:
-        raise NotImplementedError("user source terms are outside the detailed-chemistry path")
+    if not reaction_config["is_detailed_chemistry"]:
+        raise NotImplementedError("non-detailed chemistry (an N2-only state) is outside the 9-species path")
 
     def flux_func(U, aux, dx, dy, dt, theta):
         Ud, kind = _state.to_device(U)
@@ -37,21 +37,52 @@ def set_rhs(dim, reaction_config, source_config=None, is_parallel=False, is_amr=
     flux_func._janc_b200_flux = True
     update_func = aux_func_1D.update_aux if dim == "1D" else aux_func.update_aux
     update_func._janc_b200_update = True
-    source_func = None
+    # detailed chemistry: a user source is added to the flux (set_simulator.py:50-54)
+    source_func = source_config["self_defined_source_terms"] if source_config is not None else None
     return flux_func, update_func, source_func
 
 
 def set_advance_func(dim, flux_config, reaction_config, time_control, is_amr, flux_func, update_func,
                      source_func):
     """advance_one_step(U, aux, dx, dy, dt, theta) as set_simulator.py:73-125
-    (Lie splitting: RK3 flux, chemistry, update_aux) -- one fused call."""
+    (Lie splitting: time-stepped flux, chemistry, update_aux).  TVD_RK3
+    without a user source is one fused native call; RK2 or a user source is
+    composed as the reference composes it, from the native flux_func,
+    update_aux and reaction_source_terms and the user's callable."""
     if is_amr:
         raise NotImplementedError("AMR is not part of this build")
-    if not reaction_config["is_detailed_chemistry"]:
-        def advance_flux(U, aux, dx, dy, dt, theta=None):
-            return time_step_dict[time_control["temporal_evolution_scheme"]](
-                U, aux, dx, dy, dt, theta, flux_func, update_func)
-        return advance_flux
+    scheme = time_control["temporal_evolution_scheme"]
+    if scheme not in time_step_dict:
+        raise KeyError(scheme)
+    step = time_step_dict[scheme]
+    if source_func is not None or scheme != "TVD_RK3" or not reaction_config["is_detailed_chemistry"]:
+        if source_func is None:
+            def advance_flux(U, aux, dx, dy, dt, theta=None):
+                return step(U, aux, dx, dy, dt, theta, flux_func, update_func)
+        elif flux_config["solver_type"] == "flux_splitting":
+            def rhs_func(U, aux, dx, dy, dt, theta=None):
+                return flux_func(U, aux, dx, dy, dt, theta) + source_func(U, aux, dt, theta)
+
+            def advance_flux(U, aux, dx, dy, dt, theta=None):
+                return step(U, aux, dx, dy, dt, theta, rhs_func, update_func)
+        else:  # godunov: the source as a second time-stepped pass
+            def wrapped_source_func(U, aux, dx, dy, dt, theta=None):
+                return source_func(U, aux, dt, theta)
+
+            def advance_flux(U, aux, dx, dy, dt, theta=None):
+                U_adv, aux_adv = step(U, aux, dx, dy, dt, theta, flux_func, update_func)
+                return step(U_adv, aux_adv, dx, dy, dt, theta, wrapped_source_func, update_func)
+        if not reaction_config["is_detailed_chemistry"]:
+            return advance_flux
+
+        def advance_composed(U, aux, dx, dy, dt, theta=None):
+            U, aux = advance_flux(U, aux, dx, dy, dt, theta)
+            dU = reaction_model.reaction_source_terms(U, aux, dt, theta)
+            U = U + dU
+            aux = update_func(U, aux)
+            return U, aux
+        advance_composed._janc_b200_composed = True
+        return advance_composed
 
     def advance_one_step(U, aux, dx, dy, dt, theta=None):
         Ud, kind = _state.to_device(U)
@@ -254,15 +285,18 @@ class Simulator:
         (flux_1D if dim == "1D" else flux).set_flux_solver(
             flux_config, simulation_config.get("transport_config", None), nondim_config)
         boundary.set_boundary(boundary_config, dim)
-        if time_control["temporal_evolution_scheme"] != "TVD_RK3":
-            raise KeyError("only 'TVD_RK3' time stepping is built")
+        if time_control["temporal_evolution_scheme"] not in time_step_dict:
+            raise KeyError(time_control["temporal_evolution_scheme"])
         self.dim = dim
         self.dx = grid_config["dx"]
         self.dy = grid_config.get("dy") if dim == "2D" else None
-        self.flux_func, self.update_func, _ = set_rhs(dim, reaction_config, None, self.is_parallel)
+        source_config = simulation_config.get("source_config", None)
+        self.flux_func, self.update_func, self.source_func = set_rhs(dim, reaction_config, source_config,
+                                                                     self.is_parallel)
         self.slab = _state.config["slab"]
         self._advance_body = set_advance_func(dim, flux_config, reaction_config, time_control, False,
-                                              self.flux_func, self.update_func, None)
+                                              self.flux_func, self.update_func, self.source_func)
+        self._composed = getattr(self._advance_body, "_janc_b200_composed", False)
         self.dt = time_control.get("dt", None)
         self.CFL = time_control.get("CFL", None)
         if self.dt is None and self.CFL is None:
@@ -272,6 +306,12 @@ class Simulator:
         Ud, kind = _state.to_device(U)
         auxd, _ = _state.to_device(aux)
         s = _state.solver_for(tuple(Ud.shape[1:]), self.dx, self.dy)
+        if self._composed:  # RK2 or a user source: CFL dt, then the composed step
+            dt = s.cfl_dt(Ud, auxd, self.CFL) if self.CFL is not None else self.dt
+            if kind == "numpy":
+                dt = float(dt)
+            U1, aux1 = self._advance_body(U, aux, self.dx, self.dy, dt, theta)
+            return U1, aux1, t + dt, dt
         if self.CFL is not None:
             U1, aux1, dts = s.advance(Ud, auxd, 1, cfl=self.CFL, theta=theta)
             dt = dts[0]

@@ -1,4 +1,5 @@
-"""SSP-RK3 (src/janc_v2/simulation/time_step/TVD_RK3.py:5-12).
+"""Time steppers (src/janc_v2/simulation/time_step): SSP-RK3
+(TVD_RK3.py:5-12) and Heun's RK2 (RK2.py:5-12).
 
 With the rhs/update functions returned by ``set_rhs`` the whole step runs as
 one fused native call (``jb_rk3``); with other callables the three stages are
@@ -23,4 +24,17 @@ def _tvd_rk3(U, aux, dx, dy, dt, theta, rhs_func, update_func):
     return U3, aux3
 
 
-time_step_dict = {"TVD_RK3": _tvd_rk3}
+def _rk2(U, aux, dx, dy, dt, theta, rhs_func, update_func):
+    """RK2.py:5-12 (Heun): two rhs evaluations composed as the reference
+    writes them, each through the native flux_func / update_aux when those
+    are the functions given."""
+    dev = rhs_func(U, aux, dx, dy, dt, theta)
+    U1 = U + dev
+    aux1 = update_func(U1, aux)
+    dev1 = rhs_func(U1, aux1, dx, dy, dt, theta)
+    U2 = U + 1 / 2 * (dev + dev1)
+    aux2 = update_func(U2, aux1)
+    return U2, aux2
+
+
+time_step_dict = {"TVD_RK3": _tvd_rk3, "RK2": _rk2}

@@ -1121,7 +1121,10 @@ class Solver:
     ``advance_one_step`` and ``advance_func`` with the reference's
     signatures (set_simulator.py:20-125, 410-447)."""
 
-    def __init__(self, mech, dim, dx, dy=None, bc=None, cfl=None, flux_config=None, transport_config=None):
+    def __init__(self, mech, dim, dx, dy=None, bc=None, cfl=None, flux_config=None, transport_config=None,
+                 time_scheme="TVD_RK3", source=None):
+        self.time_scheme = time_scheme
+        self.source = source  # source_config['self_defined_source_terms'](U, aux, dt, theta)
         self.m = mech
         self.dim = dim
         self.dx, self.dy = dx, dy
@@ -1168,9 +1171,31 @@ class Solver:
         aux3 = update_func(U3, aux2)
         return U3, aux3
 
+    def rk2(self, U, aux, dx, dy, dt, theta, rhs_func=None, update_func=None):
+        """RK2.py:5-12"""
+        rhs_func = rhs_func or self.flux_func
+        update_func = update_func or self.update_func
+        dev = rhs_func(U, aux, dx, dy, dt, theta)
+        U1 = U + dev
+        aux1 = update_func(U1, aux)
+        dev1 = rhs_func(U1, aux1, dx, dy, dt, theta)
+        U2 = U + 1 / 2 * (dev + dev1)
+        aux2 = update_func(U2, aux1)
+        return U2, aux2
+
     def advance_one_step(self, U, aux, dx, dy, dt, theta=None):
-        """set_simulator.py:117-122 (Lie splitting: RK3 flux, chemistry, T)"""
-        U, aux = self.rk3(U, aux, dx, dy, dt, theta)
+        """set_simulator.py:73-122 (Lie splitting: time-stepped flux with the
+        user source as set_advance_func composes it, chemistry, T)"""
+        step = self.rk2 if self.time_scheme == "RK2" else self.rk3
+        if self.source is None:
+            U, aux = step(U, aux, dx, dy, dt, theta)
+        elif self.solver_type == "flux_splitting":
+            def rhs(U, aux, dx, dy, dt, theta=None):
+                return self.flux_func(U, aux, dx, dy, dt, theta) + self.source(U, aux, dt, theta)
+            U, aux = step(U, aux, dx, dy, dt, theta, rhs)
+        else:
+            U, aux = step(U, aux, dx, dy, dt, theta)
+            U, aux = step(U, aux, dx, dy, dt, theta, lambda U, a, dx, dy, dt, th=None: self.source(U, a, dt, th))
         dU = reaction_source_terms(self.m, U, aux, dt)
         U = U + dU
         aux = self.update_func(U, aux)
