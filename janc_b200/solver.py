@@ -321,6 +321,68 @@ class Solver:
         self._check(rc, "jb_advance")
         return U_out, aux_out, dt_hist
 
+    def advance_host(self, inputs, outputs, nsteps=1, dt=None, cfl=None, theta=None):
+        """Advance host states through the device with the copies hidden
+        behind the steps: ``inputs`` and ``outputs`` are equal-length lists of
+        (U, aux) pinned CPU float64 tensors; item i is copied in on one
+        stream, advanced ``nsteps`` on the current stream and copied out on a
+        third, so the copy-in of item i+1 and the copy-out of item i-1 overlap
+        the steps of item i (two device buffer sets).  Items are independent
+        states (a parameter sweep, a queue of cases); a single time-stepping
+        chain keeps its state on the device instead.  Returns when every
+        result is in ``outputs``."""
+        if cfl is None and dt is None:
+            raise ValueError("need dt or cfl")
+        if len(inputs) != len(outputs):
+            raise ValueError("inputs and outputs differ in length")
+        for hU, haux in list(inputs) + list(outputs):
+            if hU.device.type != "cpu" or haux.device.type != "cpu" or not (hU.is_pinned() and haux.is_pinned()):
+                raise ValueError("advance_host takes pinned CPU tensors")
+            if tuple(hU.shape) != (self.nv,) + self.shape or tuple(haux.shape) != (2,) + self.shape:
+                raise ValueError("state shape does not match the solver")
+        self.set_theta(theta)
+        dev = self.device
+        buf = [[torch.empty((self.nv,) + self.shape, dtype=torch.float64, device=dev),
+                torch.empty((2,) + self.shape, dtype=torch.float64, device=dev)] for _ in range(4)]
+        din, dout = buf[:2], buf[2:]
+        hist = torch.empty(max(nsteps, 1), dtype=torch.float64, device=dev)
+        comp = torch.cuda.current_stream(dev)
+        s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        ev = lambda: torch.cuda.Event()  # noqa: E731
+        loaded, computed, drained = [ev(), ev()], [ev(), ev()], [ev(), ev()]
+        started = ev()
+        started.record(comp)
+        s_in.wait_event(started)
+        s_out.wait_event(started)
+        for i, ((hU, haux), (oU, oaux)) in enumerate(zip(inputs, outputs)):
+            b = i % 2
+            with torch.cuda.stream(s_in):
+                if i >= 2:
+                    s_in.wait_event(computed[b])  # the step that read din[b] is done
+                din[b][0].copy_(hU, non_blocking=True)
+                din[b][1].copy_(haux, non_blocking=True)
+                loaded[b].record(s_in)
+            comp.wait_event(loaded[b])
+            if i >= 2:
+                comp.wait_event(drained[b])  # dout[b] has been copied out
+            rc = self._lib.jb_advance(self._h, _ptr(din[b][0]), _ptr(din[b][1]), _ptr(dout[b][0]),
+                                      _ptr(dout[b][1]), float(dt or 0.0), float(cfl or 0.0), int(nsteps),
+                                      _ptr(hist), ctypes.c_void_p(comp.cuda_stream))
+            self._check(rc, "jb_advance")
+            computed[b].record(comp)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(computed[b])
+                oU.copy_(dout[b][0], non_blocking=True)
+                oaux.copy_(dout[b][1], non_blocking=True)
+                drained[b].record(s_out)
+        comp.wait_stream(s_in)
+        comp.wait_stream(s_out)
+        for t in din + dout:
+            for x in t:
+                x.record_stream(s_in)
+                x.record_stream(s_out)
+        return outputs
+
     def advance_one_step(self, U, aux, dx=None, dy=None, dt=None, theta=None):
         """set_advance_func's advance_one_step(U, aux, dx, dy, dt, theta)."""
         self._spacing(dx, dy)
