@@ -52,7 +52,8 @@ def build(force=False, verbose=False):
     def compile_unit(unit):
         src, extra = unit
         obj = os.path.join(OBJ, src.replace(".cu", ".o"))
-        cmd = [nvcc] + ARCH + COMMON + extra + ["-c", os.path.join(CSRC, src), "-o", obj]
+        flags = os.environ.get("JB_NVCC_FLAGS", "").split()  # extra -D tuning constants
+        cmd = [nvcc] + ARCH + COMMON + extra + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

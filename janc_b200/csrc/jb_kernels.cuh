@@ -1067,7 +1067,10 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
 //                the Halley iterates of the new state
 // The primitives (u, v, p as float32) of the stage state come from the
 // select pass that produced its temperature (prims[3][ncell]).
-constexpr int SX_R = 16, SX_NT = 128;
+#ifndef JB_SX_R
+#define JB_SX_R 16
+#endif
+constexpr int SX_R = JB_SX_R, SX_NT = 128;
 constexpr int YR_W = 8, YR_NT = 32 * YR_W;     // warps (runs) per block
 constexpr int YR_C = 38, YR_F = 33;            // window cells, faces per run
 constexpr size_t YR_SMEM = sizeof(float) * YR_W * (2 * 12 * YR_C + 12 * YR_F);
