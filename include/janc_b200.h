@@ -127,7 +127,9 @@ int jb_set_reconstruction(jb_handle* h, int recon);
  * viscous_flux, solver_2D/flux.py:70-115 / solver_1D/flux.py:67-99): the
  * laminar transport model of *tr is used by every later flux evaluation of
  * the handle (added to the advective flux as NS_flux does, solver_2D/flux.py:117).
- * tr = NULL switches back to Euler fluxes.  Allocates its scratch on the first
+ * tr->turbulence_model = 1 adds the LES sub-grid viscosity of the 2D Vreman
+ * model (model/LES/Verman.py; JB_ERR_UNSUPPORTED on a 1D handle, where the
+ * reference has no model).  tr = NULL switches back to Euler fluxes.  Allocates its scratch on the first
  * call.  jb_adjoint_step supports the inviscid path only. */
 int jb_set_transport(jb_handle* h, const jb_transport* tr);
 

@@ -49,7 +49,7 @@ def status_text(code):
 class Transport(ctypes.Structure):
     """jb_transport (laminar transport model of the viscous fluxes)."""
     _fields_ = [("viscosity_model", ctypes.c_int), ("conductivity_model", ctypes.c_int),
-                ("diffusivity_model", ctypes.c_int), ("pad_", ctypes.c_int)] + \
+                ("diffusivity_model", ctypes.c_int), ("turbulence_model", ctypes.c_int)] + \
         [(n, ctypes.c_double) for n in ("mu_ref", "T_ref", "S", "nu0", "Pr", "Le", "k0", "D0", "Pr_t", "Le_t")]
 
 

@@ -514,8 +514,11 @@ int jb_set_transport(jb_handle* h, const jb_transport* tr) {
   }
   const jb_transport& t = *tr;
   auto bad01 = [](int v) { return v != 0 && v != 1; };
-  if (bad01(t.viscosity_model) || bad01(t.conductivity_model) || bad01(t.diffusivity_model))
+  if (bad01(t.viscosity_model) || bad01(t.conductivity_model) || bad01(t.diffusivity_model) ||
+      bad01(t.turbulence_model))
     return set_err(h, JB_ERR_ARG, "unknown transport model");
+  if (t.turbulence_model && h->dim != 2)
+    return set_err(h, JB_ERR_UNSUPPORTED, "the LES sub-grid model (Vreman) is 2D only");
   if (!(t.Pr > 0.0) || !(t.Le > 0.0) || !(t.Pr_t > 0.0) || !(t.Le_t > 0.0) ||
       (t.viscosity_model == 0 && !(t.T_ref > 0.0)))
     return set_err(h, JB_ERR_ARG, "transport parameters must be positive");

@@ -83,9 +83,12 @@ enum jb_reconstruction { JB_RECON_WENO5 = 0, JB_RECON_MUSCL = 1 };
 // 0 Sutherland mu_ref (T/T_ref)^1.5 (T_ref+S)/(T+S), 1 constant rho nu0;
 // conductivity 0 Prandtl number mu cp/Pr, 1 constant k0; diffusivity 0 Lewis
 // number rho D_k = k_k/(Le cp_k) (a Schmidt number gives Le = Sc/Pr), 1
-// constant D0.  Pr_t and Le_t enter only through the zero turbulent viscosity.
+// constant D0.  turbulence_model 0 laminar, 1 LES with the 2D Vreman
+// sub-grid viscosity mu_t = 0.07 rho sqrt(B / (a_ij a_ij))
+// (model/LES/Verman.py); mu_t adds to mu and enters k and D through Pr_t and
+// Le_t (transport_model.py:117-157).
 typedef struct jb_transport {
-  int viscosity_model, conductivity_model, diffusivity_model, pad_;
+  int viscosity_model, conductivity_model, diffusivity_model, turbulence_model;
   double mu_ref, T_ref, S, nu0, Pr, Le, k0, D0, Pr_t, Le_t;
 } jb_transport;
 

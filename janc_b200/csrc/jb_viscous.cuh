@@ -109,13 +109,30 @@ __device__ __forceinline__ double d_line(const double* f, long long st, int n, i
 #endif
 }
 
-// transport at one node (transport_model.py:106-157, laminar: mu_t = 0)
+// transport at one node (transport_model.py:106-157); mu_t is the LES
+// sub-grid viscosity (0 for the laminar model), mu the total
 struct NodeTransport {
   double mu, k, D[NS], h[NS];
 };
 
+// Vreman's sub-grid viscosity in 2D (model/LES/Verman.py:5-27) from the
+// node's velocity gradient, in the reference's order of operations.
+__device__ __forceinline__ double vreman_mu_t(double rho, double dx, double dy, double du_dx, double du_dy,
+                                              double dv_dx, double dv_dy) {
+  const double d1s = dx * dx, d2s = dy * dy;
+  const double a11 = du_dx, a12 = dv_dx, a21 = du_dy, a22 = dv_dy;
+  const double b11 = d1s * a11 * a11 + d2s * a21 * a21;
+  const double b12 = d1s * a11 * a12 + d2s * a21 * a22;
+  const double b22 = d1s * a12 * a12 + d2s * a22 * a22;
+  double B = fabs(b11 * b22 - b12 * b12);
+  if (!(B >= 0.0)) B = 0.0;  // jnp.where(B >= 0, B, 0): NaN -> 0
+  const double a_sum = a11 * a11 + a12 * a12 + a21 * a21 + a22 * a22;
+  const double ratio = a_sum > 0.0 ? B / a_sum : 0.0;
+  return rho * 0.07 * sqrt(ratio);
+}
+
 __device__ __forceinline__ void node_transport(const MP& m, const jb_transport& tr, double rho, double T,
-                                               const double* Yf, NodeTransport& o) {
+                                               const double* Yf, double mu_t, NodeTransport& o) {
   double cpk[NS], cp = 0.0;
 #pragma unroll
   for (int k = 0; k < NS; ++k) {
@@ -124,7 +141,6 @@ __device__ __forceinline__ void node_transport(const MP& m, const jb_transport& 
     o.h[k] = lo ? poly6(m.h_lo[k], T) : poly6(m.h_hi[k], T);
     cp = k == 0 ? cpk[0] * Yf[0] : cp + cpk[k] * Yf[k];
   }
-  const double mu_t = 0.0;
 #if JB_FAST
   if (tr.viscosity_model == 0) {
     const double x = T / tr.T_ref;
@@ -132,7 +148,8 @@ __device__ __forceinline__ void node_transport(const MP& m, const jb_transport& 
   } else {
     o.mu = rho * tr.nu0;
   }
-  if (tr.conductivity_model == 0 && tr.diffusivity_model == 0) {
+  if (tr.turbulence_model) o.mu = o.mu + mu_t;
+  if (tr.conductivity_model == 0 && tr.diffusivity_model == 0 && !tr.turbulence_model) {
     // Prandtl and Lewis numbers: rho D_k = mu / (Pr Le) for every species
     // (cp_k cancels), k = mu cp / Pr
     o.k = o.mu * cp / tr.Pr;
@@ -144,6 +161,7 @@ __device__ __forceinline__ void node_transport(const MP& m, const jb_transport& 
 #else
   if (tr.viscosity_model == 0) o.mu = tr.mu_ref * pow(T / tr.T_ref, 1.5) * (tr.T_ref + tr.S) / (T + tr.S);
   else o.mu = rho * tr.nu0;
+  if (tr.turbulence_model) o.mu = o.mu + mu_t;  // mu_LES returns mu + mu_t
 #endif
   if (tr.conductivity_model == 0) o.k = o.mu * cp / tr.Pr + mu_t * cp / tr.Pr_t;
   else o.k = tr.k0 + mu_t * cp / tr.Pr_t;
@@ -207,13 +225,13 @@ __global__ void __launch_bounds__(128) k_visc_flux(MP m, Grid g, jb_transport tr
 #pragma unroll
   for (int k = 0; k < NS; ++k) Yf[k] = N[(DIM + 2 + k) * np + i];
   NodeTransport tp;
-  node_transport(m, tr, rho, T, Yf, tp);
   // derivatives along x (stride PY, PX positions) and y (stride 1, PY positions)
   const double* lx = N + (long long)py;           // line at this y, position px
   const double* ly = N + (long long)px * PY;      // line at this x, position py
   auto ddx = [&](int plane) { return d_line(lx + plane * np, PY, PX, px, g.dx); };
   auto ddy = [&](int plane) { return d_line(ly + plane * np, 1, PY, py, g.dy); };
   if (DIM == 1) {
+    node_transport(m, tr, rho, T, Yf, 0.0, tp);
     double* out;
     long long ostride, oidx;
     const double du_dx = ddx(1), dT_dx = ddx(2);
@@ -237,6 +255,8 @@ __global__ void __launch_bounds__(128) k_visc_flux(MP m, Grid g, jb_transport tr
     return;
   }
   const double du_dx = ddx(1), du_dy = ddy(1), dv_dx = ddx(2), dv_dy = ddy(2);
+  const double mu_t = tr.turbulence_model ? vreman_mu_t(rho, g.dx, g.dy, du_dx, du_dy, dv_dx, dv_dy) : 0.0;
+  node_transport(m, tr, rho, T, Yf, mu_t, tp);
   const double lam = -2.0 / 3.0 * tp.mu;
   const double S12 = 0.5 * (du_dy + dv_dx);
   const double div_u = du_dx + dv_dy;

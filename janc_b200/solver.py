@@ -46,10 +46,12 @@ def flux_scheme(flux_config):
     return split
 
 
-def transport_params(transport_config):
+def transport_params(transport_config, dim=2):
     """jb_transport from a reference ``transport_config`` (set_transport,
-    model/transport_model.py:26-104), with its defaults and errors; only the
-    laminar model is built (LES raises NotImplementedError)."""
+    model/transport_model.py:26-104), with its defaults and errors: laminar,
+    or LES with the Vreman sub-grid model, the only one the reference has
+    (``LES_model`` 'Verman', 2D; another model name raises the KeyError the
+    reference raises at its first flux evaluation)."""
     c = transport_config
     t = _native.Transport()
     t.mu_ref, t.T_ref, t.S, t.nu0 = 1.716e-5, 273.15, 110.4, 1e-4
@@ -82,8 +84,17 @@ def transport_params(transport_config):
                        "are supported.")
     model = c.get("turbulence_model", "laminar")
     if model == "LES":
-        raise NotImplementedError("LES sub-grid models are not built")
-    if model != "laminar":
+        assert "LES_model" in c, "Please specify the SGS model of LES."
+        assert "Pr_t" in c, "Key 'Pr_t'(turbulent Prandtl number) must be provided"
+        assert ("Le_t" in c) or ("Sc_t" in c), \
+            "Key 'Sc_t'(turbulent Schmidt number) or 'Le_t'(turbulent Lewis number) must be provided"
+        name = f"{c['LES_model']}_{'2D' if dim == 2 else '1D'}"
+        if name != "Verman_2D":
+            raise KeyError(name)
+        t.turbulence_model = 1
+        t.Pr_t = c["Pr_t"]
+        t.Le_t = c["Le_t"] if "Le_t" in c else c["Sc_t"] / t.Pr_t
+    elif model != "laminar":
         raise KeyError("Only 'laminar' and 'LES' model are supported.")
     return t
 
@@ -180,7 +191,7 @@ class Solver:
         if self.viscous:
             if transport_config is None:
                 raise KeyError("transport_config")  # set_flux_solver passes it to set_transport
-            self._transport = transport_params(transport_config)
+            self._transport = transport_params(transport_config, dim)
             with torch.cuda.device(self.device):
                 _native.check(L.jb_set_transport(h, ctypes.byref(self._transport)), h, "jb_set_transport")
 

@@ -1004,14 +1004,53 @@ class Transport:
         else:
             raise KeyError("Only 'Schmidt number', 'Lewis number', and 'constant' species diffusivity "
                            "model are supported.")
-        if cfg.get("turbulence_model", "laminar") != "laminar":
-            raise NotImplementedError("LES")
+        self.model, self.LES_model = "laminar", None
+        if "turbulence_model" in cfg:
+            if cfg["turbulence_model"] == "LES":
+                self.model = "LES"
+                assert "LES_model" in cfg, "Please specify the SGS model of LES."
+                self.LES_model = cfg["LES_model"]
+                assert "Pr_t" in cfg
+                assert ("Le_t" in cfg) or ("Sc_t" in cfg)
+                self.Pr_t = cfg["Pr_t"]
+                if "Le_t" in cfg:
+                    self.Le_t = cfg["Le_t"]
+                    self.Sc_t = self.Le_t * self.Pr_t
+                else:
+                    self.Sc_t = cfg["Sc_t"]
+                    self.Le_t = self.Sc_t / self.Pr_t
+            elif cfg["turbulence_model"] != "laminar":
+                raise KeyError("Only 'laminar' and 'LES' model are supported.")
 
     def mu(self, rho, T):
-        """mu_Sutherland / mu_constant (:106-112); laminar mu_t = 0"""
+        """mu_Sutherland / mu_constant (:106-112), the laminar part"""
         if self.nu_type == "Sutherland":
             return self.mu_ref * (T / self.T_ref) ** 1.5 * (self.T_ref + self.S) / (T + self.S)
         return rho * self.nu0
+
+    def mu_total(self, rho, T, dx, dy, du_dx, du_dy, dv_dx, dv_dy):
+        """transport_model.mu (:117-130): (mu, mu_t), mu = laminar + mu_t for
+        LES with the 2D Vreman model (model/LES/Verman.py:5-27, c = 0.07)."""
+        mu = self.mu(rho, T)
+        if self.model != "LES":
+            return mu, 0.0
+        if self.LES_model != "Verman" or dy is None:
+            raise KeyError(f"{self.LES_model}_{'2D' if dy is not None else '1D'}")
+        d1, d2 = dx, dy
+        a11, a12 = du_dx, dv_dx
+        a21, a22 = du_dy, dv_dy
+        b11_x, b12_x = (d1 ** 2) * a11 * a11, (d1 ** 2) * a11 * a12
+        b22_x = (d1 ** 2) * a12 * a12
+        b11_y, b12_y = (d2 ** 2) * a21 * a21, (d2 ** 2) * a21 * a22
+        b22_y = (d2 ** 2) * a22 * a22
+        b11, b12, b22 = b11_x + b11_y, b12_x + b12_y, b22_x + b22_y
+        B_b = np.abs(b11 * b22 - b12 ** 2)
+        B_b = np.where(B_b >= 0.0, B_b, np.zeros_like(B_b))
+        a_sum = a11 ** 2 + a12 ** 2 + a21 ** 2 + a22 ** 2
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = np.where(a_sum > 0.0, B_b / a_sum, np.zeros_like(a_sum))
+        mu_t = rho * 0.07 * np.sqrt(ratio)
+        return mu + mu_t, mu_t
 
     def kappa(self, mu, cp, mu_t=0.0):
         """kappa_Pr / kappa_constant (:133-137)"""
@@ -1076,9 +1115,9 @@ def viscous_flux(m, tr, Up, Ap, dx, dy=None):
         du_dx = _d_axis(u, dx, 1)
         dT_dx = _d_axis(T, dx, 1)
         dY_dx = _d_axis(Yf, dx, 1)
-        mu = tr.mu(rho, T)
-        k = tr.kappa(mu, cp)
-        D_k = tr.D(mu, rho, cp_k)
+        mu, mu_t = tr.mu_total(rho, T, dx, None, du_dx, None, None, None)
+        k = tr.kappa(mu, cp, mu_t)
+        D_k = tr.D(mu, rho, cp_k, mu_t)
         div_u = du_dx
         tau_xx = 2 * mu * du_dx - 2 / 3 * mu * div_u
         qx = -k * dT_dx
@@ -1094,9 +1133,9 @@ def viscous_flux(m, tr, Up, Ap, dx, dy=None):
     dv_dx, dv_dy = _d_axis(v, dx, 1), _d_axis(v, dy, 2)
     dT_dx, dT_dy = _d_axis(T, dx, 1), _d_axis(T, dy, 2)
     dY_dx, dY_dy = _d_axis(Yf, dx, 1), _d_axis(Yf, dy, 2)
-    mu = tr.mu(rho, T)
-    k = tr.kappa(mu, cp)
-    D_k = tr.D(mu, rho, cp_k)
+    mu, mu_t = tr.mu_total(rho, T, dx, dy, du_dx, du_dy, dv_dx, dv_dy)
+    k = tr.kappa(mu, cp, mu_t)
+    D_k = tr.D(mu, rho, cp_k, mu_t)
     lam = -2 / 3 * mu
     S12 = 0.5 * (du_dy + dv_dx)
     div_u = du_dx + dv_dy

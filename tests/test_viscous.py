@@ -5,8 +5,8 @@ CPU: set_transport's parsing and errors; the oracle's CENTRAL6 stencils are
 exact on polynomials of their order (pins the restatement without the
 reference); a uniform gas has no viscous flux.
 GPU (through the C ABI): flux_func with viscosity against the oracle for
-each transport model and boundary set (padded corners included), and RK
-steps.  Tolerances: ``fp64_strict`` 1e-12 relative L1 per field (the
+each transport model (laminar and LES with the Vreman sub-grid viscosity)
+and boundary set (padded corners included), and RK steps.  Tolerances: ``fp64_strict`` 1e-12 relative L1 per field (the
 Sutherland law goes through pow), ``fp64`` 1e-11 per flux and 1e-10 over
 steps, ``mixed`` 1e-4 per field and 1e-6 on the density.
 """
@@ -33,6 +33,14 @@ TRANSPORT = {
     "constant_mu_le": {"viscosity_model": "constant", "dynamic_viscosity": 1.5e-5,
                        "thermal_conductivity_model": "constant", "thermal_conductivity": 0.04,
                        "species_diffusivity_model": "Lewis number", "Le": 0.8},
+    # LES with the Vreman sub-grid viscosity (model/LES/Verman.py)
+    "les_pr_le": {"viscosity_model": "Sutherland", "thermal_conductivity_model": "Prandtl number", "Pr": 0.72,
+                  "species_diffusivity_model": "Lewis number", "Le": 1.0, "turbulence_model": "LES",
+                  "LES_model": "Verman", "Pr_t": 0.9, "Le_t": 1.1},
+    "les_constant": {"viscosity_model": "constant", "dynamic_viscosity": 2e-5,
+                     "thermal_conductivity_model": "constant", "thermal_conductivity": 0.05,
+                     "species_diffusivity_model": "constant", "species_diffusivity": 3e-5,
+                     "turbulence_model": "LES", "LES_model": "Verman", "Pr_t": 0.85, "Sc_t": 0.7},
 }
 
 
@@ -65,11 +73,38 @@ def test_transport_config_parsing():
         transport_params({"viscosity_model": "power_law"})
     with pytest.raises(AssertionError):
         transport_params({"viscosity_model": "Sutherland", "thermal_conductivity_model": "Prandtl number"})
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(AssertionError):  # LES needs LES_model, Pr_t and Le_t / Sc_t
         transport_params(dict(TRANSPORT["sutherland_pr_le"], turbulence_model="LES"))
+    les = dict(TRANSPORT["sutherland_pr_le"], turbulence_model="LES", LES_model="Verman", Pr_t=0.9, Sc_t=0.7)
+    t = transport_params(les)
+    assert t.turbulence_model == 1 and t.Pr_t == 0.9 and t.Le_t == 0.7 / 0.9
+    with pytest.raises(KeyError, match="Verman_1D"):
+        transport_params(les, dim=1)
+    with pytest.raises(KeyError, match="WALE_2D"):
+        transport_params(dict(les, LES_model="WALE"))
+    with pytest.raises(KeyError):
+        transport_params(dict(les, turbulence_model="RANS"))
     # the oracle parses the same way
     tr = jo.Transport(TRANSPORT["sutherland_sc"])
     assert tr.Le == 0.5 / 0.7 and tr.D_type == "Lewis number"
+
+
+def test_oracle_vreman_pure_strain_closed_form():
+    """u = a x, v = -a y: B = dx^2 dy^2 a^4, a_ij a_ij = 2 a^2, so
+    mu_t = 0.07 rho dx dy |a| / sqrt(2); simple shear gives mu_t = 0 in the
+    2D form."""
+    tr = jo.Transport(TRANSPORT["les_pr_le"])
+    rho = np.array([[1.3, 0.4]])
+    a = np.array([[250.0, -70.0]])
+    z = np.zeros_like(a)
+    mu, mu_t = tr.mu_total(rho, np.full_like(rho, 900.0), 2e-5, 3e-5, a, z, z, -a)
+    ref = 0.07 * rho * 2e-5 * 3e-5 * np.abs(a) / np.sqrt(2.0)
+    assert np.allclose(mu_t, ref, rtol=1e-13)
+    assert np.allclose(mu, tr.mu(rho, np.full_like(rho, 900.0)) + ref, rtol=1e-13)
+    _, mu_t = tr.mu_total(rho, np.full_like(rho, 900.0), 2e-5, 3e-5, z, a, z, z)
+    assert np.all(mu_t == 0.0)
+    _, mu_t = tr.mu_total(rho, np.full_like(rho, 900.0), 2e-5, 3e-5, z, z, z, z)
+    assert np.all(mu_t == 0.0)  # a_sum = 0: the reference's where() gives 0
 
 
 def test_central6_stencils_exact_on_polynomials():
@@ -148,13 +183,18 @@ def test_viscous_flux_2d_vs_oracle(omech, prec, tkey, combo):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", ["fp64_strict", "fp64", "mixed"])
-def test_viscous_godunov_steps_2d_vs_oracle(omech, prec):
+@pytest.mark.parametrize("tkey", ["sutherland_pr_le", "les_pr_le"])
+def test_viscous_godunov_steps_2d_vs_oracle(omech, prec, tkey):
+    """(``les_constant`` is left to the flux comparison: the reference's
+    constant-diffusivity turbulent term multiplies by cp_k,
+    transport_model.py:153-155, which makes D large enough that the oracle's
+    own steps go non-finite at these sizes.)"""
     from janc_b200.solver import Solver
     nx, ny = 37, 23
     U0, aux0 = _state2d(omech, nx, ny, 4)
     dx = 2e-5
     bc = dict(zip(["left_boundary", "right_boundary", "bottom_boundary", "top_boundary"], COMBOS[1]))
-    tc = TRANSPORT["sutherland_pr_le"]
+    tc = TRANSPORT[tkey]
     o = jo.Solver(omech, "2D", dx, dx, bc, 0.3, flux_config=HLLC_VISC, transport_config=tc)
     U, aux, t = U0, aux0, 0.0
     for _ in range(3):
