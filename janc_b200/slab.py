@@ -135,9 +135,12 @@ class SlabExchange:
 
     # ------------------------------------------------------------ transport
     def _callback(self, user, flags, stream):
+        """The jb_exchange_fn: 0 on success; any failure (a peer that left, a
+        process-group timeout) is kept in ``error`` and returned as 1, which
+        the library reports as a failed call (no GPU wait is involved: the
+        transport blocks on the host)."""
         try:
-            cur = torch.cuda.current_stream(self.send.device)
-            if stream and cur.cuda_stream != stream:
+            if self.send.is_cuda and stream and torch.cuda.current_stream(self.send.device).cuda_stream != stream:
                 with torch.cuda.stream(torch.cuda.ExternalStream(stream, device=self.send.device)):
                     self.transfer(flags)
             else:

@@ -123,6 +123,32 @@ def test_ring_transport_gloo(tmp_path, size):
         assert d["g"].ravel().tolist() == sum(([float(k)] * 2 for k in range(size)), [])
 
 
+def _dead_peer_worker(rank, size, port, out):
+    from janc_b200 import _native
+    from janc_b200.slab import Slab, SlabExchange
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=size,
+                            timeout=datetime.timedelta(seconds=3))
+    try:
+        if rank == 1:
+            return  # leaves between steps, before the exchange
+        x = SlabExchange(Slab(), nv=2, ny=3, device="cpu")
+        rc = x._callback(None, _native.XCH_HALO, None)
+        with open(os.path.join(out, "r0.txt"), "w") as f:
+            f.write(f"{rc} {type(x.error).__name__} {x.calls}")
+    finally:
+        if rank == 0:
+            dist.destroy_process_group()
+
+
+def test_exchange_with_a_departed_peer_fails_on_the_host(tmp_path):
+    """Failure detection on the slab path: the peer never joins the exchange;
+    the group's timeout ends the transfer with an error, which the callback
+    turns into a failed return (the library then fails the call)."""
+    mp.start_processes(_dead_peer_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, start_method="spawn")
+    rc, err, calls = (tmp_path / "r0.txt").read_text().split()
+    assert rc == "1" and calls == "0" and err != "NoneType"
+
+
 def _state2d(om, nx, ny, seed):
     rng = np.random.default_rng(seed)
     P = np.full((1, nx, ny), 101325.0)
