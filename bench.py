@@ -285,17 +285,18 @@ def _setup_workload(args, precision):
         dx, dy = LX / NX, LY / NY
         bc = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
         visc = "on" if args.viscous else "off"
-        fc = {"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS", "split_method": "LF",
+        fc = {"solver_type": "flux_splitting", "interface_reconstruction": args.recon, "split_method": args.flux,
               "viscosity": visc}
-        if args.flux != "LF":
-            fc = {"solver_type": "godunov", "interface_reconstruction": "WENO5_JS",
+        if args.flux not in ("LF", "SW"):
+            fc = {"solver_type": "godunov", "interface_reconstruction": args.recon,
                   "riemann_solver": args.flux, "viscosity": visc}
         tc = ({"viscosity_model": "Sutherland", "thermal_conductivity_model": "Prandtl number", "Pr": 0.72,
                "species_diffusivity_model": "Lewis number", "Le": 1.0} if args.viscous else None)
         s = Solver(2, nx, ny, dx, dy, bc, precision=precision, flux_config=fc, transport_config=tc)
         P, T, Y = c1_fields()
-        scheme = ("WENO5-JS + LF" if args.flux == "LF" else
-                  f"Godunov (WENO5-JS on primitives + {args.flux}, float64)")
+        rname = "WENO5-JS" if args.recon == "WENO5_JS" else "MUSCL (minmod)"
+        scheme = (f"{rname} + LF" if args.flux == "LF" else f"{rname} + Steger-Warming" if args.flux == "SW" else
+                  f"Godunov ({rname} on primitives + {args.flux}, float64)")
         if args.viscous:
             scheme += " + laminar viscous fluxes (Sutherland, Pr 0.72, Le 1, CENTRAL6)"
         workload = ("2D H2-air detonation channel 1024x256 (0.2 m x 0.05 m), 9sp/19r mechanism, "
@@ -540,18 +541,19 @@ def run_ours(args):
         # select, step begin, 3 flux stages (two kernels each in the mixed
         # variant), 2 stage selects, chemistry, final select
         # (+ 4 ghost-strip launches on the RDC workload's outlet / injector sides)
-        "gpu_launches": ((13 if args.precision == "mixed" and args.flux == "LF" else 10)
+        "gpu_launches": ((13 if args.precision == "mixed" and args.flux == "LF" and args.recon == "WENO5_JS"
+                          else 10)
                          + (4 if args.workload == "rdc" else 0) + (9 if args.viscous else 0)) * args.steps,
         "roofline": {"bound": "hbm", "kernel": {
                          "chem": "k_chem (point-implicit chemistry + final Halley)",
-                         "flux": ("k_god2d (WENO5 on primitives + Riemann solver + RK stage + Halley)"
-                                  if args.flux != "LF" else
+                         "flux": ("k_god2d (reconstruction on primitives + Riemann solver + RK stage + Halley)"
+                                  if args.flux not in ("LF", "SW") else
                                   "flux stage: k_sweep_x + k_flux_y_rk (LF + WENO5 + RK stage + Halley)"
-                                  if args.precision == "mixed" else
-                                  "k_flux2d (LF + WENO5 + RK stage + Halley)")}[dom],
+                                  if args.precision == "mixed" and args.flux == "LF" and args.recon == "WENO5_JS"
+                                  else f"k_flux2d ({args.flux} splitting + reconstruction + RK stage + Halley)")}[dom],
                      "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "traffic": (TRAFFIC_PER_CELL[dom] * ncell if args.workload == "channel" and
-                                 args.flux == "LF" and not args.viscous and
+                                 args.flux == "LF" and args.recon == "WENO5_JS" and not args.viscous and
                                  args.precision == "mixed" else None),
                      "traffic_source": "ncu dram bytes of one stage's launches on this workload, each "
                                        "launch cold (mixed precision)",
@@ -1045,9 +1047,11 @@ def main():
     ap.add_argument("--workload", default="channel", choices=["channel", "rdc", "ensemble", "adjoint"])
     ap.add_argument("--viscous", action="store_true",
                     help="channel workload with the laminar viscous fluxes")
-    ap.add_argument("--flux", default="LF", choices=["LF", "HLLC", "AUSMPW_plus"],
-                    help="advective flux of the channel workload (LF flux splitting or a Godunov "
-                         "Riemann solver)")
+    ap.add_argument("--flux", default="LF", choices=["LF", "SW", "HLLC", "AUSMPW_plus"],
+                    help="advective flux of the channel workload (LF or Steger-Warming flux splitting, "
+                         "or a Godunov Riemann solver)")
+    ap.add_argument("--recon", default="WENO5_JS", choices=["WENO5_JS", "MUSCL"],
+                    help="face reconstruction of the channel workload")
     ap.add_argument("--fd-directions", type=int, default=16,
                     help="adjoint: finite-difference directions per kind")
     ap.add_argument("--ens-shape", default="",
