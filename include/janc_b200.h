@@ -155,6 +155,17 @@ typedef int (*jb_exchange_fn)(void* user, int flags, void* stream);
 int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb_exchange_fn fn,
                     void* user);
 
+/* Caller-computed ghost columns on the x sides created with JB_BC_HALO, for
+ * boundary conditions given as functions (boundary/boundary.py:16-21,
+ * 37-42: a callable receives the 3 boundary-adjacent columns of U and aux
+ * and returns the 3 ghost columns).  Before each flux evaluation the handle
+ * packs send[2][nv+2][3][ny] as jb_set_exchange does and calls
+ * fn(user, JB_XCH_HALO, stream); fn writes halo[side] (ghost layer l at
+ * padded column l of the left side, nx + l of the right one).  The padded
+ * corners keep the single-domain periodic wrap; no reduction is asked for.
+ * fn = NULL detaches. */
+int jb_set_ghost_columns(jb_handle* h, double* send, double* halo, jb_exchange_fn fn, void* user);
+
 /* sizeof(jb_mech_params) and sizeof(jb_grid) as compiled, for binding checks. */
 int jb_sizeof_mech_params(void);
 int jb_sizeof_grid(void);

@@ -234,6 +234,8 @@ static int check_theta(jb_handle* h) {
 // for a handle without an exchange.
 static int exchange(jb_handle* h, const double* U, const double* aux, int flags, int aidx, cudaStream_t st) {
   if (!h->xch) return JB_OK;
+  if (!h->grid.halo_ring) flags &= ~JB_XCH_DT;  // one domain: its own CFL minimum
+  if (!flags) return JB_OK;
   const jb::Ops& o = *h->ops;
   JB_TRY(o.xch_pre(h->dim, h->grid, U, aux, h->xsend, h->slots, h->xred, flags, st), "exchange pack");
   const int rc = h->xch(h->xch_user, flags, (void*)st);
@@ -250,6 +252,7 @@ int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb
     h->xsend = nullptr;
     h->xred = nullptr;
     h->grid.halo = nullptr;
+    h->grid.halo_ring = 0;
     return JB_OK;
   }
   if (!send || !halo || !red) return set_err(h, JB_ERR_ARG, "exchange needs send, halo and red buffers");
@@ -259,6 +262,21 @@ int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb
   h->xsend = send;
   h->xred = red;
   h->grid.halo = halo;
+  h->grid.halo_ring = 1;
+  return JB_OK;
+}
+
+int jb_set_ghost_columns(jb_handle* h, double* send, double* halo, jb_exchange_fn fn, void* user) {
+  if (!h) return JB_ERR_ARG;
+  if (!fn) return jb_set_exchange(h, nullptr, nullptr, nullptr, nullptr, nullptr);
+  if (!send || !halo) return set_err(h, JB_ERR_ARG, "ghost columns need send and halo buffers");
+  if (h->grid.nx < 3) return set_err(h, JB_ERR_ARG, "ghost columns need at least 3 columns");
+  h->xch = fn;
+  h->xch_user = user;
+  h->xsend = send;
+  h->xred = nullptr;
+  h->grid.halo = halo;
+  h->grid.halo_ring = 0;
   return JB_OK;
 }
 

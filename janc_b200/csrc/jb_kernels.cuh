@@ -2038,7 +2038,9 @@ __global__ void __launch_bounds__(256) k_halo_pack(Grid g, const double* __restr
 // aidx (flux_splitting/LF.py takes nanmax over the padded array).  A halo
 // side contributes every row; a physical x side of a 2D slab only the rows
 // its padded corners copy (y-periodic wrap: 1..3 and ny-4..ny-2), because the
-// boundary condition overwrites the ghost columns' rows 3:-3 only.
+// boundary condition overwrites the ghost columns' rows 3:-3 only.  Without
+// the ring (caller-computed ghost columns) the corners are the single-domain
+// periodic wrap of interior cells and add nothing.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_halo_alpha(MP m, Grid g, Slots* slots, int aidx) {
   constexpr int nY = DIM == 1 ? 3 : 4;
@@ -2048,7 +2050,7 @@ __global__ void __launch_bounds__(128) k_halo_alpha(MP m, Grid g, Slots* slots, 
   if (t < 6 * g.ny) {
     const int side = t / (3 * g.ny), l = (t / g.ny) % 3, y = t % g.ny;
     const bool corner_row = (y >= 1 && y <= 3) || (y >= g.ny - 4 && y <= g.ny - 2);
-    if (g.bc[side] == JB_BC_HALO || (DIM == 2 && corner_row)) {
+    if (g.bc[side] == JB_BC_HALO || (DIM == 2 && g.halo_ring && corner_row)) {
       double q[nv + 2];
 #pragma unroll
       for (int f = 0; f < nv + 2; ++f) q[f] = g.halo[halo_idx(g, side, l, f, y)];

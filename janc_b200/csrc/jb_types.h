@@ -46,9 +46,10 @@ enum jb_bc_kind {
   JB_BC_NO_SLIP_WALL = 3,
   JB_BC_PRESSURE_OUTLET = 4,
   JB_BC_RDC_INJECTOR = 5,
-  // x side of an x slab that borders another slab (parallel/boundary.py):
-  // its 3 ghost columns are the neighbour's 3 edge columns, exchanged into
-  // the handle's halo buffer before each flux evaluation
+  // x side whose 3 ghost columns come from a buffer filled before each flux
+  // evaluation: an x slab's neighbour columns (parallel/boundary.py), or the
+  // caller's boundary function of the 3 edge columns (a Python callable
+  // boundary, boundary/boundary.py:16-21)
   JB_BC_HALO = 6
 };
 
@@ -118,7 +119,8 @@ typedef struct jb_grid {
   int scheme;            // advective flux (jb_flux_scheme): LF splitting or Godunov + Riemann solver
   int recon;             // face reconstruction (jb_reconstruction): WENO5-JS or MUSCL
   const double* visc;    // viscous rhs of the stage state (ncell x nv) or null: Euler fluxes
-  const double* halo;    // x-slab mode: ghost columns [2][nv+2][3][ny] from the neighbours, else null
+  const double* halo;    // ghost columns [2][nv+2][3][ny] of the JB_BC_HALO x sides, else null
+  int halo_ring;         // 1: x slabs (neighbours' columns, ring corners); 0: caller-computed ghost columns
 } jb_grid;
 
 // Per-step reduction results.  Doubles reduced with atomics are stored as

@@ -29,7 +29,7 @@ __device__ __forceinline__ Src map_padded(const Grid& g, int x, int y) {
     s.pos = 0;
     s.flip = 0;
     s.layer = -1;
-    if (g.halo) {
+    if (g.halo && g.halo_ring) {
       s.kind = 1;
       s.side = x < 0 ? 0 : 1;
       s.layer = x < 0 ? x + 3 : x - g.nx;

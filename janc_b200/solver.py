@@ -103,6 +103,55 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+class _GhostColumns:
+    """Left / right boundary functions (boundary/boundary.py:16-21, 37-42):
+    before each flux evaluation the library packs the 3 boundary-adjacent
+    columns of (U, aux) and calls back here; the function gets them as the
+    reference passes them (``padded_U[:, 3:6(, 3:-3)]`` for the left side,
+    ``[:, -6:-3]`` for the right, as CUDA tensors), with theta, and returns
+    the 3 ghost columns in padded order, which go to the kernels'
+    ghost-column buffer (``jb_set_ghost_columns``)."""
+
+    def __init__(self, solver, fns):
+        shape = (2, solver.nv + 2, 3, solver.ny)
+        self.send = torch.zeros(shape, dtype=torch.float64, device=solver.device)
+        self.halo = torch.zeros(shape, dtype=torch.float64, device=solver.device)
+        self.fns = [fns.get("left_boundary"), fns.get("right_boundary")]
+        self.solver = solver
+        self.error = None
+        self.calls = 0
+        self._fn = _native.EXCHANGE_FN(self._callback)
+
+    def _callback(self, user, flags, stream):
+        try:
+            dev = self.send.device
+            ctx = (torch.cuda.stream(torch.cuda.ExternalStream(stream, device=dev))
+                   if stream and torch.cuda.current_stream(dev).cuda_stream != stream else None)
+            if ctx is not None:
+                with ctx:
+                    self._fill()
+            else:
+                self._fill()
+            self.calls += 1
+            return 0
+        except BaseException as e:  # reported by the library as a failed call
+            self.error = e
+            return 1
+
+    def _fill(self):
+        s = self.solver
+        nv = s.nv
+        for side, fn in enumerate(self.fns):
+            if fn is None:
+                continue
+            Ub, ab = self.send[side, :nv], self.send[side, nv:]
+            if s.dim == 1:
+                Ub, ab = Ub[..., 0], ab[..., 0]
+            Ug, ag = fn(Ub, ab, s._theta)
+            self.halo[side, :nv].copy_(torch.as_tensor(Ug, device=self.send.device).reshape(nv, 3, s.ny))
+            self.halo[side, nv:].copy_(torch.as_tensor(ag, device=self.send.device).reshape(2, 3, s.ny))
+
+
 class Solver:
     """Native solver for a fixed grid.
 
@@ -152,16 +201,24 @@ class Solver:
         self._params = _mech.pack(self.mech)
         bc = boundary_config or {}
         kinds = []
+        ghost_fns = {}
         for key in BOUNDARY_KEYS[: 2 * dim]:
             name = bc.get(key, "periodic")
             if callable(name):
-                raise NotImplementedError(
-                    f"{key}: Python callables cannot run inside the kernels; use a named "
-                    f"boundary ({', '.join(_native.BC_KIND)})")
+                if key in ("bottom_boundary", "top_boundary"):
+                    raise NotImplementedError(
+                        f"{key}: boundary functions are taken on the left and right sides; use a named "
+                        f"boundary ({', '.join(_native.BC_KIND)}) here")
+                ghost_fns[key] = name
+                kinds.append(_native.BC_HALO)
+                continue
             if name not in _native.BC_KIND:
                 raise KeyError(f"{key}: unknown boundary condition {name!r}")
             kinds.append(_native.BC_KIND[name])
         kinds += [0] * (4 - len(kinds))
+        if ghost_fns and slab is not None:
+            raise NotImplementedError("boundary functions on x slabs")
+        self._theta = None
         self.slab = slab
         if slab is not None:
             kinds = slab.boundary_kinds(kinds)
@@ -182,6 +239,10 @@ class Solver:
             from .slab import SlabExchange
             self._exchange = SlabExchange(slab, self.nv, self.ny, self.device)
             self._exchange.attach(L, h)
+        elif ghost_fns:
+            self._exchange = _GhostColumns(self, ghost_fns)
+            _native.check(L.jb_set_ghost_columns(h, _ptr(self._exchange.send), _ptr(self._exchange.halo),
+                                                 self._exchange._fn, None), h, "jb_set_ghost_columns")
         self.flux_scheme = flux_scheme(flux_config)
         _native.check(L.jb_set_flux_scheme(h, _native.FLUX_SCHEME[self.flux_scheme]), h, "jb_set_flux_scheme")
         self.reconstruction = (flux_config or {}).get("interface_reconstruction", "WENO5_JS")
@@ -241,6 +302,7 @@ class Solver:
     def set_theta(self, theta):
         """theta['Pb'] for pressure outlets; theta['Yinj'] (8, nx[, 1]) or (8,)
         for the injector."""
+        self._theta = theta
         if theta is None:
             theta = {}
         Pb = float(theta.get("Pb", 0.0))

@@ -520,6 +520,8 @@ def _bc_side(m, kind, side, Ub, auxb, theta):
     """One side's 3 ghost layers from the 3 boundary-adjacent layers
     (boundary_conditions_{1D,2D}/*.py).  ``side`` in L/R/B/T; layers are
     along axis 1 (L/R) or axis 2 (B/T), ordered as in the padded array."""
+    if callable(kind):  # a user function of the 3 adjacent layers (boundary.py:16-21, 37-42)
+        return kind(Ub, auxb, theta)
     ax = 1 if side in "LR" else 2
     lo = side in "LB"
     two_d = Ub.ndim == 3
