@@ -155,16 +155,20 @@ typedef int (*jb_exchange_fn)(void* user, int flags, void* stream);
 int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb_exchange_fn fn,
                     void* user);
 
-/* Caller-computed ghost columns on the x sides created with JB_BC_HALO, for
+/* Caller-computed ghost layers on the sides created with JB_BC_HALO, for
  * boundary conditions given as functions (boundary/boundary.py:16-21,
- * 37-42: a callable receives the 3 boundary-adjacent columns of U and aux
- * and returns the 3 ghost columns).  Before each flux evaluation the handle
- * packs send[2][nv+2][3][ny] as jb_set_exchange does and calls
- * fn(user, JB_XCH_HALO, stream); fn writes halo[side] (ghost layer l at
- * padded column l of the left side, nx + l of the right one).  The padded
- * corners keep the single-domain periodic wrap; no reduction is asked for.
- * fn = NULL detaches. */
-int jb_set_ghost_columns(jb_handle* h, double* send, double* halo, jb_exchange_fn fn, void* user);
+ * 37-42, 58-63, 79-84: a callable receives the 3 boundary-adjacent layers of
+ * U and aux and returns the 3 ghost layers).  Before each flux evaluation
+ * the handle packs the x sides' edge columns into sendx[2][nv+2][3][ny] (as
+ * jb_set_exchange does) and the y sides' edge rows into
+ * sendy[2][nv+2][nx][3] (bottom: rows 0..2, top: rows ny-3..ny-1), then
+ * calls fn(user, JB_XCH_HALO, stream); fn writes halox[side] / haloy[side]
+ * with ghost layer l at padded position l (left, bottom) or n + l (right,
+ * top), in the same layouts.  The padded corners keep the single-domain
+ * periodic wrap; no reduction is asked for.  Buffers of a direction without
+ * a JB_BC_HALO side may be NULL; fn = NULL detaches. */
+int jb_set_ghost_cells(jb_handle* h, double* sendx, double* halox, double* sendy, double* haloy,
+                       jb_exchange_fn fn, void* user);
 
 /* sizeof(jb_mech_params) and sizeof(jb_grid) as compiled, for binding checks. */
 int jb_sizeof_mech_params(void);

@@ -55,6 +55,7 @@ struct jb_handle {
   jb_exchange_fn xch;
   void* xch_user;
   double* xsend;  // [2][nv+2][3][ny] edge columns packed for the neighbours
+  double* xsendy;   // [2][nv+2][nx][3] edge rows for the bottom / top boundary functions
   long long* xred;  // CFL pair reduced over the ranks
   char err[512];
 };
@@ -136,7 +137,7 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   if (dim == 1) ny = 1;
   if (!(dx > 0.0) || (dim == 2 && !(dy > 0.0))) return JB_ERR_ARG;
   for (int s = 0; s < 2 * dim; ++s)
-    if (!bc_ok(bc[s]) && !(s < 2 && bc[s] == JB_BC_HALO)) return JB_ERR_ARG;
+    if (!bc_ok(bc[s]) && bc[s] != JB_BC_HALO) return JB_ERR_ARG;
   if (dim == 1 && (bc[0] == JB_BC_RDC_INJECTOR || bc[1] == JB_BC_RDC_INJECTOR)) return JB_ERR_UNSUPPORTED;
   if (precision != JB_PREC_STRICT && precision != JB_PREC_FP64 && precision != JB_PREC_MIXED)
     return JB_ERR_UNSUPPORTED;
@@ -237,7 +238,7 @@ static int exchange(jb_handle* h, const double* U, const double* aux, int flags,
   if (!h->grid.halo_ring) flags &= ~JB_XCH_DT;  // one domain: its own CFL minimum
   if (!flags) return JB_OK;
   const jb::Ops& o = *h->ops;
-  JB_TRY(o.xch_pre(h->dim, h->grid, U, aux, h->xsend, h->slots, h->xred, flags, st), "exchange pack");
+  JB_TRY(o.xch_pre(h->dim, h->grid, U, aux, h->xsend, h->xsendy, h->slots, h->xred, flags, st), "exchange pack");
   const int rc = h->xch(h->xch_user, flags, (void*)st);
   if (rc != 0) return set_err(h, JB_ERR_ARG, "exchange transport failed (%d)", rc);
   JB_TRY(o.xch_post(h->dim, h->mech, h->grid, h->slots, h->xred, aidx, flags, st), "exchange unpack");
@@ -251,7 +252,9 @@ int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb
     h->xch_user = nullptr;
     h->xsend = nullptr;
     h->xred = nullptr;
+    h->xsendy = nullptr;
     h->grid.halo = nullptr;
+    h->grid.haloy = nullptr;
     h->grid.halo_ring = 0;
     return JB_OK;
   }
@@ -266,16 +269,23 @@ int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb
   return JB_OK;
 }
 
-int jb_set_ghost_columns(jb_handle* h, double* send, double* halo, jb_exchange_fn fn, void* user) {
+int jb_set_ghost_cells(jb_handle* h, double* sendx, double* halox, double* sendy, double* haloy,
+                       jb_exchange_fn fn, void* user) {
   if (!h) return JB_ERR_ARG;
   if (!fn) return jb_set_exchange(h, nullptr, nullptr, nullptr, nullptr, nullptr);
-  if (!send || !halo) return set_err(h, JB_ERR_ARG, "ghost columns need send and halo buffers");
-  if (h->grid.nx < 3) return set_err(h, JB_ERR_ARG, "ghost columns need at least 3 columns");
+  const jb_grid& g = h->grid;
+  const bool hx = g.bc[0] == JB_BC_HALO || g.bc[1] == JB_BC_HALO;
+  const bool hy = h->dim == 2 && (g.bc[2] == JB_BC_HALO || g.bc[3] == JB_BC_HALO);
+  if (hx && (!sendx || !halox)) return set_err(h, JB_ERR_ARG, "x ghost sides need sendx and halox buffers");
+  if (hy && (!sendy || !haloy)) return set_err(h, JB_ERR_ARG, "y ghost sides need sendy and haloy buffers");
+  if (!hx && !hy) return set_err(h, JB_ERR_ARG, "no side was created with JB_BC_HALO");
   h->xch = fn;
   h->xch_user = user;
-  h->xsend = send;
+  h->xsend = hx ? sendx : nullptr;
+  h->xsendy = hy ? sendy : nullptr;
   h->xred = nullptr;
-  h->grid.halo = halo;
+  h->grid.halo = hx ? halox : nullptr;
+  h->grid.haloy = hy ? haloy : nullptr;
   h->grid.halo_ring = 0;
   return JB_OK;
 }

@@ -601,7 +601,11 @@ __device__ __forceinline__ Src map_cell(const Grid& g, int x, int y) {
     int cs, flip;
     bool strip;
     map_axis(y, g.ny, g.bc[side], lo, cs, flip, strip, 2, DIM);
-    if (strip) { s.kind = 1; s.side = side; s.pos = x; return s; }
+    if (strip) {
+      s.kind = 1; s.side = side; s.pos = x;
+      if (g.bc[side] == JB_BC_HALO) s.layer = lo ? y + 3 : y - g.ny;
+      return s;
+    }
     s.kind = 0; s.xs = x; s.ys = cs; s.flip = flip;
     return s;
   }
@@ -617,9 +621,15 @@ __device__ __forceinline__ size_t halo_idx(const Grid& g, int side, int layer, i
   return (((size_t)side * (g.nv + 2) + q) * 3 + layer) * g.ny + y;
 }
 
+// haloy[2][nv+2][nx][3]: y side - 2, field, column, ghost layer
+__device__ __forceinline__ size_t haloy_idx(const Grid& g, int side, int layer, int q, int x) {
+  return (((size_t)(side - 2) * (g.nv + 2) + q) * g.nx + x) * 3 + layer;
+}
+
 // Field q (U..., gamma at nv, T at nv + 1) of a kind-1 ghost.
 __device__ __forceinline__ double ghost(const Grid& g, const double* strips, const Src& s, int q) {
-  return s.layer < 0 ? strips[strip_idx(g, s.side, q, s.pos)] : g.halo[halo_idx(g, s.side, s.layer, q, s.pos)];
+  if (s.layer < 0) return strips[strip_idx(g, s.side, q, s.pos)];
+  return s.side < 2 ? g.halo[halo_idx(g, s.side, s.layer, q, s.pos)] : g.haloy[haloy_idx(g, s.side, s.layer, q, s.pos)];
 }
 
 // LF split flux F(f) of one cell in direction dir (0: x, 1: y) as the
@@ -2032,6 +2042,43 @@ __global__ void __launch_bounds__(256) k_halo_pack(Grid g, const double* __restr
   const int side = (int)(r / (g.nv + 2));
   const long long c = (long long)(side == 0 ? l : g.nx - 3 + l) * g.ny + y;
   send[i] = q < g.nv ? U[q * g.ncell + c] : aux[(q - g.nv) * g.ncell + c];
+}
+
+// The 3 edge rows of each y side of (U, aux) as send[2][nv+2][nx][3]:
+// side 0 (bottom) rows 0..2, side 1 (top) rows ny-3..ny-1.
+__global__ void __launch_bounds__(256) k_halo_pack_y(Grid g, const double* __restrict__ U,
+                                                     const double* __restrict__ aux, double* __restrict__ send) {
+  const long long n = 6LL * (g.nv + 2) * g.nx;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int l = (int)(i % 3);
+  long long r = i / 3;
+  const int x = (int)(r % g.nx);
+  r /= g.nx;
+  const int q = (int)(r % (g.nv + 2));
+  const int side = (int)(r / (g.nv + 2));
+  const long long c = (long long)x * g.ny + (side == 0 ? l : g.ny - 3 + l);
+  send[i] = q < g.nv ? U[q * g.ncell + c] : aux[(q - g.nv) * g.ncell + c];
+}
+
+// Wave speeds of caller-computed ghost rows (JB_BC_HALO y sides) into the
+// alpha maxima of slot aidx: every row of both ghost layers' columns.
+__global__ void __launch_bounds__(128) k_halo_alpha_y(MP m, Grid g, Slots* slots, int aidx) {
+  constexpr int nv = 12;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double amx = 0.0, amy = 0.0;
+  if (t < 6 * g.nx) {
+    const int side = 2 + t / (3 * g.nx), x = (t / 3) % g.nx, l = t % 3;
+    if (g.bc[side] == JB_BC_HALO) {
+      double q[nv + 2];
+#pragma unroll
+      for (int f = 0; f < nv + 2; ++f) q[f] = g.haloy[haloy_idx(g, side, l, f, x)];
+      Prim<2> pr = u_to_prim<2>(m, q, q[nv], q[nv + 1]);
+      amx = fabs(pr.u) + pr.a;
+      amy = fabs(pr.v) + pr.a;
+    }
+  }
+  block_reduce_store(amx, amy, 0.0, 0u, slots, aidx, true, false, -1);
 }
 
 // Wave speeds of the received ghost columns into the LF alpha maxima of slot

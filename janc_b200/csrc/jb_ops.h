@@ -41,11 +41,11 @@ struct Ops {
   cudaError_t (*step_begin)(jb_slots* s, double cfl, double dt_fixed, double* dt_hist, int step,
                             cudaStream_t st);
   cudaError_t (*dt_from_slots)(const jb_slots* s, double cfl, double* dt_out, cudaStream_t st);
-  // x-slab exchange (jb_exchange_flags): pack the CFL pair into red and the
-  // edge columns of (U, aux) into send; after the exchange, unpack the pair
-  // and fold the received halo columns' wave speeds into alpha slot aidx
+  // exchange (jb_exchange_flags): pack the CFL pair into red and the edge
+  // columns (rows) of (U, aux) into send (sendy); after the exchange,
+  // unpack the pair and fold the ghost layers' wave speeds into alpha slot aidx
   cudaError_t (*xch_pre)(int dim, const jb_grid& g, const double* U, const double* aux, double* send,
-                         const jb_slots* slots, long long* red, int flags, cudaStream_t st);
+                         double* sendy, const jb_slots* slots, long long* red, int flags, cudaStream_t st);
   cudaError_t (*xch_post)(int dim, const jb_mech_params& m, const jb_grid& g, jb_slots* slots,
                           const long long* red, int aidx, int flags, cudaStream_t st);
 };

@@ -46,9 +46,9 @@ enum jb_bc_kind {
   JB_BC_NO_SLIP_WALL = 3,
   JB_BC_PRESSURE_OUTLET = 4,
   JB_BC_RDC_INJECTOR = 5,
-  // x side whose 3 ghost columns come from a buffer filled before each flux
+  // side whose 3 ghost layers come from a buffer filled before each flux
   // evaluation: an x slab's neighbour columns (parallel/boundary.py), or the
-  // caller's boundary function of the 3 edge columns (a Python callable
+  // caller's boundary function of the 3 edge layers (a Python callable
   // boundary, boundary/boundary.py:16-21)
   JB_BC_HALO = 6
 };
@@ -121,6 +121,7 @@ typedef struct jb_grid {
   const double* visc;    // viscous rhs of the stage state (ncell x nv) or null: Euler fluxes
   const double* halo;    // ghost columns [2][nv+2][3][ny] of the JB_BC_HALO x sides, else null
   int halo_ring;         // 1: x slabs (neighbours' columns, ring corners); 0: caller-computed ghost columns
+  const double* haloy;   // ghost rows [2][nv+2][nx][3] of JB_BC_HALO y sides (caller-computed), else null
 } jb_grid;
 
 // Per-step reduction results.  Doubles reduced with atomics are stored as

@@ -103,32 +103,36 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-class _GhostColumns:
-    """Left / right boundary functions (boundary/boundary.py:16-21, 37-42):
+class _GhostCells:
+    """Boundary functions (boundary/boundary.py:16-21, 37-42, 58-63, 79-84):
     before each flux evaluation the library packs the 3 boundary-adjacent
-    columns of (U, aux) and calls back here; the function gets them as the
-    reference passes them (``padded_U[:, 3:6(, 3:-3)]`` for the left side,
-    ``[:, -6:-3]`` for the right, as CUDA tensors), with theta, and returns
-    the 3 ghost columns in padded order, which go to the kernels'
-    ghost-column buffer (``jb_set_ghost_columns``)."""
+    layers of (U, aux) and calls back here; each function gets them as the
+    reference passes them (left ``padded_U[:, 3:6(, 3:-3)]``, right
+    ``[:, -6:-3]``, bottom ``[:, 3:-3, 3:6]``, top ``[:, 3:-3, -6:-3]``, as
+    CUDA tensors) with theta, and returns the 3 ghost layers in padded
+    order, which go to the kernels' ghost buffers (``jb_set_ghost_cells``)."""
 
     def __init__(self, solver, fns):
-        shape = (2, solver.nv + 2, 3, solver.ny)
-        self.send = torch.zeros(shape, dtype=torch.float64, device=solver.device)
-        self.halo = torch.zeros(shape, dtype=torch.float64, device=solver.device)
-        self.fns = [fns.get("left_boundary"), fns.get("right_boundary")]
+        nv, nx, ny, dev = solver.nv, solver.nx, solver.ny, solver.device
+        self.sendx = torch.zeros((2, nv + 2, 3, ny), dtype=torch.float64, device=dev)
+        self.halox = torch.zeros_like(self.sendx)
+        self.sendy = torch.zeros((2, nv + 2, nx, 3), dtype=torch.float64, device=dev)
+        self.haloy = torch.zeros_like(self.sendy)
+        self.fns = [fns.get(k) for k in BOUNDARY_KEYS]
         self.solver = solver
         self.error = None
         self.calls = 0
         self._fn = _native.EXCHANGE_FN(self._callback)
 
+    def attach(self, lib, h):
+        _native.check(lib.jb_set_ghost_cells(h, _ptr(self.sendx), _ptr(self.halox), _ptr(self.sendy),
+                                             _ptr(self.haloy), self._fn, None), h, "jb_set_ghost_cells")
+
     def _callback(self, user, flags, stream):
         try:
-            dev = self.send.device
-            ctx = (torch.cuda.stream(torch.cuda.ExternalStream(stream, device=dev))
-                   if stream and torch.cuda.current_stream(dev).cuda_stream != stream else None)
-            if ctx is not None:
-                with ctx:
+            dev = self.sendx.device
+            if stream and torch.cuda.current_stream(dev).cuda_stream != stream:
+                with torch.cuda.stream(torch.cuda.ExternalStream(stream, device=dev)):
                     self._fill()
             else:
                 self._fill()
@@ -144,12 +148,14 @@ class _GhostColumns:
         for side, fn in enumerate(self.fns):
             if fn is None:
                 continue
-            Ub, ab = self.send[side, :nv], self.send[side, nv:]
+            send, halo = (self.sendx, self.halox) if side < 2 else (self.sendy, self.haloy)
+            b = side % 2
+            Ub, ab = send[b, :nv], send[b, nv:]
             if s.dim == 1:
                 Ub, ab = Ub[..., 0], ab[..., 0]
             Ug, ag = fn(Ub, ab, s._theta)
-            self.halo[side, :nv].copy_(torch.as_tensor(Ug, device=self.send.device).reshape(nv, 3, s.ny))
-            self.halo[side, nv:].copy_(torch.as_tensor(ag, device=self.send.device).reshape(2, 3, s.ny))
+            halo[b, :nv].copy_(torch.as_tensor(Ug, device=halo.device).reshape(halo[b, :nv].shape))
+            halo[b, nv:].copy_(torch.as_tensor(ag, device=halo.device).reshape(halo[b, nv:].shape))
 
 
 class Solver:
@@ -205,10 +211,6 @@ class Solver:
         for key in BOUNDARY_KEYS[: 2 * dim]:
             name = bc.get(key, "periodic")
             if callable(name):
-                if key in ("bottom_boundary", "top_boundary"):
-                    raise NotImplementedError(
-                        f"{key}: boundary functions are taken on the left and right sides; use a named "
-                        f"boundary ({', '.join(_native.BC_KIND)}) here")
                 ghost_fns[key] = name
                 kinds.append(_native.BC_HALO)
                 continue
@@ -240,9 +242,8 @@ class Solver:
             self._exchange = SlabExchange(slab, self.nv, self.ny, self.device)
             self._exchange.attach(L, h)
         elif ghost_fns:
-            self._exchange = _GhostColumns(self, ghost_fns)
-            _native.check(L.jb_set_ghost_columns(h, _ptr(self._exchange.send), _ptr(self._exchange.halo),
-                                                 self._exchange._fn, None), h, "jb_set_ghost_columns")
+            self._exchange = _GhostCells(self, ghost_fns)
+            self._exchange.attach(L, h)
         self.flux_scheme = flux_scheme(flux_config)
         _native.check(L.jb_set_flux_scheme(h, _native.FLUX_SCHEME[self.flux_scheme]), h, "jb_set_flux_scheme")
         self.reconstruction = (flux_config or {}).get("interface_reconstruction", "WENO5_JS")

@@ -1,14 +1,16 @@
-"""Boundary conditions given as functions on the left / right sides
-(boundary/boundary.py:16-21, 37-42): the function receives the 3
-boundary-adjacent columns of U and aux (``padded[:, 3:6(, 3:-3)]`` on the
-left, ``[:, -6:-3]`` on the right) and theta, and returns the 3 ghost
-columns in padded order.  The library packs the columns and calls back
-before each flux evaluation (``jb_set_ghost_columns``); the kernels read the
-ghost columns as they read any ghost state.
+"""Boundary conditions given as functions (boundary/boundary.py:16-21,
+37-42, 58-63, 79-84): the function receives the 3 boundary-adjacent layers
+of U and aux (``padded[:, 3:6, 3:-3]`` left, ``[:, -6:-3, 3:-3]`` right,
+``[:, 3:-3, 3:6]`` bottom, ``[:, 3:-3, -6:-3]`` top; 1D without the second
+index) and theta, and returns the 3 ghost layers in padded order.  The
+library packs the layers and calls back before each flux evaluation
+(``jb_set_ghost_cells``); the kernels read the ghost layers as they read
+any ghost state.
 
 GPU: flux_func and RK steps against the oracle, which calls the same
-functions on NumPy arrays, in 2D (LF, HLLC, viscous: the padded corners keep
-the periodic wrap) and 1D.  Tolerances: ``fp64_strict`` 1e-13 relative L1
+functions on NumPy arrays, in 2D (functions on all four sides or mixed with
+named sides; LF, HLLC, viscous: the padded corners keep the periodic wrap)
+and 1D.  Tolerances: ``fp64_strict`` 1e-13 relative L1
 per field for one flux and 1e-12 over steps; ``fp64`` 1e-12 and 1e-10;
 ``mixed`` 1e-4 per field and 1e-6 on the density against ``fp64``.
 """
@@ -20,8 +22,10 @@ torch = pytest.importorskip("torch")
 from oracle import janc_oracle as jo  # noqa: E402
 
 
-def _flip(a):
-    return a.flip(1) if hasattr(a, "flip") and not isinstance(a, np.ndarray) else a[:, ::-1]
+def _flip(a, axis=1):
+    if isinstance(a, np.ndarray):
+        return np.flip(a, axis=axis)
+    return a.flip(axis)
 
 
 def _like(a, v):
@@ -45,6 +49,22 @@ def reflect(U, aux, theta=None):
     Ug = _flip(U) * 1.0
     Ug[1] = -Ug[1]
     return Ug, _flip(aux) * 1.0
+
+
+def make_inflow_y(U_in, aux_in):
+    """Bottom: the inflow state (momentum along y) in all three ghost rows."""
+    def bottom(U, aux, theta=None):
+        Ug = U * 0 + _like(U, U_in.reshape(-1, 1, 1))
+        ag = aux * 0 + _like(aux, aux_in.reshape(-1, 1, 1))
+        return Ug, ag
+    return bottom
+
+
+def reflect_y(U, aux, theta=None):
+    """Bottom or top: mirror the three rows with the y momentum negated."""
+    Ug = _flip(U, 2) * 1.0
+    Ug[2] = -Ug[2]
+    return Ug, _flip(aux, 2) * 1.0
 
 
 def field_err(a, b):
@@ -81,6 +101,13 @@ def _case(om, dim, seed=3):
     return U, aux, Ui[:, 0], ai[:, 0]
 
 
+def _inflow_y(om):
+    one = np.ones((1, 1))
+    Ui, ai = jo.state_from_PTY(om, 2 * 101325.0 * one, 500.0 * one, jo.stoich_Y(om, 1.0)[:, None],
+                               vel=[0.0 * one, 150.0 * one])
+    return Ui[:, 0], ai[:, 0]
+
+
 CASES = {"lf": None,
          "hllc": {"solver_type": "godunov", "interface_reconstruction": "WENO5_JS", "riemann_solver": "HLLC",
                   "viscosity": "off"},
@@ -101,7 +128,14 @@ def test_boundary_functions_vs_oracle(omech, prec, case, dim):
     U0, a0, Ui, ai = _case(omech, dim)
     left = make_inflow(Ui, ai)
     keys = ["left_boundary", "right_boundary", "bottom_boundary", "top_boundary"][: 2 * dim]
-    bc = dict(zip(keys, [left, reflect, "slip_wall", "slip_wall"]))
+    if dim == 2 and case == "lf":  # functions on all four sides
+        Uy, ay = _inflow_y(omech)
+        sides = [left, reflect, make_inflow_y(Uy, ay), reflect_y]
+    elif dim == 2 and case == "visc":  # mixed with a named side
+        sides = [left, reflect, reflect_y, "slip_wall"]
+    else:
+        sides = [left, reflect, "slip_wall", "slip_wall"]
+    bc = dict(zip(keys, sides))
     dx = 5e-5
     fc, tc = CASES[case], (TC if case == "visc" else None)
     o = jo.Solver(omech, "2D" if dim == 2 else "1D", dx, dx if dim == 2 else None, bc, 0.4, flux_config=fc,
@@ -136,10 +170,10 @@ def test_boundary_function_errors_propagate(omech):
         s.flux_func(torch.as_tensor(U0, device="cuda"), torch.as_tensor(a0, device="cuda"), 5e-5, None, 1e-8)
 
 
-def test_bottom_top_functions_refused():
+def test_set_boundary_takes_functions_on_every_side():
     from janc_b200.janc.boundary import boundary
-    with pytest.raises(NotImplementedError):
-        boundary.set_boundary({"left_boundary": "slip_wall", "right_boundary": "slip_wall",
-                               "bottom_boundary": reflect, "top_boundary": "slip_wall"}, "2D")
     boundary.set_boundary({"left_boundary": reflect, "right_boundary": "slip_wall",
-                           "bottom_boundary": "slip_wall", "top_boundary": "slip_wall"}, "2D")
+                           "bottom_boundary": reflect_y, "top_boundary": reflect_y}, "2D")
+    with pytest.raises(KeyError):
+        boundary.set_boundary({"left_boundary": "inflow", "right_boundary": "slip_wall",
+                               "bottom_boundary": "slip_wall", "top_boundary": "slip_wall"}, "2D")

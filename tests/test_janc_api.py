@@ -78,8 +78,8 @@ def test_config_errors_raise_like_reference(tmp_path):
         Simulator(cfg)  # missing boundary sides
     bad = sim_config("2D", {"dx": 1e-4, "dy": 1e-4},
                      {"left_boundary": "slip_wall", "right_boundary": "slip_wall",
-                      "bottom_boundary": lambda U, a, t: (U, a), "top_boundary": "slip_wall"})
-    with pytest.raises(NotImplementedError):
+                      "bottom_boundary": "inflow", "top_boundary": "slip_wall"})
+    with pytest.raises(KeyError):
         Simulator(bad)
 
 
