@@ -155,6 +155,13 @@ typedef int (*jb_exchange_fn)(void* user, int flags, void* stream);
 int jb_set_exchange(jb_handle* h, double* send, double* halo, long long* red, jb_exchange_fn fn,
                     void* user);
 
+/* The ghost-padded arrays (replaces boundary_conditions_1D / _2D,
+ * boundary/boundary.py:120-132, and parallel/boundary.py:6-25 on a slab):
+ * Up [nv][nx+6][ny+6] and auxp [2][nx+6][ny+6] (1D: [nv][nx+6], [2][nx+6]),
+ * every entry as the flux kernels see it, padded corners included. */
+int jb_boundary_conditions(jb_handle* h, const double* U, const double* aux, double* Up, double* auxp,
+                           void* stream);
+
 /* Caller-computed ghost layers on the sides created with JB_BC_HALO, for
  * boundary conditions given as functions (boundary/boundary.py:16-21,
  * 37-42, 58-63, 79-84: a callable receives the 3 boundary-adjacent layers of

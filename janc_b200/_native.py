@@ -24,7 +24,7 @@ STATUS = {1: "bad argument", 2: "CUDA error", 4: "non-finite state", 8: "singula
 
 EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_func", "jb_update_aux",
            "jb_reaction_source_terms", "jb_advance", "jb_cfl_dt", "jb_get_thermo", "jb_status",
-           "jb_workspace_bytes", "jb_set_spacing", "jb_set_flux_scheme", "jb_set_reconstruction", "jb_set_transport", "jb_set_exchange", "jb_set_ghost_cells",
+           "jb_workspace_bytes", "jb_set_spacing", "jb_set_flux_scheme", "jb_set_reconstruction", "jb_set_transport", "jb_set_exchange", "jb_set_ghost_cells", "jb_boundary_conditions",
            "jb_sizeof_mech_params",
            "jb_sizeof_grid",
            "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times",
@@ -86,6 +86,7 @@ def lib(path=None):
     L.jb_set_transport.argtypes = [vp, ctypes.POINTER(Transport)]
     L.jb_set_exchange.argtypes = [vp, dp, dp, dp, EXCHANGE_FN, vp]
     L.jb_set_ghost_cells.argtypes = [vp, dp, dp, dp, dp, EXCHANGE_FN, vp]
+    L.jb_boundary_conditions.argtypes = [vp, dp, dp, dp, dp, vp]
     L.jb_probe_fp64_fma.argtypes = [i, i, dp, vp]
     L.jb_set_kernel_timing.argtypes = [vp, i]
     L.jb_update_aux_noalloc.argtypes = [ctypes.POINTER(_mech.MechParams), i, i, i, i, dp, dp, dp, vp]

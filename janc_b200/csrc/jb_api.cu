@@ -309,6 +309,22 @@ int jb_flux_func(jb_handle* h, const double* U, const double* aux, double dt, do
   return JB_OK;
 }
 
+int jb_boundary_conditions(jb_handle* h, const double* U, const double* aux, double* Up, double* auxp,
+                           void* stream) {
+  if (!h || !U || !aux || !Up || !auxp) return set_err(h, JB_ERR_ARG, "null pointer");
+  if (int rc = check_theta(h)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const jb::Ops& o = *h->ops;
+  // the ghost strips (outlet / injector states) and ghost layers of (U, aux)
+  JB_TRY(o.slots_reset(h->slots, st), "slots_reset");
+  JB_TRY(o.select(h->dim, false, true, false, h->mech, h->grid, U, aux, nullptr, nullptr, h->strips, h->slots,
+                  -1, 3, nullptr, st),
+         "strips");
+  if (int rc = exchange(h, U, aux, JB_XCH_HALO, 3, st)) return rc;
+  JB_TRY(o.pad(h->dim, h->grid, U, aux, h->strips, Up, auxp, st), "pad");
+  return JB_OK;
+}
+
 int jb_update_aux(jb_handle* h, const double* U, const double* aux_in, double* aux_out,
                   void* stream) {
   if (!h || !U || !aux_in || !aux_out) return set_err(h, JB_ERR_ARG, "null pointer");

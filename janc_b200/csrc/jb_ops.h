@@ -48,6 +48,9 @@ struct Ops {
                          double* sendy, const jb_slots* slots, long long* red, int flags, cudaStream_t st);
   cudaError_t (*xch_post)(int dim, const jb_mech_params& m, const jb_grid& g, jb_slots* slots,
                           const long long* red, int aidx, int flags, cudaStream_t st);
+  // ghost-padded copies of (U, aux) (the ghost strips and ghost layers must be current)
+  cudaError_t (*pad)(int dim, const jb_grid& g, const double* U, const double* aux, const double* strips,
+                     double* Up, double* auxp, cudaStream_t st);
 };
 
 // Doubles of the viscous scratch (node planes and node fluxes) of a grid.

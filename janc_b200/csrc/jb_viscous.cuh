@@ -339,3 +339,40 @@ __global__ void __launch_bounds__(128) k_visc_div(Grid g, const double* __restri
     V[f * nc + c] = r;
   }
 }
+
+// The ghost-padded arrays themselves (boundary/boundary.py:120-132,
+// boundary_conditions_{1D,2D}): every padded entry from the same mapping
+// the stencils read, corners included (their periodic wrap, or the ring's
+// on an x slab).  Up [nv][nx+6][ny+6], auxp [2][nx+6][ny+6] (1D: [.][nx+6]).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_pad(Grid g, const double* __restrict__ U, const double* __restrict__ aux,
+                                             const double* __restrict__ strips, double* __restrict__ Up,
+                                             double* __restrict__ auxp) {
+  constexpr int nv = DIM == 1 ? 11 : 12;
+  const int PY = DIM == 2 ? g.ny + 6 : 1;
+  const long long np = (long long)(g.nx + 6) * PY;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int px = (int)(i / PY), py = (int)(i % PY);
+  const Src s = map_padded<DIM>(g, px - 3, DIM == 2 ? py - 3 : 0);
+  const long long nc = g.ncell;
+  if (s.kind == 0) {
+    const long long c = DIM == 2 ? (long long)s.xs * g.ny + s.ys : s.xs;
+#pragma unroll
+    for (int f = 0; f < nv; ++f) {
+      const double v = U[f * nc + c];
+      Up[f * np + i] = ((s.flip >> f) & 1) ? -v : v;
+    }
+    auxp[i] = aux[c];
+    auxp[np + i] = aux[nc + c];
+  } else if (s.kind == 1) {
+#pragma unroll
+    for (int f = 0; f < nv; ++f) Up[f * np + i] = ghost(g, strips, s, f);
+    auxp[i] = ghost(g, strips, s, nv);
+    auxp[np + i] = ghost(g, strips, s, nv + 1);
+  } else {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int f = 0; f < nv; ++f) Up[f * np + i] = nan;
+    auxp[i] = auxp[np + i] = nan;
+  }
+}

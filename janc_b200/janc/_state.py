@@ -46,6 +46,50 @@ def solver_for(shape, dx=1.0, dy=1.0):
     return s
 
 
+class _Padded:
+    """The ghost layers of the padded arrays a padded-input flux call was
+    given, served to the solver as its boundary functions."""
+    Up = None
+    Ap = None
+
+    @staticmethod
+    def side(k):
+        def fn(U, aux, theta=None):
+            Up, Ap = _Padded.Up, _Padded.Ap
+            one_d = Up.ndim == 2
+            sl = {"left_boundary": (slice(0, 3),) if one_d else (slice(0, 3), slice(3, -3)),
+                  "right_boundary": (slice(-3, None),) if one_d else (slice(-3, None), slice(3, -3)),
+                  "bottom_boundary": (slice(3, -3), slice(0, 3)),
+                  "top_boundary": (slice(3, -3), slice(-3, None))}[k]
+            return Up[(slice(None),) + sl], Ap[(slice(None),) + sl]
+        return fn
+
+
+_PADDED_FNS = {k: _Padded.side(k) for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
+
+
+def solver_for_padded(Up, Ap, dx=1.0, dy=1.0):
+    """Cached native solver that takes its ghost layers from the padded
+    arrays (Up, Ap) of a total_flux call; returns the solver and the
+    contiguous interior (U, aux)."""
+    from ..solver import Solver
+    dim = Up.ndim - 1
+    shape = tuple(n - 6 for n in Up.shape[1:])
+    key = ("padded", dim, shape, config["precision"], config["mechanism"], repr(config["nondim"]),
+           repr(config["flux"]), repr(config["transport"]))
+    s = _solvers.get(key)
+    if s is None:
+        keys = ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")[: 2 * dim]
+        s = Solver(dim, shape[0], shape[1] if dim == 2 else None, dx, dy if dim == 2 else None,
+                   {k: _PADDED_FNS[k] for k in keys}, mechanism(), precision=config["precision"],
+                   flux_config=config["flux"], transport_config=config["transport"])
+        _solvers[key] = s
+    s._spacing(dx, dy if dim == 2 else None)
+    _Padded.Up, _Padded.Ap = Up, Ap
+    inner = (slice(None), slice(3, -3)) + ((slice(3, -3),) if dim == 2 else ())
+    return s, Up[inner].contiguous(), Ap[inner].contiguous()
+
+
 def reset_solvers():
     for s in _solvers.values():
         s.close()

@@ -23,3 +23,22 @@ def set_boundary(boundary_config, dim):
         bc[k] = v
     _state.config["boundary"] = bc
     _state.config["dim"] = dim
+
+
+def _padded(U, aux, theta):
+    Ud, kind = _state.to_device(U)
+    ad, _ = _state.to_device(aux)
+    s = _state.solver_for(tuple(Ud.shape[1:]))
+    Up, Ap = s.boundary_conditions(Ud, ad, theta)
+    return _state.back(Up, kind), _state.back(Ap, kind)
+
+
+def boundary_conditions_1D(U, aux, theta=None):
+    """boundary.py:120-124: the ghost-padded (U, aux), (nv, nx+6), (2, nx+6)."""
+    return _padded(U, aux, theta)
+
+
+def boundary_conditions_2D(U, aux, theta=None):
+    """boundary.py:126-132: the ghost-padded (U, aux), (nv, nx+6, ny+6),
+    (2, nx+6, ny+6), corners included."""
+    return _padded(U, aux, theta)

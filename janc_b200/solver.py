@@ -362,6 +362,19 @@ class Solver:
                     "jb_flux_func")
         return out
 
+    def boundary_conditions(self, U, aux, theta=None):
+        """boundary_conditions_1D / _2D (boundary/boundary.py:120-132; on a
+        slab parallel/boundary.py): the ghost-padded (U, aux), (nv, nx+6[,
+        ny+6]) and (2, nx+6[, ny+6]), corners included."""
+        self._check_state(U, aux)
+        self.set_theta(theta)
+        pad = (self.nx + 6,) + ((self.ny + 6,) if self.dim == 2 else ())
+        Up = torch.empty((self.nv,) + pad, dtype=torch.float64, device=U.device)
+        Ap = torch.empty((2,) + pad, dtype=torch.float64, device=U.device)
+        self._check(self._lib.jb_boundary_conditions(self._h, _ptr(U), _ptr(aux), _ptr(Up), _ptr(Ap), _stream()),
+                    "jb_boundary_conditions")
+        return Up, Ap
+
     def update_aux(self, U, aux):
         """aux_func.update_aux: (gamma, T) from the Halley solve."""
         self._check_state(U, aux)

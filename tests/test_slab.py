@@ -258,10 +258,13 @@ def _gpu_worker(rank, size, port, out, case, precs):
             s = Solver(dim, nx // size, ny, dx, dx if dim == 2 else None, _case_bc(case), precision=prec,
                        flux_config=fc, transport_config=TRANSPORT.get(tkey), slab=slab)
             rhs = s.flux_func(Ul, al, dx, dx if dim == 2 else None, 1e-8, theta)
+            Upad, Apad = s.boundary_conditions(Ul, al, theta)
+            calls0 = s._exchange.calls
             Uo, ao, dts = s.advance(Ul, al, steps, cfl=0.4, theta=theta)
             torch.cuda.synchronize()
             np.savez(os.path.join(out, f"{prec}_{rank}.npz"), rhs=rhs.cpu().numpy(), U=Uo.cpu().numpy(),
-                     aux=ao.cpu().numpy(), dts=dts.cpu().numpy(), status=s.status(), calls=s._exchange.calls)
+                     aux=ao.cpu().numpy(), dts=dts.cpu().numpy(), status=s.status(),
+                     calls=s._exchange.calls - calls0 + 1, Upad=Upad.cpu().numpy(), Apad=Apad.cpu().numpy())
             s.close()
     finally:
         dist.destroy_process_group()
@@ -293,6 +296,8 @@ def test_slabs_vs_oracle(omech, tmp_path, case, size, precs):
     mp.start_processes(_gpu_worker, args=(size, _free_port(), str(tmp_path), case, precs), nprocs=size,
                        start_method="spawn")
     rhs, Us, As, dts = _oracle_run(omech, case, size)
+    U0, a0 = _case_state(omech, case)
+    Us0, As0 = np.split(U0, size, axis=1), np.split(a0, size, axis=1)
     steps = CASES[case][6]
     for prec in precs:
         tol = {"fp64_strict": 1e-12, "fp64": 1e-10, "mixed": 1e-4}[prec]
@@ -306,6 +311,10 @@ def test_slabs_vs_oracle(omech, tmp_path, case, size, precs):
             assert np.max(np.abs(d["dts"] - np.array(dts)) / np.array(dts)) < (1e-6 if prec == "mixed" else tol)
             if prec != "mixed":
                 assert field_err(d["rhs"], rhs[r]) < (1e-12 if prec == "fp64_strict" else 1e-11)
+            if prec == "fp64_strict":  # parallel/boundary.py padding, ring corners included
+                Ur, Ar = jo.parallel_boundary_conditions(omech, Us0, As0, r, _case_bc(case), {"Pb": 101325.0 * 1.2})
+                np.testing.assert_array_equal(d["Upad"], Ur)
+                np.testing.assert_array_equal(d["Apad"], Ar)
 
 
 @pytest.mark.gpu
