@@ -16,3 +16,25 @@ def U_to_prim(U, aux):
     auxd, _ = _state.to_device(aux)
     s = _state.solver_for(tuple(Ud.shape[1:]))
     return tuple(_state.back(o, kind) for o in s.u_to_prim(Ud, auxd))
+
+
+_user_source = None
+
+
+def set_source_terms(user_set):
+    """aux_func.py:6-18: the user's source function, or zeros."""
+    global _user_source
+    fn = None if user_set is None else user_set.get("self_defined_source_terms")
+    _user_source = fn
+
+
+def source_terms(U, aux, theta=None):
+    """aux_func.py source_terms: the user's source, zeros without one."""
+    if _user_source is None:
+        return U * 0
+    return _user_source(U, aux, theta)
+
+
+def aux_to_thermo(U, aux):
+    """aux_func.py aux_to_thermo: (gamma, T)."""
+    return aux[0:1], aux[1:2]

@@ -16,3 +16,43 @@ def U_to_prim(U, aux):
     auxd, _ = _state.to_device(aux)
     s = _state.solver_for(tuple(Ud.shape[1:]))
     return tuple(_state.back(o, kind) for o in s.u_to_prim(Ud, auxd))
+
+
+_user_source = None
+
+
+def set_source_terms(user_set):
+    """aux_func.py:6-18: the user's source function, or zeros."""
+    global _user_source
+    fn = None if user_set is None else user_set.get("self_defined_source_terms")
+    _user_source = fn
+
+
+def source_terms(U, aux, theta=None):
+    """aux_func.py source_terms: the user's source, zeros without one."""
+    if _user_source is None:
+        return U * 0
+    return _user_source(U, aux, theta)
+
+
+def aux_to_thermo(U, aux):
+    """aux_func.py aux_to_thermo: (gamma, T)."""
+    return aux[0:1], aux[1:2]
+
+
+def prim_to_U(q):
+    """aux_func.py prim_to_U: (U, aux) from the primitives q = (rho, u, v, p,
+    Y[8]) with T = p / (rho R) and NASA7 h and gamma.  The reference writes
+    the kinetic term as ``0.5*rho(u**2+v**2)`` (a call of rho, a TypeError);
+    this is the product it means: rho E = rho h - p + 0.5 rho (u^2 + v^2)."""
+    import torch
+    qd, kind = _state.to_device(q)
+    rho, u, v, p, Y = qd[0:1], qd[1:2], qd[2:3], qd[3:4], qd[4:]
+    s = _state.solver_for(tuple(qd.shape[1:]))
+    _, _, _, R, _ = s.get_thermo(torch.ones_like(rho), Y)  # R depends on Y only
+    T = p / (rho * R)
+    _, gamma, h, _, _ = s.get_thermo(T, Y)
+    rhoE = rho * h - p + 0.5 * rho * (u ** 2 + v ** 2)
+    U = torch.cat([rho, rho * u, rho * v, rhoE, rho * Y], dim=0)
+    aux = torch.cat([gamma, T], dim=0)
+    return _state.back(U, kind), _state.back(aux, kind)

@@ -86,3 +86,27 @@ def test_total_flux_of_padded_arrays(case, dim):
     err = max(np.sum(np.abs(got[i] - ref[i])) / np.sum(np.abs(ref[i])) for i in range(ref.shape[0])
               if np.sum(np.abs(ref[i])) > 1e-30)
     assert err < 1e-13
+
+
+@pytest.mark.gpu
+def test_prim_to_U_inverts_U_to_prim():
+    """aux_func.prim_to_U(U_to_prim(U)) returns U and the state's (gamma, T)
+    (the reference's own prim_to_U cannot run: its kinetic term calls rho)."""
+    from janc_b200.janc.solver_2D import aux_func
+    from janc_b200.mechanism import DEFAULT_MECHANISM
+    om = jo.load_mechanism(DEFAULT_MECHANISM)
+    _configure(2, dict(zip(KEYS, COMBOS[0])))
+    U, aux = _state(om, 2)
+    rho, u, v, Y, p, a = aux_func.U_to_prim(U, aux)
+    U2, aux2 = aux_func.prim_to_U(np.concatenate([rho, u, v, p, Y], axis=0))
+    for i in range(U.shape[0]):
+        assert np.max(np.abs(U2[i] - U[i])) <= 1e-12 * np.max(np.abs(U[i])) + 1e-300
+    assert np.max(np.abs(aux2[1] - aux[1]) / aux[1]) < 1e-13
+    assert np.max(np.abs(aux2[0] - aux[0]) / aux[0]) < 1e-13
+    g, T = aux_func.aux_to_thermo(U, aux)
+    assert np.array_equal(g, aux[0:1]) and np.array_equal(T, aux[1:2])
+    aux_func.set_source_terms(None)
+    assert np.all(aux_func.source_terms(U, aux) == 0)
+    aux_func.set_source_terms({"self_defined_source_terms": lambda U, a, th: 2 * U})
+    assert np.array_equal(aux_func.source_terms(U, aux), 2 * U)
+    aux_func.set_source_terms(None)
