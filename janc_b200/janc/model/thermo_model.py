@@ -55,6 +55,25 @@ def get_thermo(T, Y):
     return tuple(_state.back(o, kind) for o in outs)
 
 
+def get_thermo_properties(T):
+    """thermo_model.py:107-112: per-species (cp_k, dcp_k, h_k), each of shape
+    (9,) + T.shape, from the NASA7 kernel (jb_get_thermo) evaluated with
+    one-hot mass fractions, whose mixture sums hold a single nonzero term."""
+    Td, kind = _state.to_device(T)
+    s = _state.solver_for((4,))
+    T1 = Td.reshape(1, -1).contiguous()
+    cps, dcps, hs = [], [], []
+    for k in range(9):
+        Y = torch.zeros((8, T1.shape[1]), dtype=torch.float64, device=T1.device)
+        if k < 8:
+            Y[k] = 1.0  # the ninth (N2) is the filled remainder of all-zero Y
+        cp, _, h, _, dcp = s.get_thermo(T1, Y)
+        cps.append(cp.reshape(Td.shape))
+        dcps.append(dcp.reshape(Td.shape))
+        hs.append(h.reshape(Td.shape))
+    return tuple(_state.back(torch.stack(x), kind) for x in (cps, dcps, hs))
+
+
 def get_T(e, Y, initial_T):
     """thermo_model.py:135-153 (Halley with the global stopping rule):
     returns concat([gamma, T]).  Runs the update_aux kernel on a unit-density

@@ -110,3 +110,19 @@ def test_prim_to_U_inverts_U_to_prim():
     aux_func.set_source_terms({"self_defined_source_terms": lambda U, a, th: 2 * U})
     assert np.array_equal(aux_func.source_terms(U, aux), 2 * U)
     aux_func.set_source_terms(None)
+
+
+@pytest.mark.gpu
+def test_get_thermo_properties_bitwise():
+    """thermo_model.get_thermo_properties(T): per-species cp, dcp, h across
+    both NASA7 ranges (the 1000 K switch included), bit for bit in strict."""
+    from janc_b200.janc.model import thermo_model
+    from janc_b200.mechanism import DEFAULT_MECHANISM
+    om = jo.load_mechanism(DEFAULT_MECHANISM)
+    _configure(2, dict(zip(KEYS, COMBOS[0])))
+    T = np.concatenate([np.linspace(250.0, 3500.0, 61), [999.999, 1000.0, 1000.001]]).reshape(8, 8)
+    cp, dcp, h = thermo_model.get_thermo_properties(T)
+    rcp, rdcp, rh = jo.get_thermo_properties(om, T)
+    np.testing.assert_array_equal(cp, rcp)
+    np.testing.assert_array_equal(dcp, rdcp)
+    np.testing.assert_array_equal(h, rh)
