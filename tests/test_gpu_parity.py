@@ -7,7 +7,7 @@ Tolerances (float64):
   through exp/log/pow or the 8x8 solve (chemistry, full steps) to 1e-12
   relative L1 per field.
 * ``fp64`` (FMA contraction): 1e-12 per kernel, full steps 1e-10 relative L1
-  per field (the north-star bar for the FP64 build).
+  per field (the bar for the FP64 build).
 """
 import os
 
@@ -316,7 +316,7 @@ def test_periodic_mass_conservation(prec, omech):
 
 # --------------------------------------------------------------------------
 # mixed precision: float32 flux arithmetic, float64 state / T-solve / chemistry
-# bar (north star): density relative L1 <= 1e-4, front position within 1 cell
+# bar: density relative L1 <= 1e-4, front position within 1 cell
 # --------------------------------------------------------------------------
 def _front(U, aux, omech, two_d):
     nY = 4 if two_d else 3
