@@ -225,12 +225,17 @@ class H5Saver:
 
     def load_state(self, key=None):
         """(U, aux, time, step) of snapshot ``key`` (default: the latest
-        ``save_step{k}``) for a restart."""
+        ``save_step{k}``) for a restart.  A snapshot without ``aux`` (written
+        by the reference, which saves ``u`` only) gets its (gamma, T) from
+        the temperature solve started at the reference's gamma = 1.4,
+        T = 500 K guesses, as its ``load`` does."""
         if key is None:
             keys = [k for k in self.file.keys() if k.startswith("save_step") and "_device" not in k]
             key = max(keys, key=lambda k: int(k[len("save_step"):]))
         grp = self.file[key]
         U, aux = self._state_of(grp)
+        if "aux" not in grp:
+            aux = (aux_func_1D if self.dim == "1D" else aux_func).update_aux(U, aux)
         return U, aux, float(grp.attrs["time"]), int(grp.attrs["step"])
 
     def load_all(self):

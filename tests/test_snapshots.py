@@ -190,6 +190,17 @@ def test_run_snapshots_and_bitwise_restart(tmp_path):
     s2 = H5Saver(tmp_path / "restart.h5", "1D", mode="r")
     assert "save_step0" not in s2.list_snapshots() and "save_step5" in s2.list_snapshots()
     s2.close()
+    # a snapshot as the reference writes it (u only): aux from the temperature solve
+    f = h5lite.File(tmp_path / "u_only.h5", "w")
+    g = f.create_group("save_step0")
+    g.attrs["time"] = 0.0
+    g.attrs["step"] = 0
+    g.create_dataset("u", data=U0, compression="gzip")
+    f.close()
+    s3 = H5Saver(tmp_path / "u_only.h5", "1D", mode="r")
+    U3, a3, t3, _ = s3.load_state()
+    s3.close()
+    assert np.array_equal(U3, U0) and np.max(np.abs(a3[1] - a0[1]) / a0[1]) < 1e-9
 
 
 def _parallel_worker(rank, size, port, out):
