@@ -7,9 +7,13 @@ and contiguous datasets, appends across reopenings, deletions, groups larger
 than one symbol-table node) and byte-level checks of the structures the HDF5
 file format specification fixes (superblock version 0, end-of-file address,
 version-1 object headers, the local heap's leading empty name, names sorted
-across symbol-table nodes and B-tree keys); H5Saver's save / parallel
-layout / collect / load_state.  The files are not opened by libhdf5 here:
-their compatibility with it is unpinned.
+across symbol-table nodes and B-tree keys); the reader on hand-assembled
+structures its writer does not produce but h5py files contain (object header
+continuations, attribute messages 2 and 3, dataspace 2, compact layout,
+multi-chunk shuffle + deflate datasets, version-2 object headers with link
+messages); H5Saver's save / parallel layout / collect / load_state.  The
+files are not opened by libhdf5 here: their compatibility with it is
+unpinned.
 GPU: Simulator.run writes the snapshots; a restart from a middle snapshot
 reproduces the uninterrupted run bit for bit; load / load_all primitives.
 """
@@ -245,4 +249,132 @@ def test_parallel_snapshots_collect_and_restart(tmp_path):
     keys = set(f.keys())
     assert {"save_step0_device0", "save_step0_device1", "save_step0", "save_step3"} <= keys
     assert f["save_step0_device1"]["u"].shape == (11, 200) and f["save_step0"]["u"].shape == (11, 400)
+    f.close()
+
+
+# ------------------------------------------------ reader paths h5py files use
+def _h5_file(objs, root_addr_key="root"):
+    """Assemble a file from hand-built objects: objs is an ordered list of
+    (name, bytes-builder(addr_of) -> bytes); addresses are assigned in order
+    after a version-0 superblock."""
+    import struct as st
+    addr, blobs = {}, []
+    pos = 96
+    for name, build in objs:
+        addr[name] = pos
+        size = len(build(lambda k: 0))
+        pos += size + (-size % 8)
+    for name, build in objs:
+        b = build(lambda k: addr[k])
+        blobs.append(b + b"\0" * (-len(b) % 8))
+    sb = (b"\x89HDF\r\n\x1a\n" + st.pack("<8BHHI", 0, 0, 0, 0, 0, 8, 8, 0, 4, 16, 0)
+          + st.pack("<QQQQ", 0, 0xFFFFFFFFFFFFFFFF, pos, 0xFFFFFFFFFFFFFFFF)
+          + st.pack("<QQII", 0, addr[root_addr_key], 0, 0) + b"\0" * 16)
+    return sb + b"".join(blobs)
+
+
+def test_h5lite_reads_continuations_v2_v3_messages_and_chunks(tmp_path):
+    """Structures h5py / libhdf5 write that h5lite's writer does not:
+    a version-1 object header continued in a second block, attribute
+    messages of versions 2 and 3, a version-2 dataspace, a compact layout,
+    a chunked dataset of several chunks with shuffle + deflate, a
+    version-2 object header with compact link messages."""
+    import struct as st
+    import zlib
+    H = h5lite
+    f64 = H._encode_dtype(np.float64)
+    i32 = H._encode_dtype(np.int32)
+
+    def msg1(t, data, fl=0):
+        data = H._pad8(data)
+        return st.pack("<HHB3x", t, len(data), fl) + data
+
+    def attr_v3(name, val):
+        v = np.asarray(val, dtype=np.float64)
+        nm = name.encode() + b"\0"
+        sp = st.pack("<BBBB", 2, 1, 0, 1) + st.pack("<Q", v.size)  # dataspace v2, simple
+        return st.pack("<BBHHHB", 3, 0, len(nm), len(f64), len(sp), 0) + nm + f64 + sp + v.tobytes()
+
+    def attr_v2(name, val):
+        v = np.asarray(val, dtype=np.int32)
+        nm = name.encode() + b"\0"
+        sp = st.pack("<BBBB", 2, 0, 0, 0)  # scalar dataspace v2
+        return st.pack("<BBHHH", 2, 0, len(nm), len(i32), len(sp)) + nm + i32 + sp + v.tobytes()
+
+    a = np.arange(6 * 10, dtype=np.float64).reshape(6, 10) * 0.5
+    chunks = {}
+    for cx in (0, 4):
+        for cy in (0, 4, 8):
+            c = np.zeros((4, 4))
+            blk = a[cx:cx + 4, cy:cy + 4]
+            c[:blk.shape[0], :blk.shape[1]] = blk
+            sh = np.frombuffer(c.tobytes(), np.uint8).reshape(-1, 8).T.tobytes()  # shuffle
+            chunks[(cx, cy)] = zlib.compress(sh)
+    keys = sorted(chunks)
+    ks = 8 + 8 * 3
+
+    def btree(A):
+        body = b""
+        for i, k in enumerate(keys):
+            body += st.pack("<II3Q", len(chunks[k]), 0, k[0], k[1], 0) + st.pack("<Q", A(f"c{i}"))
+        body += st.pack("<II3Q", 0, 0, 6, 10, 0)
+        node = b"TREE" + bytes([1, 0]) + st.pack("<HQQ", len(keys), H.UNDEF, H.UNDEF) + body
+        return node + b"\0" * (24 + 64 * 8 + 65 * ks - len(node))
+
+    filt = (st.pack("<BB6x", 1, 2) + st.pack("<HHHH", 2, 8, 0, 1) + H._pad8(b"shuffle\0") + st.pack("<I4x", 8)
+            + st.pack("<HHHH", 1, 8, 0, 1) + H._pad8(b"deflate\0") + st.pack("<I4x", 6))
+
+    def ds_chunked(A):
+        msgs = (msg1(1, H._space_msg((6, 10))) + msg1(3, f64, 1)
+                + msg1(8, st.pack("<BBBQ3I", 3, 2, 3, A("bt"), 4, 4, 8)) + msg1(11, filt))
+        return st.pack("<BBHII4x", 1, 0, 4, 1, len(msgs)) + msgs
+
+    small = np.array([1.5, -2.0, 7.25])
+
+    def ds_compact(A):
+        lay = st.pack("<BBH", 3, 0, small.nbytes) + small.tobytes()
+        msgs = msg1(1, st.pack("<BBBB", 2, 1, 0, 1) + st.pack("<Q", 3)) + msg1(3, f64, 1) + msg1(8, lay)
+        return st.pack("<BBHII4x", 1, 0, 3, 1, len(msgs)) + msgs
+
+    def grp(A):  # version-1 header: link table in a continuation block
+        cont = msg1(16, st.pack("<QQ", A("cont"), len(grp_cont(A))))
+        msgs = msg1(12, attr_v3("time", [2.5e-6])) + cont
+        return st.pack("<BBHII4x", 1, 0, 3, 1, len(msgs)) + msgs
+
+    def grp_cont(A):
+        return msg1(12, attr_v2("step", 42)) + msg1(17, st.pack("<QQ", A("gbt"), A("gheap")))
+
+    names = [b"chunked", b"compact"]
+    heap_data = b"\0" * 8 + H._pad8(names[0] + b"\0") + H._pad8(names[1] + b"\0")
+    offs = [8, 8 + len(H._pad8(names[0] + b"\0"))]
+
+    def gheap(A):
+        return b"HEAP" + bytes(4) + st.pack("<QQQ", len(heap_data), H.FREE_NULL, A("gheapdata"))
+
+    def gsnod(A):
+        ent = b"".join(st.pack("<QQII16x", o, A(n), 0, 0) for o, n in zip(offs, ("ds1", "ds2")))
+        return b"SNOD" + bytes([1, 0]) + st.pack("<H", 2) + ent + b"\0" * (40 * 6)
+
+    def gbt(A):
+        node = (b"TREE" + bytes([0, 0]) + st.pack("<HQQ", 1, H.UNDEF, H.UNDEF)
+                + st.pack("<QQQ", 0, A("gsnod"), offs[1]))
+        return node + b"\0" * (24 + 32 * 8 + 33 * 8 - len(node))
+
+    def root(A):  # version-2 object header with one compact hard link
+        link = bytes([1, 0x00]) + bytes([len(b"save_step7")]) + b"save_step7" + st.pack("<Q", A("grp"))
+        body = bytes([6]) + st.pack("<H", len(link)) + bytes([0]) + link
+        return b"OHDR" + bytes([2, 0]) + bytes([len(body)]) + body + b"\0\0\0\0"
+
+    objs = [("root", root), ("grp", grp), ("cont", grp_cont), ("gbt", gbt), ("gsnod", gsnod), ("gheap", gheap),
+            ("gheapdata", lambda A: heap_data), ("ds1", ds_chunked), ("ds2", ds_compact), ("bt", btree)]
+    objs += [(f"c{i}", (lambda k: lambda A: chunks[k])(k)) for i, k in enumerate(keys)]
+    p = tmp_path / "handmade.h5"
+    p.write_bytes(_h5_file(objs))
+    f = h5lite.File(p, "r")
+    assert list(f.keys()) == ["save_step7"]
+    g = f["save_step7"]
+    assert g.attrs["time"] == 2.5e-6 and g.attrs["step"] == 42
+    assert sorted(g.keys()) == ["chunked", "compact"]
+    assert np.array_equal(np.asarray(g["chunked"]), a)
+    assert np.array_equal(np.asarray(g["compact"]), small)
     f.close()
