@@ -1189,8 +1189,11 @@ __global__ void __launch_bounds__(SX_NT) k_sweep_x(MP m, Grid g, const double* _
   }
 }
 
+#ifndef JB_YR_MINB
+#define JB_YR_MINB 3
+#endif
 template <int STAGE, bool VISC>
-__global__ void __launch_bounds__(YR_NT, 3) k_flux_y_rk(MP m, Grid g, const double* __restrict__ Uk,
+__global__ void __launch_bounds__(YR_NT, JB_YR_MINB) k_flux_y_rk(MP m, Grid g, const double* __restrict__ Uk,
                                                        const double* __restrict__ auxk,
                                                        const double* __restrict__ Un, const float* __restrict__ prims,
                                                        const double* __restrict__ strips,
