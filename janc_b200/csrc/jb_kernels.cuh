@@ -1135,7 +1135,10 @@ __device__ __forceinline__ void win_load(const MP& m, const Grid& g, const doubl
   }
 }
 
-__global__ void __launch_bounds__(SX_NT) k_sweep_x(MP m, Grid g, const double* __restrict__ Uk,
+#ifndef JB_SX_MINB
+#define JB_SX_MINB 1
+#endif
+__global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, const double* __restrict__ Uk,
                                                    const float* __restrict__ prims,
                                                    const double* __restrict__ strips, const Slots* slots, int aidx,
                                                    float* __restrict__ dfx, int nlb) {
