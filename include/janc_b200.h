@@ -8,11 +8,20 @@
  *                      nv = 11 in 1D (ny = 1): rho, rho*u, rho*E, rho*Y_1..8
  *   aux  [2][nx][ny]   gamma, T
  * Species order is the mechanism's; the last species (N2) is implicit,
- * Y_N2 = 1 - sum(Y).  Every call is asynchronous on the given CUDA stream
- * (a cudaStream_t passed as void*; NULL = legacy default stream), allocates
- * nothing, and returns 0 or a jb_status bit set.  The handle owns only its
- * tables and a workspace sized at jb_create; it never frees caller memory.
- * Calls on one handle are stream-ordered and not thread-safe.
+ * Y_N2 = 1 - sum(Y).  Every call returns 0 or a jb_status bit set.
+ *
+ * Two kinds of call.  Configuration calls (jb_create, jb_destroy,
+ * jb_set_transport, jb_adjoint_reserve and the jb_ens_* set-up calls) may
+ * allocate or free device memory and may synchronise the device.  Every
+ * other call (jb_flux_func, jb_update_aux, jb_reaction_source_terms,
+ * jb_advance, jb_advance_ex, jb_rk3, jb_u_to_prim, jb_cfl_dt, jb_get_thermo,
+ * jb_boundary_conditions, jb_adjoint_step, jb_state_from_PTY_vjp, ...)
+ * allocates nothing, is asynchronous on the given CUDA stream (a
+ * cudaStream_t passed as void*; NULL = legacy default stream) and does not
+ * synchronise, except jb_status, which synchronises its stream by design.
+ * The handle owns its tables and the workspaces its configuration calls
+ * sized; it never frees caller memory.  Calls on one handle are
+ * stream-ordered and not thread-safe.
  */
 #ifndef JANC_B200_H
 #define JANC_B200_H
@@ -129,8 +138,9 @@ int jb_set_reconstruction(jb_handle* h, int recon);
  * the handle (added to the advective flux as NS_flux does, solver_2D/flux.py:117).
  * tr->turbulence_model = 1 adds the LES sub-grid viscosity of the 2D Vreman
  * model (model/LES/Verman.py; JB_ERR_UNSUPPORTED on a 1D handle, where the
- * reference has no model).  tr = NULL switches back to Euler fluxes.  Allocates its scratch on the first
- * call.  jb_adjoint_step supports the inviscid path only. */
+ * reference has no model).  tr = NULL switches back to Euler fluxes (and frees
+ * the scratch).  A configuration call: the first call with a model allocates
+ * the viscous scratch.  jb_adjoint_step supports the inviscid path only. */
 int jb_set_transport(jb_handle* h, const jb_transport* tr);
 
 /* x-slab decomposition (replaces the reference's is_parallel mode:
@@ -186,15 +196,19 @@ int jb_sizeof_grid(void);
  * callers that cannot allocate device memory themselves - a plugin inside a
  * host code that reserves all device memory at start-up, or a call made from
  * within another runtime's operator whose memory that runtime owns - and so
- * cannot call jb_create().  Same arguments and result as jb_update_aux() on a
- * solver of that grid and precision, with U, aux_in and aux_out supplied by
- * the caller.  Its scratch lives in one static device array inside the
+ * cannot call jb_create().  Same result as jb_update_aux() on a solver of
+ * that grid and precision, with U, aux_in and aux_out supplied by the
+ * caller.  precision is JB_PREC_STRICT or JB_PREC_FP64; JB_PREC_MIXED returns
+ * JB_ERR_UNSUPPORTED (the mixed variant's temperature solve is the fp64 one,
+ * so pass JB_PREC_FP64 for it).  Its scratch lives in one static device array inside the
  * library, sized for at most JB_NOALLOC_MAX_CELLS cells (about 3.1 MB, held
  * on every GPU that loads the library until exit); larger grids return
- * JB_ERR_ARG.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race and must be serialised
- * by the caller. */
+ * JB_ERR_ARG.  Outside stream capture every call looks up the array's device
+ * address (cudaGetSymbolAddress), so a device reset between calls is safe; a
+ * captured call reuses the address of the device's last uncaptured call, so
+ * make the first call on a device before any stream capture (a captured
+ * first call returns JB_ERR_ARG).  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
 #define JB_NOALLOC_MAX_CELLS 65536
 int jb_update_aux_noalloc(const jb_mech_params* mech, int dim, int nx, int ny, int precision,
                           const double* U, const double* aux_in, double* aux_out, void* stream);
@@ -239,7 +253,14 @@ long long jb_record_doubles(const jb_handle* h);
 int jb_advance_ex(jb_handle* h, const double* U, const double* aux, double* U_out, double* aux_out,
                   double dt_fixed, double cfl, int nsteps, double* dt_hist, double* probe_p, double* rec,
                   double* rec_slots, void* stream);
-/* One step of the adjoint.  rec points at step n's record (step n+1's
+/* Configuration call: allocate the adjoint's workspace (stage adjoints,
+ * primitives, face scratch, reductions) and upload the padded-grid
+ * multiplicity of the handle's sides; synchronous.  Returns
+ * JB_ERR_UNSUPPORTED for what jb_adjoint_step cannot differentiate.  Call it
+ * once before the first jb_adjoint_step, outside any stream capture. */
+int jb_adjoint_reserve(jb_handle* h);
+/* One step of the adjoint (needs jb_adjoint_reserve; allocates nothing).
+ * rec points at step n's record (step n+1's
  * record follows it), rec_slots at step n's slots; cfl as given to the
  * forward (<= 0: fixed time step).  On entry Ubar / Abar hold the adjoint
  * of the state after the step (U_{n+1}: nv x ncell, aux_{n+1}: 2 x ncell);

@@ -32,7 +32,7 @@ EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_fun
            "jb_ens_create", "jb_ens_destroy", "jb_ens_instance", "jb_ens_total_cells", "jb_ens_configure",
            "jb_ens_autotune", "jb_ens_launch_shape", "jb_ens_advance", "jb_ens_advance_direct",
            "jb_ens_status", "jb_ens_last_error", "jb_ens_selftest_timeout",
-           "jb_set_probe", "jb_set_log_A_offset", "jb_record_doubles", "jb_advance_ex", "jb_adjoint_step",
+           "jb_set_probe", "jb_set_log_A_offset", "jb_record_doubles", "jb_advance_ex", "jb_adjoint_reserve", "jb_adjoint_step",
            "jb_state_from_PTY_vjp"]
 
 _lib = None
@@ -110,6 +110,7 @@ def lib(path=None):
     L.jb_record_doubles.argtypes = [vp]
     L.jb_record_doubles.restype = ll
     L.jb_advance_ex.argtypes = [vp, dp, dp, dp, dp, d, d, i, dp, dp, dp, dp, vp]
+    L.jb_adjoint_reserve.argtypes = [vp]
     L.jb_adjoint_step.argtypes = [vp, dp, dp, d, dp, dp, dp, dp, dp, vp]
     L.jb_state_from_PTY_vjp.argtypes = [vp, dp, dp, dp, dp, dp, dp, vp]
     L.jb_ens_selftest_timeout.argtypes = [vp, d, ctypes.POINTER(ctypes.c_uint), vp]

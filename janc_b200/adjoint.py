@@ -44,6 +44,7 @@ class Trajectory:
         self.K = int(checkpoint)
         L = solver._lib
         _native.check(L.jb_set_probe(solver._h, *self.probe), solver._h, "jb_set_probe")
+        _native.check(L.jb_adjoint_reserve(solver._h), solver._h, "jb_adjoint_reserve")
         self.rec_doubles = int(L.jb_record_doubles(solver._h))
         self._lnA = None
 

@@ -659,8 +659,9 @@ static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mu
     }
 }
 
-static int adj_workspace(jb_handle* h) {
-  if (h->adj_ws) return JB_OK;
+// What jb_adjoint_step differentiates; checked when the workspace is reserved
+// and again at every step (the flux scheme can change in between).
+static int adj_supported(jb_handle* h) {
   if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
   if (h->grid.scheme != JB_FLUX_LF || h->grid.visc || h->grid.recon != JB_RECON_WENO5)
     return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint differentiates the inviscid LF / WENO5-JS path");
@@ -669,21 +670,36 @@ static int adj_workspace(jb_handle* h) {
   for (int s = 0; s < 4; ++s)
     if (h->grid.bc[s] == JB_BC_PRESSURE_OUTLET || h->grid.bc[s] == JB_BC_RDC_INJECTOR)
       return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint supports periodic, slip, no-slip and zero-gradient sides");
+  return JB_OK;
+}
+
+int jb_adjoint_reserve(jb_handle* h) {
+  if (!h) return JB_ERR_ARG;
+  if (h->adj_ws) return JB_OK;
+  if (int rc = adj_supported(h)) return rc;
   const jb_grid& g = h->grid;
   const size_t nc = (size_t)g.ncell, nU = (size_t)g.nv * nc;
   const size_t nsc = jb::adj::flux_scratch_doubles(g);
   const size_t n = 2 * nU + 12 * nc + nsc + jb::adj::RED_N;
-  JB_TRY(cudaMalloc(&h->adj_ws, sizeof(double) * n), "adjoint workspace");
-  JB_TRY(cudaMemset(h->adj_ws, 0, sizeof(double) * n), "adjoint workspace clear");
+  std::vector<unsigned char> mult;
+  padded_multiplicity(g, mult);
+  cudaError_t e = cudaMalloc(&h->adj_ws, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&h->adj_mult, nc);
+  if (e == cudaSuccess) e = cudaMemset(h->adj_ws, 0, sizeof(double) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(h->adj_mult, mult.data(), nc, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    if (h->adj_ws) cudaFree(h->adj_ws);
+    if (h->adj_mult) cudaFree(h->adj_mult);
+    h->adj_ws = nullptr;
+    h->adj_mult = nullptr;
+    return check_cuda(h, e, "adjoint workspace");
+  }
   h->adj_B1 = h->adj_ws;
   h->adj_B2 = h->adj_B1 + nU;
   h->adj_prims = h->adj_B2 + nU;
   h->adj_scratch = h->adj_prims + 12 * nc;
   h->adj_red = h->adj_scratch + nsc;
-  std::vector<unsigned char> mult;
-  padded_multiplicity(g, mult);
-  JB_TRY(cudaMalloc(&h->adj_mult, nc), "multiplicity");
-  JB_TRY(cudaMemcpy(h->adj_mult, mult.data(), nc, cudaMemcpyHostToDevice), "multiplicity copy");
+  h->ws_bytes += (long long)(sizeof(double) * n + nc);
   return JB_OK;
 }
 
@@ -691,7 +707,8 @@ int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, do
                     double* Abar, const double* dt_bar, const double* pp_bar, double* lnA_bar, void* stream) {
   if (!h || !rec || !rec_slots || !Ubar || !Abar || !lnA_bar) return set_err(h, JB_ERR_ARG, "null pointer");
   if (pp_bar && h->probe[2] * h->probe[3] <= 0) return set_err(h, JB_ERR_ARG, "probe adjoint needs jb_set_probe");
-  if (int rc = adj_workspace(h)) return rc;
+  if (int rc = adj_supported(h)) return rc;
+  if (!h->adj_ws) return set_err(h, JB_ERR_ARG, "call jb_adjoint_reserve before jb_adjoint_step");
   cudaStream_t st = (cudaStream_t)stream;
   const jb_mech_params& m = h->mech;
   const jb_grid& g = h->grid;

@@ -35,17 +35,25 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 std::mutex g_lock;
 void* g_addr[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device, looked up once
-// per device (host code only sees a stand-in for the symbol).
-int scratch_address(void** out) {
+// Device address of the scratch array on the current device (host code only
+// sees a stand-in for the symbol).  Outside stream capture it is looked up
+// on every call, so a device reset, after which the module can load at
+// another address, never leaves a stale pointer; during a capture the
+// address of this device's last uncaptured call is used (capture makes no
+// lookup, which could load the module).
+int scratch_address(cudaStream_t st, void** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return JB_ERR_CUDA;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return JB_ERR_CUDA;
   std::lock_guard<std::mutex> guard(g_lock);
-  if (!g_addr[dev]) {
+  if (cs == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) return JB_ERR_CUDA;
     g_addr[dev] = p;
+  } else if (!g_addr[dev]) {
+    return JB_ERR_ARG;  // the first call on a device must not be captured
   }
   *out = g_addr[dev];
   return JB_OK;
@@ -63,9 +71,12 @@ extern "C" int jb_update_aux_noalloc(const jb_mech_params* mech, int dim, int nx
   const long long ncell = (long long)nx * ny;
   if (ncell > JB_NOALLOC_MAX_CELLS) return JB_ERR_ARG;  // larger grids need jb_create
   if (mech->ns != 9 || mech->nr != 8 || mech->nreac != 19) return JB_ERR_UNSUPPORTED;
+  // JB_PREC_MIXED is refused: its temperature solve is the fp64 one, and a
+  // caller asking for it gets the fp64 result by passing JB_PREC_FP64
   if (precision != JB_PREC_STRICT && precision != JB_PREC_FP64) return JB_ERR_UNSUPPORTED;
+  cudaStream_t st = (cudaStream_t)stream;
   void* base = nullptr;
-  if (int rc = scratch_address(&base)) return rc;
+  if (int rc = scratch_address(st, &base)) return rc;
   jb_mech_params m = *mech;
   jb::derive_mech(m);
   jb_grid g = {};
@@ -83,7 +94,6 @@ extern "C" int jb_update_aux_noalloc(const jb_mech_params* mech, int dim, int nx
   jb_slots* slots = reinterpret_cast<jb_slots*>(base);
   double* cand = reinterpret_cast<double*>(static_cast<unsigned char*>(base) + kSlotBytes);
   const jb::Ops& o = precision == JB_PREC_STRICT ? jb::strict_ops : jb::fast_ops;
-  cudaStream_t st = (cudaStream_t)stream;
   // the slots keep the previous call's contents: clear them first
   if (o.slots_reset(slots, st) != cudaSuccess) return JB_ERR_CUDA;
   if (o.halley(dim, m, g, U, aux_in, cand, slots, 0, st) != cudaSuccess) return JB_ERR_CUDA;

@@ -468,6 +468,9 @@ class Solver:
             for x in t:
                 x.record_stream(s_in)
                 x.record_stream(s_out)
+        # the copies into ``outputs`` are asynchronous: wait for the last one
+        # so the host can read every result when this returns
+        s_out.synchronize()
         return outputs
 
     def advance_one_step(self, U, aux, dx=None, dy=None, dt=None, theta=None):

@@ -14,7 +14,7 @@ The rotating-detonation injector boundary is the user callable defined in
 ``examples/janc_basic_example2.ipynb``; its two functions are extracted from
 the notebook JSON and executed unchanged.
 
-Usage:  python tests/golden/make_golden.py [--ref /path/to/JANC]
+Usage:  python tests/golden/make_golden.py --ref /path/to/JANC   (or JANC_REF=/path/to/JANC)
 Writes ``tests/golden/*.npz`` (a few hundred KB in total).
 """
 import argparse
@@ -129,12 +129,301 @@ def _load_notebook_injector(ref, thermo_model, U_to_prim):
     return ns["bottom_boundary"], ns["inj_model"]
 
 
+def gen_long1d(ref):
+    """Config-0 physics (2000 cells, slab = first 2 %, slip wall left, zero
+    gradient right) at CFL 0.1 for 1000 steps of the reference's own
+    Simulator.advance_func; the state at steps 1, 10, 100 and 1000 and every
+    step's dt.  About 45 minutes through the NumPy stand-ins."""
+    from janc_v2.model import thermo_model
+    from janc_v2.simulation import set_simulator
+    mech = os.path.join(ref, "examples", "9sp-19r-H2-Air.yaml")
+    t_start = time.time()
+    nxc = 2000
+    cfg = _sim_config("1D", mech, {"dx": 0.1 / nxc},
+                      {"left_boundary": "slip_wall", "right_boundary": "zero_gradient"}, cfl=0.1)
+    sim = set_simulator.Simulator(cfg)
+    P = np.full((1, nxc), 101325.0)
+    T = np.full((1, nxc), 300.0)
+    Y = np.tile(_stoich_Y(1.0)[:, None], (1, nxc))
+    P[:, :40] = 30 * 101325.0
+    T[:, :40] = 3000.0
+    U0, aux0 = _state(thermo_model, P, T, Y)
+    rec = {"U0": U0, "aux0": aux0, "dx": 0.1 / nxc, "cfl": 0.1}
+    U, aux, t = C(U0), C(aux0), 0.0
+    dts = []
+    for step in range(1, 1001):
+        U, aux, t, dt = sim.advance_func(U, aux, t, None)
+        dts.append(float(dt))
+        if step in (1, 10, 100, 1000):
+            rec[f"U_{step}"] = np.asarray(U)
+            rec[f"aux_{step}"] = np.asarray(aux)
+            print(f"config 0, CFL 0.1: step {step}", time.time() - t_start, flush=True)
+    rec["dts"] = np.array(dts)
+    np.savez_compressed(os.path.join(HERE, "config0_cfl01_1000.npz"), **rec)
+
+
+# flux options of SURVEY-row (f): the reference's godunov_flux with HLLC /
+# AUSMPW+, MUSCL reconstruction, and NS_flux with its transport models and
+# the Vreman LES closure (solver_{1D,2D}/flux.py, riemann_solver/,
+# reconstruction/MUSCL.py, finite_difference/ and reconstruction/CENTRAL6.py,
+# model/transport_model.py, model/LES/Verman.py)
+FSEC_FLUX = {
+    "HLLC": {"solver_type": "godunov", "interface_reconstruction": "WENO5_JS", "riemann_solver": "HLLC",
+             "viscosity": "off"},
+    "AUSMPW_plus": {"solver_type": "godunov", "interface_reconstruction": "WENO5_JS",
+                    "riemann_solver": "AUSMPW_plus", "viscosity": "off"},
+    "MUSCL_LF": {"solver_type": "flux_splitting", "interface_reconstruction": "MUSCL", "split_method": "LF",
+                 "viscosity": "off"},
+    "MUSCL_HLLC": {"solver_type": "godunov", "interface_reconstruction": "MUSCL", "riemann_solver": "HLLC",
+                   "viscosity": "off"},
+    "LF_visc": {"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS", "split_method": "LF",
+                "viscosity": "on"},
+}
+FSEC_TRANSPORT = {
+    "sutherland_pr_le": {"viscosity_model": "Sutherland", "thermal_conductivity_model": "Prandtl number",
+                         "Pr": 0.72, "species_diffusivity_model": "Lewis number", "Le": 1.0},
+    "sutherland_sc": {"viscosity_model": "Sutherland", "reference_viscosity": 1.8e-5,
+                      "thermal_conductivity_model": "Prandtl number", "Pr": 0.7,
+                      "species_diffusivity_model": "Schmidt number", "Sc": 0.5},
+    "constant_all": {"viscosity_model": "constant", "dynamic_viscosity": 2e-5,
+                     "thermal_conductivity_model": "constant", "thermal_conductivity": 0.05,
+                     "species_diffusivity_model": "constant", "species_diffusivity": 3e-5},
+    "constant_mu_le": {"viscosity_model": "constant", "dynamic_viscosity": 1.5e-5,
+                       "thermal_conductivity_model": "constant", "thermal_conductivity": 0.04,
+                       "species_diffusivity_model": "Lewis number", "Le": 0.8},
+    "les_pr_le": {"viscosity_model": "Sutherland", "thermal_conductivity_model": "Prandtl number", "Pr": 0.72,
+                  "species_diffusivity_model": "Lewis number", "Le": 1.0, "turbulence_model": "LES",
+                  "LES_model": "Verman", "Pr_t": 0.9, "Le_t": 1.1},
+    "les_constant": {"viscosity_model": "constant", "dynamic_viscosity": 2e-5,
+                     "thermal_conductivity_model": "constant", "thermal_conductivity": 0.05,
+                     "species_diffusivity_model": "constant", "species_diffusivity": 3e-5,
+                     "turbulence_model": "LES", "LES_model": "Verman", "Pr_t": 0.85, "Sc_t": 0.7},
+}
+FSEC_BC2 = (("slip_wall", "zero_gradient", "slip_wall", "slip_wall"),
+            ("pressure_outlet", "zero_gradient", "no_slip_wall", "pressure_outlet"),
+            ("periodic", "periodic", "periodic", "periodic"))
+FSEC_BC1 = (("zero_gradient", "slip_wall"), ("pressure_outlet", "no_slip_wall"))
+FSEC_PB = 101325.0 * 1.3
+
+
+def _fsec_flux(set_simulator, dim, mech, grid, bc, fc, tc, U, aux, dx, dy, dt):
+    cfg = _sim_config(dim, mech, grid, bc)
+    cfg["flux_config"] = fc
+    if tc is not None:
+        cfg["transport_config"] = tc
+    set_simulator.Simulator(cfg)
+    flux_func, _, _ = set_simulator.set_rhs(dim, cfg["reaction_config"])
+    return np.asarray(flux_func(C(U), C(aux), dx, dy, dt, {"Pb": FSEC_PB}))
+
+
+def gen_fsec(ref):
+    """flux_func of the reference for every row-(f) flux option on the
+    boundary-test states of bc1d_si / bc2d_si, and a few steps of the
+    Godunov path (2D HLLC, 1D AUSMPW+) from the step fixtures' initial
+    states.  The reference's 2D AUSMPW+ cannot run (its y faces take gamma
+    from the x-face arrays, a shape mismatch), so it has no 2D fixture; LES
+    is 2D only (Verman_1D is not in the reference's dictionary)."""
+    from janc_v2.simulation import set_simulator
+    mech = os.path.join(ref, "examples", "9sp-19r-H2-Air.yaml")
+    t_start = time.time()
+    out = {}
+    b2 = np.load(os.path.join(HERE, "bc2d_si.npz"))
+    U2, A2 = b2["U"], b2["aux"]
+    dx2, dy2, dt2 = 1e-4, 2e-4, 2e-8
+    for name, fc in FSEC_FLUX.items():
+        if name == "AUSMPW_plus":
+            continue
+        tcs = FSEC_TRANSPORT if fc["viscosity"] == "on" else {"": None}
+        for tname, tc in tcs.items():
+            for bc in FSEC_BC2:
+                bcd = dict(zip(("left_boundary", "right_boundary", "bottom_boundary", "top_boundary"), bc))
+                key = "f2d_" + name + (("_" + tname) if tname else "") + "_" + "_".join(bc)
+                out[key] = _fsec_flux(set_simulator, "2D", mech, {"dx": dx2, "dy": dy2}, bcd, fc, tc,
+                                      U2, A2, dx2, dy2, dt2)
+        print("2D", name, time.time() - t_start, flush=True)
+    b1 = np.load(os.path.join(HERE, "bc1d_si.npz"))
+    U1, A1 = b1["U"], b1["aux"]
+    dx1, dt1 = 0.1 / U1.shape[1], 2e-8
+    for name, fc in FSEC_FLUX.items():
+        tcs = {k: v for k, v in FSEC_TRANSPORT.items() if not k.startswith("les")} \
+            if fc["viscosity"] == "on" else {"": None}
+        for tname, tc in tcs.items():
+            for bc in FSEC_BC1:
+                bcd = dict(zip(("left_boundary", "right_boundary"), bc))
+                key = "f1d_" + name + (("_" + tname) if tname else "") + "_" + "_".join(bc)
+                out[key] = _fsec_flux(set_simulator, "1D", mech, {"dx": dx1}, bcd, fc, tc, U1, A1, dx1, None, dt1)
+        print("1D", name, time.time() - t_start, flush=True)
+    # Godunov steps: advance_func of a configured Simulator (CFL 0.5)
+    s2 = np.load(os.path.join(HERE, "step2d_si.npz"))
+    bc2 = {"left_boundary": "slip_wall", "right_boundary": "zero_gradient",
+           "bottom_boundary": "slip_wall", "top_boundary": "slip_wall"}
+    cfg = _sim_config("2D", mech, {"dx": float(s2["dx"]), "dy": float(s2["dy"])}, bc2)
+    cfg["flux_config"] = FSEC_FLUX["HLLC"]
+    sim = set_simulator.Simulator(cfg)
+    U, aux, t = C(s2["U0"]), C(s2["aux0"]), 0.0
+    for step in range(1, 3):
+        U, aux, t, dt = sim.advance_func(U, aux, t, None)
+        out[f"step2d_HLLC_U_{step}"] = np.asarray(U)
+        out[f"step2d_HLLC_aux_{step}"] = np.asarray(aux)
+    s1 = np.load(os.path.join(HERE, "step1d_si.npz"))
+    bc1 = {"left_boundary": "slip_wall", "right_boundary": "zero_gradient"}
+    cfg = _sim_config("1D", mech, {"dx": float(s1["dx"])}, bc1)
+    cfg["flux_config"] = FSEC_FLUX["AUSMPW_plus"]
+    sim = set_simulator.Simulator(cfg)
+    U, aux, t = C(s1["U0"]), C(s1["aux0"]), 0.0
+    for step in range(1, 4):
+        U, aux, t, dt = sim.advance_func(U, aux, t, None)
+        out[f"step1d_AUSMPW_plus_U_{step}"] = np.asarray(U)
+        out[f"step1d_AUSMPW_plus_aux_{step}"] = np.asarray(aux)
+    print("Godunov steps", time.time() - t_start, flush=True)
+    np.savez_compressed(os.path.join(HERE, "fsec_si.npz"), **out)
+
+
+def gen_prim(ref):
+    """U_to_prim (solver_{1D,2D}/aux_func.py:39-51) of the reference on the
+    boundary-test states (moving, non-uniform gas) and on the rotating-
+    detonation initial state (nondimensional tables)."""
+    from janc_v2.model import thermo_model
+    from janc_v2.simulation import set_simulator
+    from janc_v2.solver_1D import aux_func as aux1
+    from janc_v2.solver_2D import aux_func as aux2
+    mech = os.path.join(ref, "examples", "9sp-19r-H2-Air.yaml")
+    out = {}
+    set_simulator.Simulator(_sim_config("2D", mech, {"dx": 1e-4, "dy": 1e-4},
+                                        {k: "slip_wall" for k in ("left_boundary", "right_boundary",
+                                                                  "bottom_boundary", "top_boundary")}))
+    b2 = np.load(os.path.join(HERE, "bc2d_si.npz"))
+    for n, v in zip(("rho", "u", "v", "Y", "p", "a"), aux2.U_to_prim(C(b2["U"]), C(b2["aux"]))):
+        out["p2d_" + n] = np.asarray(v)
+    # the thermo module's broadcast shapes follow the last configured dimension
+    set_simulator.Simulator(_sim_config("1D", mech, {"dx": 1e-4},
+                                        {"left_boundary": "slip_wall", "right_boundary": "slip_wall"}))
+    b1 = np.load(os.path.join(HERE, "bc1d_si.npz"))
+    for n, v in zip(("rho", "u", "Y", "p", "a"), aux1.U_to_prim(C(b1["U"]), C(b1["aux"]))):
+        out["p1d_" + n] = np.asarray(v)
+    P0, T0, R0, x0 = 10 * 101325, 300, 369, 0.08
+    cfg = _sim_config("2D", mech, {"dx": 1e-4 / x0, "dy": 1e-4 / x0},
+                      {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary",
+                                                "top_boundary")},
+                      nondim={"P0": P0, "T0": T0, "R0": R0, "x0": x0})
+    set_simulator.Simulator(cfg)
+    r = np.load(os.path.join(HERE, "step2d_rdc.npz"))
+    for n, v in zip(("rho", "u", "v", "Y", "p", "a"), aux2.U_to_prim(C(r["U_3"]), C(r["aux_3"]))):
+        out["prdc_" + n] = np.asarray(v)
+    np.savez(os.path.join(HERE, "prim_si.npz"), **out)
+
+
+def gen_cfl2d(ref):
+    """The 2D channel's time-step limit in the reference itself: a 128 x 8
+    strip at config-1 spacing (0.2 m / 1024), slab = first 21 columns at
+    30 atm and 3000 K with a seeded +-5 % temperature perturbation, slip
+    walls left, bottom and top, zero gradient right; up to 100 steps of
+    Simulator.advance_func at CFL 0.1 and 0.05.  Records the first step
+    whose state is non-finite (-1: none) and the states at steps 1 and 10."""
+    from janc_v2.model import thermo_model
+    from janc_v2.simulation import set_simulator
+    mech = os.path.join(ref, "examples", "9sp-19r-H2-Air.yaml")
+    t_start = time.time()
+    nx, ny = 128, 8
+    d = 0.2 / 1024
+    rng = np.random.default_rng(7)
+    P = np.full((1, nx, ny), 101325.0)
+    T = np.full((1, nx, ny), 300.0)
+    Y = np.tile(_stoich_Y(1.0)[:, None, None], (1, nx, ny))
+    P[:, :21] = 30 * 101325.0
+    T[:, :21] = 3000.0 * (1 + 0.05 * rng.uniform(-1, 1, (1, 21, ny)))
+    bc = {"left_boundary": "slip_wall", "right_boundary": "zero_gradient",
+          "bottom_boundary": "slip_wall", "top_boundary": "slip_wall"}
+    set_simulator.Simulator(_sim_config("2D", mech, {"dx": d, "dy": d}, bc, cfl=0.1))  # thermo tables
+    U0, aux0 = _state(thermo_model, P, T, Y)
+    rec = {"U0": U0, "aux0": aux0, "dx": d}
+    for cfl in (0.1, 0.05):
+        sim = set_simulator.Simulator(_sim_config("2D", mech, {"dx": d, "dy": d}, bc, cfl=cfl))
+        U, aux, t = C(U0), C(aux0), 0.0
+        bad = -1
+        for step in range(1, 101):
+            U, aux, t, dt = sim.advance_func(U, aux, t, None)
+            if step in (1, 10):
+                rec[f"cfl{cfl}_U_{step}"] = np.asarray(U)
+                rec[f"cfl{cfl}_aux_{step}"] = np.asarray(aux)
+            if not np.all(np.isfinite(np.asarray(U))):
+                bad = step
+                break
+        rec[f"cfl{cfl}_first_nonfinite_step"] = np.array(bad)
+        print(f"2D strip CFL {cfl}: first non-finite step {bad}", time.time() - t_start, flush=True)
+    np.savez_compressed(os.path.join(HERE, "cfl2d_strip.npz"), **rec)
+
+
+def gen_mid2d(ref):
+    """A mid-size version of the 2D channel (config-1 spacing 0.2 m / 1024,
+    128 x 64 cells, slab = first 21 columns at 30 atm / 3000 K with 8 seeded
+    Gaussian temperature blobs of +-5 % and radius 2-6 cells,
+    default_rng(1); slip walls left, bottom and top, zero gradient right) for
+    200 steps of the reference's Simulator.advance_func at CFL 0.05; the
+    state at steps 1, 20 and 200 and every dt."""
+    from janc_v2.model import thermo_model
+    from janc_v2.simulation import set_simulator
+    mech = os.path.join(ref, "examples", "9sp-19r-H2-Air.yaml")
+    t_start = time.time()
+    nx, ny, slab = 128, 64, 21
+    d = 0.2 / 1024
+    rng = np.random.default_rng(1)
+    P = np.full((1, nx, ny), 101325.0)
+    T = np.full((1, nx, ny), 300.0)
+    Y = np.tile(_stoich_Y(1.0)[:, None, None], (1, nx, ny))
+    xs = np.arange(slab)[:, None]
+    ys = np.arange(ny)[None, :]
+    bump = np.zeros((slab, ny))
+    for _ in range(8):
+        a = rng.uniform(-0.05, 0.05)
+        sig = rng.uniform(2.0, 6.0)
+        cx = rng.uniform(0, slab)
+        cy = rng.uniform(0, ny)
+        bump += a * np.exp(-((xs - cx) ** 2 + (ys - cy) ** 2) / (2 * sig ** 2))
+    P[0, :slab] = 30 * 101325.0
+    T[0, :slab] = 3000.0 * (1 + bump)
+    bc = {"left_boundary": "slip_wall", "right_boundary": "zero_gradient",
+          "bottom_boundary": "slip_wall", "top_boundary": "slip_wall"}
+    sim = set_simulator.Simulator(_sim_config("2D", mech, {"dx": d, "dy": d}, bc, cfl=0.05))
+    U0, aux0 = _state(thermo_model, P, T, Y)
+    rec = {"U0": U0, "aux0": aux0, "dx": d, "cfl": 0.05}
+    U, aux, t = C(U0), C(aux0), 0.0
+    dts = []
+    for step in range(1, 201):
+        U, aux, t, dt = sim.advance_func(U, aux, t, None)
+        dts.append(float(dt))
+        if step in (1, 20, 200):
+            rec[f"U_{step}"] = np.asarray(U)
+            rec[f"aux_{step}"] = np.asarray(aux)
+            print(f"128x64 channel: step {step}", time.time() - t_start, flush=True)
+    rec["dts"] = np.array(dts)
+    np.savez_compressed(os.path.join(HERE, "channel128x64_200.npz"), **rec)
+
+
+GROUPS = {"long1d": gen_long1d, "fsec": gen_fsec, "prim": gen_prim, "cfl2d": gen_cfl2d, "mid2d": gen_mid2d}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("JANC_REF"),
+                    help="checkout of the JANC repository (default: $JANC_REF)")
+    ap.add_argument("--groups", default="core",
+                    help="comma-separated fixture groups: core (the original set), " + ", ".join(GROUPS))
     args = ap.parse_args()
     ref = args.ref
+    if not ref:
+        ap.error("give the JANC checkout with --ref or JANC_REF")
     _setup(ref)
+    groups = args.groups.split(",")
+    for g in groups:
+        if g != "core":
+            GROUPS[g](ref)
+    if "core" in groups:
+        gen_core(ref)
+
+
+def gen_core(ref):
+    """The original fixture set (a few minutes)."""
     import jax.numpy as jnp
     from janc_v2.model import thermo_model, reaction_model
     from janc_v2.simulation import set_simulator
