@@ -1,7 +1,8 @@
 """Build the sm_100a shared library ``janc_b200/libjanc_b200.so`` in-tree.
 
-Translation units: ``jb_strict.cu`` (-fmad=false, the reference's rounding),
-``jb_fast.cu`` (FMA contraction, FP64 and mixed variants), ``jb_ensemble.cu``
+Translation units: ``jb_strict*.cu`` (-fmad=false, the reference's rounding),
+``jb_fast*.cu`` (FMA contraction, FP64 and mixed variants; each variant is
+split into parts compiled in parallel, see ``jb_variant.inc``), ``jb_ensemble.cu``
 (the persistent batched kernel and its C ABI), ``jb_adjoint.cu`` (the
 reverse-mode kernels), ``jb_api.cu`` (the C ABI of the single-case solver),
 ``jb_noalloc.cu`` and ``jb_probe.cu``.
@@ -19,8 +20,13 @@ LIB = os.path.join(HERE, "libjanc_b200.so")
 OBJ = os.path.join(HERE, "_objs")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-UNITS = [("jb_ensemble.cu", ["-fmad=true"]), ("jb_strict.cu", ["-fmad=false"]), ("jb_fast.cu", ["-fmad=true"]),
-         ("jb_adjoint.cu", ["-fmad=true"]), ("jb_api.cu", []), ("jb_probe.cu", []), ("jb_noalloc.cu", [])]
+# the slowest units first: they start before the pool fills
+UNITS = [("jb_ensemble.cu", ["-fmad=true"]), ("jb_fast_flux32.cu", ["-fmad=true"]),
+         ("jb_fast_god32.cu", ["-fmad=true"]), ("jb_fast_flux64.cu", ["-fmad=true"]),
+         ("jb_fast_god64.cu", ["-fmad=true"]), ("jb_fast.cu", ["-fmad=true"]),
+         ("jb_strict_flux.cu", ["-fmad=false"]), ("jb_strict_god.cu", ["-fmad=false"]),
+         ("jb_strict.cu", ["-fmad=false"]), ("jb_adjoint.cu", ["-fmad=true"]), ("jb_api.cu", []),
+         ("jb_probe.cu", []), ("jb_noalloc.cu", [])]
 
 
 def _nvcc():

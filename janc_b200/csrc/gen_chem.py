@@ -62,6 +62,7 @@ def generate(path=None):
     w("#ifdef JB_NS")
     w("namespace jb {")
     w("namespace JB_NS {")
+    w("namespace {")
     w("")
     w("// Phase A: rates of every reaction for one cell.  Writes q_i = kf - kb,")
     w("// F_i = M_i kf and B_i = M_i kb to shared memory (layout [i][3][stride])")
@@ -163,6 +164,7 @@ def generate(path=None):
         w("  }")
     w("}")
     w("")
+    w("}  // namespace")
     w("}  // namespace JB_NS")
     w("}  // namespace jb")
     w("#endif")

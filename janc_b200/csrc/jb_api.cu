@@ -181,8 +181,9 @@ int jb_create(const jb_mech_params* mech, int dim, int nx, int ny, double dx, do
   if (e == cudaSuccess) e = cudaMalloc(&h->slots, sizeof(jb_slots));
   if (e == cudaSuccess) e = cudaMemset(h->strips, 0, bytes_strip);
   if (e == cudaSuccess) e = cudaMemset(h->slots, 0, sizeof(jb_slots));
-  // mixed 2D: float32 primitives and x flux differences of a stage
-  const size_t bytes_fwork = precision == JB_PREC_MIXED && dim == 2 ? sizeof(float) * 15 * nc : 0;
+  // mixed 2D: float32 primitives of the stage state and of the state being
+  // written (two buffers used in turn), then the x flux differences
+  const size_t bytes_fwork = precision == JB_PREC_MIXED && dim == 2 ? sizeof(float) * 18 * nc : 0;
   if (e == cudaSuccess && bytes_fwork) e = cudaMalloc(&h->fwork, bytes_fwork);
   if (e != cudaSuccess) {
     jb_destroy(h);
@@ -303,8 +304,8 @@ int jb_flux_func(jb_handle* h, const double* U, const double* aux, double dt, do
   if (int rc = exchange(h, U, aux, JB_XCH_HALO, 3, st)) return rc;
   if (h->grid.visc)
     JB_TRY(o.visc(h->dim, h->mech, h->grid, h->tr, U, aux, h->strips, h->vbuf, h->vcell, st), "viscous");
-  JB_TRY(o.flux(h->dim, 0, h->mech, h->grid, U, aux, nullptr, rhs, nullptr, h->strips, h->slots, 3,
-                -1, dt, nullptr, st),
+  JB_TRY(o.flux(h->dim, 0, h->mech, h->grid, U, aux, nullptr, rhs, h->strips, h->slots, 3, jb_fin_cand(nullptr, -1),
+                nullptr, nullptr, dt, st),
          "flux");
   return JB_OK;
 }
@@ -343,7 +344,7 @@ int jb_reaction_source_terms(jb_handle* h, const double* U, const double* aux, d
   if (!h || !U || !aux || !S) return set_err(h, JB_ERR_ARG, "null pointer");
   if (!(dt > 0.0)) return set_err(h, JB_ERR_ARG, "dt must be positive");
   cudaStream_t st = (cudaStream_t)stream;
-  JB_TRY(h->ops->chem(h->dim, true, h->mech, h->grid, U, aux, S, nullptr, h->slots, -1, dt, st),
+  JB_TRY(h->ops->chem(h->dim, true, h->mech, h->grid, U, aux, S, jb_fin_cand(nullptr, -1), h->slots, dt, st),
          "chem");
   return JB_OK;
 }
@@ -366,6 +367,7 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     return set_err(h, JB_ERR_ARG, "probe pressures need a 2D handle with jb_set_probe");
   if (rec && (!rec_slots || !chemistry)) return set_err(h, JB_ERR_ARG, "a record needs rec_slots");
   if (rec && h->xch) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint record is single-domain");
+  if (!chemistry && nsteps != 1) return set_err(h, JB_ERR_ARG, "the flux-only step is one step");
   cudaStream_t st = (cudaStream_t)stream;
   const jb::Ops& o = *h->ops;
   const int d = h->dim;
@@ -378,10 +380,27 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     JB_TRY(cudaMemcpyAsync(rec, U, sizeof(double) * nU, cudaMemcpyDeviceToDevice, st), "record U0");
     JB_TRY(cudaMemcpyAsync(rec + nU, aux, sizeof(double) * nA, cudaMemcpyDeviceToDevice, st), "record aux0");
   }
+  // Per-cell mode (mixed, 2D): each stage kernel and the chemistry finish
+  // their new state's temperature per cell and reduce its LF alpha (and,
+  // after the chemistry, the CFL minimum) in their epilogue, so no select
+  // pass runs between them.  Global-stop mode (strict and fp64, and 1D): the
+  // kernels write the Halley iterates and a select pass after each picks the
+  // reference's iteration count.
+  const bool pc = o.per_cell_2d && d == 2;
+  // mixed 2D: float32 u, v, p of the current state (pin) and the buffer the
+  // next kernel writes (pout), swapped after each writer
+  float* pin = h->fwork ? static_cast<float*>(h->fwork) : nullptr;
+  float* pout = pin ? pin + 3 * g.ncell : nullptr;
+  void* dfx = pin ? static_cast<void*>(pin + 6 * g.ncell) : nullptr;
+  auto swap_prims = [&]() {
+    float* t = pin;
+    pin = pout;
+    pout = t;
+  };
   JB_TIMED(JB_KCAT_OTHER, o.slots_reset(h->slots, st), "slots_reset");
   // alpha (and CFL minimum) of the initial state, ghost strips for stage 1
   JB_TIMED(JB_KCAT_SELECT, o.select(d, false, true, use_cfl, m, g, U, aux, nullptr, nullptr, h->strips, h->slots, -1, 3,
-                  h->fwork, st),
+                  pin, st),
          "prep");
   for (int s = 0; s < nsteps; ++s) {
     double* r = rec ? rec + s * RS : nullptr;
@@ -395,54 +414,89 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     double* A3 = r ? W3 + nU : h->auxw[0];
     double* Uo = r ? r + RS : U_out;
     double* Ao = r ? r + RS + nU : aux_out;
+    if (!chemistry) {  // advance_flux only (TVD_RK3.py:5-12): stage 3 writes the result
+      W3 = U_out;
+      A3 = aux_out;
+    }
     // slabs: the CFL minimum over the ranks and the halo of the step's state
     if (int rc = exchange(h, Un, an, (use_cfl ? JB_XCH_DT : 0) | JB_XCH_HALO, 3, st)) return rc;
     JB_TIMED(JB_KCAT_OTHER, o.step_begin(h->slots, use_cfl ? cfl : 0.0, dt_fixed, dt_hist, s, st), "step_begin");
     // stage 1: U1 = U + L(U)
     if (g.visc)
       JB_TIMED(JB_KCAT_FLUX, o.visc(d, m, g, h->tr, Un, an, h->strips, h->vbuf, h->vcell, st), "viscous");
-    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 1, m, g, Un, an, Un, W1, h->cand, h->strips, h->slots, 0, 0, 0.0, h->fwork, st), "stage1");
-    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W1, nullptr, h->cand, A1, h->strips,
-                    h->slots, 0, 1, h->fwork, st),
-           "select1");
+    if (pc) {
+      JB_TIMED(JB_KCAT_FLUX, o.flux(d, 1, m, g, Un, an, Un, W1, h->strips, h->slots, 0,
+                                    jb_fin_cell(A1, pout, 1, 0), pin, dfx, 0.0, st), "stage1");
+      swap_prims();
+      JB_TIMED(JB_KCAT_SELECT, o.strips(d, m, g, W1, A1, h->strips, h->slots, 1, st), "strips1");
+    } else {
+      JB_TIMED(JB_KCAT_FLUX, o.flux(d, 1, m, g, Un, an, Un, W1, h->strips, h->slots, 0, jb_fin_cand(h->cand, 0),
+                                    pin, dfx, 0.0, st), "stage1");
+      JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W1, nullptr, h->cand, A1, h->strips,
+                      h->slots, 0, 1, pin, st),
+             "select1");
+    }
     if (int rc = exchange(h, W1, A1, JB_XCH_HALO, 1, st)) return rc;
     // stage 2: U2 = 3/4 U + 1/4 (U1 + L(U1))
     if (g.visc)
       JB_TIMED(JB_KCAT_FLUX, o.visc(d, m, g, h->tr, W1, A1, h->strips, h->vbuf, h->vcell, st), "viscous");
-    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 2, m, g, W1, A1, Un, W2, h->cand, h->strips, h->slots, 1, 1,
-                  0.0, h->fwork, st),
-           "stage2");
-    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W2, nullptr, h->cand, A2, h->strips,
-                    h->slots, 1, 2, h->fwork, st),
-           "select2");
+    if (pc) {
+      JB_TIMED(JB_KCAT_FLUX, o.flux(d, 2, m, g, W1, A1, Un, W2, h->strips, h->slots, 1,
+                                    jb_fin_cell(A2, pout, 2, 0), pin, dfx, 0.0, st), "stage2");
+      swap_prims();
+      JB_TIMED(JB_KCAT_SELECT, o.strips(d, m, g, W2, A2, h->strips, h->slots, 2, st), "strips2");
+    } else {
+      JB_TIMED(JB_KCAT_FLUX, o.flux(d, 2, m, g, W1, A1, Un, W2, h->strips, h->slots, 1, jb_fin_cand(h->cand, 1),
+                                    pin, dfx, 0.0, st), "stage2");
+      JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, false, m, g, W2, nullptr, h->cand, A2, h->strips,
+                      h->slots, 1, 2, pin, st),
+             "select2");
+    }
     if (int rc = exchange(h, W2, A2, JB_XCH_HALO, 2, st)) return rc;
     // stage 3: U3 = 1/3 U + 2/3 (U2 + L(U2))
     if (g.visc)
       JB_TIMED(JB_KCAT_FLUX, o.visc(d, m, g, h->tr, W2, A2, h->strips, h->vbuf, h->vcell, st), "viscous");
-    JB_TIMED(JB_KCAT_FLUX, o.flux(d, 3, m, g, W2, A2, Un, W3, h->cand, h->strips, h->slots, 2, 2,
-                  0.0, h->fwork, st),
-           "stage3");
-    if (!chemistry) {
-      // advance_flux only (TVD_RK3.py:5-12): U3, aux3 are the result
-      const size_t bytes = sizeof(double) * g.nv * (size_t)g.ncell;
-      JB_TRY(cudaMemcpyAsync(U_out, W3, bytes, cudaMemcpyDeviceToDevice, st), "copy U3");
-      JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, U_out, nullptr, h->cand, aux_out,
-                                        h->strips, h->slots, 2, 3, h->fwork, st),
+    if (pc) {
+      // without the chemistry this is the step's result: its alpha, CFL
+      // minimum and primitives serve the next step
+      const jb_fin f3 = chemistry ? jb_fin_cell(A3, nullptr, -1, 0) : jb_fin_cell(A3, pout, 3, use_cfl);
+      JB_TIMED(JB_KCAT_FLUX, o.flux(d, 3, m, g, W2, A2, Un, W3, h->strips, h->slots, 2, f3, pin, dfx, 0.0, st),
+               "stage3");
+      if (!chemistry) {
+        swap_prims();
+        JB_TIMED(JB_KCAT_SELECT, o.strips(d, m, g, W3, A3, h->strips, h->slots, 3, st), "strips3");
+        continue;
+      }
+    } else {
+      JB_TIMED(JB_KCAT_FLUX, o.flux(d, 3, m, g, W2, A2, Un, W3, h->strips, h->slots, 2, jb_fin_cand(h->cand, 2),
+                                    pin, dfx, 0.0, st), "stage3");
+      if (!chemistry) {
+        JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, W3, nullptr, h->cand, A3,
+                                          h->strips, h->slots, 2, 3, pin, st),
+                 "select3");
+        continue;
+      }
+      // the adjoint record keeps aux3; otherwise the stage-3 temperature is
+      // taken from the iterates inside the chemistry kernel
+      if (rec)
+        JB_TIMED(JB_KCAT_SELECT, o.select(d, true, false, false, m, g, W3, nullptr, h->cand, A3, h->strips,
+                        h->slots, 2, 0, nullptr, st),
                "select3");
-      continue;
     }
-    // chemistry and the final temperature solve; without a record the
-    // stage-3 temperature is taken from the iterates inside the chemistry
-    // kernel (its gamma is not used by anything that follows)
-    if (rec)
-      JB_TIMED(JB_KCAT_SELECT, o.select(d, true, false, false, m, g, W3, nullptr, h->cand, A3, h->strips,
-                      h->slots, 2, 0, nullptr, st),
-             "select3");
-    JB_TIMED(JB_KCAT_CHEM, o.chem(d, false, m, g, W3, rec ? A3 : nullptr, Uo, h->cand, h->slots, 3, 0.0, st),
-             "chem");
-    JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, Uo, nullptr, h->cand, Ao, h->strips,
-                    h->slots, 3, 3, h->fwork, st),
-           "select4");
+    // chemistry and the final temperature solve
+    if (pc) {
+      JB_TIMED(JB_KCAT_CHEM, o.chem(d, false, m, g, W3, A3, Uo, jb_fin_cell(Ao, pout, 3, use_cfl), h->slots, 0.0, st),
+               "chem");
+      swap_prims();
+      JB_TIMED(JB_KCAT_SELECT, o.strips(d, m, g, Uo, Ao, h->strips, h->slots, 3, st), "strips4");
+    } else {
+      JB_TIMED(JB_KCAT_CHEM, o.chem(d, false, m, g, W3, rec ? A3 : nullptr, Uo, jb_fin_cand(h->cand, 3), h->slots,
+                                    0.0, st),
+               "chem");
+      JB_TIMED(JB_KCAT_SELECT, o.select(d, true, true, use_cfl, m, g, Uo, nullptr, h->cand, Ao, h->strips,
+                      h->slots, 3, 3, pin, st),
+             "select4");
+    }
     if (rec)
       JB_TRY(cudaMemcpyAsync(rec_slots + s * (sizeof(jb_slots) / sizeof(double)), h->slots, sizeof(jb_slots),
                              cudaMemcpyDeviceToDevice, st),

@@ -15,6 +15,7 @@ static const signed char JB_GEN_VSUM[19] = {0, 0, 0, 0, 0, -1, -1, -1, -1, 0, 0,
 #ifdef JB_NS
 namespace jb {
 namespace JB_NS {
+namespace {
 
 // Phase A: rates of every reaction for one cell.  Writes q_i = kf - kb,
 // F_i = M_i kf and B_i = M_i kb to shared memory (layout [i][3][stride])
@@ -953,6 +954,7 @@ __device__ __forceinline__ void chem_jac_gen(const MP& m, const double* rMX, con
   }
 }
 
+}  // namespace
 }  // namespace JB_NS
 }  // namespace jb
 #endif

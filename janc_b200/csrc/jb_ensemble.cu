@@ -167,7 +167,10 @@ __device__ __noinline__ void chem_pass(const jb_ens_inst& I, int rank, int n3, d
   unsigned bits = 0, st = 0;
   for (int j = rank; j < I.nchunks; j += I.ncta) {
     long long c = (long long)j * NT + threadIdx.x;
-    if (c < nc) chem_cell_step<1, false, true>(c_mech, g, I.W0, I.cand[n3 * nc + c], I.U, I.cand, c, dt, sh, bits, st);
+    double amx = 0.0, amy = 0.0, dtm = 0.0;
+    if (c < nc)
+      chem_cell_step<1, false, true>(c_mech, g, I.W0, I.cand[n3 * nc + c], I.U, jb_fin_cand(I.cand, 0), c, dt, sh,
+                                     bits, st, amx, amy, dtm, nullptr);
   }
   block_reduce_store(0.0, 0.0, 0.0, bits | (st << 16), s, 0, false, false, 3);
 }

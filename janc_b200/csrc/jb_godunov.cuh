@@ -180,8 +180,8 @@ __host__ __device__ constexpr size_t god2_smem() {
 template <int STAGE, int RS, class RW>
 __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk, const double* __restrict__ Un,
-                                                 double* __restrict__ out, double* __restrict__ cand,
-                                                 const double* __restrict__ strips, Slots* slots, int midx,
+                                                 double* __restrict__ out,
+                                                 const double* __restrict__ strips, Slots* slots, jb_fin fin,
                                                  double dt_arg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   RW* sW = reinterpret_cast<RW*>(smraw);                                // [12][PX2][PY2]
@@ -251,6 +251,7 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
   const bool live = owner && gx < g.nx && gy < g.ny;
   const size_t cell = (size_t)gx * g.ny + gy;
   unsigned bits = 0;
+  double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
   if (live) {
     double q[12];
 #pragma unroll
@@ -271,21 +272,11 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
       out[f * nc + cell] = r;
       q[f] = r;
     }
-    if (STAGE != 0) {
-      const double rho = q[0];
-      const double u = q[1] / rho, v = q[2] / rho;
-      const double e = q[3] / rho - 0.5 * (u * u + v * v);
-      double Y8[NR], Yf[NS];
-#pragma unroll
-      for (int k = 0; k < NR; ++k) Y8[k] = q[4 + k] / rho;
-      fill_Y(Y8, Yf);
-      double cnd[JB_NCAND];
-      bits = halley_any(m, e, Yf, get_R(m, Yf), auxk[nc + cell], cnd);
-#pragma unroll
-      for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
-    }
+    // float32 reconstruction = the mixed variant: per-cell temperature solve
+    if (STAGE != 0)
+      bits = finish_state<2, sizeof(RW) == 4>(m, g, fin, q, auxk[nc + cell], cell, amx, amy, dtm, slots);
   }
-  if (STAGE != 0) block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
+  if (STAGE != 0) finish_reduce(fin, amx, amy, dtm, bits, slots);
 }
 
 // 1D: a block of NT1 threads covers NT1 - 1 cells and their NT1 faces.

@@ -17,6 +17,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "jb_fin.h"
 #include "jb_types.h"
 
 #ifndef JB_NS
@@ -25,6 +26,7 @@
 
 namespace jb {
 namespace JB_NS {
+namespace {  // internal linkage: several translation units include this header
 
 constexpr int NS = 9;
 constexpr int NR = 8;
@@ -335,6 +337,194 @@ __device__ __forceinline__ Prim<DIM> u_to_prim(const MP& m, const double* q, dou
   r.p = r.rho * r.R * T;
   r.a = sqrt(gamma * r.p / r.rho);
   return r;
+}
+
+#if JB_FAST
+// Per-cell Halley solve of the fp64 and mixed variants.  The reference
+// (thermo_model.py:135-153) iterates all cells until the largest residual is
+// within tol, so every cell except the slowest ones takes at least one more
+// step after its own residual is within tol, which polishes it to round-off.
+// Here each cell iterates until its residual is within tol and then takes
+// that one more step (at most HALLEY_MAX steps; a NaN residual stops at once,
+// as it stops the reference's loop).  The result equals the global rule's to
+// round-off except for the cells that set the global count, which differ by
+// at most tol / cv (in SI units ~1e-12 K; in nondimensional units, where e is
+// O(1), up to ~1e-9 relative).  Returns T and cp at the last evaluated
+// temperature (get_T_nasa7 returns gamma there).
+__device__ __forceinline__ bool halley_go(double res, bool& polished) {
+  if (fabs(res) > HALLEY_TOL) return true;
+  if (polished || res == 0.0 || res != res) return false;  // converged: one more step, none if exact or NaN
+  polished = true;
+  return true;
+}
+
+// Mixture enthalpy polynomial of one NASA7 range (the Y-weighted sum of the
+// species' h coefficients).  cp = dh/dT and dcp/dT = d2h/dT2 in real
+// arithmetic (the tables' cp and dcp are the same NASA7 coefficients times
+// the powers), so the per-cell solve holds six coefficients and takes h, cp
+// and dcp from one Horner pass with two derivatives.
+template <bool LO>
+__device__ __forceinline__ void mix_h_range(const MP& m, const double* Yf, double* H) {
+  const auto& h = LO ? m.h_lo : m.h_hi;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    double c = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) c += Yf[k] * h[k][j];
+    H[j] = c;
+  }
+}
+
+__device__ __forceinline__ void mix_h(const MP& m, const double* Yf, bool lo, double* H) {
+  if (lo) mix_h_range<true>(m, Yf, H);
+  else mix_h_range<false>(m, Yf, H);
+}
+
+// h(T), cp = h'(T) and dcp = h''(T) of a degree-5 polynomial in the tables' order
+__device__ __forceinline__ void poly6_d2(const double* c, double T, double& h, double& cp, double& dcp) {
+  double p = c[0], d1 = 0.0, d2 = 0.0;
+#pragma unroll
+  for (int j = 1; j < 6; ++j) {
+    d2 = d2 * T + d1;
+    d1 = d1 * T + p;
+    p = p * T + c[j];
+  }
+  h = p;
+  cp = d1;
+  dcp = 2.0 * d2;
+}
+
+__device__ __forceinline__ double halley_cell(const MP& m, double e, const double* Yf, double R, double T0,
+                                              double& cp_out) {
+  double T = T0;
+  bool polished = false;
+  if (m.tcr_uniform) {
+    const double Tcr = m.Tcr[0];
+    bool lo = T < Tcr;
+    double H[6], h, cp, d2;
+    mix_h(m, Yf, lo, H);
+    poly6_d2(H, T, h, cp, d2);
+    double res = (h - R * T) - e;
+#pragma unroll 1
+    for (int i = 0; i < HALLEY_MAX && halley_go(res, polished); ++i) {
+      const double d1 = cp - R;
+      T = T + ((-2.0 * res) * d1) / ((2.0 * (d1 * d1)) - res * d2);
+      const bool lo_i = T < Tcr;
+      if (lo_i != lo) {  // the iterate crossed the range boundary (rare)
+        lo = lo_i;
+        mix_h(m, Yf, lo, H);
+      }
+      poly6_d2(H, T, h, cp, d2);
+      res = (h - R * T) - e;
+    }
+    cp_out = cp;
+    return T;
+  }
+  Th t = thermo_mix(m, T, Yf);
+  double res = (t.h - R * T) - e;
+#pragma unroll 1
+  for (int i = 0; i < HALLEY_MAX && halley_go(res, polished); ++i) {
+    const double d1 = t.cp - R;
+    T = T + ((-2.0 * res) * d1) / ((2.0 * (d1 * d1)) - res * t.dcp);
+    t = thermo_mix(m, T, Yf);
+    res = (t.h - R * T) - e;
+  }
+  cp_out = t.cp;
+  return T;
+}
+#endif
+
+// The temperature solve of a new state q (nv float64 fields) at cell c with
+// initial guess T0 (jb_fin.h).  The mode is fixed at compile time, as the
+// host's step sequence chooses it: CELL (per-cell) in the mixed variant's 2D
+// kernels, global stop otherwise (the fp64 and strict builds keep the
+// reference's global stopping rule exactly).  Global-stop mode: the Halley iterates into
+// fin.cand; returns the mask bits.  Per-cell mode: the converged (gamma, T)
+// into fin.aux, the float32 u, v, p into fin.prims, and the new state's wave
+// speeds and CFL candidate folded into amx, amy, dtm as the select pass does
+// (LF.py nanmax(|u| + a), set_simulator.py:420-443); returns status bits
+// << 16.
+template <int DIM, bool CELL>
+__device__ __forceinline__ unsigned finish_state(const MP& m, const Grid& g, const jb_fin& fin, const double* q,
+                                                 double T0, long long c, double& amx, double& amy, double& dtm,
+                                                 Slots* slots) {
+  constexpr int nY = DIM == 1 ? 3 : 4;
+  const long long nc = g.ncell;
+  const double rho = q[0];
+#if JB_FAST
+  if constexpr (DIM == 2 && CELL) {
+    // one reciprocal of rho; the primitives of the wave speeds as u_to_prim
+    // forms them (p = T sum_k (rho Y_k)/M_k, rho Y_N2 = rho - sum rho Y_k)
+    // are taken before the solve so that the state is no longer needed
+    const double ri = 1.0 / rho;
+    const double u = q[1] * ri, v = q[2] * ri;
+    const double e = q[3] * ri - 0.5 * (u * u + v * v);
+    double Y8[NR], Yf[NS];
+    double sr = q[nY], prs = m.invM[0] * q[nY];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      Y8[k] = q[nY + k] * ri;
+      if (k > 0) {
+        sr += q[nY + k];
+        prs += m.invM[k] * q[nY + k];
+      }
+    }
+    prs += m.invM[NR] * (rho - sr);
+    fill_Y(Y8, Yf);
+    const double R = get_R(m, Yf);
+    double cp;
+    const double T = halley_cell(m, e, Yf, R, T0, cp);
+    const double gamma = cp / (cp - R);
+    fin.aux[c] = gamma;
+    fin.aux[nc + c] = T;
+    unsigned st = 0;
+    if (fin.aidx >= 0 || fin.cfl || fin.prims) {
+      const double p = prs * T;
+      const double a = sqrt(gamma * p * ri);
+      if (fin.prims) {
+        fin.prims[c] = (float)u;
+        fin.prims[nc + c] = (float)v;
+        fin.prims[2 * nc + c] = (float)p;
+      }
+      const double sx = fabs(u) + a, sy = fabs(v) + a;
+      amx = fmax(amx, sx);
+      amy = fmax(amy, sy);
+      if (!(sx == sx) || !(T == T)) st |= JB_ERR_NONFINITE;
+      if (fin.cfl) {
+        const double d = 1.0 / (sx * g.idx + sy * g.idy);
+        dtm = fmin(dtm, d);
+        if (!(d == d) || !(d > 0.0)) st |= JB_ERR_NONFINITE;
+        if (!(d == d)) atomicOr(&slots->dtnan, 1u);  // jnp.min propagates NaN
+      }
+    } else if (!(T == T)) {
+      st |= JB_ERR_NONFINITE;
+    }
+    return st << 16;
+  } else
+#endif
+  {
+    (void)amx; (void)amy; (void)dtm; (void)slots;
+    const double u = q[1] / rho, v = DIM == 2 ? q[2] / rho : 0.0;
+    const double e = q[nY - 1] / rho - 0.5 * (u * u + v * v);
+    double Y8[NR], Yf[NS];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) Y8[k] = q[nY + k] / rho;
+    fill_Y(Y8, Yf);
+    const double R = get_R(m, Yf);
+    double cnd[JB_NCAND];
+    const unsigned bits = halley_any(m, e, Yf, R, T0, cnd);
+#pragma unroll
+    for (int i = 0; i < JB_NCAND; ++i) fin.cand[i * nc + c] = cnd[i];
+    return bits;
+  }
+}
+
+// Block-level end of finish_state (all threads of the block call it).
+__device__ __forceinline__ void finish_reduce(const jb_fin& fin, double amx, double amy, double dtm,
+                                              unsigned bits, Slots* slots) {
+  const bool cell_mode = fin.aux != nullptr;
+  block_reduce_store(amx, amy, dtm, bits, slots, fin.aidx < 0 ? 0 : fin.aidx, cell_mode && fin.aidx >= 0,
+                     cell_mode && fin.cfl, cell_mode ? -1 : fin.midx);
 }
 
 // ---------------------------------------------------------------------------
@@ -866,9 +1056,9 @@ template <int STAGE, class R, bool VISC, bool SW = false>
 __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk,
                                                  const double* __restrict__ Un,
-                                                 double* __restrict__ out, double* __restrict__ cand,
+                                                 double* __restrict__ out,
                                                  const double* __restrict__ strips, Slots* slots,
-                                                 int aidx, int midx, double dt_arg) {
+                                                 int aidx, jb_fin fin, double dt_arg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   constexpr int nv = 12, nq = nv + 1;
   constexpr bool EXACT = sizeof(R) == sizeof(double);
@@ -1039,81 +1229,118 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
   }
 
   if (STAGE == 0) return;
-  // ---- Halley iterates of update_aux on the new state
+  // ---- update_aux on the new state (Halley iterates, or per cell)
   unsigned bits = 0;
+  double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
   if (live) {
     double q[12];
     for (int f = 0; f < 12; ++f) q[f] = out[f * nc + cell];
-    double rho = q[0];
-    double u = q[1] / rho, v = q[2] / rho;
-    double e = q[3] / rho - 0.5 * (u * u + v * v);
-    double Y8[NR], Yf[NS];
-#pragma unroll
-    for (int k = 0; k < NR; ++k) Y8[k] = q[4 + k] / rho;
-    fill_Y(Y8, Yf);
-    double Rmix = get_R(m, Yf);
-    double T0 = EXACT ? (double)sQ[nv * SM2_Q + (ix + 3) * PY2 + (iy + 3)] : auxk[nc + cell];
-    double cnd[JB_NCAND];
-    bits = halley_any(m, e, Yf, Rmix, T0, cnd);
-#pragma unroll
-    for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
+    const double T0 = EXACT ? (double)sQ[nv * SM2_Q + (ix + 3) * PY2 + (iy + 3)] : auxk[nc + cell];
+    bits = finish_state<2, !EXACT>(m, g, fin, q, T0, cell, amx, amy, dtm, slots);
   }
-  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
+  finish_reduce(fin, amx, amy, dtm, bits, slots);
 }
 
 #if JB_FAST
 // ---------------------------------------------------------------------------
 // mixed-precision 2D RK stage as an x-line sweep plus y runs (STAGE 1..3)
 // ---------------------------------------------------------------------------
-// The same arithmetic as k_flux2d<S, float> (float32 LF / WENO on float32
-// primitives, float64 RK combination and Halley iterates), organised
-// without block barriers:
-//   k_sweep_x    one thread per (y line, x segment of SX_R cells, field):
-//                a register window of H+ / H- walks the segment's faces and
-//                writes the x flux difference F_{i+1} - F_i of each cell
-//   k_flux_y_rk  one warp per run of 32 cells along y: H+ / H- of all fields
-//                on the run and its 3 + 3 halo cells, the 33 y faces and the
-//                differences, then the RK combination with the x part and
-//                the Halley iterates of the new state
-// The primitives (u, v, p as float32) of the stage state come from the
-// select pass that produced its temperature (prims[3][ncell]).
+// float32 LF splitting and WENO5-JS on float32 primitives, float64 RK
+// combination and temperature solve, organised without block barriers:
+//   k_sweep_x    one thread per (y line, x segment of SX_R cells, field
+//                pair): a register window of the split fluxes walks the
+//                segment's faces and writes the x flux difference
+//                F_{i+1/2} - F_{i-1/2} of each cell
+//   k_flux_y_rk  one warp per run of 32 cells along y: split fluxes of all
+//                fields on the run and its 3 + 3 halo cells, the 33 y faces
+//                and the differences, then the RK combination with the x
+//                part and the temperature solve of the new state
+// Fields are handled in pairs (rho, rho u), (rho v, rho E), (rho Y_1, rho
+// Y_2), ... with sm_100's paired float32 instructions (FFMA2 / FADD2 /
+// FMUL2), which issue two float32 operations at once.  The x differences are
+// stored as float2 pairs: dfx[6][ncell][2].  The stage state's float32 u, v,
+// p come from the kernel that wrote that state (prims[3][ncell]).
 #ifndef JB_SX_R
 #define JB_SX_R 16
 #endif
 constexpr int SX_R = JB_SX_R, SX_NT = 128;
 constexpr int YR_W = 8, YR_NT = 32 * YR_W;     // warps (runs) per block
 constexpr int YR_C = 38, YR_F = 33;            // window cells, faces per run
-constexpr size_t YR_SMEM = sizeof(float) * YR_W * (2 * 12 * YR_C + 12 * YR_F);
+constexpr size_t YR_SMEM = sizeof(float2) * YR_W * (2 * 6 * YR_C + 6 * YR_F);
 
-// Split fluxes of field f at one cell: F = vel q (+ p in the normal
-// momentum, + vel p in rho E), H+- = (F +- alpha q) / 2.
-__device__ __forceinline__ void split_h(int f, int fn, float q, float vel, float p, float al, float& hp,
-                                        float& hm) {
-  float F = vel * q;
-  if (f == fn) F += p;
-  if (f == 3) F += vel * p;
-  hp = 0.5f * (F + al * q);
-  hm = 0.5f * (F - al * q);
+typedef float2 f2;
+__device__ __forceinline__ f2 f2s(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 f2add(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 f2mul(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 f2fma(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+
+// WENO5-JS (reconstruction/WENO5_JS.py) of two fields at once: the
+// left-biased value at the face between c and d from cells a..e (the
+// right-biased value at the face between b and c is weno2(e, d, c, b, a)).
+// The inputs are split fluxes without the 1/2 (H' = F +- alpha q = 2 H), so
+// the smoothness indicators are formed as t^2 + 13/3 s^2 (16 IS) with eps
+// scaled by 16, which leaves every weight exactly as the reference's in real
+// arithmetic; the caller halves the face value.  Weights in the ratio form
+// to the smallest eps + IS (no float32 overflow for SI fluxes ~1e11), with
+// the linear weights C_k folded into the candidate polynomials.
+__device__ __forceinline__ f2 weno2(f2 a, f2 b, f2 c, f2 d, f2 e) {
+  const f2 t1 = f2fma(c, f2s(3.f), f2fma(b, f2s(-4.f), a));
+  const f2 s1 = f2add(f2fma(b, f2s(-2.f), a), c);
+  const f2 t2 = f2fma(d, f2s(-1.f), b);
+  const f2 s2 = f2add(f2fma(c, f2s(-2.f), b), d);
+  const f2 t3 = f2fma(c, f2s(3.f), f2fma(d, f2s(-4.f), e));
+  const f2 s3 = f2add(f2fma(d, f2s(-2.f), c), e);
+  const f2 e16 = f2s(16e-6f), k13 = f2s(13.f / 3.f);
+  const f2 e1 = f2fma(t1, t1, f2fma(f2mul(s1, k13), s1, e16));
+  const f2 e2 = f2fma(t2, t2, f2fma(f2mul(s2, k13), s2, e16));
+  const f2 e3 = f2fma(t3, t3, f2fma(f2mul(s3, k13), s3, e16));
+  const f2 mn = make_float2(fminf(e1.x, fminf(e2.x, e3.x)), fminf(e1.y, fminf(e2.y, e3.y)));
+  const f2 r1 = f2mul(mn, make_float2(__fdividef(1.f, e1.x), __fdividef(1.f, e1.y)));
+  const f2 r2 = f2mul(mn, make_float2(__fdividef(1.f, e2.x), __fdividef(1.f, e2.y)));
+  const f2 r3 = f2mul(mn, make_float2(__fdividef(1.f, e3.x), __fdividef(1.f, e3.y)));
+  const f2 w1 = f2mul(r1, r1), w2 = f2mul(r2, r2), w3 = f2mul(r3, r3);
+  // C_k times the candidate values (C = 1/10, 6/10, 3/10)
+  const f2 q1 = f2fma(c, f2s(11.f / 60.f), f2fma(b, f2s(-7.f / 60.f), f2mul(a, f2s(1.f / 30.f))));
+  const f2 q2 = f2fma(d, f2s(0.2f), f2fma(c, f2s(0.5f), f2mul(b, f2s(-0.1f))));
+  const f2 q3 = f2fma(e, f2s(-0.05f), f2fma(d, f2s(0.25f), f2mul(c, f2s(0.1f))));
+  const f2 num = f2fma(w3, q3, f2fma(w2, q2, f2mul(w1, q1)));
+  const f2 den = f2fma(w3, f2s(0.3f), f2fma(w2, f2s(0.6f), f2mul(w1, f2s(0.1f))));
+  return f2mul(num, make_float2(__fdividef(1.f, den.x), __fdividef(1.f, den.y)));
 }
 
-// Field f, normal velocity and pressure of padded cell (x, y) for an x sweep
-// (dir 0) or all fields for a y run (dir 1): interior and copied ghosts from
-// the state and the primitives, outlet / injector ghosts from their strips.
-// DIR 2: field f and the y velocity (halo items of a y run).
+// Doubled split fluxes of field pair j at one cell for direction dir:
+// F = vel q (+ p in the normal momentum, + vel p in rho E), H' = F +- alpha q.
+__device__ __forceinline__ void split2(int j, int dir, f2 q, float vel, float p, float al, f2& hp, f2& hm) {
+  // pair 0 = (rho, rho u), pair 1 = (rho v, rho E)
+  f2 c = make_float2(0.f, 0.f);
+  if (j == 0 && dir == 0) c.y = p;
+  if (j == 1) {
+    if (dir == 1) c.x = p;
+    c.y = vel * p;
+  }
+  const f2 F = f2fma(f2s(vel), q, c);
+  hp = f2fma(f2s(al), q, F);
+  hm = f2fma(f2s(-al), q, F);
+}
+
+// Field pair j (or all 12 fields for DIR 1, as six pairs), the normal
+// velocity and the pressure of padded cell (x, y): interior and copied ghosts
+// from the state and the primitives, outlet / injector ghosts and ghost
+// layers from their buffers.  DIR 0: x sweep; DIR 1, 2: y run (2: one pair).
 template <int DIR>
-__device__ __forceinline__ void win_load(const MP& m, const Grid& g, const double* __restrict__ Uk,
-                                         const float* __restrict__ prims, const double* __restrict__ strips, int x,
-                                         int y, int f, float* q, float& vel, float& p) {
-  constexpr int NQ = DIR == 1 ? 12 : 1;
+__device__ __forceinline__ void win_load2(const MP& m, const Grid& g, const double* __restrict__ Uk,
+                                          const float* __restrict__ prims, const double* __restrict__ strips, int x,
+                                          int y, int j, f2* q, float& vel, float& p) {
+  constexpr int NP = DIR == 1 ? 6 : 1;
   const long long nc = g.ncell;
   const Src s = map_cell<2>(g, x, y);
   if (s.kind == 0) {
     const long long src = (long long)s.xs * g.ny + s.ys;
 #pragma unroll
-    for (int i = 0; i < NQ; ++i) {
-      const int ff = DIR == 1 ? i : f;
-      const double v = Uk[ff * nc + src];
-      q[i] = (float)(((s.flip >> ff) & 1) ? -v : v);
+    for (int i = 0; i < NP; ++i) {
+      const int f = 2 * (DIR == 1 ? i : j);
+      const double v0 = Uk[f * nc + src], v1 = Uk[(f + 1) * nc + src];
+      q[i] = make_float2((float)(((s.flip >> f) & 1) ? -v0 : v0), (float)(((s.flip >> (f + 1)) & 1) ? -v1 : v1));
     }
     vel = prims[(DIR == 0 ? 0 : nc) + src];
     if (s.flip & (DIR == 0 ? 2 : 4)) vel = -vel;
@@ -1126,63 +1353,71 @@ __device__ __forceinline__ void win_load(const MP& m, const Grid& g, const doubl
     flux_prims<2>(m, qa, (float)ghost(g, strips, s, 13), rho, u, v, p);
     vel = DIR == 0 ? u : v;
 #pragma unroll
-    for (int i = 0; i < NQ; ++i) q[i] = qa[DIR == 1 ? i : f];
+    for (int i = 0; i < NP; ++i) {
+      const int f = 2 * (DIR == 1 ? i : j);
+      q[i] = make_float2(qa[f], qa[f + 1]);
+    }
   } else {
 #pragma unroll
-    for (int i = 0; i < NQ; ++i) q[i] = 1.f;
+    for (int i = 0; i < NP; ++i) q[i] = make_float2(1.f, 1.f);
     vel = 1.f;
     p = 1.f;
   }
 }
 
 #ifndef JB_SX_MINB
-#define JB_SX_MINB 1
+#define JB_SX_MINB 4  // 128 registers: the paired window and WENO fit without spills
 #endif
 __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, const double* __restrict__ Uk,
                                                    const float* __restrict__ prims,
                                                    const double* __restrict__ strips, const Slots* slots, int aidx,
-                                                   float* __restrict__ dfx, int nlb) {
-  const int f = blockIdx.x % 12;
-  const int rest = blockIdx.x / 12;
+                                                   float2* __restrict__ dfx, int nlb) {
+  const int j = blockIdx.x % 6;
+  const int rest = blockIdx.x / 6;
   const int y = (rest % nlb) * SX_NT + threadIdx.x, seg = rest / nlb;
   if (y >= g.ny) return;
   const long long nc = g.ncell;
-  const double* uf = Uk + f * nc;
+  const double* u0 = Uk + 2 * j * nc;
+  const double* u1 = u0 + nc;
   const float al = (float)bitsd(slots->ax[aidx]);
   const int a0 = seg * SX_R, a1 = min(a0 + SX_R, g.nx);  // cells [a0, a1), faces a0 .. a1
-  float Hp[6], Hm[6];
+  f2 Hp[6], Hm[6];
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
-    float q, vel, p;
-    win_load<0>(m, g, Uk, prims, strips, a0 - 3 + k, y, f, &q, vel, p);
-    split_h(f, 1, q, vel, p, al, Hp[k], Hm[k]);
+    f2 q;
+    float vel, p;
+    win_load2<0>(m, g, Uk, prims, strips, a0 - 3 + k, y, j, &q, vel, p);
+    split2(j, 0, q, vel, p, al, Hp[k], Hm[k]);
   }
   // the next cell to enter the window, fetched one face ahead and left
   // untouched until then so that its loads overlap the WENO arithmetic
-  double nq;
+  double n0, n1;
   float nv, np;
   auto fetch = [&](int a) {
     if (a >= 0 && a < g.nx) {
       const long long src = (long long)a * g.ny + y;
-      nq = uf[src];
+      n0 = u0[src];
+      n1 = u1[src];
       nv = prims[src];
       np = prims[2 * nc + src];
     } else {
-      float q;
-      win_load<0>(m, g, Uk, prims, strips, a, y, f, &q, nv, np);
-      nq = q;
+      f2 q;
+      win_load2<0>(m, g, Uk, prims, strips, a, y, j, &q, nv, np);
+      n0 = q.x;
+      n1 = q.y;
     }
   };
   fetch(a0 + 2);
-  float* out = dfx + (long long)f * nc + y;
-  float Fprev = 0.f;
+  float2* out = dfx + (long long)j * nc + y;
+  f2 Fprev = make_float2(0.f, 0.f);
 #pragma unroll 1
   for (int fa = a0; fa <= a1; ++fa) {
-    split_h(f, 1, (float)nq, nv, np, al, Hp[5], Hm[5]);  // cell fa+2
+    split2(j, 0, make_float2((float)n0, (float)n1), nv, np, al, Hp[5], Hm[5]);  // cell fa+2
     if (fa < a1) fetch(fa + 3);
     // face fa (cells fa-1 | fa): H+ of cells fa-3 .. fa+1, H- of fa-2 .. fa+2
-    const float F = weno_L(Hp[0], Hp[1], Hp[2], Hp[3], Hp[4]) + weno_R(Hm[1], Hm[2], Hm[3], Hm[4], Hm[5]);
-    if (fa > a0) out[(long long)(fa - 1) * g.ny] = F - Fprev;
+    const f2 F = f2mul(f2s(0.5f), f2add(weno2(Hp[0], Hp[1], Hp[2], Hp[3], Hp[4]),
+                                        weno2(Hm[5], Hm[4], Hm[3], Hm[2], Hm[1])));
+    if (fa > a0) out[(long long)(fa - 1) * g.ny] = f2fma(Fprev, f2s(-1.f), F);
     Fprev = F;
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
@@ -1200,103 +1435,98 @@ __global__ void __launch_bounds__(YR_NT, JB_YR_MINB) k_flux_y_rk(MP m, Grid g, c
                                                        const double* __restrict__ auxk,
                                                        const double* __restrict__ Un, const float* __restrict__ prims,
                                                        const double* __restrict__ strips,
-                                                       const float* __restrict__ dfx, double* __restrict__ out,
-                                                       double* __restrict__ cand, Slots* slots, int aidx, int midx,
-                                                       int nry) {
+                                                       const float2* __restrict__ dfx, double* __restrict__ out,
+                                                       Slots* slots, int aidx, jb_fin fin, int nry) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  float* sHp = reinterpret_cast<float*>(smraw) + (size_t)w * (2 * 12 * YR_C + 12 * YR_F);  // [12][YR_C]
-  float* sHm = sHp + 12 * YR_C;
-  float* sF = sHm + 12 * YR_C;  // [12][YR_F]
+  f2* sHp = reinterpret_cast<f2*>(smraw) + (size_t)w * (2 * 6 * YR_C + 6 * YR_F);  // [6][YR_C]
+  f2* sHm = sHp + 6 * YR_C;
+  f2* sF = sHm + 6 * YR_C;  // [6][YR_F]
   const long long nc = g.ncell;
   const int run = blockIdx.x * YR_W + w;
   const int x = run / nry, y0 = (run % nry) * 32;
   const bool xin = x < g.nx;
   const float al = (float)bitsd(slots->ay[aidx]);
-  double ukr[12];
   // ---- split fluxes on the window: cell y0 - 3 + j in slot j; the run's
-  // own cells one per lane, the 3 + 3 halo cells as 72 (cell, field) items
+  // own cells one per lane, the 3 + 3 halo cells as 36 (cell, pair) items
   // spread over the warp
   if (xin) {
     {
-      const int j = l + 3;
-      float q[12], vel, p;
+      const int jj = l + 3;
+      f2 q[6];
+      float vel, p;
       if (y0 + l < g.ny) {
         const long long cell = (long long)x * g.ny + y0 + l;
 #pragma unroll
-        for (int f = 0; f < 12; ++f) {
-          ukr[f] = Uk[f * nc + cell];
-          q[f] = (float)ukr[f];
-        }
+        for (int i = 0; i < 6; ++i)
+          q[i] = make_float2((float)Uk[2 * i * nc + cell], (float)Uk[(2 * i + 1) * nc + cell]);
         vel = prims[nc + cell];
         p = prims[2 * nc + cell];
       } else {
-        win_load<1>(m, g, Uk, prims, strips, x, y0 + l, 0, q, vel, p);
+        win_load2<1>(m, g, Uk, prims, strips, x, y0 + l, 0, q, vel, p);
       }
 #pragma unroll
-      for (int f = 0; f < 12; ++f) split_h(f, 2, q[f], vel, p, al, sHp[f * YR_C + j], sHm[f * YR_C + j]);
+      for (int i = 0; i < 6; ++i) split2(i, 1, q[i], vel, p, al, sHp[i * YR_C + jj], sHm[i * YR_C + jj]);
     }
 #pragma unroll 1
-    for (int i = l; i < 72; i += 32) {
-      const int h = i / 12, f = i % 12;
-      const int j = h < 3 ? h : 32 + h;
-      float q, vel, p;
-      win_load<2>(m, g, Uk, prims, strips, x, y0 - 3 + j, f, &q, vel, p);
-      split_h(f, 2, q, vel, p, al, sHp[f * YR_C + j], sHm[f * YR_C + j]);
+    for (int i = l; i < 36; i += 32) {
+      const int h = i / 6, pr = i % 6;
+      const int jj = h < 3 ? h : 32 + h;
+      f2 q;
+      float vel, p;
+      win_load2<2>(m, g, Uk, prims, strips, x, y0 - 3 + jj, pr, &q, vel, p);
+      split2(pr, 1, q, vel, p, al, sHp[pr * YR_C + jj], sHm[pr * YR_C + jj]);
     }
   }
   __syncwarp();
-  // ---- faces y0 + k (cells y0+k-1 | y0+k): lane k for all fields, then
-  // the run's last face by lanes 0..11, one field each
+  // ---- faces y0 + k (cells y0+k-1 | y0+k): lane k for all pairs, then the
+  // run's last face by lanes 0..5, one pair each
   if (xin) {
 #pragma unroll 1
-    for (int f = 0; f < 12; ++f) {
-      const float* hp = sHp + f * YR_C + l;
-      const float* hm = sHm + f * YR_C + l;
-      sF[f * YR_F + l] = weno_L(hp[0], hp[1], hp[2], hp[3], hp[4]) + weno_R(hm[1], hm[2], hm[3], hm[4], hm[5]);
+    for (int i = 0; i < 6; ++i) {
+      const f2* hp = sHp + i * YR_C + l;
+      const f2* hm = sHm + i * YR_C + l;
+      sF[i * YR_F + l] = f2mul(f2s(0.5f), f2add(weno2(hp[0], hp[1], hp[2], hp[3], hp[4]),
+                                                 weno2(hm[5], hm[4], hm[3], hm[2], hm[1])));
     }
-    if (l < 12) {
-      const float* hp = sHp + l * YR_C + 32;
-      const float* hm = sHm + l * YR_C + 32;
-      sF[l * YR_F + 32] = weno_L(hp[0], hp[1], hp[2], hp[3], hp[4]) + weno_R(hm[1], hm[2], hm[3], hm[4], hm[5]);
+    if (l < 6) {
+      const f2* hp = sHp + l * YR_C + 32;
+      const f2* hm = sHm + l * YR_C + 32;
+      sF[l * YR_F + 32] = f2mul(f2s(0.5f), f2add(weno2(hp[0], hp[1], hp[2], hp[3], hp[4]),
+                                                  weno2(hm[5], hm[4], hm[3], hm[2], hm[1])));
     }
   }
   __syncwarp();
-  // ---- RK combination (float64) and the Halley iterates of the new state
+  // ---- RK combination (float64) and update_aux of the new state
   const int y = y0 + l;
   const bool live = xin && y < g.ny;
   unsigned bits = 0;
+  double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
   if (live) {
     const long long cell = (long long)x * g.ny + y;
     const double dt = slots->dt;
     double q[12];
 #pragma unroll
-    for (int f = 0; f < 12; ++f) {
-      const double dF = (double)dfx[f * nc + cell];
-      const double dG = (double)(sF[f * YR_F + l + 1] - sF[f * YR_F + l]);
-      const double rhs = dt * visc_add<VISC>(g, f, cell, -(dF * g.idx + dG * g.idy));
-      const double uk = ukr[f];
-      double r;
-      if (STAGE == 1) r = uk + rhs;
-      else if (STAGE == 2) r = 3.0 / 4.0 * Un[f * nc + cell] + 1.0 / 4.0 * (uk + rhs);
-      else r = 1.0 / 3.0 * Un[f * nc + cell] + 2.0 / 3.0 * (uk + rhs);
-      out[f * nc + cell] = r;
-      q[f] = r;
+    for (int i = 0; i < 6; ++i) {
+      const float2 dF = dfx[i * nc + cell];
+      const f2 dG = f2fma(sF[i * YR_F + l], f2s(-1.f), sF[i * YR_F + l + 1]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int f = 2 * i + h;
+        const double rhs = dt * visc_add<VISC>(g, f, cell, -((double)(h ? dF.y : dF.x) * g.idx +
+                                                            (double)(h ? dG.y : dG.x) * g.idy));
+        const double uk = Uk[f * nc + cell];  // read again (L1): no registers held across the WENO
+        double r;
+        if (STAGE == 1) r = uk + rhs;
+        else if (STAGE == 2) r = 3.0 / 4.0 * Un[f * nc + cell] + 1.0 / 4.0 * (uk + rhs);
+        else r = 1.0 / 3.0 * Un[f * nc + cell] + 2.0 / 3.0 * (uk + rhs);
+        out[f * nc + cell] = r;
+        q[f] = r;
+      }
     }
-    const double rho = q[0];
-    const double u = q[1] / rho, v = q[2] / rho;
-    const double e = q[3] / rho - 0.5 * (u * u + v * v);
-    double Y8[NR], Yf[NS];
-#pragma unroll
-    for (int k = 0; k < NR; ++k) Y8[k] = q[4 + k] / rho;
-    fill_Y(Y8, Yf);
-    const double Rmix = get_R(m, Yf);
-    double cnd[JB_NCAND];
-    bits = halley_any(m, e, Yf, Rmix, auxk[nc + cell], cnd);
-#pragma unroll
-    for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
+    bits = finish_state<2, true>(m, g, fin, q, auxk[nc + cell], cell, amx, amy, dtm, slots);
   }
-  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
+  finish_reduce(fin, amx, amy, dtm, bits, slots);
 }
 #endif  // JB_FAST
 
@@ -1444,15 +1674,17 @@ template <int STAGE, class R, bool VISC, bool SW = false>
 __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __restrict__ Uk,
                                                  const double* __restrict__ auxk,
                                                  const double* __restrict__ Un,
-                                                 double* __restrict__ out, double* __restrict__ cand,
+                                                 double* __restrict__ out,
                                                  const double* __restrict__ strips, Slots* slots,
-                                                 int aidx, int midx, double dt_arg) {
+                                                 int aidx, jb_fin fin, double dt_arg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const double dt = STAGE == 0 ? dt_arg : slots->dt;
-  unsigned bits = flux1d_tile<STAGE, R, NT1, VISC, SW>(m, g, Uk, auxk, Un, out, cand, strips, bitsd(slots->ax[aidx]), dt,
-                                             blockIdx.x * (NT1 - 1), smraw);
+  // 1D stays in the global-stop mode (its tile body is shared with the
+  // persistent ensemble kernel)
+  unsigned bits = flux1d_tile<STAGE, R, NT1, VISC, SW>(m, g, Uk, auxk, Un, out, fin.cand, strips,
+                                                       bitsd(slots->ax[aidx]), dt, blockIdx.x * (NT1 - 1), smraw);
   if (STAGE == 0) return;
-  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, midx);
+  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, fin.midx);
 }
 
 // ---------------------------------------------------------------------------
@@ -1649,6 +1881,7 @@ __global__ void __launch_bounds__(128) k_strips(MP m, Grid g, const double* __re
   block_reduce_store(amx, amy, 0.0, 0u, slots, aidx, true, false, -1);
 }
 
+}  // namespace
 }  // namespace JB_NS
 }  // namespace jb
 
@@ -1656,6 +1889,7 @@ __global__ void __launch_bounds__(128) k_strips(MP m, Grid g, const double* __re
 
 namespace jb {
 namespace JB_NS {
+namespace {
 
 // ---------------------------------------------------------------------------
 // point-implicit chemistry (model/reaction_model.py:91-193)
@@ -1873,13 +2107,15 @@ __device__ __forceinline__ void chem_cell_gen(const MP& m, double rho, const dou
 
 // Chemistry of one cell at temperature T.  WRITE_S: reaction_source_terms
 // output S (zeros for the flow fields).  Otherwise U_out = U + S followed by
-// the Halley iterates of the final update_aux (set_simulator.py:117-122),
-// started from T.  sh: this thread's column of the [CHEM_SH][blockDim]
-// shared array.
-template <int DIM, bool WRITE_S, bool GEN>
+// the final update_aux (set_simulator.py:117-122) started from T, in the
+// mode of fin (finish_state; per-cell mode folds the wave speeds and the CFL
+// candidate of the new state into amx, amy, dtm).  sh: this thread's column
+// of the [CHEM_SH][blockDim] shared array.
+template <int DIM, bool WRITE_S, bool GEN, bool CELL = false>
 __device__ __forceinline__ void chem_cell_step(const MP& m, const Grid& g, const double* U, double T,
-                                               double* out, double* cand, long long c, double dt,
-                                               double* sh, unsigned& bits, unsigned& st) {
+                                               double* out, const jb_fin& fin, long long c, double dt,
+                                               double* sh, unsigned& bits, unsigned& st, double& amx,
+                                               double& amy, double& dtm, Slots* slots) {
   constexpr int nY = DIM == 1 ? 3 : 4;
   constexpr int nv = nY + NR;
   const long long nc = g.ncell;
@@ -1918,38 +2154,34 @@ __device__ __forceinline__ void chem_cell_step(const MP& m, const Grid& g, const
       for (int k = 0; k < NR; ++k) q[nY + k] = q[nY + k] + S[k];
 #pragma unroll
       for (int f = 0; f < nv; ++f) out[f * nc + c] = q[f];
-      double u = q[1] / rho;
-      double v = DIM == 2 ? q[2] / rho : 0.0;
-      double e = DIM == 2 ? q[3] / rho - 0.5 * (u * u + v * v) : q[2] / rho - 0.5 * (u * u);
-      double Yn[NR], Yf[NS];
-#pragma unroll
-      for (int k = 0; k < NR; ++k) Yn[k] = q[nY + k] / rho;
-      fill_Y(Yn, Yf);
-      double R = get_R(m, Yf);
-      double cnd[JB_NCAND];
-      bits |= halley_any(m, e, Yf, R, T, cnd);
-#pragma unroll
-      for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + c] = cnd[i];
+      bits |= finish_state<DIM, CELL>(m, g, fin, q, T, c, amx, amy, dtm, slots);
     }
   }
 }
 
-template <int DIM, bool WRITE_S, bool GEN>
+// CELL: the mixed variant's 2D step (per-cell temperature solve)
+template <int DIM, bool WRITE_S, bool GEN, bool CELL>
 __global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __restrict__ U,
                                               const double* __restrict__ aux,
-                                              double* __restrict__ out, double* __restrict__ cand,
-                                              Slots* slots, int midx, double dt_arg) {
+                                              double* __restrict__ out, jb_fin fin,
+                                              Slots* slots, double dt_arg) {
   extern __shared__ double shc[];
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const double dt = WRITE_S ? dt_arg : slots->dt;
   unsigned bits = 0, st = 0;
+  double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
   if (c < g.ncell) {
-    // aux == null: the temperature is the selected iterate of the previous
-    // solve (mask midx - 1), i.e. that solve's select pass is fused here
-    const double T = aux ? aux[g.ncell + c] : cand[(long long)halley_count(slots->mask[midx - 1]) * g.ncell + c];
-    chem_cell_step<DIM, WRITE_S, GEN>(m, g, U, T, out, cand, c, dt, shc + threadIdx.x, bits, st);
+    // aux == null (global-stop mode): the temperature is the selected
+    // iterate of the previous solve (mask midx - 1), i.e. that solve's
+    // select pass is fused here
+    const double T = aux ? aux[g.ncell + c] : fin.cand[(long long)halley_count(slots->mask[fin.midx - 1]) * g.ncell + c];
+    chem_cell_step<DIM, WRITE_S, GEN, CELL>(m, g, U, T, out, fin, c, dt, shc + threadIdx.x, bits, st, amx, amy, dtm,
+                                      slots);
   }
-  block_reduce_store(0.0, 0.0, 0.0, bits | (st << 16), slots, 0, false, false, WRITE_S ? -1 : midx);
+  if (WRITE_S)
+    block_reduce_store(0.0, 0.0, 0.0, st << 16, slots, 0, false, false, -1);
+  else
+    finish_reduce(fin, amx, amy, dtm, bits | (st << 16), slots);
 }
 
 // ---------------------------------------------------------------------------
@@ -2131,5 +2363,6 @@ __global__ void k_dt_unpack(Slots* s, const long long* red) {
 #include "jb_godunov.cuh"
 #include "jb_viscous.cuh"
 
+}  // namespace
 }  // namespace JB_NS
 }  // namespace jb

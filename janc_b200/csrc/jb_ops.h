@@ -3,20 +3,27 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "jb_fin.h"
 #include "jb_types.h"
 
 namespace jb {
 
 struct Ops {
   const char* name;
-  // STAGE 0 writes dt * flux; STAGE 1..3 writes the RK stage and Halley iterates.
-  // work: the mixed variant's float32 scratch of a 2D handle (primitives
-  // [3][ncell], then x flux differences [12][ncell]) or null; select writes
-  // the primitives of its state there when it computes alpha.
+  // 2D stepping (jb_advance) solves each new state's temperature per cell
+  // (jb_fin per-cell mode) instead of the global-stop iterates + select:
+  // the mixed variant only; strict and fp64 keep the reference's global stop
+  bool per_cell_2d;
+  // STAGE 0 writes dt * flux; STAGE 1..3 writes the RK stage and finishes
+  // its temperature solve as fin says (jb_fin.h).  aidx: the alpha slot the
+  // stage reads.  prims: float32 u, v, p of the stage state (mixed 2D) and
+  // work: float32 scratch of the x flux differences [12][ncell], or null.
   cudaError_t (*flux)(int dim, int stage, const jb_mech_params& m, const jb_grid& g,
                       const double* Uk, const double* auxk, const double* Un, double* out,
-                      double* cand, const double* strips, jb_slots* slots, int aidx, int midx,
-                      double dt, void* work, cudaStream_t st);
+                      const double* strips, jb_slots* slots, int aidx, const jb_fin& fin,
+                      const float* prims, void* work, double dt, cudaStream_t st);
+  // work: where the pass writes the float32 u, v, p of its state when it
+  // computes alpha (mixed 2D), or null
   cudaError_t (*select)(int dim, bool select, bool alpha, bool cfl, const jb_mech_params& m,
                         const jb_grid& g, const double* U, const double* aux_in,
                         const double* cand, double* aux_out, double* strips, jb_slots* slots,
@@ -24,9 +31,12 @@ struct Ops {
   cudaError_t (*halley)(int dim, const jb_mech_params& m, const jb_grid& g, const double* U,
                         const double* aux, double* cand, jb_slots* slots, int midx,
                         cudaStream_t st);
+  // write_s: reaction_source_terms into out; else out = U + S and its
+  // temperature solve as fin says (aux == null: the stage-3 temperature is
+  // the global-stop iterate of mask fin.midx - 1)
   cudaError_t (*chem)(int dim, bool write_s, const jb_mech_params& m, const jb_grid& g,
-                      const double* U, const double* aux, double* out, double* cand,
-                      jb_slots* slots, int midx, double dt, cudaStream_t st);
+                      const double* U, const double* aux, double* out, const jb_fin& fin,
+                      jb_slots* slots, double dt, cudaStream_t st);
   cudaError_t (*thermo)(const jb_mech_params& m, long long n, const double* T, const double* Y,
                         double* cp, double* gamma, double* h, double* R, double* dcp,
                         cudaStream_t st);
@@ -51,6 +61,10 @@ struct Ops {
   // ghost-padded copies of (U, aux) (the ghost strips and ghost layers must be current)
   cudaError_t (*pad)(int dim, const jb_grid& g, const double* U, const double* aux, const double* strips,
                      double* Up, double* auxp, cudaStream_t st);
+  // ghost strips of the pressure-outlet / injector sides of (U, aux) and their
+  // wave speeds into alpha slot aidx (no launch without such sides)
+  cudaError_t (*strips)(int dim, const jb_mech_params& m, const jb_grid& g, const double* U, const double* aux,
+                        double* strips, jb_slots* slots, int aidx, cudaStream_t st);
 };
 
 // Doubles of the viscous scratch (node planes and node fluxes) of a grid.

@@ -193,6 +193,7 @@ def test_single_step_vjp_matches_twin(omech, seed_kind):
     L = s._lib
     cu = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
     U0, a0 = s.state_from_PTY(cu(P), cu(T), cu(Y))
+    assert L.jb_adjoint_reserve(s._h) == 0
     R = int(L.jb_record_doubles(s._h))
     rec = torch.empty(2 * R, dtype=torch.float64, device="cuda")
     rsl = torch.empty(13, dtype=torch.float64, device="cuda")
