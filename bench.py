@@ -221,6 +221,37 @@ def job_value(world_size, cells_per_rank, steps, ms_max):
     return world_size * cells_per_rank * steps / (ms_max * 1e-3)
 
 
+def count_kernel_launches(fn):
+    """Kernel launches of fn(), counted as the kernel nodes of a CUDA graph
+    that captures it (driver API cuGraphGetNodes / cuGraphNodeGetType)."""
+    import ctypes
+    import torch
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        fn()  # warm-up on a side stream, as graph capture requires
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph(keep_graph=True)
+    with torch.cuda.graph(g, capture_error_mode="relaxed"):
+        fn()
+    torch.cuda.synchronize()
+    cu = ctypes.CDLL("libcuda.so.1")
+    h = ctypes.c_void_p(g.raw_cuda_graph())
+    n = ctypes.c_size_t(0)
+    if cu.cuGraphGetNodes(h, None, ctypes.byref(n)) != 0:
+        return None
+    nodes = (ctypes.c_void_p * n.value)()
+    cu.cuGraphGetNodes(h, nodes, ctypes.byref(n))
+    kernels = 0
+    for i in range(n.value):
+        t = ctypes.c_int(-1)
+        cu.cuGraphNodeGetType(ctypes.c_void_p(nodes[i]), ctypes.byref(t))
+        kernels += t.value == 0  # CU_GRAPH_NODE_TYPE_KERNEL
+    del g
+    return kernels
+
+
 def fp64_peak_tflops(L, torch):
     """Measured FP64 FMA throughput of this device (TFLOP/s)."""
     import ctypes
@@ -496,6 +527,7 @@ def run_ours(args):
         # contraction, table-driven chemistry
         sp, _, _, _, _, _ = _setup_workload(args, "fp64_strict")
         plain = _time_path(args, sp, U0, aux0, theta, ncell, dist)
+    launches_per_step = count_kernel_launches(lambda: s.advance(U0, aux0, 1, cfl=CFL, theta=theta))
     kms = head["kernel_ms_per_launch"]
     chem_ms = kms["chem"]
     flux_ms = kms["flux"]
@@ -518,6 +550,9 @@ def run_ours(args):
     chem_tflops = arith * ncell / (chem_ms * 1e-3) / 1e12
     step_gbs = BYTES_STEP_PER_CELL * ncell / (head["ms_per_step"] * 1e-3) / 1e9
 
+    subs = None
+    if args.workload == "channel" and ws == 1 and not args.no_sub:
+        subs = sub_records(args)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "channel":
         cpu = cpu_baseline(args.cpu_steps)
@@ -537,13 +572,10 @@ def run_ours(args):
                    "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "status_bits": head["status"],
         "kernel_ms_per_step": head["kernel_ms_per_step"],
-        # per timed step (one jb_advance call of one step): slots reset, first
-        # select, step begin, 3 flux stages (two kernels each in the mixed
-        # variant), 2 stage selects, chemistry, final select
-        # (+ 4 ghost-strip launches on the RDC workload's outlet / injector sides)
-        "gpu_launches": ((13 if args.precision == "mixed" and args.flux == "LF" and args.recon == "WENO5_JS"
-                          else 10)
-                         + (4 if args.workload == "rdc" else 0) + (9 if args.viscous else 0)) * args.steps,
+        # kernels of one timed step (one jb_advance call), counted as the
+        # kernel nodes of a captured graph of that call, times the steps
+        "gpu_launches": launches_per_step * args.steps if launches_per_step is not None else None,
+        "gpu_launches_per_step": launches_per_step,
         "roofline": {"bound": "hbm", "kernel": {
                          "chem": "k_chem (point-implicit chemistry + final Halley)",
                          "flux": ("k_god2d (reconstruction on primitives + Riemann solver + RK stage + Halley)"
@@ -573,18 +605,60 @@ def run_ours(args):
         line["fp64"] = {"value": other["value"], "ms_per_step": other["ms_per_step"],
                         "kernel_ms_per_step": other["kernel_ms_per_step"], "e2e": other["e2e"]["value"],
                         "status_bits": other["status"]}
+        # the mixed-precision gain: the same step with float64 fluxes (FMA
+        # contraction, generated chemistry, the reference's global Halley stop)
         line["speedup_vs_fp64"] = head["value"] / other["value"]
     if plain is not None:
-        line["fp64_plain"] = {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
-                              "kernel_ms_per_step": plain["kernel_ms_per_step"], "e2e": plain["e2e"]["value"],
-                              "build": "fp64_strict: reference operation order, -fmad=false, "
-                                       "table-driven chemistry"}
-        line["speedup_vs_fp64_plain"] = head["value"] / plain["value"]
+        line["fp64_strict"] = {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
+                               "kernel_ms_per_step": plain["kernel_ms_per_step"], "e2e": plain["e2e"]["value"],
+                               "build": "the parity build: reference operation order, -fmad=false, "
+                                        "table-driven chemistry, the reference's global Halley stop"}
+        line["speedup_vs_fp64_strict"] = head["value"] / plain["value"]
     if acc is not None:
         line["accuracy_vs_fp64"] = acc
+    if subs is not None:
+        line["configs"] = subs
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
+
+
+def sub_records(args):
+    """The other workloads of the benchmark set, each with its own clocks, on
+    one GPU: the rotating-detonation annulus (mixed precision, 10 timed steps;
+    fp64 rate; accuracy against the fp64 path after 100 steps), the 64-tube
+    batched ensemble (mixed, args.sub_steps steps, against the tubes one by
+    one through the single-case fp64 path) and the adjoint (args.sub_steps
+    steps: 200 is the configuration's length)."""
+    import copy
+    import torch
+    global CFL
+    out = {}
+    cfl_keep = CFL
+    a = copy.copy(args)
+    a.workload, a.steps, a.viscous, a.flux, a.recon = "rdc", 10, False, "LF", "WENO5_JS"
+    dev = torch.cuda.current_device()
+    s, U0, aux0, theta, ncell, workload = _setup_workload(a, "mixed")
+    r = _time_path(a, s, U0, aux0, theta, ncell, None, ClockSampler(dev))
+    launches = count_kernel_launches(lambda: s.advance(U0, aux0, 1, cfl=CFL, theta=theta))
+    sr, _, _, _, _, _ = _setup_workload(a, "fp64")
+    rf = _time_path(a, sr, U0, aux0, theta, ncell, None)
+    Uw, auxw, _ = sr.advance(U0, aux0, 3, cfl=CFL, theta=theta)
+    acc = _accuracy(a, s, sr, Uw, auxw, theta, 100)
+    out["rdc"] = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "steps": a.steps, "ms_per_step": r["ms_per_step"],
+        "precision": "mixed", "cfl": CFL, "config": {"workload": workload, "cells": ncell},
+        "hbm_gbs_fused_step_minimum": BYTES_STEP_PER_CELL * ncell / (r["ms_per_step"] * 1e-3) / 1e9,
+        "kernel_ms_per_step": r["kernel_ms_per_step"], "gpu_launches_per_step": launches,
+        "e2e": r["e2e"], "status_bits": r["status"], "clocks": r["clocks"],
+        "fp64": {"value": rf["value"], "ms_per_step": rf["ms_per_step"]},
+        "speedup_vs_fp64": r["value"] / rf["value"], "accuracy_vs_fp64": acc,
+    }
+    del s, sr
+    CFL = cfl_keep
+    out["ensemble"] = ensemble_record(args, None, 0, 1, args.sub_steps, "mixed", with_cpu=False)
+    out["adjoint"] = adjoint_record(args, None, 1, args.sub_steps)
+    return out
 
 
 # ------------------------------------------------------------- adjoint arm
@@ -593,13 +667,23 @@ BC_SLIP4 = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_
 
 
 def run_adjoint(args):
+    dist, rank, ws = _dist()
+    line = adjoint_record(args, dist, ws, args.steps)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def adjoint_record(args, dist, ws, N):
+    """The adjoint workload (config 3) on this rank; returns its record."""
     import numpy as np
     import torch
     from janc_b200.adjoint import Trajectory, probe_trajectory
     from janc_b200.solver import Solver
-    dist, rank, ws = _dist()
     dev = torch.cuda.current_device()
-    nx, ny, N = ADJ_NX, ADJ_NY, args.steps
+    nx, ny = ADJ_NX, ADJ_NY
     dx = 0.1 / nx
     P, T, Y = c1_fields(nx=nx, ny=ny, slab=ADJ_SLAB, seed=1)
     s = Solver(2, nx, ny, dx, dx, BC_SLIP4, precision="fp64")
@@ -670,11 +754,6 @@ def run_adjoint(args):
                 a = float((gTn * Tn * d).sum())
             fd[kind].append(abs(f - a) / max(abs(f), 1e-300))
     traj.set_log_A_offset(None)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
     cells = nx * ny
     fd_sum = {k: {"directions": len(v), "max_rel_err": max(v), "median_rel_err": statistics.median(v)}
               for k, v in fd.items() if v}
@@ -706,7 +785,7 @@ def run_adjoint(args):
         # sweep and a merge per RK stage)
         "gpu_launches": 27 * N + 4 * ((N + ADJ_K - 1) // ADJ_K), "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ------------------------------------------------------------ ensemble arm
@@ -742,16 +821,26 @@ def _prim_1d(mech, U, aux):
 
 
 def run_ensemble(args):
-    import torch
-    from janc_b200 import _native
-    from janc_b200.solver import Solver
     if args.precision not in ("fp64", "mixed"):
         raise SystemExit("the ensemble runs in 'fp64' or 'mixed' precision")
     dist, rank, ws = _dist()
+    line = ensemble_record(args, dist, rank, ws, args.steps, args.precision,
+                           with_cpu=rank == 0 and ws == 1 and not args.no_cpu_baseline)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def ensemble_record(args, dist, rank, ws, K, precision, with_cpu):
+    """The batched-ensemble workload (config 4) on this rank; returns its record."""
+    import torch
+    from janc_b200 import _native
+    from janc_b200.solver import Solver
     dev = torch.cuda.current_device()
-    ens, tubes, init = _ens_setup(args.precision)
+    ens, tubes, init = _ens_setup(precision)
     cells = ens.total_cells
-    K = args.steps
     if args.ens_shape:
         block, bpsm = (int(v) for v in args.ens_shape.split("x"))
         ens.configure(block, bpsm)
@@ -811,7 +900,7 @@ def run_ensemble(args):
     e2e_ms = max_over_ranks(dist, legs[0].elapsed_time(legs[3]))
     io_bytes = sum(x.numel() for x in hU + ha) * 8
     # the 64 tubes one after another through the single-case float64 path
-    seq_steps = args.seq_steps or K
+    seq_steps = getattr(args, "seq_steps", 0) or K
     seq_ms, seq_final = 0.0, []
     for i, t in enumerate(tubes):
         s = Solver(1, t["nx"], dx=t["dx"], boundary_config=BC1, precision="fp64")
@@ -854,21 +943,14 @@ def run_ensemble(args):
     arith, special = chem_flops_per_cell()
     achieved = BYTES_ENS_STEP_PER_CELL * cells * K / (ms * 1e-3) / 1e9
     chem_tflops = arith * cells * K / (ms * 1e-3) / 1e12
-    cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_ensemble(args.cpu_steps)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
+    cpu = cpu_baseline_ensemble(args.cpu_steps) if with_cpu else None
     sizes = [t["nx"] for t in tubes]
     line = {
         "metric": "total " + METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
         "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32 flux / f64 state, T-solve, chemistry",
-        "data": "synthetic", "precision": args.precision,
+        "dtype": "f64" if precision == "fp64" else "f32 flux / f64 state, T-solve, chemistry",
+        "data": "synthetic", "precision": precision,
         "config": {"workload": f"batched ensemble: {ENS_N} 1D H2-air detonation tubes, lengths "
                                f"log-uniform 1000-16000 cells (dx 50 um), phi U(0.6,1.4), T_ign "
                                f"U(2500,3500) K, default_rng({ENS_SEED}); 30 atm slab over the first 2 %; "
@@ -883,7 +965,7 @@ def run_ensemble(args):
         "gpu_launches": 1,
         "roofline": {"bound": "hbm", "kernel": "k_ensemble (all phases of all steps)", "achieved": achieved,
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "traffic": TRAFFIC_ENS_PER_CELL_STEP * cells * K if args.precision == "mixed" else None,
+                     "traffic": TRAFFIC_ENS_PER_CELL_STEP * cells * K if precision == "mixed" else None,
                      "traffic_source": "ncu dram bytes of a 20-step launch, scaled to this launch's cell-steps",
                      "peak_source": hbm_src, "algorithmic_bytes_per_cell_step": BYTES_ENS_STEP_PER_CELL,
                      "launch_ms": ms},
@@ -904,7 +986,7 @@ def run_ensemble(args):
         line["accuracy_vs_fp64"] = acc
     if cpu is not None:
         line["cpu_baseline"] = cpu
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def _oracle_tube(args):
@@ -1043,7 +1125,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "fp64_strict", "mixed"])
     ap.add_argument("--no-compare", action="store_true", help="skip the float64 comparison run")
-    ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="steps of the mixed-vs-fp64 comparison (2000: the channel configuration's length)")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="channel: skip the sub-records of the other workloads (rdc, ensemble, adjoint)")
+    ap.add_argument("--sub-steps", type=int, default=200,
+                    help="steps of the ensemble and adjoint sub-records")
     ap.add_argument("--workload", default="channel", choices=["channel", "rdc", "ensemble", "adjoint"])
     ap.add_argument("--viscous", action="store_true",
                     help="channel workload with the laminar viscous fluxes")

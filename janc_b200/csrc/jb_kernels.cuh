@@ -1247,8 +1247,9 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
 // ---------------------------------------------------------------------------
 // float32 LF splitting and WENO5-JS on float32 primitives, float64 RK
 // combination and temperature solve, organised without block barriers:
-//   k_sweep_x    one thread per (y line, x segment of SX_R cells, field
-//                pair): a register window of the split fluxes walks the
+//   k_sweep_x    one thread per (y line, x segment of seg cells, field
+//                pair; seg chosen by the host for whole waves): a register
+//                window of the split fluxes walks the
 //                segment's faces and writes the x flux difference
 //                F_{i+1/2} - F_{i-1/2} of each cell
 //   k_flux_y_rk  one warp per run of 32 cells along y: split fluxes of all
@@ -1260,10 +1261,7 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
 // FMUL2), which issue two float32 operations at once.  The x differences are
 // stored as float2 pairs: dfx[6][ncell][2].  The stage state's float32 u, v,
 // p come from the kernel that wrote that state (prims[3][ncell]).
-#ifndef JB_SX_R
-#define JB_SX_R 16
-#endif
-constexpr int SX_R = JB_SX_R, SX_NT = 128;
+constexpr int SX_NT = 128;
 constexpr int YR_W = 8, YR_NT = 32 * YR_W;     // warps (runs) per block
 constexpr int YR_C = 38, YR_F = 33;            // window cells, faces per run
 constexpr size_t YR_SMEM = sizeof(float2) * YR_W * (2 * 6 * YR_C + 6 * YR_F);
@@ -1371,7 +1369,7 @@ __device__ __forceinline__ void win_load2(const MP& m, const Grid& g, const doub
 __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, const double* __restrict__ Uk,
                                                    const float* __restrict__ prims,
                                                    const double* __restrict__ strips, const Slots* slots, int aidx,
-                                                   float2* __restrict__ dfx, int nlb) {
+                                                   float2* __restrict__ dfx, int nlb, int seg_len) {
   const int j = blockIdx.x % 6;
   const int rest = blockIdx.x / 6;
   const int y = (rest % nlb) * SX_NT + threadIdx.x, seg = rest / nlb;
@@ -1380,7 +1378,7 @@ __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, con
   const double* u0 = Uk + 2 * j * nc;
   const double* u1 = u0 + nc;
   const float al = (float)bitsd(slots->ax[aidx]);
-  const int a0 = seg * SX_R, a1 = min(a0 + SX_R, g.nx);  // cells [a0, a1), faces a0 .. a1
+  const int a0 = seg * seg_len, a1 = min(a0 + seg_len, g.nx);  // cells [a0, a1), faces a0 .. a1
   f2 Hp[6], Hm[6];
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
@@ -1911,7 +1909,8 @@ __device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], con
     }
   }
   // Every loop has a constant trip count so the matrix stays in registers;
-  // the row exchange is branch-free (selects).
+  // the row exchange is branch-free (selects) over the columns still active
+  // (the eliminated columns are not used again).
 #if JB_FAST
   double ipv[NR];
 #endif
@@ -1932,9 +1931,11 @@ __device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], con
         const bool sw = p == r;
 #pragma unroll
         for (int j = 0; j < NR; ++j) {
-          const double x0 = J[c][j], x1 = J[r][j];
-          J[c][j] = sw ? x1 : x0;
-          J[r][j] = sw ? x0 : x1;
+          if (j >= c) {
+            const double x0 = J[c][j], x1 = J[r][j];
+            J[c][j] = sw ? x1 : x0;
+            J[r][j] = sw ? x0 : x1;
+          }
         }
         const double y0 = b[c], y1 = b[r];
         b[c] = sw ? y1 : y0;
