@@ -179,7 +179,7 @@ template <class R, int NT>
 __global__ void __launch_bounds__(NT, Shape<NT>::MINB)
     k_ensemble(const jb_ens_inst* __restrict__ insts, const int* __restrict__ cta_inst, int nsteps,
                double* dt_hist, jb_ens_ctl* ctl, unsigned long long limit_ns) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+  extern __shared__ __align__(128) unsigned char smraw[];
   __shared__ jb_ens_inst sI;
   const int tid = threadIdx.x;
   const int ii = cta_inst[blockIdx.x];

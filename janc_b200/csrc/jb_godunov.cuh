@@ -164,9 +164,12 @@ __device__ __forceinline__ void cons_to_w(const MP& m, const double* q, double T
 // Shared memory: the padded tile's primitives in RW (float32 in the mixed
 // variant: the reconstruction runs in RW; the Riemann solver, RK and Halley
 // stay float64), then the face fluxes in float64 at a 16-byte aligned offset.
+// float64: the region first receives the TMA boxes of the padded tile
+// (TQ_N fields at the staged layout, tile_ci), which the primitives then
+// replace
 template <class RW>
 __host__ __device__ constexpr size_t god2_wbytes() {
-  return (sizeof(RW) * 12 * SM2_Q + 15) / 16 * 16;
+  return sizeof(RW) == sizeof(double) ? sizeof(double) * TQ_N * SM2_QF : (sizeof(RW) * 12 * SM2_Q + 15) / 16 * 16;
 }
 template <class RW>
 __host__ __device__ constexpr size_t god2_smem() {
@@ -182,8 +185,10 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
                                                  const double* __restrict__ auxk, const double* __restrict__ Un,
                                                  double* __restrict__ out,
                                                  const double* __restrict__ strips, Slots* slots, jb_fin fin,
-                                                 double dt_arg) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+                                                 double dt_arg, const __grid_constant__ CUtensorMap tmU,
+                                                 const __grid_constant__ CUtensorMap tmA, int use_tma) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ __align__(8) unsigned long long tma_bar;
   RW* sW = reinterpret_cast<RW*>(smraw);                                // [12][PX2][PY2]
   double* sFx = reinterpret_cast<double*>(smraw + god2_wbytes<RW>());  // [12][TX2+1][TY2]
   double* sFy = sFx + 12 * SM2_FX;                 // [12][TX2][TY2+1]
@@ -191,30 +196,70 @@ __global__ void __launch_bounds__(NT2, 2) k_god2d(MP m, Grid g, const double* __
   const int x0 = blockIdx.x * TX2, y0 = blockIdx.y * TY2;
   const long long nc = g.ncell;
   const double dt = STAGE == 0 ? dt_arg : slots->dt;
-  for (int i = tid; i < SM2_Q; i += NT2) {
-    const int px = i / PY2, py = i % PY2;
-    const Src s = map_cell<2>(g, x0 + px - 3, y0 + py - 3);
-    double q[12], T = 1.0;
-    if (s.kind == 0) {
-      const size_t c = (size_t)s.xs * g.ny + s.ys;
-#pragma unroll
-      for (int f = 0; f < 12; ++f) {
-        const double v = Uk[f * nc + c];
-        q[f] = ((s.flip >> f) & 1) ? -v : v;
-      }
-      T = auxk[nc + c];
-    } else if (s.kind == 1) {
-#pragma unroll
-      for (int f = 0; f < 12; ++f) q[f] = ghost(g, strips, s, f);
-      T = ghost(g, strips, s, 13);
-    } else {
-#pragma unroll
-      for (int f = 0; f < 12; ++f) q[f] = 1.0;
+  // float64 tiles: the conserved fields and (gamma, T) of the padded tile by
+  // two TMA boxes into the start of the region (staged layout, tile_ci); the
+  // cells inside the domain are read from there, the others (ghost cells)
+  // by their boundary mapping.  The primitives overwrite the region, so each
+  // thread converts its cells (at most two) into registers first.
+  constexpr bool EXACT = sizeof(RW) == sizeof(double);
+  const bool tma = EXACT && use_tma;
+  const double* sS = reinterpret_cast<const double*>(smraw);
+  if (tma) {
+    if (tid == 0) mbar_init(&tma_bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+      mbar_expect_tx(&tma_bar, (unsigned)(sizeof(double) * (TQ_N * SM2_QF)));
+      tma_load_3d(smraw, &tmU, y0 - 4, x0 - 3, 0, &tma_bar);
+      tma_load_3d(smraw + sizeof(double) * TQ_G * SM2_QF, &tmA, y0 - 4, x0 - 3, 0, &tma_bar);
     }
-    double w[12];
-    cons_to_w<2>(m, q, T, w);
+    if (!mbar_wait_bounded(&tma_bar)) {
+      if (tid == 0) atomicOr(&slots->status, (unsigned)JB_ERR_TIMEOUT);
+      mbar_wait_bounded(&tma_bar);  // the copy must not land after the block has left
+      return;
+    }
+  }
+  constexpr int NCELL_T = (SM2_Q + NT2 - 1) / NT2;  // padded cells per thread (2)
+  double wk[NCELL_T][12];
 #pragma unroll
-    for (int f = 0; f < 12; ++f) sW[f * SM2_Q + i] = (RW)w[f];
+  for (int r = 0; r < NCELL_T; ++r) {
+    const int i = tid + r * NT2;
+    if (i >= SM2_Q) break;
+    const int px = i / PY2, py = i % PY2;
+    const int x = x0 + px - 3, y = y0 + py - 3;
+    double q[12], T = 1.0;
+    if (tma && x >= 0 && x < g.nx && y >= 0 && y < g.ny) {
+      const int k = tile_ci(px, py);
+#pragma unroll
+      for (int f = 0; f < 12; ++f) q[f] = sS[f * SM2_QF + k];
+      T = sS[TQ_T * SM2_QF + k];
+    } else {
+      const Src s = map_cell<2>(g, x, y);
+      if (s.kind == 0) {
+        const size_t c = (size_t)s.xs * g.ny + s.ys;
+#pragma unroll
+        for (int f = 0; f < 12; ++f) {
+          const double v = Uk[f * nc + c];
+          q[f] = ((s.flip >> f) & 1) ? -v : v;
+        }
+        T = auxk[nc + c];
+      } else if (s.kind == 1) {
+#pragma unroll
+        for (int f = 0; f < 12; ++f) q[f] = ghost(g, strips, s, f);
+        T = ghost(g, strips, s, 13);
+      } else {
+#pragma unroll
+        for (int f = 0; f < 12; ++f) q[f] = 1.0;
+      }
+    }
+    cons_to_w<2>(m, q, T, wk[r]);
+  }
+  if (tma) __syncthreads();  // every cell has been read from the staged boxes
+#pragma unroll
+  for (int r = 0; r < NCELL_T; ++r) {
+    const int i = tid + r * NT2;
+    if (i >= SM2_Q) break;
+#pragma unroll
+    for (int f = 0; f < 12; ++f) sW[f * SM2_Q + i] = (RW)wk[r][f];
   }
   __syncthreads();
   {
@@ -296,7 +341,7 @@ __global__ void __launch_bounds__(NT1) k_god1d(MP m, Grid g, const double* __res
                                               const double* __restrict__ strips, Slots* slots, int midx,
                                               double dt_arg) {
   constexpr int PW = NT1 + 5;
-  extern __shared__ __align__(16) unsigned char smraw[];
+  extern __shared__ __align__(128) unsigned char smraw[];
   RW* sW = reinterpret_cast<RW*>(smraw);                               // [11][PW]: padded cell x0 - 3 + j
   double* sF = reinterpret_cast<double*>(smraw + god1_wbytes<RW>());  // [11][NT1]: face x0 + t
   const int tid = threadIdx.x;

@@ -13,6 +13,7 @@
 //   cand[6][nx][ny]    Halley iterates T_0..T_5 of the last temperature solve
 //   strips[4][nv+2][L] ghost states of pressure-outlet / injector sides
 //                      (L = max(nx, ny)); fields U..., gamma, T
+#include <cuda.h>  // CUtensorMap (the tile kernels' TMA descriptors)
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -1035,18 +1036,61 @@ __device__ __forceinline__ void flux_prims(const MP& m, const float* q, float T,
 //           iterates of update_aux (solver_{1D,2D}/aux_func.py:21-29)
 constexpr int TX2 = 15, TY2 = 16, PX2 = TX2 + 6, PY2 = TY2 + 6;
 constexpr int NT2 = 256;
-constexpr int SM2_Q = PX2 * PY2;                  // per field
+constexpr int SM2_Q = PX2 * PY2;                  // padded cells of a tile
 constexpr int SM2_HX = PX2 * TY2, SM2_HY = TX2 * PY2;
 constexpr int SM2_FX = (TX2 + 1) * TY2, SM2_FY = TX2 * (TY2 + 1);
+// Shared-memory layout of the padded tile fields: rows of PYS = 24 cells
+// holding padded cells y0 - 4 .. y0 + 19 (the tile's y0 - 3 .. y0 + 18 at
+// offsets 1..22), so that a TMA box can start at the even column y0 - 4
+// (16-byte aligned for float64) and fill a field as one dense box.
+constexpr int PYS = 24, SM2_QF = PX2 * PYS;       // field stride
+__host__ __device__ constexpr int tile_ci(int px, int py) { return px * PYS + py + 1; }
+// fields of the staged tile: the 12 conserved fields, gamma, T
+constexpr int TQ_G = 12, TQ_T = 13, TQ_N = 14;
 
 template <class R>
 __host__ __device__ constexpr size_t sw_smem2d_bytes() {
-  return sizeof(R) * 2 * SM2_Q;
+  return sizeof(R) * SM2_QF;  // the sound speed a
 }
 
 template <class R>
-__host__ __device__ constexpr size_t smem2d_bytes(int nq) {
-  return sizeof(R) * ((size_t)nq * SM2_Q + 4 * SM2_Q + 2 * SM2_HX + 2 * SM2_HY + SM2_FX + SM2_FY);
+__host__ __device__ constexpr size_t smem2d_bytes(int) {
+  return sizeof(R) * ((size_t)TQ_N * SM2_QF + 4 * SM2_QF + 2 * SM2_HX + 2 * SM2_HY + SM2_FX + SM2_FY);
+}
+
+// ---- TMA: bulk tensor loads into shared memory completing on an mbarrier
+// (no cluster multicast; the tensor maps cover this GPU's own buffers)
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+// Bounded wait on a TMA mbarrier (phase 0): false after ~1 s of clock cycles.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, 0))
+    if (clock64() - t0 > 2000000000LL) return false;
+  return true;
 }
 
 // R is the arithmetic type of the flux (LF split, WENO, primitives): double
@@ -1058,21 +1102,24 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
                                                  const double* __restrict__ Un,
                                                  double* __restrict__ out,
                                                  const double* __restrict__ strips, Slots* slots,
-                                                 int aidx, jb_fin fin, double dt_arg) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int nv = 12, nq = nv + 1;
+                                                 int aidx, jb_fin fin, double dt_arg,
+                                                 const __grid_constant__ CUtensorMap tmU,
+                                                 const __grid_constant__ CUtensorMap tmA, int use_tma) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ __align__(8) unsigned long long tma_bar;
+  constexpr int nv = 12;
   constexpr bool EXACT = sizeof(R) == sizeof(double);
-  R* sQ = reinterpret_cast<R*>(smraw);   // [nq][PX2][PY2]
-  R* sP = sQ + (size_t)nq * SM2_Q;       // [4][PX2][PY2]: rho, u, v, p
-  R* sHxp = sP + 4 * SM2_Q;              // [PX2][TY2]
+  R* sQ = reinterpret_cast<R*>(smraw);   // [TQ_N][PX2][PYS]: U, gamma, T
+  R* sP = sQ + (size_t)TQ_N * SM2_QF;    // [4][PX2][PYS]: rho, u, v, p
+  R* sHxp = sP + 4 * SM2_QF;             // [PX2][TY2]
   R* sHxm = sHxp + SM2_HX;
   R* sHyp = sHxm + SM2_HX;               // [TX2][PY2]
   R* sHym = sHyp + SM2_HY;
   R* sFx = sHym + SM2_HY;                // [TX2+1][TY2]
   R* sFy = sFx + SM2_FX;                 // [TX2][TY2+1]
-  // Steger-Warming only (launched with sw_smem2d more bytes): gamma, a
-  R* sG = sFy + SM2_FY;                  // [PX2][PY2]
-  R* sA = sG + SM2_Q;
+  R* sG = sQ + TQ_G * SM2_QF;            // gamma
+  // Steger-Warming only (launched with sw_smem2d more bytes): the sound speed
+  R* sA = sFy + SM2_FY;                  // [PX2][PYS]
   constexpr bool sw = SW;
 
   const int tid = threadIdx.x;
@@ -1082,41 +1129,62 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
   const R ax = (R)bitsd(slots->ax[aidx]);
   const R ay = (R)bitsd(slots->ay[aidx]);
 
-  // ---- load the padded tile with ghost cells
+  // ---- load the padded tile with ghost cells.  float64 tiles: two TMA boxes
+  // (the 12 conserved fields, and gamma / T) over padded rows x0-3 .. x0+17
+  // and columns y0-4 .. y0+19 in one transaction; the cells outside the
+  // domain (filled with zeros by the copy) are then replaced by their ghost
+  // values.  Without TMA every padded cell is loaded here.
+  const bool tma = EXACT && use_tma;
+  if (tma) {
+    if (tid == 0) mbar_init(&tma_bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+      mbar_expect_tx(&tma_bar, (unsigned)(sizeof(double) * (TQ_N * SM2_QF)));
+      tma_load_3d(sQ, &tmU, y0 - 4, x0 - 3, 0, &tma_bar);
+      tma_load_3d(sQ + TQ_G * SM2_QF, &tmA, y0 - 4, x0 - 3, 0, &tma_bar);
+    }
+    if (!mbar_wait_bounded(&tma_bar)) {
+      if (tid == 0) atomicOr(&slots->status, (unsigned)JB_ERR_TIMEOUT);
+      mbar_wait_bounded(&tma_bar);  // the copy must not land after the block has left
+      return;
+    }
+  }
   for (int i = tid; i < SM2_Q; i += NT2) {
-    int px = i / PY2, py = i % PY2;
-    int x = x0 + px - 3, y = y0 + py - 3;
+    const int px = i / PY2, py = i % PY2;
+    const int x = x0 + px - 3, y = y0 + py - 3;
+    if (tma && x >= 0 && x < g.nx && y >= 0 && y < g.ny) continue;
+    const int k = tile_ci(px, py);
     Src s = map_cell<2>(g, x, y);
     if (s.kind == 0) {
       size_t c = (size_t)s.xs * g.ny + s.ys;
       for (int q = 0; q < nv; ++q) {
         double v = Uk[q * nc + c];
-        sQ[q * SM2_Q + i] = (R)(((s.flip >> q) & 1) ? -v : v);
+        sQ[q * SM2_QF + k] = (R)(((s.flip >> q) & 1) ? -v : v);
       }
-      sQ[nv * SM2_Q + i] = (R)auxk[nc + c];
-      if (sw) sG[i] = (R)auxk[c];
+      sQ[TQ_T * SM2_QF + k] = (R)auxk[nc + c];
+      sG[k] = (R)auxk[c];
     } else if (s.kind == 1) {
-      for (int q = 0; q < nv; ++q) sQ[q * SM2_Q + i] = (R)ghost(g, strips, s, q);
-      sQ[nv * SM2_Q + i] = (R)ghost(g, strips, s, nv + 1);
-      if (sw) sG[i] = (R)ghost(g, strips, s, nv);
+      for (int q = 0; q < nv; ++q) sQ[q * SM2_QF + k] = (R)ghost(g, strips, s, q);
+      sQ[TQ_T * SM2_QF + k] = (R)ghost(g, strips, s, nv + 1);
+      sG[k] = (R)ghost(g, strips, s, nv);
     } else {
-      for (int q = 0; q < nq; ++q) sQ[q * SM2_Q + i] = (R)1.0;
-      if (sw) sG[i] = (R)1.0;
+      for (int q = 0; q < TQ_N; ++q) sQ[q * SM2_QF + k] = (R)1.0;
     }
   }
   __syncthreads();
   // ---- primitives (aux_func.U_to_prim) on every padded cell
   for (int i = tid; i < SM2_Q; i += NT2) {
+    const int k = tile_ci(i / PY2, i % PY2);
     R q[nv];
 #pragma unroll
-    for (int f = 0; f < nv; ++f) q[f] = sQ[f * SM2_Q + i];
+    for (int f = 0; f < nv; ++f) q[f] = sQ[f * SM2_QF + k];
     R rho, u, v, p;
-    flux_prims<2>(m, q, sQ[nv * SM2_Q + i], rho, u, v, p);
-    sP[i] = rho;
-    sP[SM2_Q + i] = u;
-    sP[2 * SM2_Q + i] = v;
-    sP[3 * SM2_Q + i] = p;
-    if (sw) sA[i] = sqrt(sG[i] * p / rho);
+    flux_prims<2>(m, q, sQ[TQ_T * SM2_QF + k], rho, u, v, p);
+    sP[k] = rho;
+    sP[SM2_QF + k] = u;
+    sP[2 * SM2_QF + k] = v;
+    sP[3 * SM2_QF + k] = p;
+    if (sw) sA[k] = sqrt(sG[k] * p / rho);
   }
   __syncthreads();
 
@@ -1136,7 +1204,7 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
     int px = 0, py = 0, dst = -1;
     if (i < SM2_HX) { px = i / TY2; py = i % TY2 + 3; dst = i; }
     else if (i < SM2_HX + SM2_HY) { int j = i - SM2_HX; px = j / PY2 + 3; py = j % PY2; dst = i; }
-    h_src[r] = px * PY2 + py;
+    h_src[r] = tile_ci(px, py);
     h_dst[r] = dst;
   }
 #endif
@@ -1151,16 +1219,16 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       if (dst < 0) continue;
       const int c = h_src[r];
       const bool xdir = dst < SM2_HX;
-      const R vel = xdir ? sP[SM2_Q + c] : sP[2 * SM2_Q + c];
-      const R qf = sQ[f * SM2_Q + c];
+      const R vel = xdir ? sP[SM2_QF + c] : sP[2 * SM2_QF + c];
+      const R qf = sQ[f * SM2_QF + c];
       R F = vel * qf;
-      if (f == (xdir ? 1 : 2)) F += sP[3 * SM2_Q + c];
-      if (f == 3) F += vel * sP[3 * SM2_Q + c];
+      if (f == (xdir ? 1 : 2)) F += sP[3 * SM2_QF + c];
+      if (f == 3) F += vel * sP[3 * SM2_QF + c];
       const R al = xdir ? ax : ay;
       R hp = (R)0.5 * (F + al * qf), hm = (R)0.5 * (F - al * qf);
       if (sw)
-        sw_split<2, R>(f, xdir ? 0 : 1, qf, sP[c], sP[SM2_Q + c], sP[2 * SM2_Q + c], sP[3 * SM2_Q + c],
-                       sQ[3 * SM2_Q + c], sA[c], sG[c], hp, hm);
+        sw_split<2, R>(f, xdir ? 0 : 1, qf, sP[c], sP[SM2_QF + c], sP[2 * SM2_QF + c], sP[3 * SM2_QF + c],
+                       sQ[3 * SM2_QF + c], sA[c], sG[c], hp, hm);
       if (xdir) { sHxp[dst] = hp; sHxm[dst] = hm; }
       else { sHyp[dst - SM2_HX] = hp; sHym[dst - SM2_HX] = hm; }
     }
@@ -1169,10 +1237,10 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       int px, py, dir;
       if (i < SM2_HX) { px = i / TY2; py = i % TY2 + 3; dir = 0; }
       else { int j = i - SM2_HX; px = j / PY2 + 3; py = j % PY2; dir = 1; }
-      int c = px * PY2 + py;
-      R rho = sP[c], u = sP[SM2_Q + c], v = sP[2 * SM2_Q + c], p = sP[3 * SM2_Q + c];
-      R E = sQ[3 * SM2_Q + c];
-      R qf = sQ[f * SM2_Q + c];
+      int c = tile_ci(px, py);
+      R rho = sP[c], u = sP[SM2_QF + c], v = sP[2 * SM2_QF + c], p = sP[3 * SM2_QF + c];
+      R E = sQ[3 * SM2_QF + c];
+      R qf = sQ[f * SM2_QF + c];
       R hp, hm;
       if (sw) {
         sw_split<2, R>(f, dir, qf, rho, u, v, p, E, sA[c], sG[c], hp, hm);
@@ -1217,7 +1285,7 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
       double rhs = dt * visc_add<VISC>(g, f, cell, -(dF / g.dx + dG / g.dy));
 #endif
       // the state itself is float64 in every variant
-      double uk = EXACT ? (double)sQ[f * SM2_Q + (ix + 3) * PY2 + (iy + 3)] : Uk[f * nc + cell];
+      double uk = EXACT ? (double)sQ[f * SM2_QF + tile_ci(ix + 3, iy + 3)] : Uk[f * nc + cell];
       double r;
       if (STAGE == 0) r = rhs;
       else if (STAGE == 1) r = uk + rhs;
@@ -1235,7 +1303,7 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
   if (live) {
     double q[12];
     for (int f = 0; f < 12; ++f) q[f] = out[f * nc + cell];
-    const double T0 = EXACT ? (double)sQ[nv * SM2_Q + (ix + 3) * PY2 + (iy + 3)] : auxk[nc + cell];
+    const double T0 = EXACT ? (double)sQ[TQ_T * SM2_QF + tile_ci(ix + 3, iy + 3)] : auxk[nc + cell];
     bits = finish_state<2, !EXACT>(m, g, fin, q, T0, cell, amx, amy, dtm, slots);
   }
   finish_reduce(fin, amx, amy, dtm, bits, slots);
@@ -1435,7 +1503,7 @@ __global__ void __launch_bounds__(YR_NT, JB_YR_MINB) k_flux_y_rk(MP m, Grid g, c
                                                        const double* __restrict__ strips,
                                                        const float2* __restrict__ dfx, double* __restrict__ out,
                                                        Slots* slots, int aidx, jb_fin fin, int nry) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+  extern __shared__ __align__(128) unsigned char smraw[];
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   f2* sHp = reinterpret_cast<f2*>(smraw) + (size_t)w * (2 * 6 * YR_C + 6 * YR_F);  // [6][YR_C]
   f2* sHm = sHp + 6 * YR_C;
@@ -1675,7 +1743,7 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
                                                  double* __restrict__ out,
                                                  const double* __restrict__ strips, Slots* slots,
                                                  int aidx, jb_fin fin, double dt_arg) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+  extern __shared__ __align__(128) unsigned char smraw[];
   const double dt = STAGE == 0 ? dt_arg : slots->dt;
   // 1D stays in the global-stop mode (its tile body is shared with the
   // persistent ensemble kernel)
