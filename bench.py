@@ -74,10 +74,13 @@ BYTES_CHEM_PER_CELL = 224      # read U,aux (112 B) + write U,aux (112 B), float
 BYTES_STEP_PER_CELL = 864 + 224  # fused-step minimum + separate chemistry pass (2D)
 BYTES_FLUX_STAGE_PER_CELL = 288  # one RK stage of the fused minimum: (224 + 320 + 320) / 3
 # DRAM bytes per cell measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum,
-# each launch cold) on the 1024x256 channel, mixed precision: one RK stage 2/3
-# (k_sweep_x 27.3 + 0.8 MB, k_flux_y_rk 67.2 + 34.8 MB) and one chemistry
-# launch; and per cell-step of the persistent ensemble kernel
-TRAFFIC_PER_CELL = {"flux": 496.5, "chem": 148.0}
+# each launch cold) on the 1024x256 channel, mixed precision, with this tree's
+# kernels: one RK stage 2/3 (k_sweep_x 27.34 + 0.00 MB, k_flux_y_rk 67.19 +
+# 1.65 MB) and one chemistry launch (27.39 + 7.58 MB); the capture and its
+# command are in profiles/launches_channel1024x256_mixed.md.  Per cell-step of
+# the persistent ensemble kernel: profiles/k_ensemble_64tubes.md.
+TRAFFIC_PER_CELL = {"flux": 366.9, "chem": 133.4}
+TRAFFIC_SOURCE = "profiles/launches_channel1024x256_mixed.md"
 TRAFFIC_ENS_PER_CELL_STEP = 1125.0
 
 
@@ -588,7 +591,7 @@ def run_ours(args):
                                  args.flux == "LF" and args.recon == "WENO5_JS" and not args.viscous and
                                  args.precision == "mixed" else None),
                      "traffic_source": "ncu dram bytes of one stage's launches on this workload, each "
-                                       "launch cold (mixed precision)",
+                                       "launch cold (mixed precision): " + TRAFFIC_SOURCE,
                      "peak_source": hbm_src,
                      "algorithmic_bytes_per_cell": bytes_cell, "launch_ms": launch_ms,
                      "step_achieved_gbs": step_gbs,
