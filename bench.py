@@ -757,6 +757,38 @@ def adjoint_record(args, dist, ws, N):
                 a = float((gTn * Tn * d).sum())
             fd[kind].append(abs(f - a) / max(abs(f), 1e-300))
     traj.set_log_A_offset(None)
+    # (1) h-sweep along two full-field directions: on the exactly uniform
+    # ambient gas the central difference plateaus away from the adjoint
+    # instead of converging to it
+    sweep = []
+    rng_s = np.random.default_rng(5)
+    for _ in range(2):
+        d = rng_s.standard_normal(T.shape)
+        d /= np.linalg.norm(d)
+        a = float((gTn * Tn * d).sum())
+        row = {"adjoint": a}
+        for hh in (1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8, 1e-9):
+            f = (loss_at(cu(Tn * (1 + hh * d)), None) - loss_at(cu(Tn * (1 - hh * d)), None)) / (2 * hh)
+            row[f"{hh:.0e}"] = abs(f - a) / max(abs(f), 1e-300)
+        sweep.append(row)
+    # (2) the same workload with 1 % seeded noise on the ambient temperature
+    # (no exactly uniform region): the full-field directions against the
+    # adjoint of that state
+    Tz = T.copy()
+    Tz[:, ADJ_SLAB:] *= 1.0 + 0.01 * np.random.default_rng(6).standard_normal(Tz[:, ADJ_SLAB:].shape)
+    Tzc = cu(Tz)
+    Tg2 = Tzc.clone().requires_grad_()
+    dts2, pps2 = probe_trajectory(traj, Pc, Tg2, Yc, None, N)
+    (dts2 * pps2).sum().backward()
+    gTz = Tg2.grad.cpu().numpy()
+    noised = []
+    rng_n = np.random.default_rng(7)
+    for _ in range(nd):
+        d = rng_n.standard_normal(T.shape)
+        d /= np.linalg.norm(d)
+        f = (loss_at(cu(Tz * (1 + h * d)), None) - loss_at(cu(Tz * (1 - h * d)), None)) / (2 * h)
+        a = float((gTz * Tz * d).sum())
+        noised.append(abs(f - a) / max(abs(f), 1e-300))
     cells = nx * ny
     fd_sum = {k: {"directions": len(v), "max_rel_err": max(v), "median_rel_err": statistics.median(v)}
               for k, v in fd.items() if v}
@@ -778,6 +810,12 @@ def adjoint_record(args, dist, ws, N):
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "loss": loss,
         "finite_difference_check": {"h_rel": h, **fd_sum,
+                                    "T_full_field_noised_ambient": {
+                                        "directions": len(noised), "max_rel_err": max(noised),
+                                        "median_rel_err": statistics.median(noised),
+                                        "state": "the same workload with 1 % seeded noise (default_rng(6)) on "
+                                                 "the ambient temperature"},
+                                    "T_full_field_h_sweep": sweep,
                                     "note": "full-field directions perturb the exactly uniform ambient gas, "
                                             "where WENO5-JS (eps = 1e-6 against split fluxes ~1e8) is linear "
                                             "only below ~1e-11 relative perturbations"},

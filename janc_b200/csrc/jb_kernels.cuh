@@ -1963,51 +1963,44 @@ namespace {
 // (I/dt - M_k J) x = M_k w by LU with partial pivoting (first maximal
 // |pivot| as LAPACK idamax), then detailed_reaction's clip and S = rho dY
 // (construct_matrix_equation, reaction_model.py:132-159 and :183-193).
-__device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], const double* w, double rho,
-                                           const double* Y8, double dt, double* S, unsigned& st) {
-  double b[NR];
-  const double idt = 1.0 / dt;
-#pragma unroll
-  for (int k = 0; k < NR; ++k) {
-    b[k] = m.M[k] * w[k];
-#pragma unroll
-    for (int n = 0; n < NR; ++n) {
-      double jk = m.M[k] * J[k][n];
-      J[k][n] = (k == n ? idt : 0.0) - jk;  // J now holds A
-    }
-  }
-  // Every loop has a constant trip count so the matrix stays in registers;
-  // the row exchange is branch-free (selects) over the columns still active
-  // (the eliminated columns are not used again).
+// Gaussian elimination of A x = b in registers with partial pivoting (first
+// maximal |pivot|, as LAPACK idamax) when PIVOT, else without exchanges;
+// every loop has a constant trip count so the matrix stays in registers.
+template <bool PIVOT>
+__device__ __forceinline__ void lu_solve(double (&J)[NR][NR], double (&b)[NR], double (&x)[NR], unsigned& st) {
 #if JB_FAST
   double ipv[NR];
 #endif
 #pragma unroll
   for (int c = 0; c < NR; ++c) {
-    int p = c;
-    double best = fabs(J[c][c]);
+    if (PIVOT) {
+      int p = c;
+      double best = fabs(J[c][c]);
 #pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      if (r > c) {
-        double v = fabs(J[r][c]);
-        if (v > best) { best = v; p = r; }
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      if (r > c) {
-        const bool sw = p == r;
-#pragma unroll
-        for (int j = 0; j < NR; ++j) {
-          if (j >= c) {
-            const double x0 = J[c][j], x1 = J[r][j];
-            J[c][j] = sw ? x1 : x0;
-            J[r][j] = sw ? x0 : x1;
-          }
+      for (int r = 0; r < NR; ++r) {
+        if (r > c) {
+          double v = fabs(J[r][c]);
+          if (v > best) { best = v; p = r; }
         }
-        const double y0 = b[c], y1 = b[r];
-        b[c] = sw ? y1 : y0;
-        b[r] = sw ? y0 : y1;
+      }
+      // branch-free row exchange over the columns still active (the
+      // eliminated columns are not used again)
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        if (r > c) {
+          const bool sw = p == r;
+#pragma unroll
+          for (int j = 0; j < NR; ++j) {
+            if (j >= c) {
+              const double x0 = J[c][j], x1 = J[r][j];
+              J[c][j] = sw ? x1 : x0;
+              J[r][j] = sw ? x0 : x1;
+            }
+          }
+          const double y0 = b[c], y1 = b[r];
+          b[c] = sw ? y1 : y0;
+          b[r] = sw ? y0 : y1;
+        }
       }
     }
     if (J[c][c] == 0.0) st |= JB_ERR_SINGULAR;
@@ -2030,7 +2023,6 @@ __device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], con
       }
     }
   }
-  double x[NR];
 #pragma unroll
   for (int i = 0; i < NR; ++i) {
     const int r = NR - 1 - i;
@@ -2044,6 +2036,46 @@ __device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], con
     x[r] = s / J[r][r];
 #endif
   }
+}
+
+// (I/dt - M_k J) x = M_k w by LU with partial pivoting, then
+// detailed_reaction's clip and S = rho dY (construct_matrix_equation,
+// reaction_model.py:132-159 and :183-193; the reference solves with
+// jnp.linalg.solve, a partially pivoted LU).  The fast variants first test
+// the matrix for diagonal dominance by columns: partial pivoting then never
+// exchanges rows (each diagonal entry is the first maximum of its column, and
+// elimination keeps the dominance), so the elimination without the pivot
+// search and exchanges computes the same values; the other cells (the hot
+// reaction zone, where M_k J outweighs 1/dt) take the pivoted form.
+__device__ __forceinline__ void chem_solve(const MP& m, double (&J)[NR][NR], const double* w, double rho,
+                                           const double* Y8, double dt, double* S, unsigned& st) {
+  double b[NR];
+  const double idt = 1.0 / dt;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    b[k] = m.M[k] * w[k];
+#pragma unroll
+    for (int n = 0; n < NR; ++n) {
+      double jk = m.M[k] * J[k][n];
+      J[k][n] = (k == n ? idt : 0.0) - jk;  // J now holds A
+    }
+  }
+  double x[NR];
+#if JB_FAST
+  bool cdd = true;
+#pragma unroll
+  for (int c = 0; c < NR; ++c) {
+    double off = 0.0;
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      if (r != c) off += fabs(J[r][c]);
+    cdd = cdd && fabs(J[c][c]) > off;
+  }
+  if (cdd) lu_solve<false>(J, b, x, st);
+  else lu_solve<true>(J, b, x, st);
+#else
+  lu_solve<true>(J, b, x, st);
+#endif
   // detailed_reaction (:183-193): dY = clip(drhoY/rho, -Y, 1-Y); S = rho dY
 #if JB_FAST
   const double irho = 1.0 / rho;
