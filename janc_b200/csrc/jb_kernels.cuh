@@ -898,13 +898,23 @@ __device__ __forceinline__ void sw_split(int f, int dir, R qf, R rho, R u, R v, 
 // ~1e11, so (eps + IS)^2 overflows float32.  The weights are formed as ratios
 // to the smallest (eps + IS_k), alpha_k ~ C_k (min/(eps + IS_k))^2, which is
 // the same normalised weight in real arithmetic and cannot overflow.
+// One approximate reciprocal (MUFU.RCP, ~1 ulp).  The WENO weights' operands
+// are at least eps (smoothness sums eps + IS) or the smallest linear weight
+// (weight sums, where one ratio is 1), never denormal or huge, so no range
+// fix-up is needed around it.
+__device__ __forceinline__ float rcp_fast(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __device__ __forceinline__ float weno_combine32(float IS1, float IS2, float IS3, float q1, float q2,
                                                 float q3, float eps) {
   const float e1 = eps + IS1, e2 = eps + IS2, e3 = eps + IS3;
   const float mn = fminf(e1, fminf(e2, e3));
-  const float r1 = __fdividef(mn, e1), r2 = __fdividef(mn, e2), r3 = __fdividef(mn, e3);
+  const float r1 = mn * rcp_fast(e1), r2 = mn * rcp_fast(e2), r3 = mn * rcp_fast(e3);
   const float a1 = 0.1f * (r1 * r1), a2 = 0.6f * (r2 * r2), a3 = 0.3f * (r3 * r3);
-  return __fdividef(a1 * q1 + a2 * q2 + a3 * q3, a1 + a2 + a3);
+  return (a1 * q1 + a2 * q2 + a3 * q3) * rcp_fast(a1 + a2 + a3);
 }
 
 // Left/right-biased float32 values.  The ratio form of the weights never
@@ -1361,9 +1371,9 @@ __device__ __forceinline__ f2 weno2(f2 a, f2 b, f2 c, f2 d, f2 e) {
   const f2 e2 = f2fma(t2, t2, f2fma(f2mul(s2, k13), s2, e16));
   const f2 e3 = f2fma(t3, t3, f2fma(f2mul(s3, k13), s3, e16));
   const f2 mn = make_float2(fminf(e1.x, fminf(e2.x, e3.x)), fminf(e1.y, fminf(e2.y, e3.y)));
-  const f2 r1 = f2mul(mn, make_float2(__fdividef(1.f, e1.x), __fdividef(1.f, e1.y)));
-  const f2 r2 = f2mul(mn, make_float2(__fdividef(1.f, e2.x), __fdividef(1.f, e2.y)));
-  const f2 r3 = f2mul(mn, make_float2(__fdividef(1.f, e3.x), __fdividef(1.f, e3.y)));
+  const f2 r1 = f2mul(mn, make_float2(rcp_fast(e1.x), rcp_fast(e1.y)));
+  const f2 r2 = f2mul(mn, make_float2(rcp_fast(e2.x), rcp_fast(e2.y)));
+  const f2 r3 = f2mul(mn, make_float2(rcp_fast(e3.x), rcp_fast(e3.y)));
   const f2 w1 = f2mul(r1, r1), w2 = f2mul(r2, r2), w3 = f2mul(r3, r3);
   // C_k times the candidate values (C = 1/10, 6/10, 3/10)
   const f2 q1 = f2fma(c, f2s(11.f / 60.f), f2fma(b, f2s(-7.f / 60.f), f2mul(a, f2s(1.f / 30.f))));
@@ -1371,7 +1381,7 @@ __device__ __forceinline__ f2 weno2(f2 a, f2 b, f2 c, f2 d, f2 e) {
   const f2 q3 = f2fma(e, f2s(-0.05f), f2fma(d, f2s(0.25f), f2mul(c, f2s(0.1f))));
   const f2 num = f2fma(w3, q3, f2fma(w2, q2, f2mul(w1, q1)));
   const f2 den = f2fma(w3, f2s(0.3f), f2fma(w2, f2s(0.6f), f2mul(w1, f2s(0.1f))));
-  return f2mul(num, make_float2(__fdividef(1.f, den.x), __fdividef(1.f, den.y)));
+  return f2mul(num, make_float2(rcp_fast(den.x), rcp_fast(den.y)));
 }
 
 // Doubled split fluxes of field pair j at one cell for direction dir:
@@ -1476,19 +1486,23 @@ __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, con
   fetch(a0 + 2);
   float2* out = dfx + (long long)j * nc + y;
   f2 Fprev = make_float2(0.f, 0.f);
+  // cell c lives in window slot (c - a0 + 3) % 6: the face loop is unrolled
+  // over the window's period so that the window rotates by renaming
 #pragma unroll 1
-  for (int fa = a0; fa <= a1; ++fa) {
-    split2(j, 0, make_float2((float)n0, (float)n1), nv, np, al, Hp[5], Hm[5]);  // cell fa+2
-    if (fa < a1) fetch(fa + 3);
-    // face fa (cells fa-1 | fa): H+ of cells fa-3 .. fa+1, H- of fa-2 .. fa+2
-    const f2 F = f2mul(f2s(0.5f), f2add(weno2(Hp[0], Hp[1], Hp[2], Hp[3], Hp[4]),
-                                        weno2(Hm[5], Hm[4], Hm[3], Hm[2], Hm[1])));
-    if (fa > a0) out[(long long)(fa - 1) * g.ny] = f2fma(Fprev, f2s(-1.f), F);
-    Fprev = F;
+  for (int fb = a0; fb <= a1; fb += 6) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      Hp[k] = Hp[k + 1];
-      Hm[k] = Hm[k + 1];
+    for (int r = 0; r < 6; ++r) {
+      const int fa = fb + r;
+      if (fa > a1) break;
+      split2(j, 0, make_float2((float)n0, (float)n1), nv, np, al, Hp[(r + 5) % 6], Hm[(r + 5) % 6]);  // cell fa+2
+      if (fa < a1) fetch(fa + 3);
+      // face fa (cells fa-1 | fa): H+ of cells fa-3 .. fa+1, H- of fa-2 .. fa+2
+      const f2 F = f2mul(f2s(0.5f), f2add(weno2(Hp[r % 6], Hp[(r + 1) % 6], Hp[(r + 2) % 6], Hp[(r + 3) % 6],
+                                                Hp[(r + 4) % 6]),
+                                          weno2(Hm[(r + 5) % 6], Hm[(r + 4) % 6], Hm[(r + 3) % 6],
+                                                Hm[(r + 2) % 6], Hm[(r + 1) % 6])));
+      if (fa > a0) out[(long long)(fa - 1) * g.ny] = f2fma(Fprev, f2s(-1.f), F);
+      Fprev = F;
     }
   }
 }
