@@ -1444,6 +1444,9 @@ __device__ __forceinline__ void win_load2(const MP& m, const Grid& g, const doub
 #ifndef JB_SX_MINB
 #define JB_SX_MINB 4  // 128 registers: the paired window and WENO fit without spills
 #endif
+#ifndef JB_SX_PF
+#define JB_SX_PF 1  // cells fetched ahead of the window (a divisor of 6)
+#endif
 __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, const double* __restrict__ Uk,
                                                    const float* __restrict__ prims,
                                                    const double* __restrict__ strips, const Slots* slots, int aidx,
@@ -1465,25 +1468,27 @@ __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, con
     win_load2<0>(m, g, Uk, prims, strips, a0 - 3 + k, y, j, &q, vel, p);
     split2(j, 0, q, vel, p, al, Hp[k], Hm[k]);
   }
-  // the next cell to enter the window, fetched one face ahead and left
-  // untouched until then so that its loads overlap the WENO arithmetic
-  double n0, n1;
-  float nv, np;
-  auto fetch = [&](int a) {
+  // the cells about to enter the window, fetched JB_SX_PF faces ahead into
+  // buffer (c - a0) % JB_SX_PF and left untouched until then so that their
+  // loads overlap the WENO arithmetic
+  double n0[JB_SX_PF], n1[JB_SX_PF];
+  float nv[JB_SX_PF], np[JB_SX_PF];
+  auto fetch = [&](int a, int b) {
     if (a >= 0 && a < g.nx) {
       const long long src = (long long)a * g.ny + y;
-      n0 = u0[src];
-      n1 = u1[src];
-      nv = prims[src];
-      np = prims[2 * nc + src];
+      n0[b] = u0[src];
+      n1[b] = u1[src];
+      nv[b] = prims[src];
+      np[b] = prims[2 * nc + src];
     } else {
       f2 q;
-      win_load2<0>(m, g, Uk, prims, strips, a, y, j, &q, nv, np);
-      n0 = q.x;
-      n1 = q.y;
+      win_load2<0>(m, g, Uk, prims, strips, a, y, j, &q, nv[b], np[b]);
+      n0[b] = q.x;
+      n1[b] = q.y;
     }
   };
-  fetch(a0 + 2);
+#pragma unroll
+  for (int k = 0; k < JB_SX_PF; ++k) fetch(a0 + 2 + k, (2 + k) % JB_SX_PF);
   float2* out = dfx + (long long)j * nc + y;
   f2 Fprev = make_float2(0.f, 0.f);
   // cell c lives in window slot (c - a0 + 3) % 6: the face loop is unrolled
@@ -1494,8 +1499,10 @@ __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, con
     for (int r = 0; r < 6; ++r) {
       const int fa = fb + r;
       if (fa > a1) break;
-      split2(j, 0, make_float2((float)n0, (float)n1), nv, np, al, Hp[(r + 5) % 6], Hm[(r + 5) % 6]);  // cell fa+2
-      if (fa < a1) fetch(fa + 3);
+      const int bc = (r + 2) % JB_SX_PF;  // buffer of cell fa + 2 ((fb - a0) is a multiple of 6)
+      split2(j, 0, make_float2((float)n0[bc], (float)n1[bc]), nv[bc], np[bc], al, Hp[(r + 5) % 6],
+             Hm[(r + 5) % 6]);  // cell fa+2
+      if (fa + JB_SX_PF <= a1) fetch(fa + 2 + JB_SX_PF, bc);
       // face fa (cells fa-1 | fa): H+ of cells fa-3 .. fa+1, H- of fa-2 .. fa+2
       const f2 F = f2mul(f2s(0.5f), f2add(weno2(Hp[r % 6], Hp[(r + 1) % 6], Hp[(r + 2) % 6], Hp[(r + 3) % 6],
                                                 Hp[(r + 4) % 6]),
