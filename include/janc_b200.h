@@ -230,8 +230,9 @@ int jb_probe_fp64_fma(int blocks, int iters, double* scratch, void* stream);
 const char* jb_last_error(const jb_handle* h);
 
 /* ------------------------------------------------------------------------
- * Reverse mode (the adjoint), 2D grids with periodic, slip, no-slip or
- * zero-gradient sides.  The reference gets these derivatives from jax.grad
+ * Reverse mode (the adjoint), 2D grids with periodic, slip, no-slip,
+ * zero-gradient or pressure-outlet sides (back pressure Pb held fixed).
+ * The reference gets these derivatives from jax.grad
  * through advance_one_step and the CFL time step (set_simulator.py:117-122,
  * 420-447) with get_T's custom VJP (src/janc_v2/model/thermo_model.py:
  * 155-190); these calls compute the same vector-Jacobian products with

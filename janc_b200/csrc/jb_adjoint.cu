@@ -20,11 +20,15 @@
 // Kernels (one thread per cell unless noted), in the order of one step:
 //   k_vjp_begin     the probe term of the loss and update_aux of U4; the
 //                   primitives and alpha / CFL tie counts of U, U1, U2
+//   k_outlet_ghosts (pressure-outlet sides) the outlet ghost states of U,
+//                   U1, U2 and their alpha tie counts
 //   k_chem_vjp      chemistry: Ubar3 = Ubar4 + dS/dU3^T Ubar4, with the
 //                   temperature, dt and ln A adjoints, then update_aux of U3
 //   per RK stage (3, 2, 1):
 //   k_flux_sweep    one thread per (direction, line, segment, field): the
 //                   WENO5 / LF face adjoints along the line (registers only)
+//   k_outlet_vjp    (pressure-outlet sides) the outlet ghosts' adjoints
+//                   into their boundary cells
 //   k_stage_merge   flux-function VJPs, ghost copies, RK combination, alpha
 //                   (and CFL) ties, update_aux of the stage state
 //   k_init_vjp      initial state from (P, T, Y): T adjoint
@@ -524,6 +528,129 @@ __device__ __forceinline__ Speeds speeds_of(const Grid& g, const Prim<2>& pr) {
 __device__ __forceinline__ bool tied(double v, double ref) { return fabs(v - ref) <= TIE_REL * fabs(ref); }
 
 // ---------------------------------------------------------------------------
+// pressure-outlet sides (boundary_conditions_2D/pressure_outlet.py:5-66)
+// ---------------------------------------------------------------------------
+// The 3 ghost layers of an outlet side all hold the outlet state of the
+// side's boundary cell.  They are padded entries of their own: the sweeps
+// read them (og), the alpha maxima see their wave speeds (3 entries per
+// boundary position), and their adjoints (flux, LF term, wave speeds) flow
+// back into the boundary cell through the VJP of the outlet state (ogb).
+//   og [stage][side][OG_F][lstrip]: ghost U (12), u, v, p
+//   ogb[side][OG_B][lstrip]: the boundary cell's U adjoint (12), T adjoint
+constexpr int OG_F = 15, OG_B = 13;
+
+__device__ __forceinline__ size_t og_idx(const Grid& g, int stage, int side, int f, int pos) {
+  return (((size_t)stage * 4 + side) * OG_F + f) * g.lstrip + pos;
+}
+
+__device__ __forceinline__ bool outlet_side(const Grid& g, int side) {
+  return g.bc[side] == JB_BC_PRESSURE_OUTLET;
+}
+
+// Boundary position t in [0, 2 ny + 2 nx): sides 0 and 1 (x = 0, nx - 1) by
+// y, then sides 2 and 3 (y = 0, ny - 1) by x; side -1 past the end.
+__device__ __forceinline__ void boundary_pos(const Grid& g, int t, int& side, int& pos, int& x, int& y) {
+  side = -1;
+  pos = 0;
+  if (t < 2 * g.ny) {
+    side = t / g.ny;
+    pos = t % g.ny;
+  } else if (t < 2 * g.ny + 2 * g.nx) {
+    side = 2 + (t - 2 * g.ny) / g.nx;
+    pos = (t - 2 * g.ny) % g.nx;
+  }
+  x = side == 0 ? 0 : side == 1 ? g.nx - 1 : pos;
+  y = side == 2 ? 0 : side == 3 ? g.ny - 1 : pos;
+}
+
+// normal velocity of boundary cell q, positive out of the domain
+__device__ __forceinline__ double outlet_un(const double* q, int side) {
+  const double un = (side < 2 ? q[1] : q[2]) / q[0];
+  return (side == 0 || side == 2) ? -un : un;
+}
+
+// ub, Tb += the VJP of the outlet state (pressure_outlet.py:5-22) of boundary
+// cell q with aux (gamma, T), given the adjoints of the ghost state (ob), of
+// its gamma (gcb) and of its T (Tcb).  The subsonic / supersonic switch has
+// no derivative and Pb is a parameter; gamma of the cell only enters the
+// switch.  Subsonic: rho_c = Pb / (p / rho), p_c = Pb, T_c = p_c / (rho_c R);
+// supersonic: the cell's rho, p, T.  Both: the ghost energy rho_c h(T_c) -
+// p_c + rho_c |u|^2 / 2 and gamma_c = cp(T_c) / (cp(T_c) - R).
+__device__ void outlet_vjp(const MP& m, const double* q, double gamma, double T, double un, double Pb,
+                           const double* ob, double gcb, double Tcb, double* ub, double& Tb) {
+  const double rho = q[0], ri = 1.0 / rho;
+  const double u = q[1] * ri, v = q[2] * ri;
+  double Y8[NR], Yf[NS];
+  cell_Y(q, ri, Y8, Yf);
+  const double R = get_R(m, Yf);
+  const double p = rho * (R * T);
+  const double a = sqrt(gamma * p / rho);
+  const bool sub = un / a < 1.0;
+  const double w = p / rho;
+  const double rho_c = sub ? Pb / w : rho;
+  const double T_c = sub ? Pb * 1.0 / (rho_c * R) : T;
+  double cp = 0.0, dcp = 0.0, h = 0.0, cpi[NS], hi[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) {
+    const bool lo = T_c < m.Tcr[k];
+    cpi[k] = lo ? poly5(m.cp_lo[k], T_c) : poly5(m.cp_hi[k], T_c);
+    hi[k] = lo ? poly6(m.h_lo[k], T_c) : poly6(m.h_hi[k], T_c);
+    const double dck = lo ? poly4(m.dcp_lo[k], T_c) : poly4(m.dcp_hi[k], T_c);
+    cp += cpi[k] * Yf[k];
+    dcp += dck * Yf[k];
+    h += hi[k] * Yf[k];
+  }
+  const double cv = cp - R, icv2 = 1.0 / (cv * cv);
+  // ghost = [rho_c, rho_c u, rho_c v, rho_c h - p_c + rho_c ke, rho_c Y8]
+  const double ke = 0.5 * (u * u + v * v);
+  double rcb = ob[0] + ob[1] * u + ob[2] * v + ob[3] * (h + ke);
+  double Y8b[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    rcb += ob[4 + k] * Y8[k];
+    Y8b[k] = ob[4 + k] * rho_c;
+  }
+  const double ubl = (ob[1] + ob[3] * u) * rho_c, vbl = (ob[2] + ob[3] * v) * rho_c;
+  const double hb = ob[3] * rho_c, pcb = -ob[3];
+  // gamma_c = cp / (cp - R), h = sum h_k Y_k, cp = sum cp_k Y_k at T_c
+  const double cpb = -gcb * R * icv2;
+  double Rb = gcb * cp * icv2;
+  const double Tct = Tcb + hb * cp + cpb * dcp;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y8b[k] += hb * (hi[k] - hi[NR]) + cpb * (cpi[k] - cpi[NR]);
+  double rb, pb, Tl;
+  if (sub) {
+    // T_c = Pb / (rho_c R), rho_c = Pb / w, w = p / rho
+    const double rcb2 = rcb - Tct * T_c / rho_c;
+    Rb -= Tct * T_c / R;
+    const double wb = -rcb2 * rho_c / w;
+    pb = wb * ri;
+    rb = -wb * w * ri;
+    Tl = 0.0;
+  } else {
+    rb = rcb;
+    pb = pcb;
+    Tl = Tct;
+  }
+  // p = rho R T, R = sum Y_k / M_k
+  rb += pb * R * T;
+  Rb += pb * rho * T;
+  Tl += pb * rho * R;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y8b[k] += Rb * (m.invM[k] - m.invM[NR]);
+  ub[1] += ubl * ri;
+  ub[2] += vbl * ri;
+  rb -= (ubl * u + vbl * v) * ri;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    ub[4 + k] += Y8b[k] * ri;
+    rb -= Y8b[k] * Y8[k] * ri;
+  }
+  ub[0] += rb;
+  Tb += Tl;
+}
+
+// ---------------------------------------------------------------------------
 // the probe term of the loss: L += dt_n * mean probe p(U_{n+1}), p = rho R T
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void probe_vjp(const MP& m, const double* q, double T, double w, double* ub, double& Tb) {
@@ -603,6 +730,39 @@ __global__ void __launch_bounds__(128) k_vjp_begin(MP m, Grid g, const double* _
   block_add(cnt[6], red + red_cnt(0, 2));
 }
 
+// The outlet ghosts of the three stage states (blockIdx.y = stage), one
+// thread per boundary position: og, and the ghosts' alpha tie counts (3
+// padded entries per position).
+__global__ void __launch_bounds__(128) k_outlet_ghosts(MP m, Grid g, const double* __restrict__ rec,
+                                                       const double* __restrict__ slots_rec, double* og,
+                                                       double* red) {
+  const long long nc = g.ncell, nU = 12 * nc;
+  const int st = blockIdx.y;
+  int side, pos, x, y;
+  boundary_pos(g, blockIdx.x * blockDim.x + threadIdx.x, side, pos, x, y);
+  double cx = 0.0, cy = 0.0;
+  if (side >= 0 && outlet_side(g, side)) {
+    const long long c = (long long)x * g.ny + y;
+    const double* S = rec + (long long)st * (nU + 2 * nc);
+    double q[12], gs[14];
+#pragma unroll
+    for (int f = 0; f < 12; ++f) q[f] = S[f * nc + c];
+    pressure_outlet_state<2>(m, q, S[nU + c], S[nU + nc + c], outlet_un(q, side), g.Pb, gs);
+    const Prim<2> pr = u_to_prim<2>(m, gs, gs[12], gs[13]);
+#pragma unroll
+    for (int f = 0; f < 12; ++f) og[og_idx(g, st, side, f, pos)] = gs[f];
+    og[og_idx(g, st, side, 12, pos)] = pr.u;
+    og[og_idx(g, st, side, 13, pos)] = pr.v;
+    og[og_idx(g, st, side, 14, pos)] = pr.p;
+    const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
+    const Speeds sp = speeds_of(g, pr);
+    if (tied(sp.sx, bitsd(rs->ax[st]))) cx = 3.0;
+    if (tied(sp.sy, bitsd(rs->ay[st]))) cy = 3.0;
+  }
+  block_add(cx, red + red_cnt(st, 0));
+  block_add(cy, red + red_cnt(st, 1));
+}
+
 // ---------------------------------------------------------------------------
 // flux VJP of one RK stage: line sweeps, then a per-cell merge
 // ---------------------------------------------------------------------------
@@ -620,19 +780,33 @@ constexpr int SW_R = 24;
 constexpr int SW_NT = 128;
 
 // H+ and H- of field f at padded cell a of a line, from the stage state and
-// its primitives (those of the source cell; ghosts flip the momentum).
+// its primitives (those of the source cell; ghosts flip the momentum), or
+// for a pressure-outlet ghost from the stage's outlet ghosts og.
 template <int D>
 __device__ __forceinline__ void sweep_load(const Grid& g, const double* __restrict__ Uk,
-                                           const double* __restrict__ Pk, int f, int line, int a, double alpha,
-                                           double& hp, double& hm, double& qv) {
+                                           const double* __restrict__ Pk, const double* __restrict__ og, int f,
+                                           int line, int a, double alpha, double& hp, double& hm, double& qv) {
   const Src s = map_cell<2>(g, D == 0 ? a : line, D == 0 ? line : a);
-  const long long nc = g.ncell, src = (long long)s.xs * g.ny + s.ys;
-  double qf = Uk[f * nc + src];
-  if ((s.flip >> f) & 1) qf = -qf;
-  const double rho = Pk[src], p = Pk[3 * nc + src];
-  double u = Pk[nc + src], v = Pk[2 * nc + src];
-  if (s.flip & 2) u = -u;
-  if (s.flip & 4) v = -v;
+  const long long nc = g.ncell;
+  double qf, rho, p, u, v;
+  if (s.kind == 1) {
+    const double* o = og + (size_t)s.side * OG_F * g.lstrip + s.pos;
+    qf = o[(size_t)f * g.lstrip];
+    rho = o[0];
+    u = o[(size_t)12 * g.lstrip];
+    v = o[(size_t)13 * g.lstrip];
+    p = o[(size_t)14 * g.lstrip];
+  } else {
+    const long long src = (long long)s.xs * g.ny + s.ys;
+    qf = Uk[f * nc + src];
+    if ((s.flip >> f) & 1) qf = -qf;
+    rho = Pk[src];
+    p = Pk[3 * nc + src];
+    u = Pk[nc + src];
+    v = Pk[2 * nc + src];
+    if (s.flip & 2) u = -u;
+    if (s.flip & 4) v = -v;
+  }
   const double un = D == 0 ? u : v;
   constexpr int mn = D == 0 ? 1 : 2;
   double F;
@@ -648,7 +822,8 @@ __device__ __forceinline__ void sweep_load(const Grid& g, const double* __restri
 
 template <int D>
 __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restrict__ Uk,
-                                           const double* __restrict__ Pk, const double* __restrict__ Uo_b,
+                                           const double* __restrict__ Pk, const double* __restrict__ og,
+                                           const double* __restrict__ Uo_b,
                                            double coef, double alpha, double dt, int f, int line, int seg,
                                            double* __restrict__ Fb, double* __restrict__ Ua, double& ab,
                                            double& dtb) {
@@ -676,7 +851,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
   double Hp[6], Hm[6], Q[6], Ap[6], Am[6];
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
-    sweep_load<D>(g, Uk, Pk, f, line, flo - 3 + k, alpha, Hp[k], Hm[k], Q[k]);
+    sweep_load<D>(g, Uk, Pk, og, f, line, flo - 3 + k, alpha, Hp[k], Hm[k], Q[k]);
     Ap[k] = 0.0;
     Am[k] = 0.0;
   }
@@ -685,7 +860,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
   double lbm = lbar(flo - 1), Fprev = 0.0;
 #pragma unroll 1
   for (int fa = flo; fa <= fhi; ++fa) {
-    sweep_load<D>(g, Uk, Pk, f, line, fa + 2, alpha, Hp[5], Hm[5], Q[5]);
+    sweep_load<D>(g, Uk, Pk, og, f, line, fa + 2, alpha, Hp[5], Hm[5], Q[5]);
     const double lbp = lbar(fa);
     // L_i = -(F_{i+1} - F_i) / d  ->  Fbar_fa = dt (Lbar_fa - Lbar_{fa-1}) / d
     const double Fbf = dt_dA * (lbp - lbm);
@@ -731,6 +906,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
 // field runs fastest over blocks, then the line block, then the segment.
 __global__ void __launch_bounds__(SW_NT, 4) k_flux_sweep(Grid g, const double* __restrict__ Uk,
                                                       const double* __restrict__ Pk,
+                                                      const double* __restrict__ og,
                                                       const double* __restrict__ Uo_b, double coef,
                                                       const double* __restrict__ slots_rec, int stage, double* FbX,
                                                       double* UaX, double* FbY, double* UaY, double* red, int nbx,
@@ -746,10 +922,10 @@ __global__ void __launch_bounds__(SW_NT, 4) k_flux_sweep(Grid g, const double* _
   double ab = 0.0, dtb = 0.0;
   if (D == 0) {
     if (line < g.ny)
-      sweep_body<0>(g, Uk, Pk, Uo_b, coef, bitsd(rs->ax[stage]), rs->dt, f, line, seg, FbX, UaX, ab, dtb);
+      sweep_body<0>(g, Uk, Pk, og, Uo_b, coef, bitsd(rs->ax[stage]), rs->dt, f, line, seg, FbX, UaX, ab, dtb);
   } else {
     if (line < g.nx)
-      sweep_body<1>(g, Uk, Pk, Uo_b, coef, bitsd(rs->ay[stage]), rs->dt, f, line, seg, FbY, UaY, ab, dtb);
+      sweep_body<1>(g, Uk, Pk, og, Uo_b, coef, bitsd(rs->ay[stage]), rs->dt, f, line, seg, FbY, UaY, ab, dtb);
   }
   block_add(ab, red + red_ab(stage, D));
   block_add(dtb, red + RED_DTB);
@@ -825,6 +1001,67 @@ __device__ __forceinline__ void merge_ghosts(const MP& m, const Grid& g, const d
   }
 }
 
+// The outlet sides of one RK stage, one thread per boundary position: the
+// 3 ghost layers' flux and LF-term adjoints (sweeps) and their alpha ties,
+// through the flux function and wave speeds at the ghost state, then the
+// outlet state's VJP into the boundary cell: ogb.
+__global__ void __launch_bounds__(128) k_outlet_vjp(MP m, Grid g, const double* __restrict__ Uk,
+                                                    const double* __restrict__ Ak,
+                                                    const double* __restrict__ slots_rec, int stage,
+                                                    const double* __restrict__ red, const double* __restrict__ FbX,
+                                                    const double* __restrict__ UaX, const double* __restrict__ FbY,
+                                                    const double* __restrict__ UaY, double* ogb) {
+  const long long nc = g.ncell;
+  int side, pos, x, y;
+  boundary_pos(g, blockIdx.x * blockDim.x + threadIdx.x, side, pos, x, y);
+  if (side < 0 || !outlet_side(g, side)) return;
+  const long long c = (long long)x * g.ny + y;
+  double q[12], gs[14], ob[12], fb[12];
+#pragma unroll
+  for (int f = 0; f < 12; ++f) q[f] = Uk[f * nc + c];
+  const double gamma = Ak[c], T = Ak[nc + c];
+  const double un = outlet_un(q, side);
+  pressure_outlet_state<2>(m, q, gamma, T, un, g.Pb, gs);
+  const int D = side < 2 ? 0 : 1;
+  const int nA = D == 0 ? g.nx : g.ny;
+  const size_t npad = D == 0 ? (size_t)(g.nx + 6) * g.ny : (size_t)g.nx * (g.ny + 6);
+  const double* Fb = D == 0 ? FbX : FbY;
+  const double* Ua = D == 0 ? UaX : UaY;
+#pragma unroll
+  for (int f = 0; f < 12; ++f) {
+    ob[f] = 0.0;
+    fb[f] = 0.0;
+  }
+#pragma unroll 1
+  for (int i = 0; i < 3; ++i) {
+    const int a = (side == 0 || side == 2) ? -1 - i : nA + i;
+    const size_t k = D == 0 ? (size_t)(a + 3) * g.ny + pos : (size_t)pos * (g.ny + 6) + (a + 3);
+#pragma unroll
+    for (int f = 0; f < 12; ++f) {
+      ob[f] += Ua[f * npad + k];
+      fb[f] += Fb[f * npad + k];
+    }
+  }
+  double gcb = 0.0, Tcb = 0.0;
+  if (D == 0) flux_fn_vjp<0>(m, gs, gs[13], fb, ob, Tcb);
+  else flux_fn_vjp<1>(m, gs, gs[13], fb, ob, Tcb);
+  const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
+  const Speeds sp = speeds_of(g, u_to_prim<2>(m, gs, gs[12], gs[13]));
+  const double cx = red[red_cnt(stage, 0)], cy = red[red_cnt(stage, 1)];
+  const double wx = (cx > 0.0 && tied(sp.sx, bitsd(rs->ax[stage]))) ? red[red_ab(stage, 0)] * 3.0 / cx : 0.0;
+  const double wy = (cy > 0.0 && tied(sp.sy, bitsd(rs->ay[stage]))) ? red[red_ab(stage, 1)] * 3.0 / cy : 0.0;
+  speed_vjp(m, gs, gs[12], gs[13], 1, wx, ob, gcb, Tcb);
+  speed_vjp(m, gs, gs[12], gs[13], 2, wy, ob, gcb, Tcb);
+  double ub[12], Tb = 0.0;
+#pragma unroll
+  for (int f = 0; f < 12; ++f) ub[f] = 0.0;
+  outlet_vjp(m, q, gamma, T, un, g.Pb, ob, gcb, Tcb, ub, Tb);
+  double* o = ogb + (size_t)side * OG_B * g.lstrip + pos;
+#pragma unroll
+  for (int f = 0; f < 12; ++f) o[(size_t)f * g.lstrip] = ub[f];
+  o[(size_t)12 * g.lstrip] = Tb;
+}
+
 // One RK stage U' = a Un + b (Uk + dt L(Uk, auxk)), per interior cell of Uk:
 // the sweeps' LF terms of the cell and of the ghost entries that copy it,
 // the flux-function VJPs of both directions, the RK combination (Ubar_k +=
@@ -837,7 +1074,7 @@ __global__ void __launch_bounds__(128, 4) k_stage_merge(
     double coef, const double* __restrict__ slots_rec, int stage, double cfl, const unsigned char* __restrict__ mult,
     const double* __restrict__ red, const double* __restrict__ dt_bar_ext, const double* __restrict__ FbX,
     const double* __restrict__ UaX, const double* __restrict__ FbY, const double* __restrict__ UaY, double* Ub,
-    int ub_add, double* Ab, double* Un_b, double un_coef, int un_add) {
+    int ub_add, double* Ab, double* Un_b, double un_coef, int un_add, const double* __restrict__ ogb) {
   const long long nc = g.ncell;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
@@ -863,6 +1100,18 @@ __global__ void __launch_bounds__(128, 4) k_stage_merge(
   // only cells within four of a side are copied into ghosts
   if (x < 4 || x >= g.nx - 4) merge_ghosts<0>(m, g, q, T, x, y, FbX, UaX, ub, Tb);
   if (y < 4 || y >= g.ny - 4) merge_ghosts<1>(m, g, q, T, x, y, FbY, UaY, ub, Tb);
+  // the outlet ghosts of the sides this cell borders (k_outlet_vjp)
+  if (ogb && (x == 0 || x == g.nx - 1 || y == 0 || y == g.ny - 1)) {
+#pragma unroll 1
+    for (int side = 0; side < 4; ++side) {
+      const bool on = side == 0 ? x == 0 : side == 1 ? x == g.nx - 1 : side == 2 ? y == 0 : y == g.ny - 1;
+      if (!on || !outlet_side(g, side)) continue;
+      const double* o = ogb + (size_t)side * OG_B * g.lstrip + (side < 2 ? y : x);
+#pragma unroll
+      for (int f = 0; f < 12; ++f) ub[f] += o[(size_t)f * g.lstrip];
+      Tb += o[(size_t)12 * g.lstrip];
+    }
+  }
 #pragma unroll
   for (int f = 0; f < 12; ++f) {
     const double uo = Uo_b[f * nc + c];
@@ -961,13 +1210,29 @@ namespace adj {
 
 static inline unsigned blocks_for(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
+static bool has_outlet(const jb_grid& g) {
+  for (int s = 0; s < 4; ++s)
+    if (g.bc[s] == JB_BC_PRESSURE_OUTLET) return true;
+  return false;
+}
+
+// The scratch: FbX, UaX (12 x (nx+6) x ny each), FbY, UaY (12 x nx x (ny+6)
+// each), og (3 x 4 x OG_F x lstrip), ogb (4 x OG_B x lstrip).
+static double* og_of(const jb_grid& g, double* scratch) {
+  return scratch + 2 * 12 * ((size_t)(g.nx + 6) * g.ny + (size_t)g.nx * (g.ny + 6));
+}
+
 cudaError_t vjp_begin(const jb_mech_params& m, const jb_grid& g, const double* U4, const double* A4,
                       const double* pp_bar, const int* probe, double* Ub, double* Ab, const double* rec,
                       double* prims, const unsigned char* mult, const double* slots_rec, double cfl, double* red,
-                      cudaStream_t st) {
+                      double* scratch, cudaStream_t st) {
   k_vjp_begin<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U4, A4, probe[2] * probe[3] > 0 ? pp_bar : nullptr,
                                                         probe[0], probe[1], probe[2], probe[3], Ub, Ab, rec, prims,
                                                         mult, slots_rec, cfl, red);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !has_outlet(g)) return e;
+  k_outlet_ghosts<<<dim3(blocks_for(2LL * (g.nx + g.ny), 128), 3), 128, 0, st>>>(m, g, rec, slots_rec,
+                                                                                og_of(g, scratch), red);
   return cudaGetLastError();
 }
 
@@ -982,7 +1247,8 @@ cudaError_t chem_vjp(const jb_mech_params& m, const jb_grid& g, const double* U3
 }
 
 size_t flux_scratch_doubles(const jb_grid& g) {
-  return 2 * 12 * ((size_t)(g.nx + 6) * g.ny + (size_t)g.nx * (g.ny + 6));
+  return 2 * 12 * ((size_t)(g.nx + 6) * g.ny + (size_t)g.nx * (g.ny + 6)) +
+         (size_t)(3 * 4 * OG_F + 4 * OG_B) * g.lstrip;
 }
 
 cudaError_t flux_stage(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
@@ -995,13 +1261,22 @@ cudaError_t flux_stage(const jb_mech_params& m, const jb_grid& g, const double* 
   const int nlx = (g.ny + SW_NT - 1) / SW_NT, nsx = (g.nx + 6 + SW_R - 1) / SW_R;
   const int nly = (g.nx + SW_NT - 1) / SW_NT, nsy = (g.ny + 6 + SW_R - 1) / SW_R;
   const int nbx = nlx * nsx * 12, nby = nly * nsy * 12;
-  k_flux_sweep<<<nbx + nby, SW_NT, 0, st>>>(g, Uk, Pk, Uo_b, coef, slots_rec, stage, FbX, UaX, FbY, UaY, red, nbx,
-                                            nlx, nly);
+  const bool outlet = has_outlet(g);
+  double* og = og_of(g, scratch);
+  double* ogb = og + (size_t)3 * 4 * OG_F * g.lstrip;
+  k_flux_sweep<<<nbx + nby, SW_NT, 0, st>>>(g, Uk, Pk, outlet ? og + (size_t)stage * 4 * OG_F * g.lstrip : nullptr,
+                                            Uo_b, coef, slots_rec, stage, FbX, UaX, FbY, UaY, red, nbx, nlx, nly);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  if (outlet) {
+    k_outlet_vjp<<<blocks_for(2LL * (g.nx + g.ny), 128), 128, 0, st>>>(m, g, Uk, Ak, slots_rec, stage, red, FbX, UaX,
+                                                                       FbY, UaY, ogb);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   k_stage_merge<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, cfl, mult, red,
                                                           dt_bar_ext, FbX, UaX, FbY, UaY, Ub, ub_add ? 1 : 0, Ab,
-                                                          Un_b, un_coef, un_add ? 1 : 0);
+                                                          Un_b, un_coef, un_add ? 1 : 0, outlet ? ogb : nullptr);
   return cudaGetLastError();
 }
 

@@ -16,15 +16,18 @@ __host__ __device__ constexpr int red_ab(int s, int d) { return 1 + 5 * s + d; }
 __host__ __device__ constexpr int red_cnt(int s, int d) { return 3 + 5 * s + d; }
 
 // probe = {px, py, wx, wy}; pp_bar may be null.  prims: 3 x 4 x ncell.
+// scratch: flux_scratch_doubles(g) doubles (the outlet ghosts of the three
+// stage states go there when a side is a pressure outlet).
 cudaError_t vjp_begin(const jb_mech_params& m, const jb_grid& g, const double* U4, const double* A4,
                       const double* pp_bar, const int* probe, double* Ub, double* Ab, const double* rec,
                       double* prims, const unsigned char* mult, const double* slots_rec, double cfl, double* red,
-                      cudaStream_t st);
+                      double* scratch, cudaStream_t st);
 cudaError_t chem_vjp(const jb_mech_params& m, const jb_grid& g, const double* U3, const double* A3,
                      const double* Ub4, double* Ub3, const double* slot_dt, double* dtb, double* lnAb,
                      cudaStream_t st);
 // Doubles of the scratch that flux_stage needs (the per-face-direction
-// flux and LF-term adjoints of the padded cells).
+// flux and LF-term adjoints of the padded cells; the pressure-outlet ghost
+// states of the three stage states and their adjoints).
 size_t flux_scratch_doubles(const jb_grid& g);
 // One RK stage U' = a Un + b (Uk + dt L(Uk)) with b = coef, a = un_coef:
 // Ub (store, or add with ub_add) = Ubar_k; Un_b (store / add) += a Ubar'.

@@ -680,7 +680,8 @@ int jb_advance_ex(jb_handle* h, const double* U, const double* aux, double* U_ou
 
 // Multiplicity of every cell in the reference's padded array (periodic pad
 // of both axes, then the four sides; corners keep the periodic wrap): how
-// many padded entries copy it.  Only copy-type sides reach here.
+// many padded entries copy it.  The ghosts of a pressure-outlet side are
+// not copies and count as entries of their own (in the adjoint kernels).
 static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mult) {
   const int nx = g.nx, ny = g.ny;
   mult.assign((size_t)nx * ny, 0);
@@ -722,8 +723,9 @@ static int adj_supported(jb_handle* h) {
   if (h->xch || h->grid.bc[0] == JB_BC_HALO || h->grid.bc[1] == JB_BC_HALO)
     return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is single-domain (no x slabs)");
   for (int s = 0; s < 4; ++s)
-    if (h->grid.bc[s] == JB_BC_PRESSURE_OUTLET || h->grid.bc[s] == JB_BC_RDC_INJECTOR)
-      return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint supports periodic, slip, no-slip and zero-gradient sides");
+    if (h->grid.bc[s] == JB_BC_RDC_INJECTOR)
+      return set_err(h, JB_ERR_UNSUPPORTED,
+                     "the adjoint supports periodic, slip, no-slip, zero-gradient and pressure-outlet sides");
   return JB_OK;
 }
 
@@ -786,7 +788,7 @@ int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, do
   JB_TRY(cudaMemsetAsync(red, 0, sizeof(double) * jb::adj::RED_N, st), "reduction clear");
   // loss term of this step, the final temperature solve; primitives and tie
   // counts of the three stage states
-  JB_TRY(jb::adj::vjp_begin(m, g, U4, A4, pp_bar, h->probe, Ubar, Abar, rec, P, mult, slots, c_cfl, red, st),
+  JB_TRY(jb::adj::vjp_begin(m, g, U4, A4, pp_bar, h->probe, Ubar, Abar, rec, P, mult, slots, c_cfl, red, sc, st),
          "adjoint begin");
   // chemistry (and update_aux of U3): B1 = Ubar3
   JB_TRY(jb::adj::chem_vjp(m, g, W3, A3, Ubar, B1, slot_dt, red + jb::adj::RED_DTB, lnA_bar, st), "chemistry");

@@ -18,8 +18,12 @@ reverse mode reproduces what ``jax.grad`` of the reference computes:
 * ``jnp.linalg.solve`` (reaction_model.py:159) -> ``torch.linalg.solve``;
   ``jnp.clip`` -> ``torch.clamp``.
 
-Only the copy-type boundaries (periodic, slip_wall, zero_gradient,
-no_slip_wall) are restated here.
+Boundaries restated here: the copy types (periodic, slip_wall,
+zero_gradient, no_slip_wall) and pressure_outlet
+(boundary_conditions_2D/pressure_outlet.py:5-66) with the back pressure
+``Pb`` a constant (its sub/supersonic switch, a ``jnp.where`` in the
+reference, passes gradients to the selected branch only, as
+``torch.where`` does).
 """
 import numpy as np
 import torch
@@ -33,9 +37,10 @@ _EPS, _C1, _C2, _C3 = 1e-6, 1 / 10, 3 / 5, 3 / 10
 class Twin:
     """Mechanism tables as float64 tensors plus the solver configuration."""
 
-    def __init__(self, mech, dx, dy, bc, cfl, device="cpu"):
+    def __init__(self, mech, dx, dy, bc, cfl, device="cpu", Pb=None):
         self.m = mech
         self.dx, self.dy, self.bc, self.cfl = dx, dy, bc, cfl
+        self.Pb = Pb
         self.dev = device
         t = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=device)
         self.M = t(mech.species_M)
@@ -220,7 +225,28 @@ def reaction_source_terms(tw, U, aux, dt, lnA_offset=None):
 
 
 # ------------------------------------------------------------------ flux
-def _bc_side(kind, side, Ub, auxb):
+def _pressure_outlet_state(tw, state, gamma, T, normal_vel):
+    """boundary_conditions_2D/pressure_outlet.py:5-22 (janc_oracle's
+    _pressure_outlet_state in torch)."""
+    rho = state[0:1]
+    u = state[1:2] / rho
+    v = state[2:3] / rho
+    Y = state[4:] / rho
+    R = get_R(tw, Y)
+    p = rho * (R * T)
+    a = torch.sqrt(gamma * p / rho)
+    mask = normal_vel / a < 1
+    Pb = tw.Pb
+    rho_c = torch.where(mask, Pb / (p / rho), rho)
+    p_c = torch.where(mask, Pb * torch.ones_like(p), p)
+    T_c = torch.where(mask, p_c / (rho_c * R), T)
+    _, gamma_c, h_c, _, _ = get_thermo(tw, T_c, Y)
+    Ub = torch.cat([rho_c, rho_c * u, rho_c * v, rho_c * h_c - p_c + 0.5 * rho_c * (u ** 2 + v ** 2),
+                    rho_c * Y], 0)
+    return Ub, torch.cat([gamma_c, T_c], 0)
+
+
+def _bc_side(tw, kind, side, Ub, auxb):
     ax = 1 if side in "LR" else 2
     lo = side in "LB"
 
@@ -243,7 +269,16 @@ def _bc_side(kind, side, Ub, auxb):
         sgn = torch.ones(Ub.shape[0], dtype=Ub.dtype, device=Ub.device)
         sgn[1 if side in "LR" else 2] = -1
         return U * sgn.reshape(-1, 1, 1), A
-    raise KeyError(f"the twin restates copy-type boundaries only, not {kind}")
+    if kind == "pressure_outlet":
+        j = 0 if lo else -1
+        st, ga, Tt = take(Ub, j), take(auxb[0:1], j), take(auxb[1:2], j)
+        mom = 1 if side in "LR" else 2
+        nv = st[mom:mom + 1] / st[0:1]
+        if lo:
+            nv = -nv
+        Us, As = _pressure_outlet_state(tw, st, ga, Tt, nv)
+        return torch.cat([Us] * 3, ax), torch.cat([As] * 3, ax)
+    raise KeyError(f"the twin does not restate the {kind} boundary")
 
 
 def boundary_conditions(tw, U, aux):
@@ -260,7 +295,8 @@ def boundary_conditions(tw, U, aux):
         kind = tw.bc[key]
         if kind == "periodic":
             continue
-        Ug, Ag = _bc_side(kind, s, Up[sl[s]], Ap[sl[s]])
+        # the side reads copies: later sides write into Up / Ap in place
+        Ug, Ag = _bc_side(tw, kind, s, Up[sl[s]].clone(), Ap[sl[s]].clone())
         Up[dst[s]] = Ug
         Ap[dst[s]] = Ag
     return Up, Ap

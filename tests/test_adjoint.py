@@ -24,6 +24,11 @@ torch = pytest.importorskip("torch")
 BC_SLIP = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
 BC_MIX = {"left_boundary": "slip_wall", "right_boundary": "zero_gradient",
           "bottom_boundary": "periodic", "top_boundary": "periodic"}
+# outlets on a lo and a hi side, one per direction; the left one borders the
+# hot region (its boundary cells can hold the alpha maximum)
+BC_OUT = {"left_boundary": "pressure_outlet", "right_boundary": "zero_gradient",
+          "bottom_boundary": "slip_wall", "top_boundary": "pressure_outlet"}
+PB = 0.8 * 101325.0
 
 
 @pytest.fixture(scope="module")
@@ -64,10 +69,63 @@ def test_twin_forward_matches_reference_steps(golden_dir, omech):
                 assert np.abs(U[i].numpy() - ref[i]).sum() / den < 1e-11
 
 
-def test_twin_gradient_matches_finite_differences(omech):
+def _moving_state(om, nx, ny, seed):
+    """A 2D state with the hot region of _fields at rest and Mach numbers up
+    to 1.5 elsewhere: supersonic outflow through the right boundary cells
+    for y < ny/2 and through the top ones for 3 <= x < nx/2, subsonic in- and
+    outflow at the other boundary cells.  The hottest cell (1, ny/2) holds
+    the maxima of |u| + a and |v| + a."""
+    rng = np.random.default_rng(seed)
+    P, T, Y = _fields(om, nx, ny, seed, noisy=True)
+    T[0, 1, ny // 2] = 3500.0
+    Mx = rng.uniform(-0.5, 0.5, (nx, ny))
+    My = rng.uniform(-0.5, 0.5, (nx, ny))
+    Mx[:3] = 0.0
+    My[:3] = 0.0
+    Mx[-1, :ny // 2] = 1.5
+    My[3:nx // 2, -1] = 1.5
+    return P, T, Y, Mx, My
+
+
+def _with_velocity(U, aux, Mx, My, R):
+    """U with velocities u = Mx a, v = My a at unchanged T (aux stays valid)."""
+    rho, T, gamma = U[0], aux[1], aux[0]
+    a = np.sqrt(gamma * R * T)
+    u, v = Mx * a, My * a
+    U = U.copy()
+    U[1] = rho * u
+    U[2] = rho * v
+    U[3] = U[3] + 0.5 * rho * (u * u + v * v)
+    return U
+
+
+def test_twin_outlet_ghosts_match_oracle(omech):
+    """The twin's pressure_outlet ghosts equal the oracle's (both branches,
+    lo and hi sides in x and y)."""
+    nx, ny = 12, 10
+    P, T, Y, Mx, My = _moving_state(omech, nx, ny, 4)
+    bc = {"left_boundary": "pressure_outlet", "right_boundary": "pressure_outlet",
+          "bottom_boundary": "pressure_outlet", "top_boundary": "pressure_outlet"}
+    tw = tt.Twin(omech, 1e-4, 1e-4, bc, 0.1, Pb=PB)
+    U0, a0 = tt.state_from_PTY(tw, torch.tensor(P), torch.tensor(T), torch.tensor(Y))
+    R = tt.get_R(tw, torch.tensor(Y)).numpy()[0]
+    A = a0.numpy()
+    U = _with_velocity(U0.numpy(), A, Mx, My, R)
+    Up, Ap = tt.boundary_conditions(tw, torch.tensor(U), a0)
+    Ur, Ar = jo.boundary_conditions(omech, U, A, bc, {"Pb": PB})
+    # both branches occur on the right side
+    mach = U[1, -1] / U[0, -1] / np.sqrt(A[0, -1] * R[-1] * A[1, -1])
+    assert (mach > 1).any() and (mach < 1).any()
+    for side in (np.s_[:, :3, 3:-3], np.s_[:, -3:, 3:-3], np.s_[:, 3:-3, :3], np.s_[:, 3:-3, -3:]):
+        np.testing.assert_allclose(Up.numpy()[side], Ur[side], rtol=1e-14, atol=0)
+        np.testing.assert_allclose(Ap.numpy()[side], Ar[side], rtol=1e-14, atol=0)
+
+
+@pytest.mark.parametrize("bc", ["slip", "outlet"])
+def test_twin_gradient_matches_finite_differences(omech, bc):
     nx, ny = 16, 12
     P, T, Y = _fields(omech, nx, ny, 5, noisy=True)
-    tw = tt.Twin(omech, 1.953125e-4, 1.953125e-4, BC_SLIP, 0.1)
+    tw = tt.Twin(omech, 1.953125e-4, 1.953125e-4, BC_SLIP if bc == "slip" else BC_OUT, 0.1, Pb=PB)
     Pt, Yt = torch.tensor(P), torch.tensor(Y)
     Tt = torch.tensor(T, requires_grad=True)
     lnA = torch.zeros(19, dtype=torch.float64, requires_grad=True)
@@ -99,6 +157,7 @@ def _native(om, nx, ny, bc, P, T, Y, nsteps, cfl, probe, K, lnA=None):
     from janc_b200.solver import Solver
     dx = dy = 1.953125e-4
     s = Solver(2, nx, ny, dx, dy, bc, precision="fp64")
+    s.set_theta({"Pb": PB})
     traj = Trajectory(s, cfl, probe, checkpoint=K)
     cu = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
     Tg = cu(T).requires_grad_()
@@ -110,7 +169,7 @@ def _native(om, nx, ny, bc, P, T, Y, nsteps, cfl, probe, K, lnA=None):
 
 
 def _twin(om, nx, ny, bc, P, T, Y, nsteps, cfl, probe):
-    tw = tt.Twin(om, 1.953125e-4, 1.953125e-4, bc, cfl)
+    tw = tt.Twin(om, 1.953125e-4, 1.953125e-4, bc, cfl, Pb=PB)
     Tt = torch.tensor(T, requires_grad=True)
     lnA = torch.zeros(19, dtype=torch.float64, requires_grad=True)
     L, _, _ = tt.trajectory_loss(tw, torch.tensor(P), Tt, torch.tensor(Y), nsteps, probe, lnA)
@@ -123,10 +182,14 @@ def _rel(a, b):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("bc,noisy", [(BC_SLIP, False), (BC_MIX, True)])
+@pytest.mark.parametrize("bc,noisy", [(BC_SLIP, False), (BC_MIX, True), (BC_OUT, True)])
 def test_adjoint_matches_autograd_twin(omech, bc, noisy):
     nx, ny, nsteps = 24, 16, 4
     P, T, Y = _fields(omech, nx, ny, 3, noisy)
+    if bc is BC_OUT:
+        # the alpha maxima start at a boundary cell of the left outlet, where
+        # its ghosts' wave speeds tie with the cell's
+        T[0, 0, ny // 2] = 3300.0
     probe = (14, 6, 4, 4)
     L, gT, gA, _ = _native(omech, nx, ny, bc, P, T, Y, nsteps, 0.1, probe, K=2)
     Lr, gTr, gAr = _twin(omech, nx, ny, bc, P, T, Y, nsteps, 0.1, probe)
@@ -180,19 +243,32 @@ def test_adjoint_checkpoint_interval_does_not_change_gradient(omech):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("bc_name", ["mix", "outlet"])
 @pytest.mark.parametrize("seed_kind", ["U", "aux", "species", "dt"])
-def test_single_step_vjp_matches_twin(omech, seed_kind):
+def test_single_step_vjp_matches_twin(omech, seed_kind, bc_name):
     """One recorded step and jb_adjoint_step against the twin's reverse mode
-    of the same step, for adjoint seeds on different outputs."""
+    of the same step, for adjoint seeds on different outputs; "outlet": right
+    and top pressure outlets with sub- and supersonic outflow (and inflow)
+    through their boundary cells."""
     import ctypes
     from janc_b200.solver import Solver
     nx, ny = 24, 16
-    P, T, Y = _fields(omech, nx, ny, 8, noisy=True)
     dx = 1.953125e-4
-    s = Solver(2, nx, ny, dx, dx, BC_MIX, precision="fp64")
+    if bc_name == "mix":
+        bc = BC_MIX
+        P, T, Y = _fields(omech, nx, ny, 8, noisy=True)
+    else:
+        bc = {"left_boundary": "slip_wall", "right_boundary": "pressure_outlet",
+              "bottom_boundary": "slip_wall", "top_boundary": "pressure_outlet"}
+        P, T, Y, Mx, My = _moving_state(omech, nx, ny, 8)
+    s = Solver(2, nx, ny, dx, dx, bc, precision="fp64")
+    s.set_theta({"Pb": PB})
     L = s._lib
     cu = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
     U0, a0 = s.state_from_PTY(cu(P), cu(T), cu(Y))
+    if bc_name == "outlet":
+        R = tt.get_R(tt.Twin(omech, dx, dx, bc, 0.1), torch.tensor(Y)).numpy()[0]
+        U0 = cu(_with_velocity(U0.cpu().numpy(), a0.cpu().numpy(), Mx, My, R)).contiguous()
     assert L.jb_adjoint_reserve(s._h) == 0
     R = int(L.jb_record_doubles(s._h))
     rec = torch.empty(2 * R, dtype=torch.float64, device="cuda")
@@ -213,7 +289,7 @@ def test_single_step_vjp_matches_twin(omech, seed_kind):
     lnAb = torch.zeros(19, dtype=torch.float64, device="cuda")
     assert L.jb_adjoint_step(s._h, p(rec), p(rsl), 0.1, p(Ub), p(Ab), p(dtb), None, p(lnAb), st) == 0
     # the twin's reverse mode of the same step from the same state
-    tw = tt.Twin(omech, dx, dx, BC_MIX, 0.1)
+    tw = tt.Twin(omech, dx, dx, bc, 0.1, Pb=PB)
     Ut = U0.cpu().clone().requires_grad_()
     at = a0.cpu().clone().requires_grad_()
     lnA = torch.zeros(19, dtype=torch.float64, requires_grad=True)
