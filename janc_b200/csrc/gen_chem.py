@@ -10,10 +10,14 @@ binary serves any non-dimensionalisation.  ``jb_create`` compares the loaded
 mechanism's structure with ``GEN_*`` below and falls back to the generic
 kernel when they differ.
 
-The arithmetic restates ``src/janc_v2/model/reaction_model.py:91-193`` in
-log space: kf = exp(ln A + B ln T - Ea/(R T) + sum vf ln X),
-kb = exp(ln A + B ln T - Ea/(R T) - sum dv g - vsum ln(101325/(P0 T)) +
-sum vb ln X); the Jacobian entry is
+The arithmetic restates ``src/janc_v2/model/reaction_model.py:91-193``
+with one exponential per reaction and one per species:
+k0 = exp(ln A + B ln T - Ea/(R T)), kf = k0 prod Xc^vf,
+kb = k0 prod E^(-dv) (T P0/101325)^vsum prod Xc^vb with E_k = exp(g_k) the
+exponentiated Gibbs terms and Xc the molar concentrations clipped at 1e-50
+(the reference's exp(sum vf log Xc), exp(sum dv g) and
+(101325/(P0 T))^vsum, whose exponents are small integers); the Jacobian
+entry is
 J_kn = M_k sum_i dv_ik [q_i a_in / M_n + (vf_in M_i kf_i - vb_in M_i kb_i)/(M_n X_n)].
 
 Usage: python gen_chem.py [mechanism.yaml] > jb_chem_gen.cuh
@@ -66,9 +70,11 @@ def generate(path=None):
     w("")
     w("// Phase A: rates of every reaction for one cell.  Writes q_i = kf - kb,")
     w("// F_i = M_i kf and B_i = M_i kb to shared memory (layout [i][3][stride])")
-    w("// and accumulates w_k = sum_i dv_ik M_i q_i.")
-    w("__device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double invT,")
-    w("    const double* X, const double* lnX, const double* g, double* sh, int stride, double* wk) {")
+    w("// and accumulates w_k = sum_i dv_ik M_i q_i.  Xc: clipped concentrations;")
+    w("// E, iE: exp(g_k) and 1 / exp(g_k); Tp = T / pref, pT = pref / T.")
+    w("__device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double invT, double Tp, double pT,")
+    w("    const double* X, const double* Xc, const double* E, const double* iE, double* sh, int stride,")
+    w("    double* wk) {")
     for k in range(nr):
         w(f"  wk[{k}] = 0.0;")
     for i in range(nreac):
@@ -76,36 +82,25 @@ def generate(path=None):
         prod = [(k, int(vb[i, k])) for k in range(nr) if vb[i, k] != 0]
         dv = [(k, int(vb[i, k] - vf[i, k])) for k in range(nr) if vb[i, k] != vf[i, k]]
 
-        def lin(terms, arr):
-            parts = []
-            for k, c in terms:
-                parts.append(f"{arr}[{k}]" if c == 1 else f"{_num(c)} * {arr}[{k}]")
-            return " + ".join(parts) if parts else "0.0"
-
-        def dvsum(terms, arr):
-            s = ""
-            for k, c in terms:
-                mag = abs(c)
-                term = f"{arr}[{k}]" if mag == 1 else f"{_num(mag)} * {arr}[{k}]"
-                s += (" + " if c > 0 else " - ") + term
-            s = s.strip()
-            return s[2:] if s.startswith("+ ") else ("-" + s[2:] if s.startswith("- ") else s)
+        def powers(terms, arr):
+            # prod arr[k]^c as repeated products (c a small positive integer)
+            return [f"{arr}[{k}]" for k, c in terms for _ in range(c)]
 
         w(f"  {{  // reaction {i}")
-        w(f"    const double lk = m.lnA[{i}] + m.B[{i}] * lT - m.EaR[{i}] * invT;")
+        w(f"    const double k0 = exp(m.lnA[{i}] + m.B[{i}] * lT - m.EaR[{i}] * invT);")
         if is_tb[i]:
             terms = [f"m.tb[{i}][{j}] * X[{j}]" for j in range(ns) if tb[i, j] != 0]
             w(f"    const double Mi = {' + '.join(terms)};")
         else:
             w("    const double Mi = 1.0;")
-        w(f"    const double sf = {lin(reac, 'lnX')};")
-        w(f"    const double sb = {lin(prod, 'lnX')};")
-        w(f"    const double sg = {dvsum(dv, 'g') if dv else '0.0'};")
+        fac_f = powers(reac, "Xc")
+        eg = [f"E[{k}]" for k, c in dv if c < 0 for _ in range(-c)] + \
+             [f"iE[{k}]" for k, c in dv if c > 0 for _ in range(c)]
         vs = int(vsum[i])
-        lpw = "0.0" if vs == 0 else ("(m.lnpref - lT)" if vs == 1 else
-                                    ("-(m.lnpref - lT)" if vs == -1 else f"{vs}.0 * (m.lnpref - lT)"))
-        w("    const double kf = exp(lk + sf);")
-        w(f"    const double kb = exp(lk - sg - {lpw} + sb);")
+        pw = ["Tp"] * vs if vs > 0 else ["pT"] * (-vs)
+        fac_b = eg + pw + powers(prod, "Xc")
+        w(f"    const double kf = {' * '.join(['k0'] + fac_f)};")
+        w(f"    const double kb = {' * '.join(['k0'] + fac_b)};")
         w("    const double q = kf - kb;")
         w("    const double Mq = Mi * q;")
         for k, c in dv:

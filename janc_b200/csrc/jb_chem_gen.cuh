@@ -19,9 +19,11 @@ namespace {
 
 // Phase A: rates of every reaction for one cell.  Writes q_i = kf - kb,
 // F_i = M_i kf and B_i = M_i kb to shared memory (layout [i][3][stride])
-// and accumulates w_k = sum_i dv_ik M_i q_i.
-__device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double invT,
-    const double* X, const double* lnX, const double* g, double* sh, int stride, double* wk) {
+// and accumulates w_k = sum_i dv_ik M_i q_i.  Xc: clipped concentrations;
+// E, iE: exp(g_k) and 1 / exp(g_k); Tp = T / pref, pT = pref / T.
+__device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double invT, double Tp, double pT,
+    const double* X, const double* Xc, const double* E, const double* iE, double* sh, int stride,
+    double* wk) {
   wk[0] = 0.0;
   wk[1] = 0.0;
   wk[2] = 0.0;
@@ -31,13 +33,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
   wk[6] = 0.0;
   wk[7] = 0.0;
   {  // reaction 0
-    const double lk = m.lnA[0] + m.B[0] * lT - m.EaR[0] * invT;
+    const double k0 = exp(m.lnA[0] + m.B[0] * lT - m.EaR[0] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[0] + lnX[1];
-    const double sb = lnX[4] + lnX[6];
-    const double sg = -g[0] - g[1] + g[4] + g[6];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[0] * Xc[1];
+    const double kb = k0 * E[0] * E[1] * iE[4] * iE[6] * Xc[4] * Xc[6];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[0] -= Mq;
@@ -49,13 +48,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(0 + 2) * stride] = Mi * kb;
   }
   {  // reaction 1
-    const double lk = m.lnA[1] + m.B[1] * lT - m.EaR[1] * invT;
+    const double k0 = exp(m.lnA[1] + m.B[1] * lT - m.EaR[1] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[1] + lnX[4];
-    const double sb = lnX[2] + lnX[3];
-    const double sg = -g[1] + g[2] + g[3] - g[4];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[1] * Xc[4];
+    const double kb = k0 * E[1] * E[4] * iE[2] * iE[3] * Xc[2] * Xc[3];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[1] -= Mq;
@@ -67,13 +63,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(3 + 2) * stride] = Mi * kb;
   }
   {  // reaction 2
-    const double lk = m.lnA[2] + m.B[2] * lT - m.EaR[2] * invT;
+    const double k0 = exp(m.lnA[2] + m.B[2] * lT - m.EaR[2] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[0] + lnX[3];
-    const double sb = lnX[2] + lnX[4];
-    const double sg = -g[0] + g[2] - g[3] + g[4];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[0] * Xc[3];
+    const double kb = k0 * E[0] * E[3] * iE[2] * iE[4] * Xc[2] * Xc[4];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[0] -= Mq;
@@ -85,13 +78,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(6 + 2) * stride] = Mi * kb;
   }
   {  // reaction 3
-    const double lk = m.lnA[3] + m.B[3] * lT - m.EaR[3] * invT;
+    const double k0 = exp(m.lnA[3] + m.B[3] * lT - m.EaR[3] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[0] + lnX[2];
-    const double sb = lnX[4] + lnX[5];
-    const double sg = -g[0] - g[2] + g[4] + g[5];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[0] * Xc[2];
+    const double kb = k0 * E[0] * E[2] * iE[4] * iE[5] * Xc[4] * Xc[5];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[0] -= Mq;
@@ -103,13 +93,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(9 + 2) * stride] = Mi * kb;
   }
   {  // reaction 4
-    const double lk = m.lnA[4] + m.B[4] * lT - m.EaR[4] * invT;
+    const double k0 = exp(m.lnA[4] + m.B[4] * lT - m.EaR[4] * invT);
     const double Mi = 1.0;
-    const double sf = 2.0 * lnX[2];
-    const double sb = lnX[3] + lnX[5];
-    const double sg = -2.0 * g[2] + g[3] + g[5];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[2] * Xc[2];
+    const double kb = k0 * E[2] * E[2] * iE[3] * iE[5] * Xc[3] * Xc[5];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[2] += -2.0 * Mq;
@@ -120,13 +107,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(12 + 2) * stride] = Mi * kb;
   }
   {  // reaction 5
-    const double lk = m.lnA[5] + m.B[5] * lT - m.EaR[5] * invT;
+    const double k0 = exp(m.lnA[5] + m.B[5] * lT - m.EaR[5] * invT);
     const double Mi = m.tb[5][0] * X[0] + m.tb[5][1] * X[1] + m.tb[5][2] * X[2] + m.tb[5][3] * X[3] + m.tb[5][4] * X[4] + m.tb[5][5] * X[5] + m.tb[5][6] * X[6] + m.tb[5][7] * X[7] + m.tb[5][8] * X[8];
-    const double sf = lnX[2] + lnX[4];
-    const double sb = lnX[5];
-    const double sg = -g[2] - g[4] + g[5];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - -(m.lnpref - lT) + sb);
+    const double kf = k0 * Xc[2] * Xc[4];
+    const double kb = k0 * E[2] * E[4] * iE[5] * pT * Xc[5];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[2] -= Mq;
@@ -137,13 +121,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(15 + 2) * stride] = Mi * kb;
   }
   {  // reaction 6
-    const double lk = m.lnA[6] + m.B[6] * lT - m.EaR[6] * invT;
+    const double k0 = exp(m.lnA[6] + m.B[6] * lT - m.EaR[6] * invT);
     const double Mi = m.tb[6][0] * X[0] + m.tb[6][1] * X[1] + m.tb[6][2] * X[2] + m.tb[6][3] * X[3] + m.tb[6][4] * X[4] + m.tb[6][5] * X[5] + m.tb[6][6] * X[6] + m.tb[6][7] * X[7] + m.tb[6][8] * X[8];
-    const double sf = 2.0 * lnX[4];
-    const double sb = lnX[0];
-    const double sg = g[0] - 2.0 * g[4];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - -(m.lnpref - lT) + sb);
+    const double kf = k0 * Xc[4] * Xc[4];
+    const double kb = k0 * E[4] * E[4] * iE[0] * pT * Xc[0];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[0] += Mq;
@@ -153,13 +134,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(18 + 2) * stride] = Mi * kb;
   }
   {  // reaction 7
-    const double lk = m.lnA[7] + m.B[7] * lT - m.EaR[7] * invT;
+    const double k0 = exp(m.lnA[7] + m.B[7] * lT - m.EaR[7] * invT);
     const double Mi = m.tb[7][0] * X[0] + m.tb[7][1] * X[1] + m.tb[7][2] * X[2] + m.tb[7][3] * X[3] + m.tb[7][4] * X[4] + m.tb[7][5] * X[5] + m.tb[7][6] * X[6] + m.tb[7][7] * X[7] + m.tb[7][8] * X[8];
-    const double sf = lnX[3] + lnX[4];
-    const double sb = lnX[2];
-    const double sg = g[2] - g[3] - g[4];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - -(m.lnpref - lT) + sb);
+    const double kf = k0 * Xc[3] * Xc[4];
+    const double kb = k0 * E[3] * E[4] * iE[2] * pT * Xc[2];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[2] += Mq;
@@ -170,13 +148,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(21 + 2) * stride] = Mi * kb;
   }
   {  // reaction 8
-    const double lk = m.lnA[8] + m.B[8] * lT - m.EaR[8] * invT;
+    const double k0 = exp(m.lnA[8] + m.B[8] * lT - m.EaR[8] * invT);
     const double Mi = m.tb[8][0] * X[0] + m.tb[8][1] * X[1] + m.tb[8][2] * X[2] + m.tb[8][3] * X[3] + m.tb[8][4] * X[4] + m.tb[8][5] * X[5] + m.tb[8][6] * X[6] + m.tb[8][7] * X[7] + m.tb[8][8] * X[8];
-    const double sf = lnX[1] + lnX[4];
-    const double sb = lnX[6];
-    const double sg = -g[1] - g[4] + g[6];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - -(m.lnpref - lT) + sb);
+    const double kf = k0 * Xc[1] * Xc[4];
+    const double kb = k0 * E[1] * E[4] * iE[6] * pT * Xc[6];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[1] -= Mq;
@@ -187,13 +162,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(24 + 2) * stride] = Mi * kb;
   }
   {  // reaction 9
-    const double lk = m.lnA[9] + m.B[9] * lT - m.EaR[9] * invT;
+    const double k0 = exp(m.lnA[9] + m.B[9] * lT - m.EaR[9] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[4] + lnX[6];
-    const double sb = 2.0 * lnX[2];
-    const double sg = 2.0 * g[2] - g[4] - g[6];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[4] * Xc[6];
+    const double kb = k0 * E[4] * E[6] * iE[2] * iE[2] * Xc[2] * Xc[2];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[2] += 2.0 * Mq;
@@ -204,13 +176,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(27 + 2) * stride] = Mi * kb;
   }
   {  // reaction 10
-    const double lk = m.lnA[10] + m.B[10] * lT - m.EaR[10] * invT;
+    const double k0 = exp(m.lnA[10] + m.B[10] * lT - m.EaR[10] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[4] + lnX[6];
-    const double sb = lnX[3] + lnX[5];
-    const double sg = g[3] - g[4] + g[5] - g[6];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[4] * Xc[6];
+    const double kb = k0 * E[4] * E[6] * iE[3] * iE[5] * Xc[3] * Xc[5];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[3] += Mq;
@@ -222,13 +191,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(30 + 2) * stride] = Mi * kb;
   }
   {  // reaction 11
-    const double lk = m.lnA[11] + m.B[11] * lT - m.EaR[11] * invT;
+    const double k0 = exp(m.lnA[11] + m.B[11] * lT - m.EaR[11] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[3] + lnX[6];
-    const double sb = lnX[1] + lnX[2];
-    const double sg = g[1] + g[2] - g[3] - g[6];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[3] * Xc[6];
+    const double kb = k0 * E[3] * E[6] * iE[1] * iE[2] * Xc[1] * Xc[2];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[1] += Mq;
@@ -240,13 +206,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(33 + 2) * stride] = Mi * kb;
   }
   {  // reaction 12
-    const double lk = m.lnA[12] + m.B[12] * lT - m.EaR[12] * invT;
+    const double k0 = exp(m.lnA[12] + m.B[12] * lT - m.EaR[12] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[2] + lnX[6];
-    const double sb = lnX[1] + lnX[5];
-    const double sg = g[1] - g[2] + g[5] - g[6];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[2] * Xc[6];
+    const double kb = k0 * E[2] * E[6] * iE[1] * iE[5] * Xc[1] * Xc[5];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[1] += Mq;
@@ -258,13 +221,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(36 + 2) * stride] = Mi * kb;
   }
   {  // reaction 13
-    const double lk = m.lnA[13] + m.B[13] * lT - m.EaR[13] * invT;
+    const double k0 = exp(m.lnA[13] + m.B[13] * lT - m.EaR[13] * invT);
     const double Mi = 1.0;
-    const double sf = 2.0 * lnX[6];
-    const double sb = lnX[1] + lnX[7];
-    const double sg = g[1] - 2.0 * g[6] + g[7];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[6] * Xc[6];
+    const double kb = k0 * E[6] * E[6] * iE[1] * iE[7] * Xc[1] * Xc[7];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[1] += Mq;
@@ -275,13 +235,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(39 + 2) * stride] = Mi * kb;
   }
   {  // reaction 14
-    const double lk = m.lnA[14] + m.B[14] * lT - m.EaR[14] * invT;
+    const double k0 = exp(m.lnA[14] + m.B[14] * lT - m.EaR[14] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[4] + lnX[7];
-    const double sb = lnX[0] + lnX[6];
-    const double sg = g[0] - g[4] + g[6] - g[7];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[4] * Xc[7];
+    const double kb = k0 * E[4] * E[7] * iE[0] * iE[6] * Xc[0] * Xc[6];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[0] += Mq;
@@ -293,13 +250,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(42 + 2) * stride] = Mi * kb;
   }
   {  // reaction 15
-    const double lk = m.lnA[15] + m.B[15] * lT - m.EaR[15] * invT;
+    const double k0 = exp(m.lnA[15] + m.B[15] * lT - m.EaR[15] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[3] + lnX[7];
-    const double sb = lnX[2] + lnX[6];
-    const double sg = g[2] - g[3] + g[6] - g[7];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[3] * Xc[7];
+    const double kb = k0 * E[3] * E[7] * iE[2] * iE[6] * Xc[2] * Xc[6];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[2] += Mq;
@@ -311,13 +265,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(45 + 2) * stride] = Mi * kb;
   }
   {  // reaction 16
-    const double lk = m.lnA[16] + m.B[16] * lT - m.EaR[16] * invT;
+    const double k0 = exp(m.lnA[16] + m.B[16] * lT - m.EaR[16] * invT);
     const double Mi = 1.0;
-    const double sf = lnX[2] + lnX[7];
-    const double sb = lnX[5] + lnX[6];
-    const double sg = -g[2] + g[5] + g[6] - g[7];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - 0.0 + sb);
+    const double kf = k0 * Xc[2] * Xc[7];
+    const double kb = k0 * E[2] * E[7] * iE[5] * iE[6] * Xc[5] * Xc[6];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[2] -= Mq;
@@ -329,13 +280,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(48 + 2) * stride] = Mi * kb;
   }
   {  // reaction 17
-    const double lk = m.lnA[17] + m.B[17] * lT - m.EaR[17] * invT;
+    const double k0 = exp(m.lnA[17] + m.B[17] * lT - m.EaR[17] * invT);
     const double Mi = m.tb[17][0] * X[0] + m.tb[17][1] * X[1] + m.tb[17][2] * X[2] + m.tb[17][3] * X[3] + m.tb[17][4] * X[4] + m.tb[17][5] * X[5] + m.tb[17][6] * X[6] + m.tb[17][7] * X[7] + m.tb[17][8] * X[8];
-    const double sf = lnX[7];
-    const double sb = 2.0 * lnX[2];
-    const double sg = 2.0 * g[2] - g[7];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - (m.lnpref - lT) + sb);
+    const double kf = k0 * Xc[7];
+    const double kb = k0 * E[7] * iE[2] * iE[2] * Tp * Xc[2] * Xc[2];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[2] += 2.0 * Mq;
@@ -345,13 +293,10 @@ __device__ __forceinline__ void chem_rates_gen(const MP& m, double lT, double in
     sh[(51 + 2) * stride] = Mi * kb;
   }
   {  // reaction 18
-    const double lk = m.lnA[18] + m.B[18] * lT - m.EaR[18] * invT;
+    const double k0 = exp(m.lnA[18] + m.B[18] * lT - m.EaR[18] * invT);
     const double Mi = m.tb[18][0] * X[0] + m.tb[18][1] * X[1] + m.tb[18][2] * X[2] + m.tb[18][3] * X[3] + m.tb[18][4] * X[4] + m.tb[18][5] * X[5] + m.tb[18][6] * X[6] + m.tb[18][7] * X[7] + m.tb[18][8] * X[8];
-    const double sf = 2.0 * lnX[3];
-    const double sb = lnX[1];
-    const double sg = g[1] - 2.0 * g[3];
-    const double kf = exp(lk + sf);
-    const double kb = exp(lk - sg - -(m.lnpref - lT) + sb);
+    const double kf = k0 * Xc[3] * Xc[3];
+    const double kb = k0 * E[3] * E[3] * iE[1] * pT * Xc[1];
     const double q = kf - kb;
     const double Mq = Mi * q;
     wk[1] += Mq;

@@ -2196,31 +2196,35 @@ __device__ void chem_cell(const MP& m, double rho, const double* Y8, double T, d
 #if JB_FAST
 constexpr int CHEM_SH = 3 * NREAC;  // per-cell shared doubles of the specialised path
 
-// Specialised chemistry (structure compiled in by gen_chem.py), log-space
-// rates, FMA-contracted.  sh points at this thread's column of a
-// [CHEM_SH][stride] shared array.
+// Specialised chemistry (structure compiled in by gen_chem.py): one
+// exponential per reaction and one per species, the concentration and
+// equilibrium factors as products (their exponents are small integers),
+// FMA-contracted.  sh points at this thread's column of a [CHEM_SH][stride]
+// shared array.
 __device__ __forceinline__ void chem_cell_gen(const MP& m, double rho, const double* Y8, double T,
                                               double dt, double* S, unsigned& st, double* sh,
                                               int stride) {
-  double Yf[NS], X[NS], lnX[NR], g[NR], rMX[NR], w[NR];
+  double Yf[NS], X[NS], Xc[NR], E[NR], iE[NR], rMX[NR], w[NR];
   fill_Y(Y8, Yf);
 #pragma unroll
   for (int k = 0; k < NS; ++k) X[k] = rho * Yf[k] * m.invM[k];
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
     const double xc = X[k] < 1e-50 ? 1e-50 : X[k];
-    lnX[k] = log(xc);
+    Xc[k] = xc;
     rMX[k] = m.invM[k] / xc;
   }
   const double lT = log(T), invT = 1.0 / T, lT0T = lT + m.lnT0;
+  // get_gibbs (reaction_model.py:78-89): g = s/R - h/(R T); E = exp(g)
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
     const bool lo = T < m.Tcr[k];
     const double h = lo ? poly6(m.hc_lo[k], T) : poly6(m.hc_hi[k], T);
     const double s = lo ? poly5(m.s_lo[k], T) + m.lg_lo[k] * lT0T : poly5(m.s_hi[k], T) + m.lg_hi[k] * lT0T;
-    g[k] = s - h * invT;
+    E[k] = exp(s - h * invT);
+    iE[k] = 1.0 / E[k];
   }
-  chem_rates_gen(m, lT, invT, X, lnX, g, sh, stride, w);
+  chem_rates_gen(m, lT, invT, T / m.pref, m.pref * invT, X, Xc, E, iE, sh, stride, w);
   double J[NR][NR];
   chem_jac_gen(m, rMX, sh, stride, J);
   chem_solve(m, J, w, rho, Y8, dt, S, st);
