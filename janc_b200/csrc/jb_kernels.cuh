@@ -1468,23 +1468,41 @@ __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, con
     win_load2<0>(m, g, Uk, prims, strips, a0 - 3 + k, y, j, &q, vel, p);
     split2(j, 0, q, vel, p, al, Hp[k], Hm[k]);
   }
+  // The hi-side ghost cells nx .. nx+2 of the line (the last segment's
+  // window reaches them) go to this thread's column of shared memory first,
+  // so that the face loop's fetch is a plain load: the ghost mapping stays
+  // out of the unrolled loop body.
+  __shared__ float gh[3][4][SX_NT];
+  if (a1 + 2 >= g.nx) {
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k) {
+      f2 q;
+      float vel, p;
+      win_load2<0>(m, g, Uk, prims, strips, g.nx + k, y, j, &q, vel, p);
+      gh[k][0][threadIdx.x] = q.x;
+      gh[k][1][threadIdx.x] = q.y;
+      gh[k][2][threadIdx.x] = vel;
+      gh[k][3][threadIdx.x] = p;
+    }
+  }
   // the cells about to enter the window, fetched JB_SX_PF faces ahead into
   // buffer (c - a0) % JB_SX_PF and left untouched until then so that their
-  // loads overlap the WENO arithmetic
+  // loads overlap the WENO arithmetic (a >= a0 + 2 >= 0 here)
   double n0[JB_SX_PF], n1[JB_SX_PF];
   float nv[JB_SX_PF], np[JB_SX_PF];
   auto fetch = [&](int a, int b) {
-    if (a >= 0 && a < g.nx) {
+    if (a < g.nx) {
       const long long src = (long long)a * g.ny + y;
       n0[b] = u0[src];
       n1[b] = u1[src];
       nv[b] = prims[src];
       np[b] = prims[2 * nc + src];
     } else {
-      f2 q;
-      win_load2<0>(m, g, Uk, prims, strips, a, y, j, &q, nv[b], np[b]);
-      n0[b] = q.x;
-      n1[b] = q.y;
+      const int k = a - g.nx;
+      n0[b] = gh[k][0][threadIdx.x];
+      n1[b] = gh[k][1][threadIdx.x];
+      nv[b] = gh[k][2][threadIdx.x];
+      np[b] = gh[k][3][threadIdx.x];
     }
   };
 #pragma unroll
