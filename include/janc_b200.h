@@ -187,6 +187,51 @@ int jb_boundary_conditions(jb_handle* h, const double* U, const double* aux, dou
 int jb_set_ghost_cells(jb_handle* h, double* sendx, double* halox, double* sendy, double* haloy,
                        jb_exchange_fn fn, void* user);
 
+/* Block-structured AMR (2D, flux splitting with LF; WENO5-JS or MUSCL from
+ * the handle; no viscosity).  Blocks are [nb][nv+2][X][Y] float64: U fields,
+ * then gamma, T (the reference's blk_data), each block's own layout.
+ *
+ * jb_amr_stage replaces one stage of advance_one_step_amr
+ * (simulation/time_step/TVD_RK3.py:15-36) with the vmapped block flux and
+ * update functions of set_rhs(is_amr=True) (simulation/set_simulator.py:
+ * 37-42): G is the stage input with its 3-cell ghost layers filled by the
+ * block layer (X = bx + 6, Y = by + 6), U0 the step's first stage input (the
+ * same layout; read for stage 2 and 3, may be NULL for stage 1), out
+ * (same layout, not overlapping G or U0) receives
+ *   stage 1: G + pad(dt L(G)),  2: 3/4 U0 + 1/4 (G + pad(dt L(G))),
+ *   3: 1/3 U0 + 2/3 (G + pad(dt L(G)))
+ * over the whole padded block (the ghost entries with a zero rhs, as the
+ * reference pads its rhs) and its update_aux started from G's temperature.
+ * Every reduction is per block, as vmap makes it: the LF wave-speed maxima
+ * over the block's padded array and the temperature solve's stop over the
+ * block's padded cells.  dx, dy: the level's spacing.
+ *
+ * jb_amr_chem replaces the detailed-chemistry part of the AMR
+ * advance_one_step (set_simulator.py:106-113): blk and out are unpadded
+ * blocks (X = bx, Y = by; out may equal blk); out = U + S(U, T, dt) and its
+ * update_aux with each block's own stop.
+ *
+ * jb_amr_flux is the block flux function alone (set_simulator.py:37-40, for
+ * time schemes composed by the caller, e.g. RK2.advance_one_step_amr,
+ * simulation/time_step/RK2.py:14-32): U [nb][nv][bx+6][by+6] and aux
+ * [nb][2][bx+6][by+6] of padded blocks -> rhs [nb][nv][bx+6][by+6] =
+ * pad(dt * total_flux(U, aux), 3) with zeros in the ghost entries.
+ * jb_amr_update_aux is vmap(update_aux) (set_simulator.py:41): U [nb][nv][nx]
+ * [ny], aux_in / aux_out [nb][2][nx][ny] (padded or not), each block's
+ * temperature solve stopping on its own residuals.
+ *
+ * All need a 2D handle (its grid is not used; its mechanism, precision and
+ * reconstruction are); the flux calls return JB_ERR_UNSUPPORTED for Godunov,
+ * Steger-Warming or viscous configurations.  A mixed-precision handle
+ * computes the blocks in float64. */
+int jb_amr_stage(jb_handle* h, int nb, int bx, int by, double dx, double dy, int stage, const double* G,
+                 const double* U0, double dt, double* out, void* stream);
+int jb_amr_chem(jb_handle* h, int nb, int bx, int by, const double* blk, double dt, double* out, void* stream);
+int jb_amr_flux(jb_handle* h, int nb, int bx, int by, double dx, double dy, const double* U, const double* aux,
+                double dt, double* rhs, void* stream);
+int jb_amr_update_aux(jb_handle* h, int nb, int nx, int ny, const double* U, const double* aux_in, double* aux_out,
+                      void* stream);
+
 /* sizeof(jb_mech_params) and sizeof(jb_grid) as compiled, for binding checks. */
 int jb_sizeof_mech_params(void);
 int jb_sizeof_grid(void);

@@ -25,7 +25,8 @@ UNITS = [("jb_ensemble.cu", ["-fmad=true"]), ("jb_fast_flux32.cu", ["-fmad=true"
          ("jb_fast_god32.cu", ["-fmad=true"]), ("jb_fast_flux64.cu", ["-fmad=true"]),
          ("jb_fast_god64.cu", ["-fmad=true"]), ("jb_fast.cu", ["-fmad=true"]),
          ("jb_strict_flux.cu", ["-fmad=false"]), ("jb_strict_god.cu", ["-fmad=false"]),
-         ("jb_strict.cu", ["-fmad=false"]), ("jb_adjoint.cu", ["-fmad=true"]), ("jb_api.cu", []),
+         ("jb_strict.cu", ["-fmad=false"]), ("jb_strict_amr.cu", ["-fmad=false"]),
+         ("jb_fast_amr.cu", ["-fmad=true"]), ("jb_adjoint.cu", ["-fmad=true"]), ("jb_api.cu", []),
          ("jb_probe.cu", []), ("jb_noalloc.cu", [])]
 
 

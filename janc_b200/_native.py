@@ -33,7 +33,8 @@ EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_fun
            "jb_ens_autotune", "jb_ens_launch_shape", "jb_ens_advance", "jb_ens_advance_direct",
            "jb_ens_status", "jb_ens_last_error", "jb_ens_selftest_timeout",
            "jb_set_probe", "jb_set_log_A_offset", "jb_record_doubles", "jb_advance_ex", "jb_adjoint_reserve", "jb_adjoint_step",
-           "jb_state_from_PTY_vjp"]
+           "jb_state_from_PTY_vjp", "jb_amr_stage", "jb_amr_chem", "jb_amr_flux",
+           "jb_amr_update_aux"]
 
 _lib = None
 
@@ -113,6 +114,10 @@ def lib(path=None):
     L.jb_adjoint_reserve.argtypes = [vp]
     L.jb_adjoint_step.argtypes = [vp, dp, dp, d, dp, dp, dp, dp, dp, vp]
     L.jb_state_from_PTY_vjp.argtypes = [vp, dp, dp, dp, dp, dp, dp, vp]
+    L.jb_amr_stage.argtypes = [vp, i, i, i, d, d, i, dp, dp, d, dp, vp]
+    L.jb_amr_chem.argtypes = [vp, i, i, i, dp, d, dp, vp]
+    L.jb_amr_flux.argtypes = [vp, i, i, i, d, d, dp, dp, d, dp, vp]
+    L.jb_amr_update_aux.argtypes = [vp, i, i, i, dp, dp, dp, vp]
     L.jb_ens_selftest_timeout.argtypes = [vp, d, ctypes.POINTER(ctypes.c_uint), vp]
     L.jb_ens_last_error.argtypes = [vp]
     L.jb_ens_last_error.restype = ctypes.c_char_p

@@ -815,6 +815,93 @@ int jb_state_from_PTY_vjp(jb_handle* h, const double* P, const double* T, const 
   return JB_OK;
 }
 
+static int amr_check(jb_handle* h, int nb, int bx, int by) {
+  if (!h) return JB_ERR_ARG;
+  if (h->dim != 2) return set_err(h, JB_ERR_ARG, "block AMR is 2D");
+  if (h->grid.scheme != JB_FLUX_LF || h->grid.visc)
+    return set_err(h, JB_ERR_UNSUPPORTED, "block AMR supports LF flux splitting without viscosity");
+  if (nb < 0 || bx < 1 || by < 1) return set_err(h, JB_ERR_ARG, "bad block shape");
+  return JB_OK;
+}
+
+static bool overlaps(const double* a, const double* b, long long n) {
+  return a && b && a < b + n && b < a + n;
+}
+
+int jb_amr_stage(jb_handle* h, int nb, int bx, int by, double dx, double dy, int stage, const double* G,
+                 const double* U0, double dt, double* out, void* stream) {
+  if (int rc = amr_check(h, nb, bx, by)) return rc;
+  if (stage < 1 || stage > 3) return set_err(h, JB_ERR_ARG, "stage must be 1, 2 or 3");
+  if (!G || !out || (stage > 1 && !U0)) return set_err(h, JB_ERR_ARG, "null pointer");
+  if (!(dx > 0.0) || !(dy > 0.0)) return set_err(h, JB_ERR_ARG, "dx and dy must be positive");
+  const int nv = h->grid.nv;
+  const long long nc = (long long)(bx + 6) * (by + 6), n = (long long)nb * (nv + 2) * nc;
+  if (overlaps(out, G, n) || (stage > 1 && overlaps(out, U0, n)))
+    return set_err(h, JB_ERR_ARG, "out must not overlap G or U0");
+  if (nb == 0) return JB_OK;
+  jb::jb_amr_io io;
+  io.gU = G;
+  io.gA = G + nv * nc;
+  io.gsU = io.gsA = (nv + 2) * nc;
+  io.u0 = stage > 1 ? U0 : nullptr;
+  io.u0s = (nv + 2) * nc;
+  io.oU = out;
+  io.oA = out + nv * nc;
+  io.osU = io.osA = (nv + 2) * nc;
+  JB_TRY(h->ops->amr_stage(h->mech, h->grid, nb, bx, by, dx, dy, stage, io, h->slots, dt, (cudaStream_t)stream),
+         "amr_stage");
+  return JB_OK;
+}
+
+int jb_amr_flux(jb_handle* h, int nb, int bx, int by, double dx, double dy, const double* U, const double* aux,
+                double dt, double* rhs, void* stream) {
+  if (int rc = amr_check(h, nb, bx, by)) return rc;
+  if (!U || !aux || !rhs) return set_err(h, JB_ERR_ARG, "null pointer");
+  if (!(dx > 0.0) || !(dy > 0.0)) return set_err(h, JB_ERR_ARG, "dx and dy must be positive");
+  const int nv = h->grid.nv;
+  const long long nc = (long long)(bx + 6) * (by + 6);
+  if (overlaps(rhs, U, (long long)nb * nv * nc)) return set_err(h, JB_ERR_ARG, "rhs must not overlap U");
+  if (nb == 0) return JB_OK;
+  jb::jb_amr_io io;
+  io.gU = U;
+  io.gA = aux;
+  io.gsU = nv * nc;
+  io.gsA = 2 * nc;
+  io.u0 = nullptr;
+  io.u0s = 0;
+  io.oU = rhs;
+  io.oA = nullptr;
+  io.osU = nv * nc;
+  io.osA = 0;
+  JB_TRY(h->ops->amr_stage(h->mech, h->grid, nb, bx, by, dx, dy, 0, io, h->slots, dt, (cudaStream_t)stream),
+         "amr_flux");
+  return JB_OK;
+}
+
+int jb_amr_update_aux(jb_handle* h, int nb, int nx, int ny, const double* U, const double* aux_in, double* aux_out,
+                      void* stream) {
+  if (!h) return JB_ERR_ARG;
+  if (h->dim != 2) return set_err(h, JB_ERR_ARG, "block AMR is 2D");
+  if (nb < 0 || nx < 1 || ny < 1) return set_err(h, JB_ERR_ARG, "bad block shape");
+  if (!U || !aux_in || !aux_out) return set_err(h, JB_ERR_ARG, "null pointer");
+  const long long nc = (long long)nx * ny;
+  if (overlaps(aux_out, aux_in, 2LL * nb * nc)) return set_err(h, JB_ERR_ARG, "aux_out must not overlap aux_in");
+  if (nb == 0) return JB_OK;
+  JB_TRY(h->ops->amr_update(h->mech, nb, nc, U, aux_in, aux_out, h->slots, (cudaStream_t)stream), "amr_update");
+  return JB_OK;
+}
+
+int jb_amr_chem(jb_handle* h, int nb, int bx, int by, const double* blk, double dt, double* out, void* stream) {
+  if (int rc = amr_check(h, nb, bx, by)) return rc;
+  if (!blk || !out) return set_err(h, JB_ERR_ARG, "null pointer");
+  if (!(dt > 0.0)) return set_err(h, JB_ERR_ARG, "dt must be positive");
+  const long long n = (long long)nb * (h->grid.nv + 2) * bx * by;
+  if (out != blk && overlaps(out, blk, n)) return set_err(h, JB_ERR_ARG, "out must equal blk or not overlap it");
+  if (nb == 0) return JB_OK;
+  JB_TRY(h->ops->amr_chem(h->mech, nb, bx, by, blk, out, h->slots, dt, (cudaStream_t)stream), "amr_chem");
+  return JB_OK;
+}
+
 int jb_sizeof_mech_params(void) { return (int)sizeof(jb_mech_params); }
 int jb_sizeof_grid(void) { return (int)sizeof(jb_grid); }
 

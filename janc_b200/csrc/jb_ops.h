@@ -8,6 +8,21 @@
 
 namespace jb {
 
+// Block arrays of one AMR stage call: U fields and (gamma, T) of each block
+// at its own block stride (one [nb][nv+2][X][Y] array gives U = base,
+// A = base + nv X Y and both strides (nv+2) X Y; separate [nb][nv][X][Y] and
+// [nb][2][X][Y] arrays give strides nv X Y and 2 X Y).
+struct jb_amr_io {
+  const double* gU;  // stage input
+  const double* gA;
+  long long gsU, gsA;
+  const double* u0;  // U fields of the step's first stage input (stage 2, 3)
+  long long u0s;
+  double* oU;        // result
+  double* oA;        // (gamma, T) of the result (stage 1..3)
+  long long osU, osA;
+};
+
 struct Ops {
   const char* name;
   // 2D stepping (jb_advance) solves each new state's temperature per cell
@@ -65,6 +80,18 @@ struct Ops {
   // wave speeds into alpha slot aidx (no launch without such sides)
   cudaError_t (*strips)(int dim, const jb_mech_params& m, const jb_grid& g, const double* U, const double* aux,
                         double* strips, jb_slots* slots, int aidx, cudaStream_t st);
+  // block-structured AMR (2D, flux splitting): one SSP-RK3 stage (1..3) of nb
+  // ghost-padded blocks [nb][nv+2][bx+6][by+6] (G the stage input, U0 the
+  // step's first stage input), and the chemistry with its temperature solve
+  // of nb unpadded blocks [nb][nv+2][bx][by]; g supplies the reconstruction
+  // (stage 0: out = pad(dt L(G)) alone) and update_aux of nb blocks of nc
+  // cells with each block's own stop (U [nb][nv][..], aux [nb][2][..])
+  cudaError_t (*amr_stage)(const jb_mech_params& m, const jb_grid& g, int nb, int bx, int by, double dx,
+                           double dy, int stage, const jb_amr_io& io, jb_slots* slots, double dt, cudaStream_t st);
+  cudaError_t (*amr_update)(const jb_mech_params& m, int nb, long long nc, const double* U, const double* aux_in,
+                            double* aux_out, jb_slots* slots, cudaStream_t st);
+  cudaError_t (*amr_chem)(const jb_mech_params& m, int nb, int bx, int by, const double* blk, double* out,
+                          jb_slots* slots, double dt, cudaStream_t st);
 };
 
 // Doubles of the viscous scratch (node planes and node fluxes) of a grid.

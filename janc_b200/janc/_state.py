@@ -90,6 +90,21 @@ def solver_for_padded(Up, Ap, dx=1.0, dy=1.0):
     return s, Up[inner].contiguous(), Ap[inner].contiguous()
 
 
+def solver_for_amr():
+    """Cached 2D native solver whose mechanism, precision and flux options
+    the block-AMR calls use (its own grid is not used by them)."""
+    from ..solver import Solver
+    key = ("amr", config["precision"], config["mechanism"], repr(config["nondim"]), repr(config["flux"]),
+           repr(config["transport"]))
+    s = _solvers.get(key)
+    if s is None:
+        bc = {k: "periodic" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
+        s = Solver(2, 8, 8, 1.0, 1.0, bc, mechanism(), precision=config["precision"], flux_config=config["flux"],
+                   transport_config=config["transport"])
+        _solvers[key] = s
+    return s
+
+
 def reset_solvers():
     for s in _solvers.values():
         s.close()

@@ -19,7 +19,7 @@ def set_rhs(dim, reaction_config, source_config=None, is_parallel=False, is_amr=
     in an initialised torch.distributed group); ghost columns come from the
     neighbouring slabs (parallel/boundary.py)."""
     if is_amr:
-        raise NotImplementedError("AMR is not part of this build")
+        return _set_rhs_amr(dim, reaction_config, source_config)
     if is_parallel and _state.config["slab"] is None:
         from ...slab import Slab
         _state.config["slab"] = Slab()
@@ -50,7 +50,8 @@ def set_advance_func(dim, flux_config, reaction_config, time_control, is_amr, fl
     composed as the reference composes it, from the native flux_func,
     update_aux and reaction_source_terms and the user's callable."""
     if is_amr:
-        raise NotImplementedError("AMR is not part of this build")
+        return _set_advance_func_amr(flux_config, reaction_config, time_control, flux_func, update_func,
+                                     source_func)
     scheme = time_control["temporal_evolution_scheme"]
     if scheme not in time_step_dict:
         raise KeyError(scheme)
@@ -91,6 +92,102 @@ def set_advance_func(dim, flux_config, reaction_config, time_control, is_amr, fl
         U1, aux1 = s.advance_one_step(Ud, auxd, dx, dy if dim == "2D" else None, float(dt), theta)
         return _state.back(U1, kind), _state.back(aux1, kind)
     return advance_one_step
+
+
+def _set_rhs_amr(dim, reaction_config, source_config):
+    """set_rhs(is_amr=True) (set_simulator.py:37-42, 64-70): the block flux
+    function pad(dt * total_flux(U, aux), 3) and update_aux of ghost-padded
+    blocks [nb][nv][bx+6][by+6], every reduction per block (vmapped in the
+    reference), as native calls.  Flux splitting with LF only (the kernels'
+    scheme), detailed chemistry, no user source: the reference adds the
+    interior-shaped AMR source to the padded flux, which cannot broadcast."""
+    if dim != "2D":
+        raise NotImplementedError("block AMR is 2D (AMR_Simulator fixes dim = '2D')")
+    fc = _state.config["flux"]
+    if (fc.get("solver_type") != "flux_splitting" or fc.get("split_method", "LF") != "LF"
+            or fc.get("viscosity", "off") == "on"):
+        raise NotImplementedError("block AMR runs flux splitting with LF (WENO5-JS or MUSCL) without viscosity")
+    if not reaction_config["is_detailed_chemistry"]:
+        raise NotImplementedError("non-detailed chemistry (an N2-only state) is outside the 9-species path")
+    if source_config is not None:
+        raise NotImplementedError("a user source with AMR: the reference adds an interior-shaped source to the "
+                                  "padded block flux (set_simulator.py:66-70), which cannot broadcast")
+
+    def flux_func(U, aux, dx, dy, dt, theta):
+        Ud, kind = _state.to_device(U)
+        auxd, _ = _state.to_device(aux)
+        return _state.back(_state.solver_for_amr().amr_flux(Ud, auxd, dx, dy, float(dt)), kind)
+
+    def update_func(U, aux):
+        Ud, kind = _state.to_device(U)
+        auxd, _ = _state.to_device(aux)
+        return _state.back(_state.solver_for_amr().amr_update_aux(Ud, auxd), kind)
+
+    flux_func._janc_b200_amr_flux = True
+    update_func._janc_b200_amr_update = True
+    return flux_func, update_func, None
+
+
+def _set_advance_func_amr(flux_config, reaction_config, time_control, flux_func, update_func, source_func):
+    """set_advance_func(is_amr=True) (set_simulator.py:73-110): the time
+    scheme's AMR form on the blocks, then the blocks' chemistry and
+    update_aux (one native call, ``jb_amr_chem``)."""
+    scheme = time_control["temporal_evolution_scheme"] + "_amr"
+    if scheme not in time_step_dict:
+        raise KeyError(scheme)
+    step = time_step_dict[scheme]
+    if source_func is not None:
+        raise NotImplementedError("a user source with AMR (see set_rhs)")
+
+    def advance_flux(level, blk_data, dx, dy, dt, ref_blk_data, ref_blk_info, theta=None):
+        return step(level, blk_data, dx, dy, dt, ref_blk_data, ref_blk_info, theta, flux_func, update_func)
+    if not reaction_config["is_detailed_chemistry"]:
+        return advance_flux
+
+    def advance_one_step(level, blk_data, dx, dy, dt, ref_blk_data, ref_blk_info, theta=None):
+        blk = advance_flux(level, blk_data, dx, dy, dt, ref_blk_data, ref_blk_info, theta=None)
+        blkd, kind = _state.to_device(blk)
+        return _state.back(_state.solver_for_amr().amr_chem(blkd, float(dt)), kind)
+    return advance_one_step
+
+
+def AMR_Simulator(simulation_config):  # noqa: N802 (the reference's name)
+    """(advance_func_amr, advance_func_base) as set_simulator.py:496-532:
+    ``advance_func_amr(level, blk_data, dx, dy, dt, ref_blk_data,
+    ref_blk_info, theta=None)`` advances one refinement level's blocks
+    (``blk_data``: the coarser level's blocks, ``ref_blk_data``: this
+    level's; the ghost layers come from the block layer, see
+    ``time_step.set_amr_module``); ``advance_func_base(blk_data, dx, dy, dt,
+    theta=None)`` advances the level-0 array [1][nv+2][nx][ny] with the
+    boundary conditions of ``boundary_config``."""
+    import torch
+    dim = "2D"
+    thermo_config = simulation_config["thermo_config"]
+    reaction_config = simulation_config["reaction_config"]
+    transport_config = simulation_config.get("transport_config", None)
+    flux_config = simulation_config["flux_config"]
+    boundary_config = simulation_config["boundary_config"]
+    source_config = simulation_config.get("source_config", None)
+    nondim_config = simulation_config.get("nondim_config", None)
+    time_control = simulation_config["time_config"]
+    _state.reset_solvers()
+    _state.config["slab"] = None
+    _state.config["precision"] = simulation_config.get("precision", "fp64")
+    thermo_model.set_thermo(thermo_config, nondim_config, dim)
+    reaction_model.set_reaction(reaction_config, nondim_config, dim)
+    flux.set_flux_solver(flux_config, transport_config, nondim_config)
+    boundary.set_boundary(boundary_config, dim)
+    ff, uf, sf = set_rhs(dim, reaction_config, source_config, False, True)
+    advance_func_amr = set_advance_func(dim, flux_config, reaction_config, time_control, True, ff, uf, sf)
+    ff, uf, sf = set_rhs(dim, reaction_config, source_config, False, False)
+    advance_func_body = set_advance_func(dim, flux_config, reaction_config, time_control, False, ff, uf, sf)
+
+    def advance_func_base(blk_data, dx, dy, dt, theta=None):
+        b, kind = _state.to_device(blk_data)
+        U, aux = b[0, :-2].contiguous(), b[0, -2:].contiguous()
+        U, aux = advance_func_body(U, aux, dx, dy, dt, theta)
+        return _state.back(torch.cat([U, aux], dim=0)[None], kind)
+    return advance_func_amr, advance_func_base
 
 
 def _h5_module():

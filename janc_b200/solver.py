@@ -391,6 +391,81 @@ class Solver:
                                                          _stream()), self._h, "jb_reaction_source_terms")
         return out
 
+    def _check_blocks(self, blk, padded, name):
+        if self.dim != 2:
+            raise ValueError("block AMR needs a 2D solver")
+        if not isinstance(blk, torch.Tensor) or blk.device.type != "cuda" or blk.dtype != torch.float64:
+            raise TypeError(f"{name} must be a float64 CUDA tensor")
+        if blk.ndim != 4 or blk.shape[1] != self.nv + 2 or (padded and min(blk.shape[2:]) < 7):
+            raise ValueError(f"{name} has shape {tuple(blk.shape)}, expected (nb, {self.nv + 2}, X, Y)"
+                             + (" with 3 ghost layers on each side" if padded else ""))
+        if not blk.is_contiguous():
+            raise ValueError(f"{name} must be contiguous")
+
+    def amr_stage(self, G, U0, stage, dx, dy, dt):
+        """One SSP-RK3 stage of ghost-padded AMR blocks (TVD_RK3.py:15-36 with
+        the vmapped block flux and update_aux of set_simulator.py:37-42):
+        G, U0 [nb][nv+2][bx+6][by+6] (U fields, gamma, T; U0 the step's
+        first stage input, unused for stage 1).  Returns the new padded
+        blocks (ghost entries combined with a zero rhs) with their (gamma,
+        T) from the block's own temperature solve."""
+        self._check_blocks(G, True, "G")
+        if stage > 1:
+            self._check_blocks(U0, True, "U0")
+            if U0.shape != G.shape:
+                raise ValueError("U0 and G differ in shape")
+        out = torch.empty_like(G)
+        nb, _, X, Y = G.shape
+        _native.check(self._lib.jb_amr_stage(self._h, nb, X - 6, Y - 6, float(dx), float(dy), int(stage), _ptr(G),
+                                             _ptr(U0) if stage > 1 else None, float(dt), _ptr(out), _stream()),
+                      self._h, "jb_amr_stage")
+        return out
+
+    def amr_flux(self, U, aux, dx, dy, dt):
+        """The vmapped block flux function (set_simulator.py:37-40): padded
+        blocks U [nb][nv][bx+6][by+6], aux [nb][2][..] -> pad(dt * total_flux,
+        3) with zeros in the ghost entries."""
+        for name, t, nf in (("U", U, self.nv), ("aux", aux, 2)):
+            if not isinstance(t, torch.Tensor) or t.device.type != "cuda" or t.dtype != torch.float64:
+                raise TypeError(f"{name} must be a float64 CUDA tensor")
+            if t.ndim != 4 or t.shape[1] != nf or min(t.shape[2:]) < 7 or not t.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous (nb, {nf}, X, Y) array of padded blocks")
+        if U.shape[0] != aux.shape[0] or U.shape[2:] != aux.shape[2:]:
+            raise ValueError("U and aux differ in their blocks")
+        out = torch.empty_like(U)
+        nb, _, X, Y = U.shape
+        _native.check(self._lib.jb_amr_flux(self._h, nb, X - 6, Y - 6, float(dx), float(dy), _ptr(U), _ptr(aux),
+                                            float(dt), _ptr(out), _stream()), self._h, "jb_amr_flux")
+        return out
+
+    def amr_update_aux(self, U, aux):
+        """vmap(update_aux) (set_simulator.py:41): U [nb][nv][X][Y], aux
+        [nb][2][X][Y]; each block's temperature solve stops on its own
+        residuals."""
+        for name, t, nf in (("U", U, self.nv), ("aux", aux, 2)):
+            if not isinstance(t, torch.Tensor) or t.device.type != "cuda" or t.dtype != torch.float64:
+                raise TypeError(f"{name} must be a float64 CUDA tensor")
+            if t.ndim != 4 or t.shape[1] != nf or not t.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous (nb, {nf}, X, Y) array of blocks")
+        if U.shape[0] != aux.shape[0] or U.shape[2:] != aux.shape[2:]:
+            raise ValueError("U and aux differ in their blocks")
+        out = torch.empty_like(aux)
+        nb, _, X, Y = U.shape
+        _native.check(self._lib.jb_amr_update_aux(self._h, nb, X, Y, _ptr(U), _ptr(aux), _ptr(out), _stream()),
+                      self._h, "jb_amr_update_aux")
+        return out
+
+    def amr_chem(self, blk, dt, out=None):
+        """Chemistry and update_aux of unpadded AMR blocks [nb][nv+2][bx][by]
+        (set_simulator.py:106-113), each block's temperature solve stopping
+        on its own residuals."""
+        self._check_blocks(blk, False, "blk")
+        out = torch.empty_like(blk) if out is None else out
+        nb, _, X, Y = blk.shape
+        _native.check(self._lib.jb_amr_chem(self._h, nb, X, Y, _ptr(blk), float(dt), _ptr(out), _stream()),
+                      self._h, "jb_amr_chem")
+        return out
+
     def advance(self, U, aux, nsteps=1, dt=None, cfl=None, theta=None, dt_hist=None):
         """``nsteps`` fused steps; CFL time steps when ``cfl`` is given,
         otherwise the fixed ``dt``.  Returns (U, aux, dt_hist) with dt_hist a

@@ -1308,6 +1308,75 @@ class SlabSolver:
 # --------------------------------------------------------------------------
 # initial-state builder (the examples' pattern)
 # --------------------------------------------------------------------------
+# --------------------------------------------------------------------------
+# block-structured AMR step  (simulation/time_step/TVD_RK3.py:15-36 with the
+# AMR block functions of simulation/set_simulator.py:37-42, 64-70, 97-113)
+# --------------------------------------------------------------------------
+def amr_flux_func(m, U, aux, dx, dy, dt, recon="WENO5_JS"):
+    """set_simulator.py:37-40: per ghost-padded block [nv][bx+6][by+6],
+    dt * total_flux padded back with three rows / columns of zeros (vmapped
+    over the blocks, so the LF maxima are each block's own)."""
+    out = np.zeros_like(U)
+    for b in range(U.shape[0]):
+        out[b, :, 3:-3, 3:-3] = dt * total_flux(m, U[b], aux[b], dx, dy, recon)
+    return out
+
+
+def amr_update_func(m, U, aux):
+    """vmap(update_aux) (set_simulator.py:41): each block's temperature
+    solve stops on its own max |res| (the batched while_loop)."""
+    return np.stack([update_aux(m, np.ascontiguousarray(U[b]), aux[b]) for b in range(U.shape[0])])
+
+
+def tvd_rk3_amr(m, amr, level, blk_data, dx, dy, dt, ref_blk_data, ref_blk_info, recon="WENO5_JS"):
+    """TVD_RK3.advance_one_step_amr (TVD_RK3.py:15-36) with the block flux
+    and update functions of set_rhs(is_amr=True).  ``amr`` is the block
+    layer (``get_ghost_block_data``, ``update_external_boundary``);
+    ``blk_data`` the coarser level's blocks, ``ref_blk_data`` this level's."""
+    def rhs(U, aux):
+        return amr_flux_func(m, U, aux, dx, dy, dt, recon)
+
+    def upd(U, aux):
+        return amr_update_func(m, U, aux)
+
+    def back(U, aux):
+        b = np.concatenate([U, aux], axis=1)[..., 3:-3, 3:-3]
+        return amr.update_external_boundary(level, blk_data, np.ascontiguousarray(b), ref_blk_info)
+
+    g = amr.get_ghost_block_data(ref_blk_data, ref_blk_info)
+    U, aux = g[:, 0:-2], g[:, -2:]
+    U1 = U + rhs(U, aux)
+    aux1 = upd(U1, aux)
+    g1 = amr.get_ghost_block_data(back(U1, aux1), ref_blk_info)
+    U1, aux1 = g1[:, 0:-2], g1[:, -2:]
+    U2 = 3 / 4 * U + 1 / 4 * (U1 + rhs(U1, aux1))
+    aux2 = upd(U2, aux1)
+    g2 = amr.get_ghost_block_data(back(U2, aux2), ref_blk_info)
+    U2, aux2 = g2[:, 0:-2], g2[:, -2:]
+    U3 = 1 / 3 * U + 2 / 3 * (U2 + rhs(U2, aux2))
+    aux3 = upd(U3, aux2)
+    return back(U3, aux3)
+
+
+def amr_chemistry(m, blk, dt):
+    """The detailed-chemistry part of the AMR advance_one_step
+    (set_simulator.py:106-113): vmapped reaction_source_terms, U + dU and
+    the blocks' update_aux, on unpadded blocks [nb][nv+2][bx][by]."""
+    Ub, auxb = blk[:, 0:-2], blk[:, -2:]
+    dU = np.stack([reaction_source_terms(m, np.ascontiguousarray(Ub[b]), auxb[b], dt) for b in range(Ub.shape[0])])
+    Ub = Ub + dU
+    auxb = amr_update_func(m, Ub, auxb)
+    return np.concatenate([Ub, auxb], axis=1)
+
+
+def advance_one_step_amr(m, amr, level, blk_data, dx, dy, dt, ref_blk_data, ref_blk_info, recon="WENO5_JS"):
+    """One AMR step of the detailed-chemistry flux-splitting path (the
+    advance_one_step of set_advance_func(is_amr=True), set_simulator.py:
+    97-113): tvd_rk3_amr, then amr_chemistry."""
+    blk = tvd_rk3_amr(m, amr, level, blk_data, dx, dy, dt, ref_blk_data, ref_blk_info, recon)
+    return amr_chemistry(m, blk, dt)
+
+
 def state_from_PTY(m, P, T, Y, vel=None):
     """rho = P/(R T), rhoE = rho h - P (+ kinetic), aux = [gamma, T]
     (examples/janc_basic_example1.ipynb, ``initial_conditions``)."""

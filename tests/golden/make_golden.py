@@ -400,7 +400,61 @@ def gen_mid2d(ref):
     np.savez_compressed(os.path.join(HERE, "channel128x64_200.npz"), **rec)
 
 
-GROUPS = {"long1d": gen_long1d, "fsec": gen_fsec, "prim": gen_prim, "cfl2d": gen_cfl2d, "mid2d": gen_mid2d}
+def gen_amr(ref):
+    """Block-AMR steps of the reference's own AMR_Simulator
+    (set_simulator.py:496-532: advance_one_step_amr of TVD_RK3.py:15-36 with
+    the vmapped block flux, update_aux and chemistry of set_simulator.py:
+    37-42, 97-113), the external jaxamr block layer played by
+    tests/golden/amr_blocks.py (a single level of blocks tiling a rectangle,
+    zero-gradient mirror outside it).  Two layouts: 3 x 2 blocks of 20 x 20
+    cells (each block two by two interior tiles of the kernel, one of them
+    partial) for two steps, and 2 x 3 blocks of 7 x 9 cells for one step;
+    SI units, dx = dy = 1e-4 m, dt = 1e-8 s; a 30 atm / 3000 K region with
+    seeded +-5 % temperature blobs (default_rng(11)) over the block seams, a
+    seeded velocity field of up to 50 m/s."""
+    sys.path.insert(0, HERE)
+    import amr_blocks
+    import jaxamr
+    from janc_v2.model import thermo_model
+    from janc_v2.simulation import set_simulator
+    jaxamr.amr.get_ghost_block_data = staticmethod(amr_blocks.get_ghost_block_data)
+    jaxamr.amr.update_external_boundary = staticmethod(amr_blocks.update_external_boundary)
+    mech = os.path.join(ref, "examples", "9sp-19r-H2-Air.yaml")
+    cfg = _sim_config("2D", mech, {"dx": 1e-4, "dy": 1e-4},
+                      {"left_boundary": "slip_wall", "right_boundary": "slip_wall",
+                       "bottom_boundary": "slip_wall", "top_boundary": "slip_wall"})
+    adv_amr, _ = set_simulator.AMR_Simulator(cfg)
+    rng = np.random.default_rng(11)
+    rec = {"dx": 1e-4, "dy": 1e-4, "dt": 1e-8}
+    for name, nbx, nby, bx, by, nsteps in (("b20", 3, 2, 20, 20, 2), ("b7x9", 2, 3, 7, 9, 1)):
+        nx, ny = nbx * bx, nby * by
+        P = np.full((1, nx, ny), 101325.0)
+        T = np.full((1, nx, ny), 300.0)
+        Y = np.tile(_stoich_Y(1.0)[:, None, None], (1, nx, ny))
+        hot = (np.arange(nx)[:, None] < int(0.45 * nx)) & (np.arange(ny)[None, :] < int(0.7 * ny))
+        xs, ys = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+        bump = np.zeros((nx, ny))
+        for _ in range(6):
+            a, sig = rng.uniform(-0.05, 0.05), rng.uniform(1.5, 4.0)
+            cx, cy = rng.uniform(0, nx), rng.uniform(0, ny)
+            bump += a * np.exp(-((xs - cx) ** 2 + (ys - cy) ** 2) / (2 * sig ** 2))
+        P[0][hot] = 30 * 101325.0
+        T[0][hot] = 3000.0 * (1 + bump[hot])
+        vel = [rng.uniform(-50.0, 50.0, (1, nx, ny)), rng.uniform(-50.0, 50.0, (1, nx, ny))]
+        U0, aux0 = _state(thermo_model, P, T, Y, vel)
+        grid = np.concatenate([U0, aux0], axis=0)
+        blk = np.ascontiguousarray(amr_blocks.blocks_from_grid(grid, nbx, nby))
+        info = amr_blocks.info(nbx, nby)
+        rec[f"{name}_layout"] = np.array([nbx, nby, bx, by])
+        rec[f"{name}_blk0"] = blk
+        for s in range(1, nsteps + 1):
+            blk = np.ascontiguousarray(np.asarray(adv_amr(1, C(blk), 1e-4, 1e-4, 1e-8, C(blk), info)))
+            rec[f"{name}_blk{s}"] = blk
+    np.savez_compressed(os.path.join(HERE, "amr_blocks.npz"), **rec)
+
+
+GROUPS = {"long1d": gen_long1d, "fsec": gen_fsec, "prim": gen_prim, "cfl2d": gen_cfl2d, "mid2d": gen_mid2d,
+          "amr": gen_amr}
 
 
 def main():
