@@ -661,7 +661,139 @@ def sub_records(args):
     CFL = cfl_keep
     out["ensemble"] = ensemble_record(args, None, 0, 1, args.sub_steps, "mixed", with_cpu=False)
     out["adjoint"] = adjoint_record(args, None, 1, args.sub_steps)
+    out["amr"] = amr_record(args)
     return out
+
+
+# --------------------------------------------------------------- AMR blocks
+AMR_NBX, AMR_NBY, AMR_B = 64, 16, 20
+
+
+class DeviceBlockLayer:
+    """A single-level block layer on the device standing in for the external
+    jaxamr package (which JANC's AMR step calls for its blocks' ghost
+    layers): nbx x nby blocks of b x b cells tiling a rectangle; a block's
+    3-cell ghost layers are its neighbours' cells, mirrored (zero gradient)
+    outside the rectangle; one gather per fill."""
+
+    def __init__(self, nbx, nby, b, device):
+        import torch
+        X, Y = nbx * b, nby * b
+
+        def mirror(n):
+            return [2 - j for j in range(3)] + list(range(n)) + [n - 1 - j for j in range(3)]
+        mx, my = torch.tensor(mirror(X)), torch.tensor(mirror(Y))
+        src = []
+        for k in range(nbx * nby):
+            i0, j0 = (k // nby) * b, (k % nby) * b
+            gx = mx[i0:i0 + b + 6][:, None]
+            gy = my[j0:j0 + b + 6][None, :]
+            src.append(((gx // b) * nby + gy // b) * b * b + (gx % b) * b + gy % b)
+        self.src = torch.stack(src).reshape(-1).to(device)
+        self.nb, self.b = nbx * nby, b
+
+    def get_ghost_block_data(self, blk, info=None):
+        nf = blk.shape[1]
+        flat = blk.reshape(self.nb, nf, self.b * self.b).permute(1, 0, 2).reshape(nf, -1)
+        g = flat[:, self.src].reshape(nf, self.nb, self.b + 6, self.b + 6)
+        return g.permute(1, 0, 2, 3).contiguous()
+
+    def update_external_boundary(self, level, blk_data, interior, info=None):
+        return interior
+
+
+def amr_record(args, steps=10):
+    """Block-AMR step of the channel physics (set_simulator.py:496-532
+    AMR_Simulator through the drop-in mirror): one level of 64 x 16 blocks
+    of 20 x 20 cells (the block size of the reference's AMR example) over
+    1280 x 320 cells at the channel's spacing, float64 blocks, dt from CFL
+    0.05 of the initial state; the ghost fills of a device block layer
+    between the stages are inside the timed step (value), and the native
+    launches alone (3 jb_amr_stage + 1 jb_amr_chem) are timed apart."""
+    import numpy as np
+    import torch
+    from janc_b200 import mechanism as jm
+    from janc_b200.janc.simulation import set_simulator as ss
+    from janc_b200.janc.simulation import time_step as ts
+    from janc_b200.janc import _state
+    dev = torch.cuda.current_device()
+    nbx, nby, b = AMR_NBX, AMR_NBY, AMR_B
+    nx, ny = nbx * b, nby * b
+    d = LX / NX
+    P, T, Y = c1_fields(nx=nx, ny=ny)
+    mpath = jm.DEFAULT_MECHANISM
+    cfg = {"thermo_config": {"thermo_model": "nasa7", "mechanism_directory": mpath},
+           "reaction_config": {"is_detailed_chemistry": True, "mechanism_directory": mpath},
+           "flux_config": {"solver_type": "flux_splitting", "interface_reconstruction": "WENO5_JS",
+                           "split_method": "LF", "viscosity": "off"},
+           "boundary_config": BC_SLIP4, "time_config": {"temporal_evolution_scheme": "TVD_RK3", "dt": 1.0},
+           "precision": "fp64"}
+    layer = DeviceBlockLayer(nbx, nby, b, "cuda")
+    ts.set_amr_module(layer)
+    try:
+        adv_amr, _ = ss.AMR_Simulator(cfg)
+        s = _state.solver_for_amr()
+        from janc_b200.solver import Solver
+        s1 = Solver(2, nx, ny, d, d, BC_SLIP4, jm.load(), precision="fp64")
+        cu = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+        U0, a0 = s1.state_from_PTY(cu(P), cu(T), cu(Y))
+        dt = float(s1.cfl_dt(U0, a0, CFL))
+        grid = torch.cat([U0, a0], dim=0)
+        blk0 = grid.reshape(14, nbx, b, nby, b).permute(1, 3, 0, 2, 4).reshape(nbx * nby, 14, b, b).contiguous()
+        del s1
+
+        def step(blk):
+            return adv_amr(1, blk, d, d, dt, blk, None)
+        blk = blk0
+        for _ in range(max(args.warmup, 3)):
+            blk = step(blk)
+        blk = blk0
+        clocks = ClockSampler(dev)
+        clocks.start()
+        time.sleep(0.3)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            blk = step(blk)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        # the native launches alone, on fixed inputs
+        G = layer.get_ghost_block_data(blk0)
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        k0.record()
+        for _ in range(steps):
+            o1 = s.amr_stage(G, None, 1, d, d, dt)
+            o2 = s.amr_stage(G, G, 2, d, d, dt)
+            o3 = s.amr_stage(G, G, 3, d, d, dt)
+            s.amr_chem(blk0, dt)
+        k1.record()
+        torch.cuda.synchronize()
+        kms = k0.elapsed_time(k1) / steps
+        clk = clocks.stop()
+        fin = bool(torch.isfinite(blk).all())
+        st = s.status()
+        del o1, o2, o3
+    finally:
+        ts.set_amr_module(None)
+    cells = nx * ny
+    pc = (b + 6) ** 2 / b ** 2  # padded entries per interior cell
+    # each stage reads G (14 fields) and, in stages 2 and 3, U0 (12), and
+    # writes out (14) over the padded blocks; the chemistry reads and writes
+    # 14 fields of the unpadded blocks
+    kbytes = 8 * cells * (pc * (28 + 2 * 40) + 28)
+    return {"metric": METRIC, "value": job_value(1, cells, 1, ms), "unit": UNIT, "steps": steps,
+            "ms_per_step": ms, "precision": "fp64 (float64 blocks)",
+            "config": {"workload": "block AMR level: 64 x 16 blocks of 20 x 20 cells (1280 x 320) of the channel "
+                                   "physics at dx = 0.2 m / 1024, slip walls around the level, device block "
+                                   "layer (mirror outside the level), dt from CFL 0.05",
+                       "cells": cells, "blocks": nbx * nby, "block": [b, b]},
+            "kernel_ms_per_step": kms, "gpu_launches_per_step": 4,
+            "kernel_hbm_gbs": kbytes / (kms * 1e-3) / 1e9,
+            "kernel_bytes_note": "padded block arrays read / written once per stage, chemistry blocks once",
+            "finite": fin, "status_bits": st, "clocks": clk}
 
 
 # ------------------------------------------------------------- adjoint arm

@@ -16,27 +16,31 @@
 // blocks; the chemistry takes unpadded blocks [nb][nv + 2][bx][by].
 //
 // One CTA per block, so each block's reductions stay inside its CTA:
-//   k_amr_stage  alpha of the padded block; the interior in tiles of
-//                ATX x ATY cells (LF + WENO5-JS / MUSCL faces in shared
-//                memory, the RK combination); every ghost entry takes the
-//                combination with a zero right-hand side (the reference pads
-//                the rhs with zeros); update_aux over the whole padded block
-//                with the block's global stop: a first pass ORs the Halley
-//                residual masks, a second recomputes the iterates and takes
-//                the block's iteration count (no iterate buffer)
-//   k_amr_chem   point-implicit chemistry per cell, U + S, and update_aux
-//                over the block with its global stop (two passes as above)
+//   k_amr_stage   alpha of the padded block; the interior in tiles of
+//                 tx x ty cells, a shape the host picks per block size so
+//                 that few, well-filled tiles cover the block (LF + WENO5-JS
+//                 / MUSCL faces in shared memory, the RK combination); every
+//                 ghost entry takes the combination with a zero right-hand
+//                 side (the reference pads the rhs with zeros); update_aux
+//                 over the whole padded block
+//   k_amr_update  update_aux of blocks alone
+// update_aux runs the reference's loop in lockstep over the block: one
+// Halley iteration of every cell per round, the block's OR of "residual
+// above tol" / "residual NaN" deciding whether another round follows (the
+// iterates live in the output's gamma / T slots), so a cell is evaluated
+// once per iteration the block takes.
+//   k_amr_chem    point-implicit chemistry, one thread per cell of all
+//                 blocks, U + S; k_amr_update then solves the temperatures
 
 namespace {  // internal linkage
 
 constexpr int AMR_NT = 256;
-constexpr int ATX = 15, ATY = 16;  // interior tile: 16 x 16 x faces for 256 threads
-constexpr int APX = ATX + 6, APY = ATY + 6, AQ = APX * APY;
-constexpr int A_HX = APX * ATY, A_HY = ATX * APY, A_FX = (ATX + 1) * ATY, A_FY = ATX * (ATY + 1);
-constexpr size_t AMR_STAGE_SMEM = sizeof(double) * (14 * AQ + 4 * AQ + 2 * A_HX + 2 * A_HY + A_FX + A_FY);
+constexpr int AMR_AQ_MAX = 640;  // padded cells of a tile, (tx + 6)(ty + 6)
+constexpr int AMR_H_MAX = 420;   // (tx + 6) ty and tx (ty + 6) when (tx + 1) ty, tx (ty + 1) <= 256
+constexpr size_t AMR_STAGE_SMEM = sizeof(double) * (4 * AMR_AQ_MAX + 4 * AMR_H_MAX + 2 * AMR_NT);
 
 struct AmrBlocks {
-  int nb, bx, by, padded;  // padded: the arrays carry the 3-cell ghost layers
+  int nb, bx, by, tx, ty;  // blocks, block cells, interior tile of k_amr_stage
   double dx, dy, idx, idy;
 };
 
@@ -91,24 +95,39 @@ __device__ __forceinline__ void amr_eYR(const MP& m, const double* Ub, long long
 }
 
 // update_aux of the nc cells of one block (state Ub, initial temperatures
-// T0b, result into Ab = [gamma][T]) with the block's global stop.
+// T0b, result into Ab = [gamma][T]) with the block's global stop
+// (thermo_model.py:135-153 on the vmapped block): round i evaluates the
+// residual at every cell's i-th iterate; the loop ends when no residual
+// exceeds tol, when one is NaN (jnp.max is then NaN and the test false) or
+// after 5 iterations.  T0b may equal Ab + nc.
 __device__ void amr_update_block(const MP& m, const double* Ub, const double* T0b, double* Ab, long long nc,
                                  unsigned& st) {
-  unsigned bits = 0;
-  for (long long c = threadIdx.x; c < nc; c += blockDim.x) {
-    double e, Yf[NS], R, cnd[JB_NCAND];
-    amr_eYR(m, Ub, nc, c, e, Yf, R);
-    bits |= halley_any(m, e, Yf, R, T0b[c], cnd);
+  double* Tn = Ab;       // each cell's next iterate (the gamma slot until the end)
+  double* Tc = Ab + nc;  // its current iterate
+  for (long long c = threadIdx.x; c < nc; c += blockDim.x) Tc[c] = T0b[c];
+  for (int i = 0;; ++i) {
+    unsigned bits = 0;
+    for (long long c = threadIdx.x; c < nc; c += blockDim.x) {
+      double e, Yf[NS], R;
+      amr_eYR(m, Ub, nc, c, e, Yf, R);
+      const double T = Tc[c];
+      const Th t = thermo_mix(m, T, Yf);
+      const double res = (t.h - R * T) - e;
+      const double d1 = t.cp - R, d2 = t.dcp;
+      if (fabs(res) > HALLEY_TOL) bits |= 1u;
+      if (res != res) bits |= 2u;
+      Tn[c] = T + ((-2.0 * res) * d1) / ((2.0 * (d1 * d1)) - res * d2);
+    }
+    bits = amr_block_or(bits);
+    if (!(bits & 1u) || (bits & 2u) || i == HALLEY_MAX) break;
+    for (long long c = threadIdx.x; c < nc; c += blockDim.x) Tc[c] = Tn[c];
   }
-  const int n = halley_count(amr_block_or(bits));
   for (long long c = threadIdx.x; c < nc; c += blockDim.x) {
-    double e, Yf[NS], R, cnd[JB_NCAND];
+    double e, Yf[NS], R;
     amr_eYR(m, Ub, nc, c, e, Yf, R);
-    halley_any(m, e, Yf, R, T0b[c], cnd);
-    const double T = cnd[n];
+    const double T = Tc[c];
     const double cp = cp_mix(m, T, Yf);
     Ab[c] = cp / (cp - R);
-    Ab[nc + c] = T;
     if (!(T == T)) st |= JB_ERR_NONFINITE;
   }
 }
@@ -125,14 +144,15 @@ __global__ void __launch_bounds__(AMR_NT) k_amr_stage(MP m, Grid g, AmrBlocks B,
                                                     double dt) {
   extern __shared__ __align__(128) unsigned char smraw[];
   constexpr int nv = 12;
-  double* sQ = reinterpret_cast<double*>(smraw);  // [14][APX][APY]: U, gamma, T
-  double* sP = sQ + 14 * AQ;                       // [4][APX][APY]: rho, u, v, p
-  double* sHxp = sP + 4 * AQ;                      // [APX][ATY]
-  double* sHxm = sHxp + A_HX;
-  double* sHyp = sHxm + A_HX;                      // [ATX][APY]
-  double* sHym = sHyp + A_HY;
-  double* sFx = sHym + A_HY;                       // [ATX+1][ATY]
-  double* sFy = sFx + A_FX;                        // [ATX][ATY+1]
+  const int TX = B.tx, TY = B.ty, APX = TX + 6, APY = TY + 6, AQ = APX * APY;
+  const int HX = APX * TY, HY = TX * APY;
+  double* sP = reinterpret_cast<double*>(smraw);  // [4][APX][APY]: rho, u, v, p
+  double* sHxp = sP + 4 * AQ;                      // [APX][TY]
+  double* sHxm = sHxp + HX;
+  double* sHyp = sHxm + HX;                        // [TX][APY]
+  double* sHym = sHyp + HY;
+  double* sFx = sHym + HY;                         // [TX+1][TY]
+  double* sFy = sFx + (TX + 1) * TY;               // [TX][TY+1]
   const int tid = threadIdx.x;
   const int PX = B.bx + 6, PY = B.by + 6;
   const long long nc = (long long)PX * PY;
@@ -142,8 +162,6 @@ __global__ void __launch_bounds__(AMR_NT) k_amr_stage(MP m, Grid g, AmrBlocks B,
   const double* u0 = STAGE >= 2 ? io.u0 + b * io.u0s : nullptr;
   double* oU = io.oU + b * io.osU;
   unsigned st = 0;
-  // field q of padded cell c of the stage input (q < nv: U, nv: gamma, nv + 1: T)
-  auto gq = [&](int q, long long c) { return q < nv ? gU[q * nc + c] : gA[(q - nv) * nc + c]; };
 
   // ---- LF wave speeds: nanmax(|u| + a), nanmax(|v| + a) over the padded
   // block (flux_splitting/LF.py:11-12 on the vmapped block)
@@ -159,31 +177,24 @@ __global__ void __launch_bounds__(AMR_NT) k_amr_stage(MP m, Grid g, AmrBlocks B,
   amr_block_max2(ax, ay);
 
   // ---- the interior, tile by tile
-  const bool owner = tid < ATX * ATY;
-  const int ix = owner ? tid / ATY : 0, iy = owner ? tid % ATY : 0;
-  const int ntx = (B.bx + ATX - 1) / ATX, nty = (B.by + ATY - 1) / ATY;
+  const bool owner = tid < TX * TY;
+  const int ix = owner ? tid / TY : 0, iy = owner ? tid % TY : 0;
+  const int ntx = (B.bx + TX - 1) / TX, nty = (B.by + TY - 1) / TY;
   for (int t = 0; t < ntx * nty; ++t) {
-    const int x0 = (t / nty) * ATX, y0 = (t % nty) * ATY;  // interior coordinates of the tile
-    // padded tile: block padded rows x0 .. x0 + APX - 1, columns y0 .. y0 + APY - 1
+    const int x0 = (t / nty) * TX, y0 = (t % nty) * TY;  // interior coordinates of the tile
+    // primitives of the padded tile (block padded rows x0 .. x0 + APX - 1,
+    // columns y0 .. y0 + APY - 1); cells beyond the padded block are read
+    // only by faces of cells outside the block
     for (int i = tid; i < AQ; i += AMR_NT) {
       const int px = x0 + i / APY, py = y0 + i % APY;
+      double rho = 1.0, u = 1.0, v = 1.0, p = 1.0;
       if (px < PX && py < PY) {
         const long long c = (long long)px * PY + py;
+        double q[nv];
 #pragma unroll
-        for (int q = 0; q < 14; ++q) sQ[q * AQ + i] = gq(q, c);
-      } else {
-        // beyond the padded block: read only by faces of cells outside the block
-#pragma unroll
-        for (int q = 0; q < 14; ++q) sQ[q * AQ + i] = 1.0;
+        for (int f = 0; f < nv; ++f) q[f] = gU[f * nc + c];
+        flux_prims<2>(m, q, gA[nc + c], rho, u, v, p);
       }
-    }
-    __syncthreads();
-    for (int i = tid; i < AQ; i += AMR_NT) {
-      double q[nv];
-#pragma unroll
-      for (int f = 0; f < nv; ++f) q[f] = sQ[f * AQ + i];
-      double rho, u, v, p;
-      flux_prims<2>(m, q, sQ[13 * AQ + i], rho, u, v, p);
       sP[i] = rho;
       sP[AQ + i] = u;
       sP[2 * AQ + i] = v;
@@ -195,49 +206,53 @@ __global__ void __launch_bounds__(AMR_NT) k_amr_stage(MP m, Grid g, AmrBlocks B,
     const long long cell = (long long)(gx + 3) * PY + (gy + 3);
     for (int f = 0; f < nv; ++f) {
       // split fluxes H+- = 0.5 (F +- alpha U) (flux_splitting/LF.py:4-16)
-      for (int i = tid; i < A_HX + A_HY; i += AMR_NT) {
+      for (int i = tid; i < HX + HY; i += AMR_NT) {
         int px, py, dir;
-        if (i < A_HX) { px = i / ATY; py = i % ATY + 3; dir = 0; }
-        else { const int j = i - A_HX; px = j / APY + 3; py = j % APY; dir = 1; }
+        if (i < HX) { px = i / TY; py = i % TY + 3; dir = 0; }
+        else { const int j = i - HX; px = j / APY + 3; py = j % APY; dir = 1; }
         const int c = px * APY + py;
-        const double qf = sQ[f * AQ + c];
-        const double F = lf_flux<2>(f, dir, qf, sP[c], sP[AQ + c], sP[2 * AQ + c], sP[3 * AQ + c], sQ[3 * AQ + c]);
+        const int bxp = x0 + px, byp = y0 + py;
+        const long long gc = (long long)bxp * PY + byp;
+        const bool in = bxp < PX && byp < PY;
+        const double qf = in ? gU[f * nc + gc] : 1.0;
+        const double E = in ? gU[3 * nc + gc] : 1.0;
+        const double F = lf_flux<2>(f, dir, qf, sP[c], sP[AQ + c], sP[2 * AQ + c], sP[3 * AQ + c], E);
         const double al = dir == 0 ? ax : ay;
         const double hp = 0.5 * (F + al * qf), hm = 0.5 * (F - al * qf);
-        if (dir == 0) { sHxp[px * ATY + (py - 3)] = hp; sHxm[px * ATY + (py - 3)] = hm; }
+        if (dir == 0) { sHxp[px * TY + (py - 3)] = hp; sHxm[px * TY + (py - 3)] = hm; }
         else { sHyp[(px - 3) * APY + py] = hp; sHym[(px - 3) * APY + py] = hm; }
       }
       __syncthreads();
       // face values F = L(H+) + R(H-) (flux.py:56-68, WENO5_JS.py / MUSCL.py)
-      {
-        const int mxf = tid / ATY, jy = tid % ATY;  // x faces: (ATX + 1) x ATY = 256
+      if (tid < (TX + 1) * TY) {
+        const int mxf = tid / TY, jy = tid % TY;
         const double* hp = sHxp + jy;
         const double* hm = sHxm + jy;
-        const double L = recon_L(g, hp[mxf * ATY], hp[(mxf + 1) * ATY], hp[(mxf + 2) * ATY], hp[(mxf + 3) * ATY],
-                                 hp[(mxf + 4) * ATY]);
-        const double Rr = recon_R(g, hm[(mxf + 1) * ATY], hm[(mxf + 2) * ATY], hm[(mxf + 3) * ATY],
-                                  hm[(mxf + 4) * ATY], hm[(mxf + 5) * ATY]);
-        sFx[mxf * ATY + jy] = L + Rr;
-        if (tid < A_FY) {
-          const int jx = tid / (ATY + 1), myf = tid % (ATY + 1);
-          const double* gp = sHyp + jx * APY + myf;
-          const double* gm = sHym + jx * APY + myf;
-          const double Lg = recon_L(g, gp[0], gp[1], gp[2], gp[3], gp[4]);
-          const double Rg = recon_R(g, gm[1], gm[2], gm[3], gm[4], gm[5]);
-          sFy[jx * (ATY + 1) + myf] = Lg + Rg;
-        }
+        const double L = recon_L(g, hp[mxf * TY], hp[(mxf + 1) * TY], hp[(mxf + 2) * TY], hp[(mxf + 3) * TY],
+                                 hp[(mxf + 4) * TY]);
+        const double Rr = recon_R(g, hm[(mxf + 1) * TY], hm[(mxf + 2) * TY], hm[(mxf + 3) * TY],
+                                  hm[(mxf + 4) * TY], hm[(mxf + 5) * TY]);
+        sFx[mxf * TY + jy] = L + Rr;
+      }
+      if (tid < TX * (TY + 1)) {
+        const int jx = tid / (TY + 1), myf = tid % (TY + 1);
+        const double* gp = sHyp + jx * APY + myf;
+        const double* gm = sHym + jx * APY + myf;
+        const double Lg = recon_L(g, gp[0], gp[1], gp[2], gp[3], gp[4]);
+        const double Rg = recon_R(g, gm[1], gm[2], gm[3], gm[4], gm[5]);
+        sFy[jx * (TY + 1) + myf] = Lg + Rg;
       }
       __syncthreads();
       // divergence and the RK combination (TVD_RK3.py:17, 24, 31)
       if (live) {
-        const double dF = sFx[(ix + 1) * ATY + iy] - sFx[ix * ATY + iy];
-        const double dG = sFy[ix * (ATY + 1) + iy + 1] - sFy[ix * (ATY + 1) + iy];
+        const double dF = sFx[(ix + 1) * TY + iy] - sFx[ix * TY + iy];
+        const double dG = sFy[ix * (TY + 1) + iy + 1] - sFy[ix * (TY + 1) + iy];
 #if JB_FAST
         const double rhs = dt * (-(dF * B.idx + dG * B.idy));
 #else
         const double rhs = dt * (-(dF / B.dx + dG / B.dy));
 #endif
-        const double uk = sQ[f * AQ + (ix + 3) * APY + (iy + 3)];
+        const double uk = gU[f * nc + cell];
         double r;
         if (STAGE == 0) r = rhs;
         else if (STAGE == 1) r = uk + rhs;
@@ -273,31 +288,35 @@ __global__ void __launch_bounds__(AMR_NT) k_amr_stage(MP m, Grid g, AmrBlocks B,
 }
 
 // update_aux of every block (vmap(update_aux), set_simulator.py:41) with
-// each block's own stop: U [nb][nv][X][Y], aux_in / aux_out [nb][2][X][Y].
+// each block's own stop: U [nb][nv][X][Y] (field stride nc, block stride
+// su), aux_in / aux_out [nb][2][X][Y] (block stride sa).
 template <int UNUSED>
-__global__ void __launch_bounds__(AMR_NT) k_amr_update(MP m, long long nc, const double* __restrict__ U,
-                                                     const double* __restrict__ aux_in, double* __restrict__ aux_out,
+__global__ void __launch_bounds__(AMR_NT) k_amr_update(MP m, long long nc, const double* U, long long su,
+                                                     const double* aux_in, double* aux_out, long long sa,
                                                      Slots* slots) {
   const long long b = blockIdx.x;
   unsigned st = 0;
-  amr_update_block(m, U + b * 12 * nc, aux_in + b * 2 * nc + nc, aux_out + b * 2 * nc, nc, st);
+  amr_update_block(m, U + b * su, aux_in + b * sa + nc, aux_out + b * sa, nc, st);
   st = amr_block_or(st);
   if (threadIdx.x == 0 && st) atomicOr(&slots->status, st);
 }
 
-// Chemistry of every unpadded block (set_simulator.py:106-113):
-// out = U + S(U, T, dt) and update_aux of the block started from its T.
+// Chemistry of every cell of nb unpadded blocks (the vmapped
+// reaction_source_terms of set_simulator.py:109-111): out = U + S(U, T, dt),
+// the flow fields copied; one thread per cell.  out may equal blk.
 // GEN: the specialised chemistry (CHEM_SH shared doubles per thread).
 template <bool GEN>
-__global__ void __launch_bounds__(128) k_amr_chem(MP m, AmrBlocks B, const double* __restrict__ blk,
-                                                  double* __restrict__ out, Slots* slots, double dt) {
+__global__ void __launch_bounds__(128, 3) k_amr_chem(MP m, AmrBlocks B, const double* blk, double* out,
+                                                     Slots* slots, double dt) {
   extern __shared__ double shc[];
   constexpr int nY = 4, nv = 12;
   const long long nc = (long long)B.bx * B.by;
-  const double* Ib = blk + (long long)blockIdx.x * (nv + 2) * nc;
-  double* Ob = out + (long long)blockIdx.x * (nv + 2) * nc;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned st = 0;
-  for (long long c = threadIdx.x; c < nc; c += blockDim.x) {
+  if (i < nc * B.nb) {
+    const long long b = i / nc, c = i % nc;
+    const double* Ib = blk + b * (nv + 2) * nc;
+    double* Ob = out + b * (nv + 2) * nc;
     const double T = Ib[(nv + 1) * nc + c];
     const double rho = Ib[c];
     double Y8[NR], S[NR];
@@ -314,10 +333,7 @@ __global__ void __launch_bounds__(128) k_amr_chem(MP m, AmrBlocks B, const doubl
 #pragma unroll
     for (int k = 0; k < NR; ++k) Ob[(nY + k) * nc + c] = Ib[(nY + k) * nc + c] + S[k];
   }
-  __syncthreads();
-  amr_update_block(m, Ob, Ib + (nv + 1) * nc, Ob + nv * nc, nc, st);
-  st = amr_block_or(st);
-  if (threadIdx.x == 0 && st) atomicOr(&slots->status, st);
+  block_reduce_store(0.0, 0.0, 0.0, st << 16, slots, 0, false, false, -1);
 }
 
 }  // namespace
