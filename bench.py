@@ -913,14 +913,24 @@ def adjoint_record(args, dist, ws, N):
     dts2, pps2 = probe_trajectory(traj, Pc, Tg2, Yc, None, N)
     (dts2 * pps2).sum().backward()
     gTz = Tg2.grad.cpu().numpy()
-    noised = []
+    # the central difference at h and at 10 h: in a direction whose
+    # derivative is small against the others the h = 1e-6 difference is
+    # dominated by the forward's round-off (its error grows as 1/h), which
+    # the 10 h column shows
+    noised, noised10, adj_n, err_abs = [], [], [], []
     rng_n = np.random.default_rng(7)
     for _ in range(nd):
         d = rng_n.standard_normal(T.shape)
         d /= np.linalg.norm(d)
         f = (loss_at(cu(Tz * (1 + h * d)), None) - loss_at(cu(Tz * (1 - h * d)), None)) / (2 * h)
+        h10 = 10 * h
+        f10 = (loss_at(cu(Tz * (1 + h10 * d)), None) - loss_at(cu(Tz * (1 - h10 * d)), None)) / (2 * h10)
         a = float((gTz * Tz * d).sum())
         noised.append(abs(f - a) / max(abs(f), 1e-300))
+        noised10.append(abs(f10 - a) / max(abs(f10), 1e-300))
+        adj_n.append(abs(a))
+        err_abs.append(abs(f - a))
+    scale = statistics.median(adj_n)
     cells = nx * ny
     fd_sum = {k: {"directions": len(v), "max_rel_err": max(v), "median_rel_err": statistics.median(v)}
               for k, v in fd.items() if v}
@@ -945,6 +955,10 @@ def adjoint_record(args, dist, ws, N):
                                     "T_full_field_noised_ambient": {
                                         "directions": len(noised), "max_rel_err": max(noised),
                                         "median_rel_err": statistics.median(noised),
+                                        "max_rel_err_h1e-5": max(noised10),
+                                        "median_rel_err_h1e-5": statistics.median(noised10),
+                                        "max_err_over_median_directional_derivative": max(err_abs) / scale,
+                                        "min_over_median_directional_derivative": min(adj_n) / scale,
                                         "state": "the same workload with 1 % seeded noise (default_rng(6)) on "
                                                  "the ambient temperature"},
                                     "T_full_field_h_sweep": sweep,
