@@ -275,15 +275,16 @@ int jb_probe_fp64_fma(int blocks, int iters, double* scratch, void* stream);
 const char* jb_last_error(const jb_handle* h);
 
 /* ------------------------------------------------------------------------
- * Reverse mode (the adjoint), 2D grids with periodic, slip, no-slip,
+ * Reverse mode (the adjoint), 2D and 1D grids with periodic, slip, no-slip,
  * zero-gradient or pressure-outlet sides (back pressure Pb held fixed).
  * The reference gets these derivatives from jax.grad
  * through advance_one_step and the CFL time step (set_simulator.py:117-122,
- * 420-447) with get_T's custom VJP (src/janc_v2/model/thermo_model.py:
- * 155-190); these calls compute the same vector-Jacobian products with
- * hand-written kernels.
+ * 420-447; 1D: CFL min dx / (|u| + a)) with get_T's custom VJP
+ * (src/janc_v2/model/thermo_model.py:155-190); these calls compute the same
+ * vector-Jacobian products with hand-written kernels.
  * ------------------------------------------------------------------------ */
-/* Pressure probe: mean p over the wx x wy cells from (x0, y0). */
+/* Pressure probe: mean p over the wx x wy cells from (x0, y0) (1D: y0 = 0,
+ * wy = 1). */
 int jb_set_probe(jb_handle* h, int x0, int y0, int wx, int wy);
 /* Scale every pre-exponential factor A_i of the handle's mechanism by
  * exp(offset[i]) relative to the tables given to jb_create (NULL restores

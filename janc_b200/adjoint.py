@@ -1,4 +1,4 @@
-"""Reverse mode of the 2D reacting step behind ``torch.autograd``.
+"""Reverse mode of the reacting step (2D and 1D) behind ``torch.autograd``.
 
 The reference obtains gradients with ``jax.grad`` through its step
 (src/janc_v2/simulation/set_simulator.py:117-122), its CFL time step
@@ -14,6 +14,8 @@ state (the only states kept by the forward pass).
     dts, pps = probe_trajectory(traj, P, T, Y, lnA, nsteps=200)
     loss = (dts * pps).sum()        # time-integrated probe pressure
     loss.backward()                 # T.grad, lnA.grad
+
+A 1D solver takes the probe as (x0, wx) (cells x0 .. x0 + wx - 1).
 """
 import ctypes
 
@@ -33,14 +35,18 @@ def _off(t, n):
 
 
 class Trajectory:
-    """A configured 2D float64 solver plus the loss probe and checkpointing."""
+    """A configured float64 solver (2D or 1D) plus the loss probe and
+    checkpointing."""
 
     def __init__(self, solver, cfl, probe, checkpoint=20):
-        if not isinstance(solver, Solver) or solver.dim != 2 or solver.precision == "mixed":
-            raise ValueError("the adjoint runs on a 2D float64 Solver")
+        if not isinstance(solver, Solver) or solver.precision == "mixed":
+            raise ValueError("the adjoint runs on a float64 Solver")
         self.s = solver
         self.cfl = float(cfl)
-        self.probe = tuple(int(v) for v in probe)
+        probe = tuple(int(v) for v in probe)
+        if solver.dim == 1 and len(probe) == 2:
+            probe = (probe[0], 0, probe[1], 1)
+        self.probe = probe
         self.K = int(checkpoint)
         L = solver._lib
         _native.check(L.jb_set_probe(solver._h, *self.probe), solver._h, "jb_set_probe")

@@ -1,9 +1,11 @@
-// Hand-written reverse-mode kernels of the 2D reacting step (the adjoint).
+// Hand-written reverse-mode kernels of the reacting step (the adjoint), 2D
+// and 1D (every kernel is a template on DIM; 1D has no y direction, the
+// energy at field 2 and the species from field 3).
 //
 // The forward step being differentiated is the reference's advance_one_step
 // (set_simulator.py:117-122) with its CFL time step (set_simulator.py:
 // 420-447):
-//   dt = CFL min 1/(sx/dx + sy/dy)         over (U, aux)
+//   dt = CFL min 1/(sx/dx + sy/dy)  (2D),  CFL min dx/sx  (1D)   over (U, aux)
 //   U1 = U  + dt L(U,  aux;  a1)           aux1 = update_aux(U1)
 //   U2 = 3/4 U + 1/4 (U1 + dt L(U1, aux1; a2))   aux2 = update_aux(U2)
 //   U3 = 1/3 U + 2/3 (U2 + dt L(U2, aux2; a3))   aux3 = update_aux(U3)
@@ -42,6 +44,12 @@ namespace jb {
 namespace adj {
 
 constexpr double TIE_REL = 1e-13;
+
+// field layout of a DIM-D state: species from NYD, energy at EI, NVD fields
+template <int DIM>
+struct Lay {
+  static constexpr int NY = DIM == 1 ? 3 : 4, EI = NY - 1, NV = NY + NR;
+};
 
 template <int N>
 __device__ __forceinline__ void poly_d(const double* c, double T, double& p, double& dp) {
@@ -92,31 +100,35 @@ __device__ __forceinline__ void t_bwd(const MP& m, double T, const double* Yf, T
   }
 }
 
-// Mass fractions of a 2D cell.
+// Mass fractions of a cell.
+template <int DIM>
 __device__ __forceinline__ void cell_Y(const double* q, double ri, double* Y8, double* Yf) {
 #pragma unroll
-  for (int k = 0; k < NR; ++k) Y8[k] = q[4 + k] * ri;
+  for (int k = 0; k < NR; ++k) Y8[k] = q[Lay<DIM>::NY + k] * ri;
   fill_Y(Y8, Yf);
 }
 
-// ub += d(gamma, T)/dq^T (gb, Tb) for aux = update_aux(q) (solver_2D/aux_func.py:21-29)
+// ub += d(gamma, T)/dq^T (gb, Tb) for aux = update_aux(q)
+// (solver_2D/aux_func.py:21-29, solver_1D/aux_func.py:21-28)
+template <int DIM>
 __device__ __forceinline__ void upd_vjp(const MP& m, const double* q, double T, double gb, double Tb, double* ub) {
+  constexpr int NY = Lay<DIM>::NY, EI = Lay<DIM>::EI;
   if (gb == 0.0 && Tb == 0.0) return;
   const double rho = q[0], ri = 1.0 / rho;
-  const double u = q[1] * ri, v = q[2] * ri;
+  const double u = q[1] * ri, v = DIM == 2 ? q[2] * ri : 0.0;
   double Y8[NR], Yf[NS];
-  cell_Y(q, ri, Y8, Yf);
+  cell_Y<DIM>(q, ri, Y8, Yf);
   TBwd b;
   t_bwd(m, T, Yf, b);
   const double eb = gb * b.dg_de + Tb * b.dT_de;
-  double rb = eb * (-q[3] * ri * ri + (u * u + v * v) * ri);
+  double rb = eb * (-q[EI] * ri * ri + (u * u + v * v) * ri);
   ub[1] += eb * (-u * ri);
-  ub[2] += eb * (-v * ri);
-  ub[3] += eb * ri;
+  if (DIM == 2) ub[2] += eb * (-v * ri);
+  ub[EI] += eb * ri;
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
     const double yb = gb * b.dg_dY[k] + Tb * b.dT_dY[k];
-    ub[4 + k] += yb * ri;
+    ub[NY + k] += yb * ri;
     rb -= yb * Y8[k] * ri;
   }
   ub[0] += rb;
@@ -124,12 +136,14 @@ __device__ __forceinline__ void upd_vjp(const MP& m, const double* q, double T, 
 
 // Adjoint of s = |u_dir| + a, a = sqrt(gamma p / rho), p = rho R T, with
 // weight w: ub, gb, Tb accumulate.
+template <int DIM>
 __device__ __forceinline__ void speed_vjp(const MP& m, const double* q, double gamma, double T, int dir, double w,
                                           double* ub, double& gb, double& Tb) {
+  constexpr int NY = Lay<DIM>::NY;
   if (w == 0.0) return;
   const double rho = q[0], ri = 1.0 / rho;
   double Y8[NR], Yf[NS];
-  cell_Y(q, ri, Y8, Yf);
+  cell_Y<DIM>(q, ri, Y8, Yf);
   const double R = get_R(m, Yf);
   const double p = rho * R * T;
   const double a = sqrt(gamma * p / rho);
@@ -146,7 +160,7 @@ __device__ __forceinline__ void speed_vjp(const MP& m, const double* q, double g
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
     const double yb = Rb * (m.invM[k] - m.invM[NR]);
-    ub[4 + k] += yb * ri;
+    ub[NY + k] += yb * ri;
     rb -= yb * Y8[k] * ri;
   }
   ub[0] += rb;
@@ -286,9 +300,11 @@ constexpr int CHEM_ADJ_SH = 3 * NREAC;  // kf, kb, M per reaction
 // chemistry's temperature adjoint; dt and ln A adjoints are reduced into
 // dtb and lnAb.  Rates in log space: kf = exp(ln A + B ln T - Ea/T +
 // sum vf ln X), kb = exp(ln kf0 - sum dv g - vsum ln(pref/T) + sum vb ln X).
+template <int DIM>
 __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
     k_chem_vjp(MP m, Grid g, const double* __restrict__ U3, const double* __restrict__ A3, const double* Ub4,
                double* Ub3, const double* __restrict__ slot_dt, double* dtb, double* lnAb) {
+  constexpr int NY = Lay<DIM>::NY, NVD = Lay<DIM>::NV;
   extern __shared__ double shk[];
   const long long nc = g.ncell;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -300,13 +316,13 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
 #pragma unroll 1
   for (int i = 0; i < NREAC; ++i) sA[i * NT] = 0.0;
   if (c < nc) {
-    double q[12];
+    double q[NVD];
 #pragma unroll
-    for (int f = 0; f < 12; ++f) q[f] = U3[f * nc + c];
+    for (int f = 0; f < NVD; ++f) q[f] = U3[f * nc + c];
     const double T = A3[nc + c];
     const double rho = q[0], ri = 1.0 / rho;
     double Y8[NR], Yf[NS], X[NS], Xc[NR], lnXc[NR], iXc[NR], gg[NR], dg[NR];
-    cell_Y(q, ri, Y8, Yf);
+    cell_Y<DIM>(q, ri, Y8, Yf);
 #pragma unroll
     for (int j = 0; j < NS; ++j) X[j] = rho * Yf[j] * m.invM[j];
 #pragma unroll
@@ -383,7 +399,7 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
     double rb = 0.0, Y8b[NR], xb[NR];
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
-      const double Sb = Ub4[(4 + k) * nc + c];
+      const double Sb = Ub4[(NY + k) * nc + c];
       const double dY = x[k] * ri;
       const double lo = -Y8[k], hi = 1.0 - Y8[k];
       const double m1 = dY < lo ? lo : dY;
@@ -456,19 +472,19 @@ __global__ void __launch_bounds__(CHEM_ADJ_NT, 2)
       rb += ryb * Yf[j];
       Yfb[j] = rho * ryb;
     }
-    double ub[12];
+    double ub[NVD];
 #pragma unroll
-    for (int f = 0; f < 12; ++f) ub[f] = Ub4[f * nc + c];
+    for (int f = 0; f < NVD; ++f) ub[f] = Ub4[f * nc + c];
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
       const double yb = Y8b[k] + Yfb[k] - Yfb[NR];
-      ub[4 + k] += yb * ri;
+      ub[NY + k] += yb * ri;
       rb -= yb * Y8[k] * ri;
     }
     ub[0] += rb;
-    upd_vjp(m, q, T, 0.0, Tb, ub);
+    upd_vjp<DIM>(m, q, T, 0.0, Tb, ub);
 #pragma unroll
-    for (int f = 0; f < 12; ++f) Ub3[f * nc + c] = ub[f];
+    for (int f = 0; f < NVD; ++f) Ub3[f * nc + c] = ub[f];
   }
   block_add(dtb_loc, dtb);
 #pragma unroll 1
@@ -517,11 +533,13 @@ struct Speeds {
   double sx, sy, d;
 };
 
-__device__ __forceinline__ Speeds speeds_of(const Grid& g, const Prim<2>& pr) {
+// wave speeds and the CFL candidate: 1 / (sx/dx + sy/dy) in 2D, dx / sx in 1D
+template <int DIM>
+__device__ __forceinline__ Speeds speeds_of(const Grid& g, const Prim<DIM>& pr) {
   Speeds s;
   s.sx = fabs(pr.u) + pr.a;
   s.sy = fabs(pr.v) + pr.a;
-  s.d = 1.0 / (s.sx / g.dx + s.sy / g.dy);
+  s.d = DIM == 1 ? g.dx / s.sx : 1.0 / (s.sx / g.dx + s.sy / g.dy);
   return s;
 }
 
@@ -535,9 +553,9 @@ __device__ __forceinline__ bool tied(double v, double ref) { return fabs(v - ref
 // read them (og), the alpha maxima see their wave speeds (3 entries per
 // boundary position), and their adjoints (flux, LF term, wave speeds) flow
 // back into the boundary cell through the VJP of the outlet state (ogb).
-//   og [stage][side][OG_F][lstrip]: ghost U (12), u, v, p
-//   ogb[side][OG_B][lstrip]: the boundary cell's U adjoint (12), T adjoint
-constexpr int OG_F = 15, OG_B = 13;
+//   og [stage][side][OG_F][lstrip]: ghost U (nv), then u, v, p at OG_U..OG_P
+//   ogb[side][OG_B][lstrip]: the boundary cell's U adjoint (nv), T adjoint at OG_T
+constexpr int OG_F = 15, OG_B = 13, OG_U = 12, OG_V = 13, OG_P = 14, OG_T = 12;
 
 __device__ __forceinline__ size_t og_idx(const Grid& g, int stage, int side, int f, int pos) {
   return (((size_t)stage * 4 + side) * OG_F + f) * g.lstrip + pos;
@@ -549,13 +567,15 @@ __device__ __forceinline__ bool outlet_side(const Grid& g, int side) {
 
 // Boundary position t in [0, 2 ny + 2 nx): sides 0 and 1 (x = 0, nx - 1) by
 // y, then sides 2 and 3 (y = 0, ny - 1) by x; side -1 past the end.
+// In 1D only sides 0 and 1 (t = 0, 1).
+template <int DIM>
 __device__ __forceinline__ void boundary_pos(const Grid& g, int t, int& side, int& pos, int& x, int& y) {
   side = -1;
   pos = 0;
   if (t < 2 * g.ny) {
     side = t / g.ny;
     pos = t % g.ny;
-  } else if (t < 2 * g.ny + 2 * g.nx) {
+  } else if (DIM == 2 && t < 2 * g.ny + 2 * g.nx) {
     side = 2 + (t - 2 * g.ny) / g.nx;
     pos = (t - 2 * g.ny) % g.nx;
   }
@@ -576,12 +596,14 @@ __device__ __forceinline__ double outlet_un(const double* q, int side) {
 // switch.  Subsonic: rho_c = Pb / (p / rho), p_c = Pb, T_c = p_c / (rho_c R);
 // supersonic: the cell's rho, p, T.  Both: the ghost energy rho_c h(T_c) -
 // p_c + rho_c |u|^2 / 2 and gamma_c = cp(T_c) / (cp(T_c) - R).
+template <int DIM>
 __device__ void outlet_vjp(const MP& m, const double* q, double gamma, double T, double un, double Pb,
                            const double* ob, double gcb, double Tcb, double* ub, double& Tb) {
+  constexpr int NY = Lay<DIM>::NY, EI = Lay<DIM>::EI;
   const double rho = q[0], ri = 1.0 / rho;
-  const double u = q[1] * ri, v = q[2] * ri;
+  const double u = q[1] * ri, v = DIM == 2 ? q[2] * ri : 0.0;
   double Y8[NR], Yf[NS];
-  cell_Y(q, ri, Y8, Yf);
+  cell_Y<DIM>(q, ri, Y8, Yf);
   const double R = get_R(m, Yf);
   const double p = rho * (R * T);
   const double a = sqrt(gamma * p / rho);
@@ -601,17 +623,18 @@ __device__ void outlet_vjp(const MP& m, const double* q, double gamma, double T,
     h += hi[k] * Yf[k];
   }
   const double cv = cp - R, icv2 = 1.0 / (cv * cv);
-  // ghost = [rho_c, rho_c u, rho_c v, rho_c h - p_c + rho_c ke, rho_c Y8]
+  // ghost = [rho_c, rho_c u, (rho_c v,) rho_c h - p_c + rho_c ke, rho_c Y8]
   const double ke = 0.5 * (u * u + v * v);
-  double rcb = ob[0] + ob[1] * u + ob[2] * v + ob[3] * (h + ke);
+  const double ob2 = DIM == 2 ? ob[2] : 0.0;
+  double rcb = ob[0] + ob[1] * u + ob2 * v + ob[EI] * (h + ke);
   double Y8b[NR];
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
-    rcb += ob[4 + k] * Y8[k];
-    Y8b[k] = ob[4 + k] * rho_c;
+    rcb += ob[NY + k] * Y8[k];
+    Y8b[k] = ob[NY + k] * rho_c;
   }
-  const double ubl = (ob[1] + ob[3] * u) * rho_c, vbl = (ob[2] + ob[3] * v) * rho_c;
-  const double hb = ob[3] * rho_c, pcb = -ob[3];
+  const double ubl = (ob[1] + ob[EI] * u) * rho_c, vbl = (ob2 + ob[EI] * v) * rho_c;
+  const double hb = ob[EI] * rho_c, pcb = -ob[EI];
   // gamma_c = cp / (cp - R), h = sum h_k Y_k, cp = sum cp_k Y_k at T_c
   const double cpb = -gcb * R * icv2;
   double Rb = gcb * cp * icv2;
@@ -639,11 +662,11 @@ __device__ void outlet_vjp(const MP& m, const double* q, double gamma, double T,
 #pragma unroll
   for (int k = 0; k < NR; ++k) Y8b[k] += Rb * (m.invM[k] - m.invM[NR]);
   ub[1] += ubl * ri;
-  ub[2] += vbl * ri;
+  if (DIM == 2) ub[2] += vbl * ri;
   rb -= (ubl * u + vbl * v) * ri;
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
-    ub[4 + k] += Y8b[k] * ri;
+    ub[NY + k] += Y8b[k] * ri;
     rb -= Y8b[k] * Y8[k] * ri;
   }
   ub[0] += rb;
@@ -653,17 +676,18 @@ __device__ void outlet_vjp(const MP& m, const double* q, double gamma, double T,
 // ---------------------------------------------------------------------------
 // the probe term of the loss: L += dt_n * mean probe p(U_{n+1}), p = rho R T
 // ---------------------------------------------------------------------------
+template <int DIM>
 __device__ __forceinline__ void probe_vjp(const MP& m, const double* q, double T, double w, double* ub, double& Tb) {
   const double rho = q[0], ri = 1.0 / rho;
   double Y8[NR], Yf[NS];
-  cell_Y(q, ri, Y8, Yf);
+  cell_Y<DIM>(q, ri, Y8, Yf);
   const double R = get_R(m, Yf);
   double rb = w * R * T;
   const double Rb = w * rho * T;
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
     const double yb = Rb * (m.invM[k] - m.invM[NR]);
-    ub[4 + k] += yb * ri;
+    ub[Lay<DIM>::NY + k] += yb * ri;
     rb -= yb * Y8[k] * ri;
   }
   ub[0] += rb;
@@ -674,32 +698,34 @@ __device__ __forceinline__ void probe_vjp(const MP& m, const double* q, double T
 // update_aux VJP of U4 (the aux adjoint is consumed and cleared), the
 // primitives (rho, u, v, p) of the three stage states U, U1, U2, and the
 // alpha and CFL tie counts of the three stages.
+template <int DIM>
 __global__ void __launch_bounds__(128) k_vjp_begin(MP m, Grid g, const double* __restrict__ U4,
                                                    const double* __restrict__ A4, const double* __restrict__ pp_bar,
                                                    int px, int py, int wx, int wy, double* Ub, double* Ab,
                                                    const double* __restrict__ rec, double* prims,
                                                    const unsigned char* __restrict__ mult,
                                                    const double* __restrict__ slots_rec, double cfl, double* red) {
-  const long long nc = g.ncell, nU = 12 * nc;
+  constexpr int NVD = Lay<DIM>::NV;
+  const long long nc = g.ncell, nU = NVD * nc;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double cnt[7];
 #pragma unroll
   for (int i = 0; i < 7; ++i) cnt[i] = 0.0;
   if (c < nc) {
     const int x = (int)(c / g.ny), y = (int)(c % g.ny);
-    double q[12], ub[12];
+    double q[NVD], ub[NVD];
     double gb = Ab[c], Tb = Ab[nc + c];
 #pragma unroll
-    for (int f = 0; f < 12; ++f) ub[f] = 0.0;
+    for (int f = 0; f < NVD; ++f) ub[f] = 0.0;
     const bool in_probe = pp_bar && x >= px && x < px + wx && y >= py && y < py + wy;
     if (in_probe || gb != 0.0 || Tb != 0.0) {
 #pragma unroll
-      for (int f = 0; f < 12; ++f) q[f] = U4[f * nc + c];
+      for (int f = 0; f < NVD; ++f) q[f] = U4[f * nc + c];
       const double T = A4[nc + c];
-      if (in_probe) probe_vjp(m, q, T, *pp_bar / (double)(wx * wy), ub, Tb);
-      upd_vjp(m, q, T, gb, Tb, ub);
+      if (in_probe) probe_vjp<DIM>(m, q, T, *pp_bar / (double)(wx * wy), ub, Tb);
+      upd_vjp<DIM>(m, q, T, gb, Tb, ub);
 #pragma unroll
-      for (int f = 0; f < 12; ++f) Ub[f * nc + c] += ub[f];
+      for (int f = 0; f < NVD; ++f) Ub[f * nc + c] += ub[f];
       Ab[c] = 0.0;
       Ab[nc + c] = 0.0;
     }
@@ -709,16 +735,16 @@ __global__ void __launch_bounds__(128) k_vjp_begin(MP m, Grid g, const double* _
       const double* S = rec + (long long)s * (nU + 2 * nc);
       const double* A = S + nU;
 #pragma unroll
-      for (int f = 0; f < 12; ++f) q[f] = S[f * nc + c];
-      const Prim<2> pr = u_to_prim<2>(m, q, A[c], A[nc + c]);
+      for (int f = 0; f < NVD; ++f) q[f] = S[f * nc + c];
+      const Prim<DIM> pr = u_to_prim<DIM>(m, q, A[c], A[nc + c]);
       double* P = prims + (long long)s * 4 * nc;
       P[c] = pr.rho;
       P[nc + c] = pr.u;
       P[2 * nc + c] = pr.v;
       P[3 * nc + c] = pr.p;
-      const Speeds sp = speeds_of(g, pr);
+      const Speeds sp = speeds_of<DIM>(g, pr);
       if (tied(sp.sx, bitsd(rs->ax[s]))) cnt[2 * s] = mult[c];
-      if (tied(sp.sy, bitsd(rs->ay[s]))) cnt[2 * s + 1] = mult[c];
+      if (DIM == 2 && tied(sp.sy, bitsd(rs->ay[s]))) cnt[2 * s + 1] = mult[c];
       if (s == 0 && cfl > 0.0 && tied(sp.d, rs->dt / cfl)) cnt[6] = 1.0;
     }
   }
@@ -733,31 +759,33 @@ __global__ void __launch_bounds__(128) k_vjp_begin(MP m, Grid g, const double* _
 // The outlet ghosts of the three stage states (blockIdx.y = stage), one
 // thread per boundary position: og, and the ghosts' alpha tie counts (3
 // padded entries per position).
+template <int DIM>
 __global__ void __launch_bounds__(128) k_outlet_ghosts(MP m, Grid g, const double* __restrict__ rec,
                                                        const double* __restrict__ slots_rec, double* og,
                                                        double* red) {
-  const long long nc = g.ncell, nU = 12 * nc;
+  constexpr int NVD = Lay<DIM>::NV;
+  const long long nc = g.ncell, nU = NVD * nc;
   const int st = blockIdx.y;
   int side, pos, x, y;
-  boundary_pos(g, blockIdx.x * blockDim.x + threadIdx.x, side, pos, x, y);
+  boundary_pos<DIM>(g, blockIdx.x * blockDim.x + threadIdx.x, side, pos, x, y);
   double cx = 0.0, cy = 0.0;
   if (side >= 0 && outlet_side(g, side)) {
     const long long c = (long long)x * g.ny + y;
     const double* S = rec + (long long)st * (nU + 2 * nc);
-    double q[12], gs[14];
+    double q[NVD], gs[NVD + 2];
 #pragma unroll
-    for (int f = 0; f < 12; ++f) q[f] = S[f * nc + c];
-    pressure_outlet_state<2>(m, q, S[nU + c], S[nU + nc + c], outlet_un(q, side), g.Pb, gs);
-    const Prim<2> pr = u_to_prim<2>(m, gs, gs[12], gs[13]);
+    for (int f = 0; f < NVD; ++f) q[f] = S[f * nc + c];
+    pressure_outlet_state<DIM>(m, q, S[nU + c], S[nU + nc + c], outlet_un(q, side), g.Pb, gs);
+    const Prim<DIM> pr = u_to_prim<DIM>(m, gs, gs[NVD], gs[NVD + 1]);
 #pragma unroll
-    for (int f = 0; f < 12; ++f) og[og_idx(g, st, side, f, pos)] = gs[f];
-    og[og_idx(g, st, side, 12, pos)] = pr.u;
-    og[og_idx(g, st, side, 13, pos)] = pr.v;
-    og[og_idx(g, st, side, 14, pos)] = pr.p;
+    for (int f = 0; f < NVD; ++f) og[og_idx(g, st, side, f, pos)] = gs[f];
+    og[og_idx(g, st, side, OG_U, pos)] = pr.u;
+    og[og_idx(g, st, side, OG_V, pos)] = pr.v;
+    og[og_idx(g, st, side, OG_P, pos)] = pr.p;
     const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
-    const Speeds sp = speeds_of(g, pr);
+    const Speeds sp = speeds_of<DIM>(g, pr);
     if (tied(sp.sx, bitsd(rs->ax[st]))) cx = 3.0;
-    if (tied(sp.sy, bitsd(rs->ay[st]))) cy = 3.0;
+    if (DIM == 2 && tied(sp.sy, bitsd(rs->ay[st]))) cy = 3.0;
   }
   block_add(cx, red + red_cnt(st, 0));
   block_add(cy, red + red_cnt(st, 1));
@@ -782,20 +810,20 @@ constexpr int SW_NT = 128;
 // H+ and H- of field f at padded cell a of a line, from the stage state and
 // its primitives (those of the source cell; ghosts flip the momentum), or
 // for a pressure-outlet ghost from the stage's outlet ghosts og.
-template <int D>
+template <int D, int DIM>
 __device__ __forceinline__ void sweep_load(const Grid& g, const double* __restrict__ Uk,
                                            const double* __restrict__ Pk, const double* __restrict__ og, int f,
                                            int line, int a, double alpha, double& hp, double& hm, double& qv) {
-  const Src s = map_cell<2>(g, D == 0 ? a : line, D == 0 ? line : a);
+  const Src s = map_cell<DIM>(g, D == 0 ? a : line, D == 0 ? line : a);
   const long long nc = g.ncell;
   double qf, rho, p, u, v;
   if (s.kind == 1) {
     const double* o = og + (size_t)s.side * OG_F * g.lstrip + s.pos;
     qf = o[(size_t)f * g.lstrip];
     rho = o[0];
-    u = o[(size_t)12 * g.lstrip];
-    v = o[(size_t)13 * g.lstrip];
-    p = o[(size_t)14 * g.lstrip];
+    u = o[(size_t)OG_U * g.lstrip];
+    v = o[(size_t)OG_V * g.lstrip];
+    p = o[(size_t)OG_P * g.lstrip];
   } else {
     const long long src = (long long)s.xs * g.ny + s.ys;
     qf = Uk[f * nc + src];
@@ -812,15 +840,15 @@ __device__ __forceinline__ void sweep_load(const Grid& g, const double* __restri
   double F;
   if (f == 0) F = rho * un;
   else if (f == mn) F = rho * un * un + p;
-  else if (f == 3 - mn) F = rho * u * v;
-  else if (f == 3) F = un * (qf + p);
+  else if (DIM == 2 && f == 3 - mn) F = rho * u * v;
+  else if (f == Lay<DIM>::EI) F = un * (qf + p);
   else F = un * qf;
   hp = 0.5 * (F + alpha * qf);
   hm = 0.5 * (F - alpha * qf);
   qv = qf;
 }
 
-template <int D>
+template <int D, int DIM>
 __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restrict__ Uk,
                                            const double* __restrict__ Pk, const double* __restrict__ og,
                                            const double* __restrict__ Uo_b,
@@ -851,7 +879,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
   double Hp[6], Hm[6], Q[6], Ap[6], Am[6];
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
-    sweep_load<D>(g, Uk, Pk, og, f, line, flo - 3 + k, alpha, Hp[k], Hm[k], Q[k]);
+    sweep_load<D, DIM>(g, Uk, Pk, og, f, line, flo - 3 + k, alpha, Hp[k], Hm[k], Q[k]);
     Ap[k] = 0.0;
     Am[k] = 0.0;
   }
@@ -860,7 +888,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
   double lbm = lbar(flo - 1), Fprev = 0.0;
 #pragma unroll 1
   for (int fa = flo; fa <= fhi; ++fa) {
-    sweep_load<D>(g, Uk, Pk, og, f, line, fa + 2, alpha, Hp[5], Hm[5], Q[5]);
+    sweep_load<D, DIM>(g, Uk, Pk, og, f, line, fa + 2, alpha, Hp[5], Hm[5], Q[5]);
     const double lbp = lbar(fa);
     // L_i = -(F_{i+1} - F_i) / d  ->  Fbar_fa = dt (Lbar_fa - Lbar_{fa-1}) / d
     const double Fbf = dt_dA * (lbp - lbm);
@@ -904,6 +932,7 @@ __device__ __forceinline__ void sweep_body(const Grid& g, const double* __restri
 // Both directions of one RK stage: blocks [0, nbx) sweep x lines (SW_NT
 // consecutive y per block), the rest y lines (SW_NT consecutive x); the
 // field runs fastest over blocks, then the line block, then the segment.
+template <int DIM>
 __global__ void __launch_bounds__(SW_NT, 4) k_flux_sweep(Grid g, const double* __restrict__ Uk,
                                                       const double* __restrict__ Pk,
                                                       const double* __restrict__ og,
@@ -915,17 +944,20 @@ __global__ void __launch_bounds__(SW_NT, 4) k_flux_sweep(Grid g, const double* _
   int b = blockIdx.x;
   const int D = b < nbx ? 0 : 1;
   if (D) b -= nbx;
-  const int f = b % 12;
-  b /= 12;
+  const int f = b % Lay<DIM>::NV;
+  b /= Lay<DIM>::NV;
   const int nl = D == 0 ? nlx : nly;
-  const int line = (b % nl) * SW_NT + threadIdx.x, seg = b / nl;
+  // 2D: a block sweeps SW_NT consecutive lines; 1D (one line): SW_NT
+  // consecutive segments of it
+  const int line = DIM == 1 ? 0 : (b % nl) * SW_NT + threadIdx.x;
+  const int seg = DIM == 1 ? b * SW_NT + threadIdx.x : b / nl;
   double ab = 0.0, dtb = 0.0;
   if (D == 0) {
-    if (line < g.ny)
-      sweep_body<0>(g, Uk, Pk, og, Uo_b, coef, bitsd(rs->ax[stage]), rs->dt, f, line, seg, FbX, UaX, ab, dtb);
-  } else {
+    if (line < g.ny && seg * SW_R < g.nx + 6)
+      sweep_body<0, DIM>(g, Uk, Pk, og, Uo_b, coef, bitsd(rs->ax[stage]), rs->dt, f, line, seg, FbX, UaX, ab, dtb);
+  } else if (DIM == 2) {
     if (line < g.nx)
-      sweep_body<1>(g, Uk, Pk, og, Uo_b, coef, bitsd(rs->ay[stage]), rs->dt, f, line, seg, FbY, UaY, ab, dtb);
+      sweep_body<1, DIM>(g, Uk, Pk, og, Uo_b, coef, bitsd(rs->ay[stage]), rs->dt, f, line, seg, FbY, UaY, ab, dtb);
   }
   block_add(ab, red + red_ab(stage, D));
   block_add(dtb, red + RED_DTB);
@@ -933,28 +965,30 @@ __global__ void __launch_bounds__(SW_NT, 4) k_flux_sweep(Grid g, const double* _
 
 // ub, Tb += the VJP of the direction-D physical flux F(q, T) (rho un, rho un
 // u + p e_n, un (rho E + p), rho un Y) with adjoint Fb.
-template <int D>
+template <int D, int DIM>
 __device__ __forceinline__ void flux_fn_vjp(const MP& m, const double* q, double T, const double* Fb, double* ub,
                                             double& Tb) {
+  constexpr int NY = Lay<DIM>::NY, EI = Lay<DIM>::EI;
   const double rho = q[0], ri = 1.0 / rho;
-  const double u = q[1] * ri, v = q[2] * ri;
+  const double u = q[1] * ri, v = DIM == 2 ? q[2] * ri : 0.0;
   double Y8[NR], Yf[NS];
-  cell_Y(q, ri, Y8, Yf);
+  cell_Y<DIM>(q, ri, Y8, Yf);
   const double R = get_R(m, Yf);
   const double p = rho * R * T;
   const double un = D == 0 ? u : v, ut = D == 0 ? v : u;
   constexpr int mn = D == 0 ? 1 : 2, mt = 3 - mn;
-  double rb = Fb[0] * un + Fb[mn] * un * un + Fb[mt] * u * v;
-  double unb = Fb[0] * rho + Fb[mn] * 2.0 * rho * un + Fb[mt] * rho * ut + Fb[3] * (q[3] + p);
-  const double utb = Fb[mt] * rho * un;
-  const double pb = Fb[mn] + Fb[3] * un;
-  ub[3] += Fb[3] * un;
+  const double fbt = DIM == 2 ? Fb[mt] : 0.0;  // the transverse momentum (2D)
+  double rb = Fb[0] * un + Fb[mn] * un * un + fbt * u * v;
+  double unb = Fb[0] * rho + Fb[mn] * 2.0 * rho * un + fbt * rho * ut + Fb[EI] * (q[EI] + p);
+  const double utb = fbt * rho * un;
+  const double pb = Fb[mn] + Fb[EI] * un;
+  ub[EI] += Fb[EI] * un;
   double Yb[NR];
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
-    rb += Fb[4 + k] * un * Y8[k];
-    unb += Fb[4 + k] * rho * Y8[k];
-    Yb[k] = Fb[4 + k] * rho * un;
+    rb += Fb[NY + k] * un * Y8[k];
+    unb += Fb[NY + k] * rho * Y8[k];
+    Yb[k] = Fb[NY + k] * rho * un;
   }
   rb += pb * R * T;
   const double Rb = pb * rho * T;
@@ -963,11 +997,11 @@ __device__ __forceinline__ void flux_fn_vjp(const MP& m, const double* q, double
   for (int k = 0; k < NR; ++k) Yb[k] += Rb * (m.invM[k] - m.invM[NR]);
   const double ubx = D == 0 ? unb : utb, uby = D == 0 ? utb : unb;
   ub[1] += ubx * ri;
-  ub[2] += uby * ri;
+  if (DIM == 2) ub[2] += uby * ri;
   rb -= ubx * u * ri + uby * v * ri;
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
-    ub[4 + k] += Yb[k] * ri;
+    ub[NY + k] += Yb[k] * ri;
     rb -= Yb[k] * Y8[k] * ri;
   }
   ub[0] += rb;
@@ -976,28 +1010,29 @@ __device__ __forceinline__ void flux_fn_vjp(const MP& m, const double* q, double
 // The ghost entries of the two direction-D sides that copy interior cell
 // (x, y): their flux-function VJP at the ghost state (flipped momentum), with
 // the flips undone on the way back.
-template <int D>
+template <int D, int DIM>
 __device__ __forceinline__ void merge_ghosts(const MP& m, const Grid& g, const double* q, double T, int x, int y,
                                              const double* __restrict__ Fb, const double* __restrict__ Ua,
                                              double* ub, double& Tb) {
+  constexpr int NVD = Lay<DIM>::NV;
   const int nA = D == 0 ? g.nx : g.ny;
   const size_t npad = D == 0 ? (size_t)(g.nx + 6) * g.ny : (size_t)g.nx * (g.ny + 6);
 #pragma unroll 1
   for (int i = 0; i < 6; ++i) {
     const int a = i < 3 ? -1 - i : nA + i - 3;
-    const Src s = map_cell<2>(g, D == 0 ? a : x, D == 0 ? y : a);
+    const Src s = map_cell<DIM>(g, D == 0 ? a : x, D == 0 ? y : a);
     if (s.kind != 0 || s.xs != x || s.ys != y) continue;
     const size_t k = D == 0 ? (size_t)(a + 3) * g.ny + y : (size_t)x * (g.ny + 6) + (a + 3);
-    double qg[12], ug[12], fb[12];
+    double qg[NVD], ug[NVD], fb[NVD];
 #pragma unroll
-    for (int f = 0; f < 12; ++f) {
+    for (int f = 0; f < NVD; ++f) {
       qg[f] = ((s.flip >> f) & 1) ? -q[f] : q[f];
       ug[f] = Ua[f * npad + k];
       fb[f] = Fb[f * npad + k];
     }
-    flux_fn_vjp<D>(m, qg, T, fb, ug, Tb);
+    flux_fn_vjp<D, DIM>(m, qg, T, fb, ug, Tb);
 #pragma unroll
-    for (int f = 0; f < 12; ++f) ub[f] += ((s.flip >> f) & 1) ? -ug[f] : ug[f];
+    for (int f = 0; f < NVD; ++f) ub[f] += ((s.flip >> f) & 1) ? -ug[f] : ug[f];
   }
 }
 
@@ -1005,30 +1040,32 @@ __device__ __forceinline__ void merge_ghosts(const MP& m, const Grid& g, const d
 // 3 ghost layers' flux and LF-term adjoints (sweeps) and their alpha ties,
 // through the flux function and wave speeds at the ghost state, then the
 // outlet state's VJP into the boundary cell: ogb.
+template <int DIM>
 __global__ void __launch_bounds__(128) k_outlet_vjp(MP m, Grid g, const double* __restrict__ Uk,
                                                     const double* __restrict__ Ak,
                                                     const double* __restrict__ slots_rec, int stage,
                                                     const double* __restrict__ red, const double* __restrict__ FbX,
                                                     const double* __restrict__ UaX, const double* __restrict__ FbY,
                                                     const double* __restrict__ UaY, double* ogb) {
+  constexpr int NVD = Lay<DIM>::NV;
   const long long nc = g.ncell;
   int side, pos, x, y;
-  boundary_pos(g, blockIdx.x * blockDim.x + threadIdx.x, side, pos, x, y);
+  boundary_pos<DIM>(g, blockIdx.x * blockDim.x + threadIdx.x, side, pos, x, y);
   if (side < 0 || !outlet_side(g, side)) return;
   const long long c = (long long)x * g.ny + y;
-  double q[12], gs[14], ob[12], fb[12];
+  double q[NVD], gs[NVD + 2], ob[NVD], fb[NVD];
 #pragma unroll
-  for (int f = 0; f < 12; ++f) q[f] = Uk[f * nc + c];
+  for (int f = 0; f < NVD; ++f) q[f] = Uk[f * nc + c];
   const double gamma = Ak[c], T = Ak[nc + c];
   const double un = outlet_un(q, side);
-  pressure_outlet_state<2>(m, q, gamma, T, un, g.Pb, gs);
+  pressure_outlet_state<DIM>(m, q, gamma, T, un, g.Pb, gs);
   const int D = side < 2 ? 0 : 1;
   const int nA = D == 0 ? g.nx : g.ny;
   const size_t npad = D == 0 ? (size_t)(g.nx + 6) * g.ny : (size_t)g.nx * (g.ny + 6);
   const double* Fb = D == 0 ? FbX : FbY;
   const double* Ua = D == 0 ? UaX : UaY;
 #pragma unroll
-  for (int f = 0; f < 12; ++f) {
+  for (int f = 0; f < NVD; ++f) {
     ob[f] = 0.0;
     fb[f] = 0.0;
   }
@@ -1037,29 +1074,30 @@ __global__ void __launch_bounds__(128) k_outlet_vjp(MP m, Grid g, const double* 
     const int a = (side == 0 || side == 2) ? -1 - i : nA + i;
     const size_t k = D == 0 ? (size_t)(a + 3) * g.ny + pos : (size_t)pos * (g.ny + 6) + (a + 3);
 #pragma unroll
-    for (int f = 0; f < 12; ++f) {
+    for (int f = 0; f < NVD; ++f) {
       ob[f] += Ua[f * npad + k];
       fb[f] += Fb[f * npad + k];
     }
   }
   double gcb = 0.0, Tcb = 0.0;
-  if (D == 0) flux_fn_vjp<0>(m, gs, gs[13], fb, ob, Tcb);
-  else flux_fn_vjp<1>(m, gs, gs[13], fb, ob, Tcb);
+  if (D == 0) flux_fn_vjp<0, DIM>(m, gs, gs[NVD + 1], fb, ob, Tcb);
+  else if (DIM == 2) flux_fn_vjp<1, DIM>(m, gs, gs[NVD + 1], fb, ob, Tcb);
   const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
-  const Speeds sp = speeds_of(g, u_to_prim<2>(m, gs, gs[12], gs[13]));
+  const Speeds sp = speeds_of<DIM>(g, u_to_prim<DIM>(m, gs, gs[NVD], gs[NVD + 1]));
   const double cx = red[red_cnt(stage, 0)], cy = red[red_cnt(stage, 1)];
   const double wx = (cx > 0.0 && tied(sp.sx, bitsd(rs->ax[stage]))) ? red[red_ab(stage, 0)] * 3.0 / cx : 0.0;
-  const double wy = (cy > 0.0 && tied(sp.sy, bitsd(rs->ay[stage]))) ? red[red_ab(stage, 1)] * 3.0 / cy : 0.0;
-  speed_vjp(m, gs, gs[12], gs[13], 1, wx, ob, gcb, Tcb);
-  speed_vjp(m, gs, gs[12], gs[13], 2, wy, ob, gcb, Tcb);
-  double ub[12], Tb = 0.0;
+  const double wy =
+      (DIM == 2 && cy > 0.0 && tied(sp.sy, bitsd(rs->ay[stage]))) ? red[red_ab(stage, 1)] * 3.0 / cy : 0.0;
+  speed_vjp<DIM>(m, gs, gs[NVD], gs[NVD + 1], 1, wx, ob, gcb, Tcb);
+  if (DIM == 2) speed_vjp<DIM>(m, gs, gs[NVD], gs[NVD + 1], 2, wy, ob, gcb, Tcb);
+  double ub[NVD], Tb = 0.0;
 #pragma unroll
-  for (int f = 0; f < 12; ++f) ub[f] = 0.0;
-  outlet_vjp(m, q, gamma, T, un, g.Pb, ob, gcb, Tcb, ub, Tb);
+  for (int f = 0; f < NVD; ++f) ub[f] = 0.0;
+  outlet_vjp<DIM>(m, q, gamma, T, un, g.Pb, ob, gcb, Tcb, ub, Tb);
   double* o = ogb + (size_t)side * OG_B * g.lstrip + pos;
 #pragma unroll
-  for (int f = 0; f < 12; ++f) o[(size_t)f * g.lstrip] = ub[f];
-  o[(size_t)12 * g.lstrip] = Tb;
+  for (int f = 0; f < NVD; ++f) o[(size_t)f * g.lstrip] = ub[f];
+  o[(size_t)OG_T * g.lstrip] = Tb;
 }
 
 // One RK stage U' = a Un + b (Uk + dt L(Uk, auxk)), per interior cell of Uk:
@@ -1069,96 +1107,102 @@ __global__ void __launch_bounds__(128) k_outlet_vjp(MP m, Grid g, const double* 
 // the CFL ties of dt), then either the update_aux VJP of Uk with its
 // completed aux adjoint (Ab null) or the aux adjoint itself added to Ab.
 // ub_add / un_add: add to Ub / Un_b instead of storing.
+template <int DIM>
 __global__ void __launch_bounds__(128, 4) k_stage_merge(
     MP m, Grid g, const double* __restrict__ Uk, const double* __restrict__ Ak, const double* __restrict__ Uo_b,
     double coef, const double* __restrict__ slots_rec, int stage, double cfl, const unsigned char* __restrict__ mult,
     const double* __restrict__ red, const double* __restrict__ dt_bar_ext, const double* __restrict__ FbX,
     const double* __restrict__ UaX, const double* __restrict__ FbY, const double* __restrict__ UaY, double* Ub,
     int ub_add, double* Ab, double* Un_b, double un_coef, int un_add, const double* __restrict__ ogb) {
+  constexpr int NVD = Lay<DIM>::NV;
   const long long nc = g.ncell;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   const int x = (int)(c / g.ny), y = (int)(c % g.ny);
-  double q[12], ub[12], fb[12];
+  double q[NVD], ub[NVD], fb[NVD];
 #pragma unroll
-  for (int f = 0; f < 12; ++f) q[f] = Uk[f * nc + c];
+  for (int f = 0; f < NVD; ++f) q[f] = Uk[f * nc + c];
   const double gamma = Ak[c], T = Ak[nc + c];
   double Tb = 0.0, gb = 0.0;
   {
     const size_t npx = (size_t)(g.nx + 6) * g.ny, npy = (size_t)g.nx * (g.ny + 6);
     const size_t ix = (size_t)(x + 3) * g.ny + y, iy = (size_t)x * (g.ny + 6) + y + 3;
 #pragma unroll
-    for (int f = 0; f < 12; ++f) {
-      ub[f] = UaX[f * npx + ix] + UaY[f * npy + iy];
+    for (int f = 0; f < NVD; ++f) {
+      ub[f] = UaX[f * npx + ix] + (DIM == 2 ? UaY[f * npy + iy] : 0.0);
       fb[f] = FbX[f * npx + ix];
     }
-    flux_fn_vjp<0>(m, q, T, fb, ub, Tb);
+    flux_fn_vjp<0, DIM>(m, q, T, fb, ub, Tb);
+    if (DIM == 2) {
 #pragma unroll
-    for (int f = 0; f < 12; ++f) fb[f] = FbY[f * npy + iy];
-    flux_fn_vjp<1>(m, q, T, fb, ub, Tb);
+      for (int f = 0; f < NVD; ++f) fb[f] = FbY[f * npy + iy];
+      flux_fn_vjp<1, DIM>(m, q, T, fb, ub, Tb);
+    }
   }
   // only cells within four of a side are copied into ghosts
-  if (x < 4 || x >= g.nx - 4) merge_ghosts<0>(m, g, q, T, x, y, FbX, UaX, ub, Tb);
-  if (y < 4 || y >= g.ny - 4) merge_ghosts<1>(m, g, q, T, x, y, FbY, UaY, ub, Tb);
+  if (x < 4 || x >= g.nx - 4) merge_ghosts<0, DIM>(m, g, q, T, x, y, FbX, UaX, ub, Tb);
+  if (DIM == 2 && (y < 4 || y >= g.ny - 4)) merge_ghosts<1, DIM>(m, g, q, T, x, y, FbY, UaY, ub, Tb);
   // the outlet ghosts of the sides this cell borders (k_outlet_vjp)
-  if (ogb && (x == 0 || x == g.nx - 1 || y == 0 || y == g.ny - 1)) {
+  if (ogb && (x == 0 || x == g.nx - 1 || (DIM == 2 && (y == 0 || y == g.ny - 1)))) {
 #pragma unroll 1
-    for (int side = 0; side < 4; ++side) {
+    for (int side = 0; side < 2 * DIM; ++side) {
       const bool on = side == 0 ? x == 0 : side == 1 ? x == g.nx - 1 : side == 2 ? y == 0 : y == g.ny - 1;
       if (!on || !outlet_side(g, side)) continue;
       const double* o = ogb + (size_t)side * OG_B * g.lstrip + (side < 2 ? y : x);
 #pragma unroll
-      for (int f = 0; f < 12; ++f) ub[f] += o[(size_t)f * g.lstrip];
-      Tb += o[(size_t)12 * g.lstrip];
+      for (int f = 0; f < NVD; ++f) ub[f] += o[(size_t)f * g.lstrip];
+      Tb += o[(size_t)OG_T * g.lstrip];
     }
   }
 #pragma unroll
-  for (int f = 0; f < 12; ++f) {
+  for (int f = 0; f < NVD; ++f) {
     const double uo = Uo_b[f * nc + c];
     ub[f] += coef * uo;
     if (Un_b) Un_b[f * nc + c] = (un_add ? Un_b[f * nc + c] : 0.0) + un_coef * uo;
   }
   // alpha ties (evenly over the tied padded entries) and the CFL ties of dt
   const jb_slots* rs = reinterpret_cast<const jb_slots*>(slots_rec);
-  const Prim<2> pr = u_to_prim<2>(m, q, gamma, T);
-  const Speeds sp = speeds_of(g, pr);
+  const Prim<DIM> pr = u_to_prim<DIM>(m, q, gamma, T);
+  const Speeds sp = speeds_of<DIM>(g, pr);
   double wx = 0.0, wy = 0.0;
   const double cx = red[red_cnt(stage, 0)], cy = red[red_cnt(stage, 1)];
   if (cx > 0.0 && tied(sp.sx, bitsd(rs->ax[stage]))) wx = red[red_ab(stage, 0)] * mult[c] / cx;
-  if (cy > 0.0 && tied(sp.sy, bitsd(rs->ay[stage]))) wy = red[red_ab(stage, 1)] * mult[c] / cy;
+  if (DIM == 2 && cy > 0.0 && tied(sp.sy, bitsd(rs->ay[stage]))) wy = red[red_ab(stage, 1)] * mult[c] / cy;
   if (stage == 0 && cfl > 0.0) {
     const double cd = red[red_cnt(0, 2)];
     if (cd > 0.0 && tied(sp.d, rs->dt / cfl)) {
+      // d = 1 / (sx/dx + sy/dy) (2D) or dx / sx (1D): dd/dsx = -d^2/dx either way
       const double db = cfl * (red[RED_DTB] + (dt_bar_ext ? *dt_bar_ext : 0.0)) / cd;
       wx += -db * sp.d * sp.d / g.dx;
-      wy += -db * sp.d * sp.d / g.dy;
+      if (DIM == 2) wy += -db * sp.d * sp.d / g.dy;
     }
   }
-  speed_vjp(m, q, gamma, T, 1, wx, ub, gb, Tb);
-  speed_vjp(m, q, gamma, T, 2, wy, ub, gb, Tb);
+  speed_vjp<DIM>(m, q, gamma, T, 1, wx, ub, gb, Tb);
+  if (DIM == 2) speed_vjp<DIM>(m, q, gamma, T, 2, wy, ub, gb, Tb);
   if (Ab) {
     Ab[c] += gb;
     Ab[nc + c] += Tb;
   } else {
-    upd_vjp(m, q, T, gb, Tb, ub);
+    upd_vjp<DIM>(m, q, T, gb, Tb, ub);
   }
 #pragma unroll
-  for (int f = 0; f < 12; ++f) Ub[f * nc + c] = (ub_add ? Ub[f * nc + c] : 0.0) + ub[f];
+  for (int f = 0; f < NVD; ++f) Ub[f * nc + c] = (ub_add ? Ub[f * nc + c] : 0.0) + ub[f];
 }
 
 // mean pressure over the probe rectangle (one block)
+template <int DIM>
 __global__ void k_probe_mean(MP m, Grid g, const double* __restrict__ U, const double* __restrict__ A, int px,
                              int py, int wx, int wy, double* out) {
   const long long nc = g.ncell;
   double s = 0.0;
   for (int t = threadIdx.x; t < wx * wy; t += blockDim.x) {
     const long long c = (long long)(px + t / wy) * g.ny + (py + t % wy);
-    double q[12];
+    double q[Lay<DIM>::NV];
 #pragma unroll
-    for (int f = 0; f < 12; ++f) q[f] = U[f * nc + c];
+    for (int f = 0; f < Lay<DIM>::NV; ++f) q[f] = U[f * nc + c];
     const double rho = q[0], ri = 1.0 / rho;
     double Y8[NR], Yf[NS];
-    cell_Y(q, ri, Y8, Yf);
+    cell_Y<DIM>(q, ri, Y8, Yf);
     s += rho * get_R(m, Yf) * A[nc + c];
   }
   __shared__ double red[32];
@@ -1176,6 +1220,7 @@ __global__ void k_probe_mean(MP m, Grid g, const double* __restrict__ U, const d
 // ---------------------------------------------------------------------------
 // initial state (rho = P/(R T), rho E = rho h - P, aux = [gamma, T]) -> T adjoint
 // ---------------------------------------------------------------------------
+template <int DIM>
 __global__ void k_init_vjp(MP m, long long n, const double* __restrict__ P, const double* __restrict__ T,
                            const double* __restrict__ Y, const double* __restrict__ Ub, const double* __restrict__ Ab,
                            double* Tb) {
@@ -1193,9 +1238,9 @@ __global__ void k_init_vjp(MP m, long long n, const double* __restrict__ P, cons
   const double dE = drho * th.h + rho * th.cp;
   const double cv = th.cp - R;
   const double dgam = -th.dcp * R / (cv * cv);
-  double tb = Ub[c] * drho + Ub[3 * n + c] * dE + Ab[c] * dgam + Ab[n + c];
+  double tb = Ub[c] * drho + Ub[Lay<DIM>::EI * n + c] * dE + Ab[c] * dgam + Ab[n + c];
 #pragma unroll
-  for (int k = 0; k < NR; ++k) tb += Ub[(4 + k) * n + c] * Y8[k] * drho;
+  for (int k = 0; k < NR; ++k) tb += Ub[(Lay<DIM>::NY + k) * n + c] * Y8[k] * drho;
   Tb[c] = tb;
 }
 
@@ -1210,85 +1255,125 @@ namespace adj {
 
 static inline unsigned blocks_for(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
-static bool has_outlet(const jb_grid& g) {
-  for (int s = 0; s < 4; ++s)
+static bool has_outlet(int dim, const jb_grid& g) {
+  for (int s = 0; s < 2 * dim; ++s)
     if (g.bc[s] == JB_BC_PRESSURE_OUTLET) return true;
   return false;
 }
 
-// The scratch: FbX, UaX (12 x (nx+6) x ny each), FbY, UaY (12 x nx x (ny+6)
-// each), og (3 x 4 x OG_F x lstrip), ogb (4 x OG_B x lstrip).
-static double* og_of(const jb_grid& g, double* scratch) {
-  return scratch + 2 * 12 * ((size_t)(g.nx + 6) * g.ny + (size_t)g.nx * (g.ny + 6));
+// The scratch: FbX, UaX (nv x (nx+6) x ny each), in 2D FbY, UaY (nv x nx x
+// (ny+6) each), og (3 x 4 x OG_F x lstrip), ogb (4 x OG_B x lstrip).
+static size_t face_doubles(int dim, const jb_grid& g) {
+  const size_t nx6 = (size_t)(g.nx + 6) * g.ny, ny6 = dim == 2 ? (size_t)g.nx * (g.ny + 6) : 0;
+  return 2 * (size_t)g.nv * (nx6 + ny6);
 }
 
-cudaError_t vjp_begin(const jb_mech_params& m, const jb_grid& g, const double* U4, const double* A4,
+static double* og_of(int dim, const jb_grid& g, double* scratch) { return scratch + face_doubles(dim, g); }
+
+template <int DIM>
+static cudaError_t vjp_begin_t(const jb_mech_params& m, const jb_grid& g, const double* U4, const double* A4,
+                               const double* pp_bar, const int* probe, double* Ub, double* Ab, const double* rec,
+                               double* prims, const unsigned char* mult, const double* slots_rec, double cfl,
+                               double* red, double* scratch, cudaStream_t st) {
+  k_vjp_begin<DIM><<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U4, A4, probe[2] * probe[3] > 0 ? pp_bar : nullptr,
+                                                             probe[0], probe[1], probe[2], probe[3], Ub, Ab, rec,
+                                                             prims, mult, slots_rec, cfl, red);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !has_outlet(DIM, g)) return e;
+  const long long npos = DIM == 2 ? 2LL * (g.nx + g.ny) : 2;
+  k_outlet_ghosts<DIM><<<dim3(blocks_for(npos, 128), 3), 128, 0, st>>>(m, g, rec, slots_rec, og_of(DIM, g, scratch),
+                                                                     red);
+  return cudaGetLastError();
+}
+
+cudaError_t vjp_begin(int dim, const jb_mech_params& m, const jb_grid& g, const double* U4, const double* A4,
                       const double* pp_bar, const int* probe, double* Ub, double* Ab, const double* rec,
                       double* prims, const unsigned char* mult, const double* slots_rec, double cfl, double* red,
                       double* scratch, cudaStream_t st) {
-  k_vjp_begin<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, U4, A4, probe[2] * probe[3] > 0 ? pp_bar : nullptr,
-                                                        probe[0], probe[1], probe[2], probe[3], Ub, Ab, rec, prims,
-                                                        mult, slots_rec, cfl, red);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || !has_outlet(g)) return e;
-  k_outlet_ghosts<<<dim3(blocks_for(2LL * (g.nx + g.ny), 128), 3), 128, 0, st>>>(m, g, rec, slots_rec,
-                                                                                og_of(g, scratch), red);
-  return cudaGetLastError();
+  return dim == 2 ? vjp_begin_t<2>(m, g, U4, A4, pp_bar, probe, Ub, Ab, rec, prims, mult, slots_rec, cfl, red,
+                                   scratch, st)
+                  : vjp_begin_t<1>(m, g, U4, A4, pp_bar, probe, Ub, Ab, rec, prims, mult, slots_rec, cfl, red,
+                                   scratch, st);
 }
 
-cudaError_t chem_vjp(const jb_mech_params& m, const jb_grid& g, const double* U3, const double* A3,
+cudaError_t chem_vjp(int dim, const jb_mech_params& m, const jb_grid& g, const double* U3, const double* A3,
                      const double* Ub4, double* Ub3, const double* slot_dt, double* dtb, double* lnAb,
                      cudaStream_t st) {
   const size_t sm = sizeof(double) * (CHEM_ADJ_SH + NREAC) * CHEM_ADJ_NT;
-  cudaError_t e = cudaFuncSetAttribute(k_chem_vjp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
-  k_chem_vjp<<<blocks_for(g.ncell, CHEM_ADJ_NT), CHEM_ADJ_NT, sm, st>>>(m, g, U3, A3, Ub4, Ub3, slot_dt, dtb, lnAb);
+  if (dim == 2) {
+    cudaError_t e = cudaFuncSetAttribute(k_chem_vjp<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_chem_vjp<2><<<blocks_for(g.ncell, CHEM_ADJ_NT), CHEM_ADJ_NT, sm, st>>>(m, g, U3, A3, Ub4, Ub3, slot_dt, dtb,
+                                                                           lnAb);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_chem_vjp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_chem_vjp<1><<<blocks_for(g.ncell, CHEM_ADJ_NT), CHEM_ADJ_NT, sm, st>>>(m, g, U3, A3, Ub4, Ub3, slot_dt, dtb,
+                                                                           lnAb);
+  }
   return cudaGetLastError();
 }
 
-size_t flux_scratch_doubles(const jb_grid& g) {
-  return 2 * 12 * ((size_t)(g.nx + 6) * g.ny + (size_t)g.nx * (g.ny + 6)) +
-         (size_t)(3 * 4 * OG_F + 4 * OG_B) * g.lstrip;
+size_t flux_scratch_doubles(int dim, const jb_grid& g) {
+  return face_doubles(dim, g) + (size_t)(3 * 4 * OG_F + 4 * OG_B) * g.lstrip;
 }
 
-cudaError_t flux_stage(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
+template <int DIM>
+static cudaError_t flux_stage_t(const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
+                                const double* Pk, const double* Uo_b, double coef, const double* slots_rec, int stage,
+                                double cfl, const unsigned char* mult, double* red, const double* dt_bar_ext,
+                                double* scratch, double* Ub, bool ub_add, double* Ab, double* Un_b, double un_coef,
+                                bool un_add, cudaStream_t st) {
+  constexpr int NVD = Lay<DIM>::NV;
+  const size_t npx = NVD * (size_t)(g.nx + 6) * g.ny, npy = DIM == 2 ? NVD * (size_t)g.nx * (g.ny + 6) : 0;
+  double *FbX = scratch, *UaX = FbX + npx, *FbY = UaX + npx, *UaY = FbY + npy;
+  const int nlx = (g.ny + SW_NT - 1) / SW_NT, nsx = (g.nx + 6 + SW_R - 1) / SW_R;
+  const int nly = (g.nx + SW_NT - 1) / SW_NT, nsy = (g.ny + 6 + SW_R - 1) / SW_R;
+  const int nbx = (DIM == 2 ? nlx * nsx : (nsx + SW_NT - 1) / SW_NT) * NVD, nby = DIM == 2 ? nly * nsy * NVD : 0;
+  const bool outlet = has_outlet(DIM, g);
+  double* og = og_of(DIM, g, scratch);
+  double* ogb = og + (size_t)3 * 4 * OG_F * g.lstrip;
+  k_flux_sweep<DIM><<<nbx + nby, SW_NT, 0, st>>>(g, Uk, Pk,
+                                                 outlet ? og + (size_t)stage * 4 * OG_F * g.lstrip : nullptr, Uo_b,
+                                                 coef, slots_rec, stage, FbX, UaX, FbY, UaY, red, nbx, nlx, nly);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (outlet) {
+    const long long npos = DIM == 2 ? 2LL * (g.nx + g.ny) : 2;
+    k_outlet_vjp<DIM><<<blocks_for(npos, 128), 128, 0, st>>>(m, g, Uk, Ak, slots_rec, stage, red, FbX, UaX, FbY, UaY,
+                                                             ogb);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  k_stage_merge<DIM><<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, cfl, mult,
+                                                               red, dt_bar_ext, FbX, UaX, FbY, UaY, Ub,
+                                                               ub_add ? 1 : 0, Ab, Un_b, un_coef, un_add ? 1 : 0,
+                                                               outlet ? ogb : nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t flux_stage(int dim, const jb_mech_params& m, const jb_grid& g, const double* Uk, const double* Ak,
                        const double* Pk, const double* Uo_b, double coef, const double* slots_rec, int stage,
                        double cfl, const unsigned char* mult, double* red, const double* dt_bar_ext, double* scratch,
                        double* Ub, bool ub_add, double* Ab, double* Un_b, double un_coef, bool un_add,
                        cudaStream_t st) {
-  const size_t npx = 12 * (size_t)(g.nx + 6) * g.ny, npy = 12 * (size_t)g.nx * (g.ny + 6);
-  double *FbX = scratch, *UaX = FbX + npx, *FbY = UaX + npx, *UaY = FbY + npy;
-  const int nlx = (g.ny + SW_NT - 1) / SW_NT, nsx = (g.nx + 6 + SW_R - 1) / SW_R;
-  const int nly = (g.nx + SW_NT - 1) / SW_NT, nsy = (g.ny + 6 + SW_R - 1) / SW_R;
-  const int nbx = nlx * nsx * 12, nby = nly * nsy * 12;
-  const bool outlet = has_outlet(g);
-  double* og = og_of(g, scratch);
-  double* ogb = og + (size_t)3 * 4 * OG_F * g.lstrip;
-  k_flux_sweep<<<nbx + nby, SW_NT, 0, st>>>(g, Uk, Pk, outlet ? og + (size_t)stage * 4 * OG_F * g.lstrip : nullptr,
-                                            Uo_b, coef, slots_rec, stage, FbX, UaX, FbY, UaY, red, nbx, nlx, nly);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  if (outlet) {
-    k_outlet_vjp<<<blocks_for(2LL * (g.nx + g.ny), 128), 128, 0, st>>>(m, g, Uk, Ak, slots_rec, stage, red, FbX, UaX,
-                                                                       FbY, UaY, ogb);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
-  k_stage_merge<<<blocks_for(g.ncell, 128), 128, 0, st>>>(m, g, Uk, Ak, Uo_b, coef, slots_rec, stage, cfl, mult, red,
-                                                          dt_bar_ext, FbX, UaX, FbY, UaY, Ub, ub_add ? 1 : 0, Ab,
-                                                          Un_b, un_coef, un_add ? 1 : 0, outlet ? ogb : nullptr);
+  return dim == 2 ? flux_stage_t<2>(m, g, Uk, Ak, Pk, Uo_b, coef, slots_rec, stage, cfl, mult, red, dt_bar_ext,
+                                    scratch, Ub, ub_add, Ab, Un_b, un_coef, un_add, st)
+                  : flux_stage_t<1>(m, g, Uk, Ak, Pk, Uo_b, coef, slots_rec, stage, cfl, mult, red, dt_bar_ext,
+                                    scratch, Ub, ub_add, Ab, Un_b, un_coef, un_add, st);
+}
+
+cudaError_t probe_mean(int dim, const jb_mech_params& m, const jb_grid& g, const double* U, const double* A, int px,
+                       int py, int wx, int wy, double* out, cudaStream_t st) {
+  if (dim == 2) k_probe_mean<2><<<1, 128, 0, st>>>(m, g, U, A, px, py, wx, wy, out);
+  else k_probe_mean<1><<<1, 128, 0, st>>>(m, g, U, A, px, py, wx, wy, out);
   return cudaGetLastError();
 }
 
-cudaError_t probe_mean(const jb_mech_params& m, const jb_grid& g, const double* U, const double* A, int px, int py,
-                       int wx, int wy, double* out, cudaStream_t st) {
-  k_probe_mean<<<1, 128, 0, st>>>(m, g, U, A, px, py, wx, wy, out);
-  return cudaGetLastError();
-}
-
-cudaError_t init_vjp(const jb_mech_params& m, long long n, const double* P, const double* T, const double* Y,
+cudaError_t init_vjp(int dim, const jb_mech_params& m, long long n, const double* P, const double* T, const double* Y,
                      const double* Ub, const double* Ab, double* Tb, cudaStream_t st) {
-  k_init_vjp<<<blocks_for(n, 128), 128, 0, st>>>(m, n, P, T, Y, Ub, Ab, Tb);
+  if (dim == 2) k_init_vjp<2><<<blocks_for(n, 128), 128, 0, st>>>(m, n, P, T, Y, Ub, Ab, Tb);
+  else k_init_vjp<1><<<blocks_for(n, 128), 128, 0, st>>>(m, n, P, T, Y, Ub, Ab, Tb);
   return cudaGetLastError();
 }
 

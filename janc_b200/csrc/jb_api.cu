@@ -363,8 +363,8 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
   if (!(cfl > 0.0) && !(dt_fixed > 0.0)) return set_err(h, JB_ERR_ARG, "need cfl > 0 or dt > 0");
   if (U == U_out || aux == aux_out) return set_err(h, JB_ERR_ARG, "outputs must not alias inputs");
   if (int rc = check_theta(h)) return rc;
-  if (probe_p && (h->dim != 2 || h->probe[2] * h->probe[3] <= 0))
-    return set_err(h, JB_ERR_ARG, "probe pressures need a 2D handle with jb_set_probe");
+  if (probe_p && h->probe[2] * h->probe[3] <= 0)
+    return set_err(h, JB_ERR_ARG, "probe pressures need jb_set_probe");
   if (rec && (!rec_slots || !chemistry)) return set_err(h, JB_ERR_ARG, "a record needs rec_slots");
   if (rec && h->xch) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint record is single-domain");
   if (!chemistry && nsteps != 1) return set_err(h, JB_ERR_ARG, "the flux-only step is one step");
@@ -502,7 +502,7 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
                              cudaMemcpyDeviceToDevice, st),
              "record slots");
     if (probe_p)
-      JB_TRY(jb::adj::probe_mean(m, g, Uo, Ao, h->probe[0], h->probe[1], h->probe[2], h->probe[3], probe_p + s, st),
+      JB_TRY(jb::adj::probe_mean(d, m, g, Uo, Ao, h->probe[0], h->probe[1], h->probe[2], h->probe[3], probe_p + s, st),
              "probe");
   }
   if (rec) {
@@ -652,8 +652,7 @@ int jb_set_spacing(jb_handle* h, double dx, double dy) {
 
 int jb_set_probe(jb_handle* h, int x0, int y0, int wx, int wy) {
   if (!h) return JB_ERR_ARG;
-  if (h->dim != 2 || x0 < 0 || y0 < 0 || wx < 0 || wy < 0 || x0 + wx > h->grid.nx || y0 + wy > h->grid.ny ||
-      wx * wy > 1024)
+  if (x0 < 0 || y0 < 0 || wx < 0 || wy < 0 || x0 + wx > h->grid.nx || y0 + wy > h->grid.ny || wx * wy > 1024)
     return set_err(h, JB_ERR_ARG, "probe outside the grid (or over 1024 cells)");
   h->probe[0] = x0;
   h->probe[1] = y0;
@@ -679,11 +678,12 @@ int jb_advance_ex(jb_handle* h, const double* U, const double* aux, double* U_ou
 }
 
 // Multiplicity of every cell in the reference's padded array (periodic pad
-// of both axes, then the four sides; corners keep the periodic wrap): how
-// many padded entries copy it.  The ghosts of a pressure-outlet side are
-// not copies and count as entries of their own (in the adjoint kernels).
-static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mult) {
-  const int nx = g.nx, ny = g.ny;
+// of both axes, then the four sides; corners keep the periodic wrap; 1D:
+// the x axis alone): how many padded entries copy it.  The ghosts of a
+// pressure-outlet side are not copies and count as entries of their own (in
+// the adjoint kernels).
+static void padded_multiplicity(int dim, const jb_grid& g, std::vector<unsigned char>& mult) {
+  const int nx = g.nx, ny = g.ny, pad_y = dim == 2 ? 3 : 0;
   mult.assign((size_t)nx * ny, 0);
   auto per = [](int c, int n) { return c < 0 ? n - 1 + c : (c >= n ? c - n + 1 : c); };
   auto side = [](int c, int n, int kind, bool& ok) {
@@ -698,7 +698,7 @@ static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mu
     }
   };
   for (int x = -3; x < nx + 3; ++x)
-    for (int y = -3; y < ny + 3; ++y) {
+    for (int y = -pad_y; y < ny + pad_y; ++y) {
       const bool xin = x >= 0 && x < nx, yin = y >= 0 && y < ny;
       int sx = x, sy = y;
       bool ok = true;
@@ -717,12 +717,11 @@ static void padded_multiplicity(const jb_grid& g, std::vector<unsigned char>& mu
 // What jb_adjoint_step differentiates; checked when the workspace is reserved
 // and again at every step (the flux scheme can change in between).
 static int adj_supported(jb_handle* h) {
-  if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
   if (h->grid.scheme != JB_FLUX_LF || h->grid.visc || h->grid.recon != JB_RECON_WENO5)
     return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint differentiates the inviscid LF / WENO5-JS path");
   if (h->xch || h->grid.bc[0] == JB_BC_HALO || h->grid.bc[1] == JB_BC_HALO)
     return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is single-domain (no x slabs)");
-  for (int s = 0; s < 4; ++s)
+  for (int s = 0; s < 2 * h->dim; ++s)
     if (h->grid.bc[s] == JB_BC_RDC_INJECTOR)
       return set_err(h, JB_ERR_UNSUPPORTED,
                      "the adjoint supports periodic, slip, no-slip, zero-gradient and pressure-outlet sides");
@@ -735,10 +734,10 @@ int jb_adjoint_reserve(jb_handle* h) {
   if (int rc = adj_supported(h)) return rc;
   const jb_grid& g = h->grid;
   const size_t nc = (size_t)g.ncell, nU = (size_t)g.nv * nc;
-  const size_t nsc = jb::adj::flux_scratch_doubles(g);
+  const size_t nsc = jb::adj::flux_scratch_doubles(h->dim, g);
   const size_t n = 2 * nU + 12 * nc + nsc + jb::adj::RED_N;
   std::vector<unsigned char> mult;
-  padded_multiplicity(g, mult);
+  padded_multiplicity(h->dim, g, mult);
   cudaError_t e = cudaMalloc(&h->adj_ws, sizeof(double) * n);
   if (e == cudaSuccess) e = cudaMalloc(&h->adj_mult, nc);
   if (e == cudaSuccess) e = cudaMemset(h->adj_ws, 0, sizeof(double) * n);
@@ -788,20 +787,21 @@ int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, do
   JB_TRY(cudaMemsetAsync(red, 0, sizeof(double) * jb::adj::RED_N, st), "reduction clear");
   // loss term of this step, the final temperature solve; primitives and tie
   // counts of the three stage states
-  JB_TRY(jb::adj::vjp_begin(m, g, U4, A4, pp_bar, h->probe, Ubar, Abar, rec, P, mult, slots, c_cfl, red, sc, st),
+  const int d = h->dim;
+  JB_TRY(jb::adj::vjp_begin(d, m, g, U4, A4, pp_bar, h->probe, Ubar, Abar, rec, P, mult, slots, c_cfl, red, sc, st),
          "adjoint begin");
   // chemistry (and update_aux of U3): B1 = Ubar3
-  JB_TRY(jb::adj::chem_vjp(m, g, W3, A3, Ubar, B1, slot_dt, red + jb::adj::RED_DTB, lnA_bar, st), "chemistry");
+  JB_TRY(jb::adj::chem_vjp(d, m, g, W3, A3, Ubar, B1, slot_dt, red + jb::adj::RED_DTB, lnA_bar, st), "chemistry");
   // stage 3: U3 = 1/3 U + 2/3 (U2 + dt L(U2, aux2)); B2 = Ubar2, Ubar = 1/3 B1
-  JB_TRY(jb::adj::flux_stage(m, g, W2, A2, P + 8 * nc, B1, 2.0 / 3.0, slots, 2, 0.0, mult, red, dt_bar, sc, B2, false,
+  JB_TRY(jb::adj::flux_stage(d, m, g, W2, A2, P + 8 * nc, B1, 2.0 / 3.0, slots, 2, 0.0, mult, red, dt_bar, sc, B2, false,
                              nullptr, Ubar, 1.0 / 3.0, false, st),
          "stage 3");
   // stage 2: U2 = 3/4 U + 1/4 (U1 + dt L(U1, aux1)); B1 = Ubar1, Ubar += 3/4 B2
-  JB_TRY(jb::adj::flux_stage(m, g, W1, A1, P + 4 * nc, B2, 0.25, slots, 1, 0.0, mult, red, dt_bar, sc, B1, false,
+  JB_TRY(jb::adj::flux_stage(d, m, g, W1, A1, P + 4 * nc, B2, 0.25, slots, 1, 0.0, mult, red, dt_bar, sc, B1, false,
                              nullptr, Ubar, 0.75, true, st),
          "stage 2");
   // stage 1: U1 = U + dt L(U, aux), with alpha 1 and the CFL time step
-  JB_TRY(jb::adj::flux_stage(m, g, Un, An, P, B1, 1.0, slots, 0, c_cfl, mult, red, dt_bar, sc, Ubar, true, Abar,
+  JB_TRY(jb::adj::flux_stage(d, m, g, Un, An, P, B1, 1.0, slots, 0, c_cfl, mult, red, dt_bar, sc, Ubar, true, Abar,
                              nullptr, 0.0, false, st),
          "stage 1");
   return JB_OK;
@@ -810,8 +810,7 @@ int jb_adjoint_step(jb_handle* h, const double* rec, const double* rec_slots, do
 int jb_state_from_PTY_vjp(jb_handle* h, const double* P, const double* T, const double* Y, const double* Ubar,
                           const double* Abar, double* Tbar, void* stream) {
   if (!h || !P || !T || !Y || !Ubar || !Abar || !Tbar) return set_err(h, JB_ERR_ARG, "null pointer");
-  if (h->dim != 2) return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is implemented for 2D grids");
-  JB_TRY(jb::adj::init_vjp(h->mech, h->grid.ncell, P, T, Y, Ubar, Abar, Tbar, (cudaStream_t)stream), "init vjp");
+  JB_TRY(jb::adj::init_vjp(h->dim, h->mech, h->grid.ncell, P, T, Y, Ubar, Abar, Tbar, (cudaStream_t)stream), "init vjp");
   return JB_OK;
 }
 

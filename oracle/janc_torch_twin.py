@@ -1,5 +1,7 @@
-"""Torch float64 autograd twin of the reference's 2D step: the stand-in for
-``jax.grad`` of JANC (``src/janc_v2``), which cannot run here (no JAX).
+"""Torch float64 autograd twin of the reference's 2D and 1D step: the
+stand-in for ``jax.grad`` of JANC (``src/janc_v2``), which cannot run here
+(no JAX).  1D arrays are (nv, nx) with nv = 11 (solver_1D/*), 2D arrays
+(nv, nx, ny) with nv = 12 (solver_2D/*).
 
 TEST INFRASTRUCTURE ONLY.  Only ``tests/`` may import this module; it is the
 checker of the hand-written adjoint, never part of the product.
@@ -140,21 +142,30 @@ class _GetT(torch.autograd.Function):
         return gg * dgamma_dT * dT_de + gT * dT_de, gg * dgamma_dY + gT * dT_dY, None, None
 
 
+def _nY(U):
+    return 3 if U.ndim == 2 else 4
+
+
 def update_aux(tw, U, aux):
+    """solver_2D/aux_func.py:21-29, solver_1D/aux_func.py:21-28"""
     rho = U[0:1]
     u = U[1:2] / rho
-    v = U[2:3] / rho
-    e = U[3:4] / rho - 0.5 * (u ** 2 + v ** 2)
-    Y = U[4:] / rho
+    if U.ndim == 2:
+        e = U[2:3] / rho - 0.5 * (u ** 2)
+    else:
+        v = U[2:3] / rho
+        e = U[3:4] / rho - 0.5 * (u ** 2 + v ** 2)
+    Y = U[_nY(U):] / rho
     return _GetT.apply(e, Y, aux[1:2], tw)
 
 
 def prims(tw, U, aux):
+    """U_to_prim (v = 0 in 1D)"""
     gamma, T = aux[0:1], aux[1:2]
     rho = U[0:1]
     u = U[1:2] / rho
-    v = U[2:3] / rho
-    Y = U[4:] / rho
+    v = U[2:3] / rho if U.ndim == 3 else torch.zeros_like(u)
+    Y = U[_nY(U):] / rho
     R = get_R(tw, Y)
     p = rho * R * T
     a = torch.sqrt(gamma * p / rho)
@@ -175,11 +186,12 @@ def get_gibbs(tw, T):
 
 
 def reaction_source_terms(tw, U, aux, dt, lnA_offset=None):
-    """reaction_model.py:91-193 (2D); lnA_offset (19) scales A_i by exp()."""
+    """reaction_model.py:91-193; lnA_offset (19) scales A_i by exp()."""
     nd = U.ndim - 1
+    nY = _nY(U)
     nr, nreac = tw.nr, tw.A.shape[0]
     rho = U[0:1]
-    Y = fill_Y(U[4:] / rho)
+    Y = fill_Y(U[nY:] / rho)
     rhoY = rho * Y
     T = aux[1:2]
     X = rhoY / _ex(tw.M, nd)
@@ -221,17 +233,18 @@ def reaction_source_terms(tw, U, aux, dt, lnA_offset=None):
     drhoY = torch.movedim(x[..., 0], -1, 0)
     dY = drhoY / rho
     dY = torch.clamp(dY, -Y[0:-1], 1 - Y[0:-1])
-    return torch.cat([torch.zeros_like(U[:4]), rho * dY], 0)
+    return torch.cat([torch.zeros_like(U[:nY]), rho * dY], 0)
 
 
 # ------------------------------------------------------------------ flux
 def _pressure_outlet_state(tw, state, gamma, T, normal_vel):
-    """boundary_conditions_2D/pressure_outlet.py:5-22 (janc_oracle's
+    """boundary_conditions_{1D,2D}/pressure_outlet.py:5-22 (janc_oracle's
     _pressure_outlet_state in torch)."""
+    two_d = state.ndim == 3
     rho = state[0:1]
     u = state[1:2] / rho
-    v = state[2:3] / rho
-    Y = state[4:] / rho
+    v = state[2:3] / rho if two_d else None
+    Y = state[_nY(state):] / rho
     R = get_R(tw, Y)
     p = rho * (R * T)
     a = torch.sqrt(gamma * p / rho)
@@ -241,14 +254,18 @@ def _pressure_outlet_state(tw, state, gamma, T, normal_vel):
     p_c = torch.where(mask, Pb * torch.ones_like(p), p)
     T_c = torch.where(mask, p_c / (rho_c * R), T)
     _, gamma_c, h_c, _, _ = get_thermo(tw, T_c, Y)
-    Ub = torch.cat([rho_c, rho_c * u, rho_c * v, rho_c * h_c - p_c + 0.5 * rho_c * (u ** 2 + v ** 2),
-                    rho_c * Y], 0)
+    if two_d:
+        Ub = torch.cat([rho_c, rho_c * u, rho_c * v, rho_c * h_c - p_c + 0.5 * rho_c * (u ** 2 + v ** 2),
+                        rho_c * Y], 0)
+    else:
+        Ub = torch.cat([rho_c, rho_c * u, rho_c * h_c - p_c + 0.5 * rho_c * (u ** 2), rho_c * Y], 0)
     return Ub, torch.cat([gamma_c, T_c], 0)
 
 
 def _bc_side(tw, kind, side, Ub, auxb):
     ax = 1 if side in "LR" else 2
     lo = side in "LB"
+    shp = (-1,) + (1,) * (Ub.ndim - 1)
 
     def take(a, j):
         return a.narrow(ax, j if j >= 0 else a.shape[ax] + j, 1)
@@ -259,8 +276,8 @@ def _bc_side(tw, kind, side, Ub, auxb):
         A = torch.cat([take(auxb, j) for j in order], ax)
         if kind == "no_slip_wall":
             sgn = torch.ones(Ub.shape[0], dtype=Ub.dtype, device=Ub.device)
-            sgn[1:3] = -1
-            U = U * sgn.reshape(-1, 1, 1)
+            sgn[1:3 if Ub.ndim == 3 else 2] = -1
+            U = U * sgn.reshape(shp)
         return U, A
     if kind == "slip_wall":
         j = 0 if lo else -1
@@ -268,7 +285,7 @@ def _bc_side(tw, kind, side, Ub, auxb):
         A = torch.cat([take(auxb, j)] * 3, ax)
         sgn = torch.ones(Ub.shape[0], dtype=Ub.dtype, device=Ub.device)
         sgn[1 if side in "LR" else 2] = -1
-        return U * sgn.reshape(-1, 1, 1), A
+        return U * sgn.reshape(shp), A
     if kind == "pressure_outlet":
         j = 0 if lo else -1
         st, ga, Tt = take(Ub, j), take(auxb[0:1], j), take(auxb[1:2], j)
@@ -282,6 +299,19 @@ def _bc_side(tw, kind, side, Ub, auxb):
 
 
 def boundary_conditions(tw, U, aux):
+    if U.ndim == 2:  # boundary.py:120-126 (1D): periodic pad, then left, right
+        f = torch.cat([U, aux], 0)
+        f = torch.cat([f[:, -4:-3], f[:, -3:-2], f[:, -2:-1], f, f[:, 1:2], f[:, 2:3], f[:, 3:4]], 1)
+        Up, Ap = f[:-2].clone(), f[-2:].clone()
+        for s, key, src, dst in (("L", "left_boundary", slice(3, 6), slice(0, 3)),
+                                 ("R", "right_boundary", slice(-6, -3), slice(-3, None))):
+            kind = tw.bc[key]
+            if kind == "periodic":
+                continue
+            Ug, Ag = _bc_side(tw, kind, s, Up[:, src].clone(), Ap[:, src].clone())
+            Up[:, dst] = Ug
+            Ap[:, dst] = Ag
+        return Up, Ap
     f = torch.cat([U, aux], 0)
     f = torch.cat([f[:, -4:-3], f[:, -3:-2], f[:, -2:-1], f, f[:, 1:2], f[:, 2:3], f[:, 3:4]], 1)
     f = torch.cat([f[:, :, -4:-3], f[:, :, -3:-2], f[:, :, -2:-1], f, f[:, :, 1:2], f[:, :, 2:3], f[:, :, 3:4]], 2)
@@ -332,6 +362,16 @@ def _faces(q, axis, lo, hi):
 
 
 def total_flux(tw, Up, Ap):
+    if Up.ndim == 2:  # solver_1D/flux.py flux_splitting with LF and WENO5-JS
+        rho, u, v, Y, p, a = prims(tw, Up, Ap)
+        um = torch.amax(torch.abs(u) + a)
+        F = torch.cat([rho * u, rho * u ** 2 + p, u * (Up[2:3] + p), rho * u * Y], 0)
+        Fp, Fm = 0.5 * (F + um * Up), 0.5 * (F - um * Up)
+        n = Up.shape[1]
+        L = _weno_L(*[Fp[:, k:n - 5 + k] for k in range(5)])
+        R = _weno_R(*[Fm[:, 1 + k:n - 4 + k] for k in range(5)])
+        Fx = L + R
+        return -(Fx[:, 1:] - Fx[:, :-1]) / tw.dx
     rho, u, v, Y, p, a = prims(tw, Up, Ap)
     rhoE = Up[3:4]
     um = torch.amax(torch.abs(u) + a)
@@ -363,6 +403,8 @@ def flux_func(tw, U, aux, dt):
 def cfl_dt(tw, U, aux):
     _, u, v, _, _, a = prims(tw, U, aux)
     sx = torch.abs(u) + a
+    if U.ndim == 2:  # CFL_1D
+        return tw.cfl * torch.amin(tw.dx / sx)
     sy = torch.abs(v) + a
     return tw.cfl * torch.amin(1 / (sx / tw.dx + sy / tw.dy))
 
@@ -384,14 +426,19 @@ def state_from_PTY(tw, P, T, Y):
     rho = P / (R * T)
     E = rho * h - P
     z = torch.zeros_like(T)
-    U = torch.cat([rho, rho * z, rho * z, E, rho * Y], 0)
+    if T.ndim == 2:
+        U = torch.cat([rho, rho * z, E, rho * Y], 0)
+    else:
+        U = torch.cat([rho, rho * z, rho * z, E, rho * Y], 0)
     return U, torch.cat([gamma, T], 0)
 
 
 def probe_pressure(tw, U, aux, probe):
-    """Mean pressure over the probe cells (x0, y0, wx, wy)."""
+    """Mean pressure over the probe cells (x0, y0, wx, wy); 1D: (x0, 0, wx, 1)."""
     x0, y0, wx, wy = probe
     _, _, _, _, p, _ = prims(tw, U, aux)
+    if U.ndim == 2:
+        return p[0, x0:x0 + wx].mean()
     return p[0, x0:x0 + wx, y0:y0 + wy].mean()
 
 
