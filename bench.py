@@ -48,6 +48,11 @@ the time of the backward pass (recomputation included) over the time of the
 forward pass; the gradients are checked against central finite differences
 of the float64 forward (h = 1e-6 relative, 16 seeded unit directions each).
 
+Block AMR (--workload amr): one refinement level of 64 x 16 blocks of 20 x 20
+cells of the channel physics through the drop-in AMR_Simulator, with a
+device block layer standing in for the external jaxamr package (also the
+default line's configs.amr).
+
 Multi-GPU: the path does not shard in this build (replicas only): each rank
 advances its own copy of the workload; value = total cells x steps / max time.
 """
@@ -75,11 +80,11 @@ BYTES_STEP_PER_CELL = 864 + 224  # fused-step minimum + separate chemistry pass 
 BYTES_FLUX_STAGE_PER_CELL = 288  # one RK stage of the fused minimum: (224 + 320 + 320) / 3
 # DRAM bytes per cell measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum,
 # each launch cold) on the 1024x256 channel, mixed precision, with this tree's
-# kernels: one RK stage 2/3 (k_sweep_x 27.34 + 0.00 MB, k_flux_y_rk 67.19 +
-# 1.65 MB) and one chemistry launch (27.39 + 7.58 MB); the capture and its
+# kernels: one RK stage 2/3 (k_sweep_x 27.35 + 0.00 MB, k_flux_y_rk 67.19 +
+# 2.66 MB) and one chemistry launch (27.39 + 3.51 MB); the capture and its
 # command are in profiles/launches_channel1024x256_mixed.md.  Per cell-step of
 # the persistent ensemble kernel: profiles/k_ensemble_64tubes.md.
-TRAFFIC_PER_CELL = {"flux": 366.9, "chem": 133.4}
+TRAFFIC_PER_CELL = {"flux": 370.8, "chem": 117.9}
 TRAFFIC_SOURCE = "profiles/launches_channel1024x256_mixed.md"
 TRAFFIC_ENS_PER_CELL_STEP = 1125.0
 
@@ -167,6 +172,13 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_first(self, timeout=5.0):
+        """Wait until the sampler has reported once (nvidia-smi's start-up,
+        whose driver queries can delay kernel launches, is then over)."""
+        t0 = time.time()
+        while self.proc is not None and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -388,7 +400,8 @@ def _time_path(args, s, U0, aux0, theta, ncell, dist, clocks=None):
     torch.cuda.synchronize()
     if clocks:
         clocks.start()
-        time.sleep(0.3)
+        clocks.wait_first()
+        time.sleep(0.1)
     t_wall0 = time.time()
     graph.replay()
     torch.cuda.synchronize()
@@ -750,7 +763,8 @@ def amr_record(args, steps=10):
         blk = blk0
         clocks = ClockSampler(dev)
         clocks.start()
-        time.sleep(0.3)
+        clocks.wait_first()
+        time.sleep(0.1)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -849,7 +863,8 @@ def adjoint_record(args, dist, ws, N):
         fwd_bwd()
     clocks = ClockSampler(dev)
     clocks.start()
-    time.sleep(0.3)
+    clocks.wait_first()
+    time.sleep(0.1)
     reps = [fwd_bwd() for _ in range(3)]
     clk = clocks.stop()
     f_ms = max_over_ranks(dist, statistics.median(r[0] for r in reps))
@@ -971,8 +986,85 @@ def adjoint_record(args, dist, ws, N):
         # segment and 8 adjoint kernels per step (begin, chemistry VJP, and a
         # sweep and a merge per RK stage)
         "gpu_launches": 27 * N + 4 * ((N + ADJ_K - 1) // ADJ_K), "clocks": clk,
+        "tube_1d": adjoint_1d_record(args, dist, N),
     }
     return line
+
+
+def adjoint_1d_record(args, dist, N):
+    """The 1D form of the adjoint workload: config-0 physics (2000 cells over
+    0.1 m, the first 40 at 30 atm / 3000 K with seeded +-5 % noise, 1 %
+    seeded noise on the ambient temperature, slip wall left, zero gradient
+    right), CFL 0.1, N steps checkpointed every 20, loss = sum_n dt_n * mean
+    p over cells 1600..1603; cost ratio and central finite differences
+    (h = 1e-6 relative, 8 seeded unit directions each for T and ln A)."""
+    import numpy as np
+    import torch
+    from janc_b200 import mechanism as jm
+    from janc_b200.adjoint import Trajectory, probe_trajectory
+    from janc_b200.solver import Solver
+    n, dx = 2000, 0.1 / 2000
+    mech = jm.load()
+    rng = np.random.default_rng(8)
+    P = np.full((1, n), 101325.0)
+    T = 300.0 * (1 + 0.01 * rng.standard_normal((1, n)))
+    P[0, :40] = 30 * 101325.0
+    T[0, :40] = 3000.0 * (1 + 0.05 * rng.uniform(-1, 1, 40))
+    Y = np.ascontiguousarray(np.tile(jm.stoichiometric_Y(mech, 1.0)[:, None], (1, n)))
+    s = Solver(1, n, None, dx, None, {"left_boundary": "slip_wall", "right_boundary": "zero_gradient"},
+               mech, precision="fp64")
+    traj = Trajectory(s, 0.1, (1600, 4), checkpoint=ADJ_K)
+    cu = lambda a: torch.as_tensor(a, dtype=torch.float64, device="cuda")
+    Pc, Tc, Yc = cu(P), cu(T), cu(Y)
+    U0, a0 = s.state_from_PTY(Pc, Tc, Yc)
+
+    def fwd_bwd():
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record()
+        _, _, dts, pps, ckpts = traj.run(U0, a0, N)
+        ev[1].record()
+        traj.backward(ckpts, N, pps, dts)
+        ev[2].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    for _ in range(3):
+        fwd_bwd()
+    reps = [fwd_bwd() for _ in range(3)]
+    f_ms = max_over_ranks(dist, statistics.median(r[0] for r in reps))
+    b_ms = max_over_ranks(dist, statistics.median(r[1] for r in reps))
+    Tg = Tc.clone().requires_grad_()
+    lg = torch.zeros(19, dtype=torch.float64, device="cuda", requires_grad=True)
+    dts, pps = probe_trajectory(traj, Pc, Tg, Yc, lg, N)
+    (dts * pps).sum().backward()
+    gT, gA = Tg.grad.cpu().numpy(), lg.grad.cpu().numpy()
+
+    def loss_at(Tn, dA):
+        traj.set_log_A_offset(dA)
+        U, a = s.state_from_PTY(Pc, Tn, Yc)
+        _, _, d, p, _ = traj.run(U, a, N)
+        return float((d * p).sum())
+    h, rng_d = 1e-6, np.random.default_rng(13)
+    errT, errA = [], []
+    for _ in range(8):
+        d = rng_d.standard_normal(T.shape)
+        d /= np.linalg.norm(d)
+        f = (loss_at(cu(T * (1 + h * d)), None) - loss_at(cu(T * (1 - h * d)), None)) / (2 * h)
+        errT.append(abs(f - float((gT * T * d).sum())) / abs(f))
+        e = rng_d.standard_normal(19)
+        e /= np.linalg.norm(e)
+        f = (loss_at(Tc, h * e) - loss_at(Tc, -h * e)) / (2 * h)
+        errA.append(abs(f - float((gA * e).sum())) / abs(f))
+    traj.set_log_A_offset(None)
+    return {"workload": "1D tube, 2000 cells (config-0 physics, 1 % noise on the ambient temperature), CFL 0.1, "
+                        f"{N} steps, checkpoint every {ADJ_K}; loss = sum_n dt_n * mean p over cells 1600..1603",
+            "value": b_ms / f_ms, "unit": "adjoint/forward cost", "forward_ms_per_step": f_ms / N,
+            "backward_ms_per_step": b_ms / N,
+            "finite_difference_check": {"h_rel": h,
+                                        "T": {"directions": len(errT), "max_rel_err": max(errT),
+                                              "median_rel_err": statistics.median(errT)},
+                                        "lnA": {"directions": len(errA), "max_rel_err": max(errA),
+                                                "median_rel_err": statistics.median(errA)}}}
 
 
 # ------------------------------------------------------------ ensemble arm
@@ -1046,7 +1138,8 @@ def ensemble_record(args, dist, rank, ws, K, precision, with_cpu):
         dist.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
-    time.sleep(0.3)
+    clocks.wait_first()
+    time.sleep(0.1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_wall0 = time.time()
     e0.record()
@@ -1318,7 +1411,7 @@ def main():
                     help="channel: skip the sub-records of the other workloads (rdc, ensemble, adjoint)")
     ap.add_argument("--sub-steps", type=int, default=200,
                     help="steps of the ensemble and adjoint sub-records")
-    ap.add_argument("--workload", default="channel", choices=["channel", "rdc", "ensemble", "adjoint"])
+    ap.add_argument("--workload", default="channel", choices=["channel", "rdc", "ensemble", "adjoint", "amr"])
     ap.add_argument("--viscous", action="store_true",
                     help="channel workload with the laminar viscous fluxes")
     ap.add_argument("--flux", default="LF", choices=["LF", "SW", "HLLC", "AUSMPW_plus"],
@@ -1343,6 +1436,8 @@ def main():
         run_ensemble(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "amr":
+        print(json.dumps(amr_record(args, steps=args.steps)), flush=True)
     else:
         run_ours(args)
 
