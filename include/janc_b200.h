@@ -276,7 +276,8 @@ const char* jb_last_error(const jb_handle* h);
 
 /* ------------------------------------------------------------------------
  * Reverse mode (the adjoint), 2D and 1D grids with periodic, slip, no-slip,
- * zero-gradient or pressure-outlet sides (back pressure Pb held fixed).
+ * zero-gradient or pressure-outlet sides (back pressure Pb held fixed) and
+ * the rotating-detonation injector on the bottom side (2D; Yinj held fixed).
  * The reference gets these derivatives from jax.grad
  * through advance_one_step and the CFL time step (set_simulator.py:117-122,
  * 420-447; 1D: CFL min dx / (|u| + a)) with get_T's custom VJP

@@ -554,8 +554,11 @@ __device__ __forceinline__ bool tied(double v, double ref) { return fabs(v - ref
 // boundary position), and their adjoints (flux, LF term, wave speeds) flow
 // back into the boundary cell through the VJP of the outlet state (ogb).
 //   og [stage][side][OG_F][lstrip]: ghost U (nv), then u, v, p at OG_U..OG_P
-//   ogb[side][OG_B][lstrip]: the boundary cell's U adjoint (nv), T adjoint at OG_T
-constexpr int OG_F = 15, OG_B = 13, OG_U = 12, OG_V = 13, OG_P = 14, OG_T = 12;
+//   ogb[side][OG_B][lstrip]: the boundary cell's U adjoint (nv), T adjoint at
+//   OG_T, gamma adjoint at OG_G (the blocked injector copies the cell's gamma)
+// The rotating-detonation injector of the bottom side (2D) is handled the same
+// way: its 3 ghost layers hold the injector state of the boundary cell.
+constexpr int OG_F = 15, OG_B = 14, OG_U = 12, OG_V = 13, OG_P = 14, OG_T = 12, OG_G = 13;
 
 __device__ __forceinline__ size_t og_idx(const Grid& g, int stage, int side, int f, int pos) {
   return (((size_t)stage * 4 + side) * OG_F + f) * g.lstrip + pos;
@@ -564,6 +567,12 @@ __device__ __forceinline__ size_t og_idx(const Grid& g, int stage, int side, int
 __device__ __forceinline__ bool outlet_side(const Grid& g, int side) {
   return g.bc[side] == JB_BC_PRESSURE_OUTLET;
 }
+
+// a side whose ghosts are states of their own (pressure outlet, injector)
+__device__ __forceinline__ bool strip_side(const Grid& g, int side) {
+  return g.bc[side] == JB_BC_PRESSURE_OUTLET || (side == 2 && g.bc[side] == JB_BC_RDC_INJECTOR);
+}
+
 
 // Boundary position t in [0, 2 ny + 2 nx): sides 0 and 1 (x = 0, nx - 1) by
 // y, then sides 2 and 3 (y = 0, ny - 1) by x; side -1 past the end.
@@ -587,6 +596,22 @@ __device__ __forceinline__ void boundary_pos(const Grid& g, int t, int& side, in
 __device__ __forceinline__ double outlet_un(const double* q, int side) {
   const double un = (side < 2 ? q[1] : q[2]) / q[0];
   return (side == 0 || side == 2) ? -un : un;
+}
+
+// The ghost state (U, gamma, T) of strip side `side` at boundary cell q.
+template <int DIM>
+__device__ __forceinline__ void strip_state(const MP& m, const Grid& g, int side, int pos, const double* q,
+                                            double gamma, double T, double* gs) {
+  if constexpr (DIM == 2) {
+    if (g.bc[side] == JB_BC_RDC_INJECTOR) {
+      double Yi[NR];
+#pragma unroll
+      for (int k = 0; k < NR; ++k) Yi[k] = g.Yinj[k * g.nx + pos];
+      injector_state(m, q, gamma, T, Yi, g.inj_block_p, gs);
+      return;
+    }
+  }
+  pressure_outlet_state<DIM>(m, q, gamma, T, outlet_un(q, side), g.Pb, gs);
 }
 
 // ub, Tb += the VJP of the outlet state (pressure_outlet.py:5-22) of boundary
@@ -671,6 +696,119 @@ __device__ void outlet_vjp(const MP& m, const double* q, double gamma, double T,
   }
   ub[0] += rb;
   Tb += Tl;
+}
+
+// ub, Tb, gb += the VJP of the rotating-detonation injector state of boundary
+// cell q with aux (gamma, T) (examples/janc_basic_example2.ipynb
+// bottom_boundary + inj_model, after Fievisohn et al. 2017), given the
+// adjoints of the ghost U (ob), its gamma (gcb) and its T (Tcb).  The
+// bisection's Mach number, the blocked / open switch (p >= block_p) and Yinj
+// carry no derivative (comparisons and jnp.where selections of constants in
+// the reference).  Open: rho_c = p / (R_i T_i), u_c = 0, v_c = V3,
+// T_c = T_i = p / (R_i rho_i), rho_i = MFC / V3 / A3, V3 = -B + sqrt(B^2 - 2C),
+// B = g/(g-1) p A3 / MFC, and the ghost energy rho_c h_i - p + rho_c V3^2 / 2
+// with gamma_c = cp(T_i) / (cp(T_i) - R_i).  Blocked: the cell's rho, u, -v,
+// T and gamma, the ghost energy rho h(T) - p + rho |u|^2 / 2.
+__device__ void injector_vjp(const MP& m, const double* q, double gamma, double T, const double* Yinj8,
+                             double block_p, const double* ob, double gcb, double Tcb, double* ub, double& Tb,
+                             double& gb) {
+  (void)gamma;
+  const double rho = q[0], ri = 1.0 / rho;
+  const double u = q[1] * ri, v = q[2] * ri;
+  double Y8[NR], Yf[NS], Y8b[NR];
+  cell_Y<2>(q, ri, Y8, Yf);
+  const double R = get_R(m, Yf);
+  const double p = rho * R * T;
+  double rb = 0.0, pb = 0.0;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) Y8b[k] = 0.0;
+  if (p >= block_p) {
+    double h = 0.0, cp = 0.0, hk[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      const bool lo = T < m.Tcr[k];
+      hk[k] = lo ? poly6(m.h_lo[k], T) : poly6(m.h_hi[k], T);
+      const double cpk = lo ? poly5(m.cp_lo[k], T) : poly5(m.cp_hi[k], T);
+      h += hk[k] * Yf[k];
+      cp += cpk * Yf[k];
+    }
+    // ghost = [rho, rho u, rho (-v), rho h - p + rho (u^2 + v^2) / 2, rho Y8]
+    const double ubl = ob[1] * rho + ob[3] * rho * u;
+    const double vbl = -ob[2] * rho + ob[3] * rho * v;
+    rb += ob[0] + ob[1] * u - ob[2] * v + ob[3] * (h + 0.5 * (u * u + v * v));
+    const double hb = ob[3] * rho;
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      rb += ob[4 + k] * Y8[k];
+      Y8b[k] += ob[4 + k] * rho + hb * (hk[k] - hk[NR]);
+    }
+    Tb += hb * cp + Tcb;
+    pb -= ob[3];
+    gb += gcb;
+    ub[1] += ubl * ri;
+    ub[2] += vbl * ri;
+    rb -= (ubl * u + vbl * v) * ri;
+  } else {
+    double Yi[NS];
+    fill_Y(Yinj8, Yi);
+    const double Ri = get_R(m, Yi);
+    const double gam = 1.29, A1 = 1.0, A3 = 5.0;
+    const double C0 = sqrt(gam * Ri * 1.0);
+    const double gh = (gam - 1.0) / 2.0;
+    const double e1 = -gam / (gam - 1.0), e2 = -(gam + 1.0) / 2.0 / (gam - 1.0), gg = gam / (gam - 1.0);
+    const double C = -gam / (gam - 1.0) * Ri * 1.0;
+    // the bisection of the forward (injector_state), for the last M's MFC
+    double M1 = 0.0, M2 = 1.0, MFC = 0.0, V3 = 0.0;
+    for (int it = 0; it < 20; ++it) {
+      const double M = 0.5 * (M1 + M2);
+      const double base = 1.0 + gh * (M * M);
+      const double P1 = 1.0 * pow(base, e1);
+      const double V1 = M * pow(base, -0.5) * C0;
+      MFC = 1.0 * sqrt(gam / Ri) * M * pow(base, e2);
+      const double B = gg * p * A3 / MFC;
+      V3 = (-B + sqrt(B * B - 2.0 * C)) / 1.0;
+      const double P2 = (MFC * (V3 - V1) - P1 * A1 + p * A3) / (A3 - A1);
+      M2 = (P2 >= P1) ? M : M2;
+      M1 = (P2 < P1) ? M : M1;
+    }
+    const double B = gg * p * A3 / MFC;
+    const double sq = sqrt(B * B - 2.0 * C);
+    const double dV3 = (-1.0 + B / sq) * (gg * A3 / MFC);  // dV3/dp
+    const double rho_i = MFC / V3 / A3;
+    const double drho_i = -rho_i / V3 * dV3;
+    const double T_i = p / (Ri * rho_i);
+    const double dT_i = 1.0 / (Ri * rho_i) - T_i / rho_i * drho_i;
+    double h_i = 0.0, cp_i = 0.0, dcp_i = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      const bool lo = T_i < m.Tcr[k];
+      h_i += (lo ? poly6(m.h_lo[k], T_i) : poly6(m.h_hi[k], T_i)) * Yi[k];
+      cp_i += (lo ? poly5(m.cp_lo[k], T_i) : poly5(m.cp_hi[k], T_i)) * Yi[k];
+      dcp_i += (lo ? poly4(m.dcp_lo[k], T_i) : poly4(m.dcp_hi[k], T_i)) * Yi[k];
+    }
+    const double cvi = cp_i - Ri;
+    const double dg_dT = -Ri * dcp_i / (cvi * cvi);
+    const double rho_c = p / (Ri * T_i);
+    const double drho_c = 1.0 / (Ri * T_i) - rho_c / T_i * dT_i;
+    // ghost = [rho_c, 0, rho_c V3, rho_c h_i - p + rho_c V3^2 / 2, rho_c Yinj8]
+    double rcb = ob[0] + ob[2] * V3 + ob[3] * (h_i + 0.5 * (V3 * V3));
+#pragma unroll
+    for (int k = 0; k < NR; ++k) rcb += ob[4 + k] * Yinj8[k];
+    const double V3b = ob[2] * rho_c + ob[3] * rho_c * V3;
+    const double hib = ob[3] * rho_c;
+    pb += -ob[3] + rcb * drho_c + V3b * dV3 + (hib * cp_i + gcb * dg_dT + Tcb) * dT_i;
+  }
+  // p = rho R T, R = sum Y_k / M_k
+  rb += pb * R * T;
+  const double Rb = pb * rho * T;
+  Tb += pb * rho * R;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    Y8b[k] += Rb * (m.invM[k] - m.invM[NR]);
+    ub[4 + k] += Y8b[k] * ri;
+    rb -= Y8b[k] * Y8[k] * ri;
+  }
+  ub[0] += rb;
 }
 
 // ---------------------------------------------------------------------------
@@ -769,13 +907,13 @@ __global__ void __launch_bounds__(128) k_outlet_ghosts(MP m, Grid g, const doubl
   int side, pos, x, y;
   boundary_pos<DIM>(g, blockIdx.x * blockDim.x + threadIdx.x, side, pos, x, y);
   double cx = 0.0, cy = 0.0;
-  if (side >= 0 && outlet_side(g, side)) {
+  if (side >= 0 && strip_side(g, side)) {
     const long long c = (long long)x * g.ny + y;
     const double* S = rec + (long long)st * (nU + 2 * nc);
     double q[NVD], gs[NVD + 2];
 #pragma unroll
     for (int f = 0; f < NVD; ++f) q[f] = S[f * nc + c];
-    pressure_outlet_state<DIM>(m, q, S[nU + c], S[nU + nc + c], outlet_un(q, side), g.Pb, gs);
+    strip_state<DIM>(m, g, side, pos, q, S[nU + c], S[nU + nc + c], gs);
     const Prim<DIM> pr = u_to_prim<DIM>(m, gs, gs[NVD], gs[NVD + 1]);
 #pragma unroll
     for (int f = 0; f < NVD; ++f) og[og_idx(g, st, side, f, pos)] = gs[f];
@@ -1051,14 +1189,14 @@ __global__ void __launch_bounds__(128) k_outlet_vjp(MP m, Grid g, const double* 
   const long long nc = g.ncell;
   int side, pos, x, y;
   boundary_pos<DIM>(g, blockIdx.x * blockDim.x + threadIdx.x, side, pos, x, y);
-  if (side < 0 || !outlet_side(g, side)) return;
+  if (side < 0 || !strip_side(g, side)) return;
   const long long c = (long long)x * g.ny + y;
   double q[NVD], gs[NVD + 2], ob[NVD], fb[NVD];
 #pragma unroll
   for (int f = 0; f < NVD; ++f) q[f] = Uk[f * nc + c];
   const double gamma = Ak[c], T = Ak[nc + c];
   const double un = outlet_un(q, side);
-  pressure_outlet_state<DIM>(m, q, gamma, T, un, g.Pb, gs);
+  strip_state<DIM>(m, g, side, pos, q, gamma, T, gs);
   const int D = side < 2 ? 0 : 1;
   const int nA = D == 0 ? g.nx : g.ny;
   const size_t npad = D == 0 ? (size_t)(g.nx + 6) * g.ny : (size_t)g.nx * (g.ny + 6);
@@ -1090,14 +1228,26 @@ __global__ void __launch_bounds__(128) k_outlet_vjp(MP m, Grid g, const double* 
       (DIM == 2 && cy > 0.0 && tied(sp.sy, bitsd(rs->ay[stage]))) ? red[red_ab(stage, 1)] * 3.0 / cy : 0.0;
   speed_vjp<DIM>(m, gs, gs[NVD], gs[NVD + 1], 1, wx, ob, gcb, Tcb);
   if (DIM == 2) speed_vjp<DIM>(m, gs, gs[NVD], gs[NVD + 1], 2, wy, ob, gcb, Tcb);
-  double ub[NVD], Tb = 0.0;
+  double ub[NVD], Tb = 0.0, gb = 0.0;
 #pragma unroll
   for (int f = 0; f < NVD; ++f) ub[f] = 0.0;
-  outlet_vjp<DIM>(m, q, gamma, T, un, g.Pb, ob, gcb, Tcb, ub, Tb);
+  if constexpr (DIM == 2) {
+    if (g.bc[side] == JB_BC_RDC_INJECTOR) {
+      double Yi[NR];
+#pragma unroll
+      for (int k = 0; k < NR; ++k) Yi[k] = g.Yinj[k * g.nx + pos];
+      injector_vjp(m, q, gamma, T, Yi, g.inj_block_p, ob, gcb, Tcb, ub, Tb, gb);
+    } else {
+      outlet_vjp<DIM>(m, q, gamma, T, un, g.Pb, ob, gcb, Tcb, ub, Tb);
+    }
+  } else {
+    outlet_vjp<DIM>(m, q, gamma, T, un, g.Pb, ob, gcb, Tcb, ub, Tb);
+  }
   double* o = ogb + (size_t)side * OG_B * g.lstrip + pos;
 #pragma unroll
   for (int f = 0; f < NVD; ++f) o[(size_t)f * g.lstrip] = ub[f];
   o[(size_t)OG_T * g.lstrip] = Tb;
+  o[(size_t)OG_G * g.lstrip] = gb;
 }
 
 // One RK stage U' = a Un + b (Uk + dt L(Uk, auxk)), per interior cell of Uk:
@@ -1147,11 +1297,12 @@ __global__ void __launch_bounds__(128, 4) k_stage_merge(
 #pragma unroll 1
     for (int side = 0; side < 2 * DIM; ++side) {
       const bool on = side == 0 ? x == 0 : side == 1 ? x == g.nx - 1 : side == 2 ? y == 0 : y == g.ny - 1;
-      if (!on || !outlet_side(g, side)) continue;
+      if (!on || !strip_side(g, side)) continue;
       const double* o = ogb + (size_t)side * OG_B * g.lstrip + (side < 2 ? y : x);
 #pragma unroll
       for (int f = 0; f < NVD; ++f) ub[f] += o[(size_t)f * g.lstrip];
       Tb += o[(size_t)OG_T * g.lstrip];
+      gb += o[(size_t)OG_G * g.lstrip];
     }
   }
 #pragma unroll
@@ -1255,9 +1406,10 @@ namespace adj {
 
 static inline unsigned blocks_for(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
+// a pressure-outlet side, or the 2D injector side (ghosts that are states of their own)
 static bool has_outlet(int dim, const jb_grid& g) {
   for (int s = 0; s < 2 * dim; ++s)
-    if (g.bc[s] == JB_BC_PRESSURE_OUTLET) return true;
+    if (g.bc[s] == JB_BC_PRESSURE_OUTLET || (dim == 2 && s == 2 && g.bc[s] == JB_BC_RDC_INJECTOR)) return true;
   return false;
 }
 

@@ -722,9 +722,8 @@ static int adj_supported(jb_handle* h) {
   if (h->xch || h->grid.bc[0] == JB_BC_HALO || h->grid.bc[1] == JB_BC_HALO)
     return set_err(h, JB_ERR_UNSUPPORTED, "the adjoint is single-domain (no x slabs)");
   for (int s = 0; s < 2 * h->dim; ++s)
-    if (h->grid.bc[s] == JB_BC_RDC_INJECTOR)
-      return set_err(h, JB_ERR_UNSUPPORTED,
-                     "the adjoint supports periodic, slip, no-slip, zero-gradient and pressure-outlet sides");
+    if (h->grid.bc[s] == JB_BC_RDC_INJECTOR && s != 2)
+      return set_err(h, JB_ERR_UNSUPPORTED, "the injector side of the adjoint is the bottom side (2D)");
   return JB_OK;
 }
 

@@ -21,11 +21,14 @@ reverse mode reproduces what ``jax.grad`` of the reference computes:
   ``jnp.clip`` -> ``torch.clamp``.
 
 Boundaries restated here: the copy types (periodic, slip_wall,
-zero_gradient, no_slip_wall) and pressure_outlet
+zero_gradient, no_slip_wall), pressure_outlet
 (boundary_conditions_2D/pressure_outlet.py:5-66) with the back pressure
 ``Pb`` a constant (its sub/supersonic switch, a ``jnp.where`` in the
 reference, passes gradients to the selected branch only, as
-``torch.where`` does).
+``torch.where`` does), and the rotating-detonation injector of the bottom
+side (examples/janc_basic_example2.ipynb ``bottom_boundary`` + ``inj_model``)
+with ``Yinj`` a constant (its bisection moves constants through
+``jnp.where``, so the Mach number carries no gradient).
 """
 import numpy as np
 import torch
@@ -39,10 +42,12 @@ _EPS, _C1, _C2, _C3 = 1e-6, 1 / 10, 3 / 5, 3 / 10
 class Twin:
     """Mechanism tables as float64 tensors plus the solver configuration."""
 
-    def __init__(self, mech, dx, dy, bc, cfl, device="cpu", Pb=None):
+    def __init__(self, mech, dx, dy, bc, cfl, device="cpu", Pb=None, Yinj=None, inj_block_p=1.0):
         self.m = mech
         self.dx, self.dy, self.bc, self.cfl = dx, dy, bc, cfl
         self.Pb = Pb
+        self.Yinj = None if Yinj is None else torch.as_tensor(np.asarray(Yinj, dtype=np.float64), device=device)
+        self.inj_block_p = inj_block_p
         self.dev = device
         t = lambda a: torch.as_tensor(np.asarray(a, dtype=np.float64), device=device)
         self.M = t(mech.species_M)
@@ -262,6 +267,62 @@ def _pressure_outlet_state(tw, state, gamma, T, normal_vel):
     return Ub, torch.cat([gamma_c, T_c], 0)
 
 
+def _inj_model(tw, p, Y_inj):
+    """inj_model of examples/janc_basic_example2.ipynb (janc_oracle's
+    inj_model in torch)."""
+    A1, A3 = 1, 5
+    A2 = A3 - A1
+    R = get_R(tw, Y_inj)
+    gamma = 1.29
+    C0 = torch.sqrt(gamma * R * 1.0)
+    P3 = p
+    M1 = torch.zeros_like(p)
+    M2 = torch.ones_like(p)
+    for _ in range(20):
+        M = 0.5 * (M1 + M2)
+        P1 = 1.0 * (1 + (gamma - 1) / 2 * M ** 2) ** (-gamma / (gamma - 1))
+        V1 = M * (1 + (gamma - 1) / 2 * M ** 2) ** (-0.5) * C0
+        MFC = A1 * 1.0 / np.sqrt(1.0) * torch.sqrt(gamma / R) * M * (1 + (gamma - 1) / 2 * M ** 2) ** (
+            -(gamma + 1) / 2 / (gamma - 1))
+        A = 0.5
+        B = gamma / (gamma - 1) * P3 * A3 / MFC
+        C = -gamma / (gamma - 1) * R * 1.0
+        V3 = (-B + torch.sqrt(B ** 2 - 4 * A * C)) / (2 * A)
+        P2 = (MFC * (V3 - V1) - P1 * A1 + P3 * A3) / A2
+        M2 = torch.where(P2 >= P1, M, M2)
+        M1 = torch.where(P2 < P1, M, M1)
+    rho_c = MFC / V3 / A3
+    v_c = V3
+    T_c = p / (R * rho_c)
+    _, gamma_c, h_c, _, _ = get_thermo(tw, T_c, Y_inj)
+    return v_c, T_c, h_c, gamma_c
+
+
+def _injector_state(tw, state, aux, Yinj):
+    """bottom_boundary of examples/janc_basic_example2.ipynb on the first
+    interior row (janc_oracle's _injector_state in torch)."""
+    rho, u, v, Y, p, a = prims(tw, state, aux)
+    T = aux[1:2]
+    gamma = aux[0:1]
+    _, _, h, R, _ = get_thermo(tw, T, Y)
+    u_inj = torch.zeros_like(u)
+    v_inj, T_inj, h_inj, g_inj = _inj_model(tw, p, Yinj)
+    R_inj = get_R(tw, Yinj)
+    rho_inj = p / (R_inj * T_inj)
+    blk = p >= tw.inj_block_p
+    rho_c = torch.where(blk, rho, rho_inj)
+    u_c = torch.where(blk, u, u_inj)
+    v_c = torch.where(blk, -v, v_inj)
+    T_c = torch.where(blk, T, T_inj)
+    p_c = p
+    h_c = torch.where(blk, h, h_inj)
+    Y_c = torch.where(blk.expand(Yinj.shape[0], -1, -1), Y, Yinj)
+    g_c = torch.where(blk, gamma, g_inj)
+    Ub = torch.cat([rho_c, rho_c * u_c, rho_c * v_c,
+                    rho_c * h_c - p_c + 0.5 * rho_c * (u_c ** 2 + v_c ** 2), rho_c * Y_c], 0)
+    return Ub, torch.cat([g_c, T_c], 0)
+
+
 def _bc_side(tw, kind, side, Ub, auxb):
     ax = 1 if side in "LR" else 2
     lo = side in "LB"
@@ -286,6 +347,14 @@ def _bc_side(tw, kind, side, Ub, auxb):
         sgn = torch.ones(Ub.shape[0], dtype=Ub.dtype, device=Ub.device)
         sgn[1 if side in "LR" else 2] = -1
         return U * sgn.reshape(shp), A
+    if kind == "rdc_injector":
+        assert side == "B" and Ub.ndim == 3
+        st, au = Ub[:, :, 0:1], auxb[:, :, 0:1]
+        Yinj = tw.Yinj
+        if Yinj.ndim == 1:
+            Yinj = Yinj[:, None, None].expand(-1, Ub.shape[1], 1)
+        Us, As = _injector_state(tw, st, au, Yinj)
+        return torch.cat([Us] * 3, 2), torch.cat([As] * 3, 2)
     if kind == "pressure_outlet":
         j = 0 if lo else -1
         st, ga, Tt = take(Ub, j), take(auxb[0:1], j), take(auxb[1:2], j)

@@ -240,3 +240,25 @@ def test_amr_argument_checks(mech_path):
     # a 1D handle
     h1 = Solver(1, 8, None, 1.0, None, {"left_boundary": "periodic", "right_boundary": "periodic"}, mechp)
     assert lib.jb_amr_update_aux(h1._h, 1, 8, 8, p, p, ctypes.c_void_p(out.data_ptr()), None) == 1
+
+
+@pytest.mark.gpu
+def test_amr_muscl_stages_strict_bitwise(fx, mech, mech_path):
+    """The block stages with MUSCL reconstruction (the handle's
+    interface_reconstruction) against the oracle's block functions with
+    MUSCL (whose MUSCL is pinned to the reference elsewhere), fp64_strict."""
+    from janc_b200.janc.simulation import set_simulator as ss
+    from janc_b200.janc.simulation import time_step as ts
+    ss.AMR_Simulator(_cfg(mech_path, "fp64_strict", recon="MUSCL"))
+    ff, uf, _ = ss.set_rhs("2D", {"is_detailed_chemistry": True}, None, False, True)
+    nbx, nby, bx, by = (int(v) for v in fx["b20_layout"])
+    info = amr_blocks.info(nbx, nby)
+    blk0 = fx["b20_blk0"]
+    ts.set_amr_module(amr_blocks)
+    try:
+        b = _blocks_dev(blk0)
+        got = ts.time_step_dict["TVD_RK3_amr"](1, b, 1e-4, 1e-4, 1e-8, b, info, None, ff, uf).cpu().numpy()
+    finally:
+        ts.set_amr_module(None)
+    ref = jo.tvd_rk3_amr(mech, amr_blocks, 1, blk0, 1e-4, 1e-4, 1e-8, blk0, info, recon="MUSCL")
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
