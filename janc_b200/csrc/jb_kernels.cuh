@@ -1442,7 +1442,7 @@ __device__ __forceinline__ void win_load2(const MP& m, const Grid& g, const doub
 }
 
 #ifndef JB_SX_MINB
-#define JB_SX_MINB 4  // 128 registers: the paired window and WENO fit without spills
+#define JB_SX_MINB 7  // 72 registers: the paired window and WENO still fit without spills
 #endif
 #ifndef JB_SX_PF
 #define JB_SX_PF 1  // cells fetched ahead of the window (a divisor of 6)
@@ -2305,7 +2305,10 @@ __device__ __forceinline__ void chem_cell_step(const MP& m, const Grid& g, const
 
 // CELL: the mixed variant's 2D step (per-cell temperature solve)
 template <int DIM, bool WRITE_S, bool GEN, bool CELL>
-__global__ void __launch_bounds__(128, 3) k_chem(MP m, Grid g, const double* __restrict__ U,
+#ifndef JB_CHEM_MINB
+#define JB_CHEM_MINB 3
+#endif
+__global__ void __launch_bounds__(128, JB_CHEM_MINB) k_chem(MP m, Grid g, const double* __restrict__ U,
                                               const double* __restrict__ aux,
                                               double* __restrict__ out, jb_fin fin,
                                               Slots* slots, double dt_arg) {
