@@ -1324,25 +1324,30 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
 // mixed-precision 2D RK stage as an x-line sweep plus y runs (STAGE 1..3)
 // ---------------------------------------------------------------------------
 // float32 LF splitting and WENO5-JS on float32 primitives, float64 RK
-// combination and temperature solve, organised without block barriers:
+// combination and temperature solve:
 //   k_sweep_x    one thread per (y line, x segment of seg cells, field
 //                pair; seg chosen by the host for whole waves): a register
 //                window of the split fluxes walks the
 //                segment's faces and writes the x flux difference
 //                F_{i+1/2} - F_{i-1/2} of each cell
-//   k_flux_y_rk  one warp per run of 32 cells along y: split fluxes of all
-//                fields on the run and its 3 + 3 halo cells, the 33 y faces
-//                and the differences, then the RK combination with the x
-//                part and the temperature solve of the new state
+//   k_flux_y_rk  one block per segment of S cells of a column (S = 32 x
+//                warps, up to 256, one cell per thread): split fluxes of all
+//                fields on the segment and its 3 + 3 halo cells in shared
+//                memory, the S + 1 y faces and the differences, then the
+//                RK combination with the x part and the temperature solve
+//                of the new state
 // Fields are handled in pairs (rho, rho u), (rho v, rho E), (rho Y_1, rho
 // Y_2), ... with sm_100's paired float32 instructions (FFMA2 / FADD2 /
 // FMUL2), which issue two float32 operations at once.  The x differences are
 // stored as float2 pairs: dfx[6][ncell][2].  The stage state's float32 u, v,
 // p come from the kernel that wrote that state (prims[3][ncell]).
 constexpr int SX_NT = 128;
-constexpr int YR_W = 8, YR_NT = 32 * YR_W;     // warps (runs) per block
-constexpr int YR_C = 38, YR_F = 33;            // window cells, faces per run
-constexpr size_t YR_SMEM = sizeof(float2) * YR_W * (2 * 6 * YR_C + 6 * YR_F);
+constexpr int YR_W = 8, YR_NT = 32 * YR_W;  // most warps of a y-run block
+// shared memory of a y-run block of S cells: H+ and H- of the S + 6 window
+// cells and the S + 1 face values, six field pairs each
+__host__ __device__ constexpr size_t yr_smem(int S) {
+  return sizeof(float2) * (2 * 6 * (size_t)(S + 6) + 6 * (size_t)(S + 1));
+}
 
 typedef float2 f2;
 __device__ __forceinline__ f2 f2s(float a) { return make_float2(a, a); }
@@ -1541,70 +1546,64 @@ __global__ void __launch_bounds__(YR_NT, JB_YR_MINB) k_flux_y_rk(MP m, Grid g, c
                                                        const double* __restrict__ Un, const float* __restrict__ prims,
                                                        const double* __restrict__ strips,
                                                        const float2* __restrict__ dfx, double* __restrict__ out,
-                                                       Slots* slots, int aidx, jb_fin fin, int nry) {
+                                                       Slots* slots, int aidx, jb_fin fin, int nsy) {
   extern __shared__ __align__(128) unsigned char smraw[];
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  f2* sHp = reinterpret_cast<f2*>(smraw) + (size_t)w * (2 * 6 * YR_C + 6 * YR_F);  // [6][YR_C]
-  f2* sHm = sHp + 6 * YR_C;
-  f2* sF = sHm + 6 * YR_C;  // [6][YR_F]
+  const int S = blockDim.x, t = threadIdx.x;
+  const int C = S + 6, NF = S + 1;
+  f2* sHp = reinterpret_cast<f2*>(smraw);  // [6][C]: cell y0 - 3 + j in slot j
+  f2* sHm = sHp + 6 * C;
+  f2* sF = sHm + 6 * C;  // [6][NF]: face y0 + k (cells y0+k-1 | y0+k)
   const long long nc = g.ncell;
-  const int run = blockIdx.x * YR_W + w;
-  const int x = run / nry, y0 = (run % nry) * 32;
-  const bool xin = x < g.nx;
+  const int x = blockIdx.x / nsy, y0 = (blockIdx.x % nsy) * S;
   const float al = (float)bitsd(slots->ay[aidx]);
-  // ---- split fluxes on the window: cell y0 - 3 + j in slot j; the run's
-  // own cells one per lane, the 3 + 3 halo cells as 36 (cell, pair) items
-  // spread over the warp
-  if (xin) {
-    {
-      const int jj = l + 3;
-      f2 q[6];
-      float vel, p;
-      if (y0 + l < g.ny) {
-        const long long cell = (long long)x * g.ny + y0 + l;
+  // ---- split fluxes on the window: the segment's own cells one per
+  // thread, the 3 + 3 halo cells as 36 (cell, pair) items
+  {
+    const int jj = t + 3;
+    f2 q[6];
+    float vel, p;
+    if (y0 + t < g.ny) {
+      const long long cell = (long long)x * g.ny + y0 + t;
 #pragma unroll
-        for (int i = 0; i < 6; ++i)
-          q[i] = make_float2((float)Uk[2 * i * nc + cell], (float)Uk[(2 * i + 1) * nc + cell]);
-        vel = prims[nc + cell];
-        p = prims[2 * nc + cell];
-      } else {
-        win_load2<1>(m, g, Uk, prims, strips, x, y0 + l, 0, q, vel, p);
-      }
+      for (int i = 0; i < 6; ++i)
+        q[i] = make_float2((float)Uk[2 * i * nc + cell], (float)Uk[(2 * i + 1) * nc + cell]);
+      vel = prims[nc + cell];
+      p = prims[2 * nc + cell];
+    } else {
+      win_load2<1>(m, g, Uk, prims, strips, x, y0 + t, 0, q, vel, p);
+    }
 #pragma unroll
-      for (int i = 0; i < 6; ++i) split2(i, 1, q[i], vel, p, al, sHp[i * YR_C + jj], sHm[i * YR_C + jj]);
-    }
-#pragma unroll 1
-    for (int i = l; i < 36; i += 32) {
-      const int h = i / 6, pr = i % 6;
-      const int jj = h < 3 ? h : 32 + h;
-      f2 q;
-      float vel, p;
-      win_load2<2>(m, g, Uk, prims, strips, x, y0 - 3 + jj, pr, &q, vel, p);
-      split2(pr, 1, q, vel, p, al, sHp[pr * YR_C + jj], sHm[pr * YR_C + jj]);
-    }
+    for (int i = 0; i < 6; ++i) split2(i, 1, q[i], vel, p, al, sHp[i * C + jj], sHm[i * C + jj]);
   }
-  __syncwarp();
-  // ---- faces y0 + k (cells y0+k-1 | y0+k): lane k for all pairs, then the
-  // run's last face by lanes 0..5, one pair each
-  if (xin) {
 #pragma unroll 1
-    for (int i = 0; i < 6; ++i) {
-      const f2* hp = sHp + i * YR_C + l;
-      const f2* hm = sHm + i * YR_C + l;
-      sF[i * YR_F + l] = f2mul(f2s(0.5f), f2add(weno2(hp[0], hp[1], hp[2], hp[3], hp[4]),
-                                                 weno2(hm[5], hm[4], hm[3], hm[2], hm[1])));
-    }
-    if (l < 6) {
-      const f2* hp = sHp + l * YR_C + 32;
-      const f2* hm = sHm + l * YR_C + 32;
-      sF[l * YR_F + 32] = f2mul(f2s(0.5f), f2add(weno2(hp[0], hp[1], hp[2], hp[3], hp[4]),
-                                                  weno2(hm[5], hm[4], hm[3], hm[2], hm[1])));
-    }
+  for (int i = t; i < 36; i += S) {
+    const int h = i / 6, pr = i % 6;
+    const int jj = h < 3 ? h : S + h;
+    f2 q;
+    float vel, p;
+    win_load2<2>(m, g, Uk, prims, strips, x, y0 - 3 + jj, pr, &q, vel, p);
+    split2(pr, 1, q, vel, p, al, sHp[pr * C + jj], sHm[pr * C + jj]);
   }
-  __syncwarp();
+  __syncthreads();
+  // ---- faces: face y0 + t of every pair, and face y0 + S by threads 0..5
+  // (one pair each)
+#pragma unroll 1
+  for (int i = 0; i < 6; ++i) {
+    const f2* hp = sHp + i * C + t;
+    const f2* hm = sHm + i * C + t;
+    sF[i * NF + t] = f2mul(f2s(0.5f), f2add(weno2(hp[0], hp[1], hp[2], hp[3], hp[4]),
+                                             weno2(hm[5], hm[4], hm[3], hm[2], hm[1])));
+  }
+  if (t < 6) {
+    const f2* hp = sHp + t * C + S;
+    const f2* hm = sHm + t * C + S;
+    sF[t * NF + S] = f2mul(f2s(0.5f), f2add(weno2(hp[0], hp[1], hp[2], hp[3], hp[4]),
+                                             weno2(hm[5], hm[4], hm[3], hm[2], hm[1])));
+  }
+  __syncthreads();
   // ---- RK combination (float64) and update_aux of the new state
-  const int y = y0 + l;
-  const bool live = xin && y < g.ny;
+  const int y = y0 + t;
+  const bool live = y < g.ny;
   unsigned bits = 0;
   double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
   if (live) {
@@ -1614,7 +1613,7 @@ __global__ void __launch_bounds__(YR_NT, JB_YR_MINB) k_flux_y_rk(MP m, Grid g, c
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
       const float2 dF = dfx[i * nc + cell];
-      const f2 dG = f2fma(sF[i * YR_F + l], f2s(-1.f), sF[i * YR_F + l + 1]);
+      const f2 dG = f2fma(sF[i * NF + t], f2s(-1.f), sF[i * NF + t + 1]);
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int f = 2 * i + h;
