@@ -1342,7 +1342,10 @@ __global__ void __launch_bounds__(NT2, sizeof(R) == 4 ? 3 : 2) k_flux2d(MP m, Gr
 // stored as float2 pairs: dfx[6][ncell][2].  The stage state's float32 u, v,
 // p come from the kernel that wrote that state (prims[3][ncell]).
 constexpr int SX_NT = 128;
-constexpr int YR_W = 8, YR_NT = 32 * YR_W;  // most warps of a y-run block
+#ifndef JB_YR_W
+#define JB_YR_W 4
+#endif
+constexpr int YR_W = JB_YR_W, YR_NT = 32 * YR_W;  // most warps of a y-run block
 // shared memory of a y-run block of S cells: H+ and H- of the S + 6 window
 // cells and the S + 1 face values, six field pairs each
 __host__ __device__ constexpr size_t yr_smem(int S) {
@@ -1538,7 +1541,7 @@ __global__ void __launch_bounds__(SX_NT, JB_SX_MINB) k_sweep_x(MP m, Grid g, con
 }
 
 #ifndef JB_YR_MINB
-#define JB_YR_MINB 3
+#define JB_YR_MINB (32 / JB_YR_W)  // 64 registers (64 B of spills)
 #endif
 template <int STAGE, bool VISC>
 __global__ void __launch_bounds__(YR_NT, JB_YR_MINB) k_flux_y_rk(MP m, Grid g, const double* __restrict__ Uk,
