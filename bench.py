@@ -80,11 +80,11 @@ BYTES_STEP_PER_CELL = 864 + 224  # fused-step minimum + separate chemistry pass 
 BYTES_FLUX_STAGE_PER_CELL = 288  # one RK stage of the fused minimum: (224 + 320 + 320) / 3
 # DRAM bytes per cell measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum,
 # each launch cold) on the 1024x256 channel, mixed precision, with this tree's
-# kernels: one RK stage 2/3 (k_sweep_x 27.35 + 0.00 MB, k_flux_y_rk 67.19 +
-# 2.66 MB) and one chemistry launch (27.39 + 3.51 MB); the capture and its
+# kernels: one RK stage 2/3 (k_sweep_x 27.35 + 0.00 MB, k_flux_y_rk 67.43 +
+# 5.98 MB) and one chemistry launch (27.38 + 3.46 MB); the capture and its
 # command are in profiles/launches_channel1024x256_mixed.md.  Per cell-step of
 # the persistent ensemble kernel: profiles/k_ensemble_64tubes.md.
-TRAFFIC_PER_CELL = {"flux": 370.8, "chem": 117.9}
+TRAFFIC_PER_CELL = {"flux": 384.3, "chem": 117.6}
 TRAFFIC_SOURCE = "profiles/launches_channel1024x256_mixed.md"
 TRAFFIC_ENS_PER_CELL_STEP = 1125.0
 
