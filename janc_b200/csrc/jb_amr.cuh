@@ -140,7 +140,10 @@ typedef jb_amr_io AmrIO;  // the stage call's block arrays (jb_ops.h)
 // (set_simulator.py:37-40).  G: the stage input with its ghost layers
 // filled; U0: the step's first stage input.
 template <int STAGE>
-__global__ void __launch_bounds__(AMR_NT) k_amr_stage(MP m, Grid g, AmrBlocks B, AmrIO io, Slots* slots,
+#ifndef JB_AMR_MINB
+#define JB_AMR_MINB 4  // 64 registers (8 B of spills)
+#endif
+__global__ void __launch_bounds__(AMR_NT, JB_AMR_MINB) k_amr_stage(MP m, Grid g, AmrBlocks B, AmrIO io, Slots* slots,
                                                     double dt) {
   extern __shared__ __align__(128) unsigned char smraw[];
   constexpr int nv = 12;

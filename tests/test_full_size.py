@@ -5,7 +5,11 @@
   step against the oracle (a NumPy restatement of
   src/janc_v2/simulation/set_simulator.py:410-447 that finishes one step of
   this grid in seconds) in every precision.
-* Size-independent properties of the same step, over many steps:
+* Rotating-detonation annulus, 1600 x 1000 (the bench's rdc workload:
+  periodic x, injector bottom, pressure outlet top, nondimensional): one
+  step against the oracle in every precision (the oracle's step of this
+  grid takes a minute or two).
+* Size-independent properties of the same steps, over many steps:
   - mirror symmetry of the channel in x and in y (slip walls on both ends of
     each axis; the mirrored state has its normal momentum negated): WENO5-JS
     right-biased reconstruction is the left-biased one with the stencil
@@ -92,6 +96,38 @@ def test_channel_full_size_step_vs_oracle(channel, prec):
     U0, aux0, U1, aux1, dt = channel
     s = _channel_solver(prec)
     Ug, ag, dts = s.advance(_cuda(U0), _cuda(aux0), 1, cfl=CFL_CH)
+    torch.cuda.synchronize()
+    assert s.status() == 0
+    Ug, ag = Ug.cpu().numpy(), ag.cpu().numpy()
+    tol = {"fp64_strict": 1e-12, "fp64": 1e-10, "mixed": 1e-4}[prec]
+    assert abs(float(dts[0]) - dt) <= 1e-13 * dt
+    err = _errors(Ug, ag, U1, aux1)
+    assert max(err.values()) < tol, err
+    assert err["rho"] < (1e-6 if prec == "mixed" else tol), err
+
+
+@pytest.fixture(scope="module")
+def rdc():
+    """Initial state of the rotating-detonation workload, its theta and the
+    oracle's first step."""
+    from janc_b200.mechanism import DEFAULT_MECHANISM
+    nm = jo.load_mechanism(DEFAULT_MECHANISM, bench.RDC_ND)
+    P, T, Y, Yinj = bench.rdc_fields()
+    theta = {"Yinj": Yinj, "Pb": 101325.0 / bench.RDC_ND["P0"]}
+    U0, aux0 = jo.state_from_PTY(nm, P, T, Y)
+    dx = 1e-4 / bench.RDC_ND["x0"]
+    o = jo.Solver(nm, "2D", dx, dx, BC_RDC, CFL_RDC)
+    U1, aux1, _, dt = o.advance_func(U0, aux0, 0.0, theta)
+    return U0, aux0, theta, U1, aux1, dt
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_rdc_full_size_step_vs_oracle(rdc, prec):
+    U0, aux0, theta, U1, aux1, dt = rdc
+    nx, ny = bench.RDC_NX, bench.RDC_NY
+    dx = 1e-4 / bench.RDC_ND["x0"]
+    s = Solver(2, nx, ny, dx, dx, BC_RDC, nondim_config=bench.RDC_ND, precision=prec)
+    Ug, ag, dts = s.advance(_cuda(U0), _cuda(aux0), 1, cfl=CFL_RDC, theta=theta)
     torch.cuda.synchronize()
     assert s.status() == 0
     Ug, ag = Ug.cpu().numpy(), ag.cpu().numpy()
