@@ -1271,7 +1271,7 @@ def ensemble_record(args, dist, rank, ws, K, precision, with_cpu):
 
 def _oracle_tube(args):
     """One replica: the NumPy oracle advancing ensemble tube i for `steps` steps."""
-    i, steps = args
+    i, steps, warm = args
     import warnings
     warnings.simplefilter("ignore")
     sys.path.insert(0, ROOT)
@@ -1282,14 +1282,16 @@ def _oracle_tube(args):
     t = detonation_tubes(ENS_N, seed=ENS_SEED)[i]
     U, aux = jo.state_from_PTY(m, t["P"], t["T"], t["Y"])
     s = jo.Solver(m, "1D", t["dx"], None, BC1, ENS_CFL)
-    U, aux, tt, _ = s.advance_func(U, aux, 0.0)  # warm-up step
+    tt = 0.0
+    for _ in range(warm):  # untimed warm-up steps
+        U, aux, tt, _ = s.advance_func(U, aux, tt)
     t0 = time.perf_counter()
     for _ in range(steps):
         U, aux, tt, _ = s.advance_func(U, aux, tt)
     return time.perf_counter() - t0, t["nx"] * steps
 
 
-def cpu_baseline_ensemble(steps):
+def cpu_baseline_ensemble(steps, warm=1):
     """The oracle on all host cores, one ensemble tube per process."""
     import concurrent.futures as cf
     import multiprocessing as mp
@@ -1300,7 +1302,7 @@ def cpu_baseline_ensemble(steps):
         os.environ[k] = "1"
     t0 = time.perf_counter()
     with cf.ProcessPoolExecutor(nrep, mp_context=mp.get_context("spawn")) as ex:
-        res = list(ex.map(_oracle_tube, [(i, steps) for i in range(nrep)]))
+        res = list(ex.map(_oracle_tube, [(i, steps, warm) for i in range(nrep)]))
     wall = time.perf_counter() - t0
     for k, v in env_keep.items():
         if v is None:
@@ -1319,7 +1321,7 @@ def cpu_baseline_ensemble(steps):
 def _oracle_replica(args):
     """One replica: the NumPy oracle advancing a 32 x 256 strip of the channel
     (slab columns included, same boundaries and CFL) for `steps` steps."""
-    nx, steps = args
+    nx, steps, warm = args
     import warnings
     import numpy as np
     warnings.simplefilter("ignore")
@@ -1331,14 +1333,16 @@ def _oracle_replica(args):
     U, aux = jo.state_from_PTY(m, P, T, Y)
     bc = {k: "slip_wall" for k in ("left_boundary", "right_boundary", "bottom_boundary", "top_boundary")}
     s = jo.Solver(m, "2D", LX / NX, LY / NY, bc, CFL)
-    U, aux, t, _ = s.advance_func(U, aux, 0.0)  # warm-up step
+    t = 0.0
+    for _ in range(warm):  # untimed warm-up steps
+        U, aux, t, _ = s.advance_func(U, aux, t)
     t0 = time.perf_counter()
     for _ in range(steps):
         U, aux, t, _ = s.advance_func(U, aux, t)
     return time.perf_counter() - t0, nx * NY * steps
 
 
-def cpu_baseline(steps):
+def cpu_baseline(steps, warm=1):
     """The oracle on all host cores as independent replicas (spawned
     processes, one BLAS thread each); returns the cpu_baseline record."""
     import concurrent.futures as cf
@@ -1351,7 +1355,7 @@ def cpu_baseline(steps):
         os.environ[k] = "1"
     t0 = time.perf_counter()
     with cf.ProcessPoolExecutor(nrep, mp_context=mp.get_context("spawn")) as ex:
-        res = list(ex.map(_oracle_replica, [(nx, steps)] * nrep))
+        res = list(ex.map(_oracle_replica, [(nx, steps, warm)] * nrep))
     wall = time.perf_counter() - t0
     for k, v in env_keep.items():
         if v is None:
@@ -1370,11 +1374,13 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    # the driver's warm-up count, bounded so that the run stays short
+    warm = max(1, min(args.warmup, 5))
     if args.workload == "ensemble":
         steps = max(1, min(args.steps, 10))
-        cpu = cpu_baseline_ensemble(steps)
+        cpu = cpu_baseline_ensemble(steps, warm)
         line = {"impl": "reference", "metric": "total " + METRIC, "value": cpu["value"], "unit": UNIT,
-                "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": 1,
+                "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": warm,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": {"workload": f"batched ensemble of {ENS_N} 1D tubes, CPU reference path", "cfl": ENS_CFL},
@@ -1383,9 +1389,9 @@ def run_reference(args):
         print(json.dumps(line), flush=True)
         return
     steps = max(1, min(args.steps, 20))
-    cpu = cpu_baseline(steps)
+    cpu = cpu_baseline(steps, warm)
     line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT,
-            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": 1,
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": steps, "warmup": warm,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": "2D H2-air detonation channel (strips of 32x256 cells of the 1024x256 "
