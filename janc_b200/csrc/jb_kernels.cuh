@@ -2307,10 +2307,13 @@ __device__ __forceinline__ void chem_cell_step(const MP& m, const Grid& g, const
 
 // CELL: the mixed variant's 2D step (per-cell temperature solve)
 template <int DIM, bool WRITE_S, bool GEN, bool CELL>
-#ifndef JB_CHEM_MINB
-#define JB_CHEM_MINB 3
+#ifndef JB_CHEM_NT
+#define JB_CHEM_NT 128
 #endif
-__global__ void __launch_bounds__(128, JB_CHEM_MINB) k_chem(MP m, Grid g, const double* __restrict__ U,
+#ifndef JB_CHEM_MINB
+#define JB_CHEM_MINB (384 / JB_CHEM_NT)
+#endif
+__global__ void __launch_bounds__(JB_CHEM_NT, JB_CHEM_MINB) k_chem(MP m, Grid g, const double* __restrict__ U,
                                               const double* __restrict__ aux,
                                               double* __restrict__ out, jb_fin fin,
                                               Slots* slots, double dt_arg) {
