@@ -86,15 +86,18 @@ BYTES_FLUX_STAGE_PER_CELL = 288  # one RK stage of the fused minimum: (224 + 320
 # the persistent ensemble kernel: profiles/k_ensemble_64tubes.md.
 TRAFFIC_PER_CELL = {"flux": 384.3, "chem": 117.6}
 TRAFFIC_SOURCE = "profiles/launches_channel1024x256_mixed.md"
-TRAFFIC_ENS_PER_CELL_STEP = 1125.0
+TRAFFIC_ENS_PER_CELL_STEP = 764.0
 
 
 ENS_N, ENS_SEED, ENS_CFL = 64, 4, 0.1
 # 1D step, float64, each pass reading its inputs once and writing its outputs
-# once (fields: 11 conserved, aux T, 6 Halley iterates): stage 1 (12 in, 17
-# out), select 1 (12 in, 2 out), stages 2 and 3 (23 in, 17 out), select 2
-# (14), chemistry (12 in, 17 out), select 4 (14) -> 180 doubles
-BYTES_ENS_STEP_PER_CELL = 1440
+# once (fields: 11 conserved, aux gamma and T, 6 Halley iterates).  fp64
+# (global stop): stage 1 (12 in, 17 out), select 1 (12 in, 2 out), stages 2
+# and 3 (23 in, 17 out), select 2 (14), chemistry (12 in, 17 out), select 4
+# (14) -> 180 doubles.  mixed (per-cell solves, no select passes): stage 1
+# (12 in, 13 out), stages 2 and 3 (23 in, 13 out), chemistry (12 in, 13 out)
+# -> 122 doubles.
+BYTES_ENS_STEP_PER_CELL = {"fp64": 1440, "mixed": 976}
 
 RDC_NX, RDC_NY = 1600, 1000
 RDC_ND = {"P0": 10 * 101325, "T0": 300, "R0": 369, "x0": 0.08}
@@ -1221,7 +1224,7 @@ def ensemble_record(args, dist, rank, ws, K, precision, with_cpu):
             pass
     fp64_peak = fp64_peak_tflops(_native.lib(), torch)
     arith, special = chem_flops_per_cell()
-    achieved = BYTES_ENS_STEP_PER_CELL * cells * K / (ms * 1e-3) / 1e9
+    achieved = BYTES_ENS_STEP_PER_CELL[precision] * cells * K / (ms * 1e-3) / 1e9
     chem_tflops = arith * cells * K / (ms * 1e-3) / 1e12
     cpu = cpu_baseline_ensemble(args.cpu_steps) if with_cpu else None
     sizes = [t["nx"] for t in tubes]
@@ -1247,7 +1250,7 @@ def ensemble_record(args, dist, rank, ws, K, precision, with_cpu):
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      "traffic": TRAFFIC_ENS_PER_CELL_STEP * cells * K if precision == "mixed" else None,
                      "traffic_source": "ncu dram bytes of a 20-step launch, scaled to this launch's cell-steps",
-                     "peak_source": hbm_src, "algorithmic_bytes_per_cell_step": BYTES_ENS_STEP_PER_CELL,
+                     "peak_source": hbm_src, "algorithmic_bytes_per_cell_step": BYTES_ENS_STEP_PER_CELL[precision],
                      "launch_ms": ms},
         "compute_roofline": {"bound": "fp64", "kernel": "k_ensemble (chemistry share of the flops only)",
                              "achieved": chem_tflops, "peak": fp64_peak, "unit": "TFLOP/s",

@@ -380,13 +380,14 @@ static int advance_impl(jb_handle* h, const double* U, const double* aux, double
     JB_TRY(cudaMemcpyAsync(rec, U, sizeof(double) * nU, cudaMemcpyDeviceToDevice, st), "record U0");
     JB_TRY(cudaMemcpyAsync(rec + nU, aux, sizeof(double) * nA, cudaMemcpyDeviceToDevice, st), "record aux0");
   }
-  // Per-cell mode (mixed, 2D): each stage kernel and the chemistry finish
-  // their new state's temperature per cell and reduce its LF alpha (and,
-  // after the chemistry, the CFL minimum) in their epilogue, so no select
-  // pass runs between them.  Global-stop mode (strict and fp64, and 1D): the
-  // kernels write the Halley iterates and a select pass after each picks the
-  // reference's iteration count.
-  const bool pc = o.per_cell_2d && d == 2;
+  // Per-cell mode (mixed: 2D, and 1D with flux splitting): each stage kernel
+  // and the chemistry finish their new state's temperature per cell and
+  // reduce its LF alpha (and, after the chemistry, the CFL minimum) in their
+  // epilogue, so no select pass runs between them.  Global-stop mode (strict
+  // and fp64, and the mixed 1D Godunov path): the kernels write the Halley
+  // iterates and a select pass after each picks the reference's iteration
+  // count.
+  const bool pc = o.per_cell && (d == 2 || g.scheme == JB_FLUX_LF || g.scheme == JB_FLUX_SW);
   // mixed 2D: float32 u, v, p of the current state (pin) and the buffer the
   // next kernel writes (pout), swapped after each writer
   float* pin = h->fwork ? static_cast<float*>(h->fwork) : nullptr;

@@ -23,9 +23,19 @@
 //            temperature is taken straight from the Halley iterates)
 //   select 4 U, cand          -> aux           (alpha of the next stage 1,
 //                                               CFL minimum of the next dt)
-// with a group barrier after each, seven per step.  Slot sets alternate
-// between even and odd steps, so clearing one never races with reading the
-// other.
+// with a group barrier after each, seven per step (the float64 ensemble,
+// whose instances keep the reference's global stop of the temperature
+// solve).  The mixed variant solves each cell's temperature where its new
+// state is written (as its single-case step does), so no select pass
+// follows and a step has four phases:
+//   stage 1  U, aux      -> W0, A0      (alpha 1)
+//   stage 2  W0, A0, U   -> W1, A1      (alpha 2)
+//   stage 3  W1, A1, U   -> W0, A0
+//   chem     W0, A0      -> U, aux      (alpha of the next stage 1, CFL
+//                                        minimum of the next dt)
+// each also writing the outlet ghost strips of its new state.  Slot sets
+// alternate between even and odd steps, so clearing one never races with
+// reading the other.
 #define JB_NS ens
 #define JB_FAST 1
 #include "jb_kernels.cuh"
@@ -145,15 +155,62 @@ __device__ __noinline__ void select_pass(const jb_ens_inst& I, int rank, const d
   block_reduce_store(amx, amy, dtm, st << 16, s, aidx, true, CFL, -1);
 }
 
-// One RK stage over this CTA's tiles; Halley mask into s->mask[STAGE - 1].
+// The outlet ghost strips of this instance from the boundary cells' new
+// (U, gamma, T), computed by the CTA that wrote those cells (its writes are
+// visible to its own threads after a block barrier), their wave speeds
+// folded into amx.  chunk: cells per work item of the pass that wrote them.
+__device__ __forceinline__ void ens_strips(const jb_ens_inst& I, int rank, int chunk, int nitems,
+                                           const double* U, const double* aux, double& amx) {
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    const int side = threadIdx.x;
+    const int x = side == 0 ? 0 : I.g.nx - 1;
+    const int kind = I.g.bc[side];
+    if ((kind == JB_BC_PRESSURE_OUTLET || kind == JB_BC_RDC_INJECTOR) && (x / chunk) % I.ncta == rank &&
+        x / chunk < nitems) {
+      double amy = 0.0;
+      strip_one<1>(c_mech, I.g, U, aux, I.strips, side, 0, amx, amy);
+    }
+  }
+}
+
+// One RK stage over this CTA's tiles.  Global-stop mode (float64 tiles):
+// Halley mask into s->mask[STAGE - 1]; per-cell mode (float tiles of the
+// mixed variant): each cell's temperature solve into fin.aux, and the new
+// state's alpha (with the outlet strips) into s->ax[fin.aidx].
 template <int STAGE, class R, int NT>
 __device__ __noinline__ void flux_pass(const jb_ens_inst& I, int rank, const double* Uk, const double* auxk,
-                                       double* out, double alpha, double dt, Slots* s, unsigned char* smraw) {
+                                       double* out, double alpha, double dt, Slots* s, unsigned char* smraw,
+                                       const jb_fin& fin) {
   unsigned bits = 0;
+  double amx = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
   for (int t = rank; t < I.ntiles; t += I.ncta)
-    bits |= flux1d_tile<STAGE, R, NT>(c_mech, I.g, Uk, auxk, I.U, out, I.cand, I.strips, alpha, dt, t * (NT - 1),
-                                      smraw);
-  block_reduce_store(0.0, 0.0, 0.0, bits, s, 0, false, false, STAGE - 1);
+    bits |= flux1d_tile<STAGE, R, NT>(c_mech, I.g, Uk, auxk, I.U, out, fin, I.strips, alpha, dt, t * (NT - 1),
+                                      smraw, amx, dtm, s);
+  if (fin.aux && fin.aidx >= 0) ens_strips(I, rank, NT - 1, I.ntiles, out, fin.aux, amx);
+  finish_reduce(fin, amx, 0.0, dtm, bits, s);
+}
+
+// Per-cell mode: chemistry of this CTA's cells at the stage-3 temperature
+// in A0, then each cell's temperature solve into aux, the new state's alpha
+// (with the outlet strips) into s->ax[3] and its CFL minimum.
+template <int NT>
+__device__ __noinline__ void chem_pass_cell(const jb_ens_inst& I, int rank, double dt, Slots* s,
+                                            unsigned char* smraw) {
+  const Grid& g = I.g;
+  const long long nc = g.ncell;
+  double* sh = reinterpret_cast<double*>(smraw) + threadIdx.x;
+  const jb_fin fin = jb_fin_cell(I.aux, nullptr, 3, 1);
+  unsigned bits = 0, st = 0;
+  double amx = 0.0, amy = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
+  for (int j = rank; j < I.nchunks; j += I.ncta) {
+    long long c = (long long)j * NT + threadIdx.x;
+    if (c < nc)
+      chem_cell_step<1, false, true, true>(c_mech, g, I.W0, I.A0[nc + c], I.U, fin, c, dt, sh, bits, st, amx, amy,
+                                           dtm, s);
+  }
+  ens_strips(I, rank, NT, I.nchunks, I.U, I.aux, amx);
+  finish_reduce(fin, amx, 0.0, dtm, bits | (st << 16), s);
 }
 
 // Chemistry of this CTA's cells at the stage-3 temperature (iterate n3 of
@@ -213,24 +270,47 @@ __global__ void __launch_bounds__(NT, Shape<NT>::MINB)
                                                                   : bitsd(__ldcg(&prv->dtmin_next)))
                                   : I.dt;
     if (dt_hist && rank == 0 && tid == 0) dt_hist[(long long)ii * nsteps + step] = dt;
+    if constexpr (sizeof(R) == sizeof(float)) {
+      // mixed variant, per-cell temperature solves: four phases a step
+      // stage 1: U1 = U + L(U), (gamma, T)_1 and alpha 1
+      flux_pass<1, R, NT>(I, rank, I.U, I.aux, I.W0, bitsd(__ldcg(&prv->ax[3])), dt, cur, smraw,
+                          jb_fin_cell(I.A0, nullptr, 1, 0));
+      JB_ENS_SYNC();
+      if (rank == 0 && tid == 0) slots_clear(prv);  // every CTA has read it
+      // stage 2: U2 = 3/4 U + 1/4 (U1 + L(U1))
+      flux_pass<2, R, NT>(I, rank, I.W0, I.A0, I.W1, bitsd(__ldcg(&cur->ax[1])), dt, cur, smraw,
+                          jb_fin_cell(I.A1, nullptr, 2, 0));
+      JB_ENS_SYNC();
+      // stage 3: U3 = 1/3 U + 2/3 (U2 + L(U2)), T3 into A0
+      flux_pass<3, R, NT>(I, rank, I.W1, I.A1, I.W0, bitsd(__ldcg(&cur->ax[2])), dt, cur, smraw,
+                          jb_fin_cell(I.A0, nullptr, -1, 0));
+      JB_ENS_SYNC();
+      // chemistry, the final solve, alpha and CFL minimum of the next step
+      chem_pass_cell<NT>(I, rank, dt, cur, smraw);
+      JB_ENS_SYNC();
+    } else {
     // stage 1: U1 = U + L(U)
-    flux_pass<1, R, NT>(I, rank, I.U, I.aux, I.W0, bitsd(__ldcg(&prv->ax[3])), dt, cur, smraw);
+    flux_pass<1, R, NT>(I, rank, I.U, I.aux, I.W0, bitsd(__ldcg(&prv->ax[3])), dt, cur, smraw,
+                        jb_fin_cand(I.cand, 0));
     JB_ENS_SYNC();
     if (rank == 0 && tid == 0) slots_clear(prv);  // every CTA has read it
     select_pass<true, false, NT>(I, rank, I.W0, nullptr, I.A0, __ldcg(&cur->mask[0]), cur, 1);
     JB_ENS_SYNC();
     // stage 2: U2 = 3/4 U + 1/4 (U1 + L(U1))
-    flux_pass<2, R, NT>(I, rank, I.W0, I.A0, I.W1, bitsd(__ldcg(&cur->ax[1])), dt, cur, smraw);
+    flux_pass<2, R, NT>(I, rank, I.W0, I.A0, I.W1, bitsd(__ldcg(&cur->ax[1])), dt, cur, smraw,
+                        jb_fin_cand(I.cand, 1));
     JB_ENS_SYNC();
     select_pass<true, false, NT>(I, rank, I.W1, nullptr, I.A1, __ldcg(&cur->mask[1]), cur, 2);
     JB_ENS_SYNC();
     // stage 3: U3 = 1/3 U + 2/3 (U2 + L(U2))
-    flux_pass<3, R, NT>(I, rank, I.W1, I.A1, I.W0, bitsd(__ldcg(&cur->ax[2])), dt, cur, smraw);
+    flux_pass<3, R, NT>(I, rank, I.W1, I.A1, I.W0, bitsd(__ldcg(&cur->ax[2])), dt, cur, smraw,
+                        jb_fin_cand(I.cand, 2));
     JB_ENS_SYNC();
     chem_pass<NT>(I, rank, halley_count(__ldcg(&cur->mask[2])), dt, cur, smraw);
     JB_ENS_SYNC();
     select_pass<true, true, NT>(I, rank, I.U, nullptr, I.aux, __ldcg(&cur->mask[3]), cur, 3);
     JB_ENS_SYNC();
+    }
   }
 #undef JB_ENS_SYNC
 }

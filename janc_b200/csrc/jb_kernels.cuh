@@ -453,13 +453,13 @@ __device__ __forceinline__ unsigned finish_state(const MP& m, const Grid& g, con
   const long long nc = g.ncell;
   const double rho = q[0];
 #if JB_FAST
-  if constexpr (DIM == 2 && CELL) {
+  if constexpr (CELL) {
     // one reciprocal of rho; the primitives of the wave speeds as u_to_prim
     // forms them (p = T sum_k (rho Y_k)/M_k, rho Y_N2 = rho - sum rho Y_k)
     // are taken before the solve so that the state is no longer needed
     const double ri = 1.0 / rho;
-    const double u = q[1] * ri, v = q[2] * ri;
-    const double e = q[3] * ri - 0.5 * (u * u + v * v);
+    const double u = q[1] * ri, v = DIM == 2 ? q[2] * ri : 0.0;
+    const double e = DIM == 2 ? q[3] * ri - 0.5 * (u * u + v * v) : q[2] * ri - 0.5 * (u * u);
     double Y8[NR], Yf[NS];
     double sr = q[nY], prs = m.invM[0] * q[nY];
 #pragma unroll
@@ -482,7 +482,7 @@ __device__ __forceinline__ unsigned finish_state(const MP& m, const Grid& g, con
     if (fin.aidx >= 0 || fin.cfl || fin.prims) {
       const double p = prs * T;
       const double a = sqrt(gamma * p * ri);
-      if (fin.prims) {
+      if (DIM == 2 && fin.prims) {
         fin.prims[c] = (float)u;
         fin.prims[nc + c] = (float)v;
         fin.prims[2 * nc + c] = (float)p;
@@ -492,7 +492,8 @@ __device__ __forceinline__ unsigned finish_state(const MP& m, const Grid& g, con
       amy = fmax(amy, sy);
       if (!(sx == sx) || !(T == T)) st |= JB_ERR_NONFINITE;
       if (fin.cfl) {
-        const double d = 1.0 / (sx * g.idx + sy * g.idy);
+        // the CFL candidate as the select pass forms it (1D: dx / (|u| + a))
+        const double d = DIM == 1 ? g.dx / sx : 1.0 / (sx * g.idx + sy * g.idy);
         dtm = fmin(dtm, d);
         if (!(d == d) || !(d > 0.0)) st |= JB_ERR_NONFINITE;
         if (!(d == d)) atomicOr(&slots->dtnan, 1u);  // jnp.min propagates NaN
@@ -1658,8 +1659,9 @@ __host__ __device__ constexpr size_t smem1d_bytes(int nq) {
 template <int STAGE, class R, int NT, bool VISC = false, bool SW = false>
 __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, const double* Uk,
                                                 const double* auxk, const double* Un, double* out,
-                                                double* cand, const double* strips, double alpha,
-                                                double dt, int x0, unsigned char* smraw) {
+                                                const jb_fin& fin, const double* strips, double alpha,
+                                                double dt, int x0, unsigned char* smraw, double& amx,
+                                                double& dtm, Slots* slots) {
   constexpr int TX1 = NT - 1, PX1 = NT + 5;
   constexpr int nv = 11, nq = nv + 1;
   constexpr bool EXACT = sizeof(R) == sizeof(double);
@@ -1760,18 +1762,12 @@ __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, cons
   if (live) {
     double q[11];
     for (int f = 0; f < 11; ++f) q[f] = out[f * nc + cell];
-    double rho = q[0];
-    double u = q[1] / rho;
-    double e = q[2] / rho - 0.5 * (u * u);
-    double Y8[NR], Yf[NS];
-#pragma unroll
-    for (int k = 0; k < NR; ++k) Y8[k] = q[3 + k] / rho;
-    fill_Y(Y8, Yf);
-    double Rmix = get_R(m, Yf);
-    double cnd[JB_NCAND];
-    bits = halley_any(m, e, Yf, Rmix, EXACT ? (double)sQ[nv * PX1 + tid + 3] : auxk[nc + cell], cnd);
-#pragma unroll
-    for (int i = 0; i < JB_NCAND; ++i) cand[i * nc + cell] = cnd[i];
+    const double T0 = EXACT ? (double)sQ[nv * PX1 + tid + 3] : auxk[nc + cell];
+    // float tiles (the mixed variant): the temperature solve per cell, with
+    // the new state's alpha and CFL candidate; float64 tiles: the Halley
+    // iterates of the global stop
+    double amy = 0.0;
+    bits = finish_state<1, !EXACT>(m, g, fin, q, T0, cell, amx, amy, dtm, slots);
   }
   __syncthreads();  // the tile's shared memory is reused by the next tile
   return bits;
@@ -1786,12 +1782,13 @@ __global__ void __launch_bounds__(NT1) k_flux1d(MP m, Grid g, const double* __re
                                                  int aidx, jb_fin fin, double dt_arg) {
   extern __shared__ __align__(128) unsigned char smraw[];
   const double dt = STAGE == 0 ? dt_arg : slots->dt;
-  // 1D stays in the global-stop mode (its tile body is shared with the
-  // persistent ensemble kernel)
-  unsigned bits = flux1d_tile<STAGE, R, NT1, VISC, SW>(m, g, Uk, auxk, Un, out, fin.cand, strips,
-                                                       bitsd(slots->ax[aidx]), dt, blockIdx.x * (NT1 - 1), smraw);
+  // the tile body is shared with the persistent ensemble kernel
+  double amx = 0.0, dtm = __longlong_as_double(0x7ff0000000000000LL);
+  unsigned bits = flux1d_tile<STAGE, R, NT1, VISC, SW>(m, g, Uk, auxk, Un, out, fin, strips,
+                                                       bitsd(slots->ax[aidx]), dt, blockIdx.x * (NT1 - 1), smraw,
+                                                       amx, dtm, slots);
   if (STAGE == 0) return;
-  block_reduce_store(0.0, 0.0, 0.0, bits, slots, 0, false, false, fin.midx);
+  finish_reduce(fin, amx, 0.0, dtm, bits, slots);
 }
 
 // ---------------------------------------------------------------------------
@@ -1941,24 +1938,15 @@ __global__ void __launch_bounds__(256, 4) k_select(MP m, Grid g, const double* _
   if (ALPHA || CFL) block_reduce_store(amx, amy, dtm, st << 16, slots, aidx, ALPHA, CFL, -1);
 }
 
-// Ghost strips of the pressure-outlet and injector sides (the padded grid's
-// entries that are not copies of interior cells) and their wave speeds into
-// the alpha maxima: one thread per boundary position, after the select pass
-// that wrote the boundary cells' (gamma, T) into aux.  Positions: side 0 and
-// 1 (x = 0, nx-1) ny each, then sides 2 and 3 (y = 0, ny-1) nx each.
+// The ghost state of an outlet / injector side at boundary position pos from
+// the boundary cell's (U, gamma, T) into the strip, and its wave speeds
+// folded into amx, amy (nothing for other sides).
 template <int DIM>
-__global__ void __launch_bounds__(128) k_strips(MP m, Grid g, const double* __restrict__ U,
-                                                const double* __restrict__ aux, double* __restrict__ strips,
-                                                Slots* slots, int aidx) {
+__device__ __forceinline__ void strip_one(const MP& m, const Grid& g, const double* U, const double* aux,
+                                          double* strips, int side, int pos, double& amx, double& amy) {
   constexpr int nY = DIM == 1 ? 3 : 4;
   constexpr int nv = nY + NR;
   const long long nc = g.ncell;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int ns = DIM == 1 ? 1 : g.ny;
-  double amx = 0.0, amy = 0.0;
-  int side = -1, pos = 0;
-  if (t < 2 * ns) { side = t / ns; pos = t % ns; }
-  else if (DIM == 2 && t < 2 * ns + 2 * g.nx) { side = 2 + (t - 2 * ns) / g.nx; pos = (t - 2 * ns) % g.nx; }
   const int kind = side >= 0 ? g.bc[side] : JB_BC_PERIODIC;
   if (kind == JB_BC_PRESSURE_OUTLET || kind == JB_BC_RDC_INJECTOR) {
     const int x = side == 0 ? 0 : side == 1 ? g.nx - 1 : pos;
@@ -1982,9 +1970,27 @@ __global__ void __launch_bounds__(128) k_strips(MP m, Grid g, const double* __re
     }
     for (int f = 0; f < nv + 2; ++f) strips[strip_idx(g, side, f, pos)] = gs[f];
     Prim<DIM> pg = u_to_prim<DIM>(m, gs, gs[nv], gs[nv + 1]);
-    amx = fabs(pg.u) + pg.a;
-    amy = fabs(pg.v) + pg.a;
+    amx = fmax(amx, fabs(pg.u) + pg.a);
+    amy = fmax(amy, fabs(pg.v) + pg.a);
   }
+}
+
+// Ghost strips of the pressure-outlet and injector sides (the padded grid's
+// entries that are not copies of interior cells) and their wave speeds into
+// the alpha maxima: one thread per boundary position, after the pass that
+// wrote the boundary cells' (gamma, T) into aux.  Positions: side 0 and 1
+// (x = 0, nx-1) ny each, then sides 2 and 3 (y = 0, ny-1) nx each.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_strips(MP m, Grid g, const double* __restrict__ U,
+                                                const double* __restrict__ aux, double* __restrict__ strips,
+                                                Slots* slots, int aidx) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ns = DIM == 1 ? 1 : g.ny;
+  double amx = 0.0, amy = 0.0;
+  int side = -1, pos = 0;
+  if (t < 2 * ns) { side = t / ns; pos = t % ns; }
+  else if (DIM == 2 && t < 2 * ns + 2 * g.nx) { side = 2 + (t - 2 * ns) / g.nx; pos = (t - 2 * ns) % g.nx; }
+  strip_one<DIM>(m, g, U, aux, strips, side, pos, amx, amy);
   block_reduce_store(amx, amy, 0.0, 0u, slots, aidx, true, false, -1);
 }
 

@@ -25,10 +25,11 @@ struct jb_amr_io {
 
 struct Ops {
   const char* name;
-  // 2D stepping (jb_advance) solves each new state's temperature per cell
-  // (jb_fin per-cell mode) instead of the global-stop iterates + select:
-  // the mixed variant only; strict and fp64 keep the reference's global stop
-  bool per_cell_2d;
+  // stepping (jb_advance) solves each new state's temperature per cell
+  // (jb_fin per-cell mode) instead of the global-stop iterates + select: the
+  // mixed variant only (2D, and 1D with flux splitting); strict and fp64
+  // keep the reference's global stop
+  bool per_cell;
   // STAGE 0 writes dt * flux; STAGE 1..3 writes the RK stage and finishes
   // its temperature solve as fin says (jb_fin.h).  aidx: the alpha slot the
   // stage reads.  prims: float32 u, v, p of the stage state (mixed 2D) and
