@@ -349,6 +349,10 @@ long long jb_ens_total_cells(const jb_ensemble* e);
 /* Launch shape: block = 64, 128 or 256 threads, blocks_per_sm resident CTAs
  * per SM; CTAs are assigned to instances in proportion to their flux tiles. */
 int jb_ens_configure(jb_ensemble* e, int block, int blocks_per_sm);
+/* Back pressure of each instance's pressure-outlet sides, pb[n] (theta['Pb']
+ * of boundary_conditions_1D/pressure_outlet.py:5-22, in the ensemble's
+ * units); 0 until set.  A set-up call: it uploads the instance table. */
+int jb_ens_set_back_pressure(jb_ensemble* e, const double* pb);
 /* Times every launch shape the device fits on `trial_steps` steps (the
  * state is restored afterwards) and keeps the fastest. */
 int jb_ens_autotune(jb_ensemble* e, int trial_steps, void* stream, int* best_block, int* best_bpsm,

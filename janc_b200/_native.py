@@ -30,6 +30,7 @@ EXPORTS = ["jb_version", "jb_create", "jb_destroy", "jb_set_theta", "jb_flux_fun
            "jb_last_error", "jb_probe_fp64_fma", "jb_set_kernel_timing", "jb_kernel_times",
            "jb_update_aux_noalloc", "jb_rk3", "jb_u_to_prim",
            "jb_ens_create", "jb_ens_destroy", "jb_ens_instance", "jb_ens_total_cells", "jb_ens_configure",
+           "jb_ens_set_back_pressure",
            "jb_ens_autotune", "jb_ens_launch_shape", "jb_ens_advance", "jb_ens_advance_direct",
            "jb_ens_status", "jb_ens_last_error", "jb_ens_selftest_timeout",
            "jb_set_probe", "jb_set_log_A_offset", "jb_record_doubles", "jb_advance_ex", "jb_adjoint_reserve", "jb_adjoint_step",
@@ -101,6 +102,7 @@ def lib(path=None):
     L.jb_ens_total_cells.argtypes = [vp]
     L.jb_ens_total_cells.restype = ll
     L.jb_ens_configure.argtypes = [vp, i, i]
+    L.jb_ens_set_back_pressure.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.jb_ens_autotune.argtypes = [vp, i, vp, ip, ip, dpp]
     L.jb_ens_launch_shape.argtypes = [vp, ip, ip, ip, ip, ip]
     L.jb_ens_advance.argtypes = [vp, i, dp, vp]

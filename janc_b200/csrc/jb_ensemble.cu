@@ -666,6 +666,17 @@ int jb_ens_configure(jb_ensemble* e, int block, int blocks_per_sm) {
   return configure(e, block, blocks_per_sm);
 }
 
+int jb_ens_set_back_pressure(jb_ensemble* e, const double* pb) {
+  if (!e || !pb) return set_err(e, JB_ERR_ARG, "null pointer");
+  for (int i = 0; i < e->n; ++i)
+    if (!(pb[i] >= 0.0)) return set_err(e, JB_ERR_ARG, "back pressure of instance %d is not >= 0", i);
+  for (int i = 0; i < e->n; ++i) e->host_insts[i].g.Pb = pb[i];
+  drop_graph(e);
+  JB_ETRY(cudaMemcpy(e->d_insts, e->host_insts.data(), sizeof(jb_ens_inst) * e->n, cudaMemcpyHostToDevice),
+          "instance table copy");
+  return JB_OK;
+}
+
 int jb_ens_launch_shape(const jb_ensemble* e, int* block, int* blocks_per_sm, int* nblocks, int* max_tiles,
                         int* graph_mode) {
   if (!e) return JB_ERR_ARG;

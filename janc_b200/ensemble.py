@@ -52,10 +52,13 @@ class Ensemble:
     """``nx[i]`` cells of spacing ``dx[i]`` per instance; ``boundary`` is a
     (left, right) pair of boundary names for all instances or a list of
     pairs; ``cfl`` (scalar or list) > 0 selects CFL time steps, otherwise
-    ``dt`` (scalar or list) is the fixed step."""
+    ``dt`` (scalar or list) is the fixed step.  ``Pb`` (scalar or list) is
+    the back pressure of pressure-outlet sides (the reference's
+    theta['Pb']); required when an instance has one, as the reference's
+    boundary function requires it."""
 
     def __init__(self, nx, dx, boundary=("slip_wall", "zero_gradient"), cfl=0.1, dt=None,
-                 mechanism=_mech.DEFAULT_MECHANISM, nondim_config=None, precision="mixed", device=None):
+                 mechanism=_mech.DEFAULT_MECHANISM, nondim_config=None, precision="mixed", device=None, Pb=None):
         if precision not in ("fp64", "mixed"):
             raise KeyError("ensemble precision must be 'fp64' or 'mixed'")
         n = len(nx)
@@ -75,6 +78,9 @@ class Ensemble:
                 if name not in _native.BC_KIND:
                     raise KeyError(f"unknown boundary condition {name!r}")
                 kinds.append(_native.BC_KIND[name])
+        if Pb is None and _native.BC_KIND["pressure_outlet"] in kinds:
+            raise KeyError("Pb")
+        self.Pb = [float(v) for v in _per_instance(0.0 if Pb is None else Pb, n, "Pb")]
         self.cfl = [float(v) for v in _per_instance(0.0 if cfl is None else cfl, n, "cfl")]
         self.dt = [float(v) for v in _per_instance(0.0 if dt is None else dt, n, "dt")]
         self.precision = precision
@@ -90,6 +96,9 @@ class Ensemble:
                 (ctypes.c_double * n)(*self.dt), _native.PRECISION[precision], ctypes.byref(h))
         _native.check(rc, None, "jb_ens_create")
         self._h = h
+        if any(v != 0.0 for v in self.Pb):
+            _native.check(self._lib.jb_ens_set_back_pressure(h, (ctypes.c_double * n)(*self.Pb)), h,
+                          "jb_ens_set_back_pressure", ensemble=True)
         self._U, self._aux = [], []
         for i in range(n):
             pu, pa, m = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_int()

@@ -101,6 +101,55 @@ def test_ensemble_matches_single_solver(precision):
     print(f"bitwise equal instances: {n_exact} of {len(tubes)}")
 
 
+def test_ensemble_outlet_needs_back_pressure():
+    """An instance with a pressure outlet needs Pb (theta['Pb'] of the
+    reference's boundary function); checked before any device work."""
+    from janc_b200.ensemble import Ensemble
+    with pytest.raises(KeyError):
+        Ensemble([40, 50], [1e-4, 1e-4], boundary=[("slip_wall", "pressure_outlet"), ("slip_wall", "zero_gradient")])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ensemble_outlets_match_single_solver(precision):
+    """Instances with pressure outlets on either side (the outlet ghost strips
+    are written by the CTA that wrote the boundary cell in the mixed
+    ensemble, by the select pass in the fp64 one) against the single-case
+    Solver with the same back pressure."""
+    import torch
+    from janc_b200.ensemble import Ensemble
+    from janc_b200.solver import Solver
+    tubes = _small_tubes()[:4]
+    pairs = [("slip_wall", "pressure_outlet"), ("pressure_outlet", "zero_gradient"),
+             ("pressure_outlet", "pressure_outlet"), ("slip_wall", "zero_gradient")]
+    Pb = [0.5 * ATM, 0.8 * ATM, 0.6 * ATM, 0.0]
+    ens = Ensemble([t["nx"] for t in tubes], [t["dx"] for t in tubes], boundary=pairs, cfl=0.1,
+                   precision=precision, Pb=Pb)
+    states = []
+    for i, t in enumerate(tubes):
+        U, aux = ens.state_from_PTY(t["P"], t["T"], t["Y"])
+        ens.set_state(i, U, aux)
+        states.append((U, aux))
+    nsteps = 30
+    dts = ens.advance(nsteps, record_dt=True)
+    comb, per = ens.status()
+    assert comb == 0, per
+    for i, t in enumerate(tubes):
+        bc = {"left_boundary": pairs[i][0], "right_boundary": pairs[i][1]}
+        s = Solver(1, t["nx"], dx=t["dx"], boundary_config=bc, precision=precision)
+        U, aux, hist = s.advance(states[i][0], states[i][1], nsteps, cfl=0.1, theta={"Pb": Pb[i]})
+        Ue, auxe = ens.get_state(i)
+        torch.cuda.synchronize()
+        assert torch.all(torch.isfinite(Ue))
+        assert _max_rel(Ue, U) <= 1e-12, i
+        assert _max_rel(auxe, aux) <= 1e-12, i
+        np.testing.assert_allclose(dts[i].cpu().numpy(), hist.cpu().numpy(), rtol=1e-12)
+        if "pressure_outlet" in pairs[i]:
+            # the outlet has acted: the edge cell's pressure moved towards Pb
+            x = 0 if pairs[i][0] == "pressure_outlet" else -1
+            assert not torch.equal(Ue[:, x], states[i][0][:, x]), i
+
+
 @pytest.mark.gpu
 def test_ensemble_launch_shapes_agree():
     """The result does not depend on the block size or CTAs per SM, and two
