@@ -1653,9 +1653,13 @@ __host__ __device__ constexpr size_t smem1d_bytes(int nq) {
 }
 
 // One tile [x0, x0 + NT - 1) of a 1D stage (see k_flux2d for STAGE and R).
-// Every thread of the block must call it; returns this thread's Halley mask.
-// Pointers are plain (not restrict) because the persistent ensemble kernel
-// calls it on buffers written by other blocks of the same launch.
+// Every thread of the block must call it.  The new state's temperature is
+// finished as fin says: float64 tiles write the Halley iterates and return
+// this thread's mask bits; float tiles (the mixed variant) solve per cell
+// into fin.aux, fold the new state's wave speed (and, with fin.cfl, the CFL
+// candidate) into amx and dtm, and return status bits << 16.  Pointers are
+// plain (not restrict) because the persistent ensemble kernel calls it on
+// buffers written by other blocks of the same launch.
 template <int STAGE, class R, int NT, bool VISC = false, bool SW = false>
 __device__ __forceinline__ unsigned flux1d_tile(const MP& m, const Grid& g, const double* Uk,
                                                 const double* auxk, const double* Un, double* out,
