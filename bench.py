@@ -404,12 +404,24 @@ def _time_path(args, s, U0, aux0, theta, ncell, dist, clocks=None):
     if clocks:
         clocks.start()
         clocks.wait_first()
-        time.sleep(0.1)
+        # the same replayed steps for ~0.45 s up to the timed replay (every
+        # replay starts from the same state), so that the 200 ms sampler
+        # records the clocks and throttle reasons under this load right up
+        # to the timed region, which is a few ms long
+        t_soak = time.time() + 0.45
+        while time.time() < t_soak:
+            graph.replay()
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
     t_wall0 = time.time()
     graph.replay()
     torch.cuda.synchronize()
     t_wall = time.time() - t_wall0
     clk = clocks.stop() if clocks else None
+    if clk is not None:
+        clk["sampled"] = "under the same replayed steps during the 0.45 s before and through the timed replay"
     ms_total = max_over_ranks(dist, sum(a.elapsed_time(b) for a, b in ev))
     U, aux = Uk.clone(), auxk.clone()
     del graph
@@ -763,11 +775,19 @@ def amr_record(args, steps=10):
         blk = blk0
         for _ in range(max(args.warmup, 3)):
             blk = step(blk)
-        blk = blk0
         clocks = ClockSampler(dev)
         clocks.start()
         clocks.wait_first()
-        time.sleep(0.1)
+        # the timed steps repeated from the same blocks for ~0.45 s up to the
+        # timed region, so that the 200 ms sampler sees the clocks under
+        # this load (the timed region itself is a few tens of ms)
+        t_soak = time.time() + 0.45
+        while time.time() < t_soak:
+            blk = blk0
+            for _ in range(steps):
+                blk = step(blk)
+            torch.cuda.synchronize()
+        blk = blk0
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
