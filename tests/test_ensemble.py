@@ -98,7 +98,8 @@ def test_ensemble_matches_single_solver(precision):
         assert _max_rel(auxe, aux) <= 1e-12, i
         np.testing.assert_allclose(dts[i].cpu().numpy(), hist.cpu().numpy(), rtol=1e-12)
         n_exact += int(torch.equal(Ue, U) and torch.equal(auxe, aux))
-    print(f"bitwise equal instances: {n_exact} of {len(tubes)}")
+    # the same cell and tile bodies and order-independent reductions: exact
+    assert n_exact == len(tubes), f"bitwise equal instances: {n_exact} of {len(tubes)}"
 
 
 def test_ensemble_outlet_needs_back_pressure():
