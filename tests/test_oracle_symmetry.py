@@ -2,7 +2,7 @@
 oracle (CPU): the GPU tests at the benchmarks' full sizes
 (tests/test_full_size.py) rely on them.
 
-* Mirror symmetry: a channel with slip walls at both ends of each axis,
+* Mirror symmetry: a channel (and a 1D tube) with slip walls at both ends of each axis,
   mirrored in x or y with its normal momentum negated, steps to the mirror of
   the original's steps bit for bit (WENO5_JS.py's right-biased reconstruction
   is the left-biased one with the stencil reversed, and LF.py's split swaps
@@ -75,3 +75,29 @@ def test_oracle_rdc_ring_shift_invariance():
         Us, as_ = _run(o, _ring_shift(U0, k), _ring_shift(a0, k), 3, theta)
         np.testing.assert_array_equal(Us, _ring_shift(U, k))
         np.testing.assert_array_equal(as_, _ring_shift(a, k))
+
+
+def test_oracle_tube_mirror_symmetry():
+    """The 1D step (config-0 physics) of a tube with slip walls at both
+    ends, mirrored with its velocity negated."""
+    from janc_b200.mechanism import DEFAULT_MECHANISM
+    om = jo.load_mechanism(DEFAULT_MECHANISM)
+    n = 80
+    rng = np.random.default_rng(8)
+    P = np.full((1, n), 101325.0)
+    T = 300.0 * (1 + 0.02 * rng.uniform(-1, 1, (1, n)))
+    P[:, :6] = 30 * 101325.0
+    T[:, :6] = 3000.0
+    Y = np.tile(jo.stoich_Y(om, 1.0)[:, None], (1, n))
+    U0, a0 = jo.state_from_PTY(om, P, T, Y)
+    U0[1] += U0[0] * 20.0 * rng.uniform(-1, 1, U0[0].shape)
+    a0 = jo.update_aux(om, U0, a0)
+    o = jo.Solver(om, "1D", 5e-5, None, {"left_boundary": "slip_wall", "right_boundary": "slip_wall"}, 0.1)
+    U, a = _run(o, U0, a0, 4)
+    Um0 = U0[:, ::-1].copy()
+    Um0[1] = -Um0[1]
+    Um, am = _run(o, Um0, a0[:, ::-1].copy(), 4)
+    Ue = U[:, ::-1].copy()
+    Ue[1] = -Ue[1]
+    np.testing.assert_array_equal(Um, Ue)
+    np.testing.assert_array_equal(am, a[:, ::-1])
